@@ -1,0 +1,205 @@
+"""ctypes front end of ``libmercury_cuda.so``, mirroring the Fortran bridge.
+
+The reference host drives its CUDA backend through the ``gpu_*`` wrappers of
+mercury_gpu.f90 (gpu_select, gpu_push, gpu_advance, gpu_find_events,
+gpu_central, gpu_pull, gpu_old, gpu_bcoord/gpu_export, gpu_limits, gpu_free).
+:class:`Backend` exposes the same calls with the same argument meaning and
+failure behaviour (a nonzero status from the library raises
+:class:`BackendError` carrying the bridge's message, e.g. "CUDA integration
+step failed"), plus the library's multi-step extension.
+
+There is no CPU fallback here: if the library cannot be loaded, or no CUDA
+device is present when one is needed, the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+from .system import System
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libmercury_cuda.so"
+
+D = C.c_double
+I = C.c_int
+PD = C.POINTER(C.c_double)
+PI = C.POINTER(C.c_int)
+PI64 = C.POINTER(C.c_int64)
+
+ALGORITHMS = {"MVS": 1, "BS": 2, "BS2": 3, "RADAU": 4, "TEST": 9, "HYBRID": 10}
+
+EVENT_DTYPE = np.dtype([("i", np.int32), ("j", np.int32), ("kind", np.int32), ("now", np.int32),
+                        ("distance", np.float64), ("time", np.float64),
+                        ("xi", np.float64, 6), ("xj", np.float64, 6)])
+
+# Every symbol include/mercury_cuda.h and include/mercury_b200.h declare.
+DROP_IN_SYMBOLS = [
+    "mercury_cuda_available", "mercury_cuda_configure", "mercury_cuda_reset", "mercury_cuda_limits",
+    "mercury_cuda_export", "mercury_cuda_upload", "mercury_cuda_step", "mercury_cuda_download",
+    "mercury_cuda_events", "mercury_cuda_force", "mercury_cuda_hybrid_begin", "mercury_cuda_hybrid_finish",
+    "mercury_cuda_encounter_enter", "mercury_cuda_encounter_update", "mercury_cuda_encounter_exit",
+    "mercury_cuda_free",
+]
+EXTENSION_SYMBOLS = ["mercury_b200_mvs_advance", "mercury_b200_events", "mercury_b200_timing",
+                     "mercury_b200_set_launch", "mercury_b200_fp64_peak"]
+
+
+class BackendError(RuntimeError):
+    pass
+
+
+_lib: C.CDLL | None = None
+
+
+def load_library(path: Path | str | None = None) -> C.CDLL:
+    """Load the CUDA library (built in-tree by mercuda_b200.build)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise BackendError(f"{p} is missing: run `python -m mercuda_b200.build`")
+    L = C.CDLL(str(p))
+    L.mercury_cuda_available.restype = I
+    L.mercury_cuda_configure.argtypes = [I]
+    L.mercury_cuda_reset.argtypes = [I]
+    L.mercury_cuda_reset.restype = None
+    L.mercury_cuda_limits.argtypes = [PD]
+    L.mercury_cuda_export.argtypes = [D, I, PD, PD]
+    L.mercury_cuda_upload.argtypes = [I, I, I, I, PD, PD, PD, PD, PD, PD, PD]
+    L.mercury_cuda_step.argtypes = [D, PD, PD, D, PI64, PI64]
+    L.mercury_cuda_download.argtypes = [PD, PD, I]
+    L.mercury_cuda_events.argtypes = [D, D, D, C.POINTER(C.c_void_p), PI]
+    L.mercury_cuda_force.argtypes = [PD]
+    L.mercury_cuda_hybrid_begin.argtypes = [D, PD, I, I, PI, PI, PI, PI, PD, PD, PI64]
+    L.mercury_cuda_hybrid_finish.argtypes = [D, PD, PD, PD, PI64]
+    L.mercury_cuda_encounter_enter.argtypes = [I, I, PD, PD, PD, PD, PD, PD, I, PI, PI]
+    L.mercury_cuda_encounter_update.argtypes = [PD, PD, PD]
+    L.mercury_cuda_encounter_exit.restype = None
+    L.mercury_cuda_free.restype = None
+    L.mercury_b200_mvs_advance.argtypes = [D, D, I, D, I, PI]
+    L.mercury_b200_events.argtypes = [C.c_void_p, PI, I]
+    L.mercury_b200_timing.argtypes = [PD, PD, PI]
+    L.mercury_b200_set_launch.argtypes = [I, I]
+    L.mercury_b200_fp64_peak.argtypes = [PD, PD]
+    if path is None:
+        _lib = L
+    return L
+
+
+def _p(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous, "float64 C-contiguous array required"
+    return a.ctypes.data_as(PD)
+
+
+class Backend:
+    """One device context of libmercury_cuda.so, driven like mercury_gpu.f90."""
+
+    def __init__(self, algorithm: str | int = "MVS", lib: C.CDLL | None = None):
+        self.lib = lib or load_library()
+        self.algorithm = ALGORITHMS[algorithm] if isinstance(algorithm, str) else int(algorithm)
+        self.n = 0
+        self.nbig = 0
+        self.forces = 0
+        self.rejected = 0
+
+    # gpu_select (mercury_gpu.f90:115-138)
+    def available(self) -> bool:
+        return bool(self.lib.mercury_cuda_available())
+
+    def configure(self) -> None:
+        if not self.available():
+            raise BackendError("CUDA was requested but no CUDA device/build is available")
+        if self.lib.mercury_cuda_configure(self.algorithm) != 0:
+            raise BackendError("CUDA algorithm initialization failed")
+
+    # gpu_push (mercury_gpu.f90:139-151)
+    def upload(self, sys: System) -> None:
+        self.n, self.nbig = sys.n, sys.nbig
+        rc = self.lib.mercury_cuda_upload(sys.n, sys.nbig, int(sys.pn), sys.ngflag, _p(sys.m), _p(sys.x), _p(sys.v),
+                                          _p(sys.ngf), _p(sys.jcen), _p(sys.rce), _p(sys.rphys))
+        if rc != 0:
+            raise BackendError("CUDA state upload failed")
+
+    def reset(self, dtflag: int = 0) -> None:
+        self.lib.mercury_cuda_reset(int(dtflag))
+
+    # gpu_advance (mercury_gpu.f90:168-179)
+    def step(self, time: float, h: float, tol: float = 0.0, dtflag: int = 2):
+        self.reset(dtflag)
+        hh, hdid = D(h), D(0.0)
+        nf, nr = C.c_int64(0), C.c_int64(0)
+        if self.lib.mercury_cuda_step(time, C.byref(hh), C.byref(hdid), tol, C.byref(nf), C.byref(nr)) != 0:
+            raise BackendError("CUDA integration step failed")
+        self.forces += nf.value
+        self.rejected += nr.value
+        return hdid.value, hh.value
+
+    # gpu_refresh_events (mercury_gpu.f90:108-114)
+    def events(self, time: float, h: float, rcen: float) -> np.ndarray:
+        ptr, count = C.c_void_p(), I(0)
+        if self.lib.mercury_cuda_events(time, h, rcen, C.byref(ptr), C.byref(count)) != 0:
+            raise BackendError("CUDA event screening failed")
+        if count.value == 0:
+            return np.zeros(0, dtype=EVENT_DTYPE)
+        buf = (C.c_char * (count.value * EVENT_DTYPE.itemsize)).from_address(ptr.value)
+        return np.frombuffer(bytes(buf), dtype=EVENT_DTYPE).copy()
+
+    # gpu_pull / gpu_old (mercury_gpu.f90:180-185, 202-205)
+    def download(self, previous: bool = False):
+        x = np.zeros((self.n, 3))
+        v = np.zeros((self.n, 3))
+        if self.lib.mercury_cuda_download(_p(x), _p(v), int(previous)) != 0:
+            raise BackendError("CUDA previous state download failed" if previous else "CUDA download failed")
+        return x, v
+
+    # gpu_export (mercury_gpu.f90:186-191)
+    def export(self, h: float, physical: bool = True):
+        x = np.zeros((self.n, 3))
+        v = np.zeros((self.n, 3))
+        if self.lib.mercury_cuda_export(h, int(physical), _p(x), _p(v)) != 0:
+            raise BackendError("CUDA coordinate export failed")
+        return x, v
+
+    # gpu_limits (mercury_gpu.f90:88-92)
+    def limits(self, rce: np.ndarray) -> None:
+        if self.lib.mercury_cuda_limits(_p(np.ascontiguousarray(rce, dtype=np.float64))) != 0:
+            raise BackendError("CUDA encounter-radius update failed")
+
+    def force(self) -> np.ndarray:
+        a = np.zeros((self.n, 3))
+        if self.lib.mercury_cuda_force(_p(a)) != 0:
+            raise BackendError("CUDA force evaluation failed")
+        return a
+
+    def free(self) -> None:
+        self.lib.mercury_cuda_free()
+
+    # extension: fused multi-step MVS run
+    def mvs_advance(self, time: float, h: float, nsteps: int, rcen: float, steps_per_launch: int = 0):
+        nev = I(0)
+        if self.lib.mercury_b200_mvs_advance(time, h, int(nsteps), rcen, int(steps_per_launch), C.byref(nev)) != 0:
+            raise BackendError("CUDA integration step failed")
+        events = np.zeros(nev.value, dtype=EVENT_DTYPE)
+        steps = np.zeros(nev.value, dtype=np.int32)
+        if nev.value:
+            self.lib.mercury_b200_events(events.ctypes.data_as(C.c_void_p), steps.ctypes.data_as(PI), nev.value)
+        return events, steps
+
+    def timing(self):
+        a, k, n = D(0.0), D(0.0), I(0)
+        self.lib.mercury_b200_timing(C.byref(a), C.byref(k), C.byref(n))
+        return {"advance_ms": a.value, "particle_kernel_ms": k.value, "particle_launches": n.value}
+
+    def fp64_peak(self):
+        tf, ms = D(0.0), D(0.0)
+        if self.lib.mercury_b200_fp64_peak(C.byref(tf), C.byref(ms)) != 0:
+            raise BackendError("FP64 peak probe failed")
+        return tf.value
+
+    def set_launch(self, threads: int = -1, steps_per_launch: int = -1) -> None:
+        if self.lib.mercury_b200_set_launch(int(threads), int(steps_per_launch)) != 0:
+            raise BackendError("invalid launch shape")

@@ -1,0 +1,684 @@
+// The drop-in C ABI (include/mercury_cuda.h) and the MVS extension entry
+// points (include/mercury_b200.h): host orchestration of the device context.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "../../include/mercury_b200.h"
+#include "context.cuh"
+#include "mvs_device.cuh"
+
+namespace mb200 {
+
+Context& ctx() {
+    static Context c;
+    return c;
+}
+
+int report(const std::exception& e) {
+    std::fprintf(stderr, "MERCURY CUDA: %s\n", e.what());
+    return 1;
+}
+
+namespace {
+
+__global__ void scatter_kernel(const double* rows, int n, int comps, int nbig, double* big, int bs, double* part,
+                               int ps) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    for (int c = 0; c < comps; ++c) {
+        const double v = rows[(size_t)j * comps + c];
+        if (j < nbig) {
+            if (big) big[(size_t)c * bs + j] = v;
+        } else {
+            part[(size_t)c * ps + (j - nbig)] = v;
+        }
+    }
+}
+
+__global__ void gather_kernel(double* rows, int n, int comps, int nbig, const double* big, int bs,
+                              const double* part, int ps) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    for (int c = 0; c < comps; ++c)
+        rows[(size_t)j * comps + c] = j < nbig ? big[(size_t)c * bs + j] : part[(size_t)c * ps + (j - nbig)];
+}
+
+// mce_cent over every body for the drop-in events call (mercury6_2.for:1059-1167):
+// start-of-step states from the previous buffers, end states from the current.
+struct CentralArgs {
+    int nbig, np, npcap;
+    double mu, h, rcen;
+    const double *big0, *big1, *part0, *part1, *pm, *mbig;
+    MercuryEvent* events;
+    int* event_step;
+    int cap;
+    DeviceStatus* status;
+};
+
+__global__ void central_kernel(CentralArgs A) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nb = A.nbig - 1, total = nb + A.np;
+    bool hit = false;
+    double temp = 0.0;
+    int id = 0;
+    if (q < total) {
+        double3 p0, u0, p1, u1;
+        double mj;
+        if (q < nb) {
+            const int k = q + 1, N = A.nbig;
+            p0 = make_double3(A.big0[k], A.big0[N + k], A.big0[2 * N + k]);
+            u0 = make_double3(A.big0[3 * N + k], A.big0[4 * N + k], A.big0[5 * N + k]);
+            p1 = make_double3(A.big1[k], A.big1[N + k], A.big1[2 * N + k]);
+            u1 = make_double3(A.big1[3 * N + k], A.big1[4 * N + k], A.big1[5 * N + k]);
+            mj = A.mbig[k];
+            id = k + 1;
+        } else {
+            const int p = q - nb, S = A.npcap;
+            p0 = make_double3(A.part0[p], A.part0[S + p], A.part0[2 * S + p]);
+            u0 = make_double3(A.part0[3 * S + p], A.part0[4 * S + p], A.part0[5 * S + p]);
+            p1 = make_double3(A.part1[p], A.part1[S + p], A.part1[2 * S + p]);
+            u1 = make_double3(A.part1[3 * S + p], A.part1[4 * S + p], A.part1[5 * S + p]);
+            mj = A.pm[p];
+            id = A.nbig + p + 1;
+        }
+        hit = central_impact(p0, u0, p1, u1, A.mu, mj, A.h, A.rcen, temp);
+    }
+    if (hit) {
+        const int slot = atomicAdd(&A.status->events, 1);
+        if (slot < A.cap) {
+            MercuryEvent rec = {};
+            rec.i = 1;
+            rec.j = id;
+            rec.kind = EV_CENTRAL;
+            rec.time = temp;
+            rec.distance = A.rcen;
+            store_event(A.events + slot, rec);
+            A.event_step[slot] = 0;
+        } else {
+            atomicExch(&A.status->overflow, 1);
+        }
+    }
+}
+
+int blocks(int n, int t = 256) { return (n + t - 1) / t; }
+
+bool is_mvs(int alg) { return alg == 1 || alg == 9; }
+
+void require_system() {
+    if (ctx().n <= 0) throw std::runtime_error("no system uploaded");
+}
+
+void ensure_events(int cap) {
+    Context& c = ctx();
+    if ((int)c.events.n < cap) {
+        c.events.reserve(cap);
+        c.event_step.reserve(cap);
+    }
+}
+
+void read_status() {
+    Context& c = ctx();
+    check(cudaMemcpyAsync(c.status_host, c.status.p, sizeof(DeviceStatus), cudaMemcpyDeviceToHost, c.stream), "status");
+    check(cudaStreamSynchronize(c.stream), "step");
+}
+
+// Fixed-size table space for a run of `rows` table rows and `steps` detail rows.
+void ensure_tables(int rows, int steps) {
+    Context& c = ctx();
+    const int nb = c.nbig - 1;
+    c.tab.reserve((size_t)rows * tab_stride(nb));
+    c.detail.reserve((size_t)std::max(1, steps) * std::max(1, nb) * TAB_DETAIL);
+}
+
+MvsBigArgs big_args(int in, int out, int nsteps, int reset, int central, int step0, double h, double rcen,
+                    double* tab, double* detail) {
+    Context& c = ctx();
+    MvsBigArgs a{};
+    a.nbig = c.nbig;
+    a.ngflag = c.ngflag;
+    a.obl = (c.jcen[0] != 0.0 || c.jcen[1] != 0.0 || c.jcen[2] != 0.0);
+    a.reset = reset;
+    a.nsteps = nsteps;
+    a.central = central;
+    a.step0 = step0;
+    for (int k = 0; k < 3; ++k) a.jcen[k] = c.jcen[k];
+    a.h = h;
+    a.rcen = rcen;
+    a.m = c.mbig.p;
+    a.rce = c.rcebig.p;
+    a.rphys = c.rphysbig.p;
+    a.ngf = c.ngfbig.p;
+    a.in = c.big(in);
+    a.out = c.big(out);
+    a.tab = tab;
+    a.detail = detail;
+    a.events = c.events.p;
+    a.event_step = c.event_step.p;
+    a.event_cap = (int)c.events.n;
+    a.status = c.status.p;
+    return a;
+}
+
+MvsParticleArgs particle_args(int in, int out, int nsteps, int reset, int central, int step0, double h,
+                              double rcen, const double* tab, const double* detail) {
+    Context& c = ctx();
+    MvsParticleArgs a{};
+    a.np = c.np;
+    a.npcap = c.npcap;
+    a.nb = c.nbig - 1;
+    a.nbig = c.nbig;
+    a.nsteps = nsteps;
+    a.reset = reset;
+    a.central = central;
+    a.step0 = step0;
+    a.ngf_on = (c.ngflag == 1 || c.ngflag == 3);
+    a.mu = c.m_host[0];
+    a.h = h;
+    a.rcen = rcen;
+    for (int k = 0; k < 3; ++k) a.jcen[k] = c.jcen[k];
+    a.xin = c.pstate[in].p;
+    a.xout = c.pstate[out].p;
+    a.m = c.pm.p;
+    a.rce = c.prce.p;
+    a.rphys = c.prphys.p;
+    a.ngf = c.pngf.p;
+    a.tab = tab;
+    a.detail = detail;
+    a.events = c.events.p;
+    a.event_step = c.event_step.p;
+    a.event_cap = (int)c.events.n;
+    a.status = c.status.p;
+    return a;
+}
+
+// One MVS step (mdt_mvs) of the whole system: Big-body CTA then the particle
+// kernel, double-buffered so the pre-step state stays available. Pair events
+// are left in the event buffer with tmin in their time field.
+void mvs_step_once(double h) {
+    Context& c = ctx();
+    for (int attempt = 0;; ++attempt) {
+        ensure_tables(2, 1);
+        check(cudaMemsetAsync(c.status.p, 0, sizeof(DeviceStatus), c.stream), "memset");
+        const int in = c.cur, out = 1 - c.cur;
+        const int reset = c.reset ? 1 : 0;
+        launch_mvs_big(big_args(in, out, 1, reset, 0, 0, h, 0.0, c.tab.p, c.detail.p), c.stream);
+        if (c.np > 0)
+            launch_mvs_particles(particle_args(in, out, 1, reset, 0, 0, h, 0.0, c.tab.p, c.detail.p), c.stream,
+                                 c.particle_threads);
+        check(cudaGetLastError(), "launch");
+        read_status();
+        if (c.status_host->fault) throw std::runtime_error("MVS force failed");
+        if (c.status_host->overflow) {
+            if (attempt > 8) throw std::runtime_error("event buffer growth failed");
+            ensure_events(std::max(2 * (int)c.events.n, c.status_host->events + 1024));
+            continue;  // the input buffers are untouched: redo the step
+        }
+        c.nforces += 1 + reset;
+        c.pair_events = c.status_host->events;
+        c.cur = out;
+        c.reset = false;
+        c.stepped = true;
+        return;
+    }
+}
+
+void sort_events(std::vector<MercuryEvent>& ev, std::vector<int>* steps) {
+    std::vector<size_t> idx(ev.size());
+    for (size_t k = 0; k < idx.size(); ++k) idx[k] = k;
+    auto key = [&](size_t k) {
+        const MercuryEvent& e = ev[k];
+        const int s = steps ? (*steps)[k] : 0;
+        return std::make_tuple(s, std::min(e.i, e.j), std::max(e.i, e.j));
+    };
+    std::stable_sort(idx.begin(), idx.end(), [&](size_t a, size_t b) { return key(a) < key(b); });
+    std::vector<MercuryEvent> out(ev.size());
+    std::vector<int> so(ev.size());
+    for (size_t k = 0; k < idx.size(); ++k) {
+        out[k] = ev[idx[k]];
+        if (steps) so[k] = (*steps)[idx[k]];
+    }
+    ev.swap(out);
+    if (steps) steps->swap(so);
+}
+
+void download_buffer(int which, double* xx, double* vv) {
+    Context& c = ctx();
+    c.transfer.reserve((size_t)6 * c.n);
+    // x and v rows as two 3-component passes
+    for (int part = 0; part < 2; ++part) {
+        const double* big = c.bigstate[which].p + 3 * part * c.nbig;
+        const double* prt = c.pstate[which].p + (size_t)3 * part * c.npcap;
+        gather_kernel<<<blocks(c.n), 256, 0, c.stream>>>(c.transfer.p, c.n, 3, c.nbig, big, c.nbig, prt, c.npcap);
+        check(cudaMemcpyAsync(part ? vv : xx, c.transfer.p, sizeof(double) * 3 * c.n, cudaMemcpyDeviceToHost,
+                              c.stream),
+              "download");
+        check(cudaStreamSynchronize(c.stream), "download");
+    }
+}
+
+}  // namespace
+
+void scatter_rows(const double* rows, int n, int comps, int nbig, double* big, int big_stride, double* part,
+                  int part_stride, cudaStream_t s) {
+    scatter_kernel<<<blocks(n), 256, 0, s>>>(rows, n, comps, nbig, big, big_stride, part, part_stride);
+}
+void gather_rows(double* rows, int n, int comps, int nbig, const double* big, int big_stride, const double* part,
+                 int part_stride, cudaStream_t s) {
+    gather_kernel<<<blocks(n), 256, 0, s>>>(rows, n, comps, nbig, big, big_stride, part, part_stride);
+}
+
+}  // namespace mb200
+
+using namespace mb200;
+
+extern "C" {
+
+int mercury_cuda_available(void) {
+    int n = 0;
+    return cudaGetDeviceCount(&n) == cudaSuccess && n > 0;
+}
+
+void mercury_cuda_free(void) {
+    Context& c = ctx();
+    c.release_all();
+}
+
+int mercury_cuda_configure(int method) {
+    if (method != 1 && method != 2 && method != 3 && method != 4 && method != 9 && method != 10) return 1;
+    Context& c = ctx();
+    try {
+        if (!is_mvs(method)) throw std::runtime_error("algorithm not available in this build");
+        if (method != c.algorithm) mercury_cuda_free();
+        c.algorithm = method;
+        c.reset = true;
+        return 0;
+    } catch (const std::exception& e) {
+        return report(e);
+    }
+}
+
+void mercury_cuda_reset(int flag) {
+    if (flag != 2) ctx().reset = true;
+}
+
+int mercury_cuda_upload(int n, int nbig, int pn, int ngflag, const double* m, const double* xx, const double* vv,
+                        const double* ng, const double* jcen, const double* limits, const double* radii) {
+    Context& c = ctx();
+    try {
+        if (n < 1 || nbig < 1 || nbig > n) throw std::runtime_error("invalid body counts");
+        if (is_mvs(c.algorithm) && nbig > 512) throw std::runtime_error("more than 512 Big bodies");
+        c.ensure_streams();
+        bool obl = jcen[0] != 0.0 || jcen[1] != 0.0 || jcen[2] != 0.0;
+        if (is_mvs(c.algorithm) && obl)
+            for (int j = nbig; j < n; ++j)
+                if (m[j] != 0.0)
+                    throw std::runtime_error("MVS with central-body oblateness and massive Small bodies");
+        c.n = n;
+        c.nbig = nbig;
+        c.np = n - nbig;
+        c.npcap = std::max(2, (c.np + 1) & ~1);
+        c.pn = pn;
+        c.ngflag = ngflag;
+        for (int k = 0; k < 3; ++k) c.jcen[k] = jcen[k];
+        c.m_host.assign(m, m + n);
+        c.mbig.reserve(nbig);
+        c.rcebig.reserve(nbig);
+        c.rphysbig.reserve(nbig);
+        c.ngfbig.reserve((size_t)5 * nbig);
+        for (int k = 0; k < 2; ++k) {
+            c.bigstate[k].reserve((size_t)9 * nbig);
+            c.pstate[k].reserve((size_t)9 * c.npcap);
+        }
+        c.pm.reserve(c.npcap);
+        c.prce.reserve(c.npcap);
+        c.prphys.reserve(c.npcap);
+        c.pngf.reserve((size_t)5 * c.npcap);
+        c.status.reserve(1);
+        ensure_events(std::max(4096, c.np / 64));
+        c.transfer.reserve((size_t)6 * n);
+        cudaStream_t s = c.stream;
+        // zero padding and cached accelerations
+        check(cudaMemsetAsync(c.pstate[0].p, 0, sizeof(double) * 9 * c.npcap, s), "memset");
+        check(cudaMemsetAsync(c.pstate[1].p, 0, sizeof(double) * 9 * c.npcap, s), "memset");
+        check(cudaMemsetAsync(c.bigstate[0].p, 0, sizeof(double) * 9 * nbig, s), "memset");
+        check(cudaMemsetAsync(c.bigstate[1].p, 0, sizeof(double) * 9 * nbig, s), "memset");
+        check(cudaMemsetAsync(c.pm.p, 0, sizeof(double) * c.npcap, s), "memset");
+        check(cudaMemsetAsync(c.prce.p, 0, sizeof(double) * c.npcap, s), "memset");
+        check(cudaMemsetAsync(c.prphys.p, 0, sizeof(double) * c.npcap, s), "memset");
+        check(cudaMemsetAsync(c.pngf.p, 0, sizeof(double) * 5 * c.npcap, s), "memset");
+        c.cur = 0;
+        // positions and velocities
+        for (int part = 0; part < 2; ++part) {
+            check(cudaMemcpyAsync(c.transfer.p, part ? vv : xx, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s),
+                  "upload");
+            scatter_rows(c.transfer.p, n, 3, nbig, c.bigstate[0].p + 3 * part * nbig, nbig,
+                         c.pstate[0].p + (size_t)3 * part * c.npcap, c.npcap, s);
+            check(cudaStreamSynchronize(s), "upload");
+        }
+        // per-body scalars: masses, radii
+        const double* scalars[3] = {m, limits, radii};
+        double* bigdst[3] = {c.mbig.p, c.rcebig.p, c.rphysbig.p};
+        double* pdst[3] = {c.pm.p, c.prce.p, c.prphys.p};
+        for (int q = 0; q < 3; ++q) {
+            check(cudaMemcpyAsync(c.transfer.p, scalars[q], sizeof(double) * n, cudaMemcpyHostToDevice, s), "upload");
+            scatter_rows(c.transfer.p, n, 1, nbig, bigdst[q], nbig, pdst[q], c.npcap, s);
+            check(cudaStreamSynchronize(s), "upload");
+        }
+        // ngf: Big rows stay interleaved (5 per body); particles become SoA
+        check(cudaMemcpyAsync(c.ngfbig.p, ng, sizeof(double) * 5 * nbig, cudaMemcpyHostToDevice, s), "upload");
+        c.transfer.reserve((size_t)6 * n);
+        check(cudaMemcpyAsync(c.transfer.p, ng, sizeof(double) * 5 * n, cudaMemcpyHostToDevice, s), "upload");
+        scatter_rows(c.transfer.p, n, 5, nbig, nullptr, 0, c.pngf.p, c.npcap, s);
+        check(cudaStreamSynchronize(s), "upload");
+        check(cudaGetLastError(), "upload");
+        c.reset = true;
+        c.stepped = false;
+        return 0;
+    } catch (const std::exception& e) {
+        return report(e);
+    }
+}
+
+int mercury_cuda_step(double time, double* h, double* hdid, double tol, int64_t* forces, int64_t* rejected) {
+    (void)time;
+    (void)tol;
+    Context& c = ctx();
+    try {
+        require_system();
+        *rejected = 0;
+        const int64_t before = c.nforces;
+        if (!is_mvs(c.algorithm)) throw std::runtime_error("algorithm not available in this build");
+        mvs_step_once(*h);
+        *hdid = *h;
+        *forces = c.nforces - before;
+        return 0;
+    } catch (const std::exception& e) {
+        return report(e);
+    }
+}
+
+int mercury_cuda_download(double* xx, double* vv, int previous) {
+    Context& c = ctx();
+    try {
+        require_system();
+        download_buffer(previous ? 1 - c.cur : c.cur, xx, vv);
+        return 0;
+    } catch (const std::exception& e) {
+        return report(e);
+    }
+}
+
+int mercury_cuda_events(double time, double h, double rcen, const MercuryEvent** result, int* count) {
+    Context& c = ctx();
+    try {
+        require_system();
+        const int prev = 1 - c.cur;
+        for (int attempt = 0;; ++attempt) {
+            // restart the counter after the step's pair events, then screen for central impacts
+            DeviceStatus st = {0, c.pair_events, 0, 0};
+            check(cudaMemcpyAsync(c.status.p, &st, sizeof(st), cudaMemcpyHostToDevice, c.stream), "status");
+            const int total = c.nbig - 1 + c.np;
+            if (c.stepped && total > 0) {
+                CentralArgs a;
+                a.nbig = c.nbig;
+                a.np = c.np;
+                a.npcap = c.npcap;
+                a.mu = c.m_host[0];
+                a.h = h;
+                a.rcen = rcen;
+                a.big0 = c.bigstate[prev].p;
+                a.big1 = c.bigstate[c.cur].p;
+                a.part0 = c.pstate[prev].p;
+                a.part1 = c.pstate[c.cur].p;
+                a.pm = c.pm.p;
+                a.mbig = c.mbig.p;
+                a.events = c.events.p;
+                a.event_step = c.event_step.p;
+                a.cap = (int)c.events.n;
+                a.status = c.status.p;
+                central_kernel<<<blocks(total), 256, 0, c.stream>>>(a);
+                check(cudaGetLastError(), "central");
+            }
+            read_status();
+            if (!c.status_host->overflow) break;
+            if (attempt > 8) throw std::runtime_error("event buffer growth failed");
+            // keep the pair events: copy them out, grow, copy back
+            std::vector<MercuryEvent> keep(c.pair_events);
+            if (c.pair_events)
+                check(cudaMemcpy(keep.data(), c.events.p, sizeof(MercuryEvent) * c.pair_events, cudaMemcpyDeviceToHost),
+                      "events");
+            DBuf<MercuryEvent> grown;
+            grown.reserve(std::max(2 * (int)c.events.n, c.status_host->events + 1024));
+            c.events.release();
+            c.events = grown;
+            c.event_step.release();
+            c.event_step.reserve(c.events.n);
+            if (c.pair_events)
+                check(cudaMemcpy(c.events.p, keep.data(), sizeof(MercuryEvent) * c.pair_events, cudaMemcpyHostToDevice),
+                      "events");
+        }
+        const int nev = c.stepped ? c.status_host->events : 0;
+        c.host_events.resize(nev);
+        if (nev)
+            check(cudaMemcpy(c.host_events.data(), c.events.p, sizeof(MercuryEvent) * nev, cudaMemcpyDeviceToHost),
+                  "events");
+        for (auto& e : c.host_events) {
+            if (e.kind == EV_CENTRAL) e.time = time - h + e.time;
+            else e.time = e.time + time;
+        }
+        sort_events(c.host_events, nullptr);
+        *count = nev;
+        *result = c.host_events.data();
+        return 0;
+    } catch (const std::exception& e) {
+        return report(e);
+    }
+}
+
+int mercury_cuda_force(double* a) {
+    (void)a;
+    try {
+        throw std::runtime_error("force interface not available in this build");
+    } catch (const std::exception& e) {
+        return report(e);
+    }
+}
+
+int mercury_cuda_export(double h, int physical, double* xx, double* vv) {
+    (void)h;
+    Context& c = ctx();
+    try {
+        require_system();
+        if (physical && c.algorithm == 1) throw std::runtime_error("output corrector not available in this build");
+        download_buffer(c.cur, xx, vv);
+        return 0;
+    } catch (const std::exception& e) {
+        return report(e);
+    }
+}
+
+int mercury_cuda_limits(const double* limits) {
+    Context& c = ctx();
+    try {
+        require_system();
+        check(cudaMemcpyAsync(c.transfer.p, limits, sizeof(double) * c.n, cudaMemcpyHostToDevice, c.stream), "limits");
+        scatter_rows(c.transfer.p, c.n, 1, c.nbig, c.rcebig.p, c.nbig, c.prce.p, c.npcap, c.stream);
+        check(cudaStreamSynchronize(c.stream), "limits");
+        return 0;
+    } catch (const std::exception& e) {
+        return report(e);
+    }
+}
+
+int mercury_cuda_hybrid_begin(double, const double*, int, int, int*, int*, int*, int*, double*, double*, int64_t*) {
+    std::fprintf(stderr, "MERCURY CUDA: HYBRID not available in this build\n");
+    return 1;
+}
+int mercury_cuda_hybrid_finish(double, const double*, const double*, const double*, int64_t*) {
+    std::fprintf(stderr, "MERCURY CUDA: HYBRID not available in this build\n");
+    return 1;
+}
+int mercury_cuda_encounter_enter(int, int, const double*, const double*, const double*, const double*,
+                                 const double*, const double*, int, const int*, const int*) {
+    std::fprintf(stderr, "MERCURY CUDA: HYBRID not available in this build\n");
+    return 1;
+}
+int mercury_cuda_encounter_update(const double*, const double*, const double*) {
+    std::fprintf(stderr, "MERCURY CUDA: HYBRID not available in this build\n");
+    return 1;
+}
+void mercury_cuda_encounter_exit(void) {}
+
+// ---------------------------------------------------------------- extensions
+
+int mercury_b200_mvs_advance(double time, double h, int nsteps, double rcen, int steps_per_launch,
+                             int* nevents) {
+    (void)time;
+    Context& c = ctx();
+    try {
+        require_system();
+        if (!is_mvs(c.algorithm)) throw std::runtime_error("MVS advance needs algorithm 1 or 9");
+        if (nsteps < 1) throw std::runtime_error("nsteps must be positive");
+        const int nb = c.nbig - 1;
+        int K = steps_per_launch > 0 ? steps_per_launch : (c.steps_per_launch > 0 ? c.steps_per_launch : 0);
+        if (K <= 0) K = mvs_max_steps_per_launch(nb);
+        K = std::min(K, mvs_max_steps_per_launch(nb));
+        K = std::max(1, std::min(K, nsteps));
+        const int nchunks = (nsteps + K - 1) / K;
+        const int stride = tab_stride(nb);
+        ensure_tables(nsteps + nchunks, nsteps);
+        if ((int)c.chunk_done.size() < nchunks) {
+            size_t old = c.chunk_done.size();
+            c.chunk_done.resize(nchunks);
+            c.kt0.resize(nchunks);
+            c.kt1.resize(nchunks);
+            for (size_t k = old; k < (size_t)nchunks; ++k) {
+                check(cudaEventCreateWithFlags(&c.chunk_done[k], cudaEventDisableTiming), "event");
+                check(cudaEventCreate(&c.kt0[k]), "event");
+                check(cudaEventCreate(&c.kt1[k]), "event");
+            }
+        }
+        // keep the starting state so that an event-buffer overflow can be redone
+        c.snapshot.reserve((size_t)9 * c.npcap + 9 * c.nbig);
+        check(cudaMemcpyAsync(c.snapshot.p, c.pstate[c.cur].p, sizeof(double) * 9 * c.npcap, cudaMemcpyDeviceToDevice,
+                              c.stream),
+              "snapshot");
+        check(cudaMemcpyAsync(c.snapshot.p + 9 * c.npcap, c.bigstate[c.cur].p, sizeof(double) * 9 * c.nbig,
+                              cudaMemcpyDeviceToDevice, c.stream),
+              "snapshot");
+        const bool reset0 = c.reset;
+        for (int attempt = 0;; ++attempt) {
+            check(cudaMemsetAsync(c.status.p, 0, sizeof(DeviceStatus), c.stream), "memset");
+            check(cudaEventRecord(c.t0, c.stream), "event");
+            check(cudaStreamWaitEvent(c.stream_big, c.t0, 0), "wait");
+            int bcur = c.cur, pcur = c.cur;
+            size_t row = 0;
+            for (int ch = 0; ch < nchunks; ++ch) {
+                const int s0 = ch * K, ks = std::min(K, nsteps - s0);
+                const int reset = (ch == 0 && reset0) ? 1 : 0;
+                double* tab = c.tab.p + row * stride;
+                double* det = c.detail.p + (size_t)s0 * std::max(1, nb) * TAB_DETAIL;
+                launch_mvs_big(big_args(bcur, 1 - bcur, ks, reset, 1, s0, h, rcen, tab, det), c.stream_big);
+                check(cudaEventRecord(c.chunk_done[ch], c.stream_big), "event");
+                bcur = 1 - bcur;
+                if (c.np > 0) {
+                    check(cudaStreamWaitEvent(c.stream, c.chunk_done[ch], 0), "wait");
+                    check(cudaEventRecord(c.kt0[ch], c.stream), "event");
+                    launch_mvs_particles(particle_args(pcur, 1 - pcur, ks, reset, 1, s0, h, rcen, tab, det), c.stream,
+                                         c.particle_threads);
+                    check(cudaEventRecord(c.kt1[ch], c.stream), "event");
+                }
+                pcur = 1 - pcur;
+                row += ks + 1;
+            }
+            check(cudaStreamWaitEvent(c.stream, c.chunk_done[nchunks - 1], 0), "wait");
+            check(cudaEventRecord(c.t1, c.stream), "event");
+            check(cudaGetLastError(), "launch");
+            read_status();
+            if (c.status_host->fault) throw std::runtime_error("MVS force failed");
+            if (!c.status_host->overflow) {
+                check(cudaEventElapsedTime(&c.last_advance_ms, c.t0, c.t1), "timer");
+                double ksum = 0.0;
+                if (c.np > 0)
+                    for (int ch = 0; ch < nchunks; ++ch) {
+                        float ms = 0.0f;
+                        check(cudaEventElapsedTime(&ms, c.kt0[ch], c.kt1[ch]), "timer");
+                        ksum += ms;
+                    }
+                c.last_particle_kernel_ms = ksum;
+                c.last_particle_launches = c.np > 0 ? nchunks : 0;
+                // both state sets end in the same buffer index parity
+                c.cur = pcur;  // Big and particle buffers flip together
+                break;
+            }
+            if (attempt > 8) throw std::runtime_error("event buffer growth failed");
+            ensure_events(std::max(2 * (int)c.events.n, c.status_host->events + 1024));
+            check(cudaMemcpyAsync(c.pstate[c.cur].p, c.snapshot.p, sizeof(double) * 9 * c.npcap,
+                                  cudaMemcpyDeviceToDevice, c.stream),
+                  "restore");
+            check(cudaMemcpyAsync(c.bigstate[c.cur].p, c.snapshot.p + 9 * c.npcap, sizeof(double) * 9 * c.nbig,
+                                  cudaMemcpyDeviceToDevice, c.stream),
+                  "restore");
+        }
+        c.nforces += nsteps + (reset0 ? 1 : 0);
+        c.reset = false;
+        c.stepped = false;  // per-step event/previous semantics do not apply after a multi-step run
+        c.pair_events = 0;
+        const int nev = c.status_host->events;
+        c.host_events.resize(nev);
+        c.host_steps.resize(nev);
+        if (nev) {
+            check(cudaMemcpy(c.host_events.data(), c.events.p, sizeof(MercuryEvent) * nev, cudaMemcpyDeviceToHost),
+                  "events");
+            check(cudaMemcpy(c.host_steps.data(), c.event_step.p, sizeof(int) * nev, cudaMemcpyDeviceToHost), "events");
+        }
+        // absolute times: the driver's clock advances by time = time + h per step
+        std::vector<double> tend(nsteps);
+        double t = time;
+        for (int s = 0; s < nsteps; ++s) {
+            t = t + h;
+            tend[s] = t;
+        }
+        for (int k = 0; k < nev; ++k) {
+            MercuryEvent& e = c.host_events[k];
+            const double te = tend[c.host_steps[k]];
+            if (e.kind == EV_CENTRAL) e.time = te - h + e.time;
+            else e.time = e.time + te;
+        }
+        sort_events(c.host_events, &c.host_steps);
+        *nevents = nev;
+        return 0;
+    } catch (const std::exception& e) {
+        return report(e);
+    }
+}
+
+int mercury_b200_events(MercuryEvent* dst, int* steps, int cap) {
+    Context& c = ctx();
+    const int nev = (int)c.host_events.size();
+    const int k = std::min(cap, nev);
+    if (k > 0) std::memcpy(dst, c.host_events.data(), sizeof(MercuryEvent) * k);
+    if (steps && k > 0 && (int)c.host_steps.size() >= k) std::memcpy(steps, c.host_steps.data(), sizeof(int) * k);
+    return nev;
+}
+
+int mercury_b200_timing(double* advance_ms, double* particle_kernel_ms, int* particle_launches) {
+    Context& c = ctx();
+    if (advance_ms) *advance_ms = c.last_advance_ms;
+    if (particle_kernel_ms) *particle_kernel_ms = c.last_particle_kernel_ms;
+    if (particle_launches) *particle_launches = c.last_particle_launches;
+    return 0;
+}
+
+int mercury_b200_set_launch(int particle_threads, int steps_per_launch) {
+    Context& c = ctx();
+    if (particle_threads > 0) {
+        if (particle_threads % 32 != 0 || particle_threads > 1024) return 1;
+        c.particle_threads = particle_threads;
+    }
+    if (steps_per_launch >= 0) c.steps_per_launch = steps_per_launch;
+    return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,37 @@
+// Shared definitions of the B200 test-particle library.
+//
+// Every translation unit is compiled with --fmad=false and IEEE division and
+// square root, so each FP64 statement rounds exactly as the Fortran reference
+// (built with -ffp-contract=off) rounds it; the statement order of each routine
+// follows the Fortran routine it restates (cited at each function).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/mercury_cuda.h"
+
+namespace mb200 {
+
+constexpr double K2 = 2.959122082855911e-4;
+constexpr double HUGE_VAL_F = 9.9e29;          // mercury.inc HUGE
+constexpr double PI_D = 3.141592653589793;
+constexpr double TWOPI_SWIFT = 2.0 * PI_D;     // swift.inc TWOPI
+constexpr double DANBYB = 1.0e-13;             // swift.inc DANBYB
+// Speed of light in AU/day from the exact SI value and the IAU 2012 au.
+constexpr double C_LIGHT = 299792458.0 * 86400.0 / 1.495978707e11;
+
+// Event kinds of the reference ABI (mercury_cuda.h:7-11, mercury_gpu.f90:215-246).
+constexpr int EV_CLOSE = 1, EV_NEAR = 2, EV_HIT = 4, EV_CENTRAL = 8;
+
+// Device-side status word written by kernels (never a trap): bit 0 non-finite
+// force, bit 1 undefined non-gravitational direction, bit 2 bound exceeded.
+struct DeviceStatus {
+    int fault;
+    int events;        // pair/central events claimed (may exceed capacity)
+    int overflow;      // 1 if any event slot was beyond capacity
+    int pad;
+};
+
+__device__ __forceinline__ void raise_fault(DeviceStatus* st, int bit) { atomicOr(&st->fault, bit); }
+
+}  // namespace mb200

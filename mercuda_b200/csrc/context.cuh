@@ -1,0 +1,128 @@
+// Host-side state of the library: one device context, as the reference's
+// single global context (mercury_cuda.cu:16-33), plus the helpers every entry
+// point uses (allocation, error reporting, layout kernels).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "mvs.cuh"
+
+namespace mb200 {
+
+struct CudaError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+inline void check(cudaError_t code, const char* what = nullptr) {
+    if (code != cudaSuccess) {
+        std::string msg = cudaGetErrorString(code);
+        if (what) msg = std::string(what) + ": " + msg;
+        throw CudaError(msg);
+    }
+}
+
+// Growable device array.
+template <class T> struct DBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    void reserve(size_t count) {
+        if (count <= n) return;
+        release();
+        check(cudaMalloc(reinterpret_cast<void**>(&p), sizeof(T) * (count ? count : 1)), "cudaMalloc");
+        n = count;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+};
+
+struct Context {
+    int algorithm = 2;
+    // system
+    int n = 0, nbig = 0, np = 0, npcap = 0;
+    int pn = 0, ngflag = 0;
+    double jcen[3] = {0, 0, 0};
+    std::vector<double> m_host;
+    // Big bodies: masses, radii, ngf rows, double-buffered state
+    DBuf<double> mbig, rcebig, rphysbig, ngfbig;
+    DBuf<double> bigstate[2];   // [9][nbig]: x(3) v(3) a(3)
+    // particles
+    DBuf<double> pstate[2];     // [9][npcap]
+    DBuf<double> pm, prce, prphys, pngf;
+    int cur = 0;
+    bool reset = true;
+    bool stepped = false;
+    // MVS tables
+    DBuf<double> tab, detail;
+    // events
+    DBuf<MercuryEvent> events;
+    DBuf<int> event_step;
+    DBuf<DeviceStatus> status;
+    DeviceStatus* status_host = nullptr;
+    std::vector<MercuryEvent> host_events;
+    std::vector<int> host_steps;
+    int pair_events = 0;
+    // staging
+    DBuf<double> transfer;
+    DBuf<double> snapshot;
+    // streams and timers
+    cudaStream_t stream = nullptr, stream_big = nullptr;
+    std::vector<cudaEvent_t> chunk_done;
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    std::vector<cudaEvent_t> kt0, kt1;
+    float last_advance_ms = 0.0f;
+    double last_particle_kernel_ms = 0.0;
+    int last_particle_launches = 0;
+    int64_t nforces = 0;
+    int particle_threads = 128;
+    int steps_per_launch = 0;   // 0 = automatic
+
+    BigState big(int k) {
+        BigState b;
+        b.x = bigstate[k].p;
+        b.v = bigstate[k].p + 3 * nbig;
+        b.a = bigstate[k].p + 6 * nbig;
+        return b;
+    }
+    void ensure_streams() {
+        if (!stream) {
+            check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "stream");
+            check(cudaStreamCreateWithFlags(&stream_big, cudaStreamNonBlocking), "stream");
+            check(cudaEventCreate(&t0), "event");
+            check(cudaEventCreate(&t1), "event");
+            check(cudaMallocHost(reinterpret_cast<void**>(&status_host), sizeof(DeviceStatus)), "pinned");
+        }
+    }
+    void release_all() {
+        DBuf<double>* bufs[] = {&mbig, &rcebig, &rphysbig, &ngfbig, &bigstate[0], &bigstate[1], &pstate[0],
+                                &pstate[1], &pm, &prce, &prphys, &pngf, &tab, &detail, &transfer, &snapshot};
+        for (auto* b : bufs) b->release();
+        events.release();
+        event_step.release();
+        status.release();
+        host_events.clear();
+        host_steps.clear();
+        n = nbig = np = npcap = 0;
+        stepped = false;
+        reset = true;
+    }
+};
+
+Context& ctx();
+
+// Layout kernels between the host's interleaved rows and the device SoA.
+void scatter_rows(const double* rows, int n, int comps, int nbig, double* big, int big_stride, double* part,
+                  int part_stride, cudaStream_t s);
+void gather_rows(double* rows, int n, int comps, int nbig, const double* big, int big_stride, const double* part,
+                 int part_stride, cudaStream_t s);
+
+int report(const std::exception& e);
+
+}  // namespace mb200

@@ -1,0 +1,621 @@
+// MVS kernels: the Big-body integrator (one CTA) and the fused test-particle
+// step (kick, Kepler drift, encounter screen, interaction kick) for K steps
+// per launch with the particle state in registers.
+#include <stdexcept>
+
+#include "kepler.cuh"
+#include "mvs.cuh"
+#include "mvs_device.cuh"
+
+namespace mb200 {
+
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+
+// Warp-aggregated append of this lane's record (if `has`) to the event list:
+// one atomic per warp, slots assigned in lane order by a ballot prefix count.
+// Must be reached by all 32 lanes.
+__device__ __forceinline__ void emit_event(bool has, const MercuryEvent& rec, int step, MercuryEvent* events,
+                                           int* event_step, int cap, DeviceStatus* st) {
+    const unsigned mask = __ballot_sync(FULL, has);
+    if (mask == 0) return;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(mask) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(&st->events, __popc(mask));
+    base = __shfl_sync(FULL, base, leader);
+    if (has) {
+        const int slot = base + __popc(mask & ((1u << lane) - 1u));
+        if (slot < cap) {
+            store_event(events + slot, rec);
+            event_step[slot] = step;
+        } else {
+            atomicExch(&st->overflow, 1);
+        }
+    }
+}
+
+// Scalar append used by the single-CTA Big-body kernel (rare events).
+__device__ __forceinline__ void append_event(const MercuryEvent& rec, int step, MercuryEvent* events,
+                                             int* event_step, int cap, DeviceStatus* st) {
+    const int slot = atomicAdd(&st->events, 1);
+    if (slot < cap) {
+        store_event(events + slot, rec);
+        event_step[slot] = step;
+    } else {
+        atomicExch(&st->overflow, 1);
+    }
+}
+
+__device__ __forceinline__ double3 ld3(const double* p, int stride, int k) {
+    return make_double3(p[k], p[stride + k], p[2 * stride + k]);
+}
+__device__ __forceinline__ void st3(double* p, int stride, int k, double3 v) {
+    p[k] = v.x;
+    p[stride + k] = v.y;
+    p[2 * stride + k] = v.z;
+}
+
+// ------------------------------------------------------------ Big bodies
+// Shared-memory workspace of the Big-body CTA, all [3][nbig] unless noted.
+struct BigSmem {
+    double *X, *V, *XJ, *VJ, *ACC, *X0, *V0, *XS, *VS, *A1, *A2, *AOBL, *GM, *misc;
+    __device__ void carve(double* base, int nbig) {
+        double* p = base;
+        double** arrays[] = {&X, &V, &XJ, &VJ, &ACC, &X0, &V0, &XS, &VS, &A1, &A2, &AOBL};
+        for (double** a : arrays) { *a = p; p += 3 * nbig; }
+        GM = p; p += nbig;
+        misc = p;  // a0[3], a0tp[3], acen[3]
+    }
+};
+
+// mco_h2j for the Big bodies (mercury6_2.for:2613-2682), one thread.
+__device__ void big_h2j(int nbig, const double* m, const double* X, const double* V, double* XJ, double* VJ) {
+    if (nbig < 2) return;
+    const int S = nbig;
+    double mtot = m[1];
+    double mx[3], mv[3];
+    for (int c = 0; c < 3; ++c) {
+        XJ[c * S + 1] = X[c * S + 1];
+        VJ[c * S + 1] = V[c * S + 1];
+        mx[c] = m[1] * X[c * S + 1];
+        mv[c] = m[1] * V[c * S + 1];
+    }
+    for (int j = 2; j <= nbig - 2; ++j) {
+        const double temp = 1.0 / (mtot + m[0]);
+        mtot = mtot + m[j];
+        for (int c = 0; c < 3; ++c) {
+            XJ[c * S + j] = X[c * S + j] - temp * mx[c];
+            VJ[c * S + j] = V[c * S + j] - temp * mv[c];
+        }
+        for (int c = 0; c < 3; ++c) {
+            mx[c] = mx[c] + m[j] * X[c * S + j];
+            mv[c] = mv[c] + m[j] * V[c * S + j];
+        }
+    }
+    if (nbig > 2) {
+        const double temp = 1.0 / (mtot + m[0]);
+        const int j = nbig - 1;
+        for (int c = 0; c < 3; ++c) {
+            XJ[c * S + j] = X[c * S + j] - temp * mx[c];
+            VJ[c * S + j] = V[c * S + j] - temp * mv[c];
+        }
+    }
+}
+
+// mco_j2h for the Big bodies (mercury6_2.for:2700-2770), one thread.
+__device__ void big_j2h(int nbig, const double* m, const double* XJ, const double* VJ, double* X, double* V) {
+    if (nbig < 2) return;
+    const int S = nbig;
+    double mtot = m[1];
+    double temp = m[1] / (mtot + m[0]);
+    double mx[3], mv[3];
+    for (int c = 0; c < 3; ++c) {
+        X[c * S + 1] = XJ[c * S + 1];
+        V[c * S + 1] = VJ[c * S + 1];
+        mx[c] = temp * XJ[c * S + 1];
+        mv[c] = temp * VJ[c * S + 1];
+    }
+    for (int j = 2; j <= nbig - 2; ++j) {
+        for (int c = 0; c < 3; ++c) {
+            X[c * S + j] = XJ[c * S + j] + mx[c];
+            V[c * S + j] = VJ[c * S + j] + mv[c];
+        }
+        mtot = mtot + m[j];
+        temp = m[j] / (mtot + m[0]);
+        for (int c = 0; c < 3; ++c) {
+            mx[c] = mx[c] + temp * XJ[c * S + j];
+            mv[c] = mv[c] + temp * VJ[c * S + j];
+        }
+    }
+    if (nbig > 2) {
+        const int j = nbig - 1;
+        for (int c = 0; c < 3; ++c) {
+            X[c * S + j] = XJ[c * S + j] + mx[c];
+            V[c * S + j] = VJ[c * S + j] + mv[c];
+        }
+    }
+}
+
+// mfo_mvs for the Big bodies plus the indirect term a0tp that every Small
+// body receives (mercury6_2.for:4946-5070), with mfo_ngf for Big bodies.
+// Writes S.ACC = (angf + 0) + a and S.misc = {a0, a0tp, acen}. All threads.
+__device__ void big_force(const MvsBigArgs& A, BigSmem& S, const double* V_ngf) {
+    const int nbig = A.nbig, N = nbig, tid = threadIdx.x, nt = blockDim.x;
+    const double* m = A.m;
+    double* a0 = S.misc;
+    double* a0tp = S.misc + 3;
+    double* acen = S.misc + 6;
+    if (tid == 0) {
+        a0[0] = a0[1] = a0[2] = 0.0;
+        if (nbig >= 2)
+            for (int c = 0; c < 3; ++c) { S.A1[c * N + 1] = 0.0; S.A2[c * N + 1] = 0.0; }
+        double minside = 0.0;
+        for (int k = 2; k < nbig; ++k) {
+            const int k1 = k - 1;
+            minside = minside + m[k1];
+            const double3 p = ld3(S.X, N, k), pj = ld3(S.XJ, N, k);
+            const double r2 = p.x * p.x + p.y * p.y + p.z * p.z;
+            const double rj2 = pj.x * pj.x + pj.y * pj.y + pj.z * pj.z;
+            const double r = 1.0 / sqrt(r2);
+            const double rj = 1.0 / sqrt(rj2);
+            const double r3 = r * r * r;
+            const double rj3 = rj * rj * rj;
+            const double fac0 = m[k] * r3;
+            const double fac12 = m[0] * rj3;
+            const double fac2 = m[k] * fac12 / (minside + m[0]);
+            const double q = (r2 - rj2) * 0.5 / rj2;
+            const double q2 = q * q, q3 = q * q2, q4 = q2 * q2, q5 = q2 * q3, q6 = q3 * q3, q7 = q3 * q4;
+            const double fac1 = 402.1875 * q7 - 187.6875 * q6 + 86.625 * q5 - 39.375 * q4 + 17.5 * q3 -
+                                7.5 * q2 + 3.0 * q - 1.0;
+            const double pc[3] = {p.x, p.y, p.z}, pjc[3] = {pj.x, pj.y, pj.z};
+            for (int c = 0; c < 3; ++c) {
+                a0[c] = a0[c] - fac0 * pc[c];
+                S.A1[c * N + k] = fac12 * (pjc[c] + fac1 * pc[c]);
+                S.A2[c * N + k] = S.A2[c * N + k1] + fac2 * pjc[c];
+            }
+        }
+        a0tp[0] = a0tp[1] = a0tp[2] = 0.0;
+        if (nbig >= 2) {
+            const double3 p = ld3(S.X, N, 1);
+            const double r2 = p.x * p.x + p.y * p.y + p.z * p.z;
+            const double r = 1.0 / sqrt(r2);
+            const double r3 = r * r * r;
+            const double fac0 = m[1] * r3;
+            a0tp[0] = a0[0] - fac0 * p.x;
+            a0tp[1] = a0[1] - fac0 * p.y;
+            a0tp[2] = a0[2] - fac0 * p.z;
+        }
+    }
+    if (A.obl)
+        for (int k = 1 + tid; k < nbig; k += nt) st3(S.AOBL, N, k, oblate_accel(ld3(S.X, N, k), A.jcen, m[0]));
+    __syncthreads();
+    if (tid == 0) {
+        acen[0] = acen[1] = acen[2] = 0.0;
+        if (A.obl)
+            for (int k = 1; k < nbig; ++k) {
+                const double tmp4 = m[k] / m[0];
+                const double3 ao = ld3(S.AOBL, N, k);
+                acen[0] = acen[0] - tmp4 * ao.x;
+                acen[1] = acen[1] - tmp4 * ao.y;
+                acen[2] = acen[2] - tmp4 * ao.z;
+            }
+    }
+    __syncthreads();
+    for (int k = 1 + tid; k < nbig; k += nt) {
+        const double3 pk = ld3(S.X, N, k);
+        double3 a3 = make_double3(0.0, 0.0, 0.0);
+        for (int i = 1; i < nbig; ++i) {
+            if (i == k) continue;
+            const double3 pi = ld3(S.X, N, i);
+            // The pair (lower, higher) is differenced higher - lower in mfo_mvs.
+            const bool lower = i < k;
+            const double dx = lower ? pk.x - pi.x : pi.x - pk.x;
+            const double dy = lower ? pk.y - pi.y : pi.y - pk.y;
+            const double dz = lower ? pk.z - pi.z : pi.z - pk.z;
+            const double s2 = dx * dx + dy * dy + dz * dz;
+            const double s_1 = 1.0 / sqrt(s2);
+            const double s_3 = s_1 * s_1 * s_1;
+            const double fac = m[i] * s_3;
+            if (lower) { a3.x = a3.x - fac * dx; a3.y = a3.y - fac * dy; a3.z = a3.z - fac * dz; }
+            else { a3.x = a3.x + fac * dx; a3.y = a3.y + fac * dy; a3.z = a3.z + fac * dz; }
+        }
+        double3 a;
+        a.x = a0[0] + S.A1[k] + S.A2[k] + a3.x;
+        a.y = a0[1] + S.A1[N + k] + S.A2[N + k] + a3.y;
+        a.z = a0[2] + S.A1[2 * N + k] + S.A2[2 * N + k] + a3.z;
+        if (A.obl) {
+            const double3 ao = ld3(S.AOBL, N, k);
+            a.x = a.x + (ao.x - acen[0]);
+            a.y = a.y + (ao.y - acen[1]);
+            a.z = a.z + (ao.z - acen[2]);
+        }
+        if (A.ngflag == 1 || A.ngflag == 3) {
+            double3 g;
+            if (!nongrav_accel(pk, ld3(V_ngf, N, k), A.ngf + 5 * k, g)) raise_fault(A.status, 2);
+            a.x = g.x + 0.0 + a.x;
+            a.y = g.y + 0.0 + a.y;
+            a.z = g.z + 0.0 + a.z;
+        }
+        if (!isfinite(a.x) || !isfinite(a.y) || !isfinite(a.z)) raise_fault(A.status, 1);
+        st3(S.ACC, N, k, a);
+    }
+    __syncthreads();
+}
+
+// Force row of a table: head {a0tp, acen} and per-body {x, m}.
+__device__ void write_force_table(const MvsBigArgs& A, const BigSmem& S, double* row) {
+    const int nbig = A.nbig, N = nbig;
+    if (threadIdx.x == 0)
+        for (int c = 0; c < 6; ++c) row[c] = S.misc[3 + c];
+    for (int k = 1 + threadIdx.x; k < nbig; k += blockDim.x) {
+        double* b = row + TAB_HEAD + (k - 1) * TAB_BODY;
+        b[0] = S.X[k];
+        b[1] = S.X[N + k];
+        b[2] = S.X[2 * N + k];
+        b[3] = A.m[k];
+    }
+}
+
+__global__ void __launch_bounds__(128) mvs_big_kernel(MvsBigArgs A) {
+    extern __shared__ double smem[];
+    const int nbig = A.nbig, N = nbig, nb = nbig - 1, tid = threadIdx.x, nt = blockDim.x;
+    const int stride = tab_stride(nb);
+    BigSmem S;
+    S.carve(smem, nbig);
+    for (int k = tid; k < nbig; k += nt)
+        for (int c = 0; c < 3; ++c) {
+            S.X[c * N + k] = A.in.x[c * N + k];
+            S.V[c * N + k] = A.in.v[c * N + k];
+            S.ACC[c * N + k] = A.in.a[c * N + k];
+        }
+    if (tid == 0) {
+        double minside = A.m[0];
+        for (int j = 1; j < nbig; ++j) {
+            const double msofar = minside + A.m[j];
+            S.GM[j] = A.m[0] * msofar / minside;
+            minside = msofar;
+        }
+    }
+    __syncthreads();
+    if (A.reset) {
+        if (tid == 0) big_h2j(nbig, A.m, S.X, S.V, S.XJ, S.VJ);
+        __syncthreads();
+        big_force(A, S, S.V);
+        write_force_table(A, S, A.tab);
+        __syncthreads();
+    }
+    const double h = A.h, hby2 = 0.5 * h, hm1 = 1.0 / h;
+    for (int s = 0; s < A.nsteps; ++s) {
+        for (int k = 1 + tid; k < nbig; k += nt)
+            for (int c = 0; c < 3; ++c) {
+                const int z = c * N + k;
+                S.XS[z] = S.X[z];
+                S.VS[z] = S.V[z];
+                S.V[z] = S.V[z] + hby2 * S.ACC[z];
+                S.X0[z] = S.X[z];
+                S.V0[z] = S.V[z];
+            }
+        __syncthreads();
+        if (tid == 0) big_h2j(nbig, A.m, S.X, S.V, S.XJ, S.VJ);
+        __syncthreads();
+        for (int k = 1 + tid; k < nbig; k += nt) {
+            double3 p = ld3(S.XJ, N, k), w = ld3(S.VJ, N, k);
+            drift_one(S.GM[k], p, w, h);
+            st3(S.XJ, N, k, p);
+            st3(S.VJ, N, k, w);
+        }
+        __syncthreads();
+        if (tid == 0) big_j2h(nbig, A.m, S.XJ, S.VJ, S.X, S.V);
+        __syncthreads();
+        double* row = A.tab + (size_t)(s + 1) * stride;
+        double* det = A.detail + (size_t)s * nb * TAB_DETAIL;
+        for (int k = 1 + tid; k < nbig; k += nt) {
+            double* b = row + TAB_HEAD + (k - 1) * TAB_BODY;
+            const double pad = A.rce[k] * 1.2;
+            double lo, hi;
+            box_extent(S.X0[k], S.X[k], S.V0[k], S.V[k], h, lo, hi);
+            b[4] = lo - pad;
+            b[5] = hi + pad;
+            box_extent(S.X0[N + k], S.X[N + k], S.V0[N + k], S.V[N + k], h, lo, hi);
+            b[6] = lo - pad;
+            b[7] = hi + pad;
+            double* d = det + (k - 1) * TAB_DETAIL;
+            for (int c = 0; c < 3; ++c) {
+                d[c] = S.X0[c * N + k];
+                d[3 + c] = S.V0[c * N + k];
+                d[6 + c] = S.X[c * N + k];
+                d[9 + c] = S.V[c * N + k];
+            }
+            d[12] = A.rce[k];
+            d[13] = A.rphys[k];
+        }
+        // mce_stat between Big bodies (pairs 1 <= i < j < nbig).
+        const int npair = nb * (nb - 1) / 2;
+        for (int q = tid; q < npair; q += nt) {
+            int i = 1, rem = q;
+            while (rem >= nbig - 1 - i) { rem -= nbig - 1 - i; ++i; }
+            const int j = i + 1 + rem;
+            double lo_i, hi_i, lo_j, hi_j, ylo_i, yhi_i, ylo_j, yhi_j;
+            const double pi_ = A.rce[i] * 1.2, pj_ = A.rce[j] * 1.2;
+            box_extent(S.X0[i], S.X[i], S.V0[i], S.V[i], h, lo_i, hi_i);
+            box_extent(S.X0[N + i], S.X[N + i], S.V0[N + i], S.V[N + i], h, ylo_i, yhi_i);
+            box_extent(S.X0[j], S.X[j], S.V0[j], S.V[j], h, lo_j, hi_j);
+            box_extent(S.X0[N + j], S.X[N + j], S.V0[N + j], S.V[N + j], h, ylo_j, yhi_j);
+            lo_i = lo_i - pi_; hi_i = hi_i + pi_; ylo_i = ylo_i - pi_; yhi_i = yhi_i + pi_;
+            lo_j = lo_j - pj_; hi_j = hi_j + pj_; ylo_j = ylo_j - pj_; yhi_j = yhi_j + pj_;
+            if (!(hi_i >= lo_j && hi_j >= lo_i && yhi_i >= ylo_j && yhi_j >= ylo_i)) continue;
+            PairEnds I{ld3(S.X0, N, i), ld3(S.V0, N, i), ld3(S.X, N, i), ld3(S.V, N, i)};
+            PairEnds J{ld3(S.X0, N, j), ld3(S.V0, N, j), ld3(S.X, N, j), ld3(S.V, N, j)};
+            MercuryEvent rec;
+            if (pair_event(I, J, A.rce[i], A.rce[j], A.rphys[i], A.rphys[j], h, hm1, i + 1, j + 1,
+                           A.m[j] > A.m[i], &rec))
+                append_event(rec, A.step0 + s, A.events, A.event_step, A.event_cap, A.status);
+        }
+        __syncthreads();
+        big_force(A, S, S.V);
+        write_force_table(A, S, row);
+        for (int k = 1 + tid; k < nbig; k += nt)
+            for (int c = 0; c < 3; ++c) {
+                const int z = c * N + k;
+                S.V[z] = S.V[z] + hby2 * S.ACC[z];
+            }
+        __syncthreads();
+        if (A.central)
+            for (int k = 1 + tid; k < nbig; k += nt) {
+                double temp;
+                if (central_impact(ld3(S.XS, N, k), ld3(S.VS, N, k), ld3(S.X, N, k), ld3(S.V, N, k), A.m[0],
+                                   A.m[k], h, A.rcen, temp)) {
+                    MercuryEvent rec = {};
+                    rec.i = 1;
+                    rec.j = k + 1;
+                    rec.kind = EV_CENTRAL;
+                    rec.time = temp;
+                    rec.distance = A.rcen;
+                    append_event(rec, A.step0 + s, A.events, A.event_step, A.event_cap, A.status);
+                }
+            }
+    }
+    __syncthreads();
+    for (int k = tid; k < nbig; k += nt)
+        for (int c = 0; c < 3; ++c) {
+            A.out.x[c * N + k] = S.X[c * N + k];
+            A.out.v[c * N + k] = S.V[c * N + k];
+            A.out.a[c * N + k] = S.ACC[c * N + k];
+        }
+}
+
+// ------------------------------------------------------------ test particles
+struct Particle {
+    double3 x, v, acc;
+    double rce, rphys, m;
+};
+
+// mfo_mvs for one Small body (mercury6_2.for:5034-5060) plus mfo_ngf, i.e. the
+// total acceleration (angf + 0) + a of the kick; T is a staged force table.
+template <bool NGF, bool OBL>
+__device__ __forceinline__ double3 particle_force(const double3 x, const double3 v_ngf, const double* g,
+                                                  const double* T, int nb, const double* jcen, double mu,
+                                                  DeviceStatus* st) {
+    double3 a3 = make_double3(0.0, 0.0, 0.0);
+    for (int b = 0; b < nb; ++b) {
+        const double* row = T + TAB_HEAD + b * TAB_BODY;
+        const double dx = x.x - row[0], dy = x.y - row[1], dz = x.z - row[2];
+        const double s2 = dx * dx + dy * dy + dz * dz;
+        const double s_1 = 1.0 / sqrt(s2);
+        const double s_3 = s_1 * s_1 * s_1;
+        const double faci = row[3] * s_3;
+        a3.x = a3.x - faci * dx;
+        a3.y = a3.y - faci * dy;
+        a3.z = a3.z - faci * dz;
+    }
+    double3 a = make_double3(T[0] + a3.x, T[1] + a3.y, T[2] + a3.z);
+    if (OBL) {
+        const double3 ao = oblate_accel(x, jcen, mu);
+        a.x = a.x + (ao.x - T[3]);
+        a.y = a.y + (ao.y - T[4]);
+        a.z = a.z + (ao.z - T[5]);
+    }
+    if (NGF) {
+        double3 ng;
+        if (!nongrav_accel(x, v_ngf, g, ng)) raise_fault(st, 2);
+        a.x = ng.x + 0.0 + a.x;
+        a.y = ng.y + 0.0 + a.y;
+        a.z = ng.z + 0.0 + a.z;
+    }
+    if (!isfinite(a.x) || !isfinite(a.y) || !isfinite(a.z)) raise_fault(st, 1);
+    return a;
+}
+
+template <bool NGF, bool OBL, bool CENTRAL>
+__device__ __forceinline__ void particle_step(Particle& P, bool ok, int p, const double* g, const double* T,
+                                              int s, const MvsParticleArgs& A, double hby2, double hm1) {
+    const int nb = A.nb;
+    const double h = A.h;
+    double3 xs, vs, x0, v0;
+    double bxlo = 0.0, bxhi = 0.0, bylo = 0.0, byhi = 0.0;
+    if (ok) {
+        if (CENTRAL) { xs = P.x; vs = P.v; }
+        P.v.x = P.v.x + hby2 * P.acc.x;
+        P.v.y = P.v.y + hby2 * P.acc.y;
+        P.v.z = P.v.z + hby2 * P.acc.z;
+        x0 = P.x;
+        v0 = P.v;
+        drift_one(A.mu, P.x, P.v, h);
+        box_extent(x0.x, P.x.x, v0.x, P.v.x, h, bxlo, bxhi);
+        box_extent(x0.y, P.x.y, v0.y, P.v.y, h, bylo, byhi);
+        const double pad = P.rce * 1.2;
+        bxlo = bxlo - pad;
+        bxhi = bxhi + pad;
+        bylo = bylo - pad;
+        byhi = byhi + pad;
+    }
+    // mce_stat against each Big body; the loop is uniform across the warp.
+    for (int b = 0; b < nb; ++b) {
+        const double* row = T + TAB_HEAD + b * TAB_BODY;
+        const bool cand = ok && row[5] >= bxlo && bxhi >= row[4] && row[7] >= bylo && byhi >= row[6];
+        if (__any_sync(FULL, cand)) {
+            MercuryEvent rec;
+            bool has = false;
+            if (cand) {
+                const double* d = A.detail + ((size_t)s * nb + b) * TAB_DETAIL;
+                PairEnds I{make_double3(d[0], d[1], d[2]), make_double3(d[3], d[4], d[5]),
+                           make_double3(d[6], d[7], d[8]), make_double3(d[9], d[10], d[11])};
+                PairEnds J{x0, v0, P.x, P.v};
+                has = pair_event(I, J, d[12], P.rce, d[13], P.rphys, h, hm1, b + 2, A.nbig + p + 1, false, &rec);
+            }
+            emit_event(has, rec, A.step0 + s, A.events, A.event_step, A.event_cap, A.status);
+        }
+    }
+    if (ok) {
+        P.acc = particle_force<NGF, OBL>(P.x, P.v, g, T, nb, A.jcen, A.mu, A.status);
+        P.v.x = P.v.x + hby2 * P.acc.x;
+        P.v.y = P.v.y + hby2 * P.acc.y;
+        P.v.z = P.v.z + hby2 * P.acc.z;
+    }
+    if (CENTRAL) {
+        double temp = 0.0;
+        const bool hit = ok && central_impact(xs, vs, P.x, P.v, A.mu, P.m, h, A.rcen, temp);
+        MercuryEvent rec = {};
+        if (hit) {
+            rec.i = 1;
+            rec.j = A.nbig + p + 1;
+            rec.kind = EV_CENTRAL;
+            rec.time = temp;
+            rec.distance = A.rcen;
+        }
+        emit_event(hit, rec, A.step0 + s, A.events, A.event_step, A.event_cap, A.status);
+    }
+}
+
+template <bool NGF, bool OBL, bool CENTRAL>
+__global__ void __launch_bounds__(128) mvs_particle_kernel(MvsParticleArgs A) {
+    extern __shared__ double stab[];
+    const int nb = A.nb, stride = tab_stride(nb);
+    const int rows = A.nsteps + (A.reset ? 1 : 0);
+    const double* gtab = A.tab + (A.reset ? 0 : stride);
+    for (int k = threadIdx.x; k < rows * stride; k += blockDim.x) stab[k] = gtab[k];
+    __syncthreads();
+    const double* steps_tab = stab + (A.reset ? stride : 0);
+    const double hby2 = 0.5 * A.h, hm1 = 1.0 / A.h;
+    const int lane = threadIdx.x & 31;
+    const int npairs = (A.np + 1) >> 1;
+    const int ntiles = (npairs + blockDim.x - 1) / blockDim.x;
+    const int S = A.npcap;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int pair = tile * blockDim.x + threadIdx.x;
+        if (pair - lane >= npairs) continue;  // whole warp past the end
+        const bool live = pair < npairs;
+        const int j0 = 2 * pair;
+        // Two particles per thread (one double2 per component); the step body is
+        // instantiated once and applied to each in turn by swapping registers.
+        Particle Pa, Pb;
+        double ga[5], gb[5];
+        if (live) {
+            const double2* in = reinterpret_cast<const double2*>(A.xin);
+            const int q = pair, H = S / 2;
+            double2 t;
+            t = in[0 * H + q]; Pa.x.x = t.x; Pb.x.x = t.y;
+            t = in[1 * H + q]; Pa.x.y = t.x; Pb.x.y = t.y;
+            t = in[2 * H + q]; Pa.x.z = t.x; Pb.x.z = t.y;
+            t = in[3 * H + q]; Pa.v.x = t.x; Pb.v.x = t.y;
+            t = in[4 * H + q]; Pa.v.y = t.x; Pb.v.y = t.y;
+            t = in[5 * H + q]; Pa.v.z = t.x; Pb.v.z = t.y;
+            t = in[6 * H + q]; Pa.acc.x = t.x; Pb.acc.x = t.y;
+            t = in[7 * H + q]; Pa.acc.y = t.x; Pb.acc.y = t.y;
+            t = in[8 * H + q]; Pa.acc.z = t.x; Pb.acc.z = t.y;
+            t = reinterpret_cast<const double2*>(A.rce)[q]; Pa.rce = t.x; Pb.rce = t.y;
+            t = reinterpret_cast<const double2*>(A.rphys)[q]; Pa.rphys = t.x; Pb.rphys = t.y;
+            t = reinterpret_cast<const double2*>(A.m)[q]; Pa.m = t.x; Pb.m = t.y;
+            if (NGF)
+                for (int c = 0; c < 5; ++c) {
+                    t = reinterpret_cast<const double2*>(A.ngf + (size_t)c * S)[q];
+                    ga[c] = t.x;
+                    gb[c] = t.y;
+                }
+        }
+        bool oka = live && j0 < A.np, okb = live && j0 + 1 < A.np;
+        if (A.reset) {
+            if (oka) Pa.acc = particle_force<NGF, OBL>(Pa.x, Pa.v, ga, stab, nb, A.jcen, A.mu, A.status);
+            if (okb) Pb.acc = particle_force<NGF, OBL>(Pb.x, Pb.v, gb, stab, nb, A.jcen, A.mu, A.status);
+        }
+        for (int s = 0; s < A.nsteps; ++s) {
+            const double* T = steps_tab + s * stride;
+#pragma unroll 1
+            for (int u = 0; u < 2; ++u) {
+                particle_step<NGF, OBL, CENTRAL>(Pa, oka, j0 + u, ga, T, s, A, hby2, hm1);
+                const Particle tp = Pa; Pa = Pb; Pb = tp;
+                const bool tk = oka; oka = okb; okb = tk;
+                if (NGF)
+                    for (int c = 0; c < 5; ++c) { const double tg = ga[c]; ga[c] = gb[c]; gb[c] = tg; }
+            }
+        }
+        if (live) {
+            double2* out = reinterpret_cast<double2*>(A.xout);
+            const int q = pair, H = S / 2;
+            out[0 * H + q] = make_double2(Pa.x.x, Pb.x.x);
+            out[1 * H + q] = make_double2(Pa.x.y, Pb.x.y);
+            out[2 * H + q] = make_double2(Pa.x.z, Pb.x.z);
+            out[3 * H + q] = make_double2(Pa.v.x, Pb.v.x);
+            out[4 * H + q] = make_double2(Pa.v.y, Pb.v.y);
+            out[5 * H + q] = make_double2(Pa.v.z, Pb.v.z);
+            out[6 * H + q] = make_double2(Pa.acc.x, Pb.acc.x);
+            out[7 * H + q] = make_double2(Pa.acc.y, Pb.acc.y);
+            out[8 * H + q] = make_double2(Pa.acc.z, Pb.acc.z);
+        }
+    }
+}
+
+template <bool NGF, bool OBL, bool CENTRAL>
+void launch_variant(const MvsParticleArgs& a, cudaStream_t s, int threads) {
+    auto kern = mvs_particle_kernel<NGF, OBL, CENTRAL>;
+    const size_t smem = mvs_particle_smem(a.nb, a.nsteps, a.reset);
+    if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const int npairs = (a.np + 1) / 2;
+    int tiles = (npairs + threads - 1) / threads;
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+    if (per_sm < 1) per_sm = 1;
+    const int grid = tiles < sms * per_sm ? tiles : sms * per_sm;
+    if (grid > 0) kern<<<grid, threads, smem, s>>>(a);
+}
+
+}  // namespace
+
+size_t mvs_particle_smem(int nb, int nsteps, int reset) {
+    return sizeof(double) * (size_t)tab_stride(nb) * (size_t)(nsteps + (reset ? 1 : 0));
+}
+
+int mvs_max_steps_per_launch(int nb) {
+    const size_t budget = 64 * 1024;
+    const size_t row = sizeof(double) * (size_t)tab_stride(nb);
+    long k = (long)(budget / row) - 1;
+    if (k < 1) k = 1;
+    if (k > 64) k = 64;
+    return (int)k;
+}
+
+void launch_mvs_big(const MvsBigArgs& a, cudaStream_t s) {
+    const size_t smem = sizeof(double) * ((size_t)12 * 3 * a.nbig + a.nbig + 16);
+    if (smem > 48 * 1024)
+        cudaFuncSetAttribute(mvs_big_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    mvs_big_kernel<<<1, 128, smem, s>>>(a);
+}
+
+void launch_mvs_particles(const MvsParticleArgs& a, cudaStream_t s, int threads) {
+    const bool ngf = a.ngf_on != 0;
+    const bool obl = a.jcen[0] != 0.0 || a.jcen[1] != 0.0 || a.jcen[2] != 0.0;
+    const bool cen = a.central != 0;
+    if (ngf) {
+        if (obl) cen ? launch_variant<true, true, true>(a, s, threads) : launch_variant<true, true, false>(a, s, threads);
+        else cen ? launch_variant<true, false, true>(a, s, threads) : launch_variant<true, false, false>(a, s, threads);
+    } else {
+        if (obl) cen ? launch_variant<false, true, true>(a, s, threads) : launch_variant<false, true, false>(a, s, threads);
+        else cen ? launch_variant<false, false, true>(a, s, threads) : launch_variant<false, false, false>(a, s, threads);
+    }
+}
+
+}  // namespace mb200

@@ -1,0 +1,89 @@
+// MVS map on the device (mdt_mvs, mercury6_2.for:3987-4101).
+//
+// The Big bodies never feel the test particles in this map (mfo_mvs,
+// mercury6_2.for:5034-5045 is one-way), so their trajectory is integrated by
+// one CTA (mvs_big_kernel), which writes for every step a table of what the
+// particles need: post-drift Big positions and masses for the kick, each Big
+// body's padded x-y box and end states for the encounter screen, and the
+// indirect term a0tp. The particle kernel stages those tables in shared memory
+// and advances every test particle through K steps in registers.
+#pragma once
+#include "common.cuh"
+
+namespace mb200 {
+
+// Per-step table, in doubles. The head and per-body force/box rows are staged
+// in shared memory by the particle kernel; the per-body detail rows (end
+// states, radii) are read from global memory only when a box overlaps.
+constexpr int TAB_HEAD = 8;        // a0tp[3], acen[3], pad[2]
+constexpr int TAB_BODY = 8;        // x1, y1, z1, m, xmin, xmax, ymin, ymax
+constexpr int TAB_DETAIL = 16;     // x0[3], v0[3], x1[3], v1[3], rce, rphys, pad[2]
+
+__host__ __device__ constexpr int tab_stride(int nb) { return TAB_HEAD + TAB_BODY * nb; }
+
+// Device-resident Big-body state, Fortran-style C indices 0..nbig-1 (0 is the
+// central body). SoA with stride nbig.
+struct BigState {
+    double* x;   // [3][nbig]
+    double* v;   // [3][nbig]
+    double* a;   // [3][nbig] cached total acceleration (angf + a) of the last force call
+};
+
+struct MvsBigArgs {
+    int nbig;
+    int ngflag;
+    int obl;
+    int reset;          // recompute the cached acceleration before the first kick
+    int nsteps;
+    int central;        // screen Big bodies against the central body (fused runs)
+    int step0;          // global index of the first step (for event step tags)
+    double jcen[3];
+    double h;
+    double rcen;
+    const double* m;    // [nbig]
+    const double* rce;  // [nbig]
+    const double* rphys;
+    const double* ngf;  // [nbig][5]
+    BigState in, out;
+    double* tab;        // [(nsteps + 1)][tab_stride(nb)], row 0 = start-of-run force table
+    double* detail;     // [nsteps][nb][TAB_DETAIL]
+    MercuryEvent* events;
+    int* event_step;
+    int event_cap;
+    DeviceStatus* status;
+};
+
+struct MvsParticleArgs {
+    int np;             // number of test particles
+    int npcap;          // allocated length of every particle array (even)
+    int nb;             // Big bodies (nbig - 1)
+    int nbig;
+    int nsteps;
+    int reset;
+    int central;
+    int step0;
+    int ngf_on;         // mfo_ngf terms present
+    double mu;          // central mass
+    double h;
+    double rcen;
+    double jcen[3];
+    const double* xin;  // [9][npcap]: x y z vx vy vz ax ay az
+    double* xout;
+    const double* m;    // [npcap]
+    const double* rce;
+    const double* rphys;
+    const double* ngf;  // [5][npcap]
+    const double* tab;
+    const double* detail;
+    MercuryEvent* events;
+    int* event_step;
+    int event_cap;
+    DeviceStatus* status;
+};
+
+void launch_mvs_big(const MvsBigArgs& a, cudaStream_t s);
+void launch_mvs_particles(const MvsParticleArgs& a, cudaStream_t s, int threads);
+size_t mvs_particle_smem(int nb, int nsteps, int reset);
+int mvs_max_steps_per_launch(int nb);
+
+}  // namespace mb200

@@ -1,0 +1,188 @@
+"""Test infrastructure only: ctypes front end of the CPU oracle.
+
+The oracle (``oracle_mvs.hpp`` and friends, built into ``liboracle.so``) is a
+statement-for-statement C++ restatement of MERCURY6's Fortran hot path
+(mercury6_2.for). It is the parity checker for the CUDA library: only tests/,
+``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg may load it, and
+never as the thing measured or shipped.
+
+Arrays follow the reference host's Fortran layout: ``x`` is (n, 3) row-major,
+which is byte-identical to Fortran's x(3,n); ``ngf`` is (n, 5).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "liboracle.so"
+REF_KEPLER = HERE / "_ref" / "libkepler_ref.so"
+REF_CUDA = HERE / "_ref" / "libmercury_cuda_ref.so"
+
+D = C.c_double
+I = C.c_int
+PD = C.POINTER(C.c_double)
+
+
+class Event(C.Structure):
+    """Layout of the reference's MercuryEvent (mercury_cuda.h:7-11)."""
+
+    _fields_ = [("i", C.c_int), ("j", C.c_int), ("kind", C.c_int), ("now", C.c_int),
+                ("distance", C.c_double), ("time", C.c_double),
+                ("xi", C.c_double * 6), ("xj", C.c_double * 6)]
+
+
+EVENT_DTYPE = np.dtype([("i", np.int32), ("j", np.int32), ("kind", np.int32), ("now", np.int32),
+                        ("distance", np.float64), ("time", np.float64),
+                        ("xi", np.float64, 6), ("xj", np.float64, 6)])
+assert EVENT_DTYPE.itemsize == C.sizeof(Event) == 128
+
+
+def build() -> None:
+    """Compile liboracle.so with the Makefile beside this file (g++ only)."""
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            build()
+        L = C.CDLL(str(LIB))
+        L.oracle_drift_one.argtypes = [D, PD, D]
+        L.oracle_drift_one.restype = I
+        L.oracle_mvs_step.argtypes = [I, I, PD, PD, PD, PD, I, PD, PD, PD, D, D, PD, PD,
+                                      C.POINTER(I), C.c_void_p, I, C.POINTER(I)]
+        L.oracle_mvs_step.restype = I
+        L.oracle_mce_cent.argtypes = [I, PD, PD, PD, PD, PD, D, D, D, C.c_void_p, I, C.POINTER(I)]
+        L.oracle_mvs_corrector.argtypes = [I, I, I, PD, PD, PD, PD, I, PD, D, PD, PD]
+        L.oracle_mvs_corrector.restype = I
+        L.oracle_mce_hill.argtypes = [I, PD, PD, PD, PD, PD]
+        L.oracle_mvs_run.argtypes = [I, I, PD, PD, PD, PD, I, PD, PD, PD, D, D, I, D, I, I]
+        L.oracle_mvs_run.restype = C.c_void_p
+        L.oracle_run_status.argtypes = [C.c_void_p]
+        L.oracle_run_event_count.argtypes = [C.c_void_p]
+        L.oracle_run_events.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.oracle_run_free.argtypes = [C.c_void_p]
+        L.oracle_count_mvs.argtypes = [I, I, PD, PD, PD, PD, I, PD, PD, PD, D, D, I, D,
+                                       C.POINTER(C.c_uint64)]
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(PD)
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def drift_one(mu: float, xv, dt: float):
+    """drift_one (mercury6_2.for:8296-8330) on one 6-vector; returns (xv', iflg)."""
+    s = _f64(xv).copy()
+    flag = lib().oracle_drift_one(mu, _p(s), dt)
+    return s, flag
+
+
+def ref_drift_one(mu: float, xv, dt: float):
+    """The reference's own drift_one__ (mercury_cuda_kepler.cuh) built for the host."""
+    L = C.CDLL(str(REF_KEPLER))
+    L.ref_drift_one.argtypes = [D, PD, D]
+    L.ref_drift_one.restype = I
+    s = _f64(xv).copy()
+    flag = L.ref_drift_one(mu, _p(s), dt)
+    return s, flag
+
+
+class MvsStepper:
+    """mdt_mvs with its saved state (cached accelerations, dtflag) held here."""
+
+    def __init__(self, sys):
+        self.sys = sys
+        n = sys.n
+        self.acc = np.zeros((n, 3))
+        self.angf = np.zeros((n, 3))
+        self.dtflag = I(0)
+
+    def step(self, time: float, h: float):
+        s = self.sys
+        cap = max(64, s.n)
+        buf = np.zeros(cap, dtype=EVENT_DTYPE)
+        count = I(0)
+        rc = lib().oracle_mvs_step(s.n, s.nbig, _p(s.m), _p(s.x), _p(s.v), _p(s.ngf), s.ngflag,
+                                   _p(s.jcen), _p(s.rce), _p(s.rphys), time, h, _p(self.acc),
+                                   _p(self.angf), C.byref(self.dtflag),
+                                   buf.ctypes.data_as(C.c_void_p), cap, C.byref(count))
+        if rc:
+            raise RuntimeError("oracle mdt_mvs failed (mfo_ngf undefined direction)")
+        assert count.value <= cap
+        return buf[:count.value].copy()
+
+
+def mce_cent(m, x0, v0, x1, v1, time, h, rcen):
+    n = len(m)
+    cap = max(16, n)
+    buf = np.zeros(cap, dtype=EVENT_DTYPE)
+    count = I(0)
+    lib().oracle_mce_cent(n, _p(_f64(m)), _p(_f64(x0)), _p(_f64(v0)), _p(_f64(x1)), _p(_f64(v1)),
+                          time, h, rcen, buf.ctypes.data_as(C.c_void_p), cap, C.byref(count))
+    return buf[:count.value].copy()
+
+
+def mvs_corrector(sys, h: float, forward: bool = True):
+    """mco_mvs2h (forward) or mco_h2mvs (inverse) on copies of sys.x, sys.v."""
+    xh = np.zeros_like(sys.x)
+    vh = np.zeros_like(sys.v)
+    rc = lib().oracle_mvs_corrector(int(forward), sys.n, sys.nbig, _p(sys.m), _p(sys.x), _p(sys.v),
+                                    _p(sys.ngf), sys.ngflag, _p(sys.jcen), h, _p(xh), _p(vh))
+    if rc:
+        raise RuntimeError("oracle corrector failed")
+    return xh, vh
+
+
+def mce_hill(m, x, v):
+    m = _f64(m)
+    n = len(m)
+    hill = np.zeros(n)
+    a = np.zeros(n)
+    lib().oracle_mce_hill(n, _p(m), _p(_f64(x)), _p(_f64(v)), _p(hill), _p(a))
+    return hill, a
+
+
+def mvs_run(sys, time0: float, h: float, nsteps: int, rcen: float, central: bool = True,
+            threads: int | None = None):
+    """mal_hcon's MVS step loop on sys (in place). Returns (events, steps)."""
+    threads = threads or os.cpu_count() or 1
+    s = sys
+    handle = lib().oracle_mvs_run(s.n, s.nbig, _p(s.m), _p(s.x), _p(s.v), _p(s.ngf), s.ngflag,
+                                  _p(s.jcen), _p(s.rce), _p(s.rphys), time0, h, nsteps, rcen,
+                                  int(central), threads)
+    try:
+        if lib().oracle_run_status(handle):
+            raise RuntimeError("oracle MVS run failed")
+        count = lib().oracle_run_event_count(handle)
+        events = np.zeros(count, dtype=EVENT_DTYPE)
+        steps = np.zeros(count, dtype=np.int32)
+        lib().oracle_run_events(handle, events.ctypes.data_as(C.c_void_p),
+                                steps.ctypes.data_as(C.c_void_p))
+    finally:
+        lib().oracle_run_free(handle)
+    return events, steps
+
+
+def count_mvs(sys, time0: float, h: float, nsteps: int, rcen: float):
+    """Algorithmic operation tally {add, mul, div, sqrt, cmp, libm} of nsteps steps."""
+    s = sys
+    out = (C.c_uint64 * 6)()
+    lib().oracle_count_mvs(s.n, s.nbig, _p(s.m), _p(s.x), _p(s.v), _p(s.ngf), s.ngflag,
+                           _p(s.jcen), _p(s.rce), _p(s.rphys), time0, h, nsteps, rcen, out)
+    return dict(zip(["add", "mul", "div", "sqrt", "cmp", "libm"], list(out)))

@@ -1,0 +1,251 @@
+// Test infrastructure only: the C entry points of the CPU oracle, called through
+// ctypes by tests/ and by bench.py's CPU-baseline leg. Arrays keep the Fortran
+// layout of the reference host (x(3,n), ngf(5,n)); events use the layout of the
+// reference's MercuryEvent (mercury_cuda.h:7-11).
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+#include "oracle_mvs.hpp"
+
+namespace oracle {
+thread_local Tally tally;
+}
+
+using oracle::Counted;
+using oracle::Event;
+using oracle::MvsState;
+
+namespace {
+
+template <class R> std::vector<R> widen(const double* p, size_t n) {
+    std::vector<R> out(n);
+    for (size_t k = 0; k < n; ++k) out[k] = R(p[k]);
+    return out;
+}
+
+bool event_less(const Event& a, const Event& b) {
+    int ai = std::min(a.i, a.j), aj = std::max(a.i, a.j);
+    int bi = std::min(b.i, b.j), bj = std::max(b.i, b.j);
+    return ai < bi || (ai == bi && aj < bj);
+}
+
+struct StepEvent {
+    int step;
+    Event e;
+};
+
+}  // namespace
+
+struct OracleRun {
+    std::vector<StepEvent> events;
+    int status = 0;
+};
+
+extern "C" {
+
+// drift_one on one body; xv = {x, y, z, vx, vy, vz} updated in place.
+// Returns drift_one's iflg.
+int oracle_drift_one(double mu, double* xv, double dt) {
+    int iflg = 0;
+    oracle::drift_one<double>(mu, xv[0], xv[1], xv[2], xv[3], xv[4], xv[5], dt, iflg);
+    return iflg;
+}
+
+// One mdt_mvs step (mercury6_2.for:3987-4101) over the whole system in place.
+// acc/angf (3n each) and *dtflag carry mdt_mvs's saved state between calls.
+// Pair events are written to ev (up to cap); *count receives the total.
+int oracle_mvs_step(int n, int nbig, const double* m, double* x, double* v, const double* ngf,
+                    int ngflag, const double* jcen, const double* rce, const double* rphys,
+                    double time, double h, double* acc, double* angf, int* dtflag, Event* ev,
+                    int cap, int* count) {
+    MvsState<double> st;
+    st.size(n);
+    std::memcpy(st.a.data(), acc, sizeof(double) * 3 * n);
+    std::memcpy(st.angf.data(), angf, sizeof(double) * 3 * n);
+    st.dtflag = *dtflag;
+    double minside = m[0];
+    for (int j = 1; j < nbig; ++j) {
+        double msofar = minside + m[j];
+        st.gm[j] = m[0] * msofar / minside;
+        minside = msofar;
+    }
+    std::vector<Event> events;
+    int rc = oracle::mdt_mvs<double>(time, h, jcen, n, nbig, m, x, v, rce, rphys, ngf, ngflag, st, events);
+    std::memcpy(acc, st.a.data(), sizeof(double) * 3 * n);
+    std::memcpy(angf, st.angf.data(), sizeof(double) * 3 * n);
+    *dtflag = st.dtflag;
+    *count = (int)events.size();
+    for (int k = 0; k < (int)events.size() && k < cap; ++k) ev[k] = events[k];
+    return rc;
+}
+
+// mce_cent over bodies 2..n (mercury6_2.for:1059-1167).
+int oracle_mce_cent(int n, const double* m, const double* x0, const double* v0, const double* x1,
+                    const double* v1, double time, double h, double rcen, Event* ev, int cap,
+                    int* count) {
+    std::vector<Event> events;
+    oracle::mce_cent<double>(time, h, rcen, 1, n, m, x0, v0, x1, v1, events);
+    *count = (int)events.size();
+    for (int k = 0; k < (int)events.size() && k < cap; ++k) ev[k] = events[k];
+    return 0;
+}
+
+// Output corrector: forward != 0 is mco_mvs2h, forward == 0 is mco_h2mvs.
+int oracle_mvs_corrector(int forward, int n, int nbig, const double* m, const double* x,
+                         const double* v, const double* ngf, int ngflag, const double* jcen,
+                         double h, double* xh, double* vh) {
+    return oracle::mvs_corrector<double>(forward != 0, h, jcen, n, nbig, m, x, v, ngf, ngflag, xh, vh);
+}
+
+// mce_hill (mercury6_2.for:1285-1314): Hill radii and semi-major axes.
+void oracle_mce_hill(int n, const double* m, const double* x, const double* v, double* hill,
+                     double* a) {
+    oracle::mce_hill<double>(n, m, x, v, hill, a);
+}
+
+// The step loop of mal_hcon (mercury6_2.for:700-781) for MVS: nsteps calls of
+// mdt_mvs, each followed (if central != 0) by mce_cent on the heliocentric
+// states before and after the step; time advances by time = time + h.
+// Particles are split into nthreads contiguous ranges; each thread integrates
+// the Big bodies plus its range with the same statements, which gives the
+// same bits as one pass over the whole system because massless bodies never
+// act on anything in the MVS map. (Semi-active Small bodies with mass couple
+// only through the central-body oblateness reaction; with jcen != 0 and such
+// bodies present the run uses one thread.)
+OracleRun* oracle_mvs_run(int n, int nbig, const double* m, double* x, double* v,
+                          const double* ngf, int ngflag, const double* jcen, const double* rce,
+                          const double* rphys, double time0, double h, int nsteps, double rcen,
+                          int central, int nthreads) {
+    OracleRun* run = new OracleRun();
+    int nsmall = n - nbig;
+    bool coupled = false;
+    if (jcen[0] != 0.0 || jcen[1] != 0.0 || jcen[2] != 0.0)
+        for (int j = nbig; j < n; ++j) coupled = coupled || m[j] != 0.0;
+    if (nthreads < 1 || coupled) nthreads = 1;
+    if (nthreads > nsmall) nthreads = std::max(1, nsmall);
+    std::vector<std::vector<StepEvent>> per(nthreads);
+    std::vector<int> status(nthreads, 0), lo(nthreads), hi(nthreads);
+    struct Sub { std::vector<double> m, x, v, g, r, p; };
+    std::vector<Sub> sub(nthreads);
+    // Every thread's subsystem is gathered before any thread starts, and the
+    // results are scattered back after all have joined.
+    for (int t = 0; t < nthreads; ++t) {
+        lo[t] = nbig + (int)((long long)nsmall * t / nthreads);
+        hi[t] = nbig + (int)((long long)nsmall * (t + 1) / nthreads);
+        int ns = nbig + (hi[t] - lo[t]);
+        Sub& S = sub[t];
+        S.m.resize(ns); S.x.resize(3 * ns); S.v.resize(3 * ns); S.g.resize(5 * ns);
+        S.r.resize(ns); S.p.resize(ns);
+        auto take = [&](int dst, int src) {
+            S.m[dst] = m[src]; S.r[dst] = rce[src]; S.p[dst] = rphys[src];
+            for (int c = 0; c < 3; ++c) { S.x[3 * dst + c] = x[3 * src + c]; S.v[3 * dst + c] = v[3 * src + c]; }
+            for (int c = 0; c < 5; ++c) S.g[5 * dst + c] = ngf[5 * src + c];
+        };
+        for (int k = 0; k < nbig; ++k) take(k, k);
+        for (int k = lo[t]; k < hi[t]; ++k) take(nbig + (k - lo[t]), k);
+    }
+    auto work = [&](int t) {
+        Sub& S = sub[t];
+        int ns = (int)S.m.size();
+        int offset = lo[t] - nbig;
+        MvsState<double> st;
+        st.size(ns);
+        std::vector<double> xh0(3 * ns), vh0(3 * ns);
+        std::vector<Event> events;
+        double time = time0;
+        for (int s = 0; s < nsteps; ++s) {
+            std::copy(S.x.begin(), S.x.end(), xh0.begin());
+            std::copy(S.v.begin(), S.v.end(), vh0.begin());
+            events.clear();
+            if (oracle::mdt_mvs<double>(time, h, jcen, ns, nbig, S.m.data(), S.x.data(), S.v.data(),
+                                        S.r.data(), S.p.data(), S.g.data(), ngflag, st, events)) {
+                status[t] = 1;
+                return;
+            }
+            time = time + h;
+            if (central)
+                oracle::mce_cent<double>(time, h, rcen, 1, ns, S.m.data(), xh0.data(), vh0.data(),
+                                         S.x.data(), S.v.data(), events);
+            for (Event e : events) {
+                bool big_only = e.i <= nbig && e.j <= nbig;
+                if (big_only && t != 0) continue;
+                if (e.i > nbig) e.i += offset;
+                if (e.j > nbig) e.j += offset;
+                per[t].push_back(StepEvent{s, e});
+            }
+        }
+    };
+    if (nthreads == 1) work(0);
+    else {
+        std::vector<std::thread> pool;
+        for (int t = 0; t < nthreads; ++t) pool.emplace_back(work, t);
+        for (auto& th : pool) th.join();
+    }
+    for (int t = 0; t < nthreads; ++t) {
+        const Sub& S = sub[t];
+        if (t == 0)
+            for (int k = 0; k < 3 * nbig; ++k) { x[k] = S.x[k]; v[k] = S.v[k]; }
+        for (int k = lo[t]; k < hi[t]; ++k)
+            for (int c = 0; c < 3; ++c) {
+                x[3 * k + c] = S.x[3 * (nbig + k - lo[t]) + c];
+                v[3 * k + c] = S.v[3 * (nbig + k - lo[t]) + c];
+            }
+    }
+    for (int t = 0; t < nthreads; ++t) {
+        run->status |= status[t];
+        run->events.insert(run->events.end(), per[t].begin(), per[t].end());
+    }
+    std::stable_sort(run->events.begin(), run->events.end(), [](const StepEvent& a, const StepEvent& b) {
+        if (a.step != b.step) return a.step < b.step;
+        return event_less(a.e, b.e);
+    });
+    return run;
+}
+
+int oracle_run_status(const OracleRun* run) { return run->status; }
+int oracle_run_event_count(const OracleRun* run) { return (int)run->events.size(); }
+void oracle_run_events(const OracleRun* run, Event* dst, int* steps) {
+    for (size_t k = 0; k < run->events.size(); ++k) {
+        dst[k] = run->events[k].e;
+        if (steps) steps[k] = run->events[k].step;
+    }
+}
+void oracle_run_free(OracleRun* run) { delete run; }
+
+// Algorithmic operation tally of nsteps MVS steps (mdt_mvs + mce_cent) of the
+// given system: out = {add, mul, div, sqrt, cmp, libm}. The state is not
+// modified. Each +,- counts as add, * as mul, / as div.
+void oracle_count_mvs(int n, int nbig, const double* m, const double* x, const double* v,
+                      const double* ngf, int ngflag, const double* jcen, const double* rce,
+                      const double* rphys, double time0, double h, int nsteps, double rcen,
+                      uint64_t* out) {
+    auto cm = widen<Counted>(m, n), cx = widen<Counted>(x, 3 * n), cv = widen<Counted>(v, 3 * n);
+    auto cg = widen<Counted>(ngf, 5 * n), cr = widen<Counted>(rce, n), cp = widen<Counted>(rphys, n);
+    MvsState<Counted> st;
+    st.size(n);
+    std::vector<Counted> xh0(3 * n), vh0(3 * n);
+    std::vector<Event> events;
+    oracle::tally = oracle::Tally();
+    Counted time = time0;
+    for (int s = 0; s < nsteps; ++s) {
+        xh0 = cx;
+        vh0 = cv;
+        events.clear();
+        oracle::mdt_mvs<Counted>(time, Counted(h), jcen, n, nbig, cm.data(), cx.data(), cv.data(),
+                                 cr.data(), cp.data(), cg.data(), ngflag, st, events);
+        time = Counted(time.v + h);
+        oracle::mce_cent<Counted>(time, Counted(h), Counted(rcen), 1, n, cm.data(), xh0.data(),
+                                  vh0.data(), cx.data(), cv.data(), events);
+    }
+    out[0] = oracle::tally.add;
+    out[1] = oracle::tally.mul;
+    out[2] = oracle::tally.div;
+    out[3] = oracle::tally.sqrt;
+    out[4] = oracle::tally.cmp;
+    out[5] = oracle::tally.libm;
+}
+
+}  // extern "C"
