@@ -22,8 +22,10 @@ int report(const std::exception& e) {
 
 namespace {
 
+// Host rows (Fortran layout, row j = body j) to the device SoA: Big bodies by
+// index, Small body j to its slot inv[j - nbig] of the particle arrays.
 __global__ void scatter_kernel(const double* rows, int n, int comps, int nbig, double* big, int bs, double* part,
-                               int ps) {
+                               int ps, const int* inv) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
     for (int c = 0; c < comps; ++c) {
@@ -31,17 +33,17 @@ __global__ void scatter_kernel(const double* rows, int n, int comps, int nbig, d
         if (j < nbig) {
             if (big) big[(size_t)c * bs + j] = v;
         } else {
-            part[(size_t)c * ps + (j - nbig)] = v;
+            part[(size_t)c * ps + inv[j - nbig]] = v;
         }
     }
 }
 
 __global__ void gather_kernel(double* rows, int n, int comps, int nbig, const double* big, int bs,
-                              const double* part, int ps) {
+                              const double* part, int ps, const int* inv) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
     for (int c = 0; c < comps; ++c)
-        rows[(size_t)j * comps + c] = j < nbig ? big[(size_t)c * bs + j] : part[(size_t)c * ps + (j - nbig)];
+        rows[(size_t)j * comps + c] = j < nbig ? big[(size_t)c * bs + j] : part[(size_t)c * ps + inv[j - nbig]];
 }
 
 // mce_cent over every body for the drop-in events call (mercury6_2.for:1059-1167):
@@ -50,6 +52,7 @@ struct CentralArgs {
     int nbig, np, npcap;
     double mu, h, rcen;
     const double *big0, *big1, *part0, *part1, *pm, *mbig;
+    const int* perm;
     MercuryEvent* events;
     int* event_step;
     int cap;
@@ -80,7 +83,7 @@ __global__ void central_kernel(CentralArgs A) {
             p1 = make_double3(A.part1[p], A.part1[S + p], A.part1[2 * S + p]);
             u1 = make_double3(A.part1[3 * S + p], A.part1[4 * S + p], A.part1[5 * S + p]);
             mj = A.pm[p];
-            id = A.nbig + p + 1;
+            id = A.nbig + A.perm[p] + 1;
         }
         hit = central_impact(p0, u0, p1, u1, A.mu, mj, A.h, A.rcen, temp);
     }
@@ -183,6 +186,7 @@ MvsParticleArgs particle_args(int in, int out, int nsteps, int reset, int centra
     a.rce = c.prce.p;
     a.rphys = c.prphys.p;
     a.ngf = c.pngf.p;
+    a.perm = c.perm.p;
     a.tab = tab;
     a.detail = detail;
     a.events = c.events.p;
@@ -223,6 +227,57 @@ void mvs_step_once(double h) {
     }
 }
 
+// Warp-coherent ordering of the Small bodies. drift_dan leaves its elliptic
+// fast path (drift_kepmd) for the Newton solver when dm^2 > 0.16 or
+// e^2 dm^2 >= 0.0016 with dm = n h (or when the orbit is unbound), i.e. when
+// max(e n / 0.04, n / 0.4) * |h| >= 1. Sorting particles by that key (largest
+// first, into 256 logarithmic buckets, stable) puts the bodies that take the
+// long path into the same warps for any step size. The order changes no
+// result: every particle's arithmetic is independent of its slot, and ids
+// are mapped back through perm.
+void order_particles(int n, int nbig, double mu, const double* xx, const double* vv) {
+    Context& c = ctx();
+    const int np = n - nbig;
+    std::vector<int> bucket(np), count(257, 0), perm(c.npcap), inv(c.npcap);
+    for (int p = 0; p < np; ++p) {
+        const double* x = xx + 3 * (size_t)(nbig + p);
+        const double* v = vv + 3 * (size_t)(nbig + p);
+        const double r = std::sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+        const double v2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+        const double u = x[0] * v[0] + x[1] * v[1] + x[2] * v[2];
+        const double alpha = 2.0 * mu / r - v2;
+        int b = 0;  // bucket 0 = highest key
+        if (alpha > 0.0 && std::isfinite(alpha)) {
+            const double a = mu / alpha;
+            const double en = std::sqrt(mu / (a * a * a));
+            const double ec = 1.0 - r / a, es = u / (en * a * a);
+            const double e = std::sqrt(ec * ec + es * es);
+            const double key = std::max(e * en / 0.04, en / 0.4);
+            if (e <= 0.6 && key > 0.0 && std::isfinite(key)) {
+                const double l = std::log2(key) * 8.0 + 128.0;  // key 2^-16 .. 2^16
+                b = 255 - (int)std::min(255.0, std::max(0.0, l));
+                b = std::max(1, b);
+            }
+        }
+        bucket[p] = b;
+        count[b + 1]++;
+    }
+    for (int k = 0; k < 256; ++k) count[k + 1] += count[k];
+    for (int p = 0; p < np; ++p) {
+        const int slot = count[bucket[p]]++;
+        perm[slot] = p;
+        inv[p] = slot;
+    }
+    for (int p = np; p < c.npcap; ++p) {  // padding slot maps to itself
+        perm[p] = p;
+        inv[p] = p;
+    }
+    c.perm.reserve(c.npcap);
+    c.inv.reserve(c.npcap);
+    check(cudaMemcpy(c.perm.p, perm.data(), sizeof(int) * c.npcap, cudaMemcpyHostToDevice), "upload");
+    check(cudaMemcpy(c.inv.p, inv.data(), sizeof(int) * c.npcap, cudaMemcpyHostToDevice), "upload");
+}
+
 void sort_events(std::vector<MercuryEvent>& ev, std::vector<int>* steps) {
     std::vector<size_t> idx(ev.size());
     for (size_t k = 0; k < idx.size(); ++k) idx[k] = k;
@@ -249,7 +304,8 @@ void download_buffer(int which, double* xx, double* vv) {
     for (int part = 0; part < 2; ++part) {
         const double* big = c.bigstate[which].p + 3 * part * c.nbig;
         const double* prt = c.pstate[which].p + (size_t)3 * part * c.npcap;
-        gather_kernel<<<blocks(c.n), 256, 0, c.stream>>>(c.transfer.p, c.n, 3, c.nbig, big, c.nbig, prt, c.npcap);
+        gather_kernel<<<blocks(c.n), 256, 0, c.stream>>>(c.transfer.p, c.n, 3, c.nbig, big, c.nbig, prt, c.npcap,
+                                                          c.inv.p);
         check(cudaMemcpyAsync(part ? vv : xx, c.transfer.p, sizeof(double) * 3 * c.n, cudaMemcpyDeviceToHost,
                               c.stream),
               "download");
@@ -260,12 +316,12 @@ void download_buffer(int which, double* xx, double* vv) {
 }  // namespace
 
 void scatter_rows(const double* rows, int n, int comps, int nbig, double* big, int big_stride, double* part,
-                  int part_stride, cudaStream_t s) {
-    scatter_kernel<<<blocks(n), 256, 0, s>>>(rows, n, comps, nbig, big, big_stride, part, part_stride);
+                  int part_stride, const int* inv, cudaStream_t s) {
+    scatter_kernel<<<blocks(n), 256, 0, s>>>(rows, n, comps, nbig, big, big_stride, part, part_stride, inv);
 }
 void gather_rows(double* rows, int n, int comps, int nbig, const double* big, int big_stride, const double* part,
-                 int part_stride, cudaStream_t s) {
-    gather_kernel<<<blocks(n), 256, 0, s>>>(rows, n, comps, nbig, big, big_stride, part, part_stride);
+                 int part_stride, const int* inv, cudaStream_t s) {
+    gather_kernel<<<blocks(n), 256, 0, s>>>(rows, n, comps, nbig, big, big_stride, part, part_stride, inv);
 }
 
 }  // namespace mb200
@@ -348,12 +404,13 @@ int mercury_cuda_upload(int n, int nbig, int pn, int ngflag, const double* m, co
         check(cudaMemsetAsync(c.prphys.p, 0, sizeof(double) * c.npcap, s), "memset");
         check(cudaMemsetAsync(c.pngf.p, 0, sizeof(double) * 5 * c.npcap, s), "memset");
         c.cur = 0;
+        order_particles(n, nbig, m[0], xx, vv);
         // positions and velocities
         for (int part = 0; part < 2; ++part) {
             check(cudaMemcpyAsync(c.transfer.p, part ? vv : xx, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s),
                   "upload");
             scatter_rows(c.transfer.p, n, 3, nbig, c.bigstate[0].p + 3 * part * nbig, nbig,
-                         c.pstate[0].p + (size_t)3 * part * c.npcap, c.npcap, s);
+                         c.pstate[0].p + (size_t)3 * part * c.npcap, c.npcap, c.inv.p, s);
             check(cudaStreamSynchronize(s), "upload");
         }
         // per-body scalars: masses, radii
@@ -362,14 +419,14 @@ int mercury_cuda_upload(int n, int nbig, int pn, int ngflag, const double* m, co
         double* pdst[3] = {c.pm.p, c.prce.p, c.prphys.p};
         for (int q = 0; q < 3; ++q) {
             check(cudaMemcpyAsync(c.transfer.p, scalars[q], sizeof(double) * n, cudaMemcpyHostToDevice, s), "upload");
-            scatter_rows(c.transfer.p, n, 1, nbig, bigdst[q], nbig, pdst[q], c.npcap, s);
+            scatter_rows(c.transfer.p, n, 1, nbig, bigdst[q], nbig, pdst[q], c.npcap, c.inv.p, s);
             check(cudaStreamSynchronize(s), "upload");
         }
         // ngf: Big rows stay interleaved (5 per body); particles become SoA
         check(cudaMemcpyAsync(c.ngfbig.p, ng, sizeof(double) * 5 * nbig, cudaMemcpyHostToDevice, s), "upload");
         c.transfer.reserve((size_t)6 * n);
         check(cudaMemcpyAsync(c.transfer.p, ng, sizeof(double) * 5 * n, cudaMemcpyHostToDevice, s), "upload");
-        scatter_rows(c.transfer.p, n, 5, nbig, nullptr, 0, c.pngf.p, c.npcap, s);
+        scatter_rows(c.transfer.p, n, 5, nbig, nullptr, 0, c.pngf.p, c.npcap, c.inv.p, s);
         check(cudaStreamSynchronize(s), "upload");
         check(cudaGetLastError(), "upload");
         c.reset = true;
@@ -433,6 +490,7 @@ int mercury_cuda_events(double time, double h, double rcen, const MercuryEvent**
                 a.part1 = c.pstate[c.cur].p;
                 a.pm = c.pm.p;
                 a.mbig = c.mbig.p;
+                a.perm = c.perm.p;
                 a.events = c.events.p;
                 a.event_step = c.event_step.p;
                 a.cap = (int)c.events.n;
@@ -503,7 +561,7 @@ int mercury_cuda_limits(const double* limits) {
     try {
         require_system();
         check(cudaMemcpyAsync(c.transfer.p, limits, sizeof(double) * c.n, cudaMemcpyHostToDevice, c.stream), "limits");
-        scatter_rows(c.transfer.p, c.n, 1, c.nbig, c.rcebig.p, c.nbig, c.prce.p, c.npcap, c.stream);
+        scatter_rows(c.transfer.p, c.n, 1, c.nbig, c.rcebig.p, c.nbig, c.prce.p, c.npcap, c.inv.p, c.stream);
         check(cudaStreamSynchronize(c.stream), "limits");
         return 0;
     } catch (const std::exception& e) {

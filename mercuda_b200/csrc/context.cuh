@@ -56,6 +56,7 @@ struct Context {
     // particles
     DBuf<double> pstate[2];     // [9][npcap]
     DBuf<double> pm, prce, prphys, pngf;
+    DBuf<int> perm, inv;        // slot -> particle index, particle index -> slot
     int cur = 0;
     bool reset = true;
     bool stepped = false;
@@ -104,6 +105,8 @@ struct Context {
         DBuf<double>* bufs[] = {&mbig, &rcebig, &rphysbig, &ngfbig, &bigstate[0], &bigstate[1], &pstate[0],
                                 &pstate[1], &pm, &prce, &prphys, &pngf, &tab, &detail, &transfer, &snapshot};
         for (auto* b : bufs) b->release();
+        perm.release();
+        inv.release();
         events.release();
         event_step.release();
         status.release();
@@ -119,9 +122,9 @@ Context& ctx();
 
 // Layout kernels between the host's interleaved rows and the device SoA.
 void scatter_rows(const double* rows, int n, int comps, int nbig, double* big, int big_stride, double* part,
-                  int part_stride, cudaStream_t s);
+                  int part_stride, const int* inv, cudaStream_t s);
 void gather_rows(double* rows, int n, int comps, int nbig, const double* big, int big_stride, const double* part,
-                 int part_stride, cudaStream_t s);
+                 int part_stride, const int* inv, cudaStream_t s);
 
 int report(const std::exception& e);
 

@@ -231,10 +231,13 @@ __device__ __forceinline__ bool drift_dan(double mu, double3& p, double3& w, dou
 
 // drift_one: the drift, else ten substeps of dt/10 (stopping at a failed one).
 // The flag is discarded by all MVS/HYBRID callers (mdt_mvs, mdt_hy, mco_mvs2h).
+// Written as one loop so that drift_dan is instantiated once: attempt 0 is the
+// whole step, attempts 1..10 the substeps.
 __device__ __forceinline__ void drift_one(double mu, double3& p, double3& w, double dt) {
-    if (drift_dan(mu, p, w, dt)) return;
-    for (int i = 1; i <= 10; ++i) {
-        if (!drift_dan(mu, p, w, dt / 10.0)) return;
+    const double sub = dt / 10.0;
+    for (int attempt = 0; attempt <= 10; ++attempt) {
+        const bool ok = drift_dan(mu, p, w, attempt == 0 ? dt : sub);
+        if (attempt == 0 ? ok : !ok) return;
     }
 }
 

@@ -7,46 +7,22 @@
 #include "mvs.cuh"
 #include "mvs_device.cuh"
 
+// Minimum resident CTAs per SM requested from ptxas for the particle kernel
+// (bounds its registers per thread at 65536 / (128 * this)).
+#ifndef MB200_PARTICLE_MIN_BLOCKS
+#define MB200_PARTICLE_MIN_BLOCKS 3
+#endif
+// Unroll factor of the per-Big-body force loop (ILP against code size).
+#ifndef MB200_FORCE_UNROLL
+#define MB200_FORCE_UNROLL 1
+#endif
+
 namespace mb200 {
 
 namespace {
 
 constexpr unsigned FULL = 0xffffffffu;
-
-// Warp-aggregated append of this lane's record (if `has`) to the event list:
-// one atomic per warp, slots assigned in lane order by a ballot prefix count.
-// Must be reached by all 32 lanes.
-__device__ __forceinline__ void emit_event(bool has, const MercuryEvent& rec, int step, MercuryEvent* events,
-                                           int* event_step, int cap, DeviceStatus* st) {
-    const unsigned mask = __ballot_sync(FULL, has);
-    if (mask == 0) return;
-    const int lane = threadIdx.x & 31;
-    const int leader = __ffs(mask) - 1;
-    int base = 0;
-    if (lane == leader) base = atomicAdd(&st->events, __popc(mask));
-    base = __shfl_sync(FULL, base, leader);
-    if (has) {
-        const int slot = base + __popc(mask & ((1u << lane) - 1u));
-        if (slot < cap) {
-            store_event(events + slot, rec);
-            event_step[slot] = step;
-        } else {
-            atomicExch(&st->overflow, 1);
-        }
-    }
-}
-
-// Scalar append used by the single-CTA Big-body kernel (rare events).
-__device__ __forceinline__ void append_event(const MercuryEvent& rec, int step, MercuryEvent* events,
-                                             int* event_step, int cap, DeviceStatus* st) {
-    const int slot = atomicAdd(&st->events, 1);
-    if (slot < cap) {
-        store_event(events + slot, rec);
-        event_step[slot] = step;
-    } else {
-        atomicExch(&st->overflow, 1);
-    }
-}
+constexpr int kForceUnroll = MB200_FORCE_UNROLL;
 
 __device__ __forceinline__ double3 ld3(const double* p, int stride, int k) {
     return make_double3(p[k], p[stride + k], p[2 * stride + k]);
@@ -348,10 +324,16 @@ __global__ void __launch_bounds__(128) mvs_big_kernel(MvsBigArgs A) {
             if (!(hi_i >= lo_j && hi_j >= lo_i && yhi_i >= ylo_j && yhi_j >= ylo_i)) continue;
             PairEnds I{ld3(S.X0, N, i), ld3(S.V0, N, i), ld3(S.X, N, i), ld3(S.V, N, i)};
             PairEnds J{ld3(S.X0, N, j), ld3(S.V0, N, j), ld3(S.X, N, j), ld3(S.V, N, j)};
-            MercuryEvent rec;
-            if (pair_event(I, J, A.rce[i], A.rce[j], A.rphys[i], A.rphys[j], h, hm1, i + 1, j + 1,
-                           A.m[j] > A.m[i], &rec))
-                append_event(rec, A.step0 + s, A.events, A.event_step, A.event_cap, A.status);
+            PairClass pc;
+            if (pair_classify(I, J, A.rce[i], A.rce[j], A.rphys[i], A.rphys[j], h, pc)) {
+                const int slot = atomicAdd(&A.status->events, 1);
+                if (slot < A.event_cap) {
+                    pair_record(A.events + slot, I, J, pc, hm1, i + 1, j + 1, A.m[j] > A.m[i]);
+                    A.event_step[slot] = A.step0 + s;
+                } else {
+                    atomicExch(&A.status->overflow, 1);
+                }
+            }
         }
         __syncthreads();
         big_force(A, S, S.V);
@@ -367,13 +349,19 @@ __global__ void __launch_bounds__(128) mvs_big_kernel(MvsBigArgs A) {
                 double temp;
                 if (central_impact(ld3(S.XS, N, k), ld3(S.VS, N, k), ld3(S.X, N, k), ld3(S.V, N, k), A.m[0],
                                    A.m[k], h, A.rcen, temp)) {
-                    MercuryEvent rec = {};
-                    rec.i = 1;
-                    rec.j = k + 1;
-                    rec.kind = EV_CENTRAL;
-                    rec.time = temp;
-                    rec.distance = A.rcen;
-                    append_event(rec, A.step0 + s, A.events, A.event_step, A.event_cap, A.status);
+                    const int slot = atomicAdd(&A.status->events, 1);
+                    if (slot < A.event_cap) {
+                        MercuryEvent rec = {};
+                        rec.i = 1;
+                        rec.j = k + 1;
+                        rec.kind = EV_CENTRAL;
+                        rec.time = temp;
+                        rec.distance = A.rcen;
+                        store_event(A.events + slot, rec);
+                        A.event_step[slot] = A.step0 + s;
+                    } else {
+                        atomicExch(&A.status->overflow, 1);
+                    }
                 }
             }
     }
@@ -387,9 +375,53 @@ __global__ void __launch_bounds__(128) mvs_big_kernel(MvsBigArgs A) {
 }
 
 // ------------------------------------------------------------ test particles
+// Warp-aggregated slot claim: one atomic per warp, slots in lane order by a
+// ballot prefix count; -1 for lanes without a record or beyond capacity.
+// Must be reached by all 32 lanes.
+__device__ __forceinline__ int claim_slot(bool has, int cap, DeviceStatus* st) {
+    const unsigned mask = __ballot_sync(FULL, has);
+    if (mask == 0) return -1;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(mask) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(&st->events, __popc(mask));
+    base = __shfl_sync(FULL, base, leader);
+    if (!has) return -1;
+    const int slot = base + __popc(mask & ((1u << lane) - 1u));
+    if (slot >= cap) {
+        atomicExch(&st->overflow, 1);
+        return -1;
+    }
+    return slot;
+}
+
 struct Particle {
     double3 x, v, acc;
     double rce, rphys, m;
+    double g[5];
+};
+
+// Shared-memory parking of a thread's second particle while the first runs:
+// thread-private slots, one column per thread so that lanes hit distinct banks.
+template <bool NGF> struct Park {
+    __device__ static void put(double* park, const Particle& P) {
+        const int t = threadIdx.x, n = blockDim.x;
+        park[0 * n + t] = P.x.x; park[1 * n + t] = P.x.y; park[2 * n + t] = P.x.z;
+        park[3 * n + t] = P.v.x; park[4 * n + t] = P.v.y; park[5 * n + t] = P.v.z;
+        park[6 * n + t] = P.acc.x; park[7 * n + t] = P.acc.y; park[8 * n + t] = P.acc.z;
+        park[9 * n + t] = P.rce; park[10 * n + t] = P.rphys; park[11 * n + t] = P.m;
+        if (NGF)
+            for (int c = 0; c < 5; ++c) park[(12 + c) * n + t] = P.g[c];
+    }
+    __device__ static void get(const double* park, Particle& P) {
+        const int t = threadIdx.x, n = blockDim.x;
+        P.x = make_double3(park[0 * n + t], park[1 * n + t], park[2 * n + t]);
+        P.v = make_double3(park[3 * n + t], park[4 * n + t], park[5 * n + t]);
+        P.acc = make_double3(park[6 * n + t], park[7 * n + t], park[8 * n + t]);
+        P.rce = park[9 * n + t]; P.rphys = park[10 * n + t]; P.m = park[11 * n + t];
+        if (NGF)
+            for (int c = 0; c < 5; ++c) P.g[c] = park[(12 + c) * n + t];
+    }
 };
 
 // mfo_mvs for one Small body (mercury6_2.for:5034-5060) plus mfo_ngf, i.e. the
@@ -399,6 +431,7 @@ __device__ __forceinline__ double3 particle_force(const double3 x, const double3
                                                   const double* T, int nb, const double* jcen, double mu,
                                                   DeviceStatus* st) {
     double3 a3 = make_double3(0.0, 0.0, 0.0);
+#pragma unroll kForceUnroll
     for (int b = 0; b < nb; ++b) {
         const double* row = T + TAB_HEAD + b * TAB_BODY;
         const double dx = x.x - row[0], dy = x.y - row[1], dz = x.z - row[2];
@@ -428,9 +461,10 @@ __device__ __forceinline__ double3 particle_force(const double3 x, const double3
     return a;
 }
 
+// One mdt_mvs step of one Small body against the staged table T of step s.
 template <bool NGF, bool OBL, bool CENTRAL>
-__device__ __forceinline__ void particle_step(Particle& P, bool ok, int p, const double* g, const double* T,
-                                              int s, const MvsParticleArgs& A, double hby2, double hm1) {
+__device__ __forceinline__ void particle_step(Particle& P, bool ok, int p, const double* T, int s,
+                                              const MvsParticleArgs& A, double hby2, double hm1) {
     const int nb = A.nb;
     const double h = A.h;
     double3 xs, vs, x0, v0;
@@ -452,24 +486,30 @@ __device__ __forceinline__ void particle_step(Particle& P, bool ok, int p, const
         byhi = byhi + pad;
     }
     // mce_stat against each Big body; the loop is uniform across the warp.
+#pragma unroll 1
     for (int b = 0; b < nb; ++b) {
         const double* row = T + TAB_HEAD + b * TAB_BODY;
         const bool cand = ok && row[5] >= bxlo && bxhi >= row[4] && row[7] >= bylo && byhi >= row[6];
         if (__any_sync(FULL, cand)) {
-            MercuryEvent rec;
+            PairEnds I, J;
+            PairClass pc;
             bool has = false;
             if (cand) {
                 const double* d = A.detail + ((size_t)s * nb + b) * TAB_DETAIL;
-                PairEnds I{make_double3(d[0], d[1], d[2]), make_double3(d[3], d[4], d[5]),
-                           make_double3(d[6], d[7], d[8]), make_double3(d[9], d[10], d[11])};
-                PairEnds J{x0, v0, P.x, P.v};
-                has = pair_event(I, J, d[12], P.rce, d[13], P.rphys, h, hm1, b + 2, A.nbig + p + 1, false, &rec);
+                I = PairEnds{make_double3(d[0], d[1], d[2]), make_double3(d[3], d[4], d[5]),
+                             make_double3(d[6], d[7], d[8]), make_double3(d[9], d[10], d[11])};
+                J = PairEnds{x0, v0, P.x, P.v};
+                has = pair_classify(I, J, d[12], P.rce, d[13], P.rphys, h, pc);
             }
-            emit_event(has, rec, A.step0 + s, A.events, A.event_step, A.event_cap, A.status);
+            const int slot = claim_slot(has, A.event_cap, A.status);
+            if (slot >= 0) {
+                pair_record(A.events + slot, I, J, pc, hm1, b + 2, A.nbig + A.perm[p] + 1, false);
+                A.event_step[slot] = A.step0 + s;
+            }
         }
     }
     if (ok) {
-        P.acc = particle_force<NGF, OBL>(P.x, P.v, g, T, nb, A.jcen, A.mu, A.status);
+        P.acc = particle_force<NGF, OBL>(P.x, P.v, P.g, T, nb, A.jcen, A.mu, A.status);
         P.v.x = P.v.x + hby2 * P.acc.x;
         P.v.y = P.v.y + hby2 * P.acc.y;
         P.v.z = P.v.z + hby2 * P.acc.z;
@@ -477,23 +517,27 @@ __device__ __forceinline__ void particle_step(Particle& P, bool ok, int p, const
     if (CENTRAL) {
         double temp = 0.0;
         const bool hit = ok && central_impact(xs, vs, P.x, P.v, A.mu, P.m, h, A.rcen, temp);
-        MercuryEvent rec = {};
-        if (hit) {
-            rec.i = 1;
-            rec.j = A.nbig + p + 1;
-            rec.kind = EV_CENTRAL;
-            rec.time = temp;
-            rec.distance = A.rcen;
+        const int slot = claim_slot(hit, A.event_cap, A.status);
+        if (slot >= 0) {
+            MercuryEvent* e = A.events + slot;
+            *reinterpret_cast<int4*>(e) = make_int4(1, A.nbig + A.perm[p] + 1, EV_CENTRAL, 0);
+            reinterpret_cast<double2*>(e)[1] = make_double2(A.rcen, temp);
+            A.event_step[slot] = A.step0 + s;
         }
-        emit_event(hit, rec, A.step0 + s, A.events, A.event_step, A.event_cap, A.status);
     }
 }
 
+// Test-particle kernel: each thread owns a pair of adjacent particles (one
+// double2 per state component), runs the first through all K steps while the
+// second waits in shared memory, then the second; the Big-body tables of the
+// K steps are staged in shared memory once per CTA.
 template <bool NGF, bool OBL, bool CENTRAL>
-__global__ void __launch_bounds__(128) mvs_particle_kernel(MvsParticleArgs A) {
-    extern __shared__ double stab[];
+__global__ void __launch_bounds__(128, MB200_PARTICLE_MIN_BLOCKS) mvs_particle_kernel(MvsParticleArgs A) {
+    extern __shared__ double smem[];
     const int nb = A.nb, stride = tab_stride(nb);
     const int rows = A.nsteps + (A.reset ? 1 : 0);
+    double* stab = smem;
+    double* park = smem + (size_t)rows * stride;
     const double* gtab = A.tab + (A.reset ? 0 : stride);
     for (int k = threadIdx.x; k < rows * stride; k += blockDim.x) stab[k] = gtab[k];
     __syncthreads();
@@ -502,67 +546,64 @@ __global__ void __launch_bounds__(128) mvs_particle_kernel(MvsParticleArgs A) {
     const int lane = threadIdx.x & 31;
     const int npairs = (A.np + 1) >> 1;
     const int ntiles = (npairs + blockDim.x - 1) / blockDim.x;
-    const int S = A.npcap;
+    const int S = A.npcap, H = S / 2;
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const int pair = tile * blockDim.x + threadIdx.x;
         if (pair - lane >= npairs) continue;  // whole warp past the end
         const bool live = pair < npairs;
         const int j0 = 2 * pair;
-        // Two particles per thread (one double2 per component); the step body is
-        // instantiated once and applied to each in turn by swapping registers.
-        Particle Pa, Pb;
-        double ga[5], gb[5];
+        Particle P;
         if (live) {
             const double2* in = reinterpret_cast<const double2*>(A.xin);
-            const int q = pair, H = S / 2;
-            double2 t;
-            t = in[0 * H + q]; Pa.x.x = t.x; Pb.x.x = t.y;
-            t = in[1 * H + q]; Pa.x.y = t.x; Pb.x.y = t.y;
-            t = in[2 * H + q]; Pa.x.z = t.x; Pb.x.z = t.y;
-            t = in[3 * H + q]; Pa.v.x = t.x; Pb.v.x = t.y;
-            t = in[4 * H + q]; Pa.v.y = t.x; Pb.v.y = t.y;
-            t = in[5 * H + q]; Pa.v.z = t.x; Pb.v.z = t.y;
-            t = in[6 * H + q]; Pa.acc.x = t.x; Pb.acc.x = t.y;
-            t = in[7 * H + q]; Pa.acc.y = t.x; Pb.acc.y = t.y;
-            t = in[8 * H + q]; Pa.acc.z = t.x; Pb.acc.z = t.y;
-            t = reinterpret_cast<const double2*>(A.rce)[q]; Pa.rce = t.x; Pb.rce = t.y;
-            t = reinterpret_cast<const double2*>(A.rphys)[q]; Pa.rphys = t.x; Pb.rphys = t.y;
-            t = reinterpret_cast<const double2*>(A.m)[q]; Pa.m = t.x; Pb.m = t.y;
+            double2 t[12];
+#pragma unroll
+            for (int c = 0; c < 9; ++c) t[c] = in[c * H + pair];
+            t[9] = reinterpret_cast<const double2*>(A.rce)[pair];
+            t[10] = reinterpret_cast<const double2*>(A.rphys)[pair];
+            t[11] = reinterpret_cast<const double2*>(A.m)[pair];
+            Particle Q;
+            P.x = make_double3(t[0].x, t[1].x, t[2].x);
+            P.v = make_double3(t[3].x, t[4].x, t[5].x);
+            P.acc = make_double3(t[6].x, t[7].x, t[8].x);
+            P.rce = t[9].x; P.rphys = t[10].x; P.m = t[11].x;
+            Q.x = make_double3(t[0].y, t[1].y, t[2].y);
+            Q.v = make_double3(t[3].y, t[4].y, t[5].y);
+            Q.acc = make_double3(t[6].y, t[7].y, t[8].y);
+            Q.rce = t[9].y; Q.rphys = t[10].y; Q.m = t[11].y;
             if (NGF)
                 for (int c = 0; c < 5; ++c) {
-                    t = reinterpret_cast<const double2*>(A.ngf + (size_t)c * S)[q];
-                    ga[c] = t.x;
-                    gb[c] = t.y;
+                    const double2 tg = reinterpret_cast<const double2*>(A.ngf + (size_t)c * S)[pair];
+                    P.g[c] = tg.x;
+                    Q.g[c] = tg.y;
                 }
+            Park<NGF>::put(park, Q);
         }
-        bool oka = live && j0 < A.np, okb = live && j0 + 1 < A.np;
-        if (A.reset) {
-            if (oka) Pa.acc = particle_force<NGF, OBL>(Pa.x, Pa.v, ga, stab, nb, A.jcen, A.mu, A.status);
-            if (okb) Pb.acc = particle_force<NGF, OBL>(Pb.x, Pb.v, gb, stab, nb, A.jcen, A.mu, A.status);
-        }
-        for (int s = 0; s < A.nsteps; ++s) {
-            const double* T = steps_tab + s * stride;
 #pragma unroll 1
-            for (int u = 0; u < 2; ++u) {
-                particle_step<NGF, OBL, CENTRAL>(Pa, oka, j0 + u, ga, T, s, A, hby2, hm1);
-                const Particle tp = Pa; Pa = Pb; Pb = tp;
-                const bool tk = oka; oka = okb; okb = tk;
-                if (NGF)
-                    for (int c = 0; c < 5; ++c) { const double tg = ga[c]; ga[c] = gb[c]; gb[c] = tg; }
+        for (int u = 0; u < 2; ++u) {
+            const bool ok = live && j0 + u < A.np;
+            if (u == 1 && live) {
+                // park the first particle's result, take the second
+                Particle done = P;
+                Park<NGF>::get(park, P);
+                Park<NGF>::put(park, done);
             }
+            if (A.reset && ok) P.acc = particle_force<NGF, OBL>(P.x, P.v, P.g, stab, nb, A.jcen, A.mu, A.status);
+            for (int s = 0; s < A.nsteps; ++s)
+                particle_step<NGF, OBL, CENTRAL>(P, ok, j0 + u, steps_tab + s * stride, s, A, hby2, hm1);
         }
         if (live) {
+            Particle F;
+            Park<NGF>::get(park, F);
             double2* out = reinterpret_cast<double2*>(A.xout);
-            const int q = pair, H = S / 2;
-            out[0 * H + q] = make_double2(Pa.x.x, Pb.x.x);
-            out[1 * H + q] = make_double2(Pa.x.y, Pb.x.y);
-            out[2 * H + q] = make_double2(Pa.x.z, Pb.x.z);
-            out[3 * H + q] = make_double2(Pa.v.x, Pb.v.x);
-            out[4 * H + q] = make_double2(Pa.v.y, Pb.v.y);
-            out[5 * H + q] = make_double2(Pa.v.z, Pb.v.z);
-            out[6 * H + q] = make_double2(Pa.acc.x, Pb.acc.x);
-            out[7 * H + q] = make_double2(Pa.acc.y, Pb.acc.y);
-            out[8 * H + q] = make_double2(Pa.acc.z, Pb.acc.z);
+            out[0 * H + pair] = make_double2(F.x.x, P.x.x);
+            out[1 * H + pair] = make_double2(F.x.y, P.x.y);
+            out[2 * H + pair] = make_double2(F.x.z, P.x.z);
+            out[3 * H + pair] = make_double2(F.v.x, P.v.x);
+            out[4 * H + pair] = make_double2(F.v.y, P.v.y);
+            out[5 * H + pair] = make_double2(F.v.z, P.v.z);
+            out[6 * H + pair] = make_double2(F.acc.x, P.acc.x);
+            out[7 * H + pair] = make_double2(F.acc.y, P.acc.y);
+            out[8 * H + pair] = make_double2(F.acc.z, P.acc.z);
         }
     }
 }
@@ -570,7 +611,7 @@ __global__ void __launch_bounds__(128) mvs_particle_kernel(MvsParticleArgs A) {
 template <bool NGF, bool OBL, bool CENTRAL>
 void launch_variant(const MvsParticleArgs& a, cudaStream_t s, int threads) {
     auto kern = mvs_particle_kernel<NGF, OBL, CENTRAL>;
-    const size_t smem = mvs_particle_smem(a.nb, a.nsteps, a.reset);
+    const size_t smem = mvs_particle_smem(a.nb, a.nsteps, a.reset, threads, NGF);
     if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     const int npairs = (a.np + 1) / 2;
     int tiles = (npairs + threads - 1) / threads;
@@ -585,8 +626,9 @@ void launch_variant(const MvsParticleArgs& a, cudaStream_t s, int threads) {
 
 }  // namespace
 
-size_t mvs_particle_smem(int nb, int nsteps, int reset) {
-    return sizeof(double) * (size_t)tab_stride(nb) * (size_t)(nsteps + (reset ? 1 : 0));
+size_t mvs_particle_smem(int nb, int nsteps, int reset, int threads, bool ngf) {
+    return sizeof(double) * ((size_t)tab_stride(nb) * (size_t)(nsteps + (reset ? 1 : 0)) +
+                             (size_t)threads * (ngf ? 17 : 12));
 }
 
 int mvs_max_steps_per_launch(int nb) {

@@ -73,6 +73,7 @@ struct MvsParticleArgs {
     const double* rce;
     const double* rphys;
     const double* ngf;  // [5][npcap]
+    const int* perm;    // slot -> particle index (ids of event records)
     const double* tab;
     const double* detail;
     MercuryEvent* events;
@@ -83,7 +84,7 @@ struct MvsParticleArgs {
 
 void launch_mvs_big(const MvsBigArgs& a, cudaStream_t s);
 void launch_mvs_particles(const MvsParticleArgs& a, cudaStream_t s, int threads);
-size_t mvs_particle_smem(int nb, int nsteps, int reset);
+size_t mvs_particle_smem(int nb, int nsteps, int reset, int threads, bool ngf);
 int mvs_max_steps_per_launch(int nb);
 
 }  // namespace mb200

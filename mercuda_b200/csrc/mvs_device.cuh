@@ -110,14 +110,16 @@ struct PairEnds {
     double3 x0, v0, x1, v1;
 };
 
-// mce_stat's test for one pair (i Big, j after it; mercury6_2.for:1815-1908).
-// Fills the merged event record and returns true when the pair is a close-
-// encounter minimum, a near miss or a collision. `swap` lists body j first
-// (the more massive Big body). rec->time holds tmin; the caller adds the end
-// time of the step.
-__device__ __forceinline__ bool pair_event(const PairEnds& I, const PairEnds& J, double rce_i, double rce_j,
-                                           double rphys_i, double rphys_j, double h, double hm1, int id_i,
-                                           int id_j, bool swap, MercuryEvent* rec) {
+// Classification of one pair by mce_stat's test (mercury6_2.for:1815-1908).
+struct PairClass {
+    double d2min, tmin;
+    int kind, now;
+};
+
+// mce_stat for one pair (i Big, j after it): true when the pair is a close-
+// encounter minimum (kind bit 1), a near miss (2) or a collision (4).
+__device__ __forceinline__ bool pair_classify(const PairEnds& I, const PairEnds& J, double rce_i, double rce_j,
+                                              double rphys_i, double rphys_j, double h, PairClass& pc) {
     const double dx0 = I.x0.x - J.x0.x, dy0 = I.x0.y - J.x0.y, dz0 = I.x0.z - J.x0.z;
     const double du0 = I.v0.x - J.v0.x, dv0 = I.v0.y - J.v0.y, dw0 = I.v0.z - J.v0.z;
     const double d0t = (dx0 * du0 + dy0 * dv0 + dz0 * dw0) * 2.0;
@@ -135,30 +137,33 @@ __device__ __forceinline__ bool pair_event(const PairEnds& I, const PairEnds& J,
     const double d2near = d2hit * 4.0;
     const bool clo = (d2min <= d2ce && d0t * h <= 0.0 && d1t * h >= 0.0) || (d2min <= d2hit);
     const bool near = d2min <= d2near;
-    if (!clo && !near) return false;
+    pc.d2min = d2min;
+    pc.tmin = tmin;
+    pc.kind = (clo ? EV_CLOSE : 0) | (near ? EV_NEAR : 0) | (d2min <= d2hit ? EV_HIT : 0);
+    pc.now = d1 <= d2hit ? 1 : 0;
+    return clo || near;
+}
+
+// Writes the merged record of a classified pair straight into its slot:
+// ids 1-based with the more massive Big body first (`swap` lists J first),
+// time holding tmin (the caller's host adds the step's end time), states
+// linearly interpolated to tmin as mce_stat:1869-1882 does.
+__device__ __forceinline__ void pair_record(MercuryEvent* dst, const PairEnds& I, const PairEnds& J,
+                                            const PairClass& pc, double hm1, int id_i, int id_j, bool swap) {
     const PairEnds& A = swap ? J : I;
     const PairEnds& B = swap ? I : J;
-    rec->i = swap ? id_j : id_i;
-    rec->j = swap ? id_i : id_j;
-    rec->kind = (clo ? EV_CLOSE : 0) | (near ? EV_NEAR : 0) | (d2min <= d2hit ? EV_HIT : 0);
-    rec->now = d1 <= d2hit ? 1 : 0;
-    rec->time = tmin;
-    rec->distance = sqrt(d2min > 0.0 ? d2min : 0.0);
-    const double tmp0 = -(tmin * hm1);
-    const double tmp1 = 1.0 + tmin * hm1;
-    rec->xi[0] = tmp0 * A.x0.x + tmp1 * A.x1.x;
-    rec->xi[1] = tmp0 * A.x0.y + tmp1 * A.x1.y;
-    rec->xi[2] = tmp0 * A.x0.z + tmp1 * A.x1.z;
-    rec->xi[3] = tmp0 * A.v0.x + tmp1 * A.v1.x;
-    rec->xi[4] = tmp0 * A.v0.y + tmp1 * A.v1.y;
-    rec->xi[5] = tmp0 * A.v0.z + tmp1 * A.v1.z;
-    rec->xj[0] = tmp0 * B.x0.x + tmp1 * B.x1.x;
-    rec->xj[1] = tmp0 * B.x0.y + tmp1 * B.x1.y;
-    rec->xj[2] = tmp0 * B.x0.z + tmp1 * B.x1.z;
-    rec->xj[3] = tmp0 * B.v0.x + tmp1 * B.v1.x;
-    rec->xj[4] = tmp0 * B.v0.y + tmp1 * B.v1.y;
-    rec->xj[5] = tmp0 * B.v0.z + tmp1 * B.v1.z;
-    return true;
+    const double tmp0 = -(pc.tmin * hm1);
+    const double tmp1 = 1.0 + pc.tmin * hm1;
+    double2* d = reinterpret_cast<double2*>(dst);
+    int4 head = make_int4(swap ? id_j : id_i, swap ? id_i : id_j, pc.kind, pc.now);
+    *reinterpret_cast<int4*>(dst) = head;
+    d[1] = make_double2(sqrt(pc.d2min > 0.0 ? pc.d2min : 0.0), pc.tmin);
+    d[2] = make_double2(tmp0 * A.x0.x + tmp1 * A.x1.x, tmp0 * A.x0.y + tmp1 * A.x1.y);
+    d[3] = make_double2(tmp0 * A.x0.z + tmp1 * A.x1.z, tmp0 * A.v0.x + tmp1 * A.v1.x);
+    d[4] = make_double2(tmp0 * A.v0.y + tmp1 * A.v1.y, tmp0 * A.v0.z + tmp1 * A.v1.z);
+    d[5] = make_double2(tmp0 * B.x0.x + tmp1 * B.x1.x, tmp0 * B.x0.y + tmp1 * B.x1.y);
+    d[6] = make_double2(tmp0 * B.x0.z + tmp1 * B.x1.z, tmp0 * B.v0.x + tmp1 * B.v1.x);
+    d[7] = make_double2(tmp0 * B.v0.y + tmp1 * B.v1.y, tmp0 * B.v0.z + tmp1 * B.v1.z);
 }
 
 // mce_cent for one body (mercury6_2.for:1091-1160), algor != 11. (p0,u0) is the

@@ -164,7 +164,7 @@ def test_backwards_integration(backend, oracle):
 def test_event_buffer_growth(backend, oracle):
     """More simultaneous encounter records than the initial buffer (4,096):
     the step is redone with a larger buffer and nothing is dropped."""
-    sys0 = make_system(seed=4, n_particles=9000, near_fraction=1.0, planet_kw=dict(mmin=1e-3, mmax=1e-3))
+    sys0 = make_system(seed=4, n_particles=20000, near_fraction=1.0, planet_kw=dict(mmin=1e-3, mmax=1e-3))
     sys0.rce[1:sys0.nbig] *= 20.0
     backend.upload(sys0)
     backend.step(0.0, 8.0, dtflag=0)
