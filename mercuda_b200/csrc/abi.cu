@@ -192,8 +192,40 @@ MvsParticleArgs particle_args(int in, int out, int nsteps, int reset, int centra
     a.events = c.events.p;
     a.event_step = c.event_step.p;
     a.event_cap = (int)c.events.n;
+    a.cands = c.cands.p;
+    a.cand_cap = (int)c.cands.n;
     a.status = c.status.p;
     return a;
+}
+
+// Particle kernel of one launch followed by the classification of its
+// encounter candidates into event records (same stream).
+void particles_and_events(const MvsParticleArgs& pa, cudaStream_t s) {
+    Context& c = ctx();
+    check(cudaMemsetAsync(&c.status.p->next_tile, 0, sizeof(int), s), "memset");
+    launch_mvs_particles(pa, s, c.particle_threads);
+    ClassifyArgs ca;
+    ca.nb = c.nbig - 1;
+    ca.nbig = c.nbig;
+    ca.h = pa.h;
+    ca.detail = c.detail.p;
+    ca.cands = c.cands.p;
+    ca.cand_cap = (int)c.cands.n;
+    ca.events = c.events.p;
+    ca.event_step = c.event_step.p;
+    ca.event_cap = (int)c.events.n;
+    ca.status = c.status.p;
+    if (ca.nb > 0) launch_classify(ca, s);
+    check(cudaMemsetAsync(&c.status.p->cands, 0, sizeof(int), s), "memset");
+}
+
+// Grows the event or candidate buffer after an overflow flagged in the status.
+void grow_after_overflow() {
+    Context& c = ctx();
+    if (c.status_host->overflow & 1) ensure_events(std::max(2 * (int)c.events.n, c.status_host->events + 1024));
+    if (c.status_host->overflow & 2) {
+        c.cands.reserve(2 * c.cands.n + 4096);
+    }
 }
 
 // One MVS step (mdt_mvs) of the whole system: Big-body CTA then the particle
@@ -208,14 +240,13 @@ void mvs_step_once(double h) {
         const int reset = c.reset ? 1 : 0;
         launch_mvs_big(big_args(in, out, 1, reset, 0, 0, h, 0.0, c.tab.p, c.detail.p), c.stream);
         if (c.np > 0)
-            launch_mvs_particles(particle_args(in, out, 1, reset, 0, 0, h, 0.0, c.tab.p, c.detail.p), c.stream,
-                                 c.particle_threads);
+            particles_and_events(particle_args(in, out, 1, reset, 0, 0, h, 0.0, c.tab.p, c.detail.p), c.stream);
         check(cudaGetLastError(), "launch");
         read_status();
         if (c.status_host->fault) throw std::runtime_error("MVS force failed");
         if (c.status_host->overflow) {
             if (attempt > 8) throw std::runtime_error("event buffer growth failed");
-            ensure_events(std::max(2 * (int)c.events.n, c.status_host->events + 1024));
+            grow_after_overflow();
             continue;  // the input buffers are untouched: redo the step
         }
         c.nforces += 1 + reset;
@@ -392,6 +423,7 @@ int mercury_cuda_upload(int n, int nbig, int pn, int ngflag, const double* m, co
         c.pngf.reserve((size_t)5 * c.npcap);
         c.status.reserve(1);
         ensure_events(std::max(4096, c.np / 64));
+        c.cands.reserve(std::max(16384, c.np / 2));
         c.transfer.reserve((size_t)6 * n);
         cudaStream_t s = c.stream;
         // zero padding and cached accelerations
@@ -643,8 +675,8 @@ int mercury_b200_mvs_advance(double time, double h, int nsteps, double rcen, int
                 if (c.np > 0) {
                     check(cudaStreamWaitEvent(c.stream, c.chunk_done[ch], 0), "wait");
                     check(cudaEventRecord(c.kt0[ch], c.stream), "event");
-                    launch_mvs_particles(particle_args(pcur, 1 - pcur, ks, reset, 1, s0, h, rcen, tab, det), c.stream,
-                                         c.particle_threads);
+                    particles_and_events(particle_args(pcur, 1 - pcur, ks, reset, 1, s0, h, rcen, tab, det),
+                                         c.stream);
                     check(cudaEventRecord(c.kt1[ch], c.stream), "event");
                 }
                 pcur = 1 - pcur;
@@ -671,7 +703,7 @@ int mercury_b200_mvs_advance(double time, double h, int nsteps, double rcen, int
                 break;
             }
             if (attempt > 8) throw std::runtime_error("event buffer growth failed");
-            ensure_events(std::max(2 * (int)c.events.n, c.status_host->events + 1024));
+            grow_after_overflow();
             check(cudaMemcpyAsync(c.pstate[c.cur].p, c.snapshot.p, sizeof(double) * 9 * c.npcap,
                                   cudaMemcpyDeviceToDevice, c.stream),
                   "restore");

@@ -28,8 +28,19 @@ constexpr int EV_CLOSE = 1, EV_NEAR = 2, EV_HIT = 4, EV_CENTRAL = 8;
 struct DeviceStatus {
     int fault;
     int events;        // pair/central events claimed (may exceed capacity)
-    int overflow;      // 1 if any event slot was beyond capacity
-    int pad;
+    int overflow;      // bit 0: an event slot was beyond capacity; bit 1: a candidate slot
+    int cands;         // encounter candidates claimed in the current launch
+    int next_tile;     // dynamic work counter of the current particle launch
+    int pad[3];
+};
+
+// A Small body whose padded x-y box overlapped a Big body's box during one
+// step (mce_stat's first test): enough to finish mce_stat's test and write the
+// record without the particle kernel holding the record path's registers.
+struct EncounterCandidate {
+    int slot, body, step, id;   // particle slot, Big body index - 1, global step, Fortran id
+    double rce, rphys;
+    double x0[3], v0[3], x1[3], v1[3];
 };
 
 __device__ __forceinline__ void raise_fault(DeviceStatus* st, int bit) { atomicOr(&st->fault, bit); }

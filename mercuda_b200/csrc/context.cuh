@@ -65,6 +65,7 @@ struct Context {
     // events
     DBuf<MercuryEvent> events;
     DBuf<int> event_step;
+    DBuf<EncounterCandidate> cands;
     DBuf<DeviceStatus> status;
     DeviceStatus* status_host = nullptr;
     std::vector<MercuryEvent> host_events;
@@ -109,6 +110,7 @@ struct Context {
         inv.release();
         events.release();
         event_step.release();
+        cands.release();
         status.release();
         host_events.clear();
         host_steps.clear();

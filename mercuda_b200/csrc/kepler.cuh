@@ -33,6 +33,7 @@ __device__ __forceinline__ void stumpff(double x, double& c0, double& c1, double
          1.666666666666667e-1;
     c1 = 1.0 - x * c3;
     c0 = 1.0 - x * c2;
+#pragma unroll 1
     for (int i = n; i >= 1; --i) {
         c3 = (c2 + c0 * c3) * 0.25;
         c2 = c1 * c1 * 0.5;
@@ -53,7 +54,7 @@ __device__ __forceinline__ double kepu_residual(double dt, double r0, double mu,
 }
 
 // drift_kepu_p3solve: Cardano seed for alpha <= 0. Returns false when no real root.
-__device__ __noinline__ bool kepu_cubic_seed(double dt, double r0, double mu, double alpha, double u,
+static __device__ __noinline__ bool kepu_cubic_seed(double dt, double r0, double mu, double alpha, double u,
                                              double& s) {
     const double denom = (mu - alpha * r0) / 6.0;
     const double a2 = 0.5 * u / denom;
@@ -102,6 +103,7 @@ __device__ __forceinline__ double kepu_guess(double dt, double r0, double mu, do
 __device__ __forceinline__ bool kepu_newton(double& s, double dt, double r0, double mu, double alpha,
                                             double u, double& fp, double& c1, double& c2, double& c3) {
     const double tol = DANBYB * DANBYB;
+#pragma unroll 1
     for (int nc = 0; nc <= 6; ++nc) {
         const double s2 = s * s;
         double c0;
@@ -124,9 +126,10 @@ __device__ __forceinline__ bool kepu_newton(double& s, double dt, double r0, dou
 }
 
 // drift_kepu_lag: Laguerre iteration (n = 5), at most 401 passes; rarely taken.
-__device__ __noinline__ bool kepu_laguerre(double& s, double dt, double r0, double mu, double alpha,
+static __device__ __noinline__ bool kepu_laguerre(double& s, double dt, double r0, double mu, double alpha,
                                            double u, double& fp, double& c1, double& c2, double& c3) {
     const double ln = 5.0, tol = DANBYB * DANBYB;
+#pragma unroll 1
     for (int nc = 0; nc <= 400; ++nc) {
         double c0;
         stumpff(s * s * alpha, c0, c1, c2, c3);
@@ -235,6 +238,7 @@ __device__ __forceinline__ bool drift_dan(double mu, double3& p, double3& w, dou
 // whole step, attempts 1..10 the substeps.
 __device__ __forceinline__ void drift_one(double mu, double3& p, double3& w, double dt) {
     const double sub = dt / 10.0;
+#pragma unroll 1
     for (int attempt = 0; attempt <= 10; ++attempt) {
         const bool ok = drift_dan(mu, p, w, attempt == 0 ? dt : sub);
         if (attempt == 0 ? ok : !ok) return;

@@ -10,7 +10,7 @@
 // Minimum resident CTAs per SM requested from ptxas for the particle kernel
 // (bounds its registers per thread at 65536 / (128 * this)).
 #ifndef MB200_PARTICLE_MIN_BLOCKS
-#define MB200_PARTICLE_MIN_BLOCKS 3
+#define MB200_PARTICLE_MIN_BLOCKS 5
 #endif
 // Unroll factor of the per-Big-body force loop (ILP against code size).
 #ifndef MB200_FORCE_UNROLL
@@ -378,56 +378,48 @@ __global__ void __launch_bounds__(128) mvs_big_kernel(MvsBigArgs A) {
 // Warp-aggregated slot claim: one atomic per warp, slots in lane order by a
 // ballot prefix count; -1 for lanes without a record or beyond capacity.
 // Must be reached by all 32 lanes.
-__device__ __forceinline__ int claim_slot(bool has, int cap, DeviceStatus* st) {
+__device__ __forceinline__ int claim_slot(bool has, int cap, DeviceStatus* st, int* counter, int overflow_bit) {
     const unsigned mask = __ballot_sync(FULL, has);
     if (mask == 0) return -1;
     const int lane = threadIdx.x & 31;
     const int leader = __ffs(mask) - 1;
     int base = 0;
-    if (lane == leader) base = atomicAdd(&st->events, __popc(mask));
+    if (lane == leader) base = atomicAdd(counter, __popc(mask));
     base = __shfl_sync(FULL, base, leader);
     if (!has) return -1;
     const int slot = base + __popc(mask & ((1u << lane) - 1u));
     if (slot >= cap) {
-        atomicExch(&st->overflow, 1);
+        atomicOr(&st->overflow, overflow_bit);
         return -1;
     }
     return slot;
 }
 
-struct Particle {
-    double3 x, v, acc;
-    double rce, rphys, m;
-    double g[5];
-};
-
-// Shared-memory parking of a thread's second particle while the first runs:
-// thread-private slots, one column per thread so that lanes hit distinct banks.
-template <bool NGF> struct Park {
-    __device__ static void put(double* park, const Particle& P) {
-        const int t = threadIdx.x, n = blockDim.x;
-        park[0 * n + t] = P.x.x; park[1 * n + t] = P.x.y; park[2 * n + t] = P.x.z;
-        park[3 * n + t] = P.v.x; park[4 * n + t] = P.v.y; park[5 * n + t] = P.v.z;
-        park[6 * n + t] = P.acc.x; park[7 * n + t] = P.acc.y; park[8 * n + t] = P.acc.z;
-        park[9 * n + t] = P.rce; park[10 * n + t] = P.rphys; park[11 * n + t] = P.m;
-        if (NGF)
-            for (int c = 0; c < 5; ++c) park[(12 + c) * n + t] = P.g[c];
-    }
-    __device__ static void get(const double* park, Particle& P) {
-        const int t = threadIdx.x, n = blockDim.x;
-        P.x = make_double3(park[0 * n + t], park[1 * n + t], park[2 * n + t]);
-        P.v = make_double3(park[3 * n + t], park[4 * n + t], park[5 * n + t]);
-        P.acc = make_double3(park[6 * n + t], park[7 * n + t], park[8 * n + t]);
-        P.rce = park[9 * n + t]; P.rphys = park[10 * n + t]; P.m = park[11 * n + t];
-        if (NGF)
-            for (int c = 0; c < 5; ++c) P.g[c] = park[(12 + c) * n + t];
-    }
+// Thread-private shared-memory columns of the particle kernel, one double per
+// thread per column (column-major, so the lanes of a warp hit distinct banks).
+// Only x, v and the cached acceleration of the particle being advanced live in
+// registers; its constants, its pre-drift state and the second particle of the
+// thread's pair wait here, which keeps the drift's register footprint small.
+struct Cols {
+    static constexpr int PARK = 0;     // 9: x, v, acc of the waiting particle
+    static constexpr int RCE = 9;      // 2: per particle of the pair
+    static constexpr int RPHYS = 11;   // 2
+    static constexpr int MASS = 13;    // 2
+    static constexpr int X0 = 15;      // 3: state after the first kick
+    static constexpr int V0 = 18;      // 3
+    static constexpr int CEN = 21;     // 4: mce_cent start quantities
+    static constexpr int NGF = 25;     // 10: five coefficients per particle
+    static constexpr int count(bool ngf) { return ngf ? 35 : 25; }
+    volatile double* base;
+    __device__ volatile double& at(int c) const { return base[c * blockDim.x + threadIdx.x]; }
+    __device__ double3 ld3(int c) const { return make_double3(at(c), at(c + 1), at(c + 2)); }
+    __device__ void st3(int c, double3 v) const { at(c) = v.x; at(c + 1) = v.y; at(c + 2) = v.z; }
 };
 
 // mfo_mvs for one Small body (mercury6_2.for:5034-5060) plus mfo_ngf, i.e. the
 // total acceleration (angf + 0) + a of the kick; T is a staged force table.
 template <bool NGF, bool OBL>
-__device__ __forceinline__ double3 particle_force(const double3 x, const double3 v_ngf, const double* g,
+__device__ __forceinline__ double3 particle_force(const double3 x, const double3 v_ngf, const Cols& cols, int u,
                                                   const double* T, int nb, const double* jcen, double mu,
                                                   DeviceStatus* st) {
     double3 a3 = make_double3(0.0, 0.0, 0.0);
@@ -451,6 +443,8 @@ __device__ __forceinline__ double3 particle_force(const double3 x, const double3
         a.z = a.z + (ao.z - T[5]);
     }
     if (NGF) {
+        double g[5];
+        for (int c = 0; c < 5; ++c) g[c] = cols.at(Cols::NGF + 5 * u + c);
         double3 ng;
         if (!nongrav_accel(x, v_ngf, g, ng)) raise_fault(st, 2);
         a.x = ng.x + 0.0 + a.x;
@@ -461,25 +455,32 @@ __device__ __forceinline__ double3 particle_force(const double3 x, const double3
     return a;
 }
 
-// One mdt_mvs step of one Small body against the staged table T of step s.
+// One mdt_mvs step of one Small body (slot p, pair member u) against the staged
+// table T of step s.
 template <bool NGF, bool OBL, bool CENTRAL>
-__device__ __forceinline__ void particle_step(Particle& P, bool ok, int p, const double* T, int s,
-                                              const MvsParticleArgs& A, double hby2, double hm1) {
+__device__ __forceinline__ void particle_step(double3& x, double3& v, double3& acc, bool ok, int p, int u,
+                                              const Cols& cols, const double* T, int s, const MvsParticleArgs& A,
+                                              double hby2, double hm1) {
     const int nb = A.nb;
     const double h = A.h;
-    double3 xs, vs, x0, v0;
     double bxlo = 0.0, bxhi = 0.0, bylo = 0.0, byhi = 0.0;
     if (ok) {
-        if (CENTRAL) { xs = P.x; vs = P.v; }
-        P.v.x = P.v.x + hby2 * P.acc.x;
-        P.v.y = P.v.y + hby2 * P.acc.y;
-        P.v.z = P.v.z + hby2 * P.acc.z;
-        x0 = P.x;
-        v0 = P.v;
-        drift_one(A.mu, P.x, P.v, h);
-        box_extent(x0.x, P.x.x, v0.x, P.v.x, h, bxlo, bxhi);
-        box_extent(x0.y, P.x.y, v0.y, P.v.y, h, bylo, byhi);
-        const double pad = P.rce * 1.2;
+        if (CENTRAL) {
+            const CentralStart c = central_start(x, v);
+            cols.at(Cols::CEN) = c.rr0;
+            cols.at(Cols::CEN + 1) = c.rv0;
+            cols.at(Cols::CEN + 2) = c.h2;
+            cols.at(Cols::CEN + 3) = c.v2;
+        }
+        v.x = v.x + hby2 * acc.x;
+        v.y = v.y + hby2 * acc.y;
+        v.z = v.z + hby2 * acc.z;
+        cols.st3(Cols::X0, x);
+        cols.st3(Cols::V0, v);
+        drift_one(A.mu, x, v, h);
+        box_extent(cols.at(Cols::X0), x.x, cols.at(Cols::V0), v.x, h, bxlo, bxhi);
+        box_extent(cols.at(Cols::X0 + 1), x.y, cols.at(Cols::V0 + 1), v.y, h, bylo, byhi);
+        const double pad = cols.at(Cols::RCE + u) * 1.2;
         bxlo = bxlo - pad;
         bxhi = bxhi + pad;
         bylo = bylo - pad;
@@ -491,33 +492,36 @@ __device__ __forceinline__ void particle_step(Particle& P, bool ok, int p, const
         const double* row = T + TAB_HEAD + b * TAB_BODY;
         const bool cand = ok && row[5] >= bxlo && bxhi >= row[4] && row[7] >= bylo && byhi >= row[6];
         if (__any_sync(FULL, cand)) {
-            PairEnds I, J;
-            PairClass pc;
-            bool has = false;
-            if (cand) {
-                const double* d = A.detail + ((size_t)s * nb + b) * TAB_DETAIL;
-                I = PairEnds{make_double3(d[0], d[1], d[2]), make_double3(d[3], d[4], d[5]),
-                             make_double3(d[6], d[7], d[8]), make_double3(d[9], d[10], d[11])};
-                J = PairEnds{x0, v0, P.x, P.v};
-                has = pair_classify(I, J, d[12], P.rce, d[13], P.rphys, h, pc);
-            }
-            const int slot = claim_slot(has, A.event_cap, A.status);
+            const int slot = claim_slot(cand, A.cand_cap, A.status, &A.status->cands, 2);
             if (slot >= 0) {
-                pair_record(A.events + slot, I, J, pc, hm1, b + 2, A.nbig + A.perm[p] + 1, false);
-                A.event_step[slot] = A.step0 + s;
+                EncounterCandidate* c = A.cands + slot;
+                *reinterpret_cast<int4*>(c) = make_int4(p, b, A.step0 + s, A.nbig + A.perm[p] + 1);
+                double2* w = reinterpret_cast<double2*>(c);
+                w[1] = make_double2(cols.at(Cols::RCE + u), cols.at(Cols::RPHYS + u));
+                w[2] = make_double2(cols.at(Cols::X0), cols.at(Cols::X0 + 1));
+                w[3] = make_double2(cols.at(Cols::X0 + 2), cols.at(Cols::V0));
+                w[4] = make_double2(cols.at(Cols::V0 + 1), cols.at(Cols::V0 + 2));
+                w[5] = make_double2(x.x, x.y);
+                w[6] = make_double2(x.z, v.x);
+                w[7] = make_double2(v.y, v.z);
             }
         }
     }
     if (ok) {
-        P.acc = particle_force<NGF, OBL>(P.x, P.v, P.g, T, nb, A.jcen, A.mu, A.status);
-        P.v.x = P.v.x + hby2 * P.acc.x;
-        P.v.y = P.v.y + hby2 * P.acc.y;
-        P.v.z = P.v.z + hby2 * P.acc.z;
+        acc = particle_force<NGF, OBL>(x, v, cols, u, T, nb, A.jcen, A.mu, A.status);
+        v.x = v.x + hby2 * acc.x;
+        v.y = v.y + hby2 * acc.y;
+        v.z = v.z + hby2 * acc.z;
     }
     if (CENTRAL) {
         double temp = 0.0;
-        const bool hit = ok && central_impact(xs, vs, P.x, P.v, A.mu, P.m, h, A.rcen, temp);
-        const int slot = claim_slot(hit, A.event_cap, A.status);
+        bool hit = false;
+        if (ok) {
+            const CentralStart c{cols.at(Cols::CEN), cols.at(Cols::CEN + 1), cols.at(Cols::CEN + 2),
+                                 cols.at(Cols::CEN + 3)};
+            hit = central_finish(c, x, v, A.mu, cols.at(Cols::MASS + u), h, A.rcen, temp);
+        }
+        const int slot = claim_slot(hit, A.event_cap, A.status, &A.status->events, 1);
         if (slot >= 0) {
             MercuryEvent* e = A.events + slot;
             *reinterpret_cast<int4*>(e) = make_int4(1, A.nbig + A.perm[p] + 1, EV_CENTRAL, 0);
@@ -527,17 +531,17 @@ __device__ __forceinline__ void particle_step(Particle& P, bool ok, int p, const
     }
 }
 
-// Test-particle kernel: each thread owns a pair of adjacent particles (one
-// double2 per state component), runs the first through all K steps while the
-// second waits in shared memory, then the second; the Big-body tables of the
-// K steps are staged in shared memory once per CTA.
+// Test-particle kernel: each thread owns a pair of adjacent particle slots (one
+// double2 per state component), advances the first through all K steps while
+// the second waits in shared memory, then the second; the Big-body tables of
+// the K steps are staged in shared memory once per CTA.
 template <bool NGF, bool OBL, bool CENTRAL>
 __global__ void __launch_bounds__(128, MB200_PARTICLE_MIN_BLOCKS) mvs_particle_kernel(MvsParticleArgs A) {
     extern __shared__ double smem[];
     const int nb = A.nb, stride = tab_stride(nb);
     const int rows = A.nsteps + (A.reset ? 1 : 0);
     double* stab = smem;
-    double* park = smem + (size_t)rows * stride;
+    const Cols cols{smem + (size_t)rows * stride};
     const double* gtab = A.tab + (A.reset ? 0 : stride);
     for (int k = threadIdx.x; k < rows * stride; k += blockDim.x) stab[k] = gtab[k];
     __syncthreads();
@@ -545,65 +549,98 @@ __global__ void __launch_bounds__(128, MB200_PARTICLE_MIN_BLOCKS) mvs_particle_k
     const double hby2 = 0.5 * A.h, hm1 = 1.0 / A.h;
     const int lane = threadIdx.x & 31;
     const int npairs = (A.np + 1) >> 1;
-    const int ntiles = (npairs + blockDim.x - 1) / blockDim.x;
+    // Warps claim 32-pair tiles from a launch-wide counter: slots are ordered
+    // slowest-first (Newton-path particles lead), so claiming dynamically
+    // balances the SMs (longest-processing-time-first).
+    const int ntiles = (npairs + 31) >> 5;
     const int S = A.npcap, H = S / 2;
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const int pair = tile * blockDim.x + threadIdx.x;
-        if (pair - lane >= npairs) continue;  // whole warp past the end
+    const double2* in = reinterpret_cast<const double2*>(A.xin);
+    double2* out = reinterpret_cast<double2*>(A.xout);
+    for (;;) {
+        int tile = 0;
+        if (lane == 0) tile = atomicAdd(&A.status->next_tile, 1);
+        tile = __shfl_sync(FULL, tile, 0);
+        if (tile >= ntiles) break;
+        const int pair = tile * 32 + lane;
         const bool live = pair < npairs;
         const int j0 = 2 * pair;
-        Particle P;
+        double3 x, v, acc;
         if (live) {
-            const double2* in = reinterpret_cast<const double2*>(A.xin);
-            double2 t[12];
+            double2 t[9];
 #pragma unroll
             for (int c = 0; c < 9; ++c) t[c] = in[c * H + pair];
-            t[9] = reinterpret_cast<const double2*>(A.rce)[pair];
-            t[10] = reinterpret_cast<const double2*>(A.rphys)[pair];
-            t[11] = reinterpret_cast<const double2*>(A.m)[pair];
-            Particle Q;
-            P.x = make_double3(t[0].x, t[1].x, t[2].x);
-            P.v = make_double3(t[3].x, t[4].x, t[5].x);
-            P.acc = make_double3(t[6].x, t[7].x, t[8].x);
-            P.rce = t[9].x; P.rphys = t[10].x; P.m = t[11].x;
-            Q.x = make_double3(t[0].y, t[1].y, t[2].y);
-            Q.v = make_double3(t[3].y, t[4].y, t[5].y);
-            Q.acc = make_double3(t[6].y, t[7].y, t[8].y);
-            Q.rce = t[9].y; Q.rphys = t[10].y; Q.m = t[11].y;
+            x = make_double3(t[0].x, t[1].x, t[2].x);
+            v = make_double3(t[3].x, t[4].x, t[5].x);
+            acc = make_double3(t[6].x, t[7].x, t[8].x);
+#pragma unroll
+            for (int c = 0; c < 9; ++c) cols.at(Cols::PARK + c) = t[c].y;
+            const double2 rc = reinterpret_cast<const double2*>(A.rce)[pair];
+            const double2 rp = reinterpret_cast<const double2*>(A.rphys)[pair];
+            const double2 ms = reinterpret_cast<const double2*>(A.m)[pair];
+            cols.at(Cols::RCE) = rc.x; cols.at(Cols::RCE + 1) = rc.y;
+            cols.at(Cols::RPHYS) = rp.x; cols.at(Cols::RPHYS + 1) = rp.y;
+            cols.at(Cols::MASS) = ms.x; cols.at(Cols::MASS + 1) = ms.y;
             if (NGF)
                 for (int c = 0; c < 5; ++c) {
-                    const double2 tg = reinterpret_cast<const double2*>(A.ngf + (size_t)c * S)[pair];
-                    P.g[c] = tg.x;
-                    Q.g[c] = tg.y;
+                    const double2 g = reinterpret_cast<const double2*>(A.ngf + (size_t)c * S)[pair];
+                    cols.at(Cols::NGF + c) = g.x;
+                    cols.at(Cols::NGF + 5 + c) = g.y;
                 }
-            Park<NGF>::put(park, Q);
         }
 #pragma unroll 1
         for (int u = 0; u < 2; ++u) {
             const bool ok = live && j0 + u < A.np;
             if (u == 1 && live) {
-                // park the first particle's result, take the second
-                Particle done = P;
-                Park<NGF>::get(park, P);
-                Park<NGF>::put(park, done);
+                // the first particle's result waits; the second comes in
+                const double3 px = cols.ld3(Cols::PARK), pv = cols.ld3(Cols::PARK + 3),
+                              pa = cols.ld3(Cols::PARK + 6);
+                cols.st3(Cols::PARK, x);
+                cols.st3(Cols::PARK + 3, v);
+                cols.st3(Cols::PARK + 6, acc);
+                x = px;
+                v = pv;
+                acc = pa;
             }
-            if (A.reset && ok) P.acc = particle_force<NGF, OBL>(P.x, P.v, P.g, stab, nb, A.jcen, A.mu, A.status);
+            if (A.reset && ok) acc = particle_force<NGF, OBL>(x, v, cols, u, stab, nb, A.jcen, A.mu, A.status);
             for (int s = 0; s < A.nsteps; ++s)
-                particle_step<NGF, OBL, CENTRAL>(P, ok, j0 + u, steps_tab + s * stride, s, A, hby2, hm1);
+                particle_step<NGF, OBL, CENTRAL>(x, v, acc, ok, j0 + u, u, cols, steps_tab + s * stride, s, A, hby2,
+                                                 hm1);
         }
         if (live) {
-            Particle F;
-            Park<NGF>::get(park, F);
-            double2* out = reinterpret_cast<double2*>(A.xout);
-            out[0 * H + pair] = make_double2(F.x.x, P.x.x);
-            out[1 * H + pair] = make_double2(F.x.y, P.x.y);
-            out[2 * H + pair] = make_double2(F.x.z, P.x.z);
-            out[3 * H + pair] = make_double2(F.v.x, P.v.x);
-            out[4 * H + pair] = make_double2(F.v.y, P.v.y);
-            out[5 * H + pair] = make_double2(F.v.z, P.v.z);
-            out[6 * H + pair] = make_double2(F.acc.x, P.acc.x);
-            out[7 * H + pair] = make_double2(F.acc.y, P.acc.y);
-            out[8 * H + pair] = make_double2(F.acc.z, P.acc.z);
+            const double3 fx = cols.ld3(Cols::PARK), fv = cols.ld3(Cols::PARK + 3), fa = cols.ld3(Cols::PARK + 6);
+            out[0 * H + pair] = make_double2(fx.x, x.x);
+            out[1 * H + pair] = make_double2(fx.y, x.y);
+            out[2 * H + pair] = make_double2(fx.z, x.z);
+            out[3 * H + pair] = make_double2(fv.x, v.x);
+            out[4 * H + pair] = make_double2(fv.y, v.y);
+            out[5 * H + pair] = make_double2(fv.z, v.z);
+            out[6 * H + pair] = make_double2(fa.x, acc.x);
+            out[7 * H + pair] = make_double2(fa.y, acc.y);
+            out[8 * H + pair] = make_double2(fa.z, acc.z);
+        }
+    }
+}
+
+// mce_stat's test for each encounter candidate of the last launch
+// (mercury6_2.for:1815-1908) and the record it produces.
+__global__ void __launch_bounds__(256) classify_kernel(ClassifyArgs A) {
+    const int count = min(A.status->cands, A.cand_cap);
+    const double hm1 = 1.0 / A.h;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
+        const EncounterCandidate& c = A.cands[k];
+        const double* d = A.detail + ((size_t)c.step * A.nb + c.body) * TAB_DETAIL;
+        const PairEnds I{make_double3(d[0], d[1], d[2]), make_double3(d[3], d[4], d[5]),
+                         make_double3(d[6], d[7], d[8]), make_double3(d[9], d[10], d[11])};
+        const PairEnds J{make_double3(c.x0[0], c.x0[1], c.x0[2]), make_double3(c.v0[0], c.v0[1], c.v0[2]),
+                         make_double3(c.x1[0], c.x1[1], c.x1[2]), make_double3(c.v1[0], c.v1[1], c.v1[2])};
+        PairClass pc;
+        if (!pair_classify(I, J, d[12], c.rce, d[13], c.rphys, A.h, pc)) continue;
+        const int slot = atomicAdd(&A.status->events, 1);
+        if (slot < A.event_cap) {
+            pair_record(A.events + slot, I, J, pc, hm1, c.body + 2, c.id, false);
+            A.event_step[slot] = c.step;
+        } else {
+            atomicOr(&A.status->overflow, 1);
         }
     }
 }
@@ -628,16 +665,22 @@ void launch_variant(const MvsParticleArgs& a, cudaStream_t s, int threads) {
 
 size_t mvs_particle_smem(int nb, int nsteps, int reset, int threads, bool ngf) {
     return sizeof(double) * ((size_t)tab_stride(nb) * (size_t)(nsteps + (reset ? 1 : 0)) +
-                             (size_t)threads * (ngf ? 17 : 12));
+                             (size_t)threads * Cols::count(ngf));
 }
 
+// Steps fused per launch: the staged tables are kept to ~18 KB so that, with
+// the 25.6 KB of per-thread columns, five 128-thread CTAs fit on an SM.
 int mvs_max_steps_per_launch(int nb) {
-    const size_t budget = 64 * 1024;
+    const size_t budget = 18 * 1024;
     const size_t row = sizeof(double) * (size_t)tab_stride(nb);
     long k = (long)(budget / row) - 1;
     if (k < 1) k = 1;
     if (k > 64) k = 64;
     return (int)k;
+}
+
+void launch_classify(const ClassifyArgs& a, cudaStream_t s) {
+    classify_kernel<<<296, 256, 0, s>>>(a);
 }
 
 void launch_mvs_big(const MvsBigArgs& a, cudaStream_t s) {

@@ -79,8 +79,25 @@ struct MvsParticleArgs {
     MercuryEvent* events;
     int* event_step;
     int event_cap;
+    EncounterCandidate* cands;
+    int cand_cap;
     DeviceStatus* status;
 };
+
+// Finishes mce_stat's test for the candidates of the last particle launch and
+// writes the event records; detail is the base of the run's detail rows.
+struct ClassifyArgs {
+    int nb, nbig;
+    double h;
+    const double* detail;
+    const EncounterCandidate* cands;
+    int cand_cap;
+    MercuryEvent* events;
+    int* event_step;
+    int event_cap;
+    DeviceStatus* status;
+};
+void launch_classify(const ClassifyArgs& a, cudaStream_t s);
 
 void launch_mvs_big(const MvsBigArgs& a, cudaStream_t s);
 void launch_mvs_particles(const MvsParticleArgs& a, cudaStream_t s, int threads);

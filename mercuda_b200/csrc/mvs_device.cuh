@@ -166,28 +166,37 @@ __device__ __forceinline__ void pair_record(MercuryEvent* dst, const PairEnds& I
     d[7] = make_double2(tmp0 * B.v0.y + tmp1 * B.v1.y, tmp0 * B.v0.z + tmp1 * B.v1.z);
 }
 
-// mce_cent for one body (mercury6_2.for:1091-1160), algor != 11. (p0,u0) is the
-// heliocentric state at the start of the step, (p1,u1) at its end. Returns
-// true on an impact and the entry time offset `temp` from the step's start,
-// so that the event time is (time_end - h) + temp.
-__device__ __forceinline__ bool central_impact(const double3 p0, const double3 u0, const double3 p1,
-                                               const double3 u1, double mcen, double mj, double h,
-                                               double rcen, double& temp) {
-    const double rcen2 = rcen * rcen;
-    const double rr0 = p0.x * p0.x + p0.y * p0.y + p0.z * p0.z;
-    const double rr1 = p1.x * p1.x + p1.y * p1.y + p1.z * p1.z;
-    const double rv0 = u0.x * p0.x + u0.y * p0.y + u0.z * p0.z;
-    const double rv1 = u1.x * p1.x + u1.y * p1.y + u1.z * p1.z;
-    const double rmin = rr0 < rr1 ? rr0 : rr1;
-    if (!((rv0 * h <= 0.0 && rv1 * h >= 0.0) || rmin <= rcen2)) return false;
+// mce_cent for one body (mercury6_2.for:1091-1160), algor != 11, split into
+// the start-of-step quantities (|x0|^2, v0.x0, |x0 x v0|^2, |v0|^2) and the
+// test at the end of the step, so that a caller may keep four numbers instead
+// of the start state. Returns true on an impact with the entry time offset
+// `temp` from the step's start; the event time is (time_end - h) + temp.
+struct CentralStart {
+    double rr0, rv0, h2, v2;
+};
+
+__device__ __forceinline__ CentralStart central_start(const double3 p0, const double3 u0) {
+    CentralStart c;
+    c.rr0 = p0.x * p0.x + p0.y * p0.y + p0.z * p0.z;
+    c.rv0 = u0.x * p0.x + u0.y * p0.y + u0.z * p0.z;
     const double hx = p0.y * u0.z - p0.z * u0.y;
     const double hy = p0.z * u0.x - p0.x * u0.z;
     const double hz = p0.x * u0.y - p0.y * u0.x;
-    const double v2 = u0.x * u0.x + u0.y * u0.y + u0.z * u0.z;
-    const double h2 = hx * hx + hy * hy + hz * hz;
-    const double p = h2 / (mcen + mj);
-    const double r0 = sqrt(rr0);
-    double t = 1.0 + p * (v2 / (mcen + mj) - 2.0 / r0);
+    c.v2 = u0.x * u0.x + u0.y * u0.y + u0.z * u0.z;
+    c.h2 = hx * hx + hy * hy + hz * hz;
+    return c;
+}
+
+static __device__ __noinline__ bool central_finish(const CentralStart c, const double3 p1, const double3 u1, double mcen,
+                                            double mj, double h, double rcen, double& temp) {
+    const double rcen2 = rcen * rcen;
+    const double rr1 = p1.x * p1.x + p1.y * p1.y + p1.z * p1.z;
+    const double rv1 = u1.x * p1.x + u1.y * p1.y + u1.z * p1.z;
+    const double rmin = c.rr0 < rr1 ? c.rr0 : rr1;
+    if (!((c.rv0 * h <= 0.0 && rv1 * h >= 0.0) || rmin <= rcen2)) return false;
+    const double p = c.h2 / (mcen + mj);
+    const double r0 = sqrt(c.rr0);
+    double t = 1.0 + p * (c.v2 / (mcen + mj) - 2.0 / r0);
     const double e = sqrt(t > 0.0 ? t : 0.0);
     const double q = p / (1.0 + e);
     if (!(q <= rcen)) return false;
@@ -198,7 +207,7 @@ __device__ __forceinline__ bool central_impact(const double3 p0, const double3 u
         c1 = c1 < 1.0 ? c1 : 1.0; c1 = c1 > -1.0 ? c1 : -1.0;
         c2 = c2 < 1.0 ? c2 : 1.0; c2 = c2 > -1.0 ? c2 : -1.0;
         const double uhit = copysign(acos(c1), -h);
-        const double uu0 = copysign(acos(c2), rv0);
+        const double uu0 = copysign(acos(c2), c.rv0);
         const double mhit = uhit - e * sin(uhit);
         const double m0 = uu0 - e * sin(uu0);
         t = (mhit - m0) / sqrt((mcen + mj) / (a * a * a));
@@ -208,18 +217,18 @@ __device__ __forceinline__ bool central_impact(const double3 p0, const double3 u
         c1 = c1 > 1.0 ? c1 : 1.0;
         c2 = c2 > 1.0 ? c2 : 1.0;
         const double uhit = copysign(acosh(c1), -h);
-        const double uu0 = copysign(acosh(c2), rv0);
+        const double uu0 = copysign(acosh(c2), c.rv0);
         const double mhit = e * sinh(uhit) - uhit;
         const double m0 = e * sinh(uu0) - uu0;
         t = (mhit - m0) / sqrt((mcen + mj) / (a * a * a));
     } else if (e == 1.0 && q > 0.0) {
         const double g1 = rcen / q - 1.0, g2 = r0 / q - 1.0;
         const double uhit = copysign(sqrt(g1 > 0.0 ? g1 : 0.0), -h);
-        const double uu0 = copysign(sqrt(g2 > 0.0 ? g2 : 0.0), rv0);
+        const double uu0 = copysign(sqrt(g2 > 0.0 ? g2 : 0.0), c.rv0);
         t = sqrt(2.0 * (q * q * q) / (mcen + mj)) *
             (uhit + (uhit * uhit * uhit) / 3.0 - uu0 - (uu0 * uu0 * uu0) / 3.0);
     }
-    if (q == 0.0 && rr1 != rr0) {
+    if (q == 0.0 && rr1 != c.rr0) {
         double w = (r0 - rcen) / (r0 - sqrt(rr1));
         w = w < 1.0 ? w : 1.0;
         w = w > 0.0 ? w : 0.0;
@@ -227,6 +236,12 @@ __device__ __forceinline__ bool central_impact(const double3 p0, const double3 u
     }
     temp = t;
     return true;
+}
+
+__device__ __forceinline__ bool central_impact(const double3 p0, const double3 u0, const double3 p1,
+                                               const double3 u1, double mcen, double mj, double h,
+                                               double rcen, double& temp) {
+    return central_finish(central_start(p0, u0), p1, u1, mcen, mj, h, rcen, temp);
 }
 
 // 128-byte record store as eight 16-byte writes.
