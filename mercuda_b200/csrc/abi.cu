@@ -105,6 +105,7 @@ __global__ void central_kernel(CentralArgs A) {
 }
 
 int blocks(int n, int t = 256) { return (n + t - 1) / t; }
+int reorder_slots(int src, cudaStream_t st);
 
 bool is_mvs(int alg) { return alg == 1 || alg == 9; }
 
@@ -182,11 +183,11 @@ MvsParticleArgs particle_args(int in, int out, int nsteps, int reset, int centra
     for (int k = 0; k < 3; ++k) a.jcen[k] = c.jcen[k];
     a.xin = c.pstate[in].p;
     a.xout = c.pstate[out].p;
-    a.m = c.pm.p;
-    a.rce = c.prce.p;
-    a.rphys = c.prphys.p;
-    a.ngf = c.pngf.p;
-    a.perm = c.perm.p;
+    a.m = c.pm();
+    a.rce = c.prce();
+    a.rphys = c.prphys();
+    a.ngf = c.pngf();
+    a.perm = c.permp();
     a.tab = tab;
     a.detail = detail;
     a.events = c.events.p;
@@ -233,6 +234,16 @@ void grow_after_overflow() {
 // are left in the event buffer with tmin in their time field.
 void mvs_step_once(double h) {
     Context& c = ctx();
+    if (c.steps_since_order >= 32) {
+        const int src = c.cur;
+        c.cur = reorder_slots(src, c.stream);
+        // the Big bodies share the buffer index: carry their state across
+        if (c.cur != src)
+            check(cudaMemcpyAsync(c.bigstate[c.cur].p, c.bigstate[src].p, sizeof(double) * 9 * c.nbig,
+                                  cudaMemcpyDeviceToDevice, c.stream),
+                  "copy");
+    }
+    c.steps_since_order += 1;
     for (int attempt = 0;; ++attempt) {
         ensure_tables(2, 1);
         check(cudaMemsetAsync(c.status.p, 0, sizeof(DeviceStatus), c.stream), "memset");
@@ -260,12 +271,30 @@ void mvs_step_once(double h) {
 
 // Warp-coherent ordering of the Small bodies. drift_dan leaves its elliptic
 // fast path (drift_kepmd) for the Newton solver when dm^2 > 0.16 or
-// e^2 dm^2 >= 0.0016 with dm = n h (or when the orbit is unbound), i.e. when
-// max(e n / 0.04, n / 0.4) * |h| >= 1. Sorting particles by that key (largest
-// first, into 256 logarithmic buckets, stable) puts the bodies that take the
-// long path into the same warps for any step size. The order changes no
-// result: every particle's arithmetic is independent of its slot, and ids
-// are mapped back through perm.
+// e^2 dm^2 >= 0.0016 with dm = n h, or when the orbit is unbound or e^2 > 0.36,
+// i.e. when max(e n / 0.04, n / 0.4) * |h| >= 1 for bound orbits with e <= 0.6.
+// Sorting the particle slots by that key (largest first, 256 logarithmic
+// buckets) puts the bodies that take the long path into the same warps for
+// any step size. Slot order changes no result: each particle's arithmetic is
+// independent of its slot, and event ids are mapped back through perm.
+__host__ __device__ inline int path_bucket(double x0, double x1, double x2, double v0, double v1, double v2,
+                                           double mu) {
+    const double r = sqrt(x0 * x0 + x1 * x1 + x2 * x2);
+    const double vv = v0 * v0 + v1 * v1 + v2 * v2;
+    const double u = x0 * v0 + x1 * v1 + x2 * v2;
+    const double alpha = 2.0 * mu / r - vv;
+    if (!(alpha > 0.0) || !isfinite(alpha)) return 0;
+    const double a = mu / alpha;
+    const double en = sqrt(mu / (a * a * a));
+    const double ec = 1.0 - r / a, es = u / (en * a * a);
+    const double e = sqrt(ec * ec + es * es);
+    const double key = fmax(e * en / 0.04, en / 0.4);
+    if (!(e <= 0.6) || !(key > 0.0) || !isfinite(key)) return 0;
+    const double l = log2(key) * 8.0 + 128.0;  // keys 2^-16 .. 2^16
+    const int b = 255 - (int)fmin(255.0, fmax(0.0, l));
+    return b < 1 ? 1 : b;
+}
+
 void order_particles(int n, int nbig, double mu, const double* xx, const double* vv) {
     Context& c = ctx();
     const int np = n - nbig;
@@ -273,23 +302,7 @@ void order_particles(int n, int nbig, double mu, const double* xx, const double*
     for (int p = 0; p < np; ++p) {
         const double* x = xx + 3 * (size_t)(nbig + p);
         const double* v = vv + 3 * (size_t)(nbig + p);
-        const double r = std::sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
-        const double v2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
-        const double u = x[0] * v[0] + x[1] * v[1] + x[2] * v[2];
-        const double alpha = 2.0 * mu / r - v2;
-        int b = 0;  // bucket 0 = highest key
-        if (alpha > 0.0 && std::isfinite(alpha)) {
-            const double a = mu / alpha;
-            const double en = std::sqrt(mu / (a * a * a));
-            const double ec = 1.0 - r / a, es = u / (en * a * a);
-            const double e = std::sqrt(ec * ec + es * es);
-            const double key = std::max(e * en / 0.04, en / 0.4);
-            if (e <= 0.6 && key > 0.0 && std::isfinite(key)) {
-                const double l = std::log2(key) * 8.0 + 128.0;  // key 2^-16 .. 2^16
-                b = 255 - (int)std::min(255.0, std::max(0.0, l));
-                b = std::max(1, b);
-            }
-        }
+        const int b = path_bucket(x[0], x[1], x[2], v[0], v[1], v[2], mu);
         bucket[p] = b;
         count[b + 1]++;
     }
@@ -303,10 +316,95 @@ void order_particles(int n, int nbig, double mu, const double* xx, const double*
         perm[p] = p;
         inv[p] = p;
     }
-    c.perm.reserve(c.npcap);
-    c.inv.reserve(c.npcap);
-    check(cudaMemcpy(c.perm.p, perm.data(), sizeof(int) * c.npcap, cudaMemcpyHostToDevice), "upload");
+    check(cudaMemcpy(c.perm[c.kc].p, perm.data(), sizeof(int) * c.npcap, cudaMemcpyHostToDevice), "upload");
     check(cudaMemcpy(c.inv.p, inv.data(), sizeof(int) * c.npcap, cudaMemcpyHostToDevice), "upload");
+    c.steps_since_order = 0;
+}
+
+// Device re-ordering of the slots by the same key as the state evolves
+// (scattered or eccentric particles move to the Newton path): bucket
+// histogram, scan, scatter of the 9 state and 8 constant columns and of perm.
+struct ReorderArgs {
+    int np, npcap;
+    double mu;
+    const double* xin;
+    double* xout;
+    const double* cin;
+    double* cout;
+    const int* pin;
+    int* pout;
+    int* inv;
+    int* bucket;
+    int* hist;  // [256] counts, then [256] cursors
+};
+
+__global__ void reorder_keys_kernel(ReorderArgs A) {
+    __shared__ int local[256];
+    for (int k = threadIdx.x; k < 256; k += blockDim.x) local[k] = 0;
+    __syncthreads();
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < A.np) {
+        const int S = A.npcap;
+        const int b = path_bucket(A.xin[s], A.xin[S + s], A.xin[2 * S + s], A.xin[3 * S + s], A.xin[4 * S + s],
+                                  A.xin[5 * S + s], A.mu);
+        A.bucket[s] = b;
+        atomicAdd(&local[b], 1);
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < 256; k += blockDim.x)
+        if (local[k]) atomicAdd(&A.hist[k], local[k]);
+}
+
+__global__ void reorder_scan_kernel(ReorderArgs A) {
+    if (threadIdx.x == 0) {
+        int sum = 0;
+        for (int k = 0; k < 256; ++k) {
+            A.hist[256 + k] = sum;
+            sum += A.hist[k];
+        }
+    }
+}
+
+__global__ void reorder_scatter_kernel(ReorderArgs A) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= A.np) return;
+    const int ns = atomicAdd(&A.hist[256 + A.bucket[s]], 1);
+    const size_t S = A.npcap;
+    for (int c = 0; c < 9; ++c) A.xout[c * S + ns] = A.xin[c * S + s];
+    for (int c = 0; c < 8; ++c) A.cout[c * S + ns] = A.cin[c * S + s];
+    const int p = A.pin[s];
+    A.pout[ns] = p;
+    A.inv[p] = ns;
+}
+
+// Re-sorts the particle slots: state from pstate[src] into pstate[1 - src],
+// constants and perm into the other buffer pair. Returns the new state index.
+int reorder_slots(int src, cudaStream_t st) {
+    Context& c = ctx();
+    c.steps_since_order = 0;
+    if (c.np < 64) return src;
+    c.order_bucket.reserve(c.npcap);
+    c.order_hist.reserve(512);
+    check(cudaMemsetAsync(c.order_hist.p, 0, sizeof(int) * 512, st), "memset");
+    ReorderArgs a;
+    a.np = c.np;
+    a.npcap = c.npcap;
+    a.mu = c.m_host[0];
+    a.xin = c.pstate[src].p;
+    a.xout = c.pstate[1 - src].p;
+    a.cin = c.pconst[c.kc].p;
+    a.cout = c.pconst[1 - c.kc].p;
+    a.pin = c.perm[c.kc].p;
+    a.pout = c.perm[1 - c.kc].p;
+    a.inv = c.inv.p;
+    a.bucket = c.order_bucket.p;
+    a.hist = c.order_hist.p;
+    reorder_keys_kernel<<<blocks(c.np), 256, 0, st>>>(a);
+    reorder_scan_kernel<<<1, 32, 0, st>>>(a);
+    reorder_scatter_kernel<<<blocks(c.np), 256, 0, st>>>(a);
+    check(cudaGetLastError(), "reorder");
+    c.kc = 1 - c.kc;
+    return 1 - src;
 }
 
 void sort_events(std::vector<MercuryEvent>& ev, std::vector<int>* steps) {
@@ -417,10 +515,12 @@ int mercury_cuda_upload(int n, int nbig, int pn, int ngflag, const double* m, co
             c.bigstate[k].reserve((size_t)9 * nbig);
             c.pstate[k].reserve((size_t)9 * c.npcap);
         }
-        c.pm.reserve(c.npcap);
-        c.prce.reserve(c.npcap);
-        c.prphys.reserve(c.npcap);
-        c.pngf.reserve((size_t)5 * c.npcap);
+        for (int k = 0; k < 2; ++k) {
+            c.pconst[k].reserve((size_t)8 * c.npcap);
+            c.perm[k].reserve(c.npcap);
+        }
+        c.inv.reserve(c.npcap);
+        c.kc = 0;
         c.status.reserve(1);
         ensure_events(std::max(4096, c.np / 64));
         c.cands.reserve(std::max(16384, c.np / 2));
@@ -431,10 +531,8 @@ int mercury_cuda_upload(int n, int nbig, int pn, int ngflag, const double* m, co
         check(cudaMemsetAsync(c.pstate[1].p, 0, sizeof(double) * 9 * c.npcap, s), "memset");
         check(cudaMemsetAsync(c.bigstate[0].p, 0, sizeof(double) * 9 * nbig, s), "memset");
         check(cudaMemsetAsync(c.bigstate[1].p, 0, sizeof(double) * 9 * nbig, s), "memset");
-        check(cudaMemsetAsync(c.pm.p, 0, sizeof(double) * c.npcap, s), "memset");
-        check(cudaMemsetAsync(c.prce.p, 0, sizeof(double) * c.npcap, s), "memset");
-        check(cudaMemsetAsync(c.prphys.p, 0, sizeof(double) * c.npcap, s), "memset");
-        check(cudaMemsetAsync(c.pngf.p, 0, sizeof(double) * 5 * c.npcap, s), "memset");
+        check(cudaMemsetAsync(c.pconst[0].p, 0, sizeof(double) * 8 * c.npcap, s), "memset");
+        check(cudaMemsetAsync(c.pconst[1].p, 0, sizeof(double) * 8 * c.npcap, s), "memset");
         c.cur = 0;
         order_particles(n, nbig, m[0], xx, vv);
         // positions and velocities
@@ -448,7 +546,7 @@ int mercury_cuda_upload(int n, int nbig, int pn, int ngflag, const double* m, co
         // per-body scalars: masses, radii
         const double* scalars[3] = {m, limits, radii};
         double* bigdst[3] = {c.mbig.p, c.rcebig.p, c.rphysbig.p};
-        double* pdst[3] = {c.pm.p, c.prce.p, c.prphys.p};
+        double* pdst[3] = {c.pm(), c.prce(), c.prphys()};
         for (int q = 0; q < 3; ++q) {
             check(cudaMemcpyAsync(c.transfer.p, scalars[q], sizeof(double) * n, cudaMemcpyHostToDevice, s), "upload");
             scatter_rows(c.transfer.p, n, 1, nbig, bigdst[q], nbig, pdst[q], c.npcap, c.inv.p, s);
@@ -458,7 +556,7 @@ int mercury_cuda_upload(int n, int nbig, int pn, int ngflag, const double* m, co
         check(cudaMemcpyAsync(c.ngfbig.p, ng, sizeof(double) * 5 * nbig, cudaMemcpyHostToDevice, s), "upload");
         c.transfer.reserve((size_t)6 * n);
         check(cudaMemcpyAsync(c.transfer.p, ng, sizeof(double) * 5 * n, cudaMemcpyHostToDevice, s), "upload");
-        scatter_rows(c.transfer.p, n, 5, nbig, nullptr, 0, c.pngf.p, c.npcap, c.inv.p, s);
+        scatter_rows(c.transfer.p, n, 5, nbig, nullptr, 0, c.pngf(), c.npcap, c.inv.p, s);
         check(cudaStreamSynchronize(s), "upload");
         check(cudaGetLastError(), "upload");
         c.reset = true;
@@ -520,9 +618,9 @@ int mercury_cuda_events(double time, double h, double rcen, const MercuryEvent**
                 a.big1 = c.bigstate[c.cur].p;
                 a.part0 = c.pstate[prev].p;
                 a.part1 = c.pstate[c.cur].p;
-                a.pm = c.pm.p;
+                a.pm = c.pm();
                 a.mbig = c.mbig.p;
-                a.perm = c.perm.p;
+                a.perm = c.permp();
                 a.events = c.events.p;
                 a.event_step = c.event_step.p;
                 a.cap = (int)c.events.n;
@@ -593,7 +691,7 @@ int mercury_cuda_limits(const double* limits) {
     try {
         require_system();
         check(cudaMemcpyAsync(c.transfer.p, limits, sizeof(double) * c.n, cudaMemcpyHostToDevice, c.stream), "limits");
-        scatter_rows(c.transfer.p, c.n, 1, c.nbig, c.rcebig.p, c.nbig, c.prce.p, c.npcap, c.inv.p, c.stream);
+        scatter_rows(c.transfer.p, c.n, 1, c.nbig, c.rcebig.p, c.nbig, c.prce(), c.npcap, c.inv.p, c.stream);
         check(cudaStreamSynchronize(c.stream), "limits");
         return 0;
     } catch (const std::exception& e) {
@@ -649,14 +747,20 @@ int mercury_b200_mvs_advance(double time, double h, int nsteps, double rcen, int
                 check(cudaEventCreate(&c.kt1[k]), "event");
             }
         }
-        // keep the starting state so that an event-buffer overflow can be redone
+        // keep the starting state (and slot order) so that an event-buffer
+        // overflow can be redone from it
         c.snapshot.reserve((size_t)9 * c.npcap + 9 * c.nbig);
-        check(cudaMemcpyAsync(c.snapshot.p, c.pstate[c.cur].p, sizeof(double) * 9 * c.npcap, cudaMemcpyDeviceToDevice,
-                              c.stream),
-              "snapshot");
-        check(cudaMemcpyAsync(c.snapshot.p + 9 * c.npcap, c.bigstate[c.cur].p, sizeof(double) * 9 * c.nbig,
-                              cudaMemcpyDeviceToDevice, c.stream),
-              "snapshot");
+        c.snap_const.reserve((size_t)8 * c.npcap);
+        c.snap_perm.reserve((size_t)2 * c.npcap);
+        const int kc0 = c.kc;
+        auto copy = [&](void* dst, const void* src, size_t bytes) {
+            check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, c.stream), "snapshot");
+        };
+        copy(c.snapshot.p, c.pstate[c.cur].p, sizeof(double) * 9 * c.npcap);
+        copy(c.snapshot.p + 9 * c.npcap, c.bigstate[c.cur].p, sizeof(double) * 9 * c.nbig);
+        copy(c.snap_const.p, c.pconst[kc0].p, sizeof(double) * 8 * c.npcap);
+        copy(c.snap_perm.p, c.perm[kc0].p, sizeof(int) * c.npcap);
+        copy(c.snap_perm.p + c.npcap, c.inv.p, sizeof(int) * c.npcap);
         const bool reset0 = c.reset;
         for (int attempt = 0;; ++attempt) {
             check(cudaMemsetAsync(c.status.p, 0, sizeof(DeviceStatus), c.stream), "memset");
@@ -673,6 +777,9 @@ int mercury_b200_mvs_advance(double time, double h, int nsteps, double rcen, int
                 check(cudaEventRecord(c.chunk_done[ch], c.stream_big), "event");
                 bcur = 1 - bcur;
                 if (c.np > 0) {
+                    // re-sort the slots by drift path before every launch (cheap
+                    // next to the launch; particles change path as they evolve)
+                    pcur = reorder_slots(pcur, c.stream);
                     check(cudaStreamWaitEvent(c.stream, c.chunk_done[ch], 0), "wait");
                     check(cudaEventRecord(c.kt0[ch], c.stream), "event");
                     particles_and_events(particle_args(pcur, 1 - pcur, ks, reset, 1, s0, h, rcen, tab, det),
@@ -698,18 +805,20 @@ int mercury_b200_mvs_advance(double time, double h, int nsteps, double rcen, int
                     }
                 c.last_particle_kernel_ms = ksum;
                 c.last_particle_launches = c.np > 0 ? nchunks : 0;
-                // both state sets end in the same buffer index parity
-                c.cur = pcur;  // Big and particle buffers flip together
+                // the Big and particle states must end in the same buffer index
+                if (bcur != pcur)
+                    copy(c.bigstate[pcur].p, c.bigstate[bcur].p, sizeof(double) * 9 * c.nbig);
+                c.cur = pcur;
                 break;
             }
             if (attempt > 8) throw std::runtime_error("event buffer growth failed");
             grow_after_overflow();
-            check(cudaMemcpyAsync(c.pstate[c.cur].p, c.snapshot.p, sizeof(double) * 9 * c.npcap,
-                                  cudaMemcpyDeviceToDevice, c.stream),
-                  "restore");
-            check(cudaMemcpyAsync(c.bigstate[c.cur].p, c.snapshot.p + 9 * c.npcap, sizeof(double) * 9 * c.nbig,
-                                  cudaMemcpyDeviceToDevice, c.stream),
-                  "restore");
+            c.kc = kc0;
+            copy(c.pstate[c.cur].p, c.snapshot.p, sizeof(double) * 9 * c.npcap);
+            copy(c.bigstate[c.cur].p, c.snapshot.p + 9 * c.npcap, sizeof(double) * 9 * c.nbig);
+            copy(c.pconst[kc0].p, c.snap_const.p, sizeof(double) * 8 * c.npcap);
+            copy(c.perm[kc0].p, c.snap_perm.p, sizeof(int) * c.npcap);
+            copy(c.inv.p, c.snap_perm.p + c.npcap, sizeof(int) * c.npcap);
         }
         c.nforces += nsteps + (reset0 ? 1 : 0);
         c.reset = false;

@@ -55,8 +55,15 @@ struct Context {
     DBuf<double> bigstate[2];   // [9][nbig]: x(3) v(3) a(3)
     // particles
     DBuf<double> pstate[2];     // [9][npcap]
-    DBuf<double> pm, prce, prphys, pngf;
-    DBuf<int> perm, inv;        // slot -> particle index, particle index -> slot
+    // per-slot constants [8][npcap]: m, rce, rphys, ngf(5); double-buffered with
+    // perm (slot -> particle index) so that the slots can be re-ordered
+    DBuf<double> pconst[2];
+    DBuf<int> perm[2];
+    DBuf<int> inv;              // particle index -> slot
+    int kc = 0;                 // constants/perm buffer in use
+    DBuf<int> order_bucket, order_hist;
+    DBuf<double> snap_const;
+    DBuf<int> snap_perm;
     int cur = 0;
     bool reset = true;
     bool stepped = false;
@@ -86,6 +93,13 @@ struct Context {
     int particle_threads = 128;
     int steps_per_launch = 0;   // 0 = automatic
 
+    double* pm() { return pconst[kc].p; }
+    double* prce() { return pconst[kc].p + npcap; }
+    double* prphys() { return pconst[kc].p + 2 * (size_t)npcap; }
+    double* pngf() { return pconst[kc].p + 3 * (size_t)npcap; }
+    int* permp() { return perm[kc].p; }
+    int steps_since_order = 0;
+
     BigState big(int k) {
         BigState b;
         b.x = bigstate[k].p;
@@ -104,10 +118,11 @@ struct Context {
     }
     void release_all() {
         DBuf<double>* bufs[] = {&mbig, &rcebig, &rphysbig, &ngfbig, &bigstate[0], &bigstate[1], &pstate[0],
-                                &pstate[1], &pm, &prce, &prphys, &pngf, &tab, &detail, &transfer, &snapshot};
+                                &pstate[1], &pconst[0], &pconst[1], &tab, &detail, &transfer, &snapshot, &snap_const};
         for (auto* b : bufs) b->release();
-        perm.release();
-        inv.release();
+        DBuf<int>* ibufs[] = {&perm[0], &perm[1], &inv, &order_bucket, &order_hist, &snap_perm};
+        for (auto* b : ibufs) b->release();
+        kc = 0;
         events.release();
         event_step.release();
         cands.release();

@@ -190,3 +190,25 @@ def test_step_failure_is_reported(backend):
     backend.upload(sys0)
     with pytest.raises(Exception, match="CUDA integration step failed"):
         backend.step(0.0, 8.0, dtflag=0)
+
+
+def test_per_step_loop_long_run_with_reordering(backend, oracle):
+    """100 drop-in steps: the slot order is rebuilt every 32 steps (and the
+    per-step previous/central buffers must follow it)."""
+    sys0 = make_system(seed=15, n_particles=1500, near_fraction=0.05)
+    backend.upload(sys0)
+    time, got = 0.0, []
+    for k in range(100):
+        backend.step(time, 8.0, dtflag=0 if k == 0 else 2)
+        x0, v0 = backend.download(previous=True)
+        ev = backend.events(time + 8.0, 8.0, 0.005)
+        got.extend((k, int(e["i"]), int(e["j"]), int(e["kind"])) for e in ev)
+        time += 8.0
+    x, v = backend.download()
+    ref = sys0.copy()
+    rev, rsteps = oracle.mvs_run(ref, 0.0, 8.0, 100, 0.005, central=True, threads=4)
+    assert rel_err(x, ref.x) < 1e-9
+    assert got == [(int(s), int(e["i"]), int(e["j"]), int(e["kind"])) for s, e in zip(rsteps, rev)]
+    prev = sys0.copy()
+    oracle.mvs_run(prev, 0.0, 8.0, 99, 0.005, central=False, threads=4)
+    assert rel_err(x0, prev.x) < 1e-9
