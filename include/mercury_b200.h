@@ -31,6 +31,35 @@ int mercury_b200_set_launch(int particle_threads, int steps_per_launch);
  * FMA), best of five launches of independent fma() chains on every SM. */
 int mercury_b200_fp64_peak(double* tflops, double* ms);
 
+/* One MVS step (kick, drift, mce_stat pair screen, kick) of a system whose
+ * arrays the caller already holds on the current device, with no device
+ * allocation: for hosts that cannot call cudaMalloc (device memory owned by
+ * another allocator or budget, or no implicit device-wide synchronization
+ * allowed). This entry point has no counterpart in the reference's C ABI.
+ *
+ * Device pointers, SoA with npcap = max(2, np rounded up to even), 16-byte
+ * aligned: mbig/rcebig/rphysbig[nbig], ngfbig[nbig][5]; big_in/big_out
+ * [9][nbig] and part_in/part_out [9][npcap] holding x,y,z, vx,vy,vz and the
+ * cached acceleration ax,ay,az of the last force call; part_const[8][npcap]
+ * holding m, rce, rphys, A1, A2, A3, beta, yar. reset != 0 recomputes the
+ * cached accelerations first (mdt_mvs with dtflag != 2). events[event_cap]
+ * receives the pair records of the step (1-based ids, times absolute), and
+ * *event_count (host) their total. No oblateness and no central-impact screen.
+ * Limits: nbig <= 64, np <= 262144, event_cap <= 8192, 8192 encounter
+ * candidates per step; beyond them the call fails with a message.
+ *
+ * Scratch lives in one static device array (about 2.2 MB per device, held
+ * until exit) that every call shares: calls that overlap on the GPU (other
+ * streams, other host threads) race on it. The first call on a device looks
+ * up the array's address and initializes it (one synchronizing kernel), so
+ * make that first call before any stream capture. The call is synchronous on
+ * `stream` (a cudaStream_t; 0 = legacy default stream). */
+int mercury_b200_mvs_step_noalloc(int nbig, int np, const double* mbig, const double* rcebig,
+                                  const double* rphysbig, const double* ngfbig, const double* big_in,
+                                  double* big_out, const double* part_in, double* part_out,
+                                  const double* part_const, int ngflag, double time, double h, int reset,
+                                  MercuryEvent* events, int event_cap, int* event_count, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -44,7 +44,7 @@ DROP_IN_SYMBOLS = [
     "mercury_cuda_free",
 ]
 EXTENSION_SYMBOLS = ["mercury_b200_mvs_advance", "mercury_b200_events", "mercury_b200_timing",
-                     "mercury_b200_set_launch", "mercury_b200_fp64_peak"]
+                     "mercury_b200_set_launch", "mercury_b200_fp64_peak", "mercury_b200_mvs_step_noalloc"]
 
 
 class BackendError(RuntimeError):
@@ -85,6 +85,9 @@ def load_library(path: Path | str | None = None) -> C.CDLL:
     L.mercury_b200_timing.argtypes = [PD, PD, PI]
     L.mercury_b200_set_launch.argtypes = [I, I]
     L.mercury_b200_fp64_peak.argtypes = [PD, PD]
+    VP = C.c_void_p
+    L.mercury_b200_mvs_step_noalloc.argtypes = [I, I, VP, VP, VP, VP, VP, VP, VP, VP, VP, I, D, D, I, VP, I,
+                                                PI, VP]
     if path is None:
         _lib = L
     return L
