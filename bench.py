@@ -42,6 +42,10 @@ RCEN = 0.005
 FLOPS_PER_PARTICLE_STEP = 376.06
 # Bytes per particle-step if every step read and wrote x, v (and nothing else).
 BYTES_PER_PARTICLE_STEP = 96.0
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of one 31-step
+# launch of the particle kernel on this 1M-particle workload, from the ncu
+# capture summarised in profiles/mvs_particle_kernel_1M.md.
+TRAFFIC_PER_31_STEP_LAUNCH = (99.764224 + 157.014528) * 1e6
 CLOCK_QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
                "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -234,7 +238,7 @@ def main():
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
-        sample_particles, sample_steps = 100_000, 457
+        sample_particles, sample_steps = 300_000, 457
         v_cpu, cores, dt = cpu_baseline(sample_particles, sample_steps, args.seed)
         cpu = {"value": v_cpu, "unit": UNIT, "cores": cores, "kind": "port",
                "sample": f"{sample_particles} particles of the same generator x {sample_steps} steps ({dt:.1f} s)"}
@@ -251,12 +255,15 @@ def main():
                        "l2": "state 9 doubles/particle double-buffered (144 MB) > 126 MB L2; "
                              "each launch reads and writes it once"},
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak_tflops, "unit": "TFLOP/s",
-                         "frac": achieved / peak_tflops, "traffic": None,
+                         "frac": achieved / peak_tflops,
+                         "traffic": (TRAFFIC_PER_31_STEP_LAUNCH * args.particles / 1e6
+                                     if steps_per_launch == 31 else None),
+                         "traffic_unit": "bytes per launch (ncu, 1M particles, 31 steps)",
                          "peak_source": "measured in this run: fma() chains on every SM (2 FLOP/FMA)",
                          "flops_per_particle_step": FLOPS_PER_PARTICLE_STEP,
                          "kernel_ms_per_launch": kernel_ms},
             "clocks": clk,
-            "gpu_launches": 2 * launches,
+            "gpu_launches": tm["kernel_launches"],
             "events": int(len(events)),
             "e2e": e2e,
             "cpu_baseline": cpu,

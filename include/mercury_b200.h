@@ -20,9 +20,11 @@ int mercury_b200_mvs_advance(double time, double h, int nsteps, double rcen, int
 /* Copy up to cap records of the last advance, sorted by (step, min(i,j),
  * max(i,j)), with the 0-based step of each; returns the total count. */
 int mercury_b200_events(MercuryEvent* events, int* steps, int cap);
-/* Device time of the last advance (CUDA events on the library's stream),
- * and the summed duration and count of its particle-kernel launches. */
-int mercury_b200_timing(double* advance_ms, double* particle_kernel_ms, int* particle_launches);
+/* Device time of the last advance (CUDA events on the library's stream), the
+ * summed duration and count of its particle-kernel launches, and the number
+ * of kernels it launched on all streams. */
+int mercury_b200_timing(double* advance_ms, double* particle_kernel_ms, int* particle_launches,
+                        int* kernel_launches);
 /* Launch shape of the particle kernel: threads per CTA (multiple of 32) and
  * steps fused per launch (0 = automatic); a negative value keeps the setting. */
 int mercury_b200_set_launch(int particle_threads, int steps_per_launch);

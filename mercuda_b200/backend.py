@@ -82,7 +82,7 @@ def load_library(path: Path | str | None = None) -> C.CDLL:
     L.mercury_cuda_free.restype = None
     L.mercury_b200_mvs_advance.argtypes = [D, D, I, D, I, PI]
     L.mercury_b200_events.argtypes = [C.c_void_p, PI, I]
-    L.mercury_b200_timing.argtypes = [PD, PD, PI]
+    L.mercury_b200_timing.argtypes = [PD, PD, PI, PI]
     L.mercury_b200_set_launch.argtypes = [I, I]
     L.mercury_b200_fp64_peak.argtypes = [PD, PD]
     VP = C.c_void_p
@@ -193,9 +193,10 @@ class Backend:
         return events, steps
 
     def timing(self):
-        a, k, n = D(0.0), D(0.0), I(0)
-        self.lib.mercury_b200_timing(C.byref(a), C.byref(k), C.byref(n))
-        return {"advance_ms": a.value, "particle_kernel_ms": k.value, "particle_launches": n.value}
+        a, k, n, L = D(0.0), D(0.0), I(0), I(0)
+        self.lib.mercury_b200_timing(C.byref(a), C.byref(k), C.byref(n), C.byref(L))
+        return {"advance_ms": a.value, "particle_kernel_ms": k.value, "particle_launches": n.value,
+                "kernel_launches": L.value}
 
     def fp64_peak(self):
         tf, ms = D(0.0), D(0.0)

@@ -105,7 +105,7 @@ __global__ void central_kernel(CentralArgs A) {
 }
 
 int blocks(int n, int t = 256) { return (n + t - 1) / t; }
-int reorder_slots(int src, cudaStream_t st);
+int reorder_slots(int src, double h, cudaStream_t st);
 
 bool is_mvs(int alg) { return alg == 1 || alg == 9; }
 
@@ -236,7 +236,7 @@ void mvs_step_once(double h) {
     Context& c = ctx();
     if (c.steps_since_order >= 32) {
         const int src = c.cur;
-        c.cur = reorder_slots(src, c.stream);
+        c.cur = reorder_slots(src, h, c.stream);
         // the Big bodies share the buffer index: carry their state across
         if (c.cur != src)
             check(cudaMemcpyAsync(c.bigstate[c.cur].p, c.bigstate[src].p, sizeof(double) * 9 * c.nbig,
@@ -321,12 +321,31 @@ void order_particles(int n, int nbig, double mu, const double* xx, const double*
     c.steps_since_order = 0;
 }
 
-// Device re-ordering of the slots by the same key as the state evolves
-// (scattered or eccentric particles move to the Newton path): bucket
-// histogram, scan, scatter of the 9 state and 8 constant columns and of perm.
-struct ReorderArgs {
-    int np, npcap;
-    double mu;
+// Device re-ordering of the slots as the state evolves (scattered or eccentric
+// particles move to the Newton path): a stable partition, for the step size h
+// of the coming launch, into the slots whose drift takes the Newton solver
+// (unbound, e > 0.6, or max(e n/0.04, n/0.4)·|h| >= 1) followed by the rest.
+// Warp ballots give in-block ranks and one scan gives block offsets, so the
+// pass is deterministic, atomic-free and writes contiguous runs.
+__device__ __forceinline__ bool newton_path(const double* x, int S, int s, double mu, double absh) {
+    const double x0 = x[s], x1 = x[S + s], x2 = x[2 * S + s];
+    const double v0 = x[3 * S + s], v1 = x[4 * S + s], v2 = x[5 * S + s];
+    const double r = sqrt(x0 * x0 + x1 * x1 + x2 * x2);
+    const double vv = v0 * v0 + v1 * v1 + v2 * v2;
+    const double u = x0 * v0 + x1 * v1 + x2 * v2;
+    const double alpha = 2.0 * mu / r - vv;
+    if (!(alpha > 0.0)) return true;
+    const double a = mu / alpha;
+    const double en = sqrt(mu / (a * a * a));
+    const double ec = 1.0 - r / a, es = u / (en * a * a);
+    const double e = sqrt(ec * ec + es * es);
+    if (!(e <= 0.6)) return true;
+    return fmax(e * en / 0.04, en / 0.4) * absh >= 1.0;
+}
+
+struct PartitionArgs {
+    int np, npcap, nblk;
+    double mu, absh;
     const double* xin;
     double* xout;
     const double* cin;
@@ -334,41 +353,88 @@ struct ReorderArgs {
     const int* pin;
     int* pout;
     int* inv;
-    int* bucket;
-    int* hist;  // [256] counts, then [256] cursors
+    int* bslow;  // [nblk] Newton-path count per block, then exclusive offsets
+    int* bfast;  // [nblk] the other count, then exclusive offsets
+    int* total;  // [1] Newton-path total
 };
 
-__global__ void reorder_keys_kernel(ReorderArgs A) {
-    __shared__ int local[256];
-    for (int k = threadIdx.x; k < 256; k += blockDim.x) local[k] = 0;
+constexpr int PART_THREADS = 256;
+
+// Rank of this thread among the threads of its block with the same flag;
+// returns the block's count of set flags in *nset. All threads must call.
+__device__ __forceinline__ int block_rank(bool flag, int* nset) {
+    __shared__ int warp_set[PART_THREADS / 32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned m = __ballot_sync(0xffffffffu, flag);
+    if (lane == 0) warp_set[w] = __popc(m);
     __syncthreads();
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s < A.np) {
-        const int S = A.npcap;
-        const int b = path_bucket(A.xin[s], A.xin[S + s], A.xin[2 * S + s], A.xin[3 * S + s], A.xin[4 * S + s],
-                                  A.xin[5 * S + s], A.mu);
-        A.bucket[s] = b;
-        atomicAdd(&local[b], 1);
+    int before_set = 0, all_set = 0;
+    for (int k = 0; k < PART_THREADS / 32; ++k) {
+        if (k < w) before_set += warp_set[k];
+        all_set += warp_set[k];
     }
     __syncthreads();
-    for (int k = threadIdx.x; k < 256; k += blockDim.x)
-        if (local[k]) atomicAdd(&A.hist[k], local[k]);
+    const unsigned lt = (1u << lane) - 1u;
+    const int set_rank = before_set + __popc(m & lt);
+    const int clear_rank = (w * 32 + lane) - set_rank;
+    *nset = all_set;
+    return flag ? set_rank : clear_rank;
 }
 
-__global__ void reorder_scan_kernel(ReorderArgs A) {
+__global__ void __launch_bounds__(PART_THREADS) partition_count_kernel(PartitionArgs A) {
+    const int s = blockIdx.x * PART_THREADS + threadIdx.x;
+    const bool valid = s < A.np;
+    const bool slow = valid && newton_path(A.xin, A.npcap, s, A.mu, A.absh);
+    int nslow;
+    block_rank(slow, &nslow);
     if (threadIdx.x == 0) {
-        int sum = 0;
-        for (int k = 0; k < 256; ++k) {
-            A.hist[256 + k] = sum;
-            sum += A.hist[k];
-        }
+        const int nvalid = min(PART_THREADS, A.np - blockIdx.x * PART_THREADS);
+        A.bslow[blockIdx.x] = nslow;
+        A.bfast[blockIdx.x] = nvalid - nslow;
     }
 }
 
-__global__ void reorder_scatter_kernel(ReorderArgs A) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= A.np) return;
-    const int ns = atomicAdd(&A.hist[256 + A.bucket[s]], 1);
+// Exclusive scans of the per-block counts (one CTA of 1024 threads).
+__global__ void __launch_bounds__(1024) partition_scan_kernel(PartitionArgs A) {
+    __shared__ int sum_slow[1024], sum_fast[1024];
+    const int t = threadIdx.x, per = (A.nblk + 1023) / 1024;
+    const int lo = t * per, hi = min(A.nblk, lo + per);
+    int a = 0, b = 0;
+    for (int k = lo; k < hi; ++k) { a += A.bslow[k]; b += A.bfast[k]; }
+    sum_slow[t] = a;
+    sum_fast[t] = b;
+    __syncthreads();
+    if (t == 0) {
+        int ra = 0, rb = 0;
+        for (int k = 0; k < 1024; ++k) {
+            const int xa = sum_slow[k], xb = sum_fast[k];
+            sum_slow[k] = ra;
+            sum_fast[k] = rb;
+            ra += xa;
+            rb += xb;
+        }
+        *A.total = ra;
+    }
+    __syncthreads();
+    a = sum_slow[t];
+    b = sum_fast[t];
+    for (int k = lo; k < hi; ++k) {
+        const int xa = A.bslow[k], xb = A.bfast[k];
+        A.bslow[k] = a;
+        A.bfast[k] = b;
+        a += xa;
+        b += xb;
+    }
+}
+
+__global__ void __launch_bounds__(PART_THREADS) partition_scatter_kernel(PartitionArgs A) {
+    const int s = blockIdx.x * PART_THREADS + threadIdx.x;
+    const bool valid = s < A.np;
+    const bool slow = valid && newton_path(A.xin, A.npcap, s, A.mu, A.absh);
+    int nslow;
+    const int rank = block_rank(slow, &nslow);
+    if (!valid) return;
+    const int ns = slow ? A.bslow[blockIdx.x] + rank : *A.total + A.bfast[blockIdx.x] + rank;
     const size_t S = A.npcap;
     for (int c = 0; c < 9; ++c) A.xout[c * S + ns] = A.xin[c * S + s];
     for (int c = 0; c < 8; ++c) A.cout[c * S + ns] = A.cin[c * S + s];
@@ -377,19 +443,21 @@ __global__ void reorder_scatter_kernel(ReorderArgs A) {
     A.inv[p] = ns;
 }
 
-// Re-sorts the particle slots: state from pstate[src] into pstate[1 - src],
-// constants and perm into the other buffer pair. Returns the new state index.
-int reorder_slots(int src, cudaStream_t st) {
+// Re-orders the particle slots for a launch with step h: state from
+// pstate[src] into pstate[1 - src], constants and perm into the other buffer
+// pair. Returns the new state index.
+int reorder_slots(int src, double h, cudaStream_t st) {
     Context& c = ctx();
     c.steps_since_order = 0;
     if (c.np < 64) return src;
-    c.order_bucket.reserve(c.npcap);
-    c.order_hist.reserve(512);
-    check(cudaMemsetAsync(c.order_hist.p, 0, sizeof(int) * 512, st), "memset");
-    ReorderArgs a;
+    const int nblk = (c.np + PART_THREADS - 1) / PART_THREADS;
+    c.order_hist.reserve((size_t)2 * nblk + 1);
+    PartitionArgs a;
     a.np = c.np;
     a.npcap = c.npcap;
+    a.nblk = nblk;
     a.mu = c.m_host[0];
+    a.absh = std::fabs(h);
     a.xin = c.pstate[src].p;
     a.xout = c.pstate[1 - src].p;
     a.cin = c.pconst[c.kc].p;
@@ -397,11 +465,12 @@ int reorder_slots(int src, cudaStream_t st) {
     a.pin = c.perm[c.kc].p;
     a.pout = c.perm[1 - c.kc].p;
     a.inv = c.inv.p;
-    a.bucket = c.order_bucket.p;
-    a.hist = c.order_hist.p;
-    reorder_keys_kernel<<<blocks(c.np), 256, 0, st>>>(a);
-    reorder_scan_kernel<<<1, 32, 0, st>>>(a);
-    reorder_scatter_kernel<<<blocks(c.np), 256, 0, st>>>(a);
+    a.bslow = c.order_hist.p;
+    a.bfast = c.order_hist.p + nblk;
+    a.total = c.order_hist.p + 2 * nblk;
+    partition_count_kernel<<<nblk, PART_THREADS, 0, st>>>(a);
+    partition_scan_kernel<<<1, 1024, 0, st>>>(a);
+    partition_scatter_kernel<<<nblk, PART_THREADS, 0, st>>>(a);
     check(cudaGetLastError(), "reorder");
     c.kc = 1 - c.kc;
     return 1 - src;
@@ -763,6 +832,7 @@ int mercury_b200_mvs_advance(double time, double h, int nsteps, double rcen, int
         copy(c.snap_perm.p + c.npcap, c.inv.p, sizeof(int) * c.npcap);
         const bool reset0 = c.reset;
         for (int attempt = 0;; ++attempt) {
+            int launches = 0;
             check(cudaMemsetAsync(c.status.p, 0, sizeof(DeviceStatus), c.stream), "memset");
             check(cudaEventRecord(c.t0, c.stream), "event");
             check(cudaStreamWaitEvent(c.stream_big, c.t0, 0), "wait");
@@ -774,16 +844,19 @@ int mercury_b200_mvs_advance(double time, double h, int nsteps, double rcen, int
                 double* tab = c.tab.p + row * stride;
                 double* det = c.detail.p + (size_t)s0 * std::max(1, nb) * TAB_DETAIL;
                 launch_mvs_big(big_args(bcur, 1 - bcur, ks, reset, 1, s0, h, rcen, tab, det), c.stream_big);
+                launches += 1;
                 check(cudaEventRecord(c.chunk_done[ch], c.stream_big), "event");
                 bcur = 1 - bcur;
                 if (c.np > 0) {
                     // re-sort the slots by drift path before every launch (cheap
                     // next to the launch; particles change path as they evolve)
-                    pcur = reorder_slots(pcur, c.stream);
+                    if (c.np >= 64) launches += 3;
+                    pcur = reorder_slots(pcur, h, c.stream);
                     check(cudaStreamWaitEvent(c.stream, c.chunk_done[ch], 0), "wait");
                     check(cudaEventRecord(c.kt0[ch], c.stream), "event");
                     particles_and_events(particle_args(pcur, 1 - pcur, ks, reset, 1, s0, h, rcen, tab, det),
                                          c.stream);
+                    launches += (nb > 0) ? 2 : 1;
                     check(cudaEventRecord(c.kt1[ch], c.stream), "event");
                 }
                 pcur = 1 - pcur;
@@ -805,6 +878,7 @@ int mercury_b200_mvs_advance(double time, double h, int nsteps, double rcen, int
                     }
                 c.last_particle_kernel_ms = ksum;
                 c.last_particle_launches = c.np > 0 ? nchunks : 0;
+                c.last_kernel_launches = launches;
                 // the Big and particle states must end in the same buffer index
                 if (bcur != pcur)
                     copy(c.bigstate[pcur].p, c.bigstate[bcur].p, sizeof(double) * 9 * c.nbig);
@@ -862,11 +936,13 @@ int mercury_b200_events(MercuryEvent* dst, int* steps, int cap) {
     return nev;
 }
 
-int mercury_b200_timing(double* advance_ms, double* particle_kernel_ms, int* particle_launches) {
+int mercury_b200_timing(double* advance_ms, double* particle_kernel_ms, int* particle_launches,
+                        int* kernel_launches) {
     Context& c = ctx();
     if (advance_ms) *advance_ms = c.last_advance_ms;
     if (particle_kernel_ms) *particle_kernel_ms = c.last_particle_kernel_ms;
     if (particle_launches) *particle_launches = c.last_particle_launches;
+    if (kernel_launches) *kernel_launches = c.last_kernel_launches;
     return 0;
 }
 

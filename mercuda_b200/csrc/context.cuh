@@ -89,6 +89,7 @@ struct Context {
     float last_advance_ms = 0.0f;
     double last_particle_kernel_ms = 0.0;
     int last_particle_launches = 0;
+    int last_kernel_launches = 0;   // every kernel of the last advance (all streams)
     int64_t nforces = 0;
     int particle_threads = 128;
     int steps_per_launch = 0;   // 0 = automatic

@@ -657,7 +657,11 @@ void launch_variant(const MvsParticleArgs& a, cudaStream_t s, int threads) {
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
     if (per_sm < 1) per_sm = 1;
-    const int grid = tiles < sms * per_sm ? tiles : sms * per_sm;
+    // One CTA slot fewer than the device holds, so that the Big-body CTA of
+    // the next chunk (another stream) can start beside this persistent grid.
+    int slots = sms * per_sm - 1;
+    if (slots < 1) slots = 1;
+    const int grid = tiles < slots ? tiles : slots;
     if (grid > 0) kern<<<grid, threads, smem, s>>>(a);
 }
 
