@@ -14,6 +14,7 @@ device is present when one is needed, the calls raise.
 from __future__ import annotations
 
 import ctypes as C
+import math
 from pathlib import Path
 
 import numpy as np
@@ -180,6 +181,34 @@ class Backend:
 
     def free(self) -> None:
         self.lib.mercury_cuda_free()
+
+    # mal_hvar's step loop (mercury6_2.for:423-470) through the drop-in calls:
+    # steps clipped to tstop, dtflag = 1 (a fresh RA15 sequence) when a clipped
+    # step changes h, events screened after every step.
+    def hvar_run(self, time0: float, tstop: float, h: float, tol: float, rcen: float, max_steps: int = 1_000_000):
+        """Returns (events, step index of each event, h after the last step, steps taken)."""
+        time, dtflag, steps = time0, 0, 0
+        events, where = [], []
+        while steps < max_steps:
+            if abs(tstop - time) <= 0.0:
+                break
+            step = math.copysign(min(abs(tstop - time), abs(h)), tstop - time)
+            if not math.isfinite(step) or time + step == time:
+                break
+            if step != h and dtflag != 0:
+                dtflag = 1
+            h = step
+            hdid, h = self.step(time, h, tol, dtflag)
+            dtflag = 2
+            time = time + hdid
+            ev = self.events(time, hdid, rcen)
+            if len(ev):
+                events.append(ev)
+                where.append(np.full(len(ev), steps, dtype=np.int32))
+            steps += 1
+        if events:
+            return np.concatenate(events), np.concatenate(where), h, steps
+        return np.zeros(0, dtype=EVENT_DTYPE), np.zeros(0, dtype=np.int32), h, steps
 
     # extension: fused multi-step MVS run
     def mvs_advance(self, time: float, h: float, nsteps: int, rcen: float, steps_per_launch: int = 0):

@@ -7,6 +7,7 @@
 #include "../../include/mercury_b200.h"
 #include "context.cuh"
 #include "mvs_device.cuh"
+#include "radau.cuh"
 
 namespace mb200 {
 
@@ -239,7 +240,7 @@ void mvs_step_once(double h) {
         c.cur = reorder_slots(src, h, c.stream);
         // the Big bodies share the buffer index: carry their state across
         if (c.cur != src)
-            check(cudaMemcpyAsync(c.bigstate[c.cur].p, c.bigstate[src].p, sizeof(double) * 9 * c.nbig,
+            check(cudaMemcpyAsync(c.bigstate[c.cur].p, c.bigstate[src].p, sizeof(double) * 9 * c.nsplit,
                                   cudaMemcpyDeviceToDevice, c.stream),
                   "copy");
     }
@@ -265,6 +266,161 @@ void mvs_step_once(double h) {
         c.cur = out;
         c.reset = false;
         c.stepped = true;
+        return;
+    }
+}
+
+ForceCfg force_cfg() {
+    Context& c = ctx();
+    ForceCfg f{};
+    f.nbig = c.nbig;
+    f.nsplit = c.nsplit;
+    f.ngflag = c.ngflag;
+    f.pn = c.pn;
+    f.obl = (c.jcen[0] != 0.0 || c.jcen[1] != 0.0 || c.jcen[2] != 0.0);
+    for (int k = 0; k < 3; ++k) f.jcen[k] = c.jcen[k];
+    f.m0 = c.m_host[0];
+    return f;
+}
+
+// One RA15 sequence with mdt_ra15's step control (mercury6_2.for:4401-4425):
+// the sequence runs on the device, the controller here reads max |b7| and
+// either retries a first sequence with 0.8 of the suggested length or
+// commits it. h is the trial length in, the next one out.
+void ra15_step_once(double time, double* h, double* hdid, double tol, int64_t* rejected) {
+    Context& c = ctx();
+    const int nb = c.nbig - 1;
+    c.ftab.reserve((size_t)(1 + 7 * 6) * force_row(nb));
+    for (;;) {
+        const double t = *h;
+        if (time + t == time) throw std::runtime_error("RADAU step cannot advance time");
+        const int reset = c.reset ? 1 : 0;
+        const int niter = reset ? 6 : 2;
+        const int in = c.cur, out = 1 - c.cur;
+        check(cudaMemsetAsync(c.status.p, 0, sizeof(DeviceStatus), c.stream), "memset");
+        check(cudaMemsetAsync(c.ra_max.p, 0, sizeof(unsigned long long), c.stream), "memset");
+        Ra15Args a{};
+        a.f = force_cfg();
+        a.np = c.np;
+        a.npcap = c.npcap;
+        a.niter = niter;
+        a.reset = reset;
+        a.t = t;
+        a.bx = c.bigstate[in].p;
+        a.bx_a1 = c.bigstate[in].p + 6 * c.nsplit;
+        a.mbig = c.mbig.p;
+        a.ngfbig = c.ngfbig.p;
+        a.bb = c.ra_bb.p;
+        a.bg = c.ra_bg.p;
+        a.bpx = c.ra_bpx.p;
+        a.px = c.pstate[in].p;
+        a.pconst = c.pconst[c.kc].p;
+        a.pb = c.ra_pb.p;
+        a.table = c.ftab.p;
+        a.maxb7 = c.ra_max.p;
+        a.status = c.status.p;
+        launch_ra15_sequence(a, c.stream);
+        check(cudaGetLastError(), "launch");
+        unsigned long long bits = 0;
+        check(cudaMemcpyAsync(&bits, c.ra_max.p, sizeof(bits), cudaMemcpyDeviceToHost, c.stream), "status");
+        read_status();
+        c.nforces += 1 + 7 * niter;
+        double err;
+        std::memcpy(&err, &bits, sizeof(err));
+        if (c.status_host->fault || !std::isfinite(err)) throw std::runtime_error("Nonfinite RADAU force or predictor");
+        err = err / (72.0 * std::pow(std::fabs(t), 7.0));
+        double next = err == 0.0 ? t * 1.4 : std::copysign(std::pow(tol / err, 1.0 / 9.0), t);
+        if (reset && std::fabs(next / t) < 1.0) {
+            *h = next * 0.8;
+            ++*rejected;
+            continue;
+        }
+        if (std::fabs(next / t) > 1.4) next = t * 1.4;
+        Ra15CommitArgs k{};
+        k.nsplit = c.nsplit;
+        k.np = c.np;
+        k.npcap = c.npcap;
+        k.reset = reset;
+        k.tdid = t;
+        k.q = next / t;
+        k.bx = c.bigstate[in].p;
+        k.bx_out = c.bigstate[out].p;
+        k.bb = c.ra_bb.p;
+        k.be = c.ra_be.p;
+        k.px = c.pstate[in].p;
+        k.px_out = c.pstate[out].p;
+        k.pb = c.ra_pb.p;
+        k.pe = c.ra_pe.p;
+        launch_ra15_commit(k, c.stream);
+        check(cudaGetLastError(), "launch");
+        check(cudaStreamSynchronize(c.stream), "step");
+        *hdid = t;
+        *h = next;
+        c.reset = false;
+        c.cur = out;
+        c.stepped = true;
+        c.pair_events = 0;
+        return;
+    }
+}
+
+// mce_stat between the buffers before and after the last step of an adaptive
+// integrator (mercury6_2.for:1765-1918): Big/massive pairs by one CTA, the
+// particles' box overlaps as candidates, classified like the MVS path's.
+void screen_pairs(double h) {
+    Context& c = ctx();
+    const int nb = c.nbig - 1;
+    c.boxes.reserve((size_t)4 * std::max(1, nb));
+    c.detail.reserve((size_t)std::max(1, nb) * TAB_DETAIL);
+    const int prev = 1 - c.cur;
+    for (int attempt = 0;; ++attempt) {
+        check(cudaMemsetAsync(c.status.p, 0, sizeof(DeviceStatus), c.stream), "memset");
+        ScreenArgs a{};
+        a.nbig = c.nbig;
+        a.nsplit = c.nsplit;
+        a.np = c.np;
+        a.npcap = c.npcap;
+        a.h = h;
+        a.b0 = c.bigstate[prev].p;
+        a.b1 = c.bigstate[c.cur].p;
+        a.mbig = c.mbig.p;
+        a.rcebig = c.rcebig.p;
+        a.rphysbig = c.rphysbig.p;
+        a.p0 = c.pstate[prev].p;
+        a.p1 = c.pstate[c.cur].p;
+        a.pconst = c.pconst[c.kc].p;
+        a.perm = c.permp();
+        a.boxes = c.boxes.p;
+        a.detail = c.detail.p;
+        a.events = c.events.p;
+        a.event_step = c.event_step.p;
+        a.event_cap = (int)c.events.n;
+        a.cands = c.cands.p;
+        a.cand_cap = (int)c.cands.n;
+        a.status = c.status.p;
+        launch_screen(a, c.stream);
+        if (nb > 0 && c.np > 0) {
+            ClassifyArgs ca;
+            ca.nb = nb;
+            ca.nbig = c.nbig;
+            ca.h = h;
+            ca.detail = c.detail.p;
+            ca.cands = c.cands.p;
+            ca.cand_cap = (int)c.cands.n;
+            ca.events = c.events.p;
+            ca.event_step = c.event_step.p;
+            ca.event_cap = (int)c.events.n;
+            ca.status = c.status.p;
+            launch_classify(ca, c.stream);
+        }
+        check(cudaGetLastError(), "screen");
+        read_status();
+        if (c.status_host->overflow) {
+            if (attempt > 8) throw std::runtime_error("event buffer growth failed");
+            grow_after_overflow();
+            continue;
+        }
+        c.pair_events = c.status_host->events;
         return;
     }
 }
@@ -500,9 +656,9 @@ void download_buffer(int which, double* xx, double* vv) {
     c.transfer.reserve((size_t)6 * c.n);
     // x and v rows as two 3-component passes
     for (int part = 0; part < 2; ++part) {
-        const double* big = c.bigstate[which].p + 3 * part * c.nbig;
+        const double* big = c.bigstate[which].p + 3 * part * c.nsplit;
         const double* prt = c.pstate[which].p + (size_t)3 * part * c.npcap;
-        gather_kernel<<<blocks(c.n), 256, 0, c.stream>>>(c.transfer.p, c.n, 3, c.nbig, big, c.nbig, prt, c.npcap,
+        gather_kernel<<<blocks(c.n), 256, 0, c.stream>>>(c.transfer.p, c.n, 3, c.nsplit, big, c.nsplit, prt, c.npcap,
                                                           c.inv.p);
         check(cudaMemcpyAsync(part ? vv : xx, c.transfer.p, sizeof(double) * 3 * c.n, cudaMemcpyDeviceToHost,
                               c.stream),
@@ -542,7 +698,7 @@ int mercury_cuda_configure(int method) {
     if (method != 1 && method != 2 && method != 3 && method != 4 && method != 9 && method != 10) return 1;
     Context& c = ctx();
     try {
-        if (!is_mvs(method)) throw std::runtime_error("algorithm not available in this build");
+        if (!is_mvs(method) && method != 4) throw std::runtime_error("algorithm not available in this build");
         if (method != c.algorithm) mercury_cuda_free();
         c.algorithm = method;
         c.reset = true;
@@ -563,25 +719,30 @@ int mercury_cuda_upload(int n, int nbig, int pn, int ngflag, const double* m, co
         if (n < 1 || nbig < 1 || nbig > n) throw std::runtime_error("invalid body counts");
         if (is_mvs(c.algorithm) && nbig > 512) throw std::runtime_error("more than 512 Big bodies");
         c.ensure_streams();
-        bool obl = jcen[0] != 0.0 || jcen[1] != 0.0 || jcen[2] != 0.0;
-        if (is_mvs(c.algorithm) && obl)
+        if (is_mvs(c.algorithm))
             for (int j = nbig; j < n; ++j)
-                if (m[j] != 0.0)
-                    throw std::runtime_error("MVS with central-body oblateness and massive Small bodies");
+                if (m[j] != 0.0) throw std::runtime_error("MVS with massive Small bodies not available in this build");
+        int nmass = nbig;
+        for (int j = nbig; j < n; ++j)
+            if (m[j] != 0.0) nmass = j + 1;
+        const int ns = is_mvs(c.algorithm) ? nbig : nmass;
+        if (ns > 512) throw std::runtime_error("more than 512 Big and massive Small bodies");
         c.n = n;
         c.nbig = nbig;
-        c.np = n - nbig;
+        c.nmass = nmass;
+        c.nsplit = ns;
+        c.np = n - ns;
         c.npcap = std::max(2, (c.np + 1) & ~1);
-        c.pn = pn;
+        c.pn = pn != 0 ? 1 : 0;
         c.ngflag = ngflag;
         for (int k = 0; k < 3; ++k) c.jcen[k] = jcen[k];
         c.m_host.assign(m, m + n);
-        c.mbig.reserve(nbig);
-        c.rcebig.reserve(nbig);
-        c.rphysbig.reserve(nbig);
-        c.ngfbig.reserve((size_t)5 * nbig);
+        c.mbig.reserve(ns);
+        c.rcebig.reserve(ns);
+        c.rphysbig.reserve(ns);
+        c.ngfbig.reserve((size_t)5 * ns);
         for (int k = 0; k < 2; ++k) {
-            c.bigstate[k].reserve((size_t)9 * nbig);
+            c.bigstate[k].reserve((size_t)9 * ns);
             c.pstate[k].reserve((size_t)9 * c.npcap);
         }
         for (int k = 0; k < 2; ++k) {
@@ -594,21 +755,30 @@ int mercury_cuda_upload(int n, int nbig, int pn, int ngflag, const double* m, co
         ensure_events(std::max(4096, c.np / 64));
         c.cands.reserve(std::max(16384, c.np / 2));
         c.transfer.reserve((size_t)6 * n);
+        if (c.algorithm == 4) {
+            c.ra_bb.reserve((size_t)21 * ns);
+            c.ra_be.reserve((size_t)21 * ns);
+            c.ra_bg.reserve((size_t)21 * ns);
+            c.ra_bpx.reserve((size_t)6 * ns);
+            c.ra_pb.reserve((size_t)21 * c.npcap);
+            c.ra_pe.reserve((size_t)21 * c.npcap);
+            c.ra_max.reserve(1);
+        }
         cudaStream_t s = c.stream;
         // zero padding and cached accelerations
         check(cudaMemsetAsync(c.pstate[0].p, 0, sizeof(double) * 9 * c.npcap, s), "memset");
         check(cudaMemsetAsync(c.pstate[1].p, 0, sizeof(double) * 9 * c.npcap, s), "memset");
-        check(cudaMemsetAsync(c.bigstate[0].p, 0, sizeof(double) * 9 * nbig, s), "memset");
-        check(cudaMemsetAsync(c.bigstate[1].p, 0, sizeof(double) * 9 * nbig, s), "memset");
+        check(cudaMemsetAsync(c.bigstate[0].p, 0, sizeof(double) * 9 * ns, s), "memset");
+        check(cudaMemsetAsync(c.bigstate[1].p, 0, sizeof(double) * 9 * ns, s), "memset");
         check(cudaMemsetAsync(c.pconst[0].p, 0, sizeof(double) * 8 * c.npcap, s), "memset");
         check(cudaMemsetAsync(c.pconst[1].p, 0, sizeof(double) * 8 * c.npcap, s), "memset");
         c.cur = 0;
-        order_particles(n, nbig, m[0], xx, vv);
+        order_particles(n, ns, m[0], xx, vv);
         // positions and velocities
         for (int part = 0; part < 2; ++part) {
             check(cudaMemcpyAsync(c.transfer.p, part ? vv : xx, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s),
                   "upload");
-            scatter_rows(c.transfer.p, n, 3, nbig, c.bigstate[0].p + 3 * part * nbig, nbig,
+            scatter_rows(c.transfer.p, n, 3, ns, c.bigstate[0].p + 3 * part * ns, ns,
                          c.pstate[0].p + (size_t)3 * part * c.npcap, c.npcap, c.inv.p, s);
             check(cudaStreamSynchronize(s), "upload");
         }
@@ -618,14 +788,14 @@ int mercury_cuda_upload(int n, int nbig, int pn, int ngflag, const double* m, co
         double* pdst[3] = {c.pm(), c.prce(), c.prphys()};
         for (int q = 0; q < 3; ++q) {
             check(cudaMemcpyAsync(c.transfer.p, scalars[q], sizeof(double) * n, cudaMemcpyHostToDevice, s), "upload");
-            scatter_rows(c.transfer.p, n, 1, nbig, bigdst[q], nbig, pdst[q], c.npcap, c.inv.p, s);
+            scatter_rows(c.transfer.p, n, 1, ns, bigdst[q], ns, pdst[q], c.npcap, c.inv.p, s);
             check(cudaStreamSynchronize(s), "upload");
         }
         // ngf: Big rows stay interleaved (5 per body); particles become SoA
-        check(cudaMemcpyAsync(c.ngfbig.p, ng, sizeof(double) * 5 * nbig, cudaMemcpyHostToDevice, s), "upload");
+        check(cudaMemcpyAsync(c.ngfbig.p, ng, sizeof(double) * 5 * ns, cudaMemcpyHostToDevice, s), "upload");
         c.transfer.reserve((size_t)6 * n);
         check(cudaMemcpyAsync(c.transfer.p, ng, sizeof(double) * 5 * n, cudaMemcpyHostToDevice, s), "upload");
-        scatter_rows(c.transfer.p, n, 5, nbig, nullptr, 0, c.pngf(), c.npcap, c.inv.p, s);
+        scatter_rows(c.transfer.p, n, 5, ns, nullptr, 0, c.pngf(), c.npcap, c.inv.p, s);
         check(cudaStreamSynchronize(s), "upload");
         check(cudaGetLastError(), "upload");
         c.reset = true;
@@ -637,16 +807,19 @@ int mercury_cuda_upload(int n, int nbig, int pn, int ngflag, const double* m, co
 }
 
 int mercury_cuda_step(double time, double* h, double* hdid, double tol, int64_t* forces, int64_t* rejected) {
-    (void)time;
-    (void)tol;
     Context& c = ctx();
     try {
         require_system();
         *rejected = 0;
         const int64_t before = c.nforces;
-        if (!is_mvs(c.algorithm)) throw std::runtime_error("algorithm not available in this build");
-        mvs_step_once(*h);
-        *hdid = *h;
+        if (is_mvs(c.algorithm)) {
+            mvs_step_once(*h);
+            *hdid = *h;
+        } else if (c.algorithm == 4) {
+            ra15_step_once(time, h, hdid, tol, rejected);
+        } else {
+            throw std::runtime_error("algorithm not available in this build");
+        }
         *forces = c.nforces - before;
         return 0;
     } catch (const std::exception& e) {
@@ -670,14 +843,15 @@ int mercury_cuda_events(double time, double h, double rcen, const MercuryEvent**
     try {
         require_system();
         const int prev = 1 - c.cur;
+        if (!is_mvs(c.algorithm) && c.stepped) screen_pairs(h);
         for (int attempt = 0;; ++attempt) {
             // restart the counter after the step's pair events, then screen for central impacts
             DeviceStatus st = {0, c.pair_events, 0, 0};
             check(cudaMemcpyAsync(c.status.p, &st, sizeof(st), cudaMemcpyHostToDevice, c.stream), "status");
-            const int total = c.nbig - 1 + c.np;
+            const int total = c.nsplit - 1 + c.np;
             if (c.stepped && total > 0) {
                 CentralArgs a;
-                a.nbig = c.nbig;
+                a.nbig = c.nsplit;
                 a.np = c.np;
                 a.npcap = c.npcap;
                 a.mu = c.m_host[0];
@@ -734,9 +908,36 @@ int mercury_cuda_events(double time, double h, double rcen, const MercuryEvent**
 }
 
 int mercury_cuda_force(double* a) {
-    (void)a;
+    Context& c = ctx();
     try {
-        throw std::runtime_error("force interface not available in this build");
+        require_system();
+        const int nb = c.nbig - 1, ns = c.nsplit;
+        c.ftab.reserve((size_t)force_row(nb));
+        c.force_out.reserve((size_t)3 * ns + (size_t)3 * c.npcap);
+        check(cudaMemsetAsync(c.status.p, 0, sizeof(DeviceStatus), c.stream), "memset");
+        ForceAllArgs f{};
+        f.f = force_cfg();
+        f.np = c.np;
+        f.npcap = c.npcap;
+        f.bx = c.bigstate[c.cur].p;
+        f.mbig = c.mbig.p;
+        f.ngfbig = c.ngfbig.p;
+        f.px = c.pstate[c.cur].p;
+        f.pconst = c.pconst[c.kc].p;
+        f.abig = c.force_out.p;
+        f.apart = c.force_out.p + 3 * (size_t)ns;
+        f.table = c.ftab.p;
+        f.status = c.status.p;
+        launch_force_all(f, c.stream);
+        check(cudaGetLastError(), "force");
+        read_status();
+        c.nforces += 1;
+        if (c.status_host->fault) throw std::runtime_error("Nonfinite force or undefined orbit direction");
+        c.transfer.reserve((size_t)6 * c.n);
+        gather_rows(c.transfer.p, c.n, 3, ns, f.abig, ns, f.apart, c.npcap, c.inv.p, c.stream);
+        check(cudaMemcpyAsync(a, c.transfer.p, sizeof(double) * 3 * c.n, cudaMemcpyDeviceToHost, c.stream), "force");
+        check(cudaStreamSynchronize(c.stream), "force");
+        return 0;
     } catch (const std::exception& e) {
         return report(e);
     }
@@ -760,7 +961,7 @@ int mercury_cuda_limits(const double* limits) {
     try {
         require_system();
         check(cudaMemcpyAsync(c.transfer.p, limits, sizeof(double) * c.n, cudaMemcpyHostToDevice, c.stream), "limits");
-        scatter_rows(c.transfer.p, c.n, 1, c.nbig, c.rcebig.p, c.nbig, c.prce(), c.npcap, c.inv.p, c.stream);
+        scatter_rows(c.transfer.p, c.n, 1, c.nsplit, c.rcebig.p, c.nsplit, c.prce(), c.npcap, c.inv.p, c.stream);
         check(cudaStreamSynchronize(c.stream), "limits");
         return 0;
     } catch (const std::exception& e) {

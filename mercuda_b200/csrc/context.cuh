@@ -47,6 +47,10 @@ struct Context {
     int algorithm = 2;
     // system
     int n = 0, nbig = 0, np = 0, npcap = 0;
+    // Bodies [0, nsplit) live in the "big" arrays, [nsplit, n) in the particle
+    // slots. MVS splits at nbig; RADAU/BS also keep every massive Small body
+    // (semi-active, it acts on the Big bodies) in the big arrays.
+    int nsplit = 0, nmass = 0;
     int pn = 0, ngflag = 0;
     double jcen[3] = {0, 0, 0};
     std::vector<double> m_host;
@@ -69,6 +73,12 @@ struct Context {
     bool stepped = false;
     // MVS tables
     DBuf<double> tab, detail;
+    // RA15: B, E, G and predictor scratch of the massive set ([21][nsplit],
+    // [6][nsplit]), B and E of the particle slots ([21][npcap]), the per-node
+    // force table, max |b7| and the force entry's output ([3][nsplit] then
+    // [3][npcap]); screen boxes of the adaptive integrators ([nbig-1][4])
+    DBuf<double> ra_bb, ra_be, ra_bg, ra_bpx, ra_pb, ra_pe, ftab, force_out, boxes;
+    DBuf<unsigned long long> ra_max;
     // events
     DBuf<MercuryEvent> events;
     DBuf<int> event_step;
@@ -119,10 +129,12 @@ struct Context {
     }
     void release_all() {
         DBuf<double>* bufs[] = {&mbig, &rcebig, &rphysbig, &ngfbig, &bigstate[0], &bigstate[1], &pstate[0],
-                                &pstate[1], &pconst[0], &pconst[1], &tab, &detail, &transfer, &snapshot, &snap_const};
+                                &pstate[1], &pconst[0], &pconst[1], &tab, &detail, &transfer, &snapshot, &snap_const,
+                                &ra_bb, &ra_be, &ra_bg, &ra_bpx, &ra_pb, &ra_pe, &ftab, &force_out, &boxes};
         for (auto* b : bufs) b->release();
         DBuf<int>* ibufs[] = {&perm[0], &perm[1], &inv, &order_bucket, &order_hist, &snap_perm};
         for (auto* b : ibufs) b->release();
+        ra_max.release();
         kc = 0;
         events.release();
         event_step.release();

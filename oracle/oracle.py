@@ -73,6 +73,13 @@ def lib() -> C.CDLL:
         L.oracle_run_free.argtypes = [C.c_void_p]
         L.oracle_count_mvs.argtypes = [I, I, PD, PD, PD, PD, I, PD, PD, PD, D, D, I, D,
                                        C.POINTER(C.c_uint64)]
+        L.oracle_force.argtypes = [I, I, PD, PD, PD, PD, I, I, PD, PD]
+        L.oracle_force.restype = I
+        L.oracle_force_term.argtypes = [I, I, PD, PD, PD, PD, PD]
+        L.oracle_force_term.restype = I
+        L.oracle_ra15_run.argtypes = [I, I, PD, PD, PD, PD, I, I, PD, PD, PD, D, D, PD, D, D, I, I,
+                                      C.POINTER(C.c_longlong)]
+        L.oracle_ra15_run.restype = C.c_void_p
         _lib = L
     return _lib
 
@@ -186,3 +193,43 @@ def count_mvs(sys, time0: float, h: float, nsteps: int, rcen: float):
     lib().oracle_count_mvs(s.n, s.nbig, _p(s.m), _p(s.x), _p(s.v), _p(s.ngf), s.ngflag,
                            _p(s.jcen), _p(s.rce), _p(s.rphys), time0, h, nsteps, rcen, out)
     return dict(zip(["add", "mul", "div", "sqrt", "cmp", "libm"], list(out)))
+
+
+def force(sys):
+    """mfo_all (mercury6_2.for:4506-4571) of the whole system, shape (n, 3)."""
+    a = np.zeros((sys.n, 3))
+    rc = lib().oracle_force(sys.n, sys.nbig, _p(sys.m), _p(sys.x), _p(sys.v), _p(sys.ngf), sys.ngflag,
+                            int(sys.pn), _p(sys.jcen), _p(a))
+    if rc:
+        raise RuntimeError("oracle mfo_all failed")
+    return a
+
+
+def force_term(which, m, x, v, ngf):
+    """One force law alone: 'pr' (mfo_pr), 'ngf' (mfo_ngf) or 'pn' (mfo_pn)."""
+    code = {"pr": 0, "ngf": 1, "pn": 2}[which]
+    m, x, v, ngf = _f64(m), _f64(x), _f64(v), _f64(ngf)
+    a = np.zeros_like(x)
+    if lib().oracle_force_term(code, len(m), _p(m), _p(x), _p(v), _p(ngf), _p(a)):
+        raise RuntimeError("oracle force law failed")
+    return a
+
+
+def ra15_run(sys, time0, tstop, h, tol, rcen=0.005, central=True, max_steps=1_000_000):
+    """mal_hvar-style RA15 loop on sys (in place). Returns (events, steps, h_next, nsteps, nforces)."""
+    s = sys
+    hh = D(h)
+    counters = (C.c_longlong * 2)()
+    handle = lib().oracle_ra15_run(s.n, s.nbig, _p(s.m), _p(s.x), _p(s.v), _p(s.ngf), s.ngflag, int(s.pn),
+                                   _p(s.jcen), _p(s.rce), _p(s.rphys), time0, tstop, C.byref(hh), tol, rcen,
+                                   int(central), int(max_steps), counters)
+    try:
+        if lib().oracle_run_status(handle):
+            raise RuntimeError("oracle RA15 run failed")
+        count = lib().oracle_run_event_count(handle)
+        events = np.zeros(count, dtype=EVENT_DTYPE)
+        steps = np.zeros(count, dtype=np.int32)
+        lib().oracle_run_events(handle, events.ctypes.data_as(C.c_void_p), steps.ctypes.data_as(C.c_void_p))
+    finally:
+        lib().oracle_run_free(handle)
+    return events, steps, hh.value, counters[0], counters[1]

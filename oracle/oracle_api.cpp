@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "oracle_mvs.hpp"
+#include "oracle_ra15.hpp"
 
 namespace oracle {
 thread_local Tally tally;
@@ -246,6 +247,68 @@ void oracle_count_mvs(int n, int nbig, const double* m, const double* x, const d
     out[3] = oracle::tally.sqrt;
     out[4] = oracle::tally.cmp;
     out[5] = oracle::tally.libm;
+}
+
+// Single force laws for known-answer tests: 0 = mfo_pr, 1 = mfo_ngf, 2 = mfo_pn.
+int oracle_force_term(int which, int n, const double* m, const double* x, const double* v, const double* ngf,
+                      double* a) {
+    if (which == 0) oracle::mfo_pr<double>(n, m, x, v, a, ngf);
+    else if (which == 1) return oracle::mfo_ngf<double>(n, x, v, a, ngf);
+    else oracle::mfo_pn<double>(n, m, x, v, a);
+    return 0;
+}
+
+// mfo_all (mercury6_2.for:4506-4571) on the whole system; a(3n) out.
+int oracle_force(int n, int nbig, const double* m, const double* x, const double* v, const double* ngf,
+                 int ngflag, int pn, const double* jcen, double* a) {
+    return oracle::mfo_all<double>(jcen, n, nbig, m, x, v, a, ngf, ngflag, pn);
+}
+
+// Variable-step RA15 loop in the manner of mal_hvar (mercury6_2.for:389-463)
+// from time0 towards tstop: each step is clipped to the remaining interval
+// (clipped_step, mercury_support.f90:207-212), a clipped step restarts the
+// predictor (dtflag = 1, mercury6_2.for:429), and after each step mce_stat
+// (x0,v0 = the state before the step) and, if central != 0, mce_cent screen
+// for events. h is the initial trial step (in/out). Returns the number of
+// steps, or -1 on failure; events are kept in the run handle.
+OracleRun* oracle_ra15_run(int n, int nbig, const double* m, double* x, double* v, const double* ngf,
+                           int ngflag, int pn, const double* jcen, const double* rce, const double* rphys,
+                           double time0, double tstop, double* h, double tol, double rcen, int central,
+                           int max_steps, long long* counters) {
+    OracleRun* run = new OracleRun();
+    oracle::Ra15State st;
+    st.size(n);
+    std::vector<double> x0(3 * n), v0(3 * n);
+    double time = time0;
+    long long forces = 0, steps = 0;
+    std::vector<Event> events;
+    while (steps < max_steps) {
+        if (std::fabs(tstop - time) <= 0.0) break;
+        double target = tstop;
+        double step = std::copysign(std::min(std::fabs(target - time), std::fabs(*h)), target - time);
+        if (!std::isfinite(step) || time + step == time) break;
+        if (step != *h && st.dtflag != 0) st.dtflag = 1;
+        *h = step;
+        std::copy(x, x + 3 * n, x0.begin());
+        std::copy(v, v + 3 * n, v0.begin());
+        double hdid = 0.0;
+        if (oracle::mdt_ra15(time, *h, hdid, tol, jcen, n, nbig, m, x, v, ngf, ngflag, pn, st, &forces)) {
+            run->status = 1;
+            break;
+        }
+        time = time + hdid;
+        events.clear();
+        oracle::mce_stat<double>(time, hdid, n, nbig, m, x0.data(), v0.data(), x, v, rce, rphys, events);
+        if (central) oracle::mce_cent<double>(time, hdid, rcen, 1, n, m, x0.data(), v0.data(), x, v, events);
+        std::stable_sort(events.begin(), events.end(), event_less);
+        for (auto& e : events) run->events.push_back(StepEvent{(int)steps, e});
+        ++steps;
+    }
+    if (counters) {
+        counters[0] = steps;
+        counters[1] = forces;
+    }
+    return run;
 }
 
 }  // extern "C"
