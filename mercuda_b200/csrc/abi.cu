@@ -7,6 +7,7 @@
 #include "../../include/mercury_b200.h"
 #include "context.cuh"
 #include "mvs_device.cuh"
+#include "bs.cuh"
 #include "radau.cuh"
 
 namespace mb200 {
@@ -364,6 +365,97 @@ void ra15_step_once(double time, double* h, double* hdid, double tol, int64_t* r
     }
 }
 
+// One mdt_bs1 (algorithm 2) or mdt_bs2 (algorithm 3) step with the Fortran's
+// control (mercury6_2.for:3380-3404, 3568-3596): the first level n > 3 whose
+// global error is <= tol^2 is taken, else the step is halved and redone.
+void bs_step_once(double time, double* h, double* hdid, double tol, int64_t* rejected) {
+    Context& c = ctx();
+    const int V = c.algorithm == 2 ? 1 : 2;
+    const int L = bs_levels(V), nb = c.nbig - 1, N = c.nsplit;
+    c.ftab.reserve((size_t)bs_rows(V) * force_row(nb));
+    c.bs_scr.reserve((size_t)bs_massive_scratch(V) * N);
+    c.bs_bcand.reserve((size_t)bs_candidates(V) * 6 * N);
+    c.bs_pcand.reserve((size_t)bs_candidates(V) * 6 * c.npcap);
+    c.bs_errs.reserve(13);
+    c.bs_lvst.reserve(13);
+    const double tol2 = tol * tol;
+    const int in = c.cur, out = 1 - c.cur;
+    int64_t forces = 1;  // the start-of-step force
+    const char* nonfinite = V == 1 ? "Nonfinite BS extrapolation; inspect input or close encounters"
+                                   : "Nonfinite BS2 force or extrapolation";
+    for (;;) {
+        if (time + *h == time) throw std::runtime_error("BS cannot advance time at the requested tolerance");
+        check(cudaMemsetAsync(c.bs_errs.p, 0, sizeof(unsigned long long) * 13, c.stream), "memset");
+        check(cudaMemsetAsync(c.bs_lvst.p, 0, sizeof(DeviceStatus) * 13, c.stream), "memset");
+        BsArgs a{};
+        a.f = force_cfg();
+        a.variant = V;
+        a.np = c.np;
+        a.npcap = c.npcap;
+        a.h0 = *h;
+        a.bx = c.bigstate[in].p;
+        a.mbig = c.mbig.p;
+        a.ngfbig = c.ngfbig.p;
+        a.bscr = c.bs_scr.p;
+        a.px = c.pstate[in].p;
+        a.pconst = c.pconst[c.kc].p;
+        a.table = c.ftab.p;
+        a.bcand = c.bs_bcand.p;
+        a.pcand = c.bs_pcand.p;
+        a.errs = c.bs_errs.p;
+        a.lvst = c.bs_lvst.p;
+        launch_bs_sequence(a, c.stream);
+        check(cudaGetLastError(), "launch");
+        unsigned long long errs[13];
+        DeviceStatus lv[13];
+        check(cudaMemcpyAsync(errs, c.bs_errs.p, sizeof(errs), cudaMemcpyDeviceToHost, c.stream), "status");
+        check(cudaMemcpyAsync(lv, c.bs_lvst.p, sizeof(lv), cudaMemcpyDeviceToHost, c.stream), "status");
+        check(cudaStreamSynchronize(c.stream), "step");
+        const int fails = FAULT_NGF | FAULT_COINCIDENT;
+        if (lv[0].fault & fails) throw std::runtime_error("BS force failed");
+        int accepted = 0;
+        for (int n = 1; n <= L && !accepted; ++n) {
+            forces += bs_level_forces(V, n);
+            if (lv[n].fault & fails) throw std::runtime_error("BS force failed");
+            if (n <= 3) continue;
+            double e;
+            std::memcpy(&e, &errs[n], sizeof(e));
+            if (!std::isfinite(e)) throw std::runtime_error(nonfinite);
+            if (e <= tol2) accepted = n;
+        }
+        if (!accepted) {
+            ++*rejected;
+            *h = *h * 0.5;
+            continue;
+        }
+        BsCommitArgs k{};
+        k.nsplit = N;
+        k.np = c.np;
+        k.npcap = c.npcap;
+        k.cand = accepted - 4;
+        k.bcand = c.bs_bcand.p;
+        k.pcand = c.bs_pcand.p;
+        k.bx = c.bigstate[in].p;
+        k.bx_out = c.bigstate[out].p;
+        k.px_out = c.pstate[out].p;
+        launch_bs_commit(k, c.stream);
+        check(cudaGetLastError(), "launch");
+        check(cudaStreamSynchronize(c.stream), "step");
+        *hdid = *h;
+        if (V == 1) {
+            if (accepted == 8) *h = *h * 0.55;
+        } else {
+            if (accepted >= 8) *h = *h * 0.55;
+        }
+        if (accepted < 7) *h = *h * 1.3;
+        c.nforces += forces;
+        c.cur = out;
+        c.stepped = true;
+        c.pair_events = 0;
+        return;
+    }
+}
+
 // mce_stat between the buffers before and after the last step of an adaptive
 // integrator (mercury6_2.for:1765-1918): Big/massive pairs by one CTA, the
 // particles' box overlaps as candidates, classified like the MVS path's.
@@ -422,6 +514,55 @@ void screen_pairs(double h) {
         }
         c.pair_events = c.status_host->events;
         return;
+    }
+}
+
+// mco_mvs2h of the current MVS state into host rows (the reference exports
+// with its corrector on scratch copies, mercury_cuda.cu:508-513); the state
+// itself is not changed.
+void export_corrected(double h, double* xx, double* vv) {
+    Context& c = ctx();
+    const int nbig = c.nbig;
+    ensure_tables(4, 1);
+    c.corr_big.reserve((size_t)9 * nbig);
+    c.corr_part.reserve((size_t)6 * c.npcap);
+    check(cudaMemsetAsync(c.status.p, 0, sizeof(DeviceStatus), c.stream), "memset");
+    MvsBigArgs b = big_args(c.cur, c.cur, 0, 0, 0, 0, h, 0.0, c.tab.p, c.detail.p);
+    b.out.x = c.corr_big.p;
+    b.out.v = c.corr_big.p + 3 * nbig;
+    b.out.a = c.corr_big.p + 6 * nbig;
+    CorrectorArgs k{};
+    k.np = c.np;
+    k.npcap = c.npcap;
+    k.nb = nbig - 1;
+    k.ngf_on = (c.ngflag == 1 || c.ngflag == 3);
+    k.obl = (c.jcen[0] != 0.0 || c.jcen[1] != 0.0 || c.jcen[2] != 0.0);
+    k.forward = 1;
+    k.mu = c.m_host[0];
+    const double rt10 = std::sqrt(10.0);
+    k.ha[0] = h * rt10 * 3.0 / 10.0;
+    k.hb[0] = -(h * rt10 / 72.0);
+    k.ha[1] = h * rt10 / 5.0;
+    k.hb[1] = h * rt10 / 24.0;
+    for (int q = 0; q < 3; ++q) k.jcen[q] = c.jcen[q];
+    k.xin = c.pstate[c.cur].p;
+    k.xout = c.corr_part.p;
+    k.ngf = c.pngf();
+    k.tab = c.tab.p;
+    k.status = c.status.p;
+    launch_mvs_corrector(b, k, c.stream);
+    check(cudaGetLastError(), "corrector");
+    read_status();
+    if (c.status_host->fault) throw std::runtime_error("Output corrector failed");
+    c.transfer.reserve((size_t)6 * c.n);
+    for (int part = 0; part < 2; ++part) {
+        gather_kernel<<<blocks(c.n), 256, 0, c.stream>>>(c.transfer.p, c.n, 3, nbig, c.corr_big.p + 3 * part * nbig,
+                                                          nbig, c.corr_part.p + (size_t)3 * part * c.npcap, c.npcap,
+                                                          c.inv.p);
+        check(cudaMemcpyAsync(part ? vv : xx, c.transfer.p, sizeof(double) * 3 * c.n, cudaMemcpyDeviceToHost,
+                              c.stream),
+              "export");
+        check(cudaStreamSynchronize(c.stream), "export");
     }
 }
 
@@ -698,7 +839,7 @@ int mercury_cuda_configure(int method) {
     if (method != 1 && method != 2 && method != 3 && method != 4 && method != 9 && method != 10) return 1;
     Context& c = ctx();
     try {
-        if (!is_mvs(method) && method != 4) throw std::runtime_error("algorithm not available in this build");
+        if (method == 10) throw std::runtime_error("algorithm not available in this build");
         if (method != c.algorithm) mercury_cuda_free();
         c.algorithm = method;
         c.reset = true;
@@ -817,6 +958,8 @@ int mercury_cuda_step(double time, double* h, double* hdid, double tol, int64_t*
             *hdid = *h;
         } else if (c.algorithm == 4) {
             ra15_step_once(time, h, hdid, tol, rejected);
+        } else if (c.algorithm == 2 || c.algorithm == 3) {
+            bs_step_once(time, h, hdid, tol, rejected);
         } else {
             throw std::runtime_error("algorithm not available in this build");
         }
@@ -944,12 +1087,11 @@ int mercury_cuda_force(double* a) {
 }
 
 int mercury_cuda_export(double h, int physical, double* xx, double* vv) {
-    (void)h;
     Context& c = ctx();
     try {
         require_system();
-        if (physical && c.algorithm == 1) throw std::runtime_error("output corrector not available in this build");
-        download_buffer(c.cur, xx, vv);
+        if (physical && c.algorithm == 1) export_corrected(h, xx, vv);
+        else download_buffer(c.cur, xx, vv);
         return 0;
     } catch (const std::exception& e) {
         return report(e);

@@ -1,0 +1,366 @@
+// Bulirsch-Stoer kernels (mdt_bs1, mdt_bs2): every statement keeps the
+// Fortran's evaluation order so that each level's extrapolated state rounds
+// as the CPU's does.
+#include "allforce.cuh"
+#include "bs.cuh"
+
+namespace mb200 {
+namespace {
+
+constexpr unsigned FULLMASK = 0xffffffffu;
+constexpr unsigned long long ERR_NONFINITE = 0x7ff0000000000000ull;  // +inf
+
+// The step length of level n and its h2 entry (mercury6_2.for:3285-3287,
+// 3476-3479).
+template <int VARIANT> __device__ __forceinline__ double level_h(double h0, int n) {
+    return VARIANT == 1 ? h0 / (2.0 * double(n)) : h0 / double(n);
+}
+template <int VARIANT> __device__ __forceinline__ double level_h2(double h0, int n) {
+    if (VARIANT == 1) return 0.25 / double(n * n);
+    const double h = h0 / double(n);
+    return h * h;
+}
+
+__device__ __forceinline__ void level_error(double err, bool finite, unsigned long long* dst) {
+    atomicMax(dst, finite ? (unsigned long long)__double_as_longlong(err) : ERR_NONFINITE);
+}
+
+// Error term of one body (mercury6_2.for:3372-3378): false if not finite.
+__device__ __forceinline__ bool body_error(const double* q, double xscal, double vscal, double& e) {
+    for (int c = 0; c < 6; ++c)
+        if (!isfinite(q[c])) return false;
+    const double tmp1 = fmax(fmax(q[0] * q[0], q[1] * q[1]), q[2] * q[2]);
+    const double tmp2 = fmax(fmax(q[3] * q[3], q[4] * q[4]), q[5] * q[5]);
+    e = fmax(tmp1 * xscal, tmp2 * vscal);
+    return true;
+}
+
+// ------------------------------------------------------------ massive set
+// Scratch rows of the massive-set CTA, each [nsplit] doubles.
+struct BsScratch {
+    double *X, *V, *XE, *VE, *A, *A0, *B, *C, *XS, *VS, *D;
+    __device__ BsScratch(double* base, int N) {
+        double* p = base;
+        double** rows[] = {&X, &V, &XE, &VE, &A, &A0, &B, &C};
+        for (double** r : rows) { *r = p; p += 3 * N; }
+        XS = p; p += N;
+        VS = p; p += N;
+        D = p;  // [levels][6][N]
+    }
+};
+
+// One force call of the massive set into S.A (or A0) and table row T.
+__device__ void massive_call(const BsArgs& A, const double* X, const double* V, double* out, double* T,
+                             DeviceStatus* st) {
+    const ForceCfg& f = A.f;
+    const int N = f.nsplit;
+    __syncthreads();
+    if (threadIdx.x == 0) row_head(X, A.mbig, f, T);
+    __syncthreads();
+    for (int k = threadIdx.x; k < N; k += blockDim.x) {
+        if (k >= 1 && k < f.nbig) {
+            double* row = T + FT_HEAD + 4 * (k - 1);
+            row[0] = X[k]; row[1] = X[N + k]; row[2] = X[2 * N + k]; row[3] = A.mbig[k];
+        }
+        if (k < 1) continue;
+        const double3 a = massive_allforce(k, X, V, A.mbig, A.ngfbig, T, f, st);
+        out[k] = a.x; out[N + k] = a.y; out[2 * N + k] = a.z;
+    }
+    __syncthreads();
+}
+
+template <int VARIANT> __global__ void __launch_bounds__(256) bs_massive_kernel(BsArgs A) {
+    const int N = A.f.nsplit, tid = threadIdx.x, nt = blockDim.x;
+    const int L = bs_levels(VARIANT), stride = force_row(A.f.nbig - 1);
+    BsScratch S(A.bscr, N);
+    const double* X0 = A.bx;
+    const double* V0 = A.bx + 3 * N;
+    __shared__ double wmax[8];
+    __shared__ int wbad[8];
+    for (int k = tid; k < N; k += nt) {
+        for (int c = 0; c < 3; ++c) {
+            const int z = c * N + k;
+            S.X[z] = X0[z]; S.V[z] = V0[z]; S.XE[z] = X0[z]; S.VE[z] = V0[z];
+        }
+        const double tmp1 = X0[k] * X0[k] + X0[N + k] * X0[N + k] + X0[2 * N + k] * X0[2 * N + k];
+        const double tmp2 = V0[k] * V0[k] + V0[N + k] * V0[N + k] + V0[2 * N + k] * V0[2 * N + k];
+        S.XS[k] = 1.0 / fmax(tmp1, 1e-300);
+        S.VS[k] = 1.0 / fmax(tmp2, 1e-300);
+    }
+    int row = 0;
+    massive_call(A, X0, V0, S.A0, A.table, &A.lvst[0]);
+    ++row;
+    for (int n = 1; n <= L; ++n) {
+        DeviceStatus* st = &A.lvst[n];
+        const double h = level_h<VARIANT>(A.h0, n);
+        const double h2n = level_h2<VARIANT>(A.h0, n);
+        if (VARIANT == 1) {
+            const double hx2 = h * 2.0;
+            for (int k = 1 + tid; k < N; k += nt)
+                for (int c = 0; c < 3; ++c) {
+                    const int z = c * N + k;
+                    S.X[z] = X0[z] + h * V0[z];
+                    S.V[z] = V0[z] + h * S.A0[z];
+                }
+            massive_call(A, S.X, S.V, S.A, A.table + (size_t)(row++) * stride, st);
+            for (int k = 1 + tid; k < N; k += nt)
+                for (int c = 0; c < 3; ++c) {
+                    const int z = c * N + k;
+                    S.XE[z] = X0[z] + hx2 * S.V[z];
+                    S.VE[z] = V0[z] + hx2 * S.A[z];
+                }
+            for (int j = 2; j <= n; ++j) {
+                massive_call(A, S.XE, S.VE, S.A, A.table + (size_t)(row++) * stride, st);
+                for (int k = 1 + tid; k < N; k += nt)
+                    for (int c = 0; c < 3; ++c) {
+                        const int z = c * N + k;
+                        S.X[z] = S.X[z] + hx2 * S.VE[z];
+                        S.V[z] = S.V[z] + hx2 * S.A[z];
+                    }
+                massive_call(A, S.X, S.V, S.A, A.table + (size_t)(row++) * stride, st);
+                for (int k = 1 + tid; k < N; k += nt)
+                    for (int c = 0; c < 3; ++c) {
+                        const int z = c * N + k;
+                        S.XE[z] = S.XE[z] + hx2 * S.V[z];
+                        S.VE[z] = S.VE[z] + hx2 * S.A[z];
+                    }
+            }
+            massive_call(A, S.XE, S.VE, S.A, A.table + (size_t)(row++) * stride, st);
+            double* Dn = S.D + (size_t)(n - 1) * 6 * N;
+            for (int k = 1 + tid; k < N; k += nt)
+                for (int c = 0; c < 3; ++c) {
+                    const int z = c * N + k;
+                    Dn[z] = 0.5 * (S.XE[z] + S.X[z] + h * S.VE[z]);
+                    Dn[3 * N + z] = 0.5 * (S.VE[z] + S.V[z] + h * S.A[z]);
+                }
+        } else {
+            const double hby2 = 0.5 * h, h2by2 = 0.5 * h2n;
+            for (int k = 1 + tid; k < N; k += nt)
+                for (int c = 0; c < 3; ++c) {
+                    const int z = c * N + k;
+                    S.B[z] = 0.5 * S.A0[z];
+                    S.C[z] = 0.0;
+                    S.XE[z] = h2by2 * S.A0[z] + h * V0[z] + X0[z];
+                }
+            for (int j = 2; j <= n; ++j) {
+                massive_call(A, S.XE, V0, S.A, A.table + (size_t)(row++) * stride, st);
+                const double tmp0 = h * double(j);
+                for (int k = 1 + tid; k < N; k += nt)
+                    for (int c = 0; c < 3; ++c) {
+                        const int z = c * N + k;
+                        S.B[z] = S.B[z] + S.A[z];
+                        S.C[z] = S.C[z] + S.B[z];
+                        S.XE[z] = h2n * S.C[z] + h2by2 * S.A0[z] + tmp0 * V0[z] + X0[z];
+                    }
+            }
+            massive_call(A, S.XE, V0, S.A, A.table + (size_t)(row++) * stride, st);
+            double* Dn = S.D + (size_t)(n - 1) * 6 * N;
+            for (int k = 1 + tid; k < N; k += nt)
+                for (int c = 0; c < 3; ++c) {
+                    const int z = c * N + k;
+                    Dn[z] = S.XE[z];
+                    Dn[3 * N + z] = h * S.B[z] + hby2 * S.A[z] + V0[z];
+                }
+        }
+        // Neville update (mercury6_2.for:3352-3366), each thread its own bodies
+        for (int j = n - 1; j >= 1; --j) {
+            const double tmp0 = 1.0 / (level_h2<VARIANT>(A.h0, j) - h2n);
+            const double tmp1 = tmp0 * level_h2<VARIANT>(A.h0, j + 1);
+            const double tmp2 = tmp0 * h2n;
+            double* Dj = S.D + (size_t)(j - 1) * 6 * N;
+            const double* Dj1 = S.D + (size_t)j * 6 * N;
+            for (int k = 1 + tid; k < N; k += nt)
+                for (int c = 0; c < 6; ++c) Dj[c * N + k] = tmp1 * Dj1[c * N + k] - tmp2 * Dj[c * N + k];
+        }
+        if (n > 3) {
+            double emax = 0.0;
+            int bad = 0;
+            double* cand = A.bcand + (size_t)(n - 4) * 6 * N;
+            for (int k = 1 + tid; k < N; k += nt) {
+                double q[6];
+                for (int c = 0; c < 6; ++c) q[c] = S.D[c * N + k];
+                double e;
+                if (body_error(q, S.XS[k], S.VS[k], e)) emax = fmax(emax, e);
+                else bad = 1;
+                for (int c = 0; c < 6; ++c) {
+                    double s = q[c];
+                    for (int j = 2; j <= n; ++j) s = s + S.D[(size_t)(j - 1) * 6 * N + c * N + k];
+                    cand[c * N + k] = s;
+                }
+            }
+            for (int o = 16; o; o >>= 1) {
+                emax = fmax(emax, __shfl_xor_sync(FULLMASK, emax, o));
+                bad |= __shfl_xor_sync(FULLMASK, bad, o);
+            }
+            if ((tid & 31) == 0) { wmax[tid >> 5] = emax; wbad[tid >> 5] = bad; }
+            __syncthreads();
+            if (tid == 0) {
+                double m = 0.0;
+                int b = 0;
+                for (int w = 0; w < (nt + 31) / 32; ++w) { m = fmax(m, wmax[w]); b |= wbad[w]; }
+                level_error(m, !b, &A.errs[n]);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------ particles
+// Each thread advances one particle slot through every level; its
+// extrapolation table lives in shared-memory columns D(j, c).
+template <int VARIANT> __global__ void __launch_bounds__(128) bs_particle_kernel(BsArgs A) {
+    extern __shared__ double dcol[];
+    const int L = bs_levels(VARIANT), nb = A.f.nbig - 1, stride = force_row(nb), S = A.npcap;
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool ok = p < A.np;
+    const int T = blockDim.x;
+    auto D = [&](int j, int c) -> double& { return dcol[((j - 1) * 6 + c) * T + threadIdx.x]; };
+    double3 x0 = make_double3(0.0, 0.0, 0.0), v0 = x0, a0 = x0;
+    double xscal = 0.0, vscal = 0.0, mj = 0.0, g5[5] = {0, 0, 0, 0, 0};
+    if (ok) {
+        x0 = make_double3(A.px[p], A.px[S + p], A.px[2 * S + p]);
+        v0 = make_double3(A.px[3 * S + p], A.px[4 * S + p], A.px[5 * S + p]);
+        mj = A.pconst[p];
+        for (int c = 0; c < 5; ++c) g5[c] = A.pconst[(3 + c) * (size_t)S + p];
+        const double tmp1 = x0.x * x0.x + x0.y * x0.y + x0.z * x0.z;
+        const double tmp2 = v0.x * v0.x + v0.y * v0.y + v0.z * v0.z;
+        xscal = 1.0 / fmax(tmp1, 1e-300);
+        vscal = 1.0 / fmax(tmp2, 1e-300);
+        a0 = particle_allforce(x0, v0, A.table, nb, A.f, mj, g5, &A.lvst[0]);
+    }
+    int row = 1;
+#pragma unroll 1
+    for (int n = 1; n <= L; ++n) {
+        DeviceStatus* st = &A.lvst[n];
+        const double h = level_h<VARIANT>(A.h0, n);
+        const double h2n = level_h2<VARIANT>(A.h0, n);
+        auto call = [&](const double3 x, const double3 v) {
+            const double* Tr = A.table + (size_t)(row++) * stride;
+            return particle_allforce(x, v, Tr, nb, A.f, mj, g5, st);
+        };
+        if (ok) {
+            if (VARIANT == 1) {
+                const double hx2 = h * 2.0;
+                double3 x = make_double3(x0.x + h * v0.x, x0.y + h * v0.y, x0.z + h * v0.z);
+                double3 v = make_double3(v0.x + h * a0.x, v0.y + h * a0.y, v0.z + h * a0.z);
+                double3 a = call(x, v);
+                double3 xe = make_double3(x0.x + hx2 * v.x, x0.y + hx2 * v.y, x0.z + hx2 * v.z);
+                double3 ve = make_double3(v0.x + hx2 * a.x, v0.y + hx2 * a.y, v0.z + hx2 * a.z);
+#pragma unroll 1
+                for (int j = 2; j <= n; ++j) {
+                    a = call(xe, ve);
+                    x = make_double3(x.x + hx2 * ve.x, x.y + hx2 * ve.y, x.z + hx2 * ve.z);
+                    v = make_double3(v.x + hx2 * a.x, v.y + hx2 * a.y, v.z + hx2 * a.z);
+                    a = call(x, v);
+                    xe = make_double3(xe.x + hx2 * v.x, xe.y + hx2 * v.y, xe.z + hx2 * v.z);
+                    ve = make_double3(ve.x + hx2 * a.x, ve.y + hx2 * a.y, ve.z + hx2 * a.z);
+                }
+                a = call(xe, ve);
+                D(n, 0) = 0.5 * (xe.x + x.x + h * ve.x);
+                D(n, 1) = 0.5 * (xe.y + x.y + h * ve.y);
+                D(n, 2) = 0.5 * (xe.z + x.z + h * ve.z);
+                D(n, 3) = 0.5 * (ve.x + v.x + h * a.x);
+                D(n, 4) = 0.5 * (ve.y + v.y + h * a.y);
+                D(n, 5) = 0.5 * (ve.z + v.z + h * a.z);
+            } else {
+                const double hby2 = 0.5 * h, h2by2 = 0.5 * h2n;
+                double3 b = make_double3(0.5 * a0.x, 0.5 * a0.y, 0.5 * a0.z);
+                double3 c = make_double3(0.0, 0.0, 0.0);
+                double3 xe = make_double3(h2by2 * a0.x + h * v0.x + x0.x, h2by2 * a0.y + h * v0.y + x0.y,
+                                          h2by2 * a0.z + h * v0.z + x0.z);
+#pragma unroll 1
+                for (int j = 2; j <= n; ++j) {
+                    const double3 a = call(xe, v0);
+                    const double tmp0 = h * double(j);
+                    b = make_double3(b.x + a.x, b.y + a.y, b.z + a.z);
+                    c = make_double3(c.x + b.x, c.y + b.y, c.z + b.z);
+                    xe = make_double3(h2n * c.x + h2by2 * a0.x + tmp0 * v0.x + x0.x,
+                                      h2n * c.y + h2by2 * a0.y + tmp0 * v0.y + x0.y,
+                                      h2n * c.z + h2by2 * a0.z + tmp0 * v0.z + x0.z);
+                }
+                const double3 a = call(xe, v0);
+                D(n, 0) = xe.x;
+                D(n, 1) = xe.y;
+                D(n, 2) = xe.z;
+                D(n, 3) = h * b.x + hby2 * a.x + v0.x;
+                D(n, 4) = h * b.y + hby2 * a.y + v0.y;
+                D(n, 5) = h * b.z + hby2 * a.z + v0.z;
+            }
+#pragma unroll 1
+            for (int j = n - 1; j >= 1; --j) {
+                const double tmp0 = 1.0 / (level_h2<VARIANT>(A.h0, j) - h2n);
+                const double tmp1 = tmp0 * level_h2<VARIANT>(A.h0, j + 1);
+                const double tmp2 = tmp0 * h2n;
+                for (int c = 0; c < 6; ++c) D(j, c) = tmp1 * D(j + 1, c) - tmp2 * D(j, c);
+            }
+        } else {
+            row += bs_level_forces(VARIANT, n);
+        }
+        if (n > 3) {
+            double emax = 0.0;
+            int bad = 0;
+            if (ok) {
+                double q[6];
+                for (int c = 0; c < 6; ++c) q[c] = D(1, c);
+                double e;
+                if (body_error(q, xscal, vscal, e)) emax = e;
+                else bad = 1;
+                double* cand = A.pcand + (size_t)(n - 4) * 6 * S;
+                for (int c = 0; c < 6; ++c) {
+                    double s = q[c];
+                    for (int j = 2; j <= n; ++j) s = s + D(j, c);
+                    cand[(size_t)c * S + p] = s;
+                }
+            }
+            for (int o = 16; o; o >>= 1) {
+                emax = fmax(emax, __shfl_xor_sync(FULLMASK, emax, o));
+                bad |= __shfl_xor_sync(FULLMASK, bad, o);
+            }
+            if ((threadIdx.x & 31) == 0 && (emax > 0.0 || bad)) level_error(emax, !bad, &A.errs[n]);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(128) bs_commit_kernel(BsCommitArgs A) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    const int N = A.nsplit, S = A.npcap;
+    if (q < N) {
+        if (q == 0) {
+            for (int c = 0; c < 9; ++c) A.bx_out[c * N] = A.bx[c * N];
+            return;
+        }
+        const double* cand = A.bcand + (size_t)A.cand * 6 * N;
+        for (int c = 0; c < 6; ++c) A.bx_out[c * N + q] = cand[c * N + q];
+        for (int c = 6; c < 9; ++c) A.bx_out[c * N + q] = 0.0;
+        return;
+    }
+    const int p = q - N;
+    if (p >= A.np) return;
+    const double* cand = A.pcand + (size_t)A.cand * 6 * S;
+    for (int c = 0; c < 6; ++c) A.px_out[(size_t)c * S + p] = cand[(size_t)c * S + p];
+    for (int c = 6; c < 9; ++c) A.px_out[(size_t)c * S + p] = 0.0;
+}
+
+template <int VARIANT> void launch_variant(const BsArgs& a, cudaStream_t s) {
+    bs_massive_kernel<VARIANT><<<1, 256, 0, s>>>(a);
+    if (a.np <= 0) return;
+    const int threads = 128;
+    const size_t smem = sizeof(double) * 6 * bs_levels(VARIANT) * threads;
+    if (smem > 48 * 1024)
+        cudaFuncSetAttribute(bs_particle_kernel<VARIANT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    bs_particle_kernel<VARIANT><<<(a.np + threads - 1) / threads, threads, smem, s>>>(a);
+}
+
+}  // namespace
+
+void launch_bs_sequence(const BsArgs& a, cudaStream_t s) {
+    if (a.variant == 1) launch_variant<1>(a, s);
+    else launch_variant<2>(a, s);
+}
+
+void launch_bs_commit(const BsCommitArgs& a, cudaStream_t s) {
+    const int total = a.nsplit + a.np;
+    bs_commit_kernel<<<(total + 127) / 128, 128, 0, s>>>(a);
+}
+
+}  // namespace mb200

@@ -1,0 +1,61 @@
+// Bulirsch-Stoer steps on the device: mdt_bs1 (modified midpoint, 8 levels,
+// mercury6_2.for:3227-3404) and mdt_bs2 (Stoermer form with the start
+// velocities, 12 levels, mercury6_2.for:3428-3596), with force = mfo_all.
+//
+// The Fortran stops at the first level n > 3 whose global error passes; that
+// decision needs the maximum over every body. One launch pair computes every
+// level instead: the massive-set CTA writes a force table row per force call
+// and the particle kernel runs all levels per particle with its extrapolation
+// table in shared memory, each reducing a per-level error maximum and storing
+// the level's extrapolated state. The host then takes the first passing level
+// (or halves the step) and a commit pass copies that level's state.
+#pragma once
+#include "allforce.cuh"
+#include "common.cuh"
+
+namespace mb200 {
+
+__host__ __device__ constexpr int bs_levels(int variant) { return variant == 1 ? 8 : 12; }
+// Force calls of level n (1-based): 2n for mdt_bs1, n for mdt_bs2.
+__host__ __device__ constexpr int bs_level_forces(int variant, int n) { return variant == 1 ? 2 * n : n; }
+// Table rows: the start-of-step force, then every force call of every level.
+__host__ __device__ constexpr int bs_rows(int variant) { return variant == 1 ? 1 + 72 : 1 + 78; }
+// Candidate states kept per body: levels 4 .. bs_levels.
+__host__ __device__ constexpr int bs_candidates(int variant) { return bs_levels(variant) - 3; }
+// Massive-set scratch rows ([rows][nsplit] doubles): eight 3-vectors, the two
+// error scales and the extrapolation table.
+__host__ __device__ constexpr int bs_massive_scratch(int variant) { return 26 + 6 * bs_levels(variant); }
+
+struct BsArgs {
+    ForceCfg f;
+    int variant;                 // 1: mdt_bs1, 2: mdt_bs2
+    int np, npcap;
+    double h0;                   // trial step
+    const double* bx;            // [9][nsplit] start-of-step state of the massive set
+    const double* mbig;
+    const double* ngfbig;        // [nsplit][5]
+    double* bscr;                // [bs_massive_scratch][nsplit]
+    const double* px;            // [9][npcap] start-of-step particle state
+    const double* pconst;        // [8][npcap]
+    double* table;               // [bs_rows][force_row(nb)]
+    double* bcand;               // [bs_candidates * 6][nsplit]
+    double* pcand;               // [bs_candidates * 6][npcap]
+    unsigned long long* errs;    // [13] max error of level n (bit pattern of a non-negative double; +inf
+                                 // when an extrapolated value is not finite)
+    DeviceStatus* lvst;          // [13] force faults of level n (0: the start-of-step force)
+};
+
+struct BsCommitArgs {
+    int nsplit, np, npcap;
+    int cand;                    // candidate index (accepted level - 4)
+    const double* bcand;
+    const double* pcand;
+    const double* bx;            // start-of-step state (central body row copied)
+    double* bx_out;              // [9][nsplit]
+    double* px_out;              // [9][npcap]
+};
+
+void launch_bs_sequence(const BsArgs& a, cudaStream_t s);
+void launch_bs_commit(const BsCommitArgs& a, cudaStream_t s);
+
+}  // namespace mb200

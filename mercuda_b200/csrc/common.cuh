@@ -23,8 +23,12 @@ constexpr double C_LIGHT = 299792458.0 * 86400.0 / 1.495978707e11;
 // Event kinds of the reference ABI (mercury_cuda.h:7-11, mercury_gpu.f90:215-246).
 constexpr int EV_CLOSE = 1, EV_NEAR = 2, EV_HIT = 4, EV_CENTRAL = 8;
 
-// Device-side status word written by kernels (never a trap): bit 0 non-finite
-// force, bit 1 undefined non-gravitational direction, bit 2 bound exceeded.
+// Fault bits of the device status word (kernels never trap): a non-finite
+// acceleration, an undefined non-gravitational direction (mfo_ngf's fail()),
+// coincident bodies (mfo_grav's fail() on a zero separation).
+constexpr int FAULT_NONFINITE = 1, FAULT_NGF = 2, FAULT_COINCIDENT = 4;
+
+// Device-side status word written by kernels.
 struct DeviceStatus {
     int fault;
     int events;        // pair/central events claimed (may exceed capacity)

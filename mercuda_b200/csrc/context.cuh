@@ -79,6 +79,13 @@ struct Context {
     // [3][npcap]); screen boxes of the adaptive integrators ([nbig-1][4])
     DBuf<double> ra_bb, ra_be, ra_bg, ra_bpx, ra_pb, ra_pe, ftab, force_out, boxes;
     DBuf<unsigned long long> ra_max;
+    // output corrector scratch: Big [9][nbig], particles [6][npcap]
+    DBuf<double> corr_big, corr_part;
+    // Bulirsch-Stoer: massive-set scratch, per-level candidate states, per-level
+    // error maxima and force-fault words
+    DBuf<double> bs_scr, bs_bcand, bs_pcand;
+    DBuf<unsigned long long> bs_errs;
+    DBuf<DeviceStatus> bs_lvst;
     // events
     DBuf<MercuryEvent> events;
     DBuf<int> event_step;
@@ -130,11 +137,14 @@ struct Context {
     void release_all() {
         DBuf<double>* bufs[] = {&mbig, &rcebig, &rphysbig, &ngfbig, &bigstate[0], &bigstate[1], &pstate[0],
                                 &pstate[1], &pconst[0], &pconst[1], &tab, &detail, &transfer, &snapshot, &snap_const,
-                                &ra_bb, &ra_be, &ra_bg, &ra_bpx, &ra_pb, &ra_pe, &ftab, &force_out, &boxes};
+                                &ra_bb, &ra_be, &ra_bg, &ra_bpx, &ra_pb, &ra_pe, &ftab, &force_out, &boxes, &corr_big, &corr_part,
+                                &bs_scr, &bs_bcand, &bs_pcand};
         for (auto* b : bufs) b->release();
         DBuf<int>* ibufs[] = {&perm[0], &perm[1], &inv, &order_bucket, &order_hist, &snap_perm};
         for (auto* b : ibufs) b->release();
         ra_max.release();
+        bs_errs.release();
+        bs_lvst.release();
         kc = 0;
         events.release();
         event_step.release();

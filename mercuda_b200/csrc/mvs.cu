@@ -234,11 +234,25 @@ __device__ void write_force_table(const MvsBigArgs& A, const BigSmem& S, double*
     }
 }
 
-__global__ void __launch_bounds__(128) mvs_big_kernel(MvsBigArgs A) {
-    extern __shared__ double smem[];
-    const int nbig = A.nbig, N = nbig, nb = nbig - 1, tid = threadIdx.x, nt = blockDim.x;
-    const int stride = tab_stride(nb);
-    BigSmem S;
+// The Big bodies' drift of mdt_mvs: h2j, Kepler drift of each Jacobi body
+// with gm_j, j2h (mercury6_2.for:4031-4046). All threads.
+__device__ void big_drift(const MvsBigArgs& A, BigSmem& S, double h) {
+    const int nbig = A.nbig, N = nbig, tid = threadIdx.x, nt = blockDim.x;
+    if (tid == 0) big_h2j(nbig, A.m, S.X, S.V, S.XJ, S.VJ);
+    __syncthreads();
+    for (int k = 1 + tid; k < nbig; k += nt) {
+        double3 p = ld3(S.XJ, N, k), w = ld3(S.VJ, N, k);
+        drift_one(S.GM[k], p, w, h);
+        st3(S.XJ, N, k, p);
+        st3(S.VJ, N, k, w);
+    }
+    __syncthreads();
+    if (tid == 0) big_j2h(nbig, A.m, S.XJ, S.VJ, S.X, S.V);
+    __syncthreads();
+}
+
+__device__ void big_load(const MvsBigArgs& A, BigSmem& S, double* smem) {
+    const int nbig = A.nbig, N = nbig, tid = threadIdx.x, nt = blockDim.x;
     S.carve(smem, nbig);
     for (int k = tid; k < nbig; k += nt)
         for (int c = 0; c < 3; ++c) {
@@ -255,6 +269,14 @@ __global__ void __launch_bounds__(128) mvs_big_kernel(MvsBigArgs A) {
         }
     }
     __syncthreads();
+}
+
+__global__ void __launch_bounds__(128) mvs_big_kernel(MvsBigArgs A) {
+    extern __shared__ double smem[];
+    const int nbig = A.nbig, N = nbig, nb = nbig - 1, tid = threadIdx.x, nt = blockDim.x;
+    const int stride = tab_stride(nb);
+    BigSmem S;
+    big_load(A, S, smem);
     if (A.reset) {
         if (tid == 0) big_h2j(nbig, A.m, S.X, S.V, S.XJ, S.VJ);
         __syncthreads();
@@ -274,17 +296,7 @@ __global__ void __launch_bounds__(128) mvs_big_kernel(MvsBigArgs A) {
                 S.V0[z] = S.V[z];
             }
         __syncthreads();
-        if (tid == 0) big_h2j(nbig, A.m, S.X, S.V, S.XJ, S.VJ);
-        __syncthreads();
-        for (int k = 1 + tid; k < nbig; k += nt) {
-            double3 p = ld3(S.XJ, N, k), w = ld3(S.VJ, N, k);
-            drift_one(S.GM[k], p, w, h);
-            st3(S.XJ, N, k, p);
-            st3(S.VJ, N, k, w);
-        }
-        __syncthreads();
-        if (tid == 0) big_j2h(nbig, A.m, S.XJ, S.VJ, S.X, S.V);
-        __syncthreads();
+        big_drift(A, S, h);
         double* row = A.tab + (size_t)(s + 1) * stride;
         double* det = A.detail + (size_t)s * nb * TAB_DETAIL;
         for (int k = 1 + tid; k < nbig; k += nt) {
@@ -417,11 +429,11 @@ struct Cols {
 };
 
 // mfo_mvs for one Small body (mercury6_2.for:5034-5060) plus mfo_ngf, i.e. the
-// total acceleration (angf + 0) + a of the kick; T is a staged force table.
-template <bool NGF, bool OBL>
-__device__ __forceinline__ double3 particle_force(const double3 x, const double3 v_ngf, const Cols& cols, int u,
-                                                  const double* T, int nb, const double* jcen, double mu,
-                                                  DeviceStatus* st) {
+// total acceleration (angf + 0) + a of the kick; T is a force table and g(c)
+// returns the body's c-th non-gravitational coefficient.
+template <bool NGF, bool OBL, class G>
+__device__ __forceinline__ double3 small_body_force(const double3 x, const double3 v_ngf, G g, const double* T,
+                                                    int nb, const double* jcen, double mu, DeviceStatus* st) {
     double3 a3 = make_double3(0.0, 0.0, 0.0);
 #pragma unroll kForceUnroll
     for (int b = 0; b < nb; ++b) {
@@ -443,16 +455,25 @@ __device__ __forceinline__ double3 particle_force(const double3 x, const double3
         a.z = a.z + (ao.z - T[5]);
     }
     if (NGF) {
-        double g[5];
-        for (int c = 0; c < 5; ++c) g[c] = cols.at(Cols::NGF + 5 * u + c);
+        double gc[5];
+        for (int c = 0; c < 5; ++c) gc[c] = g(c);
         double3 ng;
-        if (!nongrav_accel(x, v_ngf, g, ng)) raise_fault(st, 2);
+        if (!nongrav_accel(x, v_ngf, gc, ng)) raise_fault(st, 2);
         a.x = ng.x + 0.0 + a.x;
         a.y = ng.y + 0.0 + a.y;
         a.z = ng.z + 0.0 + a.z;
     }
     if (!isfinite(a.x) || !isfinite(a.y) || !isfinite(a.z)) raise_fault(st, 1);
     return a;
+}
+
+// small_body_force with the coefficients of pair member u in the columns.
+template <bool NGF, bool OBL>
+__device__ __forceinline__ double3 particle_force(const double3 x, const double3 v_ngf, const Cols& cols, int u,
+                                                  const double* T, int nb, const double* jcen, double mu,
+                                                  DeviceStatus* st) {
+    return small_body_force<NGF, OBL>(x, v_ngf, [&](int c) -> double { return cols.at(Cols::NGF + 5 * u + c); }, T,
+                                      nb, jcen, mu, st);
 }
 
 // One mdt_mvs step of one Small body (slot p, pair member u) against the staged
@@ -621,6 +642,75 @@ __global__ void __launch_bounds__(128, MB200_PARTICLE_MIN_BLOCKS) mvs_particle_k
     }
 }
 
+// ------------------------------------------------------------ output corrector
+// The Big bodies' part of the corrector (mercury6_2.for:2200-2222 in
+// mco_mvs2h, 2510-2532 in mco_h2mvs) from big.in into big.out, writing the
+// force table of each of the four kicks.
+__global__ void __launch_bounds__(128) mvs_corrector_big_kernel(MvsBigArgs A, CorrectorArgs K) {
+    extern __shared__ double smem[];
+    const int nbig = A.nbig, N = nbig, nb = nbig - 1, tid = threadIdx.x, nt = blockDim.x;
+    const int stride = tab_stride(nb);
+    BigSmem S;
+    big_load(A, S, smem);
+    auto kick = [&](double hk, bool subtract) {
+        for (int k = 1 + tid; k < nbig; k += nt)
+            for (int c = 0; c < 3; ++c) {
+                const int z = c * N + k;
+                const double term = hk * S.ACC[z];
+                S.V[z] = subtract ? S.V[z] - term : S.V[z] + term;
+            }
+        __syncthreads();
+    };
+    for (int k = 0; k < 2; ++k) {
+        big_drift(A, S, K.ha[k]);
+        big_force(A, S, S.V);
+        write_force_table(A, S, A.tab + (size_t)(2 * k) * stride);
+        kick(K.hb[k], K.forward != 0);
+        big_drift(A, S, -2.0 * K.ha[k]);
+        big_force(A, S, S.V);
+        write_force_table(A, S, A.tab + (size_t)(2 * k + 1) * stride);
+        kick(K.hb[k], K.forward == 0);
+        big_drift(A, S, K.ha[k]);
+    }
+    for (int k = tid; k < nbig; k += nt)
+        for (int c = 0; c < 3; ++c) {
+            A.out.x[c * N + k] = S.X[c * N + k];
+            A.out.v[c * N + k] = S.V[c * N + k];
+        }
+}
+
+// The Small bodies' part: heliocentric drifts with the central mass and the
+// mfo_mvs + mfo_ngf kicks against the Big-body tables; one thread per slot.
+template <bool NGF, bool OBL>
+__global__ void __launch_bounds__(128) mvs_corrector_particle_kernel(CorrectorArgs K) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x, S = K.npcap;
+    if (p >= K.np) return;
+    const int stride = tab_stride(K.nb);
+    double3 x = make_double3(K.xin[p], K.xin[S + p], K.xin[2 * S + p]);
+    double3 v = make_double3(K.xin[3 * S + p], K.xin[4 * S + p], K.xin[5 * S + p]);
+    auto g = [&](int c) -> double { return K.ngf[(size_t)c * S + p]; };
+    auto kick = [&](const double* T, double hk, bool subtract) {
+        const double3 a = small_body_force<NGF, OBL>(x, v, g, T, K.nb, K.jcen, K.mu, K.status);
+        v.x = subtract ? v.x - hk * a.x : v.x + hk * a.x;
+        v.y = subtract ? v.y - hk * a.y : v.y + hk * a.y;
+        v.z = subtract ? v.z - hk * a.z : v.z + hk * a.z;
+    };
+#pragma unroll 1
+    for (int k = 0; k < 2; ++k) {
+        drift_one(K.mu, x, v, K.ha[k]);
+        kick(K.tab + (size_t)(2 * k) * stride, K.hb[k], K.forward != 0);
+        drift_one(K.mu, x, v, -2.0 * K.ha[k]);
+        kick(K.tab + (size_t)(2 * k + 1) * stride, K.hb[k], K.forward == 0);
+        drift_one(K.mu, x, v, K.ha[k]);
+    }
+    K.xout[p] = x.x;
+    K.xout[S + p] = x.y;
+    K.xout[2 * S + p] = x.z;
+    K.xout[3 * S + p] = v.x;
+    K.xout[4 * S + p] = v.y;
+    K.xout[5 * S + p] = v.z;
+}
+
 // mce_stat's test for each encounter candidate of the last launch
 // (mercury6_2.for:1815-1908) and the record it produces.
 __global__ void __launch_bounds__(256) classify_kernel(ClassifyArgs A) {
@@ -681,6 +771,22 @@ int mvs_max_steps_per_launch(int nb) {
     if (k < 1) k = 1;
     if (k > 64) k = 64;
     return (int)k;
+}
+
+void launch_mvs_corrector(const MvsBigArgs& big, const CorrectorArgs& a, cudaStream_t s) {
+    const size_t smem = sizeof(double) * ((size_t)12 * 3 * big.nbig + big.nbig + 16);
+    if (smem > 48 * 1024)
+        cudaFuncSetAttribute(mvs_corrector_big_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    mvs_corrector_big_kernel<<<1, 128, smem, s>>>(big, a);
+    if (a.np <= 0) return;
+    const int grid = (a.np + 127) / 128;
+    if (a.ngf_on) {
+        if (a.obl) mvs_corrector_particle_kernel<true, true><<<grid, 128, 0, s>>>(a);
+        else mvs_corrector_particle_kernel<true, false><<<grid, 128, 0, s>>>(a);
+    } else {
+        if (a.obl) mvs_corrector_particle_kernel<false, true><<<grid, 128, 0, s>>>(a);
+        else mvs_corrector_particle_kernel<false, false><<<grid, 128, 0, s>>>(a);
+    }
 }
 
 void launch_classify(const ClassifyArgs& a, cudaStream_t s) {

@@ -84,6 +84,26 @@ struct MvsParticleArgs {
     DeviceStatus* status;
 };
 
+// Output corrector mco_mvs2h / mco_h2mvs (mercury6_2.for:2107-2227,
+// 2420-2535) of the whole state into scratch arrays: two stages of
+// drift(ha) kick(-+hb) drift(-2 ha) kick(+-hb) drift(ha), with the Big bodies'
+// four force tables written by the Big-body CTA for the particle kernel.
+struct CorrectorArgs {
+    int np, npcap, nb;
+    int ngf_on, obl;
+    int forward;          // mco_mvs2h (1) or mco_h2mvs (0)
+    double mu;
+    double ha[2], hb[2];
+    double jcen[3];
+    const double* xin;    // [9][npcap] particle state (x, v used)
+    double* xout;         // [6][npcap]
+    const double* ngf;    // [5][npcap]
+    const double* tab;    // [4][tab_stride(nb)] written by the Big-body CTA
+    DeviceStatus* status;
+};
+// big.in: current Big state, big.out: scratch, big.tab: 4 table rows.
+void launch_mvs_corrector(const MvsBigArgs& big, const CorrectorArgs& a, cudaStream_t s);
+
 // Finishes mce_stat's test for the candidates of the last particle launch and
 // writes the event records; detail is the base of the run's detail rows.
 struct ClassifyArgs {

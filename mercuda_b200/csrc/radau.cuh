@@ -3,26 +3,11 @@
 // adaptive integrators use (mce_stat/mce_cent on the states before and after
 // a step).
 #pragma once
+#include "allforce.cuh"
 #include "common.cuh"
 #include "mvs.cuh"
 
 namespace mb200 {
-
-// Force configuration shared by every kernel that evaluates mfo_all.
-struct ForceCfg {
-    int nbig;      // Big bodies incl. the central body
-    int nsplit;    // bodies [0, nsplit) are in the "big" arrays (Big + massive Small)
-    int ngflag;
-    int pn;
-    int obl;
-    double jcen[3];
-    double m0;
-};
-
-// Per-substep table row for the particle kernels, in doubles:
-// {sx, sy, sz, acen_x, acen_y, acen_z, pad, pad, [x, y, z, m] per Big body}.
-constexpr int FT_HEAD = 8;
-__host__ __device__ constexpr int force_row(int nb) { return FT_HEAD + 4 * nb; }
 
 struct Ra15Args {
     ForceCfg f;

@@ -77,9 +77,9 @@ def lib() -> C.CDLL:
         L.oracle_force.restype = I
         L.oracle_force_term.argtypes = [I, I, PD, PD, PD, PD, PD]
         L.oracle_force_term.restype = I
-        L.oracle_ra15_run.argtypes = [I, I, PD, PD, PD, PD, I, I, PD, PD, PD, D, D, PD, D, D, I, I,
+        L.oracle_hvar_run.argtypes = [I, I, I, PD, PD, PD, PD, I, I, PD, PD, PD, D, D, PD, D, D, I, I,
                                       C.POINTER(C.c_longlong)]
-        L.oracle_ra15_run.restype = C.c_void_p
+        L.oracle_hvar_run.restype = C.c_void_p
         _lib = L
     return _lib
 
@@ -215,21 +215,29 @@ def force_term(which, m, x, v, ngf):
     return a
 
 
-def ra15_run(sys, time0, tstop, h, tol, rcen=0.005, central=True, max_steps=1_000_000):
-    """mal_hvar-style RA15 loop on sys (in place). Returns (events, steps, h_next, nsteps, nforces)."""
+def hvar_run(sys, algorithm, time0, tstop, h, tol, rcen=0.005, central=True, max_steps=1_000_000):
+    """mal_hvar's loop with mdt_bs1 (2), mdt_bs2 (3) or mdt_ra15 (4) on sys (in place).
+
+    Returns (events, step of each event, h_next, steps, force calls, rejected)."""
     s = sys
     hh = D(h)
-    counters = (C.c_longlong * 2)()
-    handle = lib().oracle_ra15_run(s.n, s.nbig, _p(s.m), _p(s.x), _p(s.v), _p(s.ngf), s.ngflag, int(s.pn),
-                                   _p(s.jcen), _p(s.rce), _p(s.rphys), time0, tstop, C.byref(hh), tol, rcen,
-                                   int(central), int(max_steps), counters)
+    counters = (C.c_longlong * 3)()
+    handle = lib().oracle_hvar_run(int(algorithm), s.n, s.nbig, _p(s.m), _p(s.x), _p(s.v), _p(s.ngf), s.ngflag,
+                                   int(s.pn), _p(s.jcen), _p(s.rce), _p(s.rphys), time0, tstop, C.byref(hh), tol,
+                                   rcen, int(central), int(max_steps), counters)
     try:
         if lib().oracle_run_status(handle):
-            raise RuntimeError("oracle RA15 run failed")
+            raise RuntimeError("oracle integration failed")
         count = lib().oracle_run_event_count(handle)
         events = np.zeros(count, dtype=EVENT_DTYPE)
         steps = np.zeros(count, dtype=np.int32)
         lib().oracle_run_events(handle, events.ctypes.data_as(C.c_void_p), steps.ctypes.data_as(C.c_void_p))
     finally:
         lib().oracle_run_free(handle)
-    return events, steps, hh.value, counters[0], counters[1]
+    return events, steps, hh.value, counters[0], counters[1], counters[2]
+
+
+def ra15_run(sys, time0, tstop, h, tol, rcen=0.005, central=True, max_steps=1_000_000):
+    """mal_hvar-style RA15 loop on sys (in place). Returns (events, steps, h_next, nsteps, nforces)."""
+    ev, st, hn, n, f, _ = hvar_run(sys, 4, time0, tstop, h, tol, rcen, central, max_steps)
+    return ev, st, hn, n, f

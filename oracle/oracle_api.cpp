@@ -10,6 +10,7 @@
 
 #include "oracle_mvs.hpp"
 #include "oracle_ra15.hpp"
+#include "oracle_bs.hpp"
 
 namespace oracle {
 thread_local Tally tally;
@@ -271,7 +272,11 @@ int oracle_force(int n, int nbig, const double* m, const double* x, const double
 // (x0,v0 = the state before the step) and, if central != 0, mce_cent screen
 // for events. h is the initial trial step (in/out). Returns the number of
 // steps, or -1 on failure; events are kept in the run handle.
-OracleRun* oracle_ra15_run(int n, int nbig, const double* m, double* x, double* v, const double* ngf,
+// mal_hvar's step loop (mercury6_2.for:423-470) with algor 2 (mdt_bs1),
+// 3 (mdt_bs2) or 4 (mdt_ra15): steps clipped to tstop (a clipped RA15 step
+// restarts the sequence), then mce_stat and mce_cent on the step. *h is the
+// trial step in, the next one out; counters = {steps, force calls, rejected}.
+OracleRun* oracle_hvar_run(int algor, int n, int nbig, const double* m, double* x, double* v, const double* ngf,
                            int ngflag, int pn, const double* jcen, const double* rce, const double* rphys,
                            double time0, double tstop, double* h, double tol, double rcen, int central,
                            int max_steps, long long* counters) {
@@ -280,19 +285,26 @@ OracleRun* oracle_ra15_run(int n, int nbig, const double* m, double* x, double* 
     st.size(n);
     std::vector<double> x0(3 * n), v0(3 * n);
     double time = time0;
-    long long forces = 0, steps = 0;
+    long long forces = 0, steps = 0, rejected = 0;
     std::vector<Event> events;
     while (steps < max_steps) {
         if (std::fabs(tstop - time) <= 0.0) break;
         double target = tstop;
         double step = std::copysign(std::min(std::fabs(target - time), std::fabs(*h)), target - time);
         if (!std::isfinite(step) || time + step == time) break;
-        if (step != *h && st.dtflag != 0) st.dtflag = 1;
+        if (algor == 4 && step != *h && st.dtflag != 0) st.dtflag = 1;
         *h = step;
         std::copy(x, x + 3 * n, x0.begin());
         std::copy(v, v + 3 * n, v0.begin());
         double hdid = 0.0;
-        if (oracle::mdt_ra15(time, *h, hdid, tol, jcen, n, nbig, m, x, v, ngf, ngflag, pn, st, &forces)) {
+        int rc;
+        if (algor == 2)
+            rc = oracle::mdt_bs1(time, *h, hdid, tol, jcen, n, nbig, m, x, v, ngf, ngflag, pn, &forces, &rejected);
+        else if (algor == 3)
+            rc = oracle::mdt_bs2(time, *h, hdid, tol, jcen, n, nbig, m, x, v, ngf, ngflag, pn, &forces, &rejected);
+        else
+            rc = oracle::mdt_ra15(time, *h, hdid, tol, jcen, n, nbig, m, x, v, ngf, ngflag, pn, st, &forces);
+        if (rc) {
             run->status = 1;
             break;
         }
@@ -307,6 +319,7 @@ OracleRun* oracle_ra15_run(int n, int nbig, const double* m, double* x, double* 
     if (counters) {
         counters[0] = steps;
         counters[1] = forces;
+        counters[2] = rejected;
     }
     return run;
 }
