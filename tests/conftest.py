@@ -5,8 +5,9 @@ from pathlib import Path
 import pytest
 
 ROOT = Path(__file__).resolve().parents[1]
-if str(ROOT) not in sys.path:
-    sys.path.insert(0, str(ROOT))
+for path in (ROOT, ROOT / "tests"):  # the package, and the shared case modules beside the tests
+    if str(path) not in sys.path:
+        sys.path.insert(0, str(path))
 
 
 def pytest_configure(config):
