@@ -9,10 +9,17 @@ A bench "step" is one MVS step (kick, Kepler drift, mce_stat/mce_cent screen,
 kick) of every particle, events included.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                  [--workload mvs|radau|bs|bs2]
 
 --impl reference times the reference's CPU algorithm for this path (the C++
 restatement of mercury6_2.for in oracle/, all host cores) on the same
 workload; under torchrun only rank 0 runs it.
+
+--workload radau|bs|bs2 measures the adaptive integrators instead (mdt_ra15,
+mdt_bs1, mdt_bs2 through the drop-in step/events calls, as mal_hvar drives
+them) on the 100,000-particle system of the same generator with 1PN,
+radiation pressure (beta U[0.01,0.3]) and Yarkovsky (yar log-U[1e-15,1e-13],
+random sign), tol 1e-12; a step is one accepted integrator step.
 """
 from __future__ import annotations
 
@@ -63,7 +70,11 @@ def parse_args():
     p.add_argument("--threads", type=int, default=0)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    return p.parse_args()
+    p.add_argument("--workload", default="mvs", choices=["mvs", "radau", "bs", "bs2"])
+    args = p.parse_args()
+    if args.workload != "mvs" and args.particles == 1_000_000:
+        args.particles = 100_000
+    return args
 
 
 def workload(particles: int, seed: int):
@@ -153,6 +164,125 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+ADAPTIVE = {"radau": ("RADAU", 4), "bs": ("BS", 2), "bs2": ("BS2", 3)}
+ADAPTIVE_TOL = 1e-12
+ADAPTIVE_H0 = 2.0
+
+
+def adaptive_workload(particles: int, seed: int):
+    from mercuda_b200.system import make_system
+    sys_ = make_system(seed=seed, n_particles=particles, near_fraction=0.0, h=H)
+    rng = np.random.default_rng(seed + 1000)
+    npart = sys_.n - sys_.nbig
+    sys_.ngf[sys_.nbig:, 3] = rng.uniform(0.01, 0.3, npart)
+    sys_.ngf[sys_.nbig:, 4] = np.exp(rng.uniform(np.log(1e-15), np.log(1e-13), npart)) * rng.choice([-1, 1], npart)
+    sys_.pn = 1
+    return sys_
+
+
+def adaptive_cpu(name: str, particles: int, steps: int, seed: int):
+    """The oracle's mal_hvar loop (single-threaded, as the Fortran) on a sample."""
+    from oracle import oracle as O
+    sysc = adaptive_workload(particles, seed)
+    t0 = time.perf_counter()
+    _, _, _, done, _, _ = O.hvar_run(sysc, ADAPTIVE[name][1], 0.0, 1e9, ADAPTIVE_H0, ADAPTIVE_TOL, RCEN,
+                                     max_steps=steps)
+    dt = time.perf_counter() - t0
+    return particles * done / dt, done, dt
+
+
+def run_adaptive(args, rank, world, dist):
+    name, alg = ADAPTIVE[args.workload]
+    metric = f"{name} particle-steps/s"
+    workload_text = (f"{name}, {args.particles} massless particles + 8 planets, 1PN, PR beta U[0.01,0.3], "
+                     "yar log-U[1e-15,1e-13] random sign, tol 1e-12, encounter + central screens every step")
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        particles = min(args.particles, 20_000)
+        value, done, dt = adaptive_cpu(args.workload, particles, args.steps, args.seed)
+        sample = f"{particles} particles of the same generator x {done} accepted steps ({dt:.1f} s, 1 thread)"
+        line = {"impl": "reference", "metric": metric, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+                "steps": done, "warmup": 0, "ms_per_step": dt * 1e3 / max(1, done), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": workload_text, "particles": particles},
+                "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample},
+                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+    import torch
+    from mercuda_b200.backend import Backend
+
+    b = Backend(name)
+    b.configure()
+    sysw = adaptive_workload(args.particles, args.seed + rank)
+    b.upload(sysw)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def run(time0, h, nsteps):
+        t, dtflag, nev = time0, 0, 0
+        for _ in range(nsteps):
+            hdid, h = b.step(t, h, ADAPTIVE_TOL, dtflag)
+            dtflag = 2
+            t = t + hdid
+            nev += len(b.events(t, hdid, RCEN))
+        return t, h, nev
+
+    t, h, _ = run(0.0, ADAPTIVE_H0, args.warmup)
+    b.dropin_time(reset=True)
+    barrier()
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clocks:
+        t, h, nev = run(t, h, args.steps)
+    barrier()
+    ms, launches = b.dropin_time(reset=True)
+    if dist:
+        tt = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    value = world * args.particles * args.steps / (ms * 1e-3)
+    e2e = None
+    if not args.no_e2e:
+        fresh = adaptive_workload(args.particles, args.seed + rank)
+        barrier()
+        t0 = time.perf_counter()
+        b.upload(fresh)
+        run(0.0, ADAPTIVE_H0, args.steps)
+        x, v = b.download()
+        barrier()
+        e2e_s = time.perf_counter() - t0
+        if dist:
+            tt = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            e2e_s = float(tt.item())
+        h2d = fresh.n * (3 + 3 + 1 + 1 + 1 + 5) * 8
+        e2e = {"value": world * args.particles * args.steps / e2e_s, "unit": UNIT,
+               "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": fresh.n * 48 / args.steps,
+               "note": "wall clock around upload, the drop-in step + events calls of every step, download"}
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        particles = min(args.particles, 20_000)
+        v_cpu, done, dt = adaptive_cpu(args.workload, particles, 40, args.seed)
+        cpu = {"value": v_cpu, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": f"{particles} particles of the same generator x {done} accepted steps ({dt:.1f} s)"}
+    if rank == 0:
+        line = {"metric": metric, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": workload_text, "particles_per_gpu": args.particles, "seed": args.seed,
+                           "h_last": h, "t_end_days": t,
+                           "l2": "per step the state, B/E (RA15) or candidates (BS) exceed 126 MB only above "
+                                 "~300K particles; measured as is"},
+                "clocks": clocks.summary(), "gpu_launches": launches, "events": nev, "e2e": e2e,
+                "cpu_baseline": cpu}
+        print(json.dumps(line), flush=True)
+    b.free()
+
+
 def main():
     args = parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -166,6 +296,14 @@ def main():
         dist = dist_mod
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    if args.workload != "mvs":
+        if args.impl != "reference":
+            import torch
+            torch.cuda.set_device(local)
+        run_adaptive(args, rank, world, dist)
+        if dist:
+            dist.destroy_process_group()
+        return
     if args.impl == "reference":
         run_reference(args, rank)
         if dist:

@@ -45,7 +45,8 @@ DROP_IN_SYMBOLS = [
     "mercury_cuda_free",
 ]
 EXTENSION_SYMBOLS = ["mercury_b200_mvs_advance", "mercury_b200_events", "mercury_b200_timing",
-                     "mercury_b200_set_launch", "mercury_b200_fp64_peak", "mercury_b200_mvs_step_noalloc"]
+                     "mercury_b200_set_launch", "mercury_b200_fp64_peak", "mercury_b200_mvs_step_noalloc",
+                     "mercury_b200_dropin_time"]
 
 
 class BackendError(RuntimeError):
@@ -86,6 +87,7 @@ def load_library(path: Path | str | None = None) -> C.CDLL:
     L.mercury_b200_timing.argtypes = [PD, PD, PI, PI]
     L.mercury_b200_set_launch.argtypes = [I, I]
     L.mercury_b200_fp64_peak.argtypes = [PD, PD]
+    L.mercury_b200_dropin_time.argtypes = [PD, PI64, I]
     VP = C.c_void_p
     L.mercury_b200_mvs_step_noalloc.argtypes = [I, I, VP, VP, VP, VP, VP, VP, VP, VP, VP, I, D, D, I, VP, I,
                                                 PI, VP]
@@ -226,6 +228,12 @@ class Backend:
         self.lib.mercury_b200_timing(C.byref(a), C.byref(k), C.byref(n), C.byref(L))
         return {"advance_ms": a.value, "particle_kernel_ms": k.value, "particle_launches": n.value,
                 "kernel_launches": L.value}
+
+    def dropin_time(self, reset: bool = False):
+        """(device ms, kernels launched) of the drop-in step/events calls since the last reset."""
+        ms, n = D(0.0), C.c_int64(0)
+        self.lib.mercury_b200_dropin_time(C.byref(ms), C.byref(n), int(reset))
+        return ms.value, n.value
 
     def fp64_peak(self):
         tf, ms = D(0.0), D(0.0)

@@ -111,6 +111,19 @@ int reorder_slots(int src, double h, cudaStream_t st);
 
 bool is_mvs(int alg) { return alg == 1 || alg == 9; }
 
+// Adds the device time of one drop-in call (CUDA events on the library
+// stream around it) to the context's total.
+struct DropinTimer {
+    DropinTimer() { check(cudaEventRecord(ctx().d0, ctx().stream), "event"); }
+    ~DropinTimer() {
+        Context& c = ctx();
+        float ms = 0.0f;
+        if (cudaEventRecord(c.d1, c.stream) == cudaSuccess && cudaEventSynchronize(c.d1) == cudaSuccess &&
+            cudaEventElapsedTime(&ms, c.d0, c.d1) == cudaSuccess)
+            c.dropin_ms += ms;
+    }
+};
+
 void require_system() {
     if (ctx().n <= 0) throw std::runtime_error("no system uploaded");
 }
@@ -252,6 +265,7 @@ void mvs_step_once(double h) {
         const int in = c.cur, out = 1 - c.cur;
         const int reset = c.reset ? 1 : 0;
         launch_mvs_big(big_args(in, out, 1, reset, 0, 0, h, 0.0, c.tab.p, c.detail.p), c.stream);
+        c.dropin_launches += 1 + (c.np > 0 ? 1 + (c.nbig > 1 ? 1 : 0) : 0);
         if (c.np > 0)
             particles_and_events(particle_args(in, out, 1, reset, 0, 0, h, 0.0, c.tab.p, c.detail.p), c.stream);
         check(cudaGetLastError(), "launch");
@@ -321,6 +335,7 @@ void ra15_step_once(double time, double* h, double* hdid, double tol, int64_t* r
         a.maxb7 = c.ra_max.p;
         a.status = c.status.p;
         launch_ra15_sequence(a, c.stream);
+        c.dropin_launches += 1 + (c.np > 0 ? 1 : 0);
         check(cudaGetLastError(), "launch");
         unsigned long long bits = 0;
         check(cudaMemcpyAsync(&bits, c.ra_max.p, sizeof(bits), cudaMemcpyDeviceToHost, c.stream), "status");
@@ -353,6 +368,7 @@ void ra15_step_once(double time, double* h, double* hdid, double tol, int64_t* r
         k.pb = c.ra_pb.p;
         k.pe = c.ra_pe.p;
         launch_ra15_commit(k, c.stream);
+        c.dropin_launches += 1;
         check(cudaGetLastError(), "launch");
         check(cudaStreamSynchronize(c.stream), "step");
         *hdid = t;
@@ -405,6 +421,7 @@ void bs_step_once(double time, double* h, double* hdid, double tol, int64_t* rej
         a.errs = c.bs_errs.p;
         a.lvst = c.bs_lvst.p;
         launch_bs_sequence(a, c.stream);
+        c.dropin_launches += 1 + (c.np > 0 ? 1 : 0);
         check(cudaGetLastError(), "launch");
         unsigned long long errs[13];
         DeviceStatus lv[13];
@@ -439,6 +456,7 @@ void bs_step_once(double time, double* h, double* hdid, double tol, int64_t* rej
         k.bx_out = c.bigstate[out].p;
         k.px_out = c.pstate[out].p;
         launch_bs_commit(k, c.stream);
+        c.dropin_launches += 1;
         check(cudaGetLastError(), "launch");
         check(cudaStreamSynchronize(c.stream), "step");
         *hdid = *h;
@@ -491,6 +509,7 @@ void screen_pairs(double h) {
         a.cand_cap = (int)c.cands.n;
         a.status = c.status.p;
         launch_screen(a, c.stream);
+        c.dropin_launches += 1 + (c.np > 0 && nb > 0 ? 2 : 0);
         if (nb > 0 && c.np > 0) {
             ClassifyArgs ca;
             ca.nb = nb;
@@ -765,6 +784,7 @@ int reorder_slots(int src, double h, cudaStream_t st) {
     a.bslow = c.order_hist.p;
     a.bfast = c.order_hist.p + nblk;
     a.total = c.order_hist.p + 2 * nblk;
+    c.dropin_launches += 3;
     partition_count_kernel<<<nblk, PART_THREADS, 0, st>>>(a);
     partition_scan_kernel<<<1, 1024, 0, st>>>(a);
     partition_scatter_kernel<<<nblk, PART_THREADS, 0, st>>>(a);
@@ -951,6 +971,7 @@ int mercury_cuda_step(double time, double* h, double* hdid, double tol, int64_t*
     Context& c = ctx();
     try {
         require_system();
+        DropinTimer timer;
         *rejected = 0;
         const int64_t before = c.nforces;
         if (is_mvs(c.algorithm)) {
@@ -985,6 +1006,7 @@ int mercury_cuda_events(double time, double h, double rcen, const MercuryEvent**
     Context& c = ctx();
     try {
         require_system();
+        DropinTimer timer;
         const int prev = 1 - c.cur;
         if (!is_mvs(c.algorithm) && c.stepped) screen_pairs(h);
         for (int attempt = 0;; ++attempt) {
@@ -1012,6 +1034,7 @@ int mercury_cuda_events(double time, double h, double rcen, const MercuryEvent**
                 a.cap = (int)c.events.n;
                 a.status = c.status.p;
                 central_kernel<<<blocks(total), 256, 0, c.stream>>>(a);
+                c.dropin_launches += 1;
                 check(cudaGetLastError(), "central");
             }
             read_status();
@@ -1286,6 +1309,17 @@ int mercury_b200_timing(double* advance_ms, double* particle_kernel_ms, int* par
     if (particle_kernel_ms) *particle_kernel_ms = c.last_particle_kernel_ms;
     if (particle_launches) *particle_launches = c.last_particle_launches;
     if (kernel_launches) *kernel_launches = c.last_kernel_launches;
+    return 0;
+}
+
+int mercury_b200_dropin_time(double* ms, int64_t* launches, int reset) {
+    Context& c = ctx();
+    if (ms) *ms = c.dropin_ms;
+    if (launches) *launches = c.dropin_launches;
+    if (reset) {
+        c.dropin_ms = 0.0;
+        c.dropin_launches = 0;
+    }
     return 0;
 }
 

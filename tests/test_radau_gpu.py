@@ -20,6 +20,27 @@ from mercuda_b200.system import K2, System, make_system
 pytestmark = pytest.mark.gpu
 
 
+def force_matrix_system(pn, flag, n=200, seed=19):
+    rng = np.random.default_rng(seed)
+    m = np.zeros(n)
+    m[:3] = [K2, 3e-6 * K2, 1e-3 * K2]
+    m[3::7] = 1e-8 * K2
+    x = np.vstack([np.zeros(3), rng.uniform(-4, 4, (n - 1, 3))])
+    v = np.vstack([np.zeros(3), rng.uniform(-0.02, 0.02, (n - 1, 3))])
+    ngf = np.zeros((n, 5))
+    sign = np.array([(-1.0) ** j for j in range(n)])
+    if flag & 1:
+        ngf[1:, 0] = 1e-12
+        ngf[1:, 1] = sign[1:] * 2e-11
+        ngf[1:, 2] = 3e-13
+        ngf[1:, 4] = sign[1:] * 4e-11
+    if flag & 2:
+        ngf[1:, 3] = 0.001
+    rc = np.full(n, 0.01)
+    return System(m=m, x=x, v=v, nbig=3, ngf=ngf, jcen=np.array([1e-7, -1e-10, 1e-13]), rce=rc, rphys=rc.copy(),
+                  pn=int(pn))
+
+
 @pytest.mark.parametrize("pn", [0, 1])
 @pytest.mark.parametrize("flag", [0, 1, 2, 3])
 def test_force_matrix(cuda_lib, oracle, pn, flag):
