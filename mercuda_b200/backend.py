@@ -184,6 +184,95 @@ class Backend:
     def free(self) -> None:
         self.lib.mercury_cuda_free()
 
+    # gpu_hybrid_begin / gpu_hybrid_finish (mercury_gpu.f90:93-107)
+    def hybrid_begin(self, h: float, rcrit: np.ndarray, flag: int, x: np.ndarray, v: np.ndarray, cap: int = 1 << 20):
+        """Kick, solar drift, Kepler drift and mce_snif. Returns (ce, pi, pj); the
+        members' rows of x, v receive their pre-drift states."""
+        n = self.n
+        ce = np.zeros(n, dtype=np.int32)
+        pi = np.zeros(cap, dtype=np.int32)
+        pj = np.zeros(cap, dtype=np.int32)
+        count, nf = I(0), C.c_int64(0)
+        rc = self.lib.mercury_cuda_hybrid_begin(h, _p(np.ascontiguousarray(rcrit, dtype=np.float64)), int(flag),
+                                                cap, ce.ctypes.data_as(PI), C.byref(count), pi.ctypes.data_as(PI),
+                                                pj.ctypes.data_as(PI), _p(x), _p(v), C.byref(nf))
+        if rc != 0:
+            raise BackendError("CUDA hybrid drift failed")
+        self.forces += nf.value
+        return ce, pi[:count.value].copy(), pj[:count.value].copy()
+
+    def hybrid_finish(self, h: float, m: np.ndarray, x: np.ndarray, v: np.ndarray) -> None:
+        nf = C.c_int64(0)
+        if self.lib.mercury_cuda_hybrid_finish(h, _p(m), _p(x), _p(v), C.byref(nf)) != 0:
+            raise BackendError("CUDA hybrid kick failed")
+        self.forces += nf.value
+
+    # mdt_hy's CUDA branch with mdt_hkce's (mercury6_2.for:3646-3659, 3798-3940)
+    def hybrid_step(self, sys: System, time: float, h: float, tol: float, state: dict, rcen: float = 0.005):
+        """One HYBRID step of sys (democratic-heliocentric masses/radii/rcrit on
+        the host; positions live on the device). `state` carries dtflag and hrec
+        between calls. Returns the encounter records of the subsystem (global
+        1-based ids) and the number of encounter pairs."""
+        if state.get("dtflag", 0) == 0:
+            state["hrec"] = h
+        x = np.zeros((sys.n, 3))
+        v = np.zeros((sys.n, 3))
+        ce, pi, pj = self.hybrid_begin(h, sys.rcrit, state.get("dtflag", 0), x, v)
+        state["dtflag"] = 2
+        records = []
+        if len(pi):
+            sub = np.concatenate([[0], np.nonzero(ce[1:])[0] + 1])
+            index = sub.tolist()
+            back = np.full(sys.n, -1, dtype=np.int64)
+            back[sub] = np.arange(len(sub))
+            nbsbig = 1 + int(np.count_nonzero(sub[1:] < sys.nbig))
+            nbs = len(sub)
+            mbs = sys.m[sub].copy()
+            xbs = x[sub].copy()
+            vbs = v[sub].copy()
+            xbs[0] = 0.0
+            vbs[0] = 0.0
+            rcritbs = sys.rcrit[sub].copy()
+            rcebs = sys.rce[sub].copy()
+            rphybs = sys.rphys[sub].copy()
+            rcritbs[0] = rcebs[0] = rphybs[0] = 0.0
+            ibs = np.ascontiguousarray(back[pi - 1] + 1, dtype=np.int32)
+            jbs = np.ascontiguousarray(back[pj - 1] + 1, dtype=np.int32)
+            if self.lib.mercury_cuda_encounter_enter(nbs, nbsbig, _p(mbs), _p(xbs), _p(vbs), _p(rcritbs), _p(rcebs),
+                                                     _p(rphybs), len(ibs), ibs.ctypes.data_as(PI),
+                                                     jbs.ctypes.data_as(PI)) != 0:
+                raise BackendError("CUDA encounter initialization failed")
+            outer_n = self.n
+            self.n = nbs
+            try:
+                dtflag, tlocal, hlocal = 1, 0.0, math.copysign(state["hrec"], h)
+                while True:
+                    tmp0 = abs(h) - abs(tlocal)
+                    state["hrec"] = hlocal
+                    if abs(hlocal) > tmp0:
+                        hlocal = math.copysign(tmp0, h)
+                    hdid, hlocal = self.step(tlocal, hlocal, tol, dtflag)
+                    dtflag = 2
+                    xbs, vbs = self.download()
+                    tlocal = tlocal + hdid
+                    for e in self.events(time + tlocal, hdid, rcen):
+                        if e["kind"] & 8:
+                            continue
+                        e = e.copy()
+                        e["i"] = index[e["i"] - 1] + 1
+                        e["j"] = index[e["j"] - 1] + 1
+                        records.append(e)
+                    if not (tlocal - h) * h < 0.0:
+                        break
+            finally:
+                self.lib.mercury_cuda_encounter_exit()
+                self.n = outer_n
+            x[sub[1:]] = xbs[1:]
+            v[sub[1:]] = vbs[1:]
+        self.hybrid_finish(h, sys.m, x, v)
+        events = np.array(records, dtype=EVENT_DTYPE) if records else np.zeros(0, dtype=EVENT_DTYPE)
+        return events, len(pi)
+
     # mal_hvar's step loop (mercury6_2.for:423-470) through the drop-in calls:
     # steps clipped to tstop, dtflag = 1 (a fresh RA15 sequence) when a clipped
     # step changes h, events screened after every step.

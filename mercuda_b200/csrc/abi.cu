@@ -8,14 +8,19 @@
 #include "context.cuh"
 #include "mvs_device.cuh"
 #include "bs.cuh"
+#include "hybrid.cuh"
 #include "radau.cuh"
 
 namespace mb200 {
 
-Context& ctx() {
-    static Context c;
-    return c;
-}
+// The resident system and the compact close-encounter subsystem of HYBRID
+// (mercury_cuda_encounter_enter switches to the second until _exit), as the
+// reference swaps its whole context (mercury_cuda_hybrid.cuh:101-126); both
+// keep their allocations for the next use.
+Context g_contexts[2];
+int g_active = 0;
+
+Context& ctx() { return g_contexts[g_active]; }
 
 int report(const std::exception& e) {
     std::fprintf(stderr, "MERCURY CUDA: %s\n", e.what());
@@ -54,6 +59,7 @@ struct CentralArgs {
     int nbig, np, npcap;
     double mu, h, rcen;
     const double *big0, *big1, *part0, *part1, *pm, *mbig;
+    const double *voff0, *voff1;   // velocity shifts to heliocentric (HYBRID), or null
     const int* perm;
     MercuryEvent* events;
     int* event_step;
@@ -86,6 +92,10 @@ __global__ void central_kernel(CentralArgs A) {
             u1 = make_double3(A.part1[3 * S + p], A.part1[4 * S + p], A.part1[5 * S + p]);
             mj = A.pm[p];
             id = A.nbig + A.perm[p] + 1;
+        }
+        if (A.voff0) {
+            u0 = make_double3(u0.x + A.voff0[0], u0.y + A.voff0[1], u0.z + A.voff0[2]);
+            u1 = make_double3(u1.x + A.voff1[0], u1.y + A.voff1[1], u1.z + A.voff1[2]);
         }
         hit = central_impact(p0, u0, p1, u1, A.mu, mj, A.h, A.rcen, temp);
     }
@@ -420,6 +430,10 @@ void bs_step_once(double time, double* h, double* hdid, double tol, int64_t* rej
         a.pcand = c.bs_pcand.p;
         a.errs = c.bs_errs.p;
         a.lvst = c.bs_lvst.p;
+        a.hkce = c.encounter ? 1 : 0;
+        a.rcrit = c.rcritbig.p;
+        a.adj_off = c.adj_off.p;
+        a.adj = c.adj.p;
         launch_bs_sequence(a, c.stream);
         c.dropin_launches += 1 + (c.np > 0 ? 1 : 0);
         check(cudaGetLastError(), "launch");
@@ -583,6 +597,67 @@ void export_corrected(double h, double* xx, double* vv) {
               "export");
         check(cudaStreamSynchronize(c.stream), "export");
     }
+}
+
+// mco_dh2h's velocity shift (mercury6_2.for:2007-2051) of state buffer
+// `which`, added on the host to downloaded rows (the same additions).
+void add_dh_shift(int which, double* vv) {
+    Context& c = ctx();
+    c.hy_off.reserve(6);
+    launch_dh_shift(c.bigstate[which].p, c.mbig.p, c.nsplit, c.m_host[0], c.hy_off.p, c.stream);
+    double off[3];
+    check(cudaMemcpyAsync(off, c.hy_off.p, sizeof(off), cudaMemcpyDeviceToHost, c.stream), "download");
+    check(cudaStreamSynchronize(c.stream), "download");
+    for (int j = 1; j < c.n; ++j)
+        for (int q = 0; q < 3; ++q) vv[3 * j + q] = vv[3 * j + q] + off[q];
+}
+
+__global__ void scatter_members_kernel(const int* ids, int count, const double* packed, double* bx, int N, double* px,
+                                       int S, const int* inv) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= count) return;
+    const int g = ids[q];
+    for (int c = 0; c < 6; ++c) {
+        const double val = packed[6 * (size_t)q + c];
+        if (g < N) bx[c * N + g] = val;
+        else px[(size_t)c * S + inv[g - N]] = val;
+    }
+}
+
+// Members' rows {x, v} into the state buffers (massive set or particle slot).
+void scatter_members(const int* ids, int count, const double* packed, double* bx, double* px) {
+    Context& c = ctx();
+    scatter_members_kernel<<<blocks(count), 256, 0, c.stream>>>(ids, count, packed, bx, c.nsplit, px, c.npcap, c.inv.p);
+}
+
+HyArgs hybrid_args(double h, int recompute) {
+    Context& c = ctx();
+    HyArgs a{};
+    a.nbig = c.nbig;
+    a.nsplit = c.nsplit;
+    a.np = c.np;
+    a.npcap = c.npcap;
+    a.ngflag = c.ngflag;
+    a.obl = (c.jcen[0] != 0.0 || c.jcen[1] != 0.0 || c.jcen[2] != 0.0);
+    a.recompute = recompute;
+    for (int q = 0; q < 3; ++q) a.jcen[q] = c.jcen[q];
+    a.m0 = c.m_host[0];
+    a.h = h;
+    a.mbig = c.mbig.p;
+    a.rcritbig = c.rcritbig.p;
+    a.ngfbig = c.ngfbig.p;
+    a.bx_in = c.bigstate[c.cur].p;
+    a.bx_out = c.bigstate[1 - c.cur].p;
+    a.bscr = c.hy_scr.p;
+    a.px_in = c.pstate[c.cur].p;
+    a.px_out = c.pstate[1 - c.cur].p;
+    a.pconst = c.pconst[c.kc].p;
+    a.perm = c.permp();
+    a.tab = c.hy_tab.p;
+    a.pairs = c.hy_pairs.p;
+    a.pair_cap = (int)c.hy_pairs.n;
+    a.status = c.status.p;
+    return a;
 }
 
 // Warp-coherent ordering of the Small bodies. drift_dan leaves its elliptic
@@ -753,7 +828,7 @@ __global__ void __launch_bounds__(PART_THREADS) partition_scatter_kernel(Partiti
     const int ns = slow ? A.bslow[blockIdx.x] + rank : *A.total + A.bfast[blockIdx.x] + rank;
     const size_t S = A.npcap;
     for (int c = 0; c < 9; ++c) A.xout[c * S + ns] = A.xin[c * S + s];
-    for (int c = 0; c < 8; ++c) A.cout[c * S + ns] = A.cin[c * S + s];
+    for (int c = 0; c < PCONST_ROWS; ++c) A.cout[c * S + ns] = A.cin[c * S + s];
     const int p = A.pin[s];
     A.pout[ns] = p;
     A.inv[p] = ns;
@@ -859,7 +934,6 @@ int mercury_cuda_configure(int method) {
     if (method != 1 && method != 2 && method != 3 && method != 4 && method != 9 && method != 10) return 1;
     Context& c = ctx();
     try {
-        if (method == 10) throw std::runtime_error("algorithm not available in this build");
         if (method != c.algorithm) mercury_cuda_free();
         c.algorithm = method;
         c.reset = true;
@@ -886,8 +960,8 @@ int mercury_cuda_upload(int n, int nbig, int pn, int ngflag, const double* m, co
         int nmass = nbig;
         for (int j = nbig; j < n; ++j)
             if (m[j] != 0.0) nmass = j + 1;
-        const int ns = is_mvs(c.algorithm) ? nbig : nmass;
-        if (ns > 512) throw std::runtime_error("more than 512 Big and massive Small bodies");
+        const int ns = c.encounter ? n : is_mvs(c.algorithm) ? nbig : nmass;
+        if (ns > 512 && !c.encounter) throw std::runtime_error("more than 512 Big and massive Small bodies");
         c.n = n;
         c.nbig = nbig;
         c.nmass = nmass;
@@ -907,7 +981,7 @@ int mercury_cuda_upload(int n, int nbig, int pn, int ngflag, const double* m, co
             c.pstate[k].reserve((size_t)9 * c.npcap);
         }
         for (int k = 0; k < 2; ++k) {
-            c.pconst[k].reserve((size_t)8 * c.npcap);
+            c.pconst[k].reserve((size_t)PCONST_ROWS * c.npcap);
             c.perm[k].reserve(c.npcap);
         }
         c.inv.reserve(c.npcap);
@@ -931,8 +1005,8 @@ int mercury_cuda_upload(int n, int nbig, int pn, int ngflag, const double* m, co
         check(cudaMemsetAsync(c.pstate[1].p, 0, sizeof(double) * 9 * c.npcap, s), "memset");
         check(cudaMemsetAsync(c.bigstate[0].p, 0, sizeof(double) * 9 * ns, s), "memset");
         check(cudaMemsetAsync(c.bigstate[1].p, 0, sizeof(double) * 9 * ns, s), "memset");
-        check(cudaMemsetAsync(c.pconst[0].p, 0, sizeof(double) * 8 * c.npcap, s), "memset");
-        check(cudaMemsetAsync(c.pconst[1].p, 0, sizeof(double) * 8 * c.npcap, s), "memset");
+        check(cudaMemsetAsync(c.pconst[0].p, 0, sizeof(double) * PCONST_ROWS * c.npcap, s), "memset");
+        check(cudaMemsetAsync(c.pconst[1].p, 0, sizeof(double) * PCONST_ROWS * c.npcap, s), "memset");
         c.cur = 0;
         order_particles(n, ns, m[0], xx, vv);
         // positions and velocities
@@ -981,6 +1055,8 @@ int mercury_cuda_step(double time, double* h, double* hdid, double tol, int64_t*
             ra15_step_once(time, h, hdid, tol, rejected);
         } else if (c.algorithm == 2 || c.algorithm == 3) {
             bs_step_once(time, h, hdid, tol, rejected);
+        } else if (c.algorithm == 10) {
+            throw std::runtime_error("HYBRID steps go through mercury_cuda_hybrid_begin/_finish");
         } else {
             throw std::runtime_error("algorithm not available in this build");
         }
@@ -995,7 +1071,11 @@ int mercury_cuda_download(double* xx, double* vv, int previous) {
     Context& c = ctx();
     try {
         require_system();
-        download_buffer(previous ? 1 - c.cur : c.cur, xx, vv);
+        const int which = previous ? 1 - c.cur : c.cur;
+        download_buffer(which, xx, vv);
+        // HYBRID's previous state comes back with heliocentric velocities, as
+        // the reference keeps it (mercury_cuda.cu:538)
+        if (previous && c.algorithm == 10) add_dh_shift(which, vv);
         return 0;
     } catch (const std::exception& e) {
         return report(e);
@@ -1008,7 +1088,15 @@ int mercury_cuda_events(double time, double h, double rcen, const MercuryEvent**
         require_system();
         DropinTimer timer;
         const int prev = 1 - c.cur;
-        if (!is_mvs(c.algorithm) && c.stepped) screen_pairs(h);
+        if (!is_mvs(c.algorithm) && c.algorithm != 10 && c.stepped) screen_pairs(h);
+        const bool dh = c.algorithm == 10 && c.stepped;
+        if (dh) {
+            // heliocentric velocities of both states (mco_dh2h)
+            c.hy_off.reserve(6);
+            launch_dh_shift(c.bigstate[prev].p, c.mbig.p, c.nsplit, c.m_host[0], c.hy_off.p, c.stream);
+            launch_dh_shift(c.bigstate[c.cur].p, c.mbig.p, c.nsplit, c.m_host[0], c.hy_off.p + 3, c.stream);
+            c.dropin_launches += 2;
+        }
         for (int attempt = 0;; ++attempt) {
             // restart the counter after the step's pair events, then screen for central impacts
             DeviceStatus st = {0, c.pair_events, 0, 0};
@@ -1028,6 +1116,8 @@ int mercury_cuda_events(double time, double h, double rcen, const MercuryEvent**
                 a.part1 = c.pstate[c.cur].p;
                 a.pm = c.pm();
                 a.mbig = c.mbig.p;
+                a.voff0 = dh ? c.hy_off.p : nullptr;
+                a.voff1 = dh ? c.hy_off.p + 3 : nullptr;
                 a.perm = c.permp();
                 a.events = c.events.p;
                 a.event_step = c.event_step.p;
@@ -1113,8 +1203,12 @@ int mercury_cuda_export(double h, int physical, double* xx, double* vv) {
     Context& c = ctx();
     try {
         require_system();
-        if (physical && c.algorithm == 1) export_corrected(h, xx, vv);
-        else download_buffer(c.cur, xx, vv);
+        if (physical && c.algorithm == 1) {
+            export_corrected(h, xx, vv);
+        } else {
+            download_buffer(c.cur, xx, vv);
+            if (physical && c.algorithm == 10) add_dh_shift(c.cur, vv);
+        }
         return 0;
     } catch (const std::exception& e) {
         return report(e);
@@ -1134,24 +1228,199 @@ int mercury_cuda_limits(const double* limits) {
     }
 }
 
-int mercury_cuda_hybrid_begin(double, const double*, int, int, int*, int*, int*, int*, double*, double*, int64_t*) {
-    std::fprintf(stderr, "MERCURY CUDA: HYBRID not available in this build\n");
-    return 1;
+int mercury_cuda_hybrid_begin(double h, const double* crit, int flag, int cap, int* ce, int* count, int* pi, int* pj,
+                              double* xx, double* vv, int64_t* forces) {
+    Context& c = ctx();
+    try {
+        require_system();
+        if (c.algorithm != 10) throw std::runtime_error("hybrid_begin needs algorithm 10");
+        const int nb = c.nbig - 1, ns = c.nsplit;
+        c.rcritbig.reserve(ns);
+        c.hy_scr.reserve((size_t)6 * ns);
+        c.hy_tab.reserve(hy_tab_size(nb));
+        c.hy_pairs.reserve(4096);
+        const int recompute = (flag != 2 || c.reset) ? 1 : 0;
+        if (recompute) {
+            // rcrit of every body: massive set and the particles' constant row
+            c.transfer.reserve((size_t)6 * c.n);
+            check(cudaMemcpyAsync(c.transfer.p, crit, sizeof(double) * c.n, cudaMemcpyHostToDevice, c.stream),
+                  "upload");
+            scatter_rows(c.transfer.p, c.n, 1, ns, c.rcritbig.p, ns, c.pconst[c.kc].p + (size_t)PC_RCRIT * c.npcap,
+                         c.npcap, c.inv.p, c.stream);
+            c.dropin_launches += 1;
+        }
+        for (int attempt = 0;; ++attempt) {
+            check(cudaMemsetAsync(c.status.p, 0, sizeof(DeviceStatus), c.stream), "memset");
+            launch_hybrid_begin(hybrid_args(h, recompute), c.stream);
+            c.dropin_launches += 1 + (c.np > 0 ? 1 : 0);
+            check(cudaGetLastError(), "launch");
+            read_status();
+            if (!(c.status_host->overflow & 1)) break;
+            if (attempt > 8) throw std::runtime_error("pair buffer growth failed");
+            c.hy_pairs.reserve((size_t)c.status_host->events + 4096);
+        }
+        if (c.status_host->fault) throw std::runtime_error("Hybrid force failed");
+        const int64_t nf = recompute;
+        c.nforces += nf;
+        const int npairs = c.status_host->events;
+        std::vector<int2> pairs(npairs);
+        if (npairs)
+            check(cudaMemcpy(pairs.data(), c.hy_pairs.p, sizeof(int2) * npairs, cudaMemcpyDeviceToHost), "pairs");
+        std::sort(pairs.begin(), pairs.end(),
+                  [](const int2& a, const int2& b) { return a.x < b.x || (a.x == b.x && a.y < b.y); });
+        if (npairs > cap) throw std::runtime_error("Hybrid encounter capacity exceeded");
+        c.hy_members.clear();
+        if (npairs) {
+            std::fill(ce, ce + c.n, 0);
+            for (int k = 0; k < npairs; ++k) {
+                pi[k] = pairs[k].x + 1;
+                pj[k] = pairs[k].y + 1;
+                ce[pairs[k].x] = 2;
+                ce[pairs[k].y] = 2;
+            }
+            for (int j = 1; j < c.n; ++j)
+                if (ce[j]) c.hy_members.push_back(j);
+            const int nm = (int)c.hy_members.size();
+            c.hy_ids.reserve(nm);
+            c.hy_packed.reserve((size_t)6 * nm);
+            check(cudaMemcpyAsync(c.hy_ids.p, c.hy_members.data(), sizeof(int) * nm, cudaMemcpyHostToDevice,
+                                  c.stream),
+                  "members");
+            launch_hybrid_restore(hybrid_args(h, recompute), c.hy_ids.p, nm, c.inv.p, c.hy_packed.p, c.stream);
+            c.dropin_launches += 1;
+            std::vector<double> packed((size_t)6 * nm);
+            check(cudaMemcpyAsync(packed.data(), c.hy_packed.p, sizeof(double) * packed.size(),
+                                  cudaMemcpyDeviceToHost, c.stream),
+                  "members");
+            check(cudaStreamSynchronize(c.stream), "members");
+            for (int a = 0; a < nm; ++a)
+                for (int q = 0; q < 3; ++q) {
+                    xx[3 * c.hy_members[a] + q] = packed[6 * a + q];
+                    vv[3 * c.hy_members[a] + q] = packed[6 * a + 3 + q];
+                }
+        }
+        *count = npairs;
+        *forces = nf;
+        c.hy_begun = true;
+        return 0;
+    } catch (const std::exception& e) {
+        return report(e);
+    }
 }
-int mercury_cuda_hybrid_finish(double, const double*, const double*, const double*, int64_t*) {
-    std::fprintf(stderr, "MERCURY CUDA: HYBRID not available in this build\n");
-    return 1;
+
+int mercury_cuda_hybrid_finish(double h, const double* m, const double* xx, const double* vv, int64_t* forces) {
+    Context& c = ctx();
+    try {
+        require_system();
+        if (!c.hy_begun) throw std::runtime_error("hybrid_finish without hybrid_begin");
+        const int nm = (int)c.hy_members.size();
+        const int out = 1 - c.cur;
+        if (nm) {
+            // the members' states after the encounter integration, and the masses
+            std::vector<double> packed((size_t)6 * nm);
+            for (int a = 0; a < nm; ++a)
+                for (int q = 0; q < 3; ++q) {
+                    packed[6 * a + q] = xx[3 * c.hy_members[a] + q];
+                    packed[6 * a + 3 + q] = vv[3 * c.hy_members[a] + q];
+                }
+            check(cudaMemcpyAsync(c.hy_packed.p, packed.data(), sizeof(double) * packed.size(),
+                                  cudaMemcpyHostToDevice, c.stream),
+                  "members");
+            scatter_members(c.hy_ids.p, nm, c.hy_packed.p, c.bigstate[out].p, c.pstate[out].p);
+            c.transfer.reserve((size_t)6 * c.n);
+            check(cudaMemcpyAsync(c.transfer.p, m, sizeof(double) * c.n, cudaMemcpyHostToDevice, c.stream), "upload");
+            scatter_rows(c.transfer.p, c.n, 1, c.nsplit, c.mbig.p, c.nsplit, c.pm(), c.npcap, c.inv.p, c.stream);
+            check(cudaStreamSynchronize(c.stream), "upload");
+            c.m_host.assign(m, m + c.n);
+            c.dropin_launches += 2;
+        }
+        check(cudaMemsetAsync(c.status.p, 0, sizeof(DeviceStatus), c.stream), "memset");
+        launch_hybrid_finish(hybrid_args(h, 0), c.stream);
+        c.dropin_launches += 1 + (c.np > 0 ? 1 : 0);
+        check(cudaGetLastError(), "launch");
+        read_status();
+        if (c.status_host->fault) throw std::runtime_error("Hybrid final force failed");
+        c.nforces += 1;
+        *forces = 1;
+        c.cur = out;
+        c.reset = false;
+        c.stepped = true;
+        c.pair_events = 0;
+        c.hy_begun = false;
+        return 0;
+    } catch (const std::exception& e) {
+        return report(e);
+    }
 }
-int mercury_cuda_encounter_enter(int, int, const double*, const double*, const double*, const double*,
-                                 const double*, const double*, int, const int*, const int*) {
-    std::fprintf(stderr, "MERCURY CUDA: HYBRID not available in this build\n");
-    return 1;
+
+int mercury_cuda_encounter_enter(int n, int nb, const double* m, const double* xx, const double* vv,
+                                 const double* crit, const double* limits, const double* radii, int np,
+                                 const int* pi, const int* pj) {
+    try {
+        if (g_active != 0) throw std::runtime_error("encounter subsystem already active");
+        g_active = 1;
+        Context& c = ctx();
+        if (c.algorithm != 3) c.release_all();
+        c.algorithm = 3;
+        c.encounter = true;
+        std::vector<double> zero((size_t)5 * n, 0.0);
+        const double jc[3] = {0.0, 0.0, 0.0};
+        if (mercury_cuda_upload(n, nb, 0, 0, m, xx, vv, zero.data(), jc, limits, radii))
+            throw std::runtime_error("Encounter upload failed");
+        c.rcritbig.reserve(n);
+        check(cudaMemcpy(c.rcritbig.p, crit, sizeof(double) * n, cudaMemcpyHostToDevice), "upload");
+        // per-body pair lists in pair order (mfo_hkce's accumulation order)
+        std::vector<int> off(n + 1, 0);
+        for (int k = 0; k < np; ++k) {
+            const int i = pi[k] - 1, j = pj[k] - 1;
+            if (i < 0 || j < 0 || i >= n || j >= n) throw std::runtime_error("encounter pair out of range");
+            ++off[i + 1];
+            ++off[j + 1];
+        }
+        for (int k = 0; k < n; ++k) off[k + 1] += off[k];
+        std::vector<int> fill(off.begin(), off.end() - 1);
+        std::vector<int2> adj(std::max(1, 2 * np));
+        for (int k = 0; k < np; ++k) {
+            const int i = pi[k] - 1, j = pj[k] - 1;
+            adj[fill[i]++] = make_int2(j, 0);
+            adj[fill[j]++] = make_int2(i, 1);
+        }
+        c.adj_off.reserve(n + 1);
+        c.adj.reserve(adj.size());
+        check(cudaMemcpy(c.adj_off.p, off.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice), "pairs");
+        check(cudaMemcpy(c.adj.p, adj.data(), sizeof(int2) * adj.size(), cudaMemcpyHostToDevice), "pairs");
+        return 0;
+    } catch (const std::exception& e) {
+        g_active = 0;
+        return report(e);
+    }
 }
-int mercury_cuda_encounter_update(const double*, const double*, const double*) {
-    std::fprintf(stderr, "MERCURY CUDA: HYBRID not available in this build\n");
-    return 1;
+
+int mercury_cuda_encounter_update(const double* m, const double* xx, const double* vv) {
+    Context& c = ctx();
+    try {
+        require_system();
+        if (g_active != 1) throw std::runtime_error("no encounter subsystem active");
+        c.transfer.reserve((size_t)6 * c.n);
+        check(cudaMemcpyAsync(c.transfer.p, m, sizeof(double) * c.n, cudaMemcpyHostToDevice, c.stream), "upload");
+        scatter_rows(c.transfer.p, c.n, 1, c.nsplit, c.mbig.p, c.nsplit, c.pm(), c.npcap, c.inv.p, c.stream);
+        check(cudaStreamSynchronize(c.stream), "upload");
+        c.m_host.assign(m, m + c.n);
+        for (int part = 0; part < 2; ++part) {
+            check(cudaMemcpyAsync(c.transfer.p, part ? vv : xx, sizeof(double) * 3 * c.n, cudaMemcpyHostToDevice,
+                                  c.stream),
+                  "upload");
+            scatter_rows(c.transfer.p, c.n, 3, c.nsplit, c.bigstate[c.cur].p + 3 * part * c.nsplit, c.nsplit,
+                         c.pstate[c.cur].p + (size_t)3 * part * c.npcap, c.npcap, c.inv.p, c.stream);
+            check(cudaStreamSynchronize(c.stream), "upload");
+        }
+        return 0;
+    } catch (const std::exception& e) {
+        return report(e);
+    }
 }
-void mercury_cuda_encounter_exit(void) {}
+
+void mercury_cuda_encounter_exit(void) { g_active = 0; }
 
 // ---------------------------------------------------------------- extensions
 
@@ -1185,7 +1454,7 @@ int mercury_b200_mvs_advance(double time, double h, int nsteps, double rcen, int
         // keep the starting state (and slot order) so that an event-buffer
         // overflow can be redone from it
         c.snapshot.reserve((size_t)9 * c.npcap + 9 * c.nbig);
-        c.snap_const.reserve((size_t)8 * c.npcap);
+        c.snap_const.reserve((size_t)PCONST_ROWS * c.npcap);
         c.snap_perm.reserve((size_t)2 * c.npcap);
         const int kc0 = c.kc;
         auto copy = [&](void* dst, const void* src, size_t bytes) {
@@ -1193,7 +1462,7 @@ int mercury_b200_mvs_advance(double time, double h, int nsteps, double rcen, int
         };
         copy(c.snapshot.p, c.pstate[c.cur].p, sizeof(double) * 9 * c.npcap);
         copy(c.snapshot.p + 9 * c.npcap, c.bigstate[c.cur].p, sizeof(double) * 9 * c.nbig);
-        copy(c.snap_const.p, c.pconst[kc0].p, sizeof(double) * 8 * c.npcap);
+        copy(c.snap_const.p, c.pconst[kc0].p, sizeof(double) * PCONST_ROWS * c.npcap);
         copy(c.snap_perm.p, c.perm[kc0].p, sizeof(int) * c.npcap);
         copy(c.snap_perm.p + c.npcap, c.inv.p, sizeof(int) * c.npcap);
         const bool reset0 = c.reset;
@@ -1256,7 +1525,7 @@ int mercury_b200_mvs_advance(double time, double h, int nsteps, double rcen, int
             c.kc = kc0;
             copy(c.pstate[c.cur].p, c.snapshot.p, sizeof(double) * 9 * c.npcap);
             copy(c.bigstate[c.cur].p, c.snapshot.p + 9 * c.npcap, sizeof(double) * 9 * c.nbig);
-            copy(c.pconst[kc0].p, c.snap_const.p, sizeof(double) * 8 * c.npcap);
+            copy(c.pconst[kc0].p, c.snap_const.p, sizeof(double) * PCONST_ROWS * c.npcap);
             copy(c.perm[kc0].p, c.snap_perm.p, sizeof(int) * c.npcap);
             copy(c.inv.p, c.snap_perm.p + c.npcap, sizeof(int) * c.npcap);
         }

@@ -35,6 +35,54 @@ __device__ __forceinline__ bool body_error(const double* q, double xscal, double
     return true;
 }
 
+// mfo_hkce for body k (mercury6_2.for:4868-4905): the inner changeover
+// 1 - K(r) over k's pairs in pair-list order, then the central attraction.
+__device__ double3 hkce_force(const BsArgs& A, int k, const double* X) {
+    const int N = A.f.nsplit;
+    const double* m = A.mbig;
+    const double3 xk = make_double3(X[k], X[N + k], X[2 * N + k]);
+    double3 a = make_double3(0.0, 0.0, 0.0);
+    for (int e = A.adj_off[k]; e < A.adj_off[k + 1]; ++e) {
+        const int q = A.adj[e].x;
+        const bool first = A.adj[e].y == 0;
+        const int i = first ? k : q, j = first ? q : k;
+        const double dx = X[j] - X[i], dy = X[N + j] - X[N + i], dz = X[2 * N + j] - X[2 * N + i];
+        const double s2 = dx * dx + dy * dy + dz * dz;
+        const double rc = fmax(A.rcrit[i], A.rcrit[j]);
+        const double rc2 = rc * rc;
+        if (!(s2 < rc2)) continue;
+        const double s_1 = 1.0 / sqrt(s2);
+        const double s_3 = s_1 * s_1 * s_1;
+        double tmp2;
+        if (s2 <= 0.01 * rc2) {
+            tmp2 = s_3;
+        } else {
+            const double s = 1.0 / s_1;
+            const double qq = (s - 0.1 * rc) / (0.9 * rc);
+            const double q2 = qq * qq, q3 = qq * q2, q4 = q2 * q2, q5 = q2 * q3;
+            tmp2 = (1.0 - 10.0 * q3 + 15.0 * q4 - 6.0 * q5) * s_3;
+        }
+        if (first) {
+            const double facj = tmp2 * m[j];
+            a.x = a.x + facj * dx;
+            a.y = a.y + facj * dy;
+            a.z = a.z + facj * dz;
+        } else {
+            const double faci = tmp2 * m[i];
+            a.x = a.x - faci * dx;
+            a.y = a.y - faci * dy;
+            a.z = a.z - faci * dz;
+        }
+    }
+    const double s2 = xk.x * xk.x + xk.y * xk.y + xk.z * xk.z;
+    const double s_1 = 1.0 / sqrt(s2);
+    const double tmp2 = A.f.m0 * s_1 * s_1 * s_1;
+    a.x = a.x - tmp2 * xk.x;
+    a.y = a.y - tmp2 * xk.y;
+    a.z = a.z - tmp2 * xk.z;
+    return a;
+}
+
 // ------------------------------------------------------------ massive set
 // Scratch rows of the massive-set CTA, each [nsplit] doubles.
 struct BsScratch {
@@ -55,6 +103,14 @@ __device__ void massive_call(const BsArgs& A, const double* X, const double* V, 
     const ForceCfg& f = A.f;
     const int N = f.nsplit;
     __syncthreads();
+    if (A.hkce) {
+        for (int k = 1 + threadIdx.x; k < N; k += blockDim.x) {
+            const double3 a = hkce_force(A, k, X);
+            out[k] = a.x; out[N + k] = a.y; out[2 * N + k] = a.z;
+        }
+        __syncthreads();
+        return;
+    }
     if (threadIdx.x == 0) row_head(X, A.mbig, f, T);
     __syncthreads();
     for (int k = threadIdx.x; k < N; k += blockDim.x) {

@@ -36,13 +36,20 @@ struct BsArgs {
     const double* ngfbig;        // [nsplit][5]
     double* bscr;                // [bs_massive_scratch][nsplit]
     const double* px;            // [9][npcap] start-of-step particle state
-    const double* pconst;        // [8][npcap]
+    const double* pconst;        // [PCONST_ROWS][npcap]
     double* table;               // [bs_rows][force_row(nb)]
     double* bcand;               // [bs_candidates * 6][nsplit]
     double* pcand;               // [bs_candidates * 6][npcap]
     unsigned long long* errs;    // [13] max error of level n (bit pattern of a non-negative double; +inf
                                  // when an extrapolated value is not finite)
     DeviceStatus* lvst;          // [13] force faults of level n (0: the start-of-step force)
+    // mfo_hkce instead of mfo_all (the compact encounter subsystem, every body
+    // in the massive set): pairs of body k are adj[adj_off[k] .. adj_off[k+1])
+    // = {partner, 0 if k is the pair's first body else 1}, in pair-list order
+    int hkce;
+    const double* rcrit;         // [nsplit]
+    const int* adj_off;
+    const int2* adj;
 };
 
 struct BsCommitArgs {

@@ -28,6 +28,10 @@ constexpr int EV_CLOSE = 1, EV_NEAR = 2, EV_HIT = 4, EV_CENTRAL = 8;
 // coincident bodies (mfo_grav's fail() on a zero separation).
 constexpr int FAULT_NONFINITE = 1, FAULT_NGF = 2, FAULT_COINCIDENT = 4;
 
+// Rows of the per-slot particle constants: m, rce, rphys, ngf(5), rcrit.
+constexpr int PCONST_ROWS = 9;
+constexpr int PC_M = 0, PC_RCE = 1, PC_RPHYS = 2, PC_NGF = 3, PC_RCRIT = 8;
+
 // Device-side status word written by kernels.
 struct DeviceStatus {
     int fault;

@@ -59,7 +59,7 @@ struct Context {
     DBuf<double> bigstate[2];   // [9][nbig]: x(3) v(3) a(3)
     // particles
     DBuf<double> pstate[2];     // [9][npcap]
-    // per-slot constants [8][npcap]: m, rce, rphys, ngf(5); double-buffered with
+    // per-slot constants [PCONST_ROWS][npcap]: m, rce, rphys, ngf(5), rcrit; double-buffered with
     // perm (slot -> particle index) so that the slots can be re-ordered
     DBuf<double> pconst[2];
     DBuf<int> perm[2];
@@ -86,6 +86,19 @@ struct Context {
     DBuf<double> bs_scr, bs_bcand, bs_pcand;
     DBuf<unsigned long long> bs_errs;
     DBuf<DeviceStatus> bs_lvst;
+    // HYBRID: rcrit of the massive set, the massive set after the first solar
+    // drift, the three force/begin rows, dh2h velocity shifts of the previous
+    // and current states, members' packed rows, encounter pairs and member ids
+    DBuf<double> rcritbig, hy_scr, hy_tab, hy_off, hy_packed;
+    DBuf<int2> hy_pairs;
+    DBuf<int> hy_ids;
+    std::vector<int> hy_members;
+    bool hy_begun = false;
+    // compact encounter subsystem: every body in the massive arrays, BS2 with
+    // mfo_hkce over the pair list (per-body adjacency in pair order)
+    bool encounter = false;
+    DBuf<int> adj_off;
+    DBuf<int2> adj;
     // events
     DBuf<MercuryEvent> events;
     DBuf<int> event_step;
@@ -145,13 +158,20 @@ struct Context {
         DBuf<double>* bufs[] = {&mbig, &rcebig, &rphysbig, &ngfbig, &bigstate[0], &bigstate[1], &pstate[0],
                                 &pstate[1], &pconst[0], &pconst[1], &tab, &detail, &transfer, &snapshot, &snap_const,
                                 &ra_bb, &ra_be, &ra_bg, &ra_bpx, &ra_pb, &ra_pe, &ftab, &force_out, &boxes, &corr_big, &corr_part,
-                                &bs_scr, &bs_bcand, &bs_pcand};
+                                &bs_scr, &bs_bcand, &bs_pcand, &rcritbig, &hy_scr, &hy_tab, &hy_off,
+                                &hy_packed};
         for (auto* b : bufs) b->release();
         DBuf<int>* ibufs[] = {&perm[0], &perm[1], &inv, &order_bucket, &order_hist, &snap_perm};
         for (auto* b : ibufs) b->release();
         ra_max.release();
         bs_errs.release();
         bs_lvst.release();
+        hy_pairs.release();
+        hy_ids.release();
+        adj_off.release();
+        adj.release();
+        hy_members.clear();
+        hy_begun = false;
         kc = 0;
         events.release();
         event_step.release();

@@ -25,7 +25,7 @@ struct Ra15Args {
     double* bpx;           // [6][nsplit] predicted x, v scratch
     // particles
     double* px;            // [9][npcap] current buffer; a(3) receives a1
-    const double* pconst;  // [8][npcap]
+    const double* pconst;  // [PCONST_ROWS][npcap]
     double* pb;            // [21][npcap] B
     double* table;         // [1 + 7*niter][force_row(nb)]
     unsigned long long* maxb7;  // max |b7| over every coordinate (bit pattern of a non-negative double)

@@ -80,6 +80,13 @@ def lib() -> C.CDLL:
         L.oracle_hvar_run.argtypes = [I, I, I, PD, PD, PD, PD, I, I, PD, PD, PD, D, D, PD, D, D, I, I,
                                       C.POINTER(C.c_longlong)]
         L.oracle_hvar_run.restype = C.c_void_p
+        L.oracle_hy_run.argtypes = [I, I, PD, PD, PD, PD, I, PD, PD, PD, PD, D, D, I, D, D, I,
+                                    C.POINTER(C.c_longlong)]
+        L.oracle_hy_run.restype = C.c_void_p
+        PI_ = C.POINTER(I)
+        L.oracle_mce_snif.argtypes = [D, I, I, PD, PD, PD, PD, PD, PI_, PI_, I]
+        L.oracle_mce_snif.restype = I
+        L.oracle_mfo_hy.argtypes = [I, I, PD, PD, PD, PD, PD]
         _lib = L
     return _lib
 
@@ -241,3 +248,41 @@ def ra15_run(sys, time0, tstop, h, tol, rcen=0.005, central=True, max_steps=1_00
     """mal_hvar-style RA15 loop on sys (in place). Returns (events, steps, h_next, nsteps, nforces)."""
     ev, st, hn, n, f, _ = hvar_run(sys, 4, time0, tstop, h, tol, rcen, central, max_steps)
     return ev, st, hn, n, f
+
+
+def hy_run(sys, time0, h, nsteps, tol=1e-12, rcen=0.005, central=True):
+    """mal_hcon's HYBRID loop (mdt_hy) on sys's democratic-heliocentric state (in place).
+
+    Uses sys.rcrit. Returns (events, step of each event, force calls, encounter pairs)."""
+    s = sys
+    counters = (C.c_longlong * 2)()
+    handle = lib().oracle_hy_run(s.n, s.nbig, _p(s.m), _p(s.x), _p(s.v), _p(s.ngf), s.ngflag, _p(s.jcen),
+                                 _p(s.rce), _p(s.rphys), _p(s.rcrit), time0, h, int(nsteps), tol, rcen,
+                                 int(central), counters)
+    try:
+        if lib().oracle_run_status(handle):
+            raise RuntimeError("oracle HYBRID run failed")
+        count = lib().oracle_run_event_count(handle)
+        events = np.zeros(count, dtype=EVENT_DTYPE)
+        steps = np.zeros(count, dtype=np.int32)
+        lib().oracle_run_events(handle, events.ctypes.data_as(C.c_void_p), steps.ctypes.data_as(C.c_void_p))
+    finally:
+        lib().oracle_run_free(handle)
+    return events, steps, counters[0], counters[1]
+
+
+def mce_snif(h, nbig, x0, v0, x1, v1, rcrit, cap=100000):
+    x0, v0, x1, v1, rcrit = map(_f64, (x0, v0, x1, v1, rcrit))
+    n = len(rcrit)
+    ice = np.zeros(cap, dtype=np.int32)
+    jce = np.zeros(cap, dtype=np.int32)
+    PI_ = C.POINTER(I)
+    k = lib().oracle_mce_snif(h, n, nbig, _p(x0), _p(v0), _p(x1), _p(v1), _p(rcrit),
+                              ice.ctypes.data_as(PI_), jce.ctypes.data_as(PI_), cap)
+    return ice[:min(k, cap)], jce[:min(k, cap)]
+
+
+def mfo_hy(sys):
+    a = np.zeros((sys.n, 3))
+    lib().oracle_mfo_hy(sys.n, sys.nbig, _p(sys.m), _p(sys.x), _p(sys.rcrit), _p(sys.jcen), _p(a))
+    return a

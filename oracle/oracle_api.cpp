@@ -11,6 +11,7 @@
 #include "oracle_mvs.hpp"
 #include "oracle_ra15.hpp"
 #include "oracle_bs.hpp"
+#include "oracle_hy.hpp"
 
 namespace oracle {
 thread_local Tally tally;
@@ -322,6 +323,65 @@ OracleRun* oracle_hvar_run(int algor, int n, int nbig, const double* m, double* 
         counters[2] = rejected;
     }
     return run;
+}
+
+// mal_hcon's loop with algor 10 (mdt_hy, mercury6_2.for:3618-3782) on the
+// democratic-heliocentric state (x, v in place): per step the encounter
+// records of mdt_hkce, then mce_cent on the heliocentric (mco_dh2h) states
+// before and after the step. counters = {force calls, encounter pairs}.
+OracleRun* oracle_hy_run(int n, int nbig, const double* m, double* x, double* v, const double* ngf, int ngflag,
+                         const double* jcen, const double* rce, const double* rphys, const double* rcrit,
+                         double time0, double h, int nsteps, double tol, double rcen, int central,
+                         long long* counters) {
+    OracleRun* run = new OracleRun();
+    oracle::HyState st;
+    std::vector<double> xh0(3 * n), vh0(3 * n), vh1(3 * n);
+    long long forces = 0, pairs = 0;
+    double time = time0;
+    std::vector<Event> events;
+    for (int s = 0; s < nsteps; ++s) {
+        std::copy(x, x + 3 * n, xh0.begin());
+        oracle::dh2h_velocity(n, m, v, vh0.data());
+        events.clear();
+        int nce = 0;
+        if (oracle::mdt_hy(time, h, tol, jcen, n, nbig, m, x, v, ngf, ngflag, rphys, rcrit, rce, st, events, &nce,
+                           &forces)) {
+            run->status = 1;
+            break;
+        }
+        pairs += nce;
+        time = time + h;
+        if (central) {
+            oracle::dh2h_velocity(n, m, v, vh1.data());
+            oracle::mce_cent<double>(time, h, rcen, 1, n, m, xh0.data(), vh0.data(), x, vh1.data(), events);
+        }
+        std::stable_sort(events.begin(), events.end(), event_less);
+        for (auto& e : events) run->events.push_back(StepEvent{s, e});
+    }
+    if (counters) {
+        counters[0] = forces;
+        counters[1] = pairs;
+    }
+    return run;
+}
+
+// mce_snif on given states (0-based pairs into ice/jce, up to cap); returns
+// the pair count.
+int oracle_mce_snif(double h, int n, int nbig, const double* x0, const double* v0, const double* x1,
+                    const double* v1, const double* rcrit, int* ice, int* jce, int cap) {
+    std::vector<int> ce, vi, vj;
+    oracle::mce_snif(h, n, nbig, x0, v0, x1, v1, rcrit, ce, vi, vj);
+    for (size_t k = 0; k < vi.size() && (int)k < cap; ++k) {
+        ice[k] = vi[k];
+        jce[k] = vj[k];
+    }
+    return (int)vi.size();
+}
+
+// mfo_hy of the whole system into a (n, 3).
+void oracle_mfo_hy(int n, int nbig, const double* m, const double* x, const double* rcrit, const double* jcen,
+                   double* a) {
+    oracle::mfo_hy(jcen, n, nbig, m, x, rcrit, a);
 }
 
 }  // extern "C"

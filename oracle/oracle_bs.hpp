@@ -138,21 +138,18 @@ inline int mdt_bs1(double time, double& h0, double& hdid, double tol, const doub
     }
 }
 
-// mdt_bs2, mercury6_2.for:3428-3596: the force is evaluated with the
+// mdt_bs2, mercury6_2.for:3428-3596, with any force routine
+// force(x, v, a) -> nonzero on fail(); the force is evaluated with the
 // start-of-step velocities v0 (conservative systems).
-inline int mdt_bs2(double time, double& h0, double& hdid, double tol, const double* jcen, int nbod, int nbig,
-                   const double* mass, double* x0, double* v0, const double* ngf, int ngflag, int pn,
-                   long long* forces, long long* rejected) {
+template <class Force>
+int mdt_bs2_with(Force&& force, double time, double& h0, double& hdid, double tol, int nbod, double* x0, double* v0,
+                 long long* rejected) {
     const double tol2 = tol * tol;
     const size_t nv = 3 * (size_t)nbod;
     std::vector<double> xscal(nbod), vscal(nbod), xend(nv), a(nv), a0(nv), b(nv), c(nv);
     std::vector<std::vector<double>> d(13, std::vector<double>(6 * (size_t)nbod));
     double h2[13];
     bs_scales(nbod, x0, v0, xscal, vscal);
-    auto force = [&](const double* xx, const double* vv, double* aa) {
-        if (forces) ++*forces;
-        return mfo_all(jcen, nbod, nbig, mass, xx, vv, aa, ngf, ngflag, pn);
-    };
     if (force(x0, v0, a0.data())) return 1;
     for (;;) {
         if (time + h0 == time) return 1;
@@ -198,6 +195,16 @@ inline int mdt_bs2(double time, double& h0, double& hdid, double tol, const doub
         if (rejected) ++*rejected;
         h0 = h0 * 0.5;
     }
+}
+
+inline int mdt_bs2(double time, double& h0, double& hdid, double tol, const double* jcen, int nbod, int nbig,
+                   const double* mass, double* x0, double* v0, const double* ngf, int ngflag, int pn,
+                   long long* forces, long long* rejected) {
+    auto force = [&](const double* xx, const double* vv, double* aa) {
+        if (forces) ++*forces;
+        return mfo_all(jcen, nbod, nbig, mass, xx, vv, aa, ngf, ngflag, pn);
+    };
+    return mdt_bs2_with(force, time, h0, hdid, tol, nbod, x0, v0, rejected);
 }
 
 }  // namespace oracle
