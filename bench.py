@@ -15,6 +15,11 @@ kick) of every particle, events included.
 restatement of mercury6_2.for in oracle/, all host cores) on the same
 workload; under torchrun only rank 0 runs it.
 
+--workload hybrid measures HYBRID (mdt_hy through mercury_cuda_hybrid_begin /
+_finish, the encounter members' BS2 subsystem driven as mdt_hkce drives it,
+central-impact screen every step) on the MVS workload's system, rcrit from
+mce_init (cefac 3); a step is one HYBRID step.
+
 --workload radau|bs|bs2 measures the adaptive integrators instead (mdt_ra15,
 mdt_bs1, mdt_bs2 through the drop-in step/events calls, as mal_hvar drives
 them) on the 100,000-particle system of the same generator with 1PN,
@@ -70,9 +75,9 @@ def parse_args():
     p.add_argument("--threads", type=int, default=0)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", default="mvs", choices=["mvs", "radau", "bs", "bs2"])
+    p.add_argument("--workload", default="mvs", choices=["mvs", "radau", "bs", "bs2", "hybrid"])
     args = p.parse_args()
-    if args.workload != "mvs" and args.particles == 1_000_000:
+    if args.workload in ADAPTIVE and args.particles == 1_000_000:
         args.particles = 100_000
     return args
 
@@ -283,6 +288,113 @@ def run_adaptive(args, rank, world, dist):
     b.free()
 
 
+def run_hybrid(args, rank, world, dist):
+    from mercuda_b200.system import mce_init
+    metric = "HYBRID particle-steps/s"
+    workload_text = (f"HYBRID, {args.particles} massless particles + 8 planets, h=8 d, 1% near planets, "
+                     "rcrit = max(3 Hill, 0.4 h vmax), encounter subsystem by BS2, central screen every step")
+    tol = 1e-12
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        from oracle import oracle as O
+        particles = min(args.particles, 50_000)
+        sysc = mce_init(workload(particles, args.seed), H, 3.0)
+        t0 = time.perf_counter()
+        O.hy_run(sysc, 0.0, H, args.steps, tol, RCEN)
+        dt = time.perf_counter() - t0
+        value = particles * args.steps / dt
+        sample = f"{particles} particles of the same generator x {args.steps} steps ({dt:.1f} s, 1 thread)"
+        print(json.dumps({"impl": "reference", "metric": metric, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+                          "steps": args.steps, "warmup": 0, "ms_per_step": dt * 1e3 / args.steps,
+                          "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                          "data": "synthetic", "config": {"workload": workload_text, "particles": particles},
+                          "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
+                                           "sample": sample},
+                          "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}), flush=True)
+        return
+    import torch
+    from mercuda_b200.backend import Backend
+
+    b = Backend("HYBRID")
+    b.configure()
+    sysw = mce_init(workload(args.particles, args.seed + rank), H, 3.0)
+    b.upload(sysw)
+    state = {"dtflag": 0}
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def run(t, nsteps):
+        nev = pairs = 0
+        for _ in range(nsteps):
+            ev, npair = b.hybrid_step(sysw, t, H, tol, state, RCEN)
+            t = t + H
+            nev += len(ev) + len(b.events(t, H, RCEN))
+            pairs += npair
+        return t, nev, pairs
+
+    t, _, _ = run(0.0, args.warmup)
+    b.dropin_time(reset=True)
+    barrier()
+    w0 = time.perf_counter()
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clocks:
+        t, nev, pairs = run(t, args.steps)
+    barrier()
+    wall = time.perf_counter() - w0
+    ms, launches = b.dropin_time(reset=True)
+    if dist:
+        tt = torch.tensor([ms, wall], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms, wall = float(tt[0].item()), float(tt[1].item())
+    value = world * args.particles * args.steps / (ms * 1e-3)
+    e2e = None
+    if not args.no_e2e:
+        fresh = mce_init(workload(args.particles, args.seed + rank), H, 3.0)
+        barrier()
+        t0 = time.perf_counter()
+        b.upload(fresh)
+        state = {"dtflag": 0}
+        sysw = fresh
+        run(0.0, args.steps)
+        x, v = b.download()
+        barrier()
+        e2e_s = time.perf_counter() - t0
+        if dist:
+            tt = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            e2e_s = float(tt.item())
+        h2d = fresh.n * (3 + 3 + 1 + 1 + 1 + 5 + 1) * 8
+        e2e = {"value": world * args.particles * args.steps / e2e_s, "unit": UNIT,
+               "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": fresh.n * 48 / args.steps,
+               "note": "wall clock around upload, hybrid_begin, the encounter subsystem, hybrid_finish and the "
+                       "central screen of every step, download"}
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        from oracle import oracle as O
+        particles = min(args.particles, 50_000)
+        sysc = mce_init(workload(particles, args.seed), H, 3.0)
+        t0 = time.perf_counter()
+        O.hy_run(sysc, 0.0, H, 40, tol, RCEN)
+        dt = time.perf_counter() - t0
+        cpu = {"value": particles * 40 / dt, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": f"{particles} particles of the same generator x 40 steps ({dt:.1f} s)"}
+    if rank == 0:
+        print(json.dumps({"metric": metric, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                          "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+                          "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                          "config": {"workload": workload_text, "particles_per_gpu": args.particles,
+                                     "seed": args.seed, "encounter_pairs": pairs,
+                                     "wall_ms_per_step": wall * 1e3 / args.steps},
+                          "clocks": clocks.summary(), "gpu_launches": launches, "events": nev, "e2e": e2e,
+                          "cpu_baseline": cpu}), flush=True)
+    b.free()
+
+
 def main():
     args = parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -300,7 +412,10 @@ def main():
         if args.impl != "reference":
             import torch
             torch.cuda.set_device(local)
-        run_adaptive(args, rank, world, dist)
+        if args.workload == "hybrid":
+            run_hybrid(args, rank, world, dist)
+        else:
+            run_adaptive(args, rank, world, dist)
         if dist:
             dist.destroy_process_group()
         return

@@ -25,10 +25,11 @@ int mercury_b200_events(MercuryEvent* events, int* steps, int cap);
  * of kernels it launched on all streams. */
 int mercury_b200_timing(double* advance_ms, double* particle_kernel_ms, int* particle_launches,
                         int* kernel_launches);
-/* Device time (CUDA events on the library's stream) spent in the drop-in
- * mercury_cuda_step and mercury_cuda_events calls, and the number of kernels
- * they launched, since the last call with reset != 0 (which zeroes both).
- * No counterpart in the reference. */
+/* Device time (CUDA events on the library's streams) spent in the drop-in
+ * mercury_cuda_step, mercury_cuda_events and mercury_cuda_hybrid_begin/_finish
+ * calls of the resident system and the encounter subsystem, and the number of
+ * kernels they launched, since the last call with reset != 0 (which zeroes
+ * both). No counterpart in the reference. */
 int mercury_b200_dropin_time(double* ms, int64_t* launches, int reset);
 /* Launch shape of the particle kernel: threads per CTA (multiple of 32) and
  * steps fused per launch (0 = automatic); a negative value keeps the setting. */

@@ -121,16 +121,20 @@ int reorder_slots(int src, double h, cudaStream_t st);
 
 bool is_mvs(int alg) { return alg == 1 || alg == 9; }
 
+// Device time of the drop-in calls (both contexts) and the kernels they
+// launched, since the last reset.
+double g_dropin_ms = 0.0;
+
 // Adds the device time of one drop-in call (CUDA events on the library
-// stream around it) to the context's total.
+// stream around it) to the total.
 struct DropinTimer {
-    DropinTimer() { check(cudaEventRecord(ctx().d0, ctx().stream), "event"); }
+    Context& c;
+    DropinTimer() : c(ctx()) { check(cudaEventRecord(c.d0, c.stream), "event"); }
     ~DropinTimer() {
-        Context& c = ctx();
         float ms = 0.0f;
         if (cudaEventRecord(c.d1, c.stream) == cudaSuccess && cudaEventSynchronize(c.d1) == cudaSuccess &&
             cudaEventElapsedTime(&ms, c.d0, c.d1) == cudaSuccess)
-            c.dropin_ms += ms;
+            g_dropin_ms += ms;
     }
 };
 
@@ -1234,6 +1238,7 @@ int mercury_cuda_hybrid_begin(double h, const double* crit, int flag, int cap, i
     try {
         require_system();
         if (c.algorithm != 10) throw std::runtime_error("hybrid_begin needs algorithm 10");
+        DropinTimer timer;
         const int nb = c.nbig - 1, ns = c.nsplit;
         c.rcritbig.reserve(ns);
         c.hy_scr.reserve((size_t)6 * ns);
@@ -1313,6 +1318,7 @@ int mercury_cuda_hybrid_finish(double h, const double* m, const double* xx, cons
     try {
         require_system();
         if (!c.hy_begun) throw std::runtime_error("hybrid_finish without hybrid_begin");
+        DropinTimer timer;
         const int nm = (int)c.hy_members.size();
         const int out = 1 - c.cur;
         if (nm) {
@@ -1582,12 +1588,12 @@ int mercury_b200_timing(double* advance_ms, double* particle_kernel_ms, int* par
 }
 
 int mercury_b200_dropin_time(double* ms, int64_t* launches, int reset) {
-    Context& c = ctx();
-    if (ms) *ms = c.dropin_ms;
-    if (launches) *launches = c.dropin_launches;
+    if (ms) *ms = g_dropin_ms;
+    if (launches) *launches = g_contexts[0].dropin_launches + g_contexts[1].dropin_launches;
     if (reset) {
-        c.dropin_ms = 0.0;
-        c.dropin_launches = 0;
+        g_dropin_ms = 0.0;
+        g_contexts[0].dropin_launches = 0;
+        g_contexts[1].dropin_launches = 0;
     }
     return 0;
 }

@@ -121,10 +121,8 @@ struct Context {
     int last_particle_launches = 0;
     int last_kernel_launches = 0;   // every kernel of the last advance (all streams)
     int64_t nforces = 0;
-    // device time (CUDA events on the library stream) of the drop-in step and
-    // events calls, and the kernels they launched, since the last reset
+    // timing events of the drop-in calls, and the kernels they launched
     cudaEvent_t d0 = nullptr, d1 = nullptr;
-    double dropin_ms = 0.0;
     int64_t dropin_launches = 0;
     int particle_threads = 128;
     int steps_per_launch = 0;   // 0 = automatic
