@@ -438,6 +438,7 @@ void bs_step_once(double time, double* h, double* hdid, double tol, int64_t* rej
         a.rcrit = c.rcritbig.p;
         a.adj_off = c.adj_off.p;
         a.adj = c.adj.p;
+        a.perm = c.permp();
         launch_bs_sequence(a, c.stream);
         c.dropin_launches += 1 + (c.np > 0 ? 1 : 0);
         check(cudaGetLastError(), "launch");
@@ -964,8 +965,8 @@ int mercury_cuda_upload(int n, int nbig, int pn, int ngflag, const double* m, co
         int nmass = nbig;
         for (int j = nbig; j < n; ++j)
             if (m[j] != 0.0) nmass = j + 1;
-        const int ns = c.encounter ? n : is_mvs(c.algorithm) ? nbig : nmass;
-        if (ns > 512 && !c.encounter) throw std::runtime_error("more than 512 Big and massive Small bodies");
+        const int ns = is_mvs(c.algorithm) ? nbig : nmass;
+        if (ns > 512) throw std::runtime_error("more than 512 Big and massive Small bodies");
         c.n = n;
         c.nbig = nbig;
         c.nmass = nmass;
@@ -1373,8 +1374,12 @@ int mercury_cuda_encounter_enter(int n, int nb, const double* m, const double* x
         const double jc[3] = {0.0, 0.0, 0.0};
         if (mercury_cuda_upload(n, nb, 0, 0, m, xx, vv, zero.data(), jc, limits, radii))
             throw std::runtime_error("Encounter upload failed");
-        c.rcritbig.reserve(n);
-        check(cudaMemcpy(c.rcritbig.p, crit, sizeof(double) * n, cudaMemcpyHostToDevice), "upload");
+        // rcrit of the massive set and the particle slots' constant row
+        c.rcritbig.reserve(c.nsplit);
+        check(cudaMemcpyAsync(c.transfer.p, crit, sizeof(double) * n, cudaMemcpyHostToDevice, c.stream), "upload");
+        scatter_rows(c.transfer.p, n, 1, c.nsplit, c.rcritbig.p, c.nsplit,
+                     c.pconst[c.kc].p + (size_t)PC_RCRIT * c.npcap, c.npcap, c.inv.p, c.stream);
+        check(cudaStreamSynchronize(c.stream), "upload");
         // per-body pair lists in pair order (mfo_hkce's accumulation order)
         std::vector<int> off(n + 1, 0);
         for (int k = 0; k < np; ++k) {

@@ -35,33 +35,50 @@ __device__ __forceinline__ bool body_error(const double* q, double xscal, double
     return true;
 }
 
-// mfo_hkce for body k (mercury6_2.for:4868-4905): the inner changeover
-// 1 - K(r) over k's pairs in pair-list order, then the central attraction.
+// The pair term of mfo_hkce (mercury6_2.for:4875-4894): 1 - K(r) inside rc,
+// nothing outside; false when the pair is outside rc.
+__device__ __forceinline__ bool hkce_pair(double s2, double rc, double& tmp2) {
+    const double rc2 = rc * rc;
+    if (!(s2 < rc2)) return false;
+    const double s_1 = 1.0 / sqrt(s2);
+    const double s_3 = s_1 * s_1 * s_1;
+    if (s2 <= 0.01 * rc2) {
+        tmp2 = s_3;
+    } else {
+        const double s = 1.0 / s_1;
+        const double q = (s - 0.1 * rc) / (0.9 * rc);
+        const double q2 = q * q, q3 = q * q2, q4 = q2 * q2, q5 = q2 * q3;
+        tmp2 = (1.0 - 10.0 * q3 + 15.0 * q4 - 6.0 * q5) * s_3;
+    }
+    return true;
+}
+
+// mfo_hkce's central term (mercury6_2.for:4898-4905).
+__device__ __forceinline__ double3 hkce_central(double3 a, const double3 x, double m0) {
+    const double s2 = x.x * x.x + x.y * x.y + x.z * x.z;
+    const double s_1 = 1.0 / sqrt(s2);
+    const double tmp2 = m0 * s_1 * s_1 * s_1;
+    a.x = a.x - tmp2 * x.x;
+    a.y = a.y - tmp2 * x.y;
+    a.z = a.z - tmp2 * x.z;
+    return a;
+}
+
+// mfo_hkce for body k of the massive set: its pairs with massive partners in
+// pair-list order (a massless partner adds exactly zero), then the central
+// attraction.
 __device__ double3 hkce_force(const BsArgs& A, int k, const double* X) {
     const int N = A.f.nsplit;
     const double* m = A.mbig;
-    const double3 xk = make_double3(X[k], X[N + k], X[2 * N + k]);
     double3 a = make_double3(0.0, 0.0, 0.0);
     for (int e = A.adj_off[k]; e < A.adj_off[k + 1]; ++e) {
         const int q = A.adj[e].x;
+        if (q >= N) continue;
         const bool first = A.adj[e].y == 0;
         const int i = first ? k : q, j = first ? q : k;
         const double dx = X[j] - X[i], dy = X[N + j] - X[N + i], dz = X[2 * N + j] - X[2 * N + i];
-        const double s2 = dx * dx + dy * dy + dz * dz;
-        const double rc = fmax(A.rcrit[i], A.rcrit[j]);
-        const double rc2 = rc * rc;
-        if (!(s2 < rc2)) continue;
-        const double s_1 = 1.0 / sqrt(s2);
-        const double s_3 = s_1 * s_1 * s_1;
         double tmp2;
-        if (s2 <= 0.01 * rc2) {
-            tmp2 = s_3;
-        } else {
-            const double s = 1.0 / s_1;
-            const double qq = (s - 0.1 * rc) / (0.9 * rc);
-            const double q2 = qq * qq, q3 = qq * q2, q4 = q2 * q2, q5 = q2 * q3;
-            tmp2 = (1.0 - 10.0 * q3 + 15.0 * q4 - 6.0 * q5) * s_3;
-        }
+        if (!hkce_pair(dx * dx + dy * dy + dz * dz, fmax(A.rcrit[i], A.rcrit[j]), tmp2)) continue;
         if (first) {
             const double facj = tmp2 * m[j];
             a.x = a.x + facj * dx;
@@ -74,13 +91,25 @@ __device__ double3 hkce_force(const BsArgs& A, int k, const double* X) {
             a.z = a.z - faci * dz;
         }
     }
-    const double s2 = xk.x * xk.x + xk.y * xk.y + xk.z * xk.z;
-    const double s_1 = 1.0 / sqrt(s2);
-    const double tmp2 = A.f.m0 * s_1 * s_1 * s_1;
-    a.x = a.x - tmp2 * xk.x;
-    a.y = a.y - tmp2 * xk.y;
-    a.z = a.z - tmp2 * xk.z;
-    return a;
+    return hkce_central(a, make_double3(X[k], X[N + k], X[2 * N + k]), A.f.m0);
+}
+
+// mfo_hkce for a massless member (subsystem index g) against table row T:
+// every pair has a Big first body i, whose position is in the row.
+__device__ double3 hkce_particle_force(const BsArgs& A, int g, const double3 x, double rcrit_p, const double* T) {
+    double3 a = make_double3(0.0, 0.0, 0.0);
+    for (int e = A.adj_off[g]; e < A.adj_off[g + 1]; ++e) {
+        const int i = A.adj[e].x;
+        const double* row = T + FT_HEAD + 4 * (i - 1);
+        const double dx = x.x - row[0], dy = x.y - row[1], dz = x.z - row[2];
+        double tmp2;
+        if (!hkce_pair(dx * dx + dy * dy + dz * dz, fmax(A.rcrit[i], rcrit_p), tmp2)) continue;
+        const double faci = tmp2 * row[3];
+        a.x = a.x - faci * dx;
+        a.y = a.y - faci * dy;
+        a.z = a.z - faci * dz;
+    }
+    return hkce_central(a, x, A.f.m0);
 }
 
 // ------------------------------------------------------------ massive set
@@ -105,6 +134,10 @@ __device__ void massive_call(const BsArgs& A, const double* X, const double* V, 
     __syncthreads();
     if (A.hkce) {
         for (int k = 1 + threadIdx.x; k < N; k += blockDim.x) {
+            if (k < f.nbig) {
+                double* row = T + FT_HEAD + 4 * (k - 1);
+                row[0] = X[k]; row[1] = X[N + k]; row[2] = X[2 * N + k]; row[3] = A.mbig[k];
+            }
             const double3 a = hkce_force(A, k, X);
             out[k] = a.x; out[N + k] = a.y; out[2 * N + k] = a.z;
         }
@@ -273,6 +306,13 @@ template <int VARIANT> __global__ void __launch_bounds__(128) bs_particle_kernel
     auto D = [&](int j, int c) -> double& { return dcol[((j - 1) * 6 + c) * T + threadIdx.x]; };
     double3 x0 = make_double3(0.0, 0.0, 0.0), v0 = x0, a0 = x0;
     double xscal = 0.0, vscal = 0.0, mj = 0.0, g5[5] = {0, 0, 0, 0, 0};
+    // the encounter subsystem (BS2 only): mfo_hkce from the member's pairs
+    const bool hkce = VARIANT == 2 && A.hkce;
+    int g = 0;
+    double rcrit_p = 0.0;
+    auto force = [&](const double3 x, const double3 v, const double* Tr, DeviceStatus* st) {
+        return hkce ? hkce_particle_force(A, g, x, rcrit_p, Tr) : particle_allforce(x, v, Tr, nb, A.f, mj, g5, st);
+    };
     if (ok) {
         x0 = make_double3(A.px[p], A.px[S + p], A.px[2 * S + p]);
         v0 = make_double3(A.px[3 * S + p], A.px[4 * S + p], A.px[5 * S + p]);
@@ -282,7 +322,11 @@ template <int VARIANT> __global__ void __launch_bounds__(128) bs_particle_kernel
         const double tmp2 = v0.x * v0.x + v0.y * v0.y + v0.z * v0.z;
         xscal = 1.0 / fmax(tmp1, 1e-300);
         vscal = 1.0 / fmax(tmp2, 1e-300);
-        a0 = particle_allforce(x0, v0, A.table, nb, A.f, mj, g5, &A.lvst[0]);
+        if (hkce) {
+            g = A.f.nsplit + A.perm[p];
+            rcrit_p = A.pconst[(size_t)PC_RCRIT * S + p];
+        }
+        a0 = force(x0, v0, A.table, &A.lvst[0]);
     }
     int row = 1;
 #pragma unroll 1
@@ -292,7 +336,7 @@ template <int VARIANT> __global__ void __launch_bounds__(128) bs_particle_kernel
         const double h2n = level_h2<VARIANT>(A.h0, n);
         auto call = [&](const double3 x, const double3 v) {
             const double* Tr = A.table + (size_t)(row++) * stride;
-            return particle_allforce(x, v, Tr, nb, A.f, mj, g5, st);
+            return force(x, v, Tr, st);
         };
         if (ok) {
             if (VARIANT == 1) {

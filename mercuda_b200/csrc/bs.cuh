@@ -43,13 +43,17 @@ struct BsArgs {
     unsigned long long* errs;    // [13] max error of level n (bit pattern of a non-negative double; +inf
                                  // when an extrapolated value is not finite)
     DeviceStatus* lvst;          // [13] force faults of level n (0: the start-of-step force)
-    // mfo_hkce instead of mfo_all (the compact encounter subsystem, every body
-    // in the massive set): pairs of body k are adj[adj_off[k] .. adj_off[k+1])
-    // = {partner, 0 if k is the pair's first body else 1}, in pair-list order
+    // mfo_hkce instead of mfo_all (the compact encounter subsystem): pairs of
+    // body g (0-based subsystem index) are adj[adj_off[g] .. adj_off[g+1]) =
+    // {partner, 0 if g is the pair's first body else 1}, in pair-list order.
+    // A massless member's pairs all have a Big first body, and massless
+    // members add exactly zero to a massive body's sum, so the massive set and
+    // the particle slots split as for mfo_all.
     int hkce;
-    const double* rcrit;         // [nsplit]
+    const double* rcrit;         // [nsplit] massive set; particles use pconst row PC_RCRIT
     const int* adj_off;
     const int2* adj;
+    const int* perm;             // slot -> particle index
 };
 
 struct BsCommitArgs {

@@ -94,8 +94,9 @@ struct Context {
     DBuf<int> hy_ids;
     std::vector<int> hy_members;
     bool hy_begun = false;
-    // compact encounter subsystem: every body in the massive arrays, BS2 with
-    // mfo_hkce over the pair list (per-body adjacency in pair order)
+    // compact encounter subsystem: BS2 with mfo_hkce; massive members in the big
+    // arrays, massless members in particle slots; per-body pair lists in pair
+    // order (subsystem indices)
     bool encounter = false;
     DBuf<int> adj_off;
     DBuf<int2> adj;
