@@ -1380,21 +1380,25 @@ int mercury_cuda_encounter_enter(int n, int nb, const double* m, const double* x
         scatter_rows(c.transfer.p, n, 1, c.nsplit, c.rcritbig.p, c.nsplit,
                      c.pconst[c.kc].p + (size_t)PC_RCRIT * c.npcap, c.npcap, c.inv.p, c.stream);
         check(cudaStreamSynchronize(c.stream), "upload");
-        // per-body pair lists in pair order (mfo_hkce's accumulation order)
+        // per-body pair lists in pair order (mfo_hkce's accumulation order); a
+        // massive body's list leaves out massless partners, which add exactly
+        // zero to its sum
+        const int ns = c.nsplit;
+        auto keep = [&](int body, int partner) { return !(body < ns && partner >= ns); };
         std::vector<int> off(n + 1, 0);
         for (int k = 0; k < np; ++k) {
             const int i = pi[k] - 1, j = pj[k] - 1;
             if (i < 0 || j < 0 || i >= n || j >= n) throw std::runtime_error("encounter pair out of range");
-            ++off[i + 1];
-            ++off[j + 1];
+            if (keep(i, j)) ++off[i + 1];
+            if (keep(j, i)) ++off[j + 1];
         }
         for (int k = 0; k < n; ++k) off[k + 1] += off[k];
         std::vector<int> fill(off.begin(), off.end() - 1);
-        std::vector<int2> adj(std::max(1, 2 * np));
+        std::vector<int2> adj(std::max(1, off[n]));
         for (int k = 0; k < np; ++k) {
             const int i = pi[k] - 1, j = pj[k] - 1;
-            adj[fill[i]++] = make_int2(j, 0);
-            adj[fill[j]++] = make_int2(i, 1);
+            if (keep(i, j)) adj[fill[i]++] = make_int2(j, 0);
+            if (keep(j, i)) adj[fill[j]++] = make_int2(i, 1);
         }
         c.adj_off.reserve(n + 1);
         c.adj.reserve(adj.size());

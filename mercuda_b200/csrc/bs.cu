@@ -65,8 +65,8 @@ __device__ __forceinline__ double3 hkce_central(double3 a, const double3 x, doub
 }
 
 // mfo_hkce for body k of the massive set: its pairs with massive partners in
-// pair-list order (a massless partner adds exactly zero), then the central
-// attraction.
+// pair-list order (massless partners, which add exactly zero, are not in its
+// list), then the central attraction.
 __device__ double3 hkce_force(const BsArgs& A, int k, const double* X) {
     const int N = A.f.nsplit;
     const double* m = A.mbig;
