@@ -20,6 +20,11 @@ _finish, the encounter members' BS2 subsystem driven as mdt_hkce drives it,
 central-impact screen every step) on the MVS workload's system, rcrit from
 mce_init (cefac 3); a step is one HYBRID step.
 
+--workload batch measures the batched extension: 4096 independent systems
+(1-8 planets, log-uniform 10-5000 particles, h uniform 4-16 d, 3.3M particles
+in all) advanced together; the plain loop over systems through the
+single-system path is timed on a sample beside it.
+
 --workload radau|bs|bs2 measures the adaptive integrators instead (mdt_ra15,
 mdt_bs1, mdt_bs2 through the drop-in step/events calls, as mal_hvar drives
 them) on the 100,000-particle system of the same generator with 1PN,
@@ -75,7 +80,8 @@ def parse_args():
     p.add_argument("--threads", type=int, default=0)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", default="mvs", choices=["mvs", "radau", "bs", "bs2", "hybrid"])
+    p.add_argument("--workload", default="mvs", choices=["mvs", "radau", "bs", "bs2", "hybrid", "batch"])
+    p.add_argument("--systems", type=int, default=4096)
     args = p.parse_args()
     if args.workload in ADAPTIVE and args.particles == 1_000_000:
         args.particles = 100_000
@@ -403,6 +409,117 @@ def run_hybrid(args, rank, world, dist):
     b.free()
 
 
+def run_batch(args, rank, world, dist):
+    from mercuda_b200.system import make_batch
+    metric = "batched MVS particle-steps/s"
+    systems, hs = make_batch(seed=args.seed + 100 * rank, nsys=args.systems)
+    total = sum(s.n - s.nbig for s in systems)
+    workload_text = (f"batched MVS, {args.systems} systems per GPU, 1-8 planets, 10-5000 particles log-uniform "
+                     f"({total} particles), h U[4,16] d, encounter + central screens every step")
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        from oracle import oracle as O
+        cores = os.cpu_count() or 1
+        sample = systems[:: max(1, len(systems) // 256)]
+        t0 = time.perf_counter()
+        done = 0
+        for sys_, h_ in zip(sample, hs[:: max(1, len(systems) // 256)]):
+            O.mvs_run(sys_, 0.0, float(h_), args.steps, RCEN, central=True, threads=cores)
+            done += (sys_.n - sys_.nbig) * args.steps
+        dt = time.perf_counter() - t0
+        value = done / dt
+        print(json.dumps({"impl": "reference", "metric": metric, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+                          "steps": args.steps, "warmup": 0, "ms_per_step": dt * 1e3 / args.steps,
+                          "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                          "data": "synthetic", "config": {"workload": workload_text, "systems_sampled": len(sample)},
+                          "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                                           "sample": f"{len(sample)} of the systems x {args.steps} steps"},
+                          "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
+              flush=True)
+        return
+    import torch
+    from mercuda_b200.backend import Backend, Batch
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    b = Batch(systems, hs)
+    b.advance(0.0, max(1, args.warmup), RCEN)
+    barrier()
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clocks:
+        ev, _, _ = b.advance(0.0, args.steps, RCEN)
+    barrier()
+    tm = b.timing()
+    ms = tm["ms"]
+    if dist:
+        tt = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    value = world * total * args.steps / (ms * 1e-3)
+    e2e = None
+    if not args.no_e2e:
+        barrier()
+        t0 = time.perf_counter()
+        b2 = Batch(systems, hs)
+        b2.advance(0.0, args.steps, RCEN)
+        b2.download()
+        barrier()
+        e2e_s = time.perf_counter() - t0
+        if dist:
+            tt = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            e2e_s = float(tt.item())
+        nb = sum(s.n for s in systems)
+        e2e = {"value": world * total * args.steps / e2e_s, "unit": UNIT,
+               "h2d_bytes_per_step": nb * (3 + 3 + 1 + 1 + 1) * 8 / args.steps,
+               "d2h_bytes_per_step": nb * 48 / args.steps,
+               "note": "wall clock around the batched upload, advance (events included) and download"}
+    b.free()
+    # the plain loop: every system through the single-system path in turn
+    stride = max(1, len(systems) // 128)
+    sample = list(zip(systems[::stride], hs[::stride]))
+    barrier()
+    t0 = time.perf_counter()
+    for sys_, h_ in sample:
+        be = Backend("MVS")
+        be.configure()
+        be.upload(sys_)
+        be.mvs_advance(0.0, float(h_), args.steps, RCEN)
+        be.download()
+    barrier()
+    loop_s = (time.perf_counter() - t0) * len(systems) / len(sample)
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        from oracle import oracle as O
+        cores = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        done = 0
+        for sys_, h_ in sample[:32]:
+            O.mvs_run(sys_.copy(), 0.0, float(h_), args.steps, RCEN, central=True, threads=cores)
+            done += (sys_.n - sys_.nbig) * args.steps
+        dt = time.perf_counter() - t0
+        cpu = {"value": done / dt, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"32 of the systems x {args.steps} steps ({dt:.1f} s)"}
+    if rank == 0:
+        batch_s = (total * args.steps / e2e["value"]) if e2e else ms * 1e-3
+        print(json.dumps({"metric": metric, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                          "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+                          "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                          "config": {"workload": workload_text, "systems_per_gpu": args.systems,
+                                     "particles_per_gpu": total, "threads_per_cta": tm["threads"],
+                                     "steps_per_launch": tm["steps_per_launch"],
+                                     "plain_loop_s_estimated": loop_s,
+                                     "batched_e2e_s": batch_s,
+                                     "speedup_vs_plain_loop": loop_s / batch_s,
+                                     "loop_sample_systems": len(sample)},
+                          "clocks": clocks.summary(), "gpu_launches": tm["launches"], "events": int(len(ev)),
+                          "e2e": e2e, "cpu_baseline": cpu}), flush=True)
+
+
 def main():
     args = parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -422,6 +539,8 @@ def main():
             torch.cuda.set_device(local)
         if args.workload == "hybrid":
             run_hybrid(args, rank, world, dist)
+        elif args.workload == "batch":
+            run_batch(args, rank, world, dist)
         else:
             run_adaptive(args, rank, world, dist)
         if dist:

@@ -39,6 +39,36 @@ int mercury_b200_set_launch(int particle_threads, int steps_per_launch);
  * FMA), best of five launches of independent fma() chains on every SM. */
 int mercury_b200_fp64_peak(double* tflops, double* ms);
 
+/* ---- Batched systems (no counterpart in the reference, which integrates one
+ * system per process). Thousands of independent MVS systems advance together:
+ * system s owns bodies [body_offset[s], body_offset[s+1]) of the concatenated
+ * host arrays (Fortran layout as in mercury_cuda_upload: m in K2 units, x/v
+ * (n,3) rows, rce/rphys per body), its central body first, then nbig[s]-1 Big
+ * bodies, then massless Small bodies; h[s] is its step. No non-gravitational
+ * forces, no oblateness; nbig[s] <= 32. The upload replaces any previous
+ * batch and resets every system's cached acceleration. */
+int mercury_b200_batch_upload(int nsys, const int* body_offset, const int* nbig, const double* h,
+                              const double* m, const double* x, const double* v, const double* rce,
+                              const double* rphys);
+/* nsteps MVS steps of every system (mdt_mvs with mce_stat and mce_cent at
+ * radius rcen every step; system s's clock runs time, time + h[s], ...).
+ * *nevents receives the number of event records, fetched with
+ * mercury_b200_batch_events. */
+int mercury_b200_batch_advance(double time, int nsteps, double rcen, int* nevents);
+/* Copy up to cap records of the last advance, sorted by (system, step,
+ * min(i,j), max(i,j)); ids are 1-based within the system; sys/steps (may be
+ * null) receive each record's system and 0-based step. Returns the total. */
+int mercury_b200_batch_events(MercuryEvent* events, int* sys, int* steps, int cap);
+/* Current state of every body into the concatenated host arrays x, v. */
+int mercury_b200_batch_download(double* x, double* v);
+/* Launch shape: particle CTA size (64, 128 or 256; 0 = tune on the next
+ * advance), steps per launch (0 = automatic), CUDA-graph replay of the
+ * chunk loop (1/0); a negative value keeps the setting. */
+int mercury_b200_batch_set(int threads, int steps_per_launch, int use_graph);
+/* Device time and kernel count of the last advance, and the launch shape it used. */
+int mercury_b200_batch_timing(double* ms, int* launches, int* threads, int* steps_per_launch);
+void mercury_b200_batch_free(void);
+
 /* One MVS step (kick, drift, mce_stat pair screen, kick) of a system whose
  * arrays the caller already holds on the current device, with no device
  * allocation: for hosts that cannot call cudaMalloc (device memory owned by

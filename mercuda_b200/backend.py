@@ -46,7 +46,9 @@ DROP_IN_SYMBOLS = [
 ]
 EXTENSION_SYMBOLS = ["mercury_b200_mvs_advance", "mercury_b200_events", "mercury_b200_timing",
                      "mercury_b200_set_launch", "mercury_b200_fp64_peak", "mercury_b200_mvs_step_noalloc",
-                     "mercury_b200_dropin_time"]
+                     "mercury_b200_dropin_time", "mercury_b200_batch_upload", "mercury_b200_batch_advance",
+                     "mercury_b200_batch_events", "mercury_b200_batch_download", "mercury_b200_batch_set",
+                     "mercury_b200_batch_timing", "mercury_b200_batch_free"]
 
 
 class BackendError(RuntimeError):
@@ -88,6 +90,13 @@ def load_library(path: Path | str | None = None) -> C.CDLL:
     L.mercury_b200_set_launch.argtypes = [I, I]
     L.mercury_b200_fp64_peak.argtypes = [PD, PD]
     L.mercury_b200_dropin_time.argtypes = [PD, PI64, I]
+    L.mercury_b200_batch_upload.argtypes = [I, PI, PI, PD, PD, PD, PD, PD, PD]
+    L.mercury_b200_batch_advance.argtypes = [D, I, D, PI]
+    L.mercury_b200_batch_events.argtypes = [C.c_void_p, PI, PI, I]
+    L.mercury_b200_batch_download.argtypes = [PD, PD]
+    L.mercury_b200_batch_set.argtypes = [I, I, I]
+    L.mercury_b200_batch_timing.argtypes = [PD, PI, PI, PI]
+    L.mercury_b200_batch_free.restype = None
     VP = C.c_void_p
     L.mercury_b200_mvs_step_noalloc.argtypes = [I, I, VP, VP, VP, VP, VP, VP, VP, VP, VP, I, D, D, I, VP, I,
                                                 PI, VP]
@@ -333,3 +342,60 @@ class Backend:
     def set_launch(self, threads: int = -1, steps_per_launch: int = -1) -> None:
         if self.lib.mercury_b200_set_launch(int(threads), int(steps_per_launch)) != 0:
             raise BackendError("invalid launch shape")
+
+
+class Batch:
+    """Batched MVS systems (the mercury_b200_batch_* extension): many
+    independent systems, each with its own Big bodies, particles and step,
+    advanced together. Systems are given as System objects (massless Small
+    bodies, no non-gravitational forces, no oblateness)."""
+
+    def __init__(self, systems, h, lib: C.CDLL | None = None):
+        self.lib = lib or load_library()
+        self.systems = list(systems)
+        self.h = np.ascontiguousarray(h, dtype=np.float64)
+        sizes = [s.n for s in self.systems]
+        self.offsets = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int32)
+        self.nbig = np.array([s.nbig for s in self.systems], dtype=np.int32)
+        cat = lambda name: np.ascontiguousarray(np.concatenate([getattr(s, name) for s in self.systems]))
+        self.m, self.x, self.v = cat("m"), cat("x"), cat("v")
+        self.rce, self.rphys = cat("rce"), cat("rphys")
+        rc = self.lib.mercury_b200_batch_upload(len(self.systems), self.offsets.ctypes.data_as(PI),
+                                                self.nbig.ctypes.data_as(PI), _p(self.h), _p(self.m), _p(self.x),
+                                                _p(self.v), _p(self.rce), _p(self.rphys))
+        if rc != 0:
+            raise BackendError("batched upload failed")
+
+    def set(self, threads: int = -1, steps_per_launch: int = -1, graph: int = -1) -> None:
+        if self.lib.mercury_b200_batch_set(int(threads), int(steps_per_launch), int(graph)) != 0:
+            raise BackendError("invalid batched launch shape")
+
+    def advance(self, time: float, nsteps: int, rcen: float):
+        """Returns (events, system of each, step of each)."""
+        nev = I(0)
+        if self.lib.mercury_b200_batch_advance(time, int(nsteps), rcen, C.byref(nev)) != 0:
+            raise BackendError("batched advance failed")
+        ev = np.zeros(nev.value, dtype=EVENT_DTYPE)
+        sy = np.zeros(nev.value, dtype=np.int32)
+        st = np.zeros(nev.value, dtype=np.int32)
+        if nev.value:
+            self.lib.mercury_b200_batch_events(ev.ctypes.data_as(C.c_void_p), sy.ctypes.data_as(PI),
+                                               st.ctypes.data_as(PI), nev.value)
+        return ev, sy, st
+
+    def download(self):
+        """(x, v) of every system, as a list of (n_s, 3) array pairs."""
+        x = np.zeros_like(self.x)
+        v = np.zeros_like(self.v)
+        if self.lib.mercury_b200_batch_download(_p(x), _p(v)) != 0:
+            raise BackendError("batched download failed")
+        o = self.offsets
+        return [(x[o[k]:o[k + 1]], v[o[k]:o[k + 1]]) for k in range(len(self.systems))]
+
+    def timing(self):
+        ms, n, t, k = D(0.0), I(0), I(0), I(0)
+        self.lib.mercury_b200_batch_timing(C.byref(ms), C.byref(n), C.byref(t), C.byref(k))
+        return {"ms": ms.value, "launches": n.value, "threads": t.value, "steps_per_launch": k.value}
+
+    def free(self) -> None:
+        self.lib.mercury_b200_batch_free()

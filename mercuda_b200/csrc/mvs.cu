@@ -271,8 +271,8 @@ __device__ void big_load(const MvsBigArgs& A, BigSmem& S, double* smem) {
     __syncthreads();
 }
 
-__global__ void __launch_bounds__(128) mvs_big_kernel(MvsBigArgs A) {
-    extern __shared__ double smem[];
+// The Big-body integrator of one system (all threads of the CTA).
+__device__ void big_run(const MvsBigArgs& A, double* smem) {
     const int nbig = A.nbig, N = nbig, nb = nbig - 1, tid = threadIdx.x, nt = blockDim.x;
     const int stride = tab_stride(nb);
     BigSmem S;
@@ -342,6 +342,7 @@ __global__ void __launch_bounds__(128) mvs_big_kernel(MvsBigArgs A) {
                 if (slot < A.event_cap) {
                     pair_record(A.events + slot, I, J, pc, hm1, i + 1, j + 1, A.m[j] > A.m[i]);
                     A.event_step[slot] = A.step0 + s;
+                    if (A.event_sys) A.event_sys[slot] = A.sys;
                 } else {
                     atomicExch(&A.status->overflow, 1);
                 }
@@ -371,6 +372,7 @@ __global__ void __launch_bounds__(128) mvs_big_kernel(MvsBigArgs A) {
                         rec.distance = A.rcen;
                         store_event(A.events + slot, rec);
                         A.event_step[slot] = A.step0 + s;
+                        if (A.event_sys) A.event_sys[slot] = A.sys;
                     } else {
                         atomicExch(&A.status->overflow, 1);
                     }
@@ -384,6 +386,11 @@ __global__ void __launch_bounds__(128) mvs_big_kernel(MvsBigArgs A) {
             A.out.v[c * N + k] = S.V[c * N + k];
             A.out.a[c * N + k] = S.ACC[c * N + k];
         }
+}
+
+__global__ void __launch_bounds__(128) mvs_big_kernel(MvsBigArgs A) {
+    extern __shared__ double smem[];
+    big_run(A, smem);
 }
 
 // ------------------------------------------------------------ test particles
@@ -735,6 +742,161 @@ __global__ void __launch_bounds__(256) classify_kernel(ClassifyArgs A) {
     }
 }
 
+// ------------------------------------------------------------ batched systems
+__global__ void __launch_bounds__(32) mvs_big_batch_kernel(BatchBigArgs B) {
+    extern __shared__ double smem[];
+    const int q = blockIdx.x;
+    MvsBigArgs A = B.proto[q];
+    if (B.flip) {
+        const BigState t = A.in;
+        A.in = A.out;
+        A.out = t;
+    }
+    A.nsteps = B.nsteps;
+    A.reset = B.reset;
+    A.central = B.central;
+    A.step0 = B.step0;
+    A.rcen = B.rcen;
+    A.tab = B.tab + B.sys[q].tab_off;
+    A.detail = B.detail + B.sys[q].det_off;
+    A.events = B.events;
+    A.event_step = B.event_step;
+    A.event_sys = B.event_sys;
+    A.event_cap = B.event_cap;
+    A.status = B.status;
+    A.sys = q;
+    big_run(A, smem);
+}
+
+// One mdt_mvs step of one test particle of a batched system against its
+// step table T (the same statements as particle_step).
+template <bool CENTRAL>
+__device__ __forceinline__ void batch_particle_step(double3& x, double3& v, double3& acc, bool ok, int p, int sysid,
+                                                    const BatchSys& S, const double* T, int s,
+                                                    const BatchParticleArgs& A, double rce, double rphys, int id) {
+    const int nb = S.nb;
+    const double h = S.h, hby2 = 0.5 * h;
+    double bxlo = 0.0, bxhi = 0.0, bylo = 0.0, byhi = 0.0;
+    double3 x0 = x, v0 = v;
+    CentralStart c0{0.0, 0.0, 0.0, 0.0};
+    if (ok) {
+        if (CENTRAL) c0 = central_start(x, v);
+        v.x = v.x + hby2 * acc.x;
+        v.y = v.y + hby2 * acc.y;
+        v.z = v.z + hby2 * acc.z;
+        x0 = x;
+        v0 = v;
+        drift_one(S.mu, x, v, h);
+        box_extent(x0.x, x.x, v0.x, v.x, h, bxlo, bxhi);
+        box_extent(x0.y, x.y, v0.y, v.y, h, bylo, byhi);
+        const double pad = rce * 1.2;
+        bxlo = bxlo - pad;
+        bxhi = bxhi + pad;
+        bylo = bylo - pad;
+        byhi = byhi + pad;
+    }
+#pragma unroll 1
+    for (int b = 0; b < nb; ++b) {
+        const double* row = T + TAB_HEAD + b * TAB_BODY;
+        const bool cand = ok && row[5] >= bxlo && bxhi >= row[4] && row[7] >= bylo && byhi >= row[6];
+        if (__any_sync(FULL, cand)) {
+            const int slot = claim_slot(cand, A.cand_cap, A.status, &A.status->cands, 2);
+            if (slot >= 0) {
+                EncounterCandidate* c = A.cands + slot;
+                *reinterpret_cast<int4*>(c) = make_int4(sysid, b, A.step0 + s, id);
+                double2* w = reinterpret_cast<double2*>(c);
+                w[1] = make_double2(rce, rphys);
+                w[2] = make_double2(x0.x, x0.y);
+                w[3] = make_double2(x0.z, v0.x);
+                w[4] = make_double2(v0.y, v0.z);
+                w[5] = make_double2(x.x, x.y);
+                w[6] = make_double2(x.z, v.x);
+                w[7] = make_double2(v.y, v.z);
+            }
+        }
+    }
+    if (ok) {
+        acc = small_body_force<false, false>(x, v, [](int) -> double { return 0.0; }, T, nb, nullptr, S.mu,
+                                             A.status);
+        v.x = v.x + hby2 * acc.x;
+        v.y = v.y + hby2 * acc.y;
+        v.z = v.z + hby2 * acc.z;
+    }
+    if (CENTRAL) {
+        double temp = 0.0;
+        bool hit = false;
+        if (ok) hit = central_finish(c0, x, v, S.mu, 0.0, h, A.rcen, temp);
+        const int slot = claim_slot(hit, A.event_cap, A.status, &A.status->events, 1);
+        if (slot >= 0) {
+            MercuryEvent* e = A.events + slot;
+            *reinterpret_cast<int4*>(e) = make_int4(1, id, EV_CENTRAL, 0);
+            reinterpret_cast<double2*>(e)[1] = make_double2(A.rcen, temp);
+            A.event_step[slot] = A.step0 + s;
+            A.event_sys[slot] = sysid;
+        }
+    }
+    (void)p;
+}
+
+// Every test particle of every system: warps claim 32-slot tiles (each of a
+// single system) from a launch-wide counter and run K steps per particle in
+// registers; the step tables are read through the cache.
+template <bool CENTRAL> __global__ void __launch_bounds__(256) mvs_particle_batch_kernel(BatchParticleArgs A) {
+    const int lane = threadIdx.x & 31, S2 = A.npcap;
+    for (;;) {
+        int tile = 0;
+        if (lane == 0) tile = atomicAdd(&A.status->next_tile, 1);
+        tile = __shfl_sync(FULL, tile, 0);
+        if (tile >= A.ntiles) break;
+        const BatchTile t = A.tiles[tile];
+        const BatchSys S = A.sys[t.sys];
+        const bool ok = lane < t.count;
+        const int p = t.first + (ok ? lane : 0);
+        const int stride = tab_stride(S.nb);
+        const double* tab = A.tab + S.tab_off;
+        double3 x = ld3(A.xin, S2, p), v = ld3(A.xin + 3 * (size_t)S2, S2, p);
+        double3 acc = ld3(A.xin + 6 * (size_t)S2, S2, p);
+        const double rce = A.rce[p], rphys = A.rphys[p];
+        const int id = S.nbig + A.local[p] + 1;
+        if (A.reset && ok)
+            acc = small_body_force<false, false>(x, v, [](int) -> double { return 0.0; }, tab, S.nb, nullptr, S.mu,
+                                                 A.status);
+#pragma unroll 1
+        for (int s = 0; s < A.nsteps; ++s)
+            batch_particle_step<CENTRAL>(x, v, acc, ok, p, t.sys, S, tab + (size_t)(s + 1) * stride, s, A, rce,
+                                         rphys, id);
+        if (ok) {
+            st3(A.xout, S2, p, x);
+            st3(A.xout + 3 * (size_t)S2, S2, p, v);
+            st3(A.xout + 6 * (size_t)S2, S2, p, acc);
+        }
+    }
+}
+
+// mce_stat's test for the candidates of the last batched launch.
+__global__ void __launch_bounds__(256) classify_batch_kernel(BatchParticleArgs A) {
+    const int count = min(A.status->cands, A.cand_cap);
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
+        const EncounterCandidate& c = A.cands[k];
+        const BatchSys S = A.sys[c.slot];
+        const double* d = A.detail + S.det_off + ((size_t)(c.step - A.step0) * S.nb + c.body) * TAB_DETAIL;
+        const PairEnds I{make_double3(d[0], d[1], d[2]), make_double3(d[3], d[4], d[5]),
+                         make_double3(d[6], d[7], d[8]), make_double3(d[9], d[10], d[11])};
+        const PairEnds J{make_double3(c.x0[0], c.x0[1], c.x0[2]), make_double3(c.v0[0], c.v0[1], c.v0[2]),
+                         make_double3(c.x1[0], c.x1[1], c.x1[2]), make_double3(c.v1[0], c.v1[1], c.v1[2])};
+        PairClass pc;
+        if (!pair_classify(I, J, d[12], c.rce, d[13], c.rphys, S.h, pc)) continue;
+        const int slot = atomicAdd(&A.status->events, 1);
+        if (slot < A.event_cap) {
+            pair_record(A.events + slot, I, J, pc, 1.0 / S.h, c.body + 2, c.id, false);
+            A.event_step[slot] = c.step;
+            A.event_sys[slot] = c.slot;
+        } else {
+            atomicOr(&A.status->overflow, 1);
+        }
+    }
+}
+
 template <bool NGF, bool OBL, bool CENTRAL>
 void launch_variant(const MvsParticleArgs& a, cudaStream_t s, int threads) {
     auto kern = mvs_particle_kernel<NGF, OBL, CENTRAL>;
@@ -787,6 +949,36 @@ void launch_mvs_corrector(const MvsBigArgs& big, const CorrectorArgs& a, cudaStr
         if (a.obl) mvs_corrector_particle_kernel<false, true><<<grid, 128, 0, s>>>(a);
         else mvs_corrector_particle_kernel<false, false><<<grid, 128, 0, s>>>(a);
     }
+}
+
+void launch_mvs_big_batch(const BatchBigArgs& a, int nsys, int max_nbig, cudaStream_t s) {
+    const size_t smem = sizeof(double) * ((size_t)12 * 3 * max_nbig + max_nbig + 16);
+    if (smem > 48 * 1024)
+        cudaFuncSetAttribute(mvs_big_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (nsys > 0) mvs_big_batch_kernel<<<nsys, 32, smem, s>>>(a);
+}
+
+void launch_mvs_particles_batch(const BatchParticleArgs& a, cudaStream_t s, int threads) {
+    if (a.ntiles <= 0) return;
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (a.central) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mvs_particle_batch_kernel<true>, threads, 0);
+    } else {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mvs_particle_batch_kernel<false>, threads, 0);
+    }
+    if (per_sm < 1) per_sm = 1;
+    const int warps = threads / 32;
+    const int want = (a.ntiles + warps - 1) / warps;
+    const int slots = sms * per_sm;
+    const int grid = want < slots ? want : slots;
+    if (a.central) mvs_particle_batch_kernel<true><<<grid, threads, 0, s>>>(a);
+    else mvs_particle_batch_kernel<false><<<grid, threads, 0, s>>>(a);
+}
+
+void launch_classify_batch(const BatchParticleArgs& a, cudaStream_t s) {
+    classify_batch_kernel<<<296, 256, 0, s>>>(a);
 }
 
 void launch_classify(const ClassifyArgs& a, cudaStream_t s) {

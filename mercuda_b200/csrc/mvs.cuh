@@ -51,6 +51,8 @@ struct MvsBigArgs {
     int* event_step;
     int event_cap;
     DeviceStatus* status;
+    int* event_sys;     // batched systems: system index of each event record (null otherwise)
+    int sys;
 };
 
 struct MvsParticleArgs {
@@ -103,6 +105,65 @@ struct CorrectorArgs {
 };
 // big.in: current Big state, big.out: scratch, big.tab: 4 table rows.
 void launch_mvs_corrector(const MvsBigArgs& big, const CorrectorArgs& a, cudaStream_t s);
+
+// ------------------------------------------------------------ batched systems
+// Many independent planetary systems advanced together by the MVS map (no
+// counterpart in the reference, which integrates one system per process):
+// one 32-thread CTA per system runs the Big-body integrator above, and one
+// launch advances every test particle of every system, each warp on a tile of
+// 32 slots of a single system. Systems have no non-gravitational forces and
+// no central-body oblateness.
+struct BatchSys {
+    double mu, h;
+    int nbig, nb;
+    int first_slot, np;   // the system's particle slots
+    int tab_off;          // doubles into a table set: [K + 1][tab_stride(nb)]
+    int det_off;          // doubles into a detail set: [K][nb][TAB_DETAIL]
+};
+struct BatchTile {
+    int sys, first, count, pad;
+};
+
+struct BatchBigArgs {
+    const MvsBigArgs* proto;  // per system: constants, state buffers (in = set 0, out = set 1)
+    const BatchSys* sys;
+    int flip;                 // read set 1, write set 0
+    int nsteps, reset, central, step0;
+    double rcen;
+    double* tab;              // table set of this chunk
+    double* detail;           // detail set of this chunk
+    MercuryEvent* events;
+    int* event_step;
+    int* event_sys;
+    int event_cap;
+    DeviceStatus* status;
+};
+
+struct BatchParticleArgs {
+    int ntiles, npcap;
+    int nsteps, reset, central, step0;
+    double rcen;
+    const BatchSys* sys;
+    const BatchTile* tiles;
+    const double* xin;        // [9][npcap]
+    double* xout;
+    const double* rce;        // [npcap]
+    const double* rphys;
+    const int* local;         // slot -> particle index within its system
+    const double* tab;
+    const double* detail;
+    MercuryEvent* events;
+    int* event_step;
+    int* event_sys;
+    int event_cap;
+    EncounterCandidate* cands;  // slot field holds the system index
+    int cand_cap;
+    DeviceStatus* status;
+};
+
+void launch_mvs_big_batch(const BatchBigArgs& a, int nsys, int max_nbig, cudaStream_t s);
+void launch_mvs_particles_batch(const BatchParticleArgs& a, cudaStream_t s, int threads);
+void launch_classify_batch(const BatchParticleArgs& a, cudaStream_t s);
 
 // Finishes mce_stat's test for the candidates of the last particle launch and
 // writes the event records; detail is the base of the run's detail rows.

@@ -205,3 +205,19 @@ def make_system(seed: int = 1, n_particles: int = 10_000, nplanets: int = 8, nea
     rceh[1:1 + nplanets] = rceh_big
     sys = System(m=m, x=x, v=v, nbig=1 + nplanets, rceh=rceh)
     return mce_init(sys, h, cefac)
+
+
+def make_batch(seed: int = 1, nsys: int = 4096, nmin: int = 10, nmax: int = 5000, hmin: float = 4.0,
+               hmax: float = 16.0, big_max: int = 8, near_fraction: float = 0.0):
+    """Seeded batch of independent systems for the batched path: per system
+    1..big_max planets (uniform), log-uniform particle count in [nmin, nmax],
+    step h uniform in [hmin, hmax] days, the single-system distributions
+    otherwise. Returns (systems, h)."""
+    rng = np.random.default_rng(seed)
+    nbig = rng.integers(1, big_max + 1, nsys)
+    npart = np.exp(rng.uniform(np.log(nmin), np.log(nmax), nsys)).astype(int)
+    h = rng.uniform(hmin, hmax, nsys)
+    systems = [make_system(seed=int(rng.integers(1 << 30)), n_particles=int(npart[k]), nplanets=int(nbig[k]),
+                           near_fraction=near_fraction, h=float(h[k]))
+               for k in range(nsys)]
+    return systems, h

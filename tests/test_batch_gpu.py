@@ -1,0 +1,86 @@
+"""Batched MVS systems (mercury_b200_batch_*, an extension with no reference
+counterpart): every system of a batch must come out exactly as the drop-in
+single-system path integrates it alone (same states and event records, bit
+for bit), whatever the launch shape, and close to the oracle."""
+import numpy as np
+import pytest
+
+from mercuda_b200.backend import Backend, Batch
+from mercuda_b200.system import make_batch
+
+pytestmark = pytest.mark.gpu
+
+RCEN = 0.005
+
+
+def single_runs(cuda_lib, systems, h, nsteps):
+    out = []
+    for sys, hs in zip(systems, h):
+        be = Backend("MVS", cuda_lib)
+        be.configure()
+        be.upload(sys.copy())
+        ev, st = be.mvs_advance(0.0, float(hs), nsteps, RCEN)
+        x, v = be.download()
+        be.free()
+        out.append((x, v, ev, st))
+    return out
+
+
+def check_against(batch_out, events, sy, st, singles):
+    for k, ((x, v), (xs, vs, ev, est)) in enumerate(zip(batch_out, singles)):
+        assert np.array_equal(x, xs) and np.array_equal(v, vs), (k, np.max(np.abs(x - xs)))
+        mine = events[sy == k]
+        assert np.array_equal(st[sy == k], est), k
+        assert mine.tobytes() == ev.tobytes(), k
+
+
+@pytest.mark.parametrize("shape", [dict(), dict(steps_per_launch=7, graph=0, threads=64)])
+def test_batch_matches_single_system_path(cuda_lib, shape):
+    systems, h = make_batch(seed=7, nsys=24, nmin=10, nmax=400, near_fraction=0.05)
+    nsteps = 40
+    b = Batch(systems, h, cuda_lib)
+    if shape:
+        b.set(threads=shape["threads"], steps_per_launch=shape["steps_per_launch"], graph=shape["graph"])
+    ev, sy, st = b.advance(0.0, nsteps, RCEN)
+    out = b.download()
+    b.set(threads=0, steps_per_launch=0, graph=1)
+    b.free()
+    assert len(ev) > 0
+    check_against(out, ev, sy, st, single_runs(cuda_lib, systems, h, nsteps))
+
+
+def test_batch_two_advances_and_event_growth(cuda_lib):
+    """Two advances in a row (the second replays the captured graph) and
+    more event records than the initial buffer holds."""
+    systems, h = make_batch(seed=3, nsys=16, nmin=200, nmax=600, near_fraction=0.5)
+    b = Batch(systems, h, cuda_lib)
+    ev1, sy1, st1 = b.advance(0.0, 30, RCEN)
+    ev2, sy2, st2 = b.advance(0.0, 30, RCEN)
+    out = b.download()
+    b.free()
+    assert len(ev1) + len(ev2) > 4096
+    singles = single_runs(cuda_lib, systems, h, 60)
+    for k, ((x, v), (xs, vs, ev, est)) in enumerate(zip(out, singles)):
+        assert np.array_equal(x, xs) and np.array_equal(v, vs), k
+        n1 = int(np.sum(sy1 == k))
+        assert ev1[sy1 == k].tobytes() == ev[:n1].tobytes()
+        assert np.array_equal(st2[sy2 == k] + 30, est[n1:])
+        # the second advance restarts the clock at its own time argument
+        assert np.array_equal(ev2[sy2 == k][["i", "j", "kind", "now"]], ev[n1:][["i", "j", "kind", "now"]])
+
+
+def test_batch_against_oracle(cuda_lib, oracle):
+    systems, h = make_batch(seed=11, nsys=6, nmin=50, nmax=300, near_fraction=0.05)
+    b = Batch(systems, h, cuda_lib)
+    ev, sy, st = b.advance(0.0, 25, RCEN)
+    out = b.download()
+    b.free()
+    for k, (sys, hs) in enumerate(zip(systems, h)):
+        ref = sys.copy()
+        oev, ost = oracle.mvs_run(ref, 0.0, float(hs), 25, RCEN)
+        x, v = out[k]
+        scale = np.maximum(np.abs(ref.x), 1e-3)
+        assert np.max(np.abs(x - ref.x) / scale) < 1e-11
+        mine = ev[sy == k]
+        key = lambda e: (min(e["i"], e["j"]), max(e["i"], e["j"]), int(e["kind"]))
+        assert sorted(map(key, mine)) == sorted(map(key, oev))
