@@ -376,13 +376,14 @@ int mercury_b200_batch_upload(int nsys, const int* body_offset, const int* nbig,
             }
         }
         check(cudaMemcpy(B.bigbuf[0].p, hb.data(), sizeof(double) * hb.size(), cudaMemcpyHostToDevice), "upload");
-        check(cudaMemset(B.bigbuf[1].p, 0, sizeof(double) * hb.size()), "upload");
+        check(cudaMemsetAsync(B.bigbuf[1].p, 0, sizeof(double) * hb.size(), B.stream), "upload");
         check(cudaMemcpy(B.bm.p, hm.data(), sizeof(double) * bigs, cudaMemcpyHostToDevice), "upload");
         check(cudaMemcpy(B.brce.p, hrce.data(), sizeof(double) * bigs, cudaMemcpyHostToDevice), "upload");
         check(cudaMemcpy(B.brphys.p, hrph.data(), sizeof(double) * bigs, cudaMemcpyHostToDevice), "upload");
         check(cudaMemcpy(B.plocal.p, local.data(), sizeof(int) * B.npcap, cudaMemcpyHostToDevice), "upload");
-        check(cudaMemset(B.pstate[0].p, 0, sizeof(double) * 9 * B.npcap), "upload");
-        check(cudaMemset(B.pstate[1].p, 0, sizeof(double) * 9 * B.npcap), "upload");
+        // (on the stream of the layout kernels below, so that they run after)
+        check(cudaMemsetAsync(B.pstate[0].p, 0, sizeof(double) * 9 * B.npcap, B.stream), "upload");
+        check(cudaMemsetAsync(B.pstate[1].p, 0, sizeof(double) * 9 * B.npcap, B.stream), "upload");
         // particle rows through a device staging copy of the host arrays
         DBuf<double> stage;
         DBuf<int> dst;
