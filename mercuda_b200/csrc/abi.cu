@@ -712,8 +712,8 @@ void order_particles(int n, int nbig, double mu, const double* xx, const double*
         perm[p] = p;
         inv[p] = p;
     }
-    check(cudaMemcpy(c.perm[c.kc].p, perm.data(), sizeof(int) * c.npcap, cudaMemcpyHostToDevice), "upload");
-    check(cudaMemcpy(c.inv.p, inv.data(), sizeof(int) * c.npcap, cudaMemcpyHostToDevice), "upload");
+    h2d(c.perm[c.kc].p, perm.data(), sizeof(int) * c.npcap, c.stream);
+    h2d(c.inv.p, inv.data(), sizeof(int) * c.npcap, c.stream);
     c.steps_since_order = 0;
 }
 
@@ -1147,8 +1147,7 @@ int mercury_cuda_events(double time, double h, double rcen, const MercuryEvent**
             c.event_step.release();
             c.event_step.reserve(c.events.n);
             if (c.pair_events)
-                check(cudaMemcpy(c.events.p, keep.data(), sizeof(MercuryEvent) * c.pair_events, cudaMemcpyHostToDevice),
-                      "events");
+                h2d(c.events.p, keep.data(), sizeof(MercuryEvent) * c.pair_events, c.stream, "events");
         }
         const int nev = c.stepped ? c.status_host->events : 0;
         c.host_events.resize(nev);
@@ -1402,8 +1401,8 @@ int mercury_cuda_encounter_enter(int n, int nb, const double* m, const double* x
         }
         c.adj_off.reserve(n + 1);
         c.adj.reserve(adj.size());
-        check(cudaMemcpy(c.adj_off.p, off.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice), "pairs");
-        check(cudaMemcpy(c.adj.p, adj.data(), sizeof(int2) * adj.size(), cudaMemcpyHostToDevice), "pairs");
+        h2d(c.adj_off.p, off.data(), sizeof(int) * (n + 1), c.stream, "pairs");
+        h2d(c.adj.p, adj.data(), sizeof(int2) * adj.size(), c.stream, "pairs");
         return 0;
     } catch (const std::exception& e) {
         g_active = 0;

@@ -143,7 +143,7 @@ void layout_tables(Batch& B, int K) {
         if (B.tab[k].n != n0 || B.det[k].n != n1) ++B.epoch;
     }
     B.K = K;
-    check(cudaMemcpy(B.d_sys.p, B.sys.data(), sizeof(BatchSys) * B.nsys, cudaMemcpyHostToDevice), "upload");
+    h2d(B.d_sys.p, B.sys.data(), sizeof(BatchSys) * B.nsys, B.stream);
 }
 
 BatchBigArgs big_chunk(Batch& B, int ch, int ks, int reset, int central, int s0, double rcen) {
@@ -351,8 +351,7 @@ int mercury_b200_batch_upload(int nsys, const int* body_offset, const int* nbig,
         B.status.reserve(1);
         B.snap.reserve((size_t)9 * B.npcap + (size_t)9 * bigs);
         if (B.ntiles)
-            check(cudaMemcpy(B.d_tiles.p, tiles.data(), sizeof(BatchTile) * B.ntiles, cudaMemcpyHostToDevice),
-                  "upload");
+            h2d(B.d_tiles.p, tiles.data(), sizeof(BatchTile) * B.ntiles, B.stream);
         // destination index of every body: Big rows at 9 * big_off + k (stride
         // nbig within the system) are written per component below; particles
         // go to their slot
@@ -375,12 +374,12 @@ int mercury_b200_batch_upload(int nsys, const int* body_offset, const int* nbig,
                 local[B.first_slot[s] + q] = q;
             }
         }
-        check(cudaMemcpy(B.bigbuf[0].p, hb.data(), sizeof(double) * hb.size(), cudaMemcpyHostToDevice), "upload");
+        h2d(B.bigbuf[0].p, hb.data(), sizeof(double) * hb.size(), B.stream);
         check(cudaMemsetAsync(B.bigbuf[1].p, 0, sizeof(double) * hb.size(), B.stream), "upload");
-        check(cudaMemcpy(B.bm.p, hm.data(), sizeof(double) * bigs, cudaMemcpyHostToDevice), "upload");
-        check(cudaMemcpy(B.brce.p, hrce.data(), sizeof(double) * bigs, cudaMemcpyHostToDevice), "upload");
-        check(cudaMemcpy(B.brphys.p, hrph.data(), sizeof(double) * bigs, cudaMemcpyHostToDevice), "upload");
-        check(cudaMemcpy(B.plocal.p, local.data(), sizeof(int) * B.npcap, cudaMemcpyHostToDevice), "upload");
+        h2d(B.bm.p, hm.data(), sizeof(double) * bigs, B.stream);
+        h2d(B.brce.p, hrce.data(), sizeof(double) * bigs, B.stream);
+        h2d(B.brphys.p, hrph.data(), sizeof(double) * bigs, B.stream);
+        h2d(B.plocal.p, local.data(), sizeof(int) * B.npcap, B.stream);
         // (on the stream of the layout kernels below, so that they run after)
         check(cudaMemsetAsync(B.pstate[0].p, 0, sizeof(double) * 9 * B.npcap, B.stream), "upload");
         check(cudaMemsetAsync(B.pstate[1].p, 0, sizeof(double) * 9 * B.npcap, B.stream), "upload");
@@ -389,11 +388,10 @@ int mercury_b200_batch_upload(int nsys, const int* body_offset, const int* nbig,
         DBuf<int> dst;
         stage.reserve((size_t)3 * B.nbody);
         dst.reserve(B.nbody);
-        check(cudaMemcpy(dst.p, slot_of.data(), sizeof(int) * B.nbody, cudaMemcpyHostToDevice), "upload");
+        h2d(dst.p, slot_of.data(), sizeof(int) * B.nbody, B.stream);
         const int blocks = (B.nbody + 255) / 256;
         for (int part = 0; part < 2; ++part) {
-            check(cudaMemcpy(stage.p, part ? vv : xx, sizeof(double) * 3 * B.nbody, cudaMemcpyHostToDevice),
-                  "upload");
+            h2d(stage.p, part ? vv : xx, sizeof(double) * 3 * B.nbody, B.stream);
             batch_layout_kernel<<<blocks, 256, 0, B.stream>>>(stage.p, B.nbody, 3, dst.p,
                                                                B.pstate[0].p + (size_t)3 * part * B.npcap, B.npcap);
             check(cudaStreamSynchronize(B.stream), "upload");
@@ -401,7 +399,7 @@ int mercury_b200_batch_upload(int nsys, const int* body_offset, const int* nbig,
         const double* scal[2] = {rce, rphys};
         double* sdst[2] = {B.prce.p, B.prphys.p};
         for (int q = 0; q < 2; ++q) {
-            check(cudaMemcpy(stage.p, scal[q], sizeof(double) * B.nbody, cudaMemcpyHostToDevice), "upload");
+            h2d(stage.p, scal[q], sizeof(double) * B.nbody, B.stream);
             batch_layout_kernel<<<blocks, 256, 0, B.stream>>>(stage.p, B.nbody, 1, dst.p, sdst[q], B.npcap);
             check(cudaStreamSynchronize(B.stream), "upload");
         }
@@ -426,7 +424,7 @@ int mercury_b200_batch_upload(int nsys, const int* body_offset, const int* nbig,
                 st.a = base + 6 * B.nbig[s];
             }
         }
-        check(cudaMemcpy(B.d_proto.p, proto.data(), sizeof(MvsBigArgs) * nsys, cudaMemcpyHostToDevice), "upload");
+        h2d(B.d_proto.p, proto.data(), sizeof(MvsBigArgs) * nsys, B.stream);
         layout_tables(B, B.forced_K > 0 ? B.forced_K : 31);
         B.cur = 0;
         B.reset = true;

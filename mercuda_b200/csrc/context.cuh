@@ -26,6 +26,15 @@ inline void check(cudaError_t code, const char* what = nullptr) {
     }
 }
 
+// Host-to-device copy ordered on `stream` (the library's streams do not
+// synchronize with the legacy default stream, and a plain cudaMemcpy from
+// pageable memory may return before its data lands); returns once it is done.
+inline void h2d(void* dst, const void* src, size_t bytes, cudaStream_t stream, const char* what = "upload") {
+    if (bytes == 0) return;
+    check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream), what);
+    check(cudaStreamSynchronize(stream), what);
+}
+
 // Growable device array.
 template <class T> struct DBuf {
     T* p = nullptr;

@@ -71,9 +71,11 @@ void ensure_constants() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !done_on[dev]) {
+        // once per device; waits for the copy, which the library's streams
+        // would not otherwise be ordered after
         const RaConst K = make_constants();
-        cudaMemcpyToSymbol(RK, &K, sizeof(K));
-        done_on[dev] = 1;
+        if (cudaMemcpyToSymbol(RK, &K, sizeof(K)) == cudaSuccess && cudaDeviceSynchronize() == cudaSuccess)
+            done_on[dev] = 1;
     }
 }
 
