@@ -69,6 +69,32 @@ int mercury_b200_batch_set(int threads, int steps_per_launch, int use_graph);
 int mercury_b200_batch_timing(double* ms, int* launches, int* threads, int* steps_per_launch);
 void mercury_b200_batch_free(void);
 
+/* ---- Gradients through the MVS test-particle integration (no counterpart in
+ * the reference). Massless particles never act on the Big bodies, so each
+ * particle's final state depends only on its own initial state and Yarkovsky
+ * coefficient; the backward call returns those gradients for a given
+ * gradient of the final states.
+ *
+ * Forward: the Big bodies (host rows: mbig[nbig] in K2 units, xbig/vbig
+ * (nbig,3), body 0 the central body) and np massless particles (DEVICE
+ * arrays: x0/v0 (np,3) rows, yar[np] or NULL for none) advance nsteps MVS
+ * steps of h, exactly as the MVS path steps them; the final states go to the
+ * device arrays x_final/v_final (np,3). The state every checkpoint_every
+ * steps is kept for the backward call (9 doubles per particle per
+ * checkpoint, plus 12 per particle per step of one segment). The device
+ * inputs must stay unchanged until the backward call. No oblateness and no
+ * non-gravitational term other than yar. */
+int mercury_b200_adjoint_forward(int nbig, const double* mbig, const double* xbig, const double* vbig, int np,
+                                 const double* x0, const double* v0, const double* yar, double h, int nsteps,
+                                 int checkpoint_every, double* x_final, double* v_final);
+/* Backward for the last forward run: gx/gv (device (np,3); gv may be NULL)
+ * hold dL/dx_final and dL/dv_final; dx0/dv0 (device (np,3)) and dyar
+ * (device [np], may be NULL) receive dL/dx0, dL/dv0, dL/dyar. */
+int mercury_b200_adjoint_backward(const double* gx, const double* gv, double* dx0, double* dv0, double* dyar);
+/* Device time of the last forward and backward calls. */
+int mercury_b200_adjoint_timing(double* forward_ms, double* backward_ms);
+void mercury_b200_adjoint_free(void);
+
 /* One MVS step (kick, drift, mce_stat pair screen, kick) of a system whose
  * arrays the caller already holds on the current device, with no device
  * allocation: for hosts that cannot call cudaMalloc (device memory owned by

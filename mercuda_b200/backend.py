@@ -48,7 +48,8 @@ EXTENSION_SYMBOLS = ["mercury_b200_mvs_advance", "mercury_b200_events", "mercury
                      "mercury_b200_set_launch", "mercury_b200_fp64_peak", "mercury_b200_mvs_step_noalloc",
                      "mercury_b200_dropin_time", "mercury_b200_batch_upload", "mercury_b200_batch_advance",
                      "mercury_b200_batch_events", "mercury_b200_batch_download", "mercury_b200_batch_set",
-                     "mercury_b200_batch_timing", "mercury_b200_batch_free"]
+                     "mercury_b200_batch_timing", "mercury_b200_batch_free", "mercury_b200_adjoint_forward",
+                     "mercury_b200_adjoint_backward", "mercury_b200_adjoint_timing", "mercury_b200_adjoint_free"]
 
 
 class BackendError(RuntimeError):
@@ -97,6 +98,11 @@ def load_library(path: Path | str | None = None) -> C.CDLL:
     L.mercury_b200_batch_set.argtypes = [I, I, I]
     L.mercury_b200_batch_timing.argtypes = [PD, PI, PI, PI]
     L.mercury_b200_batch_free.restype = None
+    VP_ = C.c_void_p
+    L.mercury_b200_adjoint_forward.argtypes = [I, PD, PD, PD, I, VP_, VP_, VP_, D, I, I, VP_, VP_]
+    L.mercury_b200_adjoint_backward.argtypes = [VP_, VP_, VP_, VP_, VP_]
+    L.mercury_b200_adjoint_timing.argtypes = [PD, PD]
+    L.mercury_b200_adjoint_free.restype = None
     VP = C.c_void_p
     L.mercury_b200_mvs_step_noalloc.argtypes = [I, I, VP, VP, VP, VP, VP, VP, VP, VP, VP, I, D, D, I, VP, I,
                                                 PI, VP]

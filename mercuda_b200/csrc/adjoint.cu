@@ -1,0 +1,396 @@
+// Gradients through the MVS test-particle integration (no counterpart in the
+// reference): a forward run that keeps checkpoints, then a reverse sweep.
+//
+// The Big bodies never feel massless particles, so their trajectory (and
+// each step's force table) is fixed: one Big-body CTA integrates it once for
+// all steps. Each particle's final state is then a function of its own
+// initial position, velocity and Yarkovsky coefficient only, and the reverse
+// sweep is one thread per particle:
+//
+//   forward:  the mdt_mvs step of every particle (the same statements as the
+//             MVS kernels), (x, v, a) stored every K steps
+//   backward: per K-step segment, from the last: recompute the segment from
+//             its checkpoint keeping each step's drift input and output, then
+//             walk it backwards: kick, force (gravity from the table, yar) and
+//             the Kepler drift's state-transition matrix, transposed.
+#include <cmath>
+#include <cstdio>
+
+#include "../../include/mercury_b200.h"
+#include "context.cuh"
+#include "kepler.cuh"
+#include "kepler_adjoint.cuh"
+#include "mvs.cuh"
+#include "mvs_device.cuh"
+
+namespace mb200 {
+namespace {
+
+constexpr int REC = 12;  // per step of a segment: x, v after the kick (drift input), x, v after the drift
+
+struct AdjArgs {
+    int np, nb, nsteps, K, has_yar;
+    double h, mu;
+    const double* tab;       // [nsteps + 1][tab_stride(nb)]
+    const double* x0;        // (np, 3) rows
+    const double* v0;
+    const double* yar;       // [np] or null
+    double* xf;              // (np, 3)
+    double* vf;
+    double* ckpt;            // [nseg][9][np]
+    double* rec;             // [K][REC][np]
+    const double* gx;        // (np, 3) adjoint of the final positions
+    const double* gv;        // (np, 3) or null
+    double* dx0;             // (np, 3)
+    double* dv0;
+    double* dyar;            // [np] or null
+    DeviceStatus* status;
+};
+
+__device__ __forceinline__ double3 ld_row(const double* a, int p) {
+    return make_double3(a[3 * (size_t)p], a[3 * (size_t)p + 1], a[3 * (size_t)p + 2]);
+}
+__device__ __forceinline__ void st_row(double* a, int p, double3 v) {
+    a[3 * (size_t)p] = v.x;
+    a[3 * (size_t)p + 1] = v.y;
+    a[3 * (size_t)p + 2] = v.z;
+}
+
+// The kick acceleration (angf + 0) + a of mdt_mvs for a massless particle
+// with Yarkovsky coefficient yar (no other non-gravitational terms).
+template <bool YAR>
+__device__ __forceinline__ double3 accel(const double3 x, const double3 v, double yar, const double* T, int nb,
+                                         double mu, DeviceStatus* st) {
+    return small_body_force<YAR, false>(x, v, [&](int c) -> double { return c == 4 ? yar : 0.0; }, T, nb, nullptr,
+                                        mu, st);
+}
+
+// Transposed Jacobian of that acceleration applied to la: adds to gx, gv and
+// gyar. Gravity: -sum_b m_b d/|d|^3 with d = x - x_b; Yarkovsky (mfo_ngf):
+// yar t / (r^2 |t|) with t = v - (x.v / r^2) x, differentiated in yar even
+// where yar is zero.
+template <bool YAR>
+__device__ __forceinline__ void accel_vjp(const double3 x, const double3 v, double yar, const double* T, int nb,
+                                          const double3 la, double3& gx, double3& gv, double& gyar) {
+#pragma unroll 1
+    for (int b = 0; b < nb; ++b) {
+        const double* row = T + TAB_HEAD + b * TAB_BODY;
+        const double dx = x.x - row[0], dy = x.y - row[1], dz = x.z - row[2];
+        const double s2 = dx * dx + dy * dy + dz * dz;
+        const double s_1 = 1.0 / sqrt(s2);
+        const double s_3 = s_1 * s_1 * s_1;
+        const double s_5 = s_3 * s_1 * s_1;
+        const double dl = dx * la.x + dy * la.y + dz * la.z;
+        const double m = row[3];
+        gx.x -= m * (s_3 * la.x - 3.0 * s_5 * dl * dx);
+        gx.y -= m * (s_3 * la.y - 3.0 * s_5 * dl * dy);
+        gx.z -= m * (s_3 * la.z - 3.0 * s_5 * dl * dz);
+    }
+    if (YAR) {
+        const double r2 = x.x * x.x + x.y * x.y + x.z * x.z;
+        const double p = x.x * v.x + x.y * v.y + x.z * v.z;
+        const double q = p / r2;
+        const double3 t = make_double3(v.x - q * x.x, v.y - q * x.y, v.z - q * x.z);
+        const double tn = sqrt(t.x * t.x + t.y * t.y + t.z * t.z);
+        const double A = la.x * t.x + la.y * t.y + la.z * t.z;
+        const double k = yar / (r2 * tn);
+        const double kt = A * yar / (r2 * tn * tn * tn);
+        const double3 lt = make_double3(k * la.x - kt * t.x, k * la.y - kt * t.y, k * la.z - kt * t.z);
+        double lr2 = -A * yar / (r2 * r2 * tn);
+        gyar += A / (r2 * tn);
+        gv.x += lt.x;
+        gv.y += lt.y;
+        gv.z += lt.z;
+        const double lq = -(lt.x * x.x + lt.y * x.y + lt.z * x.z);
+        gx.x -= q * lt.x;
+        gx.y -= q * lt.y;
+        gx.z -= q * lt.z;
+        const double lp = lq / r2;
+        lr2 -= lq * p / (r2 * r2);
+        gx.x += lp * v.x + 2.0 * lr2 * x.x;
+        gx.y += lp * v.y + 2.0 * lr2 * x.y;
+        gx.z += lp * v.z + 2.0 * lr2 * x.z;
+        gv.x += lp * x.x;
+        gv.y += lp * x.y;
+        gv.z += lp * x.z;
+    }
+}
+
+__device__ __forceinline__ void st_ckpt(double* c, int np, int p, double3 x, double3 v, double3 a) {
+    const double q[9] = {x.x, x.y, x.z, v.x, v.y, v.z, a.x, a.y, a.z};
+    for (int k = 0; k < 9; ++k) c[(size_t)k * np + p] = q[k];
+}
+
+template <bool YAR> __global__ void __launch_bounds__(128) adj_forward_kernel(AdjArgs A) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= A.np) return;
+    const int stride = tab_stride(A.nb);
+    const double hby2 = 0.5 * A.h;
+    const double yar = YAR ? A.yar[p] : 0.0;
+    double3 x = ld_row(A.x0, p), v = ld_row(A.v0, p);
+    double3 acc = accel<YAR>(x, v, yar, A.tab, A.nb, A.mu, A.status);
+#pragma unroll 1
+    for (int s = 0; s < A.nsteps; ++s) {
+        if (s % A.K == 0) st_ckpt(A.ckpt + (size_t)(s / A.K) * 9 * A.np, A.np, p, x, v, acc);
+        v.x = v.x + hby2 * acc.x;
+        v.y = v.y + hby2 * acc.y;
+        v.z = v.z + hby2 * acc.z;
+        drift_one(A.mu, x, v, A.h);
+        acc = accel<YAR>(x, v, yar, A.tab + (size_t)(s + 1) * stride, A.nb, A.mu, A.status);
+        v.x = v.x + hby2 * acc.x;
+        v.y = v.y + hby2 * acc.y;
+        v.z = v.z + hby2 * acc.z;
+    }
+    st_row(A.xf, p, x);
+    st_row(A.vf, p, v);
+}
+
+template <bool YAR> __global__ void __launch_bounds__(128) adj_backward_kernel(AdjArgs A) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= A.np) return;
+    const int stride = tab_stride(A.nb), np = A.np;
+    const double hby2 = 0.5 * A.h;
+    const double yar = YAR ? A.yar[p] : 0.0;
+    double3 lx = ld_row(A.gx, p);
+    double3 lv = A.gv ? ld_row(A.gv, p) : make_double3(0.0, 0.0, 0.0);
+    double3 la = make_double3(0.0, 0.0, 0.0);
+    double lyar = 0.0;
+    const int nseg = (A.nsteps + A.K - 1) / A.K;
+    auto R = [&](int sl, int c) -> double& { return A.rec[((size_t)sl * REC + c) * np + p]; };
+#pragma unroll 1
+    for (int seg = nseg - 1; seg >= 0; --seg) {
+        const int s0 = seg * A.K, s1 = min(A.nsteps, s0 + A.K);
+        const double* c = A.ckpt + (size_t)seg * 9 * np;
+        double3 x = make_double3(c[p], c[np + p], c[2 * (size_t)np + p]);
+        double3 v = make_double3(c[3 * (size_t)np + p], c[4 * (size_t)np + p], c[5 * (size_t)np + p]);
+        double3 acc = make_double3(c[6 * (size_t)np + p], c[7 * (size_t)np + p], c[8 * (size_t)np + p]);
+#pragma unroll 1
+        for (int s = s0; s < s1; ++s) {
+            const int sl = s - s0;
+            v.x = v.x + hby2 * acc.x;
+            v.y = v.y + hby2 * acc.y;
+            v.z = v.z + hby2 * acc.z;
+            R(sl, 0) = x.x; R(sl, 1) = x.y; R(sl, 2) = x.z;
+            R(sl, 3) = v.x; R(sl, 4) = v.y; R(sl, 5) = v.z;
+            drift_one(A.mu, x, v, A.h);
+            R(sl, 6) = x.x; R(sl, 7) = x.y; R(sl, 8) = x.z;
+            R(sl, 9) = v.x; R(sl, 10) = v.y; R(sl, 11) = v.z;
+            acc = accel<YAR>(x, v, yar, A.tab + (size_t)(s + 1) * stride, A.nb, A.mu, A.status);
+            v.x = v.x + hby2 * acc.x;
+            v.y = v.y + hby2 * acc.y;
+            v.z = v.z + hby2 * acc.z;
+        }
+#pragma unroll 1
+        for (int s = s1 - 1; s >= s0; --s) {
+            const int sl = s - s0;
+            const double xin[3] = {R(sl, 0), R(sl, 1), R(sl, 2)};
+            const double vin[3] = {R(sl, 3), R(sl, 4), R(sl, 5)};
+            const double3 x2 = make_double3(R(sl, 6), R(sl, 7), R(sl, 8));
+            const double3 v2 = make_double3(R(sl, 9), R(sl, 10), R(sl, 11));
+            // second kick v3 = v2 + hby2 a(x2, v2)
+            const double3 lacc = make_double3(la.x + hby2 * lv.x, la.y + hby2 * lv.y, la.z + hby2 * lv.z);
+            double3 gx = make_double3(0.0, 0.0, 0.0), gv = make_double3(0.0, 0.0, 0.0);
+            accel_vjp<YAR>(x2, v2, yar, A.tab + (size_t)(s + 1) * stride, A.nb, lacc, gx, gv, lyar);
+            const double lx1[3] = {lx.x + gx.x, lx.y + gx.y, lx.z + gx.z};
+            const double lv1[3] = {lv.x + gv.x, lv.y + gv.y, lv.z + gv.z};
+            // drift
+            double lxo[3], lvo[3];
+            if (!drift_vjp(A.mu, xin, vin, A.h, lx1, lv1, lxo, lvo)) raise_fault(A.status, FAULT_NONFINITE);
+            // first kick v1 = v + hby2 acc
+            lx = make_double3(lxo[0], lxo[1], lxo[2]);
+            lv = make_double3(lvo[0], lvo[1], lvo[2]);
+            la = make_double3(hby2 * lvo[0], hby2 * lvo[1], hby2 * lvo[2]);
+        }
+    }
+    // the acceleration of the initial state (computed before the first kick)
+    const double3 x0 = ld_row(A.x0, p), v0 = ld_row(A.v0, p);
+    double3 gx = make_double3(0.0, 0.0, 0.0), gv = make_double3(0.0, 0.0, 0.0);
+    accel_vjp<YAR>(x0, v0, yar, A.tab, A.nb, la, gx, gv, lyar);
+    st_row(A.dx0, p, make_double3(lx.x + gx.x, lx.y + gx.y, lx.z + gx.z));
+    st_row(A.dv0, p, make_double3(lv.x + gv.x, lv.y + gv.y, lv.z + gv.z));
+    if (A.dyar) A.dyar[p] = lyar;
+    if (!isfinite(lx.x) || !isfinite(lv.x) || !isfinite(lyar)) raise_fault(A.status, FAULT_NONFINITE);
+}
+
+struct Adjoint {
+    int nbig = 0, np = 0, nsteps = 0, K = 0, has_yar = 0;
+    double h = 0.0, mu = 0.0;
+    const double *x0 = nullptr, *v0 = nullptr, *yar = nullptr;
+    DBuf<double> bigstate[2], mbig, zeros, tab, detail, ckpt, rec;
+    DBuf<MercuryEvent> events;
+    DBuf<int> event_step;
+    DBuf<DeviceStatus> status;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    float fwd_ms = 0.0f, bwd_ms = 0.0f;
+    bool ready = false;
+    void ensure() {
+        if (stream) return;
+        check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "stream");
+        check(cudaEventCreate(&e0), "event");
+        check(cudaEventCreate(&e1), "event");
+    }
+    void release() {
+        DBuf<double>* b[] = {&bigstate[0], &bigstate[1], &mbig, &zeros, &tab, &detail, &ckpt, &rec};
+        for (auto* d : b) d->release();
+        events.release();
+        event_step.release();
+        status.release();
+        ready = false;
+    }
+};
+
+Adjoint& adj() {
+    static Adjoint a;
+    return a;
+}
+
+AdjArgs adj_args(Adjoint& J) {
+    AdjArgs a{};
+    a.np = J.np;
+    a.nb = J.nbig - 1;
+    a.nsteps = J.nsteps;
+    a.K = J.K;
+    a.has_yar = J.has_yar;
+    a.h = J.h;
+    a.mu = J.mu;
+    a.tab = J.tab.p;
+    a.x0 = J.x0;
+    a.v0 = J.v0;
+    a.yar = J.yar;
+    a.ckpt = J.ckpt.p;
+    a.rec = J.rec.p;
+    a.status = J.status.p;
+    return a;
+}
+
+}  // namespace
+}  // namespace mb200
+
+using namespace mb200;
+
+extern "C" {
+
+int mercury_b200_adjoint_forward(int nbig, const double* mbig, const double* xbig, const double* vbig, int np,
+                                 const double* x0, const double* v0, const double* yar, double h, int nsteps,
+                                 int checkpoint_every, double* x_final, double* v_final) {
+    Adjoint& J = adj();
+    try {
+        if (nbig < 1 || nbig > 512) throw std::runtime_error("adjoint: nbig must be 1..512");
+        if (np < 1 || nsteps < 1 || checkpoint_every < 1) throw std::runtime_error("adjoint: invalid sizes");
+        if (!(h != 0.0) || !std::isfinite(h)) throw std::runtime_error("adjoint: invalid step");
+        J.ensure();
+        J.nbig = nbig;
+        J.np = np;
+        J.nsteps = nsteps;
+        J.K = std::min(checkpoint_every, nsteps);
+        J.h = h;
+        J.mu = mbig[0];
+        J.x0 = x0;
+        J.v0 = v0;
+        J.yar = yar;
+        J.has_yar = yar != nullptr;
+        const int nb = nbig - 1, nseg = (nsteps + J.K - 1) / J.K;
+        for (int k = 0; k < 2; ++k) J.bigstate[k].reserve((size_t)9 * nbig);
+        J.mbig.reserve(nbig);
+        J.zeros.reserve(nbig);
+        J.tab.reserve((size_t)(nsteps + 1) * tab_stride(nb));
+        J.detail.reserve((size_t)nsteps * std::max(1, nb) * TAB_DETAIL);
+        J.ckpt.reserve((size_t)nseg * 9 * np);
+        J.rec.reserve((size_t)J.K * REC * np);
+        J.events.reserve(4096);
+        J.event_step.reserve(4096);
+        J.status.reserve(1);
+        // Big bodies: SoA [9][nbig] from the host rows, a(3) zero (reset)
+        std::vector<double> b(9 * (size_t)nbig, 0.0);
+        for (int k = 0; k < nbig; ++k)
+            for (int c = 0; c < 3; ++c) {
+                b[c * nbig + k] = xbig[3 * k + c];
+                b[(3 + c) * nbig + k] = vbig[3 * k + c];
+            }
+        h2d(J.bigstate[0].p, b.data(), sizeof(double) * b.size(), J.stream);
+        h2d(J.mbig.p, mbig, sizeof(double) * nbig, J.stream);
+        check(cudaMemsetAsync(J.zeros.p, 0, sizeof(double) * nbig, J.stream), "memset");
+        check(cudaMemsetAsync(J.status.p, 0, sizeof(DeviceStatus), J.stream), "memset");
+        check(cudaEventRecord(J.e0, J.stream), "event");
+        // the Big bodies' steps and every step's force table, in one launch
+        MvsBigArgs a{};
+        a.nbig = nbig;
+        a.reset = 1;
+        a.nsteps = nsteps;
+        a.h = h;
+        a.m = J.mbig.p;
+        a.rce = J.zeros.p;
+        a.rphys = J.zeros.p;
+        a.in.x = J.bigstate[0].p;
+        a.in.v = J.bigstate[0].p + 3 * nbig;
+        a.in.a = J.bigstate[0].p + 6 * nbig;
+        a.out.x = J.bigstate[1].p;
+        a.out.v = J.bigstate[1].p + 3 * nbig;
+        a.out.a = J.bigstate[1].p + 6 * nbig;
+        a.tab = J.tab.p;
+        a.detail = J.detail.p;
+        a.events = J.events.p;
+        a.event_step = J.event_step.p;
+        a.event_cap = (int)J.events.n;
+        a.status = J.status.p;
+        launch_mvs_big(a, J.stream);
+        AdjArgs f = adj_args(J);
+        f.xf = x_final;
+        f.vf = v_final;
+        const int grid = (np + 127) / 128;
+        if (J.has_yar) adj_forward_kernel<true><<<grid, 128, 0, J.stream>>>(f);
+        else adj_forward_kernel<false><<<grid, 128, 0, J.stream>>>(f);
+        check(cudaEventRecord(J.e1, J.stream), "event");
+        check(cudaGetLastError(), "launch");
+        DeviceStatus st;
+        check(cudaMemcpyAsync(&st, J.status.p, sizeof(st), cudaMemcpyDeviceToHost, J.stream), "status");
+        check(cudaStreamSynchronize(J.stream), "adjoint forward");
+        check(cudaEventElapsedTime(&J.fwd_ms, J.e0, J.e1), "timer");
+        if (st.fault) throw std::runtime_error("adjoint forward: force failed");
+        J.ready = true;
+        return 0;
+    } catch (const std::exception& e) {
+        J.ready = false;
+        return report(e);
+    }
+}
+
+int mercury_b200_adjoint_backward(const double* gx, const double* gv, double* dx0, double* dv0, double* dyar) {
+    Adjoint& J = adj();
+    try {
+        if (!J.ready) throw std::runtime_error("adjoint backward without a forward run");
+        check(cudaMemsetAsync(J.status.p, 0, sizeof(DeviceStatus), J.stream), "memset");
+        AdjArgs a = adj_args(J);
+        a.gx = gx;
+        a.gv = gv;
+        a.dx0 = dx0;
+        a.dv0 = dv0;
+        a.dyar = dyar;
+        check(cudaEventRecord(J.e0, J.stream), "event");
+        const int grid = (J.np + 127) / 128;
+        if (J.has_yar) adj_backward_kernel<true><<<grid, 128, 0, J.stream>>>(a);
+        else adj_backward_kernel<false><<<grid, 128, 0, J.stream>>>(a);
+        check(cudaEventRecord(J.e1, J.stream), "event");
+        check(cudaGetLastError(), "launch");
+        DeviceStatus st;
+        check(cudaMemcpyAsync(&st, J.status.p, sizeof(st), cudaMemcpyDeviceToHost, J.stream), "status");
+        check(cudaStreamSynchronize(J.stream), "adjoint backward");
+        check(cudaEventElapsedTime(&J.bwd_ms, J.e0, J.e1), "timer");
+        if (st.fault) throw std::runtime_error("adjoint backward: non-finite gradient");
+        return 0;
+    } catch (const std::exception& e) {
+        return report(e);
+    }
+}
+
+int mercury_b200_adjoint_timing(double* forward_ms, double* backward_ms) {
+    Adjoint& J = adj();
+    if (forward_ms) *forward_ms = J.fwd_ms;
+    if (backward_ms) *backward_ms = J.bwd_ms;
+    return 0;
+}
+
+void mercury_b200_adjoint_free(void) { adj().release(); }
+
+}  // extern "C"

@@ -12,17 +12,12 @@
 #ifndef MB200_PARTICLE_MIN_BLOCKS
 #define MB200_PARTICLE_MIN_BLOCKS 5
 #endif
-// Unroll factor of the per-Big-body force loop (ILP against code size).
-#ifndef MB200_FORCE_UNROLL
-#define MB200_FORCE_UNROLL 1
-#endif
 
 namespace mb200 {
 
 namespace {
 
 constexpr unsigned FULL = 0xffffffffu;
-constexpr int kForceUnroll = MB200_FORCE_UNROLL;
 
 __device__ __forceinline__ double3 ld3(const double* p, int stride, int k) {
     return make_double3(p[k], p[stride + k], p[2 * stride + k]);
@@ -434,45 +429,6 @@ struct Cols {
     __device__ double3 ld3(int c) const { return make_double3(at(c), at(c + 1), at(c + 2)); }
     __device__ void st3(int c, double3 v) const { at(c) = v.x; at(c + 1) = v.y; at(c + 2) = v.z; }
 };
-
-// mfo_mvs for one Small body (mercury6_2.for:5034-5060) plus mfo_ngf, i.e. the
-// total acceleration (angf + 0) + a of the kick; T is a force table and g(c)
-// returns the body's c-th non-gravitational coefficient.
-template <bool NGF, bool OBL, class G>
-__device__ __forceinline__ double3 small_body_force(const double3 x, const double3 v_ngf, G g, const double* T,
-                                                    int nb, const double* jcen, double mu, DeviceStatus* st) {
-    double3 a3 = make_double3(0.0, 0.0, 0.0);
-#pragma unroll kForceUnroll
-    for (int b = 0; b < nb; ++b) {
-        const double* row = T + TAB_HEAD + b * TAB_BODY;
-        const double dx = x.x - row[0], dy = x.y - row[1], dz = x.z - row[2];
-        const double s2 = dx * dx + dy * dy + dz * dz;
-        const double s_1 = 1.0 / sqrt(s2);
-        const double s_3 = s_1 * s_1 * s_1;
-        const double faci = row[3] * s_3;
-        a3.x = a3.x - faci * dx;
-        a3.y = a3.y - faci * dy;
-        a3.z = a3.z - faci * dz;
-    }
-    double3 a = make_double3(T[0] + a3.x, T[1] + a3.y, T[2] + a3.z);
-    if (OBL) {
-        const double3 ao = oblate_accel(x, jcen, mu);
-        a.x = a.x + (ao.x - T[3]);
-        a.y = a.y + (ao.y - T[4]);
-        a.z = a.z + (ao.z - T[5]);
-    }
-    if (NGF) {
-        double gc[5];
-        for (int c = 0; c < 5; ++c) gc[c] = g(c);
-        double3 ng;
-        if (!nongrav_accel(x, v_ngf, gc, ng)) raise_fault(st, 2);
-        a.x = ng.x + 0.0 + a.x;
-        a.y = ng.y + 0.0 + a.y;
-        a.z = ng.z + 0.0 + a.z;
-    }
-    if (!isfinite(a.x) || !isfinite(a.y) || !isfinite(a.z)) raise_fault(st, 1);
-    return a;
-}
 
 // small_body_force with the coefficients of pair member u in the columns.
 template <bool NGF, bool OBL>

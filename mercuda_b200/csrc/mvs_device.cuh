@@ -3,6 +3,7 @@
 // and the event-record writer.
 #pragma once
 #include "common.cuh"
+#include "mvs.cuh"
 
 namespace mb200 {
 
@@ -250,6 +251,45 @@ __device__ __forceinline__ void store_event(MercuryEvent* dst, const MercuryEven
     double2* d = reinterpret_cast<double2*>(dst);
 #pragma unroll
     for (int k = 0; k < 8; ++k) d[k] = s[k];
+}
+
+// mfo_mvs for one Small body (mercury6_2.for:5034-5060) plus mfo_ngf, i.e. the
+// total acceleration (angf + 0) + a of the kick; T is a force table and g(c)
+// returns the body's c-th non-gravitational coefficient.
+template <bool NGF, bool OBL, class G>
+__device__ __forceinline__ double3 small_body_force(const double3 x, const double3 v_ngf, G g, const double* T,
+                                                    int nb, const double* jcen, double mu, DeviceStatus* st) {
+    double3 a3 = make_double3(0.0, 0.0, 0.0);
+#pragma unroll 1
+    for (int b = 0; b < nb; ++b) {
+        const double* row = T + TAB_HEAD + b * TAB_BODY;
+        const double dx = x.x - row[0], dy = x.y - row[1], dz = x.z - row[2];
+        const double s2 = dx * dx + dy * dy + dz * dz;
+        const double s_1 = 1.0 / sqrt(s2);
+        const double s_3 = s_1 * s_1 * s_1;
+        const double faci = row[3] * s_3;
+        a3.x = a3.x - faci * dx;
+        a3.y = a3.y - faci * dy;
+        a3.z = a3.z - faci * dz;
+    }
+    double3 a = make_double3(T[0] + a3.x, T[1] + a3.y, T[2] + a3.z);
+    if (OBL) {
+        const double3 ao = oblate_accel(x, jcen, mu);
+        a.x = a.x + (ao.x - T[3]);
+        a.y = a.y + (ao.y - T[4]);
+        a.z = a.z + (ao.z - T[5]);
+    }
+    if (NGF) {
+        double gc[5];
+        for (int c = 0; c < 5; ++c) gc[c] = g(c);
+        double3 ng;
+        if (!nongrav_accel(x, v_ngf, gc, ng)) raise_fault(st, 2);
+        a.x = ng.x + 0.0 + a.x;
+        a.y = ng.y + 0.0 + a.y;
+        a.z = ng.z + 0.0 + a.z;
+    }
+    if (!isfinite(a.x) || !isfinite(a.y) || !isfinite(a.z)) raise_fault(st, 1);
+    return a;
 }
 
 }  // namespace mb200

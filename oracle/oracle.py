@@ -87,6 +87,8 @@ def lib() -> C.CDLL:
         L.oracle_mce_snif.argtypes = [D, I, I, PD, PD, PD, PD, PD, PI_, PI_, I]
         L.oracle_mce_snif.restype = I
         L.oracle_mfo_hy.argtypes = [I, I, PD, PD, PD, PD, PD]
+        L.oracle_mvs_jacobian.argtypes = [I, I, PD, PD, PD, PD, I, PD, D, I, PD]
+        L.oracle_mvs_jacobian.restype = I
         _lib = L
     return _lib
 
@@ -286,3 +288,16 @@ def mfo_hy(sys):
     a = np.zeros((sys.n, 3))
     lib().oracle_mfo_hy(sys.n, sys.nbig, _p(sys.m), _p(sys.x), _p(sys.rcrit), _p(sys.jcen), _p(a))
     return a
+
+
+def mvs_jacobian(sys, h, nsteps):
+    """nsteps of mdt_mvs on sys (in place) with forward-mode derivatives of
+    every test particle's final (x, v) with respect to its initial (x, v) and
+    its Yarkovsky coefficient: returns J of shape (n - nbig, 6, 7)."""
+    s = sys
+    jac = np.zeros((s.n - s.nbig, 6, 7))
+    rc = lib().oracle_mvs_jacobian(s.n, s.nbig, _p(s.m), _p(s.x), _p(s.v), _p(s.ngf), s.ngflag, _p(s.jcen), h,
+                                   int(nsteps), _p(jac))
+    if rc:
+        raise RuntimeError("oracle Jacobian run failed")
+    return jac

@@ -12,6 +12,7 @@
 #include "oracle_ra15.hpp"
 #include "oracle_bs.hpp"
 #include "oracle_hy.hpp"
+#include "oracle_dual.hpp"
 
 namespace oracle {
 thread_local Tally tally;
@@ -382,6 +383,76 @@ int oracle_mce_snif(double h, int n, int nbig, const double* x0, const double* v
 void oracle_mfo_hy(int n, int nbig, const double* m, const double* x, const double* rcrit, const double* jcen,
                    double* a) {
     oracle::mfo_hy(jcen, n, nbig, m, x, rcrit, a);
+}
+
+// drift_one of one body with its 6x6 Jacobian (row-major, d out / d in) by
+// forward-mode dual numbers; xv = {x, y, z, vx, vy, vz} updated in place.
+void oracle_drift_jacobian(double mu, double* xv, double dt, double* jac) {
+    using D6 = oracle::Dual<6>;
+    D6 q[6];
+    for (int c = 0; c < 6; ++c) {
+        q[c] = D6(xv[c]);
+        q[c].d[c] = 1.0;
+    }
+    int iflg = 0;
+    oracle::drift_one<D6>(D6(mu), q[0], q[1], q[2], q[3], q[4], q[5], D6(dt), iflg);
+    for (int c = 0; c < 6; ++c) {
+        xv[c] = q[c].v;
+        for (int k = 0; k < 6; ++k) jac[6 * c + k] = q[c].d[k];
+    }
+}
+
+// nsteps of mdt_mvs (no central screen needed: states only) with the
+// derivatives of every massless particle's final state with respect to its
+// own initial position, velocity and Yarkovsky coefficient ngf(5,j), by
+// forward-mode dual numbers through the same statements. jac receives, per
+// particle (bodies nbig..n-1 in order), a 6x7 matrix row-major: rows x,y,z,
+// vx,vy,vz at the end; columns x0,y0,z0,vx0,vy0,vz0,yar. x, v are advanced in
+// place. Returns nonzero on a force failure or a massive Small body.
+int oracle_mvs_jacobian(int n, int nbig, const double* m, double* x, double* v, const double* ngf, int ngflag,
+                        const double* jcen, double h, int nsteps, double* jac) {
+    using DD = oracle::Dual<7>;
+    for (int j = nbig; j < n; ++j)
+        if (m[j] != 0.0) return 1;
+    std::vector<DD> dm(n), dx(3 * (size_t)n), dv(3 * (size_t)n), dngf(5 * (size_t)n), drce(n, DD(0.0)),
+        drph(n, DD(0.0));
+    for (int j = 0; j < n; ++j) {
+        dm[j] = DD(m[j]);
+        for (int c = 0; c < 3; ++c) {
+            dx[3 * j + c] = DD(x[3 * j + c]);
+            dv[3 * j + c] = DD(v[3 * j + c]);
+            if (j >= nbig) {
+                dx[3 * j + c].d[c] = 1.0;
+                dv[3 * j + c].d[3 + c] = 1.0;
+            }
+        }
+        for (int c = 0; c < 5; ++c) dngf[5 * j + c] = DD(ngf[5 * j + c]);
+        if (j >= nbig) dngf[5 * j + 4].d[6] = 1.0;
+    }
+    oracle::MvsState<DD> st;
+    std::vector<Event> events;
+    DD time(0.0), hh(h);
+    for (int s = 0; s < nsteps; ++s) {
+        events.clear();
+        if (oracle::mdt_mvs<DD>(time, hh, jcen, n, nbig, dm.data(), dx.data(), dv.data(), drce.data(), drph.data(),
+                                dngf.data(), ngflag, st, events))
+            return 1;
+        time = time + hh;
+    }
+    for (int j = 0; j < n; ++j)
+        for (int c = 0; c < 3; ++c) {
+            x[3 * j + c] = dx[3 * j + c].v;
+            v[3 * j + c] = dv[3 * j + c].v;
+        }
+    for (int j = nbig; j < n; ++j) {
+        double* J = jac + 42 * (size_t)(j - nbig);
+        for (int c = 0; c < 3; ++c)
+            for (int k = 0; k < 7; ++k) {
+                J[7 * c + k] = dx[3 * j + c].d[k];
+                J[7 * (3 + c) + k] = dv[3 * j + c].d[k];
+            }
+    }
+    return 0;
 }
 
 }  // extern "C"
