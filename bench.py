@@ -25,6 +25,12 @@ mce_init (cefac 3); a step is one HYBRID step.
 in all) advanced together; the plain loop over systems through the
 single-system path is timed on a sample beside it.
 
+--workload adjoint measures the gradient of sum |x_final|^2 with respect to
+every particle's initial state and Yarkovsky coefficient (forward with a
+checkpoint every 50 steps, then the reverse sweep) on 100,000 particles for
+--steps MVS steps (1,000 for the gradient benchmark); a step is one forward
+plus one backward particle-step.
+
 --workload radau|bs|bs2 measures the adaptive integrators instead (mdt_ra15,
 mdt_bs1, mdt_bs2 through the drop-in step/events calls, as mal_hvar drives
 them) on the 100,000-particle system of the same generator with 1PN,
@@ -80,10 +86,13 @@ def parse_args():
     p.add_argument("--threads", type=int, default=0)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", default="mvs", choices=["mvs", "radau", "bs", "bs2", "hybrid", "batch"])
+    p.add_argument("--workload", default="mvs", choices=["mvs", "radau", "bs", "bs2", "hybrid", "batch", "adjoint"])
+    p.add_argument("--checkpoint-every", type=int, default=50)
     p.add_argument("--systems", type=int, default=4096)
     args = p.parse_args()
     if args.workload in ADAPTIVE and args.particles == 1_000_000:
+        args.particles = 100_000
+    if args.workload == "adjoint" and args.particles == 1_000_000:
         args.particles = 100_000
     return args
 
@@ -520,6 +529,99 @@ def run_batch(args, rank, world, dist):
                           "e2e": e2e, "cpu_baseline": cpu}), flush=True)
 
 
+def run_adjoint(args, rank, world, dist):
+    from mercuda_b200.system import make_system
+    metric = "adjoint MVS particle-steps/s"
+
+    def make(seed, n):
+        s_ = make_system(seed=seed, n_particles=n, near_fraction=0.0, h=H)
+        rng = np.random.default_rng(seed + 7)
+        npart = s_.n - s_.nbig
+        s_.ngf[s_.nbig:, 4] = np.exp(rng.uniform(np.log(1e-15), np.log(1e-13), npart)) * rng.choice([-1, 1], npart)
+        return s_
+
+    workload_text = (f"gradient of sum |x_final|^2 w.r.t. initial x, v and yar of {args.particles} particles, "
+                     f"{args.steps} MVS steps of 8 d about 8 planets, checkpoint every {args.checkpoint_every}")
+
+    def cpu_sample(n, steps):
+        from oracle import oracle as O
+        s_ = make(args.seed, n)
+        t0 = time.perf_counter()
+        O.mvs_jacobian(s_, H, steps)
+        dt = time.perf_counter() - t0
+        return n * steps / dt, dt
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        n = min(args.particles, 2000)
+        value, dt = cpu_sample(n, args.steps)
+        print(json.dumps({"impl": "reference", "metric": metric, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+                          "steps": args.steps, "warmup": 0, "ms_per_step": dt * 1e3 / args.steps,
+                          "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                          "data": "synthetic", "config": {"workload": workload_text, "particles": n},
+                          "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
+                                           "sample": f"{n} particles x {args.steps} steps, forward-mode tangents "
+                                                     f"of the oracle ({dt:.1f} s)"},
+                          "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
+              flush=True)
+        return
+    import torch
+    from mercuda_b200.adjoint import mvs_trajectory, timing
+
+    sysw = make(args.seed + rank, args.particles)
+    nb = sysw.nbig
+    dev = torch.device("cuda")
+    big = (sysw.m[:nb], sysw.x[:nb], sysw.v[:nb])
+
+    def once(x0h, v0h, yh):
+        x0 = torch.tensor(x0h, device=dev, requires_grad=True)
+        v0 = torch.tensor(v0h, device=dev, requires_grad=True)
+        yar = torch.tensor(yh, device=dev, requires_grad=True)
+        xf, _ = mvs_trajectory(x0, v0, yar, big, H, args.steps, args.checkpoint_every)
+        (xf ** 2).sum().backward()
+        return x0.grad, v0.grad, yar.grad
+
+    for _ in range(max(1, args.warmup)):
+        once(sysw.x[nb:], sysw.v[nb:], sysw.ngf[nb:, 4])
+        break
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clocks:
+        t0 = time.perf_counter()
+        g = once(sysw.x[nb:], sysw.v[nb:], sysw.ngf[nb:, 4])
+        gx = g[0].cpu().numpy()
+        e2e_s = time.perf_counter() - t0
+    fwd, bwd = timing()
+    ms = fwd + bwd
+    if dist:
+        tt = torch.tensor([ms, e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms, e2e_s = float(tt[0].item()), float(tt[1].item())
+    value = world * args.particles * args.steps / (ms * 1e-3)
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        v_cpu, dt = cpu_sample(1000, args.steps)
+        cpu = {"value": v_cpu, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": f"1000 particles x {args.steps} steps, forward-mode tangents of the oracle ({dt:.1f} s)"}
+    if rank == 0:
+        print(json.dumps({"metric": metric, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                          "warmup": 1, "ms_per_step": ms / args.steps, "higher_is_better": True,
+                          "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                          "config": {"workload": workload_text, "particles_per_gpu": args.particles,
+                                     "forward_ms": fwd, "backward_ms": bwd, "backward_over_forward": bwd / fwd,
+                                     "checkpoint_every": args.checkpoint_every,
+                                     "grad_finite": bool(np.all(np.isfinite(gx)))},
+                          "clocks": clocks.summary(), "gpu_launches": 3,
+                          "e2e": {"value": world * args.particles * args.steps / e2e_s, "unit": UNIT,
+                                  "h2d_bytes_per_step": args.particles * 7 * 8 / args.steps,
+                                  "d2h_bytes_per_step": args.particles * 3 * 8 / args.steps,
+                                  "note": "wall clock around tensor creation from host arrays, the forward and "
+                                          "backward calls and the gradient copy back"},
+                          "cpu_baseline": cpu}), flush=True)
+
+
 def main():
     args = parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -541,6 +643,8 @@ def main():
             run_hybrid(args, rank, world, dist)
         elif args.workload == "batch":
             run_batch(args, rank, world, dist)
+        elif args.workload == "adjoint":
+            run_adjoint(args, rank, world, dist)
         else:
             run_adaptive(args, rank, world, dist)
         if dist:
