@@ -195,7 +195,8 @@ template <bool YAR> __global__ void __launch_bounds__(128) adj_backward_kernel(A
             const double lv1[3] = {lv.x + gv.x, lv.y + gv.y, lv.z + gv.z};
             // drift
             double lxo[3], lvo[3];
-            if (!drift_vjp(A.mu, xin, vin, A.h, lx1, lv1, lxo, lvo)) raise_fault(A.status, FAULT_NONFINITE);
+            const double xend[3] = {x2.x, x2.y, x2.z};
+            if (!drift_vjp(A.mu, xin, vin, A.h, xend, lx1, lv1, lxo, lvo)) raise_fault(A.status, FAULT_NONFINITE);
             // first kick v1 = v + hby2 acc
             lx = make_double3(lxo[0], lxo[1], lxo[2]);
             lv = make_double3(lvo[0], lvo[1], lvo[2]);

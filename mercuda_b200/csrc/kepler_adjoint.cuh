@@ -23,20 +23,24 @@
 
 namespace mb200 {
 
-// Stumpff functions c0..c5 of z: closed forms for |z| >= 1, series below.
+// Stumpff functions c0..c5 of z. For |z| < 1, c4 and c5 by their series and
+// the rest by c_k = 1/k! - z c_{k+2}; beyond, the closed forms.
 MB200_HD inline void stumpff6(double z, double c[6]) {
     if (fabs(z) < 1.0) {
         // c_k(z) = sum_j (-z)^j / (k + 2j)!
-        for (int k = 0; k < 6; ++k) {
-            double fact = 1.0;
-            for (int q = 2; q <= k; ++q) fact *= q;
-            double term = 1.0 / fact, sum = term;
-            for (int j = 1; j < 14; ++j) {
-                term = term * (-z) / ((double)(k + 2 * j - 1) * (double)(k + 2 * j));
-                sum += term;
-            }
-            c[k] = sum;
+        double t4 = 1.0 / 24.0, s4 = t4, t5 = 1.0 / 120.0, s5 = t5;
+        for (int j = 1; j < 12; ++j) {
+            t4 = t4 * (-z) / ((double)(2 * j + 3) * (double)(2 * j + 4));
+            t5 = t5 * (-z) / ((double)(2 * j + 4) * (double)(2 * j + 5));
+            s4 += t4;
+            s5 += t5;
         }
+        c[4] = s4;
+        c[5] = s5;
+        c[2] = 0.5 - z * s4;
+        c[3] = 1.0 / 6.0 - z * s5;
+        c[0] = 1.0 - z * c[2];
+        c[1] = 1.0 - z * c[3];
         return;
     }
     if (z > 0.0) {
@@ -67,10 +71,38 @@ MB200_HD inline void gfuncs(double s, double alpha, double G[6]) {
     }
 }
 
+// A starting value of the universal anomaly from the drift's end position x1:
+// g and f follow from x x x1 = g (x x v) and x1 x v = f (x x v), then
+// G2 = (1 - f) r0 / mu, G1 = (g - sigma0 G2) / r0, G0 = 1 - alpha G2, and s is
+// the angle (or hyperbolic angle) with cosine G0 and sine sqrt(alpha) G1.
+MB200_HD inline double anomaly_guess(const double x[3], const double v[3], const double x1[3], double r0,
+                                     double sig0, double alpha, double mu, double dt) {
+    const double h[3] = {x[1] * v[2] - x[2] * v[1], x[2] * v[0] - x[0] * v[2], x[0] * v[1] - x[1] * v[0]};
+    const double hh = h[0] * h[0] + h[1] * h[1] + h[2] * h[2];
+    const double fallback = dt / r0;
+    if (!(hh > 0.0)) return fallback;
+    const double a[3] = {x[1] * x1[2] - x[2] * x1[1], x[2] * x1[0] - x[0] * x1[2], x[0] * x1[1] - x[1] * x1[0]};
+    const double b[3] = {x1[1] * v[2] - x1[2] * v[1], x1[2] * v[0] - x1[0] * v[2], x1[0] * v[1] - x1[1] * v[0]};
+    const double g = (a[0] * h[0] + a[1] * h[1] + a[2] * h[2]) / hh;
+    const double f = (b[0] * h[0] + b[1] * h[1] + b[2] * h[2]) / hh;
+    const double G2 = (1.0 - f) * r0 / mu;
+    const double G1 = (g - sig0 * G2) / r0;
+    double s;
+    if (alpha > 0.0) {
+        const double w = sqrt(alpha);
+        s = atan2(w * G1, 1.0 - alpha * G2) / w;
+    } else if (alpha < 0.0) {
+        const double w = sqrt(-alpha);
+        s = asinh(w * G1) / w;
+    } else {
+        s = G1;
+    }
+    return isfinite(s) ? s : fallback;
+}
+
 // The universal anomaly of a drift of dt (Laguerre iteration on the universal
-// Kepler equation). Returns false if it did not converge.
+// Kepler equation from s). Returns false if it did not converge.
 MB200_HD inline bool universal_anomaly(double r0, double sig0, double alpha, double mu, double dt, double& s) {
-    s = dt / r0;
     for (int it = 0; it < 60; ++it) {
         double G[6];
         gfuncs(s, alpha, G);
@@ -95,14 +127,15 @@ MB200_HD inline bool universal_anomaly(double r0, double sig0, double alpha, dou
 }
 
 // lx = d(x')/dx ^T lx1 + d(v')/dx ^T lv1, lv likewise, for the drift of
-// (x, v) by dt about mu. Returns false if the anomaly did not converge.
-MB200_HD inline bool drift_vjp(double mu, const double x[3], const double v[3], double dt, const double lx1[3],
-                              const double lv1[3], double lx[3], double lv[3]) {
+// (x, v) by dt about mu that ended at x1. Returns false if the anomaly did not
+// converge.
+MB200_HD inline bool drift_vjp(double mu, const double x[3], const double v[3], double dt, const double x1[3],
+                              const double lx1[3], const double lv1[3], double lx[3], double lv[3]) {
     const double r0 = sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
     const double sig0 = x[0] * v[0] + x[1] * v[1] + x[2] * v[2];
     const double vv = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
     const double alpha = 2.0 * mu / r0 - vv;
-    double s;
+    double s = anomaly_guess(x, v, x1, r0, sig0, alpha, mu, dt);
     if (!universal_anomaly(r0, sig0, alpha, mu, dt, s)) return false;
     double G[6];
     gfuncs(s, alpha, G);
