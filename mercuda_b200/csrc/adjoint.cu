@@ -39,6 +39,7 @@ struct AdjArgs {
     double* vf;
     double* ckpt;            // [nseg][9][np]
     double* rec;             // [K][REC][np]
+    double* lam;             // [10][np] adjoint state between segments
     const double* gx;        // (np, 3) adjoint of the final positions
     const double* gv;        // (np, 3) or null
     double* dx0;             // (np, 3)
@@ -145,63 +146,91 @@ template <bool YAR> __global__ void __launch_bounds__(128) adj_forward_kernel(Ad
     st_row(A.vf, p, v);
 }
 
-template <bool YAR> __global__ void __launch_bounds__(128) adj_backward_kernel(AdjArgs A) {
+// Reverse sweep, per segment (last first): recompute the segment from its
+// checkpoint keeping each step's drift input and output ...
+template <bool YAR> __global__ void __launch_bounds__(128) adj_recompute_kernel(AdjArgs A, int seg) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= A.np) return;
     const int stride = tab_stride(A.nb), np = A.np;
     const double hby2 = 0.5 * A.h;
     const double yar = YAR ? A.yar[p] : 0.0;
-    double3 lx = ld_row(A.gx, p);
-    double3 lv = A.gv ? ld_row(A.gv, p) : make_double3(0.0, 0.0, 0.0);
-    double3 la = make_double3(0.0, 0.0, 0.0);
-    double lyar = 0.0;
-    const int nseg = (A.nsteps + A.K - 1) / A.K;
     auto R = [&](int sl, int c) -> double& { return A.rec[((size_t)sl * REC + c) * np + p]; };
+    const int s0 = seg * A.K, s1 = min(A.nsteps, s0 + A.K);
+    const double* c = A.ckpt + (size_t)seg * 9 * np;
+    double3 x = make_double3(c[p], c[np + p], c[2 * (size_t)np + p]);
+    double3 v = make_double3(c[3 * (size_t)np + p], c[4 * (size_t)np + p], c[5 * (size_t)np + p]);
+    double3 acc = make_double3(c[6 * (size_t)np + p], c[7 * (size_t)np + p], c[8 * (size_t)np + p]);
 #pragma unroll 1
-    for (int seg = nseg - 1; seg >= 0; --seg) {
-        const int s0 = seg * A.K, s1 = min(A.nsteps, s0 + A.K);
-        const double* c = A.ckpt + (size_t)seg * 9 * np;
-        double3 x = make_double3(c[p], c[np + p], c[2 * (size_t)np + p]);
-        double3 v = make_double3(c[3 * (size_t)np + p], c[4 * (size_t)np + p], c[5 * (size_t)np + p]);
-        double3 acc = make_double3(c[6 * (size_t)np + p], c[7 * (size_t)np + p], c[8 * (size_t)np + p]);
+    for (int s = s0; s < s1; ++s) {
+        const int sl = s - s0;
+        v.x = v.x + hby2 * acc.x;
+        v.y = v.y + hby2 * acc.y;
+        v.z = v.z + hby2 * acc.z;
+        R(sl, 0) = x.x; R(sl, 1) = x.y; R(sl, 2) = x.z;
+        R(sl, 3) = v.x; R(sl, 4) = v.y; R(sl, 5) = v.z;
+        drift_one(A.mu, x, v, A.h);
+        R(sl, 6) = x.x; R(sl, 7) = x.y; R(sl, 8) = x.z;
+        R(sl, 9) = v.x; R(sl, 10) = v.y; R(sl, 11) = v.z;
+        acc = accel<YAR>(x, v, yar, A.tab + (size_t)(s + 1) * stride, A.nb, A.mu, A.status);
+        v.x = v.x + hby2 * acc.x;
+        v.y = v.y + hby2 * acc.y;
+        v.z = v.z + hby2 * acc.z;
+    }
+}
+
+// ... then walk it backwards: second kick, force, Kepler drift, first kick.
+// The adjoint state (lx, lv, la, lyar) lives in A.lam [10][np] between
+// segments; the first segment also differentiates the initial acceleration
+// and writes the gradients.
+template <bool YAR> __global__ void __launch_bounds__(128) adj_vjp_kernel(AdjArgs A, int seg, int last) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= A.np) return;
+    const int stride = tab_stride(A.nb), np = A.np;
+    const double hby2 = 0.5 * A.h;
+    const double yar = YAR ? A.yar[p] : 0.0;
+    auto R = [&](int sl, int c) -> double { return A.rec[((size_t)sl * REC + c) * np + p]; };
+    auto L = [&](int c) -> double& { return A.lam[(size_t)c * np + p]; };
+    double3 lx, lv, la;
+    double lyar;
+    if (last) {
+        lx = ld_row(A.gx, p);
+        lv = A.gv ? ld_row(A.gv, p) : make_double3(0.0, 0.0, 0.0);
+        la = make_double3(0.0, 0.0, 0.0);
+        lyar = 0.0;
+    } else {
+        lx = make_double3(L(0), L(1), L(2));
+        lv = make_double3(L(3), L(4), L(5));
+        la = make_double3(L(6), L(7), L(8));
+        lyar = L(9);
+    }
+    const int s0 = seg * A.K, s1 = min(A.nsteps, s0 + A.K);
 #pragma unroll 1
-        for (int s = s0; s < s1; ++s) {
-            const int sl = s - s0;
-            v.x = v.x + hby2 * acc.x;
-            v.y = v.y + hby2 * acc.y;
-            v.z = v.z + hby2 * acc.z;
-            R(sl, 0) = x.x; R(sl, 1) = x.y; R(sl, 2) = x.z;
-            R(sl, 3) = v.x; R(sl, 4) = v.y; R(sl, 5) = v.z;
-            drift_one(A.mu, x, v, A.h);
-            R(sl, 6) = x.x; R(sl, 7) = x.y; R(sl, 8) = x.z;
-            R(sl, 9) = v.x; R(sl, 10) = v.y; R(sl, 11) = v.z;
-            acc = accel<YAR>(x, v, yar, A.tab + (size_t)(s + 1) * stride, A.nb, A.mu, A.status);
-            v.x = v.x + hby2 * acc.x;
-            v.y = v.y + hby2 * acc.y;
-            v.z = v.z + hby2 * acc.z;
-        }
-#pragma unroll 1
-        for (int s = s1 - 1; s >= s0; --s) {
-            const int sl = s - s0;
-            const double xin[3] = {R(sl, 0), R(sl, 1), R(sl, 2)};
-            const double vin[3] = {R(sl, 3), R(sl, 4), R(sl, 5)};
-            const double3 x2 = make_double3(R(sl, 6), R(sl, 7), R(sl, 8));
-            const double3 v2 = make_double3(R(sl, 9), R(sl, 10), R(sl, 11));
-            // second kick v3 = v2 + hby2 a(x2, v2)
-            const double3 lacc = make_double3(la.x + hby2 * lv.x, la.y + hby2 * lv.y, la.z + hby2 * lv.z);
-            double3 gx = make_double3(0.0, 0.0, 0.0), gv = make_double3(0.0, 0.0, 0.0);
-            accel_vjp<YAR>(x2, v2, yar, A.tab + (size_t)(s + 1) * stride, A.nb, lacc, gx, gv, lyar);
-            const double lx1[3] = {lx.x + gx.x, lx.y + gx.y, lx.z + gx.z};
-            const double lv1[3] = {lv.x + gv.x, lv.y + gv.y, lv.z + gv.z};
-            // drift
-            double lxo[3], lvo[3];
-            const double xend[3] = {x2.x, x2.y, x2.z};
-            if (!drift_vjp(A.mu, xin, vin, A.h, xend, lx1, lv1, lxo, lvo)) raise_fault(A.status, FAULT_NONFINITE);
-            // first kick v1 = v + hby2 acc
-            lx = make_double3(lxo[0], lxo[1], lxo[2]);
-            lv = make_double3(lvo[0], lvo[1], lvo[2]);
-            la = make_double3(hby2 * lvo[0], hby2 * lvo[1], hby2 * lvo[2]);
-        }
+    for (int s = s1 - 1; s >= s0; --s) {
+        const int sl = s - s0;
+        const double xin[3] = {R(sl, 0), R(sl, 1), R(sl, 2)};
+        const double vin[3] = {R(sl, 3), R(sl, 4), R(sl, 5)};
+        const double xend[3] = {R(sl, 6), R(sl, 7), R(sl, 8)};
+        const double3 x2 = make_double3(xend[0], xend[1], xend[2]);
+        const double3 v2 = make_double3(R(sl, 9), R(sl, 10), R(sl, 11));
+        // second kick v3 = v2 + hby2 a(x2, v2)
+        const double3 lacc = make_double3(la.x + hby2 * lv.x, la.y + hby2 * lv.y, la.z + hby2 * lv.z);
+        double3 gx = make_double3(0.0, 0.0, 0.0), gv = make_double3(0.0, 0.0, 0.0);
+        accel_vjp<YAR>(x2, v2, yar, A.tab + (size_t)(s + 1) * stride, A.nb, lacc, gx, gv, lyar);
+        const double lx1[3] = {lx.x + gx.x, lx.y + gx.y, lx.z + gx.z};
+        const double lv1[3] = {lv.x + gv.x, lv.y + gv.y, lv.z + gv.z};
+        double lxo[3], lvo[3];
+        if (!drift_vjp(A.mu, xin, vin, A.h, xend, lx1, lv1, lxo, lvo)) raise_fault(A.status, FAULT_NONFINITE);
+        // first kick v1 = v + hby2 acc
+        lx = make_double3(lxo[0], lxo[1], lxo[2]);
+        lv = make_double3(lvo[0], lvo[1], lvo[2]);
+        la = make_double3(hby2 * lvo[0], hby2 * lvo[1], hby2 * lvo[2]);
+    }
+    if (seg > 0) {
+        L(0) = lx.x; L(1) = lx.y; L(2) = lx.z;
+        L(3) = lv.x; L(4) = lv.y; L(5) = lv.z;
+        L(6) = la.x; L(7) = la.y; L(8) = la.z;
+        L(9) = lyar;
+        return;
     }
     // the acceleration of the initial state (computed before the first kick)
     const double3 x0 = ld_row(A.x0, p), v0 = ld_row(A.v0, p);
@@ -217,7 +246,7 @@ struct Adjoint {
     int nbig = 0, np = 0, nsteps = 0, K = 0, has_yar = 0;
     double h = 0.0, mu = 0.0;
     const double *x0 = nullptr, *v0 = nullptr, *yar = nullptr;
-    DBuf<double> bigstate[2], mbig, zeros, tab, detail, ckpt, rec;
+    DBuf<double> bigstate[2], mbig, zeros, tab, detail, ckpt, rec, lam;
     DBuf<MercuryEvent> events;
     DBuf<int> event_step;
     DBuf<DeviceStatus> status;
@@ -232,7 +261,7 @@ struct Adjoint {
         check(cudaEventCreate(&e1), "event");
     }
     void release() {
-        DBuf<double>* b[] = {&bigstate[0], &bigstate[1], &mbig, &zeros, &tab, &detail, &ckpt, &rec};
+        DBuf<double>* b[] = {&bigstate[0], &bigstate[1], &mbig, &zeros, &tab, &detail, &ckpt, &rec, &lam};
         for (auto* d : b) d->release();
         events.release();
         event_step.release();
@@ -261,6 +290,7 @@ AdjArgs adj_args(Adjoint& J) {
     a.yar = J.yar;
     a.ckpt = J.ckpt.p;
     a.rec = J.rec.p;
+    a.lam = J.lam.p;
     a.status = J.status.p;
     return a;
 }
@@ -299,6 +329,7 @@ int mercury_b200_adjoint_forward(int nbig, const double* mbig, const double* xbi
         J.detail.reserve((size_t)nsteps * std::max(1, nb) * TAB_DETAIL);
         J.ckpt.reserve((size_t)nseg * 9 * np);
         J.rec.reserve((size_t)J.K * REC * np);
+        J.lam.reserve((size_t)10 * np);
         J.events.reserve(4096);
         J.event_step.reserve(4096);
         J.status.reserve(1);
@@ -370,8 +401,17 @@ int mercury_b200_adjoint_backward(const double* gx, const double* gv, double* dx
         a.dyar = dyar;
         check(cudaEventRecord(J.e0, J.stream), "event");
         const int grid = (J.np + 127) / 128;
-        if (J.has_yar) adj_backward_kernel<true><<<grid, 128, 0, J.stream>>>(a);
-        else adj_backward_kernel<false><<<grid, 128, 0, J.stream>>>(a);
+        const int nseg = (J.nsteps + J.K - 1) / J.K;
+        for (int seg = nseg - 1; seg >= 0; --seg) {
+            const int last = seg == nseg - 1 ? 1 : 0;
+            if (J.has_yar) {
+                adj_recompute_kernel<true><<<grid, 128, 0, J.stream>>>(a, seg);
+                adj_vjp_kernel<true><<<grid, 128, 0, J.stream>>>(a, seg, last);
+            } else {
+                adj_recompute_kernel<false><<<grid, 128, 0, J.stream>>>(a, seg);
+                adj_vjp_kernel<false><<<grid, 128, 0, J.stream>>>(a, seg, last);
+            }
+        }
         check(cudaEventRecord(J.e1, J.stream), "event");
         check(cudaGetLastError(), "launch");
         DeviceStatus st;
