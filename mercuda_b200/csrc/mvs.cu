@@ -14,6 +14,7 @@
 #endif
 
 namespace mb200 {
+static_assert(sizeof(MercuryEvent) == 8 * sizeof(double2), "event records are eight double2 words");
 
 namespace {
 
@@ -510,6 +511,8 @@ __device__ __forceinline__ void particle_step(double3& x, double3& v, double3& a
             MercuryEvent* e = A.events + slot;
             *reinterpret_cast<int4*>(e) = make_int4(1, A.nbig + A.perm[p] + 1, EV_CENTRAL, 0);
             reinterpret_cast<double2*>(e)[1] = make_double2(A.rcen, temp);
+            // a central-body record carries no states (xi = xj = 0)
+            for (int k = 2; k < 8; ++k) reinterpret_cast<double2*>(e)[k] = make_double2(0.0, 0.0);
             A.event_step[slot] = A.step0 + s;
         }
     }
@@ -787,6 +790,7 @@ __device__ __forceinline__ void batch_particle_step(double3& x, double3& v, doub
             MercuryEvent* e = A.events + slot;
             *reinterpret_cast<int4*>(e) = make_int4(1, id, EV_CENTRAL, 0);
             reinterpret_cast<double2*>(e)[1] = make_double2(A.rcen, temp);
+            for (int k = 2; k < 8; ++k) reinterpret_cast<double2*>(e)[k] = make_double2(0.0, 0.0);
             A.event_step[slot] = A.step0 + s;
             A.event_sys[slot] = sysid;
         }
