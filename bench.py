@@ -54,6 +54,8 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
+from mercuda_b200.shards import Ranks, ShardedRun  # noqa: E402
+
 METRIC = "MVS particle-steps/s"
 UNIT = "particle-steps/s"
 H = 8.0
@@ -97,9 +99,13 @@ def parse_args():
     return args
 
 
-def workload(particles: int, seed: int, near_fraction: float = 0.01):
+def workload(particles: int, seed: int, near_fraction: float = 0.01, rank: int = 0):
+    """Rank `rank`'s shard of the job's system: the planets of `seed` on every
+    rank, the particles of rank 0 from the same generator (the one-GPU
+    workload) and those of rank r > 0 from the seed (seed, r)."""
     from mercuda_b200.system import make_system
-    return make_system(seed=seed, n_particles=particles, near_fraction=near_fraction, h=H)
+    return make_system(seed=seed, n_particles=particles, near_fraction=near_fraction, h=H,
+                       particle_seed=None if rank == 0 else (seed, rank))
 
 
 # HYBRID's encounter members go through BS2 at tol 1e-12 without collision
@@ -197,10 +203,9 @@ ADAPTIVE_TOL = 1e-12
 ADAPTIVE_H0 = 2.0
 
 
-def adaptive_workload(particles: int, seed: int):
-    from mercuda_b200.system import make_system
-    sys_ = make_system(seed=seed, n_particles=particles, near_fraction=0.0, h=H)
-    rng = np.random.default_rng(seed + 1000)
+def adaptive_workload(particles: int, seed: int, rank: int = 0):
+    sys_ = workload(particles, seed, 0.0, rank)
+    rng = np.random.default_rng(seed + 1000 if rank == 0 else (seed + 1000, rank))
     npart = sys_.n - sys_.nbig
     sys_.ngf[sys_.nbig:, 3] = rng.uniform(0.01, 0.3, npart)
     sys_.ngf[sys_.nbig:, 4] = np.exp(rng.uniform(np.log(1e-15), np.log(1e-13), npart)) * rng.choice([-1, 1], npart)
@@ -243,14 +248,11 @@ def run_adaptive(args, rank, world, dist):
 
     b = Backend(name)
     b.configure()
-    sysw = adaptive_workload(args.particles, args.seed + rank)
+    sysw = adaptive_workload(args.particles, args.seed, rank)
     b.upload(sysw)
 
-    def barrier():
-        torch.cuda.synchronize()
-        if dist:
-            dist.barrier()
-        torch.cuda.synchronize()
+    ranks = Ranks(dist, device="cuda")
+    barrier = ranks.barrier
 
     def run(time0, h, nsteps):
         t, dtflag, nev = time0, 0, 0
@@ -268,14 +270,11 @@ def run_adaptive(args, rank, world, dist):
         t, h, nev = run(t, h, args.steps)
     barrier()
     ms, launches = b.dropin_time(reset=True)
-    if dist:
-        tt = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
+    ms = ranks.max(ms)
     value = world * args.particles * args.steps / (ms * 1e-3)
     e2e = None
     if not args.no_e2e:
-        fresh = adaptive_workload(args.particles, args.seed + rank)
+        fresh = adaptive_workload(args.particles, args.seed, rank)
         barrier()
         t0 = time.perf_counter()
         b.upload(fresh)
@@ -283,10 +282,7 @@ def run_adaptive(args, rank, world, dist):
         x, v = b.download()
         barrier()
         e2e_s = time.perf_counter() - t0
-        if dist:
-            tt = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            e2e_s = float(tt.item())
+        e2e_s = ranks.max(e2e_s)
         h2d = fresh.n * (3 + 3 + 1 + 1 + 1 + 5) * 8
         e2e = {"value": world * args.particles * args.steps / e2e_s, "unit": UNIT,
                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": fresh.n * 48 / args.steps,
@@ -342,15 +338,12 @@ def run_hybrid(args, rank, world, dist):
 
     b = Backend("HYBRID")
     b.configure()
-    sysw = mce_init(workload(args.particles, args.seed + rank, HYBRID_NEAR), H, 3.0)
+    sysw = mce_init(workload(args.particles, args.seed, HYBRID_NEAR, rank), H, 3.0)
     b.upload(sysw)
     state = {"dtflag": 0}
 
-    def barrier():
-        torch.cuda.synchronize()
-        if dist:
-            dist.barrier()
-        torch.cuda.synchronize()
+    ranks = Ranks(dist, device="cuda")
+    barrier = ranks.barrier
 
     def run(t, nsteps):
         nev = pairs = 0
@@ -370,14 +363,11 @@ def run_hybrid(args, rank, world, dist):
     barrier()
     wall = time.perf_counter() - w0
     ms, launches = b.dropin_time(reset=True)
-    if dist:
-        tt = torch.tensor([ms, wall], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms, wall = float(tt[0].item()), float(tt[1].item())
+    ms, wall = ranks.max(ms), ranks.max(wall)
     value = world * args.particles * args.steps / (ms * 1e-3)
     e2e = None
     if not args.no_e2e:
-        fresh = mce_init(workload(args.particles, args.seed + rank, HYBRID_NEAR), H, 3.0)
+        fresh = mce_init(workload(args.particles, args.seed, HYBRID_NEAR, rank), H, 3.0)
         barrier()
         t0 = time.perf_counter()
         b.upload(fresh)
@@ -387,10 +377,7 @@ def run_hybrid(args, rank, world, dist):
         x, v = b.download()
         barrier()
         e2e_s = time.perf_counter() - t0
-        if dist:
-            tt = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            e2e_s = float(tt.item())
+        e2e_s = ranks.max(e2e_s)
         h2d = fresh.n * (3 + 3 + 1 + 1 + 1 + 5 + 1) * 8
         e2e = {"value": world * args.particles * args.steps / e2e_s, "unit": UNIT,
                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": fresh.n * 48 / args.steps,
@@ -450,11 +437,8 @@ def run_batch(args, rank, world, dist):
     import torch
     from mercuda_b200.backend import Backend, Batch
 
-    def barrier():
-        torch.cuda.synchronize()
-        if dist:
-            dist.barrier()
-        torch.cuda.synchronize()
+    ranks = Ranks(dist, device="cuda")
+    barrier = ranks.barrier
 
     b = Batch(systems, hs)
     b.advance(0.0, max(1, args.warmup), RCEN)
@@ -464,10 +448,7 @@ def run_batch(args, rank, world, dist):
     barrier()
     tm = b.timing()
     ms = tm["ms"]
-    if dist:
-        tt = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
+    ms = ranks.max(ms)
     value = world * total * args.steps / (ms * 1e-3)
     e2e = None
     if not args.no_e2e:
@@ -478,10 +459,7 @@ def run_batch(args, rank, world, dist):
         b2.download()
         barrier()
         e2e_s = time.perf_counter() - t0
-        if dist:
-            tt = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            e2e_s = float(tt.item())
+        e2e_s = ranks.max(e2e_s)
         nb = sum(s.n for s in systems)
         e2e = {"value": world * total * args.steps / e2e_s, "unit": UNIT,
                "h2d_bytes_per_step": nb * (3 + 3 + 1 + 1 + 1) * 8 / args.steps,
@@ -530,12 +508,11 @@ def run_batch(args, rank, world, dist):
 
 
 def run_adjoint(args, rank, world, dist):
-    from mercuda_b200.system import make_system
     metric = "adjoint MVS particle-steps/s"
 
-    def make(seed, n):
-        s_ = make_system(seed=seed, n_particles=n, near_fraction=0.0, h=H)
-        rng = np.random.default_rng(seed + 7)
+    def make(seed, n, rank=0):
+        s_ = workload(n, seed, 0.0, rank)
+        rng = np.random.default_rng(seed + 7 if rank == 0 else (seed + 7, rank))
         npart = s_.n - s_.nbig
         s_.ngf[s_.nbig:, 4] = np.exp(rng.uniform(np.log(1e-15), np.log(1e-13), npart)) * rng.choice([-1, 1], npart)
         return s_
@@ -569,7 +546,7 @@ def run_adjoint(args, rank, world, dist):
     import torch
     from mercuda_b200.adjoint import mvs_trajectory, timing
 
-    sysw = make(args.seed + rank, args.particles)
+    sysw = make(args.seed, args.particles, rank)
     nb = sysw.nbig
     dev = torch.device("cuda")
     big = (sysw.m[:nb], sysw.x[:nb], sysw.v[:nb])
@@ -582,12 +559,10 @@ def run_adjoint(args, rank, world, dist):
         (xf ** 2).sum().backward()
         return x0.grad, v0.grad, yar.grad
 
+    ranks = Ranks(dist, device="cuda")
     for _ in range(max(1, args.warmup)):
         once(sysw.x[nb:], sysw.v[nb:], sysw.ngf[nb:, 4])
-        break
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
+    ranks.barrier()
     with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clocks:
         t0 = time.perf_counter()
         g = once(sysw.x[nb:], sysw.v[nb:], sysw.ngf[nb:, 4])
@@ -595,10 +570,7 @@ def run_adjoint(args, rank, world, dist):
         e2e_s = time.perf_counter() - t0
     fwd, bwd = timing()
     ms = fwd + bwd
-    if dist:
-        tt = torch.tensor([ms, e2e_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms, e2e_s = float(tt[0].item()), float(tt[1].item())
+    ms, e2e_s = ranks.max(ms), ranks.max(e2e_s)
     value = world * args.particles * args.steps / (ms * 1e-3)
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -607,7 +579,7 @@ def run_adjoint(args, rank, world, dist):
                "sample": f"1000 particles x {args.steps} steps, forward-mode tangents of the oracle ({dt:.1f} s)"}
     if rank == 0:
         print(json.dumps({"metric": metric, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                          "warmup": 1, "ms_per_step": ms / args.steps, "higher_is_better": True,
+                          "warmup": max(1, args.warmup), "ms_per_step": ms / args.steps, "higher_is_better": True,
                           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                           "config": {"workload": workload_text, "particles_per_gpu": args.particles,
                                      "forward_ms": fwd, "backward_ms": bwd, "backward_over_forward": bwd / fwd,
@@ -664,32 +636,28 @@ def main():
     b.configure()
     if args.threads:
         b.set_launch(threads=args.threads)
-    # Weak scaling: every rank integrates its own independent particle set
-    # (no data-path collective); the seed differs per rank.
-    sysw = workload(args.particles, args.seed + rank)
+    # Weak scaling: every rank integrates its own share of the job's
+    # particles about the same planets (no data-path collective).
+    sysw = workload(args.particles, args.seed, rank=rank)
     b.upload(sysw)
+    e_start, l_start = b.energy(H, physical=True)    # mxx_en of the corrected start state
     peak_tflops = b.fp64_peak()
     # warm-up
     if args.warmup > 0:
         b.mvs_advance(0.0, H, args.warmup, RCEN, args.steps_per_launch)
     t_start = args.warmup * H
 
-    def barrier():
-        torch.cuda.synchronize()
-        if dist:
-            dist.barrier()
-        torch.cuda.synchronize()
+    ranks = Ranks(dist, device="cuda")
+    barrier = ranks.barrier
 
     barrier()
     with ClockSampler(local) as clocks:
         events, steps = b.mvs_advance(t_start, H, args.steps, RCEN, args.steps_per_launch)
     barrier()
     tm = b.timing()
+    e_end, l_end = b.energy(H, physical=True)
     ms = tm["advance_ms"]
-    if dist:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = ranks.max(ms)
     value = world * args.particles * args.steps / (ms * 1e-3)
     launches = tm["particle_launches"]
     kernel_ms = tm["particle_kernel_ms"] / max(1, launches)
@@ -702,20 +670,22 @@ def main():
     if not args.no_e2e:
         # Through the public C ABI with host buffers: upload (H2D) + the fused
         # multi-step run + event records and final state back (D2H).
-        fresh = workload(args.particles, args.seed + rank)
+        # Through the sharded driver: rank 0 receives the whole job's event
+        # records (global ids); each rank reads its own states back.
+        fresh = workload(args.particles, args.seed, rank=rank)
+        nbig = fresh.nbig
+        ids = np.concatenate([np.arange(nbig), nbig + rank * args.particles + np.arange(args.particles)])
+        run = ShardedRun(ranks, b)
         barrier()
         t0 = time.perf_counter()
-        b.upload(fresh)
-        ev2, _ = b.mvs_advance(0.0, H, args.steps, RCEN, args.steps_per_launch)
-        x, v = b.download()
+        run.upload(fresh, ids, nbig + world * args.particles)
+        got = run.advance(0.0, H, args.steps, RCEN, args.steps_per_launch)
+        x, v = run.download(gather=False)
         barrier()
         e2e_s = time.perf_counter() - t0
-        if dist:
-            t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_s = float(t.item())
+        e2e_s = ranks.max(e2e_s)
         h2d = fresh.n * (3 + 3 + 1 + 1 + 1 + 5) * 8
-        d2h = fresh.n * 6 * 8 + len(ev2) * 128
+        d2h = fresh.n * 6 * 8 + run.local_events * 128
         e2e = {"value": world * args.particles * args.steps / e2e_s, "unit": UNIT,
                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                "note": "wall clock around the synchronous C-ABI calls: upload, fused run, download, events"}
@@ -749,6 +719,8 @@ def main():
             "clocks": clk,
             "gpu_launches": tm["kernel_launches"],
             "events": int(len(events)),
+            "energy_error": abs(e_end - e_start) / abs(e_start),
+            "angular_momentum_error": abs(l_end - l_start) / abs(l_start),
             "e2e": e2e,
             "cpu_baseline": cpu,
         }

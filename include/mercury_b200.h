@@ -31,6 +31,16 @@ int mercury_b200_timing(double* advance_ms, double* particle_kernel_ms, int* par
  * kernels they launched, since the last call with reset != 0 (which zeroes
  * both). No counterpart in the reference. */
 int mercury_b200_dropin_time(double* ms, int64_t* launches, int reset);
+/* Energy and angular momentum of the resident system: mxx_en
+ * (mercury6_2.for:7226-7315, barycentric through mco_h2b, 2348-2405) applied
+ * to the heliocentric state that mercury_cuda_export(h, physical, ...) would
+ * return, computed on the device with the same statement order as the
+ * Fortran, so that e and l2 equal a CPU mxx_en on the exported arrays bit for
+ * bit. spin is the (3, n) array of spin angular momenta (Fortran s(3,nbod)),
+ * or NULL for none; *e receives the energy, *l2 the angular momentum's
+ * magnitude. The reference host calls mxx_en itself after downloading every
+ * body (mercury6_2.for:919-920); this reads back two numbers instead. */
+int mercury_b200_energy(double h, int physical, const double* spin, double* e, double* l2);
 /* Launch shape of the particle kernel: threads per CTA (multiple of 32) and
  * steps fused per launch (0 = automatic); a negative value keeps the setting. */
 int mercury_b200_set_launch(int particle_threads, int steps_per_launch);

@@ -49,7 +49,8 @@ EXTENSION_SYMBOLS = ["mercury_b200_mvs_advance", "mercury_b200_events", "mercury
                      "mercury_b200_dropin_time", "mercury_b200_batch_upload", "mercury_b200_batch_advance",
                      "mercury_b200_batch_events", "mercury_b200_batch_download", "mercury_b200_batch_set",
                      "mercury_b200_batch_timing", "mercury_b200_batch_free", "mercury_b200_adjoint_forward",
-                     "mercury_b200_adjoint_backward", "mercury_b200_adjoint_timing", "mercury_b200_adjoint_free"]
+                     "mercury_b200_adjoint_backward", "mercury_b200_adjoint_timing", "mercury_b200_adjoint_free",
+                     "mercury_b200_energy"]
 
 
 class BackendError(RuntimeError):
@@ -91,6 +92,7 @@ def load_library(path: Path | str | None = None) -> C.CDLL:
     L.mercury_b200_set_launch.argtypes = [I, I]
     L.mercury_b200_fp64_peak.argtypes = [PD, PD]
     L.mercury_b200_dropin_time.argtypes = [PD, PI64, I]
+    L.mercury_b200_energy.argtypes = [D, I, PD, PD, PD]
     L.mercury_b200_batch_upload.argtypes = [I, PI, PI, PD, PD, PD, PD, PD, PD]
     L.mercury_b200_batch_advance.argtypes = [D, I, D, PI]
     L.mercury_b200_batch_events.argtypes = [C.c_void_p, PI, PI, I]
@@ -338,6 +340,16 @@ class Backend:
         ms, n = D(0.0), C.c_int64(0)
         self.lib.mercury_b200_dropin_time(C.byref(ms), C.byref(n), int(reset))
         return ms.value, n.value
+
+    def energy(self, h: float = 0.0, physical: bool = False, spin: np.ndarray | None = None):
+        """(e, l2) of mxx_en on the state export(h, physical) returns; spin is
+        (n, 3) or None."""
+        e, l2 = D(0.0), D(0.0)
+        sp = None if spin is None else np.ascontiguousarray(spin, dtype=np.float64)
+        if self.lib.mercury_b200_energy(float(h), int(physical), _p(sp) if sp is not None else None,
+                                        C.byref(e), C.byref(l2)) != 0:
+            raise BackendError("energy check failed")
+        return e.value, l2.value
 
     def fp64_peak(self):
         tf, ms = D(0.0), D(0.0)

@@ -10,6 +10,7 @@
 #include "bs.cuh"
 #include "hybrid.cuh"
 #include "radau.cuh"
+#include "energy.cuh"
 
 namespace mb200 {
 
@@ -558,7 +559,9 @@ void screen_pairs(double h) {
 // mco_mvs2h of the current MVS state into host rows (the reference exports
 // with its corrector on scratch copies, mercury_cuda.cu:508-513); the state
 // itself is not changed.
-void export_corrected(double h, double* xx, double* vv) {
+// The output corrector of MVS (mco_mvs2h) on scratch copies: corr_big and
+// (unless big_only) corr_part receive the corrected heliocentric states.
+void run_corrector(double h, bool big_only = false) {
     Context& c = ctx();
     const int nbig = c.nbig;
     ensure_tables(4, 1);
@@ -570,7 +573,7 @@ void export_corrected(double h, double* xx, double* vv) {
     b.out.v = c.corr_big.p + 3 * nbig;
     b.out.a = c.corr_big.p + 6 * nbig;
     CorrectorArgs k{};
-    k.np = c.np;
+    k.np = big_only ? 0 : c.np;
     k.npcap = c.npcap;
     k.nb = nbig - 1;
     k.ngf_on = (c.ngflag == 1 || c.ngflag == 3);
@@ -592,6 +595,12 @@ void export_corrected(double h, double* xx, double* vv) {
     check(cudaGetLastError(), "corrector");
     read_status();
     if (c.status_host->fault) throw std::runtime_error("Output corrector failed");
+}
+
+void export_corrected(double h, double* xx, double* vv) {
+    Context& c = ctx();
+    const int nbig = c.nbig;
+    run_corrector(h);
     c.transfer.reserve((size_t)6 * c.n);
     for (int part = 0; part < 2; ++part) {
         gather_kernel<<<blocks(c.n), 256, 0, c.stream>>>(c.transfer.p, c.n, 3, nbig, c.corr_big.p + 3 * part * nbig,
@@ -1604,6 +1613,51 @@ int mercury_b200_dropin_time(double* ms, int64_t* launches, int reset) {
         g_contexts[1].dropin_launches = 0;
     }
     return 0;
+}
+
+int mercury_b200_energy(double h, int physical, const double* spin, double* e, double* l2) {
+    Context& c = ctx();
+    try {
+        require_system();
+        // the massive set ends at the last massive body (MVS takes massless
+        // Small bodies only; the other integrators keep bodies up to nmass)
+        if (c.nmass != c.nsplit) throw std::runtime_error("massive bodies outside the massive set");
+        EnergyArgs a{};
+        a.nm = c.nmass;
+        a.mbig = c.mbig.p;
+        if (physical && c.algorithm == 1) {
+            run_corrector(h, true);
+            a.big = c.corr_big.p;
+            a.bs = c.nbig;
+        } else {
+            a.big = c.bigstate[c.cur].p;
+            a.bs = c.nsplit;
+            if (physical && c.algorithm == 10) {
+                c.hy_off.reserve(6);
+                launch_dh_shift(c.bigstate[c.cur].p, c.mbig.p, c.nsplit, c.m_host[0], c.hy_off.p, c.stream);
+                a.voff = c.hy_off.p;
+            }
+        }
+        for (int q = 0; q < 3; ++q) a.jcen[q] = c.jcen[q];
+        // spin angular momenta first, in body order (mxx_en's first loop)
+        for (int q = 0; q < 3; ++q) a.spin[q] = 0.0;
+        if (spin)
+            for (int j = 0; j < c.n; ++j)
+                for (int q = 0; q < 3; ++q) a.spin[q] = a.spin[q] + spin[3 * (size_t)j + q];
+        c.energy_scr.reserve((size_t)c.nmass + 2);
+        a.tmp = c.energy_scr.p;
+        a.out = c.energy_scr.p + c.nmass;
+        launch_energy(a, c.stream);
+        check(cudaGetLastError(), "energy");
+        double out[2];
+        check(cudaMemcpyAsync(out, a.out, sizeof(out), cudaMemcpyDeviceToHost, c.stream), "energy");
+        check(cudaStreamSynchronize(c.stream), "energy");
+        if (e) *e = out[0];
+        if (l2) *l2 = out[1];
+        return 0;
+    } catch (const std::exception& ex) {
+        return report(ex);
+    }
 }
 
 int mercury_b200_set_launch(int particle_threads, int steps_per_launch) {

@@ -90,6 +90,7 @@ struct Context {
     DBuf<unsigned long long> ra_max;
     // output corrector scratch: Big [9][nbig], particles [6][npcap]
     DBuf<double> corr_big, corr_part;
+    DBuf<double> energy_scr;         // mxx_en: per-body pair sums, then e and l2
     // Bulirsch-Stoer: massive-set scratch, per-level candidate states, per-level
     // error maxima and force-fault words
     DBuf<double> bs_scr, bs_bcand, bs_pcand;
@@ -165,7 +166,7 @@ struct Context {
     void release_all() {
         DBuf<double>* bufs[] = {&mbig, &rcebig, &rphysbig, &ngfbig, &bigstate[0], &bigstate[1], &pstate[0],
                                 &pstate[1], &pconst[0], &pconst[1], &tab, &detail, &transfer, &snapshot, &snap_const,
-                                &ra_bb, &ra_be, &ra_bg, &ra_bpx, &ra_pb, &ra_pe, &ftab, &force_out, &boxes, &corr_big, &corr_part,
+                                &ra_bb, &ra_be, &ra_bg, &ra_bpx, &ra_pb, &ra_pe, &ftab, &force_out, &boxes, &corr_big, &corr_part, &energy_scr,
                                 &bs_scr, &bs_bcand, &bs_pcand, &rcritbig, &hy_scr, &hy_tab, &hy_off,
                                 &hy_packed};
         for (auto* b : bufs) b->release();

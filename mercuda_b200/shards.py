@@ -1,0 +1,165 @@
+"""Test particles split across ranks (one process per GPU).
+
+Massless test particles act on nothing, so the MVS integration of one system
+shards by particle with no data-path exchange: every rank holds the central
+body and all Big bodies (integrated redundantly, the same way on every rank)
+and its own subset of the particles. The only collective steps are the
+barriers around a timed region, the maximum of the ranks' times, and the
+gathering of event records and final states at the output boundary — the
+host-side equivalent of the reference's per-step event list and download
+(mercury_cuda.cu:466-493, the records of mercury_gpu.f90:206-247), now with
+global body ids.
+
+Every rank takes the same collective steps in the same order. The classes are
+backend-agnostic: `ShardedRun` drives any object with the `upload`,
+`mvs_advance`, `download` methods of `backend.Backend`, and `Ranks` works over
+NCCL (CUDA tensors) or gloo (CPU tensors).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .system import System
+
+
+class Ranks:
+    """Rank plumbing over a torch.distributed process group (or one process)."""
+
+    def __init__(self, dist=None, device=None):
+        self.dist = dist if dist is not None and dist.is_initialized() else None
+        self.world = self.dist.get_world_size() if self.dist else 1
+        self.rank = self.dist.get_rank() if self.dist else 0
+        if device is None:
+            device = "cuda" if self.dist and self.dist.get_backend() == "nccl" else "cpu"
+        self.device = device
+
+    def _sync(self):
+        if str(self.device).startswith("cuda"):
+            import torch
+            torch.cuda.synchronize()
+
+    def barrier(self) -> None:
+        """Device idle, then all ranks, then device idle again."""
+        self._sync()
+        if self.dist:
+            self.dist.barrier()
+        self._sync()
+
+    def max(self, value: float) -> float:
+        """The maximum of a per-rank number (a time) over all ranks."""
+        if not self.dist:
+            return float(value)
+        import torch
+        t = torch.tensor([float(value)], dtype=torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def gather(self, obj, everywhere: bool = False):
+        """Every rank's object in rank order: on rank 0 (None elsewhere), or on
+        every rank."""
+        if not self.dist:
+            return [obj]
+        out = [None] * self.world
+        if everywhere:
+            self.dist.all_gather_object(out, obj)
+            return out
+        self.dist.gather_object(obj, out if self.rank == 0 else None, dst=0)
+        return out if self.rank == 0 else None
+
+    def whole_job(self, units_per_rank: float, seconds: float) -> float:
+        """Throughput of the job: all ranks' units over the slowest rank's time."""
+        return self.world * units_per_rank / seconds
+
+
+def particle_shard(sys: System, rank: int, world: int) -> tuple[System, np.ndarray]:
+    """The system with all Big bodies and every world-th particle starting at
+    `rank`, and the 0-based body indices in `sys` of the shard's bodies."""
+    if not 0 <= rank < world:
+        raise ValueError("rank outside the world")
+    idx = np.concatenate([np.arange(sys.nbig), np.arange(sys.nbig + rank, sys.n, world)])
+    take = lambda a: np.ascontiguousarray(a[idx])
+    shard = System(m=take(sys.m), x=take(sys.x), v=take(sys.v), nbig=sys.nbig, ngf=take(sys.ngf),
+                   jcen=sys.jcen.copy(), rce=take(sys.rce), rphys=take(sys.rphys), rcrit=take(sys.rcrit),
+                   rceh=take(sys.rceh), rho=take(sys.rho), pn=sys.pn)
+    return shard, idx
+
+
+def order_events(events: np.ndarray, steps: np.ndarray):
+    """Records ordered by step, then by the pair (min(i, j), max(i, j)) as the
+    reference sorts one step's list (mercury_cuda.cu:487-490); stable."""
+    lo = np.minimum(events["i"], events["j"])
+    hi = np.maximum(events["i"], events["j"])
+    order = np.lexsort((hi, lo, steps))
+    return events[order], steps[order]
+
+
+class ShardedRun:
+    """One rank's share of an MVS integration whose particles are split
+    across ranks. `advance` returns the whole system's event records (global
+    1-based ids) on rank 0 and None elsewhere; `download` the whole system's
+    states on rank 0 (or each rank's own shard with gather=False)."""
+
+    def __init__(self, ranks: Ranks, backend):
+        self.ranks = ranks
+        self.backend = backend
+        self.ids = None
+        self.nbig = 0
+        self.n = 0
+        self.local_events = 0
+
+    def upload(self, shard: System, ids: np.ndarray, n_total: int) -> None:
+        """This rank's shard and the global 0-based index of each of its bodies
+        (Big bodies first, the same on every rank); n_total bodies in all."""
+        ids = np.asarray(ids, dtype=np.int64)
+        if len(ids) != shard.n or np.any(ids[:shard.nbig] != np.arange(shard.nbig)):
+            raise ValueError("a shard holds every Big body first, then its particles")
+        self.ids = ids
+        self.identity = bool(np.array_equal(ids, np.arange(len(ids))))
+        self.nbig = shard.nbig
+        self.n = int(n_total)
+        # every rank must agree on the Big bodies and the total
+        seen = self.ranks.gather((self.nbig, self.n), everywhere=True)
+        if any(s != seen[0] for s in seen):
+            raise ValueError("ranks disagree on the Big bodies or the body count")
+        self.backend.upload(shard)
+
+    def _to_global(self, events: np.ndarray) -> np.ndarray:
+        if self.identity:
+            return events
+        ev = events.copy()
+        for f in ("i", "j"):
+            ev[f] = self.ids[ev[f] - 1] + 1
+        return ev
+
+    def advance(self, time: float, h: float, nsteps: int, rcen: float, steps_per_launch: int = 0):
+        events, steps = self.backend.mvs_advance(time, h, nsteps, rcen, steps_per_launch)
+        self.local_events = len(events)   # records read back from this rank's device
+        events = self._to_global(events)
+        if self.ranks.rank != 0:
+            # records among the central and Big bodies are the same on every
+            # rank: rank 0 reports them
+            particle = np.maximum(events["i"], events["j"]) > self.nbig
+            events, steps = events[particle], steps[particle]
+        parts = self.ranks.gather((events, steps))
+        if parts is None:
+            return None
+        if len(parts) == 1:
+            # the backend's order, which the monotone id map keeps
+            return parts[0]
+        ev = np.concatenate([p[0] for p in parts])
+        st = np.concatenate([p[1] for p in parts])
+        return order_events(ev, st)
+
+    def download(self, gather: bool = True):
+        x, v = self.backend.download()
+        if not gather:
+            return x, v
+        parts = self.ranks.gather((self.ids, x, v))
+        if parts is None:
+            return None
+        X = np.zeros((self.n, 3))
+        V = np.zeros((self.n, 3))
+        for ids, xs, vs in parts:
+            X[ids] = xs
+            V[ids] = vs
+        return X, V

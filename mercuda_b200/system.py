@@ -160,7 +160,8 @@ def planets(rng: np.random.Generator, nplanets: int = 8, mmin: float = 1.7e-7, m
 
 def make_system(seed: int = 1, n_particles: int = 10_000, nplanets: int = 8, near_fraction: float = 0.0,
                 h: float = 8.0, rceh_big: float = 3.0, cefac: float = 3.0, pa=(0.5, 5.0),
-                pe_max: float = 0.2, pi_max_deg: float = 10.0, planet_kw: dict | None = None) -> System:
+                pe_max: float = 0.2, pi_max_deg: float = 10.0, planet_kw: dict | None = None,
+                particle_seed=None) -> System:
     """Seeded synthetic system with the element distributions of the MVS workloads.
 
     Central mass 1 Msun; ``nplanets`` Big bodies (masses log-uniform 1.7e-7 to
@@ -169,11 +170,15 @@ def make_system(seed: int = 1, n_particles: int = 10_000, nplanets: int = 8, nea
     uniform. ``near_fraction`` of the particles are instead placed inside 5 Hill
     radii of a randomly chosen planet (a offset <= 5 R_H, same mean anomaly
     within R_H/a) so that encounter events fire. ``rceh_big`` is the Big bodies'
-    ``r=`` token (encounter radius in Hill radii).
+    ``r=`` token (encounter radius in Hill radii). With ``particle_seed`` the
+    particles come from their own generator of that seed and the planets from
+    ``seed`` alone: shards of one system with the same planets.
     """
     rng = np.random.default_rng(seed)
     m0 = K2
     mass, pa_, pe_, pi_, pn_, pw_, pM_ = planets(rng, nplanets, **(planet_kw or {}))
+    if particle_seed is not None:
+        rng = np.random.default_rng(particle_seed)
     n = 1 + nplanets + n_particles
     m = np.zeros(n)
     m[0] = m0

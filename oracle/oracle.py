@@ -89,6 +89,8 @@ def lib() -> C.CDLL:
         L.oracle_mfo_hy.argtypes = [I, I, PD, PD, PD, PD, PD]
         L.oracle_mvs_jacobian.argtypes = [I, I, PD, PD, PD, PD, I, PD, D, I, PD]
         L.oracle_mvs_jacobian.restype = I
+        L.oracle_mxx_en.argtypes = [I, PD, PD, PD, C.c_void_p, PD, PD]
+        L.oracle_mxx_en.restype = None
         _lib = L
     return _lib
 
@@ -301,3 +303,16 @@ def mvs_jacobian(sys, h, nsteps):
     if rc:
         raise RuntimeError("oracle Jacobian run failed")
     return jac
+
+
+def mxx_en(m, x, v, jcen, spin=None):
+    """mxx_en (mercury6_2.for:7226-7315) of heliocentric x, v (n, 3): (e, l2)."""
+    m = np.ascontiguousarray(m, dtype=np.float64)
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    v = np.ascontiguousarray(v, dtype=np.float64)
+    jcen = np.ascontiguousarray(jcen, dtype=np.float64)
+    sp = None if spin is None else np.ascontiguousarray(spin, dtype=np.float64)
+    out = np.zeros(2)
+    lib().oracle_mxx_en(len(m), _p(m), _p(x), _p(v), sp.ctypes.data_as(C.c_void_p) if sp is not None else None,
+                        _p(jcen), _p(out))
+    return float(out[0]), float(out[1])

@@ -13,6 +13,7 @@
 #include "oracle_bs.hpp"
 #include "oracle_hy.hpp"
 #include "oracle_dual.hpp"
+#include "oracle_energy.hpp"
 
 namespace oracle {
 thread_local Tally tally;
@@ -453,6 +454,12 @@ int oracle_mvs_jacobian(int n, int nbig, const double* m, double* x, double* v, 
             }
     }
     return 0;
+}
+
+// mxx_en of n bodies (Fortran layout); s may be null. out = {e, l2}.
+void oracle_mxx_en(int n, const double* m, const double* xh, const double* vh, const double* s, const double* jcen,
+                   double* out) {
+    oracle::mxx_en<double>(jcen, n, m, xh, vh, s, out[0], out[1]);
 }
 
 }  // extern "C"
