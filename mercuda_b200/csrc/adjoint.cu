@@ -2,17 +2,21 @@
 // reference): a forward run that keeps checkpoints, then a reverse sweep.
 //
 // The Big bodies never feel massless particles, so their trajectory (and
-// each step's force table) is fixed: one Big-body CTA integrates it once for
-// all steps. Each particle's final state is then a function of its own
-// initial position, velocity and Yarkovsky coefficient only, and the reverse
-// sweep is one thread per particle:
+// each step's force table) is fixed: one Big-body CTA integrates it, K steps
+// per launch on a second stream, ahead of the particles. Each particle's
+// final state is then a function of its own initial position, velocity and
+// Yarkovsky coefficient only, and the reverse sweep is one thread per
+// particle:
 //
-//   forward:  the mdt_mvs step of every particle (the same statements as the
-//             MVS kernels), (x, v, a) stored every K steps
-//   backward: per K-step segment, from the last: recompute the segment from
-//             its checkpoint keeping each step's drift input and output, then
+//   forward:  per K-step segment, the mdt_mvs step of every particle (the
+//             same statements as the MVS kernels); (x, v, a) at each
+//             segment's start is the checkpoint
+//   backward: per segment, from the last: recompute the segment from its
+//             checkpoint keeping each step's drift input and output, then
 //             walk it backwards: kick, force (gravity from the table, yar) and
-//             the Kepler drift's state-transition matrix, transposed.
+//             the Kepler drift's state-transition matrix, transposed. The
+//             recomputation of segment k-1 (second stream, second record
+//             buffer) overlaps the walk through segment k.
 #include <cmath>
 #include <cstdio>
 
@@ -38,7 +42,7 @@ struct AdjArgs {
     double* xf;              // (np, 3)
     double* vf;
     double* ckpt;            // [nseg][9][np]
-    double* rec;             // [K][REC][np]
+    double* rec;             // [K][REC][np] records of one segment
     double* lam;             // [10][np] adjoint state between segments
     const double* gx;        // (np, 3) adjoint of the final positions
     const double* gv;        // (np, 3) or null
@@ -122,17 +126,29 @@ __device__ __forceinline__ void st_ckpt(double* c, int np, int p, double3 x, dou
     for (int k = 0; k < 9; ++k) c[(size_t)k * np + p] = q[k];
 }
 
-template <bool YAR> __global__ void __launch_bounds__(128) adj_forward_kernel(AdjArgs A) {
+// One K-step segment of the forward run: from the initial state (segment 0)
+// or the segment's checkpoint, to the next checkpoint or the final state.
+template <bool YAR> __global__ void __launch_bounds__(128) adj_forward_kernel(AdjArgs A, int seg) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= A.np) return;
-    const int stride = tab_stride(A.nb);
+    const int stride = tab_stride(A.nb), np = A.np;
     const double hby2 = 0.5 * A.h;
     const double yar = YAR ? A.yar[p] : 0.0;
-    double3 x = ld_row(A.x0, p), v = ld_row(A.v0, p);
-    double3 acc = accel<YAR>(x, v, yar, A.tab, A.nb, A.mu, A.status);
+    const int s0 = seg * A.K, s1 = min(A.nsteps, s0 + A.K);
+    double3 x, v, acc;
+    if (seg == 0) {
+        x = ld_row(A.x0, p);
+        v = ld_row(A.v0, p);
+        acc = accel<YAR>(x, v, yar, A.tab, A.nb, A.mu, A.status);
+        st_ckpt(A.ckpt, np, p, x, v, acc);
+    } else {
+        const double* c = A.ckpt + (size_t)seg * 9 * np;
+        x = make_double3(c[p], c[np + p], c[2 * (size_t)np + p]);
+        v = make_double3(c[3 * (size_t)np + p], c[4 * (size_t)np + p], c[5 * (size_t)np + p]);
+        acc = make_double3(c[6 * (size_t)np + p], c[7 * (size_t)np + p], c[8 * (size_t)np + p]);
+    }
 #pragma unroll 1
-    for (int s = 0; s < A.nsteps; ++s) {
-        if (s % A.K == 0) st_ckpt(A.ckpt + (size_t)(s / A.K) * 9 * A.np, A.np, p, x, v, acc);
+    for (int s = s0; s < s1; ++s) {
         v.x = v.x + hby2 * acc.x;
         v.y = v.y + hby2 * acc.y;
         v.z = v.z + hby2 * acc.z;
@@ -142,8 +158,12 @@ template <bool YAR> __global__ void __launch_bounds__(128) adj_forward_kernel(Ad
         v.y = v.y + hby2 * acc.y;
         v.z = v.z + hby2 * acc.z;
     }
-    st_row(A.xf, p, x);
-    st_row(A.vf, p, v);
+    if (s1 < A.nsteps) {
+        st_ckpt(A.ckpt + (size_t)(seg + 1) * 9 * np, np, p, x, v, acc);
+    } else {
+        st_row(A.xf, p, x);
+        st_row(A.vf, p, v);
+    }
 }
 
 // Reverse sweep, per segment (last first): recompute the segment from its
@@ -246,22 +266,33 @@ struct Adjoint {
     int nbig = 0, np = 0, nsteps = 0, K = 0, has_yar = 0;
     double h = 0.0, mu = 0.0;
     const double *x0 = nullptr, *v0 = nullptr, *yar = nullptr;
-    DBuf<double> bigstate[2], mbig, zeros, tab, detail, ckpt, rec, lam;
+    DBuf<double> bigstate[2], mbig, zeros, tab, detail, ckpt, rec[2], lam;
     DBuf<MercuryEvent> events;
     DBuf<int> event_step;
     DBuf<DeviceStatus> status;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr, stream2 = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
+    std::vector<cudaEvent_t> done2, done1;   // per segment: second-stream and main-stream work finished
     float fwd_ms = 0.0f, bwd_ms = 0.0f;
     bool ready = false;
     void ensure() {
         if (stream) return;
         check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "stream");
+        check(cudaStreamCreateWithFlags(&stream2, cudaStreamNonBlocking), "stream");
         check(cudaEventCreate(&e0), "event");
         check(cudaEventCreate(&e1), "event");
     }
+    void ensure_events(int n) {
+        while ((int)done2.size() < n) {
+            cudaEvent_t a, b;
+            check(cudaEventCreateWithFlags(&a, cudaEventDisableTiming), "event");
+            check(cudaEventCreateWithFlags(&b, cudaEventDisableTiming), "event");
+            done2.push_back(a);
+            done1.push_back(b);
+        }
+    }
     void release() {
-        DBuf<double>* b[] = {&bigstate[0], &bigstate[1], &mbig, &zeros, &tab, &detail, &ckpt, &rec, &lam};
+        DBuf<double>* b[] = {&bigstate[0], &bigstate[1], &mbig, &zeros, &tab, &detail, &ckpt, &rec[0], &rec[1], &lam};
         for (auto* d : b) d->release();
         events.release();
         event_step.release();
@@ -289,7 +320,7 @@ AdjArgs adj_args(Adjoint& J) {
     a.v0 = J.v0;
     a.yar = J.yar;
     a.ckpt = J.ckpt.p;
-    a.rec = J.rec.p;
+    a.rec = J.rec[0].p;
     a.lam = J.lam.p;
     a.status = J.status.p;
     return a;
@@ -328,7 +359,9 @@ int mercury_b200_adjoint_forward(int nbig, const double* mbig, const double* xbi
         J.tab.reserve((size_t)(nsteps + 1) * tab_stride(nb));
         J.detail.reserve((size_t)nsteps * std::max(1, nb) * TAB_DETAIL);
         J.ckpt.reserve((size_t)nseg * 9 * np);
-        J.rec.reserve((size_t)J.K * REC * np);
+        J.rec[0].reserve((size_t)J.K * REC * np);
+        J.rec[1].reserve(nseg > 1 ? (size_t)J.K * REC * np : 1);
+        J.ensure_events(nseg);
         J.lam.reserve((size_t)10 * np);
         J.events.reserve(4096);
         J.event_step.reserve(4096);
@@ -345,34 +378,44 @@ int mercury_b200_adjoint_forward(int nbig, const double* mbig, const double* xbi
         check(cudaMemsetAsync(J.zeros.p, 0, sizeof(double) * nbig, J.stream), "memset");
         check(cudaMemsetAsync(J.status.p, 0, sizeof(DeviceStatus), J.stream), "memset");
         check(cudaEventRecord(J.e0, J.stream), "event");
-        // the Big bodies' steps and every step's force table, in one launch
-        MvsBigArgs a{};
-        a.nbig = nbig;
-        a.reset = 1;
-        a.nsteps = nsteps;
-        a.h = h;
-        a.m = J.mbig.p;
-        a.rce = J.zeros.p;
-        a.rphys = J.zeros.p;
-        a.in.x = J.bigstate[0].p;
-        a.in.v = J.bigstate[0].p + 3 * nbig;
-        a.in.a = J.bigstate[0].p + 6 * nbig;
-        a.out.x = J.bigstate[1].p;
-        a.out.v = J.bigstate[1].p + 3 * nbig;
-        a.out.a = J.bigstate[1].p + 6 * nbig;
-        a.tab = J.tab.p;
-        a.detail = J.detail.p;
-        a.events = J.events.p;
-        a.event_step = J.event_step.p;
-        a.event_cap = (int)J.events.n;
-        a.status = J.status.p;
-        launch_mvs_big(a, J.stream);
+        check(cudaStreamWaitEvent(J.stream2, J.e0, 0), "wait");
         AdjArgs f = adj_args(J);
         f.xf = x_final;
         f.vf = v_final;
-        const int grid = (np + 127) / 128;
-        if (J.has_yar) adj_forward_kernel<true><<<grid, 128, 0, J.stream>>>(f);
-        else adj_forward_kernel<false><<<grid, 128, 0, J.stream>>>(f);
+        const int grid = (np + 127) / 128, stride = tab_stride(nb);
+        for (int seg = 0; seg < nseg; ++seg) {
+            const int s0 = seg * J.K, ks = std::min(J.K, nsteps - s0);
+            // the Big bodies' steps of this segment and their force tables
+            // (rows s0 + 1 .. s0 + ks; row 0 too on the first)
+            MvsBigArgs a{};
+            a.nbig = nbig;
+            a.reset = seg == 0 ? 1 : 0;
+            a.nsteps = ks;
+            a.step0 = s0;
+            a.h = h;
+            a.m = J.mbig.p;
+            a.rce = J.zeros.p;
+            a.rphys = J.zeros.p;
+            double* bin = J.bigstate[seg & 1].p;
+            double* bout = J.bigstate[(seg + 1) & 1].p;
+            a.in.x = bin;
+            a.in.v = bin + 3 * nbig;
+            a.in.a = bin + 6 * nbig;
+            a.out.x = bout;
+            a.out.v = bout + 3 * nbig;
+            a.out.a = bout + 6 * nbig;
+            a.tab = J.tab.p + (size_t)s0 * stride;
+            a.detail = J.detail.p + (size_t)s0 * std::max(1, nb) * TAB_DETAIL;
+            a.events = J.events.p;
+            a.event_step = J.event_step.p;
+            a.event_cap = (int)J.events.n;
+            a.status = J.status.p;
+            launch_mvs_big(a, J.stream2);
+            check(cudaEventRecord(J.done2[seg], J.stream2), "event");
+            check(cudaStreamWaitEvent(J.stream, J.done2[seg], 0), "wait");
+            if (J.has_yar) adj_forward_kernel<true><<<grid, 128, 0, J.stream>>>(f, seg);
+            else adj_forward_kernel<false><<<grid, 128, 0, J.stream>>>(f, seg);
+        }
         check(cudaEventRecord(J.e1, J.stream), "event");
         check(cudaGetLastError(), "launch");
         DeviceStatus st;
@@ -400,17 +443,30 @@ int mercury_b200_adjoint_backward(const double* gx, const double* gv, double* dx
         a.dv0 = dv0;
         a.dyar = dyar;
         check(cudaEventRecord(J.e0, J.stream), "event");
+        check(cudaStreamWaitEvent(J.stream2, J.e0, 0), "wait");
         const int grid = (J.np + 127) / 128;
         const int nseg = (J.nsteps + J.K - 1) / J.K;
+        // segment seg's records live in rec[seg & 1]: recomputing seg - 1 on
+        // the second stream waits only for the walk through seg + 1, the last
+        // reader of that buffer
+        auto recompute = [&](int seg) {
+            AdjArgs r = a;
+            r.rec = J.rec[seg & 1].p;
+            if (seg + 2 < nseg) check(cudaStreamWaitEvent(J.stream2, J.done1[seg + 2], 0), "wait");
+            if (J.has_yar) adj_recompute_kernel<true><<<grid, 128, 0, J.stream2>>>(r, seg);
+            else adj_recompute_kernel<false><<<grid, 128, 0, J.stream2>>>(r, seg);
+            check(cudaEventRecord(J.done2[seg], J.stream2), "event");
+        };
+        recompute(nseg - 1);
         for (int seg = nseg - 1; seg >= 0; --seg) {
             const int last = seg == nseg - 1 ? 1 : 0;
-            if (J.has_yar) {
-                adj_recompute_kernel<true><<<grid, 128, 0, J.stream>>>(a, seg);
-                adj_vjp_kernel<true><<<grid, 128, 0, J.stream>>>(a, seg, last);
-            } else {
-                adj_recompute_kernel<false><<<grid, 128, 0, J.stream>>>(a, seg);
-                adj_vjp_kernel<false><<<grid, 128, 0, J.stream>>>(a, seg, last);
-            }
+            if (seg > 0) recompute(seg - 1);
+            check(cudaStreamWaitEvent(J.stream, J.done2[seg], 0), "wait");
+            AdjArgs w = a;
+            w.rec = J.rec[seg & 1].p;
+            if (J.has_yar) adj_vjp_kernel<true><<<grid, 128, 0, J.stream>>>(w, seg, last);
+            else adj_vjp_kernel<false><<<grid, 128, 0, J.stream>>>(w, seg, last);
+            check(cudaEventRecord(J.done1[seg], J.stream), "event");
         }
         check(cudaEventRecord(J.e1, J.stream), "event");
         check(cudaGetLastError(), "launch");

@@ -27,13 +27,22 @@ namespace mb200 {
 // the rest by c_k = 1/k! - z c_{k+2}; beyond, the closed forms.
 MB200_HD inline void stumpff6(double z, double c[6]) {
     if (fabs(z) < 1.0) {
-        // c_k(z) = sum_j (-z)^j / (k + 2j)!
-        double t4 = 1.0 / 24.0, s4 = t4, t5 = 1.0 / 120.0, s5 = t5;
-        for (int j = 1; j < 12; ++j) {
-            t4 = t4 * (-z) / ((double)(2 * j + 3) * (double)(2 * j + 4));
-            t5 = t5 * (-z) / ((double)(2 * j + 4) * (double)(2 * j + 5));
-            s4 += t4;
-            s5 += t5;
+        // c_k(z) = sum_j (-z)^j / (k + 2j)!, j = 0..11 (the next term is below
+        // 1e-28 of the first), by Horner's rule on the coefficients 1/(k+2j)!
+        const double C4[12] = {4.1666666666666664e-02, 1.388888888888889e-03,  2.48015873015873e-05,
+                               2.755731922398589e-07,  2.08767569878681e-09,   1.1470745597729725e-11,
+                               4.779477332387385e-14,  1.5619206968586225e-16, 4.110317623312165e-19,
+                               8.896791392450574e-22,  1.6117375710961184e-24, 2.4795962632247976e-27};
+        const double C5[12] = {8.333333333333333e-03,  1.984126984126984e-04,  2.7557319223985893e-06,
+                               2.505210838544172e-08,  1.6059043836821613e-10, 7.647163731819816e-13,
+                               2.8114572543455206e-15, 8.22063524662433e-18,   1.9572941063391263e-20,
+                               3.868170170630684e-23,  6.446950284384474e-26,  9.183689863795546e-29};
+        const double w = -z;
+        double s4 = C4[11], s5 = C5[11];
+#pragma unroll
+        for (int j = 10; j >= 0; --j) {
+            s4 = fma(s4, w, C4[j]);
+            s5 = fma(s5, w, C5[j]);
         }
         c[4] = s4;
         c[5] = s5;
