@@ -1,6 +1,7 @@
 // Bulirsch-Stoer kernels (mdt_bs1, mdt_bs2): every statement keeps the
 // Fortran's evaluation order so that each level's extrapolated state rounds
 // as the CPU's does.
+#include <algorithm>
 #include "allforce.cuh"
 #include "bs.cuh"
 
@@ -126,9 +127,11 @@ struct BsScratch {
     }
 };
 
-// One force call of the massive set into S.A (or A0) and table row T.
+// One force call of the massive set into S.A (or A0) and table row T; mb
+// and ngf are the set's masses and non-gravitational constants, head a
+// shared copy of the row's head for the set's own forces.
 __device__ void massive_call(const BsArgs& A, const double* X, const double* V, double* out, double* T,
-                             DeviceStatus* st) {
+                             DeviceStatus* st, const double* mb, const double* ngf, double* head) {
     const ForceCfg& f = A.f;
     const int N = f.nsplit;
     __syncthreads();
@@ -136,7 +139,7 @@ __device__ void massive_call(const BsArgs& A, const double* X, const double* V, 
         for (int k = 1 + threadIdx.x; k < N; k += blockDim.x) {
             if (k < f.nbig) {
                 double* row = T + FT_HEAD + 4 * (k - 1);
-                row[0] = X[k]; row[1] = X[N + k]; row[2] = X[2 * N + k]; row[3] = A.mbig[k];
+                row[0] = X[k]; row[1] = X[N + k]; row[2] = X[2 * N + k]; row[3] = mb[k];
             }
             const double3 a = hkce_force(A, k, X);
             out[k] = a.x; out[N + k] = a.y; out[2 * N + k] = a.z;
@@ -144,26 +147,52 @@ __device__ void massive_call(const BsArgs& A, const double* X, const double* V, 
         __syncthreads();
         return;
     }
-    if (threadIdx.x == 0) row_head(X, A.mbig, f, T);
+    if (threadIdx.x == 0) {
+        row_head(X, mb, f, T);
+        for (int q = 0; q < FT_HEAD; ++q) head[q] = T[q];
+    }
     __syncthreads();
     for (int k = threadIdx.x; k < N; k += blockDim.x) {
         if (k >= 1 && k < f.nbig) {
             double* row = T + FT_HEAD + 4 * (k - 1);
-            row[0] = X[k]; row[1] = X[N + k]; row[2] = X[2 * N + k]; row[3] = A.mbig[k];
+            row[0] = X[k]; row[1] = X[N + k]; row[2] = X[2 * N + k]; row[3] = mb[k];
         }
         if (k < 1) continue;
-        const double3 a = massive_allforce(k, X, V, A.mbig, A.ngfbig, T, f, st);
+        const double3 a = massive_allforce(k, X, V, mb, ngf, head, f, st);
         out[k] = a.x; out[N + k] = a.y; out[2 * N + k] = a.z;
     }
     __syncthreads();
 }
 
-template <int VARIANT> __global__ void __launch_bounds__(256) bs_massive_kernel(BsArgs A) {
+// The massive set through every level: one CTA. With STAGED the scratch
+// (states, accelerations, the extrapolation table), the starting state, the
+// masses and the non-gravitational constants live in shared memory.
+template <int VARIANT, bool STAGED> __global__ void __launch_bounds__(256) bs_massive_kernel(BsArgs A) {
+    extern __shared__ double sm[];
     const int N = A.f.nsplit, tid = threadIdx.x, nt = blockDim.x;
     const int L = bs_levels(VARIANT), stride = force_row(A.f.nbig - 1);
-    BsScratch S(A.bscr, N);
-    const double* X0 = A.bx;
-    const double* V0 = A.bx + 3 * N;
+    BsScratch S(STAGED ? sm : A.bscr, N);
+    const double *X0, *V0, *mb, *ngf;
+    if (STAGED) {
+        double* p = sm + (size_t)bs_massive_scratch(VARIANT) * N;
+        for (int q = tid; q < 6 * N; q += nt) p[q] = A.bx[q];
+        for (int q = tid; q < N; q += nt) p[6 * N + q] = A.mbig[q];
+        for (int q = tid; q < 5 * N; q += nt) p[7 * N + q] = A.ngfbig[q];
+        X0 = p;
+        V0 = p + 3 * N;
+        mb = p + 6 * N;
+        ngf = p + 7 * N;
+        __syncthreads();
+    } else {
+        X0 = A.bx;
+        V0 = A.bx + 3 * N;
+        mb = A.mbig;
+        ngf = A.ngfbig;
+    }
+    __shared__ double head[FT_HEAD];
+    auto call = [&](const double* X, const double* V, double* out, double* T, DeviceStatus* st) {
+        massive_call(A, X, V, out, T, st, mb, ngf, head);
+    };
     __shared__ double wmax[8];
     __shared__ int wbad[8];
     for (int k = tid; k < N; k += nt) {
@@ -177,7 +206,7 @@ template <int VARIANT> __global__ void __launch_bounds__(256) bs_massive_kernel(
         S.VS[k] = 1.0 / fmax(tmp2, 1e-300);
     }
     int row = 0;
-    massive_call(A, X0, V0, S.A0, A.table, &A.lvst[0]);
+    call(X0, V0, S.A0, A.table, &A.lvst[0]);
     ++row;
     for (int n = 1; n <= L; ++n) {
         DeviceStatus* st = &A.lvst[n];
@@ -191,7 +220,7 @@ template <int VARIANT> __global__ void __launch_bounds__(256) bs_massive_kernel(
                     S.X[z] = X0[z] + h * V0[z];
                     S.V[z] = V0[z] + h * S.A0[z];
                 }
-            massive_call(A, S.X, S.V, S.A, A.table + (size_t)(row++) * stride, st);
+            call(S.X, S.V, S.A, A.table + (size_t)(row++) * stride, st);
             for (int k = 1 + tid; k < N; k += nt)
                 for (int c = 0; c < 3; ++c) {
                     const int z = c * N + k;
@@ -199,14 +228,14 @@ template <int VARIANT> __global__ void __launch_bounds__(256) bs_massive_kernel(
                     S.VE[z] = V0[z] + hx2 * S.A[z];
                 }
             for (int j = 2; j <= n; ++j) {
-                massive_call(A, S.XE, S.VE, S.A, A.table + (size_t)(row++) * stride, st);
+                call(S.XE, S.VE, S.A, A.table + (size_t)(row++) * stride, st);
                 for (int k = 1 + tid; k < N; k += nt)
                     for (int c = 0; c < 3; ++c) {
                         const int z = c * N + k;
                         S.X[z] = S.X[z] + hx2 * S.VE[z];
                         S.V[z] = S.V[z] + hx2 * S.A[z];
                     }
-                massive_call(A, S.X, S.V, S.A, A.table + (size_t)(row++) * stride, st);
+                call(S.X, S.V, S.A, A.table + (size_t)(row++) * stride, st);
                 for (int k = 1 + tid; k < N; k += nt)
                     for (int c = 0; c < 3; ++c) {
                         const int z = c * N + k;
@@ -214,7 +243,7 @@ template <int VARIANT> __global__ void __launch_bounds__(256) bs_massive_kernel(
                         S.VE[z] = S.VE[z] + hx2 * S.A[z];
                     }
             }
-            massive_call(A, S.XE, S.VE, S.A, A.table + (size_t)(row++) * stride, st);
+            call(S.XE, S.VE, S.A, A.table + (size_t)(row++) * stride, st);
             double* Dn = S.D + (size_t)(n - 1) * 6 * N;
             for (int k = 1 + tid; k < N; k += nt)
                 for (int c = 0; c < 3; ++c) {
@@ -232,7 +261,7 @@ template <int VARIANT> __global__ void __launch_bounds__(256) bs_massive_kernel(
                     S.XE[z] = h2by2 * S.A0[z] + h * V0[z] + X0[z];
                 }
             for (int j = 2; j <= n; ++j) {
-                massive_call(A, S.XE, V0, S.A, A.table + (size_t)(row++) * stride, st);
+                call(S.XE, V0, S.A, A.table + (size_t)(row++) * stride, st);
                 const double tmp0 = h * double(j);
                 for (int k = 1 + tid; k < N; k += nt)
                     for (int c = 0; c < 3; ++c) {
@@ -242,7 +271,7 @@ template <int VARIANT> __global__ void __launch_bounds__(256) bs_massive_kernel(
                         S.XE[z] = h2n * S.C[z] + h2by2 * S.A0[z] + tmp0 * V0[z] + X0[z];
                     }
             }
-            massive_call(A, S.XE, V0, S.A, A.table + (size_t)(row++) * stride, st);
+            call(S.XE, V0, S.A, A.table + (size_t)(row++) * stride, st);
             double* Dn = S.D + (size_t)(n - 1) * 6 * N;
             for (int k = 1 + tid; k < N; k += nt)
                 for (int c = 0; c < 3; ++c) {
@@ -442,7 +471,17 @@ __global__ void __launch_bounds__(128) bs_commit_kernel(BsCommitArgs A) {
 }
 
 template <int VARIANT> void launch_variant(const BsArgs& a, cudaStream_t s) {
-    bs_massive_kernel<VARIANT><<<1, 256, 0, s>>>(a);
+    const int N = a.f.nsplit;
+    const size_t msmem = sizeof(double) * ((size_t)bs_massive_scratch(VARIANT) + 12) * N;
+    if (msmem <= 200 * 1024) {
+        if (msmem > 48 * 1024)
+            cudaFuncSetAttribute(bs_massive_kernel<VARIANT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)msmem);
+        const int threads = std::min(256, std::max(32, (N + 31) / 32 * 32));
+        bs_massive_kernel<VARIANT, true><<<1, threads, msmem, s>>>(a);
+    } else {
+        bs_massive_kernel<VARIANT, false><<<1, 256, 0, s>>>(a);
+    }
     if (a.np <= 0) return;
     const int threads = 128;
     const size_t smem = sizeof(double) * 6 * bs_levels(VARIANT) * threads;

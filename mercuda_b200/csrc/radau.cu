@@ -9,6 +9,7 @@
 // kernel then runs the whole sequence (7 Gauss-Radau nodes x 2 or 6
 // iterations) per particle in registers and reduces max |b7| for the global
 // step controller; a commit pass applies the accepted sequence.
+#include <algorithm>
 #include <cstring>
 
 #include "allforce.cuh"
@@ -209,18 +210,62 @@ __device__ __forceinline__ void atomic_max_abs(unsigned long long* dst, double v
 }
 
 // The massive set's sequence: one CTA. Writes table rows 0 (sequence start)
-// and 1 + (n-1)*7 + (j-2) (iteration n, node j) for the particles.
-__global__ void __launch_bounds__(256) ra15_massive_kernel(Ra15Args A) {
+// and 1 + (n-1)*7 + (j-2) (iteration n, node j) for the particles. With
+// STAGED the set's positions, velocities, B, G, accelerations, masses and
+// non-gravitational constants live in shared memory for the whole sequence
+// (the set is small and every node reads all of it after a barrier); B, G
+// and a1 go back to global memory at the end. The arithmetic is the same.
+template <bool STAGED> __global__ void __launch_bounds__(256) ra15_massive_kernel(Ra15Args A) {
+    extern __shared__ double sm[];
     const ForceCfg& f = A.f;
     const int N = f.nsplit, nb = f.nbig - 1, tid = threadIdx.x, nt = blockDim.x;
     const int stride = force_row(nb);
     const bool vpred = (f.ngflag != 0 || f.pn == 1);
-    double* X = A.bpx;
-    double* V = A.bpx + 3 * N;
-    const double* x1 = A.bx;
-    const double* v1 = A.bx + 3 * N;
-    double* a1 = A.bx_a1;
     __shared__ double blockmax[8];
+    __shared__ double head[FT_HEAD];
+    double *X, *V, *B, *G, *a1;
+    const double *x1, *v1, *mb, *ngf;
+    if (STAGED) {
+        X = sm;
+        V = X + 3 * N;
+        B = V + 3 * N;
+        G = B + 21 * N;
+        a1 = G + 21 * N;
+        double* sx1 = a1 + 3 * N;
+        double* sv1 = sx1 + 3 * N;
+        double* smb = sv1 + 3 * N;
+        double* sngf = smb + N;
+        for (int q = tid; q < 3 * N; q += nt) {
+            sx1[q] = A.bx[q];
+            sv1[q] = A.bx[3 * N + q];
+        }
+        for (int q = tid; q < 21 * N; q += nt) B[q] = A.reset ? 0.0 : A.bb[q];
+        for (int q = tid; q < N; q += nt) smb[q] = A.mbig[q];
+        for (int q = tid; q < 5 * N; q += nt) sngf[q] = A.ngfbig[q];
+        x1 = sx1;
+        v1 = sv1;
+        mb = smb;
+        ngf = sngf;
+        __syncthreads();
+    } else {
+        X = A.bpx;
+        V = A.bpx + 3 * N;
+        B = A.bb;
+        G = A.bg;
+        a1 = A.bx_a1;
+        x1 = A.bx;
+        v1 = A.bx + 3 * N;
+        mb = A.mbig;
+        ngf = A.ngfbig;
+    }
+    // the head of a table row: written to the table for the particles and
+    // kept in shared memory for the massive set's forces
+    auto write_head = [&](double* T) {
+        if (tid == 0) {
+            row_head(X, mb, f, T);
+            for (int q = 0; q < FT_HEAD; ++q) head[q] = T[q];
+        }
+    };
     double localmax = 0.0;
     // sequence start: force at (x1, v1), G from B
     for (int k = tid; k < N; k += nt)
@@ -229,23 +274,23 @@ __global__ void __launch_bounds__(256) ra15_massive_kernel(Ra15Args A) {
             V[c * N + k] = v1[c * N + k];
         }
     __syncthreads();
-    if (tid == 0) row_head(X, A.mbig, f, A.table);
+    write_head(A.table);
     __syncthreads();
     for (int k = tid; k < N; k += nt) {
         if (k >= 1 && k < f.nbig) {
             double* row = A.table + FT_HEAD + 4 * (k - 1);
-            row[0] = X[k]; row[1] = X[N + k]; row[2] = X[2 * N + k]; row[3] = A.mbig[k];
+            row[0] = X[k]; row[1] = X[N + k]; row[2] = X[2 * N + k]; row[3] = mb[k];
         }
         if (k < 1) continue;
-        const double3 a = massive_allforce(k, X, V, A.mbig, A.ngfbig, A.table, f, A.status);
+        const double3 a = massive_allforce(k, X, V, mb, ngf, head, f, A.status);
         a1[k] = a.x; a1[N + k] = a.y; a1[2 * N + k] = a.z;
         for (int c = 0; c < 3; ++c) {
             double b[7], g[7];
-            for (int m = 0; m < 7; ++m) b[m] = A.reset ? 0.0 : A.bb[(c * 7 + m) * N + k];
+            for (int m = 0; m < 7; ++m) b[m] = (A.reset && !STAGED) ? 0.0 : B[(c * 7 + m) * N + k];
             g_from_b(b, g);
             for (int m = 0; m < 7; ++m) {
-                A.bb[(c * 7 + m) * N + k] = b[m];
-                A.bg[(c * 7 + m) * N + k] = g[m];
+                B[(c * 7 + m) * N + k] = b[m];
+                G[(c * 7 + m) * N + k] = g[m];
             }
         }
     }
@@ -258,42 +303,52 @@ __global__ void __launch_bounds__(256) ra15_massive_kernel(Ra15Args A) {
                 if (k < 1) continue;
                 for (int c = 0; c < 3; ++c) {
                     double b[7];
-                    for (int m = 0; m < 7; ++m) b[m] = A.bb[(c * 7 + m) * N + k];
+                    for (int m = 0; m < 7; ++m) b[m] = B[(c * 7 + m) * N + k];
                     X[c * N + k] = pred_x(P, b, a1[c * N + k], v1[c * N + k], x1[c * N + k]);
                     if (vpred) V[c * N + k] = pred_v(P, b, a1[c * N + k], v1[c * N + k]);
                 }
             }
             __syncthreads();
-            if (tid == 0) row_head(X, A.mbig, f, T);
+            write_head(T);
             __syncthreads();
             for (int k = tid; k < N; k += nt) {
                 if (k >= 1 && k < f.nbig) {
                     double* row = T + FT_HEAD + 4 * (k - 1);
-                    row[0] = X[k]; row[1] = X[N + k]; row[2] = X[2 * N + k]; row[3] = A.mbig[k];
+                    row[0] = X[k]; row[1] = X[N + k]; row[2] = X[2 * N + k]; row[3] = mb[k];
                 }
                 if (k < 1) continue;
-                const double3 a = massive_allforce(k, X, vpred ? V : v1, A.mbig, A.ngfbig, T, f, A.status);
+                const double3 a = massive_allforce(k, X, vpred ? V : v1, mb, ngf, head, f, A.status);
                 const double ac[3] = {a.x, a.y, a.z};
                 for (int c = 0; c < 3; ++c) {
                     double b[7], g[7];
                     for (int m = 0; m < 7; ++m) {
-                        b[m] = A.bb[(c * 7 + m) * N + k];
-                        g[m] = A.bg[(c * 7 + m) * N + k];
+                        b[m] = B[(c * 7 + m) * N + k];
+                        g[m] = G[(c * 7 + m) * N + k];
                     }
                     update_gb(j, ac[c], a1[c * N + k], g, b);
                     for (int m = 0; m < 7; ++m) {
-                        A.bb[(c * 7 + m) * N + k] = b[m];
-                        A.bg[(c * 7 + m) * N + k] = g[m];
+                        B[(c * 7 + m) * N + k] = b[m];
+                        G[(c * 7 + m) * N + k] = g[m];
                     }
                 }
             }
             __syncthreads();
         }
     }
+    if (STAGED) {
+        // every body but the central one (whose entries the sequence leaves alone)
+        for (int q = tid; q < 21 * N; q += nt)
+            if (q % N != 0) {
+                A.bb[q] = B[q];
+                A.bg[q] = G[q];
+            }
+        for (int q = tid; q < 3 * N; q += nt)
+            if (q % N != 0) A.bx_a1[q] = a1[q];
+    }
     for (int k = tid; k < N; k += nt) {
         if (k < 1) continue;
         for (int c = 0; c < 3; ++c) {
-            const double b7 = A.bb[(c * 7 + 6) * N + k];
+            const double b7 = B[(c * 7 + 6) * N + k];
             if (!isfinite(b7)) raise_fault(A.status, FAULT_NONFINITE);
             else localmax = fmax(localmax, fabs(b7));
         }
@@ -581,7 +636,17 @@ int nblocks(int n, int t) { return (n + t - 1) / t; }
 
 void launch_ra15_sequence(const Ra15Args& a, cudaStream_t s) {
     ensure_constants();
-    ra15_massive_kernel<<<1, 256, 0, s>>>(a);
+    const int N = a.f.nsplit;
+    const size_t smem = sizeof(double) * (size_t)63 * N;  // x, v, B, G, a1, x1, v1 (57 N), m, ngf
+    if (smem <= 200 * 1024) {
+        if (smem > 48 * 1024)
+            cudaFuncSetAttribute(ra15_massive_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        // one warp per 32 bodies, at most 8
+        const int threads = std::min(256, std::max(32, (N + 31) / 32 * 32));
+        ra15_massive_kernel<true><<<1, threads, smem, s>>>(a);
+    } else {
+        ra15_massive_kernel<false><<<1, 256, 0, s>>>(a);
+    }
     if (a.np > 0) ra15_particle_kernel<<<nblocks(a.np, 128), 128, 0, s>>>(a);
 }
 
