@@ -89,6 +89,8 @@ def lib() -> C.CDLL:
         L.oracle_mfo_hy.argtypes = [I, I, PD, PD, PD, PD, PD]
         L.oracle_mvs_jacobian.argtypes = [I, I, PD, PD, PD, PD, I, PD, D, I, PD]
         L.oracle_mvs_jacobian.restype = I
+        L.oracle_hy_jacobian.argtypes = [I, I, PD, PD, PD, PD, I, PD, D, I, D, PD]
+        L.oracle_hy_jacobian.restype = I
         L.oracle_mxx_en.argtypes = [I, PD, PD, PD, C.c_void_p, PD, PD]
         L.oracle_mxx_en.restype = None
         _lib = L
@@ -302,6 +304,21 @@ def mvs_jacobian(sys, h, nsteps):
                                    int(nsteps), _p(jac))
     if rc:
         raise RuntimeError("oracle Jacobian run failed")
+    return jac
+
+
+def hy_jacobian(sys, h, nsteps, tol=1e-12):
+    """nsteps of mdt_hy on sys's democratic-heliocentric state (in place, no
+    oblateness) with forward-mode derivatives of every test particle's final
+    (x, v) with respect to its initial (x, v) and its Yarkovsky coefficient,
+    through the encounter subsystem's BS2 substeps where it is a member: J of
+    shape (n - nbig, 6, 7). Uses sys.rcrit."""
+    s = sys
+    jac = np.zeros((s.n - s.nbig, 6, 7))
+    rc = lib().oracle_hy_jacobian(s.n, s.nbig, _p(s.m), _p(s.x), _p(s.v), _p(s.ngf), s.ngflag, _p(s.rcrit), h,
+                                  int(nsteps), tol, _p(jac))
+    if rc:
+        raise RuntimeError("oracle HYBRID Jacobian run failed")
     return jac
 
 

@@ -336,7 +336,7 @@ OracleRun* oracle_hy_run(int n, int nbig, const double* m, double* x, double* v,
                          double time0, double h, int nsteps, double tol, double rcen, int central,
                          long long* counters) {
     OracleRun* run = new OracleRun();
-    oracle::HyState st;
+    oracle::HyState<double> st;
     std::vector<double> xh0(3 * n), vh0(3 * n), vh1(3 * n);
     long long forces = 0, pairs = 0;
     double time = time0;
@@ -439,6 +439,63 @@ int oracle_mvs_jacobian(int n, int nbig, const double* m, double* x, double* v, 
                                 dngf.data(), ngflag, st, events))
             return 1;
         time = time + hh;
+    }
+    for (int j = 0; j < n; ++j)
+        for (int c = 0; c < 3; ++c) {
+            x[3 * j + c] = dx[3 * j + c].v;
+            v[3 * j + c] = dv[3 * j + c].v;
+        }
+    for (int j = nbig; j < n; ++j) {
+        double* J = jac + 42 * (size_t)(j - nbig);
+        for (int c = 0; c < 3; ++c)
+            for (int k = 0; k < 7; ++k) {
+                J[7 * c + k] = dx[3 * j + c].d[k];
+                J[7 * (3 + c) + k] = dv[3 * j + c].d[k];
+            }
+    }
+    return 0;
+}
+
+// nsteps of mdt_hy (democratic-heliocentric x, v in place) with the
+// derivatives of every massless particle's final state with respect to its own
+// initial position, velocity and Yarkovsky coefficient ngf(5,j), by
+// forward-mode dual numbers through the same statements: the kicks with the
+// changeover force, the solar drifts, the Kepler drift and, for the steps in
+// which a particle is an encounter member, mdt_hkce's BS2 integration with the
+// substep sequence its step control chooses (decisions read the values).
+// jac as for oracle_mvs_jacobian (6x7 per particle, row-major). Returns
+// nonzero on a failure or a massive Small body.
+int oracle_hy_jacobian(int n, int nbig, const double* m, double* x, double* v, const double* ngf, int ngflag,
+                       const double* rcrit, double h, int nsteps, double tol, double* jac) {
+    using DD = oracle::Dual<7>;
+    for (int j = nbig; j < n; ++j)
+        if (m[j] != 0.0) return 1;
+    std::vector<DD> dm(n), dx(3 * (size_t)n), dv(3 * (size_t)n), dngf(5 * (size_t)n);
+    for (int j = 0; j < n; ++j) {
+        dm[j] = DD(m[j]);
+        for (int c = 0; c < 3; ++c) {
+            dx[3 * j + c] = DD(x[3 * j + c]);
+            dv[3 * j + c] = DD(v[3 * j + c]);
+            if (j >= nbig) {
+                dx[3 * j + c].d[c] = 1.0;
+                dv[3 * j + c].d[3 + c] = 1.0;
+            }
+        }
+        for (int c = 0; c < 5; ++c) dngf[5 * j + c] = DD(ngf[5 * j + c]);
+        if (j >= nbig) dngf[5 * j + 4].d[6] = 1.0;
+    }
+    const double jcen[3] = {0.0, 0.0, 0.0};
+    std::vector<double> zeros(n, 0.0);
+    oracle::HyState<DD> st;
+    std::vector<Event> events;
+    double time = 0.0;
+    for (int s = 0; s < nsteps; ++s) {
+        events.clear();
+        int nce = 0;
+        if (oracle::mdt_hy<DD>(time, h, tol, jcen, n, nbig, dm.data(), dx.data(), dv.data(), dngf.data(), ngflag,
+                               zeros.data(), rcrit, zeros.data(), st, events, &nce, nullptr))
+            return 1;
+        time = time + h;
     }
     for (int j = 0; j < n; ++j)
         for (int c = 0; c < 3; ++c) {

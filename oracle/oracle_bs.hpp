@@ -15,11 +15,13 @@ constexpr double BS_SHRINK = 0.55, BS_GROW = 1.3;
 // The error test shared by both routines (mercury6_2.for:3369-3380,
 // 3557-3568): max over bodies of the squared last extrapolation term scaled by
 // 1/R^2 and 1/V^2. Returns false when a term is not finite (the Fortran fails).
-inline bool bs_error(int nbod, const std::vector<double>& d1, const std::vector<double>& xscal,
-                     const std::vector<double>& vscal, double& errmax) {
+template <class R>
+bool bs_error(int nbod, const std::vector<R>& d1, const std::vector<double>& xscal, const std::vector<double>& vscal,
+              double& errmax) {
     errmax = 0.0;
     for (int k = 1; k < nbod; ++k) {
-        const double* q = d1.data() + 6 * (size_t)k;
+        double q[6];
+        for (int c = 0; c < 6; ++c) q[c] = val(d1[6 * (size_t)k + c]);
         for (int c = 0; c < 6; ++c)
             if (!std::isfinite(q[c])) return false;
         const double tmp1 = std::max(std::max(q[0] * q[0], q[1] * q[1]), q[2] * q[2]);
@@ -31,7 +33,7 @@ inline bool bs_error(int nbod, const std::vector<double>& d1, const std::vector<
 
 // Neville update of the extrapolation table after level n (1-based), the
 // loop both routines share (mercury6_2.for:3352-3366, 3540-3554).
-inline void bs_extrapolate(int nbod, int n, const double* h2, std::vector<std::vector<double>>& d) {
+template <class R> void bs_extrapolate(int nbod, int n, const double* h2, std::vector<std::vector<R>>& d) {
     for (int j = n - 1; j >= 1; --j) {
         const int j1 = j + 1;
         const double tmp0 = 1.0 / (h2[j] - h2[n]);
@@ -39,11 +41,11 @@ inline void bs_extrapolate(int nbod, int n, const double* h2, std::vector<std::v
         const double tmp2 = tmp0 * h2[n];
         for (int k = 1; k < nbod; ++k)
             for (int c = 0; c < 6; ++c)
-                d[j][6 * k + c] = tmp1 * d[j1][6 * k + c] - tmp2 * d[j][6 * k + c];
+                d[j][6 * k + c] = R(tmp1) * d[j1][6 * k + c] - R(tmp2) * d[j][6 * k + c];
     }
 }
 
-inline void bs_accept(int nbod, int n, const std::vector<std::vector<double>>& d, double* x0, double* v0) {
+template <class R> void bs_accept(int nbod, int n, const std::vector<std::vector<R>>& d, R* x0, R* v0) {
     for (int k = 1; k < nbod; ++k)
         for (int c = 0; c < 3; ++c) {
             x0[3 * k + c] = d[1][6 * k + c];
@@ -57,11 +59,11 @@ inline void bs_accept(int nbod, int n, const std::vector<std::vector<double>>& d
             }
 }
 
-inline void bs_scales(int nbod, const double* x0, const double* v0, std::vector<double>& xscal,
-                      std::vector<double>& vscal) {
+template <class R>
+void bs_scales(int nbod, const R* x0, const R* v0, std::vector<double>& xscal, std::vector<double>& vscal) {
     for (int k = 1; k < nbod; ++k) {
-        const double* p = x0 + 3 * k;
-        const double* u = v0 + 3 * k;
+        const double p[3] = {val(x0[3 * k]), val(x0[3 * k + 1]), val(x0[3 * k + 2])};
+        const double u[3] = {val(v0[3 * k]), val(v0[3 * k + 1]), val(v0[3 * k + 2])};
         const double tmp1 = p[0] * p[0] + p[1] * p[1] + p[2] * p[2];
         const double tmp2 = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
         xscal[k] = 1.0 / std::max(tmp1, 1e-300);
@@ -140,14 +142,17 @@ inline int mdt_bs1(double time, double& h0, double& hdid, double tol, const doub
 
 // mdt_bs2, mercury6_2.for:3428-3596, with any force routine
 // force(x, v, a) -> nonzero on fail(); the force is evaluated with the
-// start-of-step velocities v0 (conservative systems).
-template <class Force>
-int mdt_bs2_with(Force&& force, double time, double& h0, double& hdid, double tol, int nbod, double* x0, double* v0,
+// start-of-step velocities v0 (conservative systems). The state may be any
+// scalar type R (dual numbers propagate tangents); the step control reads the
+// values only.
+template <class R, class Force>
+int mdt_bs2_with(Force&& force, double time, double& h0, double& hdid, double tol, int nbod, R* x0, R* v0,
                  long long* rejected) {
     const double tol2 = tol * tol;
     const size_t nv = 3 * (size_t)nbod;
-    std::vector<double> xscal(nbod), vscal(nbod), xend(nv), a(nv), a0(nv), b(nv), c(nv);
-    std::vector<std::vector<double>> d(13, std::vector<double>(6 * (size_t)nbod));
+    std::vector<double> xscal(nbod), vscal(nbod);
+    std::vector<R> xend(nv), a(nv), a0(nv), b(nv), c(nv);
+    std::vector<std::vector<R>> d(13, std::vector<R>(6 * (size_t)nbod));
     double h2[13];
     bs_scales(nbod, x0, v0, xscal, vscal);
     if (force(x0, v0, a0.data())) return 1;
@@ -159,9 +164,9 @@ int mdt_bs2_with(Force&& force, double time, double& h0, double& hdid, double to
             h2[n] = h * h;
             const double h2by2 = 0.5 * h2[n];
             for (size_t k = 3; k < nv; ++k) {
-                b[k] = 0.5 * a0[k];
-                c[k] = 0.0;
-                xend[k] = h2by2 * a0[k] + h * v0[k] + x0[k];
+                b[k] = R(0.5) * a0[k];
+                c[k] = R(0.0);
+                xend[k] = R(h2by2) * a0[k] + R(h) * v0[k] + x0[k];
             }
             for (int j = 2; j <= n; ++j) {
                 if (force(xend.data(), v0, a.data())) return 1;
@@ -169,7 +174,7 @@ int mdt_bs2_with(Force&& force, double time, double& h0, double& hdid, double to
                 for (size_t k = 3; k < nv; ++k) {
                     b[k] = b[k] + a[k];
                     c[k] = c[k] + b[k];
-                    xend[k] = h2[n] * c[k] + h2by2 * a0[k] + tmp0 * v0[k] + x0[k];
+                    xend[k] = R(h2[n]) * c[k] + R(h2by2) * a0[k] + R(tmp0) * v0[k] + x0[k];
                 }
             }
             if (force(xend.data(), v0, a.data())) return 1;
@@ -177,7 +182,7 @@ int mdt_bs2_with(Force&& force, double time, double& h0, double& hdid, double to
                 for (int q = 0; q < 3; ++q) {
                     const size_t z = 3 * (size_t)k + q;
                     d[n][6 * k + q] = xend[z];
-                    d[n][6 * k + 3 + q] = h * b[z] + hby2 * a[z] + v0[z];
+                    d[n][6 * k + 3 + q] = R(h) * b[z] + R(hby2) * a[z] + v0[z];
                 }
             bs_extrapolate(nbod, n, h2, d);
             if (n > 3) {

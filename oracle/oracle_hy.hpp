@@ -20,32 +20,33 @@ namespace oracle {
 // mfo_drct, mercury6_2.for:4708-4765: direct terms between Big i >= i0 and
 // every j > i with the changeover K(r) = 10q^3 - 15q^4 + 6q^5 (0 inside
 // 0.1 rc, 1 outside rc).
-inline void mfo_drct(int i0, int nbod, int nbig, const double* m, const double* x, const double* rcrit, double* a) {
+template <class R>
+void mfo_drct(int i0, int nbod, int nbig, const R* m, const R* x, const double* rcrit, R* a) {
     if (i0 <= 0) i0 = 1;
     for (int i = i0; i < nbig; ++i)
         for (int j = i + 1; j < nbod; ++j) {
-            const double dx = x[3 * j] - x[3 * i];
-            const double dy = x[3 * j + 1] - x[3 * i + 1];
-            const double dz = x[3 * j + 2] - x[3 * i + 2];
-            const double s2 = dx * dx + dy * dy + dz * dz;
+            const R dx = x[3 * j] - x[3 * i];
+            const R dy = x[3 * j + 1] - x[3 * i + 1];
+            const R dz = x[3 * j + 2] - x[3 * i + 2];
+            const R s2 = dx * dx + dy * dy + dz * dz;
             const double rc = std::max(rcrit[i], rcrit[j]);
             const double rc2 = rc * rc;
-            double tmp2;
-            if (s2 >= rc2) {
-                const double s_1 = 1.0 / std::sqrt(s2);
+            R tmp2;
+            if (s2 >= R(rc2)) {
+                const R s_1 = R(1.0) / Sqrt(s2);
                 tmp2 = s_1 * s_1 * s_1;
-            } else if (s2 <= 0.01 * rc2) {
-                tmp2 = 0.0;
+            } else if (s2 <= R(0.01 * rc2)) {
+                tmp2 = R(0.0);
             } else {
-                const double s_1 = 1.0 / std::sqrt(s2);
-                const double s = 1.0 / s_1;
-                const double s_3 = s_1 * s_1 * s_1;
-                const double q = (s - 0.1 * rc) / (0.9 * rc);
-                const double q2 = q * q, q3 = q * q2, q4 = q2 * q2, q5 = q2 * q3;
-                tmp2 = (10.0 * q3 - 15.0 * q4 + 6.0 * q5) * s_3;
+                const R s_1 = R(1.0) / Sqrt(s2);
+                const R s = R(1.0) / s_1;
+                const R s_3 = s_1 * s_1 * s_1;
+                const R q = (s - R(0.1 * rc)) / R(0.9 * rc);
+                const R q2 = q * q, q3 = q * q2, q4 = q2 * q2, q5 = q2 * q3;
+                tmp2 = (R(10.0) * q3 - R(15.0) * q4 + R(6.0) * q5) * s_3;
             }
-            const double faci = tmp2 * m[i];
-            const double facj = tmp2 * m[j];
+            const R faci = tmp2 * m[i];
+            const R facj = tmp2 * m[j];
             a[3 * j] = a[3 * j] - faci * dx;
             a[3 * j + 1] = a[3 * j + 1] - faci * dy;
             a[3 * j + 2] = a[3 * j + 2] - faci * dz;
@@ -57,13 +58,13 @@ inline void mfo_drct(int i0, int nbod, int nbig, const double* m, const double* 
 
 // mfo_hy, mercury6_2.for:4781-4819: the interaction part of the hybrid
 // Hamiltonian (no indirect term in democratic heliocentric coordinates).
-inline void mfo_hy(const double* jcen, int nbod, int nbig, const double* m, const double* x, const double* rcrit,
-                   double* a) {
-    for (int k = 0; k < 3 * nbod; ++k) a[k] = 0.0;
+template <class R>
+void mfo_hy(const double* jcen, int nbod, int nbig, const R* m, const R* x, const double* rcrit, R* a) {
+    for (int k = 0; k < 3 * nbod; ++k) a[k] = R(0.0);
     mfo_drct(1, nbod, nbig, m, x, rcrit, a);
     if (jcen[0] != 0.0 || jcen[1] != 0.0 || jcen[2] != 0.0) {
-        std::vector<double> aobl(3 * (size_t)nbod);
-        double acen[3];
+        std::vector<R> aobl(3 * (size_t)nbod);
+        R acen[3];
         mfo_obl(jcen, nbod, m, x, aobl.data(), acen);
         for (int k = 1; k < nbod; ++k)
             for (int c = 0; c < 3; ++c) a[3 * k + c] = a[3 * k + c] + aobl[3 * k + c] - acen[c];
@@ -73,31 +74,31 @@ inline void mfo_hy(const double* jcen, int nbod, int nbig, const double* m, cons
 // mfo_hkce, mercury6_2.for:4836-4910: the Keplerian part during encounters:
 // the inner changeover 1 - K(r) over the listed pairs (0-based ice, jce)
 // plus the central body's attraction.
-inline void mfo_hkce(int nbod, const double* m, const double* x, const double* rcrit, double* a, int nce,
-                     const int* ice, const int* jce) {
-    for (int k = 0; k < 3 * nbod; ++k) a[k] = 0.0;
+template <class R>
+void mfo_hkce(int nbod, const R* m, const R* x, const double* rcrit, R* a, int nce, const int* ice, const int* jce) {
+    for (int k = 0; k < 3 * nbod; ++k) a[k] = R(0.0);
     for (int k = 0; k < nce; ++k) {
         const int i = ice[k], j = jce[k];
-        const double dx = x[3 * j] - x[3 * i];
-        const double dy = x[3 * j + 1] - x[3 * i + 1];
-        const double dz = x[3 * j + 2] - x[3 * i + 2];
-        const double s2 = dx * dx + dy * dy + dz * dz;
+        const R dx = x[3 * j] - x[3 * i];
+        const R dy = x[3 * j + 1] - x[3 * i + 1];
+        const R dz = x[3 * j + 2] - x[3 * i + 2];
+        const R s2 = dx * dx + dy * dy + dz * dz;
         const double rc = std::max(rcrit[i], rcrit[j]);
         const double rc2 = rc * rc;
-        if (s2 < rc2) {
-            const double s_1 = 1.0 / std::sqrt(s2);
-            const double s_3 = s_1 * s_1 * s_1;
-            double tmp2;
-            if (s2 <= 0.01 * rc2) {
+        if (s2 < R(rc2)) {
+            const R s_1 = R(1.0) / Sqrt(s2);
+            const R s_3 = s_1 * s_1 * s_1;
+            R tmp2;
+            if (s2 <= R(0.01 * rc2)) {
                 tmp2 = s_3;
             } else {
-                const double s = 1.0 / s_1;
-                const double q = (s - 0.1 * rc) / (0.9 * rc);
-                const double q2 = q * q, q3 = q * q2, q4 = q2 * q2, q5 = q2 * q3;
-                tmp2 = (1.0 - 10.0 * q3 + 15.0 * q4 - 6.0 * q5) * s_3;
+                const R s = R(1.0) / s_1;
+                const R q = (s - R(0.1 * rc)) / R(0.9 * rc);
+                const R q2 = q * q, q3 = q * q2, q4 = q2 * q2, q5 = q2 * q3;
+                tmp2 = (R(1.0) - R(10.0) * q3 + R(15.0) * q4 - R(6.0) * q5) * s_3;
             }
-            const double faci = tmp2 * m[i];
-            const double facj = tmp2 * m[j];
+            const R faci = tmp2 * m[i];
+            const R facj = tmp2 * m[j];
             a[3 * j] = a[3 * j] - faci * dx;
             a[3 * j + 1] = a[3 * j + 1] - faci * dy;
             a[3 * j + 2] = a[3 * j + 2] - faci * dz;
@@ -107,9 +108,9 @@ inline void mfo_hkce(int nbod, const double* m, const double* x, const double* r
         }
     }
     for (int i = 1; i < nbod; ++i) {
-        const double s2 = x[3 * i] * x[3 * i] + x[3 * i + 1] * x[3 * i + 1] + x[3 * i + 2] * x[3 * i + 2];
-        const double s_1 = 1.0 / std::sqrt(s2);
-        const double tmp2 = m[0] * s_1 * s_1 * s_1;
+        const R s2 = x[3 * i] * x[3 * i] + x[3 * i + 1] * x[3 * i + 1] + x[3 * i + 2] * x[3 * i + 2];
+        const R s_1 = R(1.0) / Sqrt(s2);
+        const R tmp2 = m[0] * s_1 * s_1 * s_1;
         a[3 * i] = a[3 * i] - tmp2 * x[3 * i];
         a[3 * i + 1] = a[3 * i + 1] - tmp2 * x[3 * i + 1];
         a[3 * i + 2] = a[3 * i + 2] - tmp2 * x[3 * i + 2];
@@ -189,11 +190,11 @@ inline void h2dh_velocity(int nbod, const double* m, const double* vh, double* v
 }
 
 // The solar-drift half step of mdt_hy (mercury6_2.for:3693-3711).
-inline void solar_drift(int nbod, const double* m, double* x, const double* v, double hby2) {
-    double mvsum[3] = {0.0, 0.0, 0.0};
+template <class R> void solar_drift(int nbod, const R* m, R* x, const R* v, double hby2) {
+    R mvsum[3] = {R(0.0), R(0.0), R(0.0)};
     for (int j = 1; j < nbod; ++j)
         for (int c = 0; c < 3; ++c) mvsum[c] = mvsum[c] + m[j] * v[3 * j + c];
-    const double temp = hby2 / m[0];
+    const R temp = R(hby2) / m[0];
     for (int c = 0; c < 3; ++c) mvsum[c] = temp * mvsum[c];
     for (int j = 1; j < nbod; ++j)
         for (int c = 0; c < 3; ++c) x[3 * j + c] = x[3 * j + c] + mvsum[c];
@@ -201,8 +202,8 @@ inline void solar_drift(int nbod, const double* m, double* x, const double* v, d
 
 // State mdt_hy keeps between calls: the cached interaction and
 // non-gravitational accelerations and the encounter step hrec.
-struct HyState {
-    std::vector<double> a, angf;
+template <class R> struct HyState {
+    std::vector<R> a, angf;
     double hrec = 0.0;
     int dtflag = 0;
 };
@@ -211,11 +212,11 @@ struct HyState {
 // encounter members (ce != 0) and the central body integrated together by
 // mdt_bs2 with mfo_hkce on a local clock, mce_stat after every substep.
 // Event ids are mapped back to the global (1-based) numbering. Returns
-// nonzero on a fail().
-inline int mdt_hkce(double time, double h0, double& hrec, double tol, int nbod, int nbig, const double* m,
-                    double* x, double* v, const double* rphys, const double* rcrit, const double* rce,
-                    const std::vector<int>& ce, const std::vector<int>& ice, const std::vector<int>& jce,
-                    std::vector<Event>& events, long long* forces) {
+// nonzero on a fail(). Any scalar type R: mce_stat reads the values.
+template <class R>
+int mdt_hkce(double time, double h0, double& hrec, double tol, int nbod, int nbig, const R* m, R* x, R* v,
+             const double* rphys, const double* rcrit, const double* rce, const std::vector<int>& ce,
+             const std::vector<int>& ice, const std::vector<int>& jce, std::vector<Event>& events, long long* forces) {
     std::vector<int> index(1, 0), iback(nbod, -1);
     int nbsbig = 0;
     for (int j = 1; j < nbod; ++j)
@@ -226,8 +227,8 @@ inline int mdt_hkce(double time, double h0, double& hrec, double tol, int nbod, 
         }
     const int nbs = (int)index.size();
     nbsbig = nbsbig + 1;  // count of Big bodies incl. the central body
-    std::vector<double> mbs(nbs), xbs(3 * (size_t)nbs, 0.0), vbs(3 * (size_t)nbs, 0.0), rcritbs(nbs, 0.0),
-        rcebs(nbs, 0.0), rphybs(nbs, 0.0);
+    std::vector<R> mbs(nbs), xbs(3 * (size_t)nbs, R(0.0)), vbs(3 * (size_t)nbs, R(0.0));
+    std::vector<double> rcritbs(nbs, 0.0), rcebs(nbs, 0.0), rphybs(nbs, 0.0);
     mbs[0] = m[0];
     for (int k = 1; k < nbs; ++k) {
         const int j = index[k];
@@ -246,14 +247,17 @@ inline int mdt_hkce(double time, double h0, double& hrec, double tol, int nbod, 
         ibs[k] = iback[ice[k]];
         jbs[k] = iback[jce[k]];
     }
-    auto force = [&](const double* xx, const double*, double* aa) {
+    auto force = [&](const R* xx, const R*, R* aa) {
         if (forces) ++*forces;
         mfo_hkce(nbs, mbs.data(), xx, rcritbs.data(), aa, nce, ibs.data(), jbs.data());
         return 0;
     };
     double tlocal = 0.0;
     double hlocal = std::copysign(hrec, h0);
-    std::vector<double> x0(3 * (size_t)nbs), v0(3 * (size_t)nbs);
+    std::vector<R> x0(3 * (size_t)nbs), v0(3 * (size_t)nbs);
+    std::vector<double> mv(nbs), x0v(3 * (size_t)nbs), v0v(3 * (size_t)nbs), x1v(3 * (size_t)nbs),
+        v1v(3 * (size_t)nbs);
+    for (int k = 0; k < nbs; ++k) mv[k] = val(mbs[k]);
     std::vector<Event> stat;
     do {
         const double tmp0 = std::fabs(h0) - std::fabs(tlocal);
@@ -265,8 +269,14 @@ inline int mdt_hkce(double time, double h0, double& hrec, double tol, int nbod, 
         if (mdt_bs2_with(force, tlocal, hlocal, hdid, tol, nbs, xbs.data(), vbs.data(), nullptr)) return 1;
         tlocal = tlocal + hdid;
         const double temp = time + tlocal;
+        for (size_t k = 0; k < 3 * (size_t)nbs; ++k) {
+            x0v[k] = val(x0[k]);
+            v0v[k] = val(v0[k]);
+            x1v[k] = val(xbs[k]);
+            v1v[k] = val(vbs[k]);
+        }
         stat.clear();
-        mce_stat<double>(temp, hdid, nbs, nbsbig, mbs.data(), x0.data(), v0.data(), xbs.data(), vbs.data(),
+        mce_stat<double>(temp, hdid, nbs, nbsbig, mv.data(), x0v.data(), v0v.data(), x1v.data(), v1v.data(),
                          rcebs.data(), rphybs.data(), stat);
         for (Event e : stat) {
             e.i = index[e.i - 1] + 1;
@@ -286,38 +296,46 @@ inline int mdt_hkce(double time, double h0, double& hrec, double tol, int nbod, 
 
 // mdt_hy, mercury6_2.for:3618-3782 (the CPU branch): democratic-heliocentric
 // x, v in place; events receive the encounter records of mdt_hkce; *nce the
-// number of encounter pairs of the step.
-inline int mdt_hy(double time, double h0, double tol, const double* jcen, int nbod, int nbig, const double* m,
-                  double* x, double* v, const double* ngf, int ngflag, const double* rphys, const double* rcrit,
-                  const double* rce, HyState& st, std::vector<Event>& events, int* nce_out, long long* forces) {
+// number of encounter pairs of the step. Any scalar type R: mce_snif and the
+// step control of the encounter subsystem read the values.
+template <class R>
+int mdt_hy(double time, double h0, double tol, const double* jcen, int nbod, int nbig, const R* m, R* x, R* v,
+           const R* ngf, int ngflag, const double* rphys, const double* rcrit, const double* rce, HyState<R>& st,
+           std::vector<Event>& events, int* nce_out, long long* forces) {
     const double hby2 = h0 * 0.5;
     const size_t nv = 3 * (size_t)nbod;
     if (st.a.size() < nv) {
-        st.a.assign(nv, 0.0);
-        st.angf.assign(nv, 0.0);
+        st.a.assign(nv, R(0.0));
+        st.angf.assign(nv, R(0.0));
     }
-    double* a = st.a.data();
-    double* angf = st.angf.data();
+    R* a = st.a.data();
+    R* angf = st.angf.data();
     if (st.dtflag != 2) {
         if (st.dtflag == 0) st.hrec = h0;
         mfo_hy(jcen, nbod, nbig, m, x, rcrit, a);
         if (forces) ++*forces;
         st.dtflag = 2;
-        for (size_t k = 3; k < nv; ++k) angf[k] = 0.0;
+        for (size_t k = 3; k < nv; ++k) angf[k] = R(0.0);
         if (ngflag == 1 || ngflag == 3)
             if (mfo_ngf(nbod, x, v, angf, ngf)) return 1;
     }
-    const double ausr = 0.0;
-    for (size_t k = 3; k < nv; ++k) v[k] = v[k] + hby2 * (angf[k] + ausr + a[k]);
+    const R ausr = R(0.0);
+    for (size_t k = 3; k < nv; ++k) v[k] = v[k] + R(hby2) * (angf[k] + ausr + a[k]);
     solar_drift(nbod, m, x, v, hby2);
-    std::vector<double> x0(x, x + nv), v0(v, v + nv);
+    std::vector<R> x0(x, x + nv), v0(v, v + nv);
     for (int j = 1; j < nbod; ++j) {
         int iflag = 0;
-        drift_one<double>(m[0], x[3 * j], x[3 * j + 1], x[3 * j + 2], v[3 * j], v[3 * j + 1], v[3 * j + 2], h0,
-                          iflag);
+        drift_one<R>(m[0], x[3 * j], x[3 * j + 1], x[3 * j + 2], v[3 * j], v[3 * j + 1], v[3 * j + 2], R(h0), iflag);
+    }
+    std::vector<double> x0v(nv), v0v(nv), x1v(nv), v1v(nv);
+    for (size_t k = 0; k < nv; ++k) {
+        x0v[k] = val(x0[k]);
+        v0v[k] = val(v0[k]);
+        x1v[k] = val(x[k]);
+        v1v[k] = val(v[k]);
     }
     std::vector<int> ce, ice, jce;
-    mce_snif(h0, nbod, nbig, x0.data(), v0.data(), x, v, rcrit, ce, ice, jce);
+    mce_snif(h0, nbod, nbig, x0v.data(), v0v.data(), x1v.data(), v1v.data(), rcrit, ce, ice, jce);
     *nce_out = (int)ice.size();
     if (!ice.empty()) {
         for (int j = 1; j < nbod; ++j)
@@ -334,7 +352,7 @@ inline int mdt_hy(double time, double h0, double tol, const double* jcen, int nb
     if (forces) ++*forces;
     if (ngflag == 1 || ngflag == 3)
         if (mfo_ngf(nbod, x, v, angf, ngf)) return 1;
-    for (size_t k = 3; k < nv; ++k) v[k] = v[k] + hby2 * (angf[k] + ausr + a[k]);
+    for (size_t k = 3; k < nv; ++k) v[k] = v[k] + R(hby2) * (angf[k] + ausr + a[k]);
     return 0;
 }
 
