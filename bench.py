@@ -88,7 +88,8 @@ def parse_args():
     p.add_argument("--threads", type=int, default=0)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", default="mvs", choices=["mvs", "radau", "bs", "bs2", "hybrid", "batch", "adjoint"])
+    p.add_argument("--workload", default="mvs", choices=["mvs", "radau", "bs", "bs2", "hybrid", "batch", "adjoint",
+                                                         "hybrid_adjoint"])
     p.add_argument("--checkpoint-every", type=int, default=50)
     p.add_argument("--systems", type=int, default=4096)
     args = p.parse_args()
@@ -96,6 +97,8 @@ def parse_args():
         args.particles = 100_000
     if args.workload == "adjoint" and args.particles == 1_000_000:
         args.particles = 100_000
+    if args.workload == "hybrid_adjoint" and args.particles == 1_000_000:
+        args.particles = 20_000
     return args
 
 
@@ -594,6 +597,99 @@ def run_adjoint(args, rank, world, dist):
                           "cpu_baseline": cpu}), flush=True)
 
 
+def run_hybrid_adjoint(args, rank, world, dist):
+    """Gradients through HYBRID: forward through the library's HYBRID path
+    (host-driven encounter subsystems), backward on the device."""
+    from mercuda_b200.system import mce_init
+    metric = "adjoint HYBRID particle-steps/s"
+
+    def make(seed, n, rank=0):
+        s_ = mce_init(workload(n, seed, HYBRID_NEAR, rank), H, 3.0)
+        rng = np.random.default_rng(seed + 7 if rank == 0 else (seed + 7, rank))
+        npart = s_.n - s_.nbig
+        s_.ngf[s_.nbig:, 4] = np.exp(rng.uniform(np.log(1e-15), np.log(1e-13), npart)) * rng.choice([-1, 1], npart)
+        return s_
+
+    tol = 1e-12
+    workload_text = (f"gradient of sum |x_final|^2 w.r.t. initial x, v and yar of {args.particles} particles, "
+                     f"{args.steps} HYBRID steps of 8 d about 8 planets (encounter subsystem by BS2, tol 1e-12), "
+                     f"checkpoint every {args.checkpoint_every}")
+
+    def cpu_sample(n, steps):
+        from oracle import oracle as O
+        s_ = make(args.seed, n)
+        t0 = time.perf_counter()
+        O.hy_jacobian(s_, H, steps, tol)
+        dt = time.perf_counter() - t0
+        return n * steps / dt, dt
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        n = min(args.particles, 1000)
+        value, dt = cpu_sample(n, args.steps)
+        print(json.dumps({"impl": "reference", "metric": metric, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+                          "steps": args.steps, "warmup": 0, "ms_per_step": dt * 1e3 / args.steps,
+                          "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                          "data": "synthetic", "config": {"workload": workload_text, "particles": n},
+                          "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
+                                           "sample": f"{n} particles x {args.steps} steps, forward-mode tangents "
+                                                     f"of the oracle's mdt_hy ({dt:.1f} s)"},
+                          "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
+              flush=True)
+        return
+    import torch
+    from mercuda_b200.adjoint import hybrid_timing, hybrid_trajectory
+
+    sysw = make(args.seed, args.particles, rank)
+    nb = sysw.nbig
+    dev = torch.device("cuda")
+    big = (sysw.m[:nb], sysw.x[:nb], sysw.v[:nb], sysw.rcrit[:nb])
+
+    def once():
+        x0 = torch.tensor(sysw.x[nb:], device=dev, requires_grad=True)
+        v0 = torch.tensor(sysw.v[nb:], device=dev, requires_grad=True)
+        yar = torch.tensor(sysw.ngf[nb:, 4], device=dev, requires_grad=True)
+        xf, _ = hybrid_trajectory(x0, v0, yar, big, sysw.rcrit[nb:], H, args.steps, tol, args.checkpoint_every)
+        (xf ** 2).sum().backward()
+        return x0.grad.cpu().numpy()
+
+    ranks = Ranks(dist, device="cuda")
+    for _ in range(max(1, args.warmup)):
+        once()
+    ranks.barrier()
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clocks:
+        t0 = time.perf_counter()
+        gx = once()
+        e2e_s = time.perf_counter() - t0
+    fwd, bwd, members = hybrid_timing()
+    ms = fwd + bwd
+    ms, e2e_s = ranks.max(ms), ranks.max(e2e_s)
+    value = world * args.particles * args.steps / (ms * 1e-3)
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        n_cpu = min(args.particles, 500)
+        v_cpu, dt = cpu_sample(n_cpu, args.steps)
+        cpu = {"value": v_cpu, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": f"{n_cpu} particles x {args.steps} steps, forward-mode tangents of the oracle's mdt_hy "
+                         f"({dt:.1f} s)"}
+    if rank == 0:
+        print(json.dumps({"metric": metric, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                          "warmup": max(1, args.warmup), "ms_per_step": ms / args.steps, "higher_is_better": True,
+                          "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                          "config": {"workload": workload_text, "particles_per_gpu": args.particles,
+                                     "forward_wall_ms": fwd, "backward_ms": bwd, "backward_over_forward": bwd / fwd,
+                                     "member_steps": members, "checkpoint_every": args.checkpoint_every,
+                                     "grad_finite": bool(np.all(np.isfinite(gx)))},
+                          "clocks": clocks.summary(),
+                          "e2e": {"value": world * args.particles * args.steps / e2e_s, "unit": UNIT,
+                                  "h2d_bytes_per_step": args.particles * 7 * 8 / args.steps,
+                                  "d2h_bytes_per_step": args.particles * 3 * 8 / args.steps,
+                                  "note": "wall clock around tensor creation from host arrays, the forward and "
+                                          "backward calls and the gradient copy back"},
+                          "cpu_baseline": cpu}), flush=True)
+
+
 def main():
     args = parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -617,6 +713,8 @@ def main():
             run_batch(args, rank, world, dist)
         elif args.workload == "adjoint":
             run_adjoint(args, rank, world, dist)
+        elif args.workload == "hybrid_adjoint":
+            run_hybrid_adjoint(args, rank, world, dist)
         else:
             run_adaptive(args, rank, world, dist)
         if dist:

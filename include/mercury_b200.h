@@ -41,6 +41,16 @@ int mercury_b200_dropin_time(double* ms, int64_t* launches, int reset);
  * magnitude. The reference host calls mxx_en itself after downloading every
  * body (mercury6_2.for:919-920); this reads back two numbers instead. */
 int mercury_b200_energy(double h, int physical, const double* spin, double* e, double* l2);
+/* mxx_ejec's test (mercury6_2.for:7050-7085) on the device state: *count
+ * receives the number of bodies j >= i0 (1-based; i0 <= 0 means 2, as in
+ * mxx_ejec) whose heliocentric distance exceeds rmax, and ids[0 .. cap) the
+ * first cap of their 1-based ids in ascending order. Positions are those
+ * mercury_cuda_export(h, physical, ...) would return (mal_hcon tests MVS on
+ * its map variables, mco_iden, i.e. physical = 0). The state is not changed:
+ * the host flags and removes the bodies (mxx_elim) and uploads again. The
+ * reference host downloads every body at the nfun cadence for this test
+ * (mercury6_2.for:929-948); this reads back the ids only. */
+int mercury_b200_ejections(double h, int physical, double rmax, int i0, int* ids, int cap, int* count);
 /* Launch shape of the particle kernel: threads per CTA (multiple of 32) and
  * steps fused per launch (0 = automatic); a negative value keeps the setting. */
 int mercury_b200_set_launch(int particle_threads, int steps_per_launch);
@@ -104,6 +114,45 @@ int mercury_b200_adjoint_backward(const double* gx, const double* gv, double* dx
 /* Device time of the last forward and backward calls. */
 int mercury_b200_adjoint_timing(double* forward_ms, double* backward_ms);
 void mercury_b200_adjoint_free(void);
+
+/* ---- Gradients through the HYBRID test-particle integration (no counterpart
+ * in the reference). Massless particles never act on the Big bodies; each
+ * particle's final state depends on its own initial state and Yarkovsky
+ * coefficient, through mdt_hy's changeover kicks, solar drifts and Kepler
+ * drift, and, in the steps where mce_snif makes it an encounter member,
+ * through mdt_hkce's BS2 integration of the encounter subsystem.
+ *
+ * Forward: the Big bodies (host rows: mbig[nbig] in K2 units, xbig/vbig
+ * (nbig,3) democratic-heliocentric, i.e. heliocentric positions and
+ * barycentric velocities as mercury_cuda_upload receives them for HYBRID,
+ * rcrit_big[nbig] changeover radii) and np massless particles (DEVICE arrays
+ * x0/v0 (np,3) in the same coordinates, yar[np] or NULL; HOST array
+ * rcrit[np]) advance nsteps mdt_hy steps of h with encounter tolerance tol,
+ * through the library's own HYBRID path (mercury_cuda_hybrid_begin,
+ * encounter_enter/step/download/exit, hybrid_finish: it replaces the resident
+ * system, as mercury_cuda_upload does). The final states go to the device
+ * arrays x_final/v_final. Kept for the backward call: the particle state every
+ * checkpoint_every steps, the Big-body rows of every step and, per encounter
+ * member step, the member's end state and the 6x6 Jacobian of its BS2
+ * segment (accumulated in forward mode over the accepted substeps; the step
+ * control's choices are held fixed). No oblateness and no non-gravitational
+ * term other than yar. The device inputs must stay unchanged until the
+ * backward call. For massless particles the democratic-heliocentric velocity
+ * differs from the heliocentric one by a Big-body term only, so the gradients
+ * are the same in either. */
+int mercury_b200_hybrid_adjoint_forward(int nbig, const double* mbig, const double* xbig, const double* vbig,
+                                        const double* rcrit_big, int np, const double* x0, const double* v0,
+                                        const double* yar, const double* rcrit, double h, double tol, int nsteps,
+                                        int checkpoint_every, double* x_final, double* v_final);
+/* Backward for the last HYBRID forward run: gx/gv (device (np,3); gv may be
+ * NULL) hold dL/dx_final and dL/dv_final; dx0/dv0 (device (np,3)) and dyar
+ * (device [np], may be NULL) receive dL/dx0, dL/dv0, dL/dyar. */
+int mercury_b200_hybrid_adjoint_backward(const double* gx, const double* gv, double* dx0, double* dv0, double* dyar);
+/* Wall time of the last forward call (host-driven: encounter subsystems step
+ * through the drop-in calls), device time of the last backward call, and the
+ * number of (particle, step) encounter-member pairs the forward run recorded. */
+int mercury_b200_hybrid_adjoint_timing(double* forward_ms, double* backward_ms, int64_t* member_steps);
+void mercury_b200_hybrid_adjoint_free(void);
 
 /* One MVS step (kick, drift, mce_stat pair screen, kick) of a system whose
  * arrays the caller already holds on the current device, with no device

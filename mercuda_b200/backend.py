@@ -50,7 +50,9 @@ EXTENSION_SYMBOLS = ["mercury_b200_mvs_advance", "mercury_b200_events", "mercury
                      "mercury_b200_batch_events", "mercury_b200_batch_download", "mercury_b200_batch_set",
                      "mercury_b200_batch_timing", "mercury_b200_batch_free", "mercury_b200_adjoint_forward",
                      "mercury_b200_adjoint_backward", "mercury_b200_adjoint_timing", "mercury_b200_adjoint_free",
-                     "mercury_b200_energy"]
+                     "mercury_b200_energy", "mercury_b200_hybrid_adjoint_forward",
+                     "mercury_b200_hybrid_adjoint_backward", "mercury_b200_hybrid_adjoint_timing",
+                     "mercury_b200_hybrid_adjoint_free", "mercury_b200_ejections"]
 
 
 class BackendError(RuntimeError):
@@ -93,6 +95,7 @@ def load_library(path: Path | str | None = None) -> C.CDLL:
     L.mercury_b200_fp64_peak.argtypes = [PD, PD]
     L.mercury_b200_dropin_time.argtypes = [PD, PI64, I]
     L.mercury_b200_energy.argtypes = [D, I, PD, PD, PD]
+    L.mercury_b200_ejections.argtypes = [D, I, D, I, PI, I, PI]
     L.mercury_b200_batch_upload.argtypes = [I, PI, PI, PD, PD, PD, PD, PD, PD]
     L.mercury_b200_batch_advance.argtypes = [D, I, D, PI]
     L.mercury_b200_batch_events.argtypes = [C.c_void_p, PI, PI, I]
@@ -105,6 +108,10 @@ def load_library(path: Path | str | None = None) -> C.CDLL:
     L.mercury_b200_adjoint_backward.argtypes = [VP_, VP_, VP_, VP_, VP_]
     L.mercury_b200_adjoint_timing.argtypes = [PD, PD]
     L.mercury_b200_adjoint_free.restype = None
+    L.mercury_b200_hybrid_adjoint_forward.argtypes = [I, PD, PD, PD, PD, I, VP_, VP_, VP_, PD, D, D, I, I, VP_, VP_]
+    L.mercury_b200_hybrid_adjoint_backward.argtypes = [VP_, VP_, VP_, VP_, VP_]
+    L.mercury_b200_hybrid_adjoint_timing.argtypes = [PD, PD, PI64]
+    L.mercury_b200_hybrid_adjoint_free.restype = None
     VP = C.c_void_p
     L.mercury_b200_mvs_step_noalloc.argtypes = [I, I, VP, VP, VP, VP, VP, VP, VP, VP, VP, I, D, D, I, VP, I,
                                                 PI, VP]
@@ -350,6 +357,17 @@ class Backend:
                                         C.byref(e), C.byref(l2)) != 0:
             raise BackendError("energy check failed")
         return e.value, l2.value
+
+    def ejections(self, h: float, physical: bool, rmax: float, i0: int = 2, cap: int | None = None) -> np.ndarray:
+        """mxx_ejec's test on the device: ascending 1-based ids of the bodies
+        j >= i0 beyond rmax (positions as export(h, physical) returns them)."""
+        cap = self.n if cap is None else cap
+        ids = np.zeros(max(1, cap), dtype=np.int32)
+        count = C.c_int(0)
+        if self.lib.mercury_b200_ejections(h, int(physical), rmax, i0, ids.ctypes.data_as(PI), cap,
+                                           C.byref(count)) != 0:
+            raise BackendError("ejection screen failed")
+        return ids[:min(count.value, cap)].copy()
 
     def fp64_peak(self):
         tf, ms = D(0.0), D(0.0)

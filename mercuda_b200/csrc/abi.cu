@@ -22,6 +22,7 @@ Context g_contexts[2];
 int g_active = 0;
 
 Context& ctx() { return g_contexts[g_active]; }
+int active_context() { return g_active; }
 
 int report(const std::exception& e) {
     std::fprintf(stderr, "MERCURY CUDA: %s\n", e.what());
@@ -477,6 +478,10 @@ void bs_step_once(double time, double* h, double* hdid, double tol, int64_t* rej
         k.px_out = c.pstate[out].p;
         launch_bs_commit(k, c.stream);
         c.dropin_launches += 1;
+        if (c.tangent && c.encounter && V == 2 && c.np > 0) {
+            launch_bs2_tangent(a, accepted, c.tg.p, c.stream);
+            c.dropin_launches += 1;
+        }
         check(cudaGetLastError(), "launch");
         check(cudaStreamSynchronize(c.stream), "step");
         *hdid = *h;
@@ -610,6 +615,42 @@ void export_corrected(double h, double* xx, double* vv) {
                               c.stream),
               "export");
         check(cudaStreamSynchronize(c.stream), "export");
+    }
+}
+
+// mxx_ejec's test (mercury6_2.for:7078-7080): bodies from index `first` on
+// whose r^2 = x*x + y*y + z*z (the Fortran's order) exceeds rmax2, as 1-based
+// ids; one atomic per warp (ballot, then each hit's rank among the warp's).
+// ids[0] counts, ids[1 ..] receive up to cap ids in no particular order.
+__global__ void ejection_kernel(const double* bx, int N, const double* px, int S, int np, const int* perm, int first,
+                                double rmax2, int* ids, int cap) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    bool hit = false;
+    int id = 0;
+    if (q < N + np) {
+        double x, y, z;
+        int body;
+        if (q < N) {
+            body = q;
+            x = bx[q]; y = bx[N + q]; z = bx[2 * N + q];
+        } else {
+            const int s = q - N;
+            body = N + perm[s];
+            x = px[s]; y = px[S + s]; z = px[2 * (size_t)S + s];
+        }
+        const double r2 = x * x + y * y + z * z;
+        hit = body >= first && r2 > rmax2;
+        id = body + 1;
+    }
+    const unsigned mask = __ballot_sync(0xffffffffu, hit);
+    if (!mask) return;
+    const int lane = threadIdx.x & 31, leader = __ffs(mask) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(ids, __popc(mask));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (hit) {
+        const int k = base + __popc(mask & ((1u << lane) - 1u));
+        if (k < cap) ids[1 + k] = id;
     }
 }
 
@@ -1657,6 +1698,44 @@ int mercury_b200_energy(double h, int physical, const double* spin, double* e, d
         return 0;
     } catch (const std::exception& ex) {
         return report(ex);
+    }
+}
+
+int mercury_b200_ejections(double h, int physical, double rmax, int i0, int* ids, int cap, int* count) {
+    Context& c = ctx();
+    try {
+        require_system();
+        if (!(rmax > 0.0) || !std::isfinite(rmax)) throw std::runtime_error("ejection radius must be positive");
+        if (cap < 0 || (cap > 0 && !ids) || !count) throw std::runtime_error("invalid ejection output");
+        const double* bx = c.bigstate[c.cur].p;
+        const double* px = c.pstate[c.cur].p;
+        if (physical && c.algorithm == 1) {
+            run_corrector(h);
+            bx = c.corr_big.p;
+            px = c.corr_part.p;
+        }
+        const int first = i0 <= 0 ? 1 : i0 - 1;   // mxx_ejec: i0 <= 0 means 2
+        const int total = c.nsplit + c.np;
+        c.ej_ids.reserve((size_t)c.n + 1);
+        check(cudaMemsetAsync(c.ej_ids.p, 0, sizeof(int), c.stream), "memset");
+        ejection_kernel<<<blocks(total), 256, 0, c.stream>>>(bx, c.nsplit, px, c.npcap, c.np, c.permp(), first,
+                                                            rmax * rmax, c.ej_ids.p, c.n);
+        check(cudaGetLastError(), "launch");
+        int found = 0;
+        check(cudaMemcpyAsync(&found, c.ej_ids.p, sizeof(int), cudaMemcpyDeviceToHost, c.stream), "ejections");
+        check(cudaStreamSynchronize(c.stream), "ejections");
+        std::vector<int> got(found);
+        if (found) {
+            check(cudaMemcpyAsync(got.data(), c.ej_ids.p + 1, sizeof(int) * found, cudaMemcpyDeviceToHost, c.stream),
+                  "ejections");
+            check(cudaStreamSynchronize(c.stream), "ejections");
+        }
+        std::sort(got.begin(), got.end());
+        for (int k = 0; k < found && k < cap; ++k) ids[k] = got[k];
+        *count = found;
+        return 0;
+    } catch (const std::exception& e) {
+        return report(e);
     }
 }
 

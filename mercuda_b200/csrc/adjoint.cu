@@ -22,6 +22,7 @@
 
 #include "../../include/mercury_b200.h"
 #include "context.cuh"
+#include "force_adjoint.cuh"
 #include "kepler.cuh"
 #include "kepler_adjoint.cuh"
 #include "mvs.cuh"
@@ -71,9 +72,7 @@ __device__ __forceinline__ double3 accel(const double3 x, const double3 v, doubl
 }
 
 // Transposed Jacobian of that acceleration applied to la: adds to gx, gv and
-// gyar. Gravity: -sum_b m_b d/|d|^3 with d = x - x_b; Yarkovsky (mfo_ngf):
-// yar t / (r^2 |t|) with t = v - (x.v / r^2) x, differentiated in yar even
-// where yar is zero.
+// gyar. Gravity: -sum_b m_b d/|d|^3 with d = x - x_b; Yarkovsky: yar_vjp.
 template <bool YAR>
 __device__ __forceinline__ void accel_vjp(const double3 x, const double3 v, double yar, const double* T, int nb,
                                           const double3 la, double3& gx, double3& gv, double& gyar) {
@@ -91,34 +90,7 @@ __device__ __forceinline__ void accel_vjp(const double3 x, const double3 v, doub
         gx.y -= m * (s_3 * la.y - 3.0 * s_5 * dl * dy);
         gx.z -= m * (s_3 * la.z - 3.0 * s_5 * dl * dz);
     }
-    if (YAR) {
-        const double r2 = x.x * x.x + x.y * x.y + x.z * x.z;
-        const double p = x.x * v.x + x.y * v.y + x.z * v.z;
-        const double q = p / r2;
-        const double3 t = make_double3(v.x - q * x.x, v.y - q * x.y, v.z - q * x.z);
-        const double tn = sqrt(t.x * t.x + t.y * t.y + t.z * t.z);
-        const double A = la.x * t.x + la.y * t.y + la.z * t.z;
-        const double k = yar / (r2 * tn);
-        const double kt = A * yar / (r2 * tn * tn * tn);
-        const double3 lt = make_double3(k * la.x - kt * t.x, k * la.y - kt * t.y, k * la.z - kt * t.z);
-        double lr2 = -A * yar / (r2 * r2 * tn);
-        gyar += A / (r2 * tn);
-        gv.x += lt.x;
-        gv.y += lt.y;
-        gv.z += lt.z;
-        const double lq = -(lt.x * x.x + lt.y * x.y + lt.z * x.z);
-        gx.x -= q * lt.x;
-        gx.y -= q * lt.y;
-        gx.z -= q * lt.z;
-        const double lp = lq / r2;
-        lr2 -= lq * p / (r2 * r2);
-        gx.x += lp * v.x + 2.0 * lr2 * x.x;
-        gx.y += lp * v.y + 2.0 * lr2 * x.y;
-        gx.z += lp * v.z + 2.0 * lr2 * x.z;
-        gv.x += lp * x.x;
-        gv.y += lp * x.y;
-        gv.z += lp * x.z;
-    }
+    if (YAR) yar_vjp(x, v, yar, la, gx, gv, gyar);
 }
 
 __device__ __forceinline__ void st_ckpt(double* c, int np, int p, double3 x, double3 v, double3 a) {

@@ -113,6 +113,57 @@ __device__ double3 hkce_particle_force(const BsArgs& A, int g, const double3 x, 
     return hkce_central(a, x, A.f.m0);
 }
 
+// hkce_particle_force and its derivative along dx (J dx with J = da/dx; the
+// partners' positions are fixed: massless members never act on the Big
+// bodies). Pair terms: a -= t(s) m_i d with t = s^-3 inside 0.1 rc and
+// (1 - K(q)) s^-3 up to rc, so J dx -= m_i [t dx + t'(s)/s (d.dx) d];
+// K'(q) = 30 q^2 (1 - q)^2.
+__device__ double3 hkce_particle_force_jvp(const BsArgs& A, int g, const double3 x, const double3 dx,
+                                           double rcrit_p, const double* T, double3& da) {
+    double3 a = make_double3(0.0, 0.0, 0.0);
+    da = a;
+    for (int e = A.adj_off[g]; e < A.adj_off[g + 1]; ++e) {
+        const int i = A.adj[e].x;
+        const double* row = T + FT_HEAD + 4 * (i - 1);
+        const double ex = x.x - row[0], ey = x.y - row[1], ez = x.z - row[2];
+        const double s2 = ex * ex + ey * ey + ez * ez;
+        const double rc = fmax(A.rcrit[i], rcrit_p);
+        double tmp2;
+        if (!hkce_pair(s2, rc, tmp2)) continue;
+        const double s_1 = 1.0 / sqrt(s2);
+        const double s_3 = s_1 * s_1 * s_1;
+        double t1;  // t'(s) / s
+        if (s2 <= 0.01 * rc * rc) {
+            t1 = -3.0 * s_3 * s_1 * s_1;
+        } else {
+            const double s = 1.0 / s_1;
+            const double q = (s - 0.1 * rc) / (0.9 * rc);
+            const double q2 = q * q, q3 = q * q2, q4 = q2 * q2, q5 = q2 * q3;
+            const double K = 10.0 * q3 - 15.0 * q4 + 6.0 * q5;
+            const double Kq = 30.0 * q2 * (1.0 - q) * (1.0 - q);
+            t1 = (-Kq / (0.9 * rc) * s_3 - 3.0 * (1.0 - K) * s_3 * s_1) * s_1;
+        }
+        const double mi = row[3];
+        const double faci = tmp2 * mi;
+        a.x = a.x - faci * ex;
+        a.y = a.y - faci * ey;
+        a.z = a.z - faci * ez;
+        const double ed = (ex * dx.x + ey * dx.y + ez * dx.z) * t1;
+        da.x -= mi * (tmp2 * dx.x + ed * ex);
+        da.y -= mi * (tmp2 * dx.y + ed * ey);
+        da.z -= mi * (tmp2 * dx.z + ed * ez);
+    }
+    const double s2 = x.x * x.x + x.y * x.y + x.z * x.z;
+    const double s_1 = 1.0 / sqrt(s2);
+    const double s_3 = s_1 * s_1 * s_1;
+    const double m0 = A.f.m0;
+    const double xd = (x.x * dx.x + x.y * dx.y + x.z * dx.z) * 3.0 * s_3 * s_1 * s_1;
+    da.x -= m0 * (s_3 * dx.x - xd * x.x);
+    da.y -= m0 * (s_3 * dx.y - xd * x.y);
+    da.z -= m0 * (s_3 * dx.z - xd * x.z);
+    return hkce_central(a, x, m0);
+}
+
 // ------------------------------------------------------------ massive set
 // Scratch rows of the massive-set CTA, each [nsplit] doubles.
 struct BsScratch {
@@ -450,6 +501,82 @@ template <int VARIANT> __global__ void __launch_bounds__(128) bs_particle_kernel
     }
 }
 
+// Tangent of one accepted BS2 step of the encounter subsystem for its
+// massless members: thread (slot p, direction d) pushes column d of the
+// slot's accumulated 6x6 Jacobian tg (entry (d * 6 + r) * npcap + p holds
+// d state_r / d start_d) through levels 1..levels and the Neville
+// extrapolation that produced the accepted state: the particle kernel's
+// statements differentiated, with the step control's choices fixed. The
+// primal midpoint states are recomputed alongside from the same table rows.
+__global__ void __launch_bounds__(64) bs2_tangent_kernel(BsArgs A, int levels, double* tg) {
+    extern __shared__ double dcol[];
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    const int p = q / 6, d = q - 6 * p;
+    if (p >= A.np) return;
+    const int nb = A.f.nbig - 1, stride = force_row(nb), S = A.npcap, T = blockDim.x;
+    auto D = [&](int j, int c) -> double& { return dcol[((j - 1) * 6 + c) * T + threadIdx.x]; };
+    const double3 x0 = make_double3(A.px[p], A.px[S + p], A.px[2 * S + p]);
+    const double3 v0 = make_double3(A.px[3 * S + p], A.px[4 * S + p], A.px[5 * S + p]);
+    const int g = A.f.nsplit + A.perm[p];
+    const double rcrit_p = A.pconst[(size_t)PC_RCRIT * S + p];
+    double* col = tg + (size_t)(6 * d) * S + p;
+    const double3 dx0 = make_double3(col[0], col[S], col[2 * (size_t)S]);
+    const double3 dv0 = make_double3(col[3 * (size_t)S], col[4 * (size_t)S], col[5 * (size_t)S]);
+    double3 da0;
+    const double3 a0 = hkce_particle_force_jvp(A, g, x0, dx0, rcrit_p, A.table, da0);
+    int row = 1;
+#pragma unroll 1
+    for (int n = 1; n <= levels; ++n) {
+        const double h = level_h<2>(A.h0, n);
+        const double h2n = level_h2<2>(A.h0, n);
+        const double hby2 = 0.5 * h, h2by2 = 0.5 * h2n;
+        double3 b = make_double3(0.5 * a0.x, 0.5 * a0.y, 0.5 * a0.z);
+        double3 c = make_double3(0.0, 0.0, 0.0);
+        double3 xe = make_double3(h2by2 * a0.x + h * v0.x + x0.x, h2by2 * a0.y + h * v0.y + x0.y,
+                                  h2by2 * a0.z + h * v0.z + x0.z);
+        double3 db = make_double3(0.5 * da0.x, 0.5 * da0.y, 0.5 * da0.z);
+        double3 dc = make_double3(0.0, 0.0, 0.0);
+        double3 dxe = make_double3(h2by2 * da0.x + h * dv0.x + dx0.x, h2by2 * da0.y + h * dv0.y + dx0.y,
+                                   h2by2 * da0.z + h * dv0.z + dx0.z);
+#pragma unroll 1
+        for (int j = 2; j <= n; ++j) {
+            double3 da;
+            const double3 a = hkce_particle_force_jvp(A, g, xe, dxe, rcrit_p, A.table + (size_t)(row++) * stride, da);
+            const double tmp0 = h * double(j);
+            b = make_double3(b.x + a.x, b.y + a.y, b.z + a.z);
+            c = make_double3(c.x + b.x, c.y + b.y, c.z + b.z);
+            xe = make_double3(h2n * c.x + h2by2 * a0.x + tmp0 * v0.x + x0.x,
+                              h2n * c.y + h2by2 * a0.y + tmp0 * v0.y + x0.y,
+                              h2n * c.z + h2by2 * a0.z + tmp0 * v0.z + x0.z);
+            db = make_double3(db.x + da.x, db.y + da.y, db.z + da.z);
+            dc = make_double3(dc.x + db.x, dc.y + db.y, dc.z + db.z);
+            dxe = make_double3(h2n * dc.x + h2by2 * da0.x + tmp0 * dv0.x + dx0.x,
+                               h2n * dc.y + h2by2 * da0.y + tmp0 * dv0.y + dx0.y,
+                               h2n * dc.z + h2by2 * da0.z + tmp0 * dv0.z + dx0.z);
+        }
+        double3 da;
+        hkce_particle_force_jvp(A, g, xe, dxe, rcrit_p, A.table + (size_t)(row++) * stride, da);
+        D(n, 0) = dxe.x;
+        D(n, 1) = dxe.y;
+        D(n, 2) = dxe.z;
+        D(n, 3) = h * db.x + hby2 * da.x + dv0.x;
+        D(n, 4) = h * db.y + hby2 * da.y + dv0.y;
+        D(n, 5) = h * db.z + hby2 * da.z + dv0.z;
+#pragma unroll 1
+        for (int j = n - 1; j >= 1; --j) {
+            const double tmp0 = 1.0 / (level_h2<2>(A.h0, j) - h2n);
+            const double tmp1 = tmp0 * level_h2<2>(A.h0, j + 1);
+            const double tmp2 = tmp0 * h2n;
+            for (int c6 = 0; c6 < 6; ++c6) D(j, c6) = tmp1 * D(j + 1, c6) - tmp2 * D(j, c6);
+        }
+    }
+    for (int c6 = 0; c6 < 6; ++c6) {
+        double s = D(1, c6);
+        for (int j = 2; j <= levels; ++j) s = s + D(j, c6);
+        col[(size_t)c6 * S] = s;
+    }
+}
+
 __global__ void __launch_bounds__(128) bs_commit_kernel(BsCommitArgs A) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     const int N = A.nsplit, S = A.npcap;
@@ -495,6 +622,14 @@ template <int VARIANT> void launch_variant(const BsArgs& a, cudaStream_t s) {
 void launch_bs_sequence(const BsArgs& a, cudaStream_t s) {
     if (a.variant == 1) launch_variant<1>(a, s);
     else launch_variant<2>(a, s);
+}
+
+void launch_bs2_tangent(const BsArgs& a, int levels, double* tg, cudaStream_t s) {
+    if (a.np <= 0 || levels < 1 || levels > bs_levels(2)) return;
+    const int threads = 64;
+    const size_t smem = sizeof(double) * 6 * bs_levels(2) * threads;
+    const long long total = 6LL * a.np;
+    bs2_tangent_kernel<<<(unsigned)((total + threads - 1) / threads), threads, smem, s>>>(a, levels, tg);
 }
 
 void launch_bs_commit(const BsCommitArgs& a, cudaStream_t s) {

@@ -68,5 +68,10 @@ struct BsCommitArgs {
 
 void launch_bs_sequence(const BsArgs& a, cudaStream_t s);
 void launch_bs_commit(const BsCommitArgs& a, cudaStream_t s);
+// Tangent of the accepted mdt_bs2 step (levels = accepted level) of the
+// encounter subsystem's massless members: tg [36][npcap], entry
+// (d * 6 + r) * npcap + slot = d state_r / d (step start)_d, is advanced in
+// place from the start-of-step state a.px and the sequence's table a.table.
+void launch_bs2_tangent(const BsArgs& a, int levels, double* tg, cudaStream_t s);
 
 }  // namespace mb200

@@ -91,6 +91,7 @@ struct Context {
     // output corrector scratch: Big [9][nbig], particles [6][npcap]
     DBuf<double> corr_big, corr_part;
     DBuf<double> energy_scr;         // mxx_en: per-body pair sums, then e and l2
+    DBuf<int> ej_ids;                // mxx_ejec screen: count, then the ids found
     // Bulirsch-Stoer: massive-set scratch, per-level candidate states, per-level
     // error maxima and force-fault words
     DBuf<double> bs_scr, bs_bcand, bs_pcand;
@@ -110,6 +111,10 @@ struct Context {
     bool encounter = false;
     DBuf<int> adj_off;
     DBuf<int2> adj;
+    // with tangent set (HYBRID adjoint), every accepted BS2 step also advances
+    // the massless members' 6x6 Jacobians tg [36][npcap]
+    bool tangent = false;
+    DBuf<double> tg;
     // events
     DBuf<MercuryEvent> events;
     DBuf<int> event_step;
@@ -168,9 +173,9 @@ struct Context {
                                 &pstate[1], &pconst[0], &pconst[1], &tab, &detail, &transfer, &snapshot, &snap_const,
                                 &ra_bb, &ra_be, &ra_bg, &ra_bpx, &ra_pb, &ra_pe, &ftab, &force_out, &boxes, &corr_big, &corr_part, &energy_scr,
                                 &bs_scr, &bs_bcand, &bs_pcand, &rcritbig, &hy_scr, &hy_tab, &hy_off,
-                                &hy_packed};
+                                &hy_packed, &tg};
         for (auto* b : bufs) b->release();
-        DBuf<int>* ibufs[] = {&perm[0], &perm[1], &inv, &order_bucket, &order_hist, &snap_perm};
+        DBuf<int>* ibufs[] = {&perm[0], &perm[1], &inv, &order_bucket, &order_hist, &snap_perm, &ej_ids};
         for (auto* b : ibufs) b->release();
         ra_max.release();
         bs_errs.release();
@@ -181,6 +186,7 @@ struct Context {
         adj.release();
         hy_members.clear();
         hy_begun = false;
+        tangent = false;
         kc = 0;
         events.release();
         event_step.release();
@@ -195,6 +201,7 @@ struct Context {
 };
 
 Context& ctx();
+int active_context();   // 0: the resident system, 1: the encounter subsystem
 
 // Layout kernels between the host's interleaved rows and the device SoA.
 void scatter_rows(const double* rows, int n, int comps, int nbig, double* big, int big_stride, double* part,
