@@ -91,6 +91,8 @@ def lib() -> C.CDLL:
         L.oracle_mvs_jacobian.restype = I
         L.oracle_hy_jacobian.argtypes = [I, I, PD, PD, PD, PD, I, PD, D, I, D, PD]
         L.oracle_hy_jacobian.restype = I
+        L.oracle_mxx_ejec.argtypes = [I, I, PD, D, C.POINTER(I)]
+        L.oracle_mxx_ejec.restype = I
         L.oracle_mxx_en.argtypes = [I, PD, PD, PD, C.c_void_p, PD, PD]
         L.oracle_mxx_en.restype = None
         _lib = L
@@ -320,6 +322,16 @@ def hy_jacobian(sys, h, nsteps, tol=1e-12):
     if rc:
         raise RuntimeError("oracle HYBRID Jacobian run failed")
     return jac
+
+
+def mxx_ejec(x, rmax, i0=2):
+    """mxx_ejec's test (mercury6_2.for:7071-7082) on heliocentric x (n, 3):
+    ascending 1-based ids of bodies j >= i0 beyond rmax."""
+    x = _f64(x)
+    n = len(x)
+    ids = np.zeros(max(1, n), dtype=np.int32)
+    k = lib().oracle_mxx_ejec(n, int(i0), _p(x), float(rmax), ids.ctypes.data_as(C.POINTER(I)))
+    return ids[:k].copy()
 
 
 def mxx_en(m, x, v, jcen, spin=None):

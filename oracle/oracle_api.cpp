@@ -513,6 +513,20 @@ int oracle_hy_jacobian(int n, int nbig, const double* m, double* x, double* v, c
     return 0;
 }
 
+// mxx_ejec's test (mercury6_2.for:7071-7082): the 1-based ids (ascending) of
+// bodies j >= i0 (1-based; i0 <= 0 means 2) with x*x + y*y + z*z > rmax^2.
+int oracle_mxx_ejec(int n, int i0, const double* x, double rmax, int* ids) {
+    if (i0 <= 0) i0 = 2;
+    const double rmax2 = rmax * rmax;
+    int k = 0;
+    for (int j = i0; j <= n; ++j) {
+        const double* p = x + 3 * (size_t)(j - 1);
+        const double r2 = p[0] * p[0] + p[1] * p[1] + p[2] * p[2];
+        if (r2 > rmax2) ids[k++] = j;
+    }
+    return k;
+}
+
 // mxx_en of n bodies (Fortran layout); s may be null. out = {e, l2}.
 void oracle_mxx_en(int n, const double* m, const double* xh, const double* vh, const double* s, const double* jcen,
                    double* out) {
