@@ -51,6 +51,18 @@ int mercury_b200_energy(double h, int physical, const double* spin, double* e, d
  * reference host downloads every body at the nfun cadence for this test
  * (mercury6_2.for:929-948); this reads back the ids only. */
 int mercury_b200_ejections(double h, int physical, double rmax, int i0, int* ids, int cap, int* count);
+/* mio_ce's close-encounter records (mercury6_2.for:5456-5510) encoded on the
+ * device: for each record of events[0 .. n) with kind bit 1 (a close
+ * encounter, as gpu_find_events selects them), in order, the 70-character
+ * record body c(1:70) that mio_ce writes after char(12)//'6b' (base-224
+ * fields from mio_fl2c, mio_re2c and mco_x2ov: time, ids, distance, then each
+ * body's log-distance, angles, velocity ratio and velocity angles), into
+ * lines + 70 k. mcen is the central mass m(1) in K2 units, rcen and rmax the
+ * run's radii. *count receives the number of lines. The reference host
+ * encodes every record itself; a 4,100-record burst (tests/test_events.py)
+ * is one launch here. */
+int mercury_b200_encode_ce(const MercuryEvent* events, int n, double mcen, double rcen, double rmax, char* lines,
+                           int* count);
 /* Launch shape of the particle kernel: threads per CTA (multiple of 32) and
  * steps fused per launch (0 = automatic); a negative value keeps the setting. */
 int mercury_b200_set_launch(int particle_threads, int steps_per_launch);

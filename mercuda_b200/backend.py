@@ -52,7 +52,8 @@ EXTENSION_SYMBOLS = ["mercury_b200_mvs_advance", "mercury_b200_events", "mercury
                      "mercury_b200_adjoint_backward", "mercury_b200_adjoint_timing", "mercury_b200_adjoint_free",
                      "mercury_b200_energy", "mercury_b200_hybrid_adjoint_forward",
                      "mercury_b200_hybrid_adjoint_backward", "mercury_b200_hybrid_adjoint_timing",
-                     "mercury_b200_hybrid_adjoint_free", "mercury_b200_ejections"]
+                     "mercury_b200_hybrid_adjoint_free", "mercury_b200_ejections",
+                     "mercury_b200_encode_ce"]
 
 
 class BackendError(RuntimeError):
@@ -96,6 +97,7 @@ def load_library(path: Path | str | None = None) -> C.CDLL:
     L.mercury_b200_dropin_time.argtypes = [PD, PI64, I]
     L.mercury_b200_energy.argtypes = [D, I, PD, PD, PD]
     L.mercury_b200_ejections.argtypes = [D, I, D, I, PI, I, PI]
+    L.mercury_b200_encode_ce.argtypes = [C.c_void_p, I, D, D, D, C.c_void_p, PI]
     L.mercury_b200_batch_upload.argtypes = [I, PI, PI, PD, PD, PD, PD, PD, PD]
     L.mercury_b200_batch_advance.argtypes = [D, I, D, PI]
     L.mercury_b200_batch_events.argtypes = [C.c_void_p, PI, PI, I]
@@ -123,6 +125,19 @@ def load_library(path: Path | str | None = None) -> C.CDLL:
 def _p(a: np.ndarray):
     assert a.dtype == np.float64 and a.flags.c_contiguous, "float64 C-contiguous array required"
     return a.ctypes.data_as(PD)
+
+
+def encode_ce(events: np.ndarray, mcen: float, rcen: float, rmax: float, lib: C.CDLL | None = None) -> np.ndarray:
+    """mio_ce's 70-character record bodies of the close encounters (kind bit 1)
+    among `events` (EVENT_DTYPE records), encoded on the device: uint8 (count, 70)."""
+    L = lib or load_library()
+    ev = np.ascontiguousarray(events, dtype=EVENT_DTYPE)
+    lines = np.zeros((max(1, len(ev)), 70), dtype=np.uint8)
+    count = C.c_int(0)
+    if L.mercury_b200_encode_ce(ev.ctypes.data_as(C.c_void_p), len(ev), mcen, rcen, rmax,
+                                lines.ctypes.data_as(C.c_void_p), C.byref(count)) != 0:
+        raise BackendError("close-encounter encoding failed")
+    return lines[:count.value].copy()
 
 
 class Backend:

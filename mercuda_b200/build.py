@@ -16,7 +16,8 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 LIB = HERE / "libmercury_cuda.so"
-SOURCES = ["mvs.cu", "abi.cu", "peak.cu", "noalloc.cu", "radau.cu", "bs.cu", "hybrid.cu", "batch.cu", "adjoint.cu", "energy.cu", "hybrid_adjoint.cu"]
+SOURCES = ["mvs.cu", "abi.cu", "peak.cu", "noalloc.cu", "radau.cu", "bs.cu", "hybrid.cu", "batch.cu", "adjoint.cu", "energy.cu", "hybrid_adjoint.cu",
+           "encode.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "--fmad=false", "-lineinfo", "-Xcompiler", "-fPIC", "-shared",
          "-cudart", "static", "-Xptxas", "-warn-spills", "-Xlinker", "--no-undefined"]

@@ -93,6 +93,8 @@ def lib() -> C.CDLL:
         L.oracle_hy_jacobian.restype = I
         L.oracle_mxx_ejec.argtypes = [I, I, PD, D, C.POINTER(I)]
         L.oracle_mxx_ejec.restype = I
+        L.oracle_mio_ce.argtypes = [C.c_void_p, I, D, D, D, C.c_void_p]
+        L.oracle_mio_ce.restype = I
         L.oracle_mxx_en.argtypes = [I, PD, PD, PD, C.c_void_p, PD, PD]
         L.oracle_mxx_en.restype = None
         _lib = L
@@ -332,6 +334,17 @@ def mxx_ejec(x, rmax, i0=2):
     ids = np.zeros(max(1, n), dtype=np.int32)
     k = lib().oracle_mxx_ejec(n, int(i0), _p(x), float(rmax), ids.ctypes.data_as(C.POINTER(I)))
     return ids[:k].copy()
+
+
+def mio_ce(events, mcen, rcen, rmax):
+    """mio_ce's 70-character record bodies (mercury6_2.for:5456-5510) of the
+    close encounters (kind bit 1) among `events` (EVENT_DTYPE), in order:
+    uint8 array (count, 70)."""
+    ev = np.ascontiguousarray(events, dtype=EVENT_DTYPE)
+    lines = np.zeros((max(1, len(ev)), 70), dtype=np.uint8)
+    k = lib().oracle_mio_ce(ev.ctypes.data_as(C.c_void_p), len(ev), float(mcen), float(rcen), float(rmax),
+                            lines.ctypes.data_as(C.c_void_p))
+    return lines[:k].copy()
 
 
 def mxx_en(m, x, v, jcen, spin=None):

@@ -14,6 +14,7 @@
 #include "oracle_hy.hpp"
 #include "oracle_dual.hpp"
 #include "oracle_energy.hpp"
+#include "oracle_io.hpp"
 
 namespace oracle {
 thread_local Tally tally;
@@ -523,6 +524,19 @@ int oracle_mxx_ejec(int n, int i0, const double* x, double rmax, int* ids) {
         const double* p = x + 3 * (size_t)(j - 1);
         const double r2 = p[0] * p[0] + p[1] * p[1] + p[2] * p[2];
         if (r2 > rmax2) ids[k++] = j;
+    }
+    return k;
+}
+
+// mio_ce's record bodies (70 characters each) of the close encounters
+// (kind bit 1) among n event records, in order; returns their count.
+int oracle_mio_ce(const Event* ev, int n, double mcen, double rcen, double rmax, unsigned char* lines) {
+    int k = 0;
+    for (int q = 0; q < n; ++q) {
+        if (!(ev[q].kind & 1)) continue;
+        oracle::mio_ce_record(ev[q].time, ev[q].i, ev[q].j, ev[q].distance, ev[q].xi, ev[q].xj, mcen, rcen, rmax,
+                              lines + 70 * (size_t)k);
+        ++k;
     }
     return k;
 }
