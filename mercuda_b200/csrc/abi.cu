@@ -405,7 +405,7 @@ void bs_step_once(double time, double* h, double* hdid, double tol, int64_t* rej
     const int V = c.algorithm == 2 ? 1 : 2;
     const int L = bs_levels(V), nb = c.nbig - 1, N = c.nsplit;
     c.ftab.reserve((size_t)bs_rows(V) * force_row(nb));
-    c.bs_scr.reserve((size_t)bs_massive_scratch(V) * N);
+    c.bs_scr.reserve(bs_massive_scratch(V, N, nb));
     c.bs_bcand.reserve((size_t)bs_candidates(V) * 6 * N);
     c.bs_pcand.reserve((size_t)bs_candidates(V) * 6 * c.npcap);
     c.bs_errs.reserve(13);
@@ -428,7 +428,8 @@ void bs_step_once(double time, double* h, double* hdid, double tol, int64_t* rej
         a.bx = c.bigstate[in].p;
         a.mbig = c.mbig.p;
         a.ngfbig = c.ngfbig.p;
-        a.bscr = c.bs_scr.p;
+        a.draw = c.bs_scr.p;
+        a.tscr = c.bs_scr.p + (size_t)L * 6 * N;
         a.px = c.pstate[in].p;
         a.pconst = c.pconst[c.kc].p;
         a.table = c.ftab.p;

@@ -165,19 +165,6 @@ __device__ double3 hkce_particle_force_jvp(const BsArgs& A, int g, const double3
 }
 
 // ------------------------------------------------------------ massive set
-// Scratch rows of the massive-set CTA, each [nsplit] doubles.
-struct BsScratch {
-    double *X, *V, *XE, *VE, *A, *A0, *B, *C, *XS, *VS, *D;
-    __device__ BsScratch(double* base, int N) {
-        double* p = base;
-        double** rows[] = {&X, &V, &XE, &VE, &A, &A0, &B, &C};
-        for (double** r : rows) { *r = p; p += 3 * N; }
-        XS = p; p += N;
-        VS = p; p += N;
-        D = p;  // [levels][6][N]
-    }
-};
-
 // One force call of the massive set into S.A (or A0) and table row T; mb
 // and ngf are the set's masses and non-gravitational constants, head a
 // shared copy of the row's head for the set's own forces.
@@ -215,129 +202,138 @@ __device__ void massive_call(const BsArgs& A, const double* X, const double* V, 
     __syncthreads();
 }
 
-// The massive set through every level: one CTA. With STAGED the scratch
-// (states, accelerations, the extrapolation table), the starting state, the
-// masses and the non-gravitational constants live in shared memory.
-template <int VARIANT, bool STAGED> __global__ void __launch_bounds__(256) bs_massive_kernel(BsArgs A) {
+// The massive set through one level per CTA (level n = blockIdx.x + 1): the
+// levels of a BS step are independent given the start-of-step state and force,
+// so the CTAs run side by side and the step's critical path is its longest
+// level instead of the sum of all levels. Each CTA keeps its states,
+// accelerations, the starting state, masses and non-gravitational constants
+// in shared memory, writes the table rows of its level's force calls and its
+// raw level state D(n) to A.draw; bs_massive_extrap_kernel then runs the
+// Neville updates in level order. The start-of-step force is computed by
+// every CTA (the same statements), level 1's writing table row 0 and the
+// others a private row.
+template <int VARIANT> __global__ void __launch_bounds__(256) bs_massive_level_kernel(BsArgs A) {
     extern __shared__ double sm[];
-    const int N = A.f.nsplit, tid = threadIdx.x, nt = blockDim.x;
-    const int L = bs_levels(VARIANT), stride = force_row(A.f.nbig - 1);
-    BsScratch S(STAGED ? sm : A.bscr, N);
-    const double *X0, *V0, *mb, *ngf;
-    if (STAGED) {
-        double* p = sm + (size_t)bs_massive_scratch(VARIANT) * N;
-        for (int q = tid; q < 6 * N; q += nt) p[q] = A.bx[q];
-        for (int q = tid; q < N; q += nt) p[6 * N + q] = A.mbig[q];
-        for (int q = tid; q < 5 * N; q += nt) p[7 * N + q] = A.ngfbig[q];
-        X0 = p;
-        V0 = p + 3 * N;
-        mb = p + 6 * N;
-        ngf = p + 7 * N;
-        __syncthreads();
-    } else {
-        X0 = A.bx;
-        V0 = A.bx + 3 * N;
-        mb = A.mbig;
-        ngf = A.ngfbig;
-    }
+    const int N = A.f.nsplit, tid = threadIdx.x, nt = blockDim.x, n = blockIdx.x + 1;
+    const int stride = force_row(A.f.nbig - 1);
+    double* X = sm;
+    double* V = sm + 3 * N;
+    double* XE = sm + 6 * N;
+    double* VE = sm + 9 * N;
+    double* Acc = sm + 12 * N;
+    double* A0 = sm + 15 * N;
+    double* B = sm + 18 * N;
+    double* C = sm + 21 * N;
+    double* p = sm + (size_t)BS_LEVEL_ROWS * N;
+    for (int q = tid; q < 6 * N; q += nt) p[q] = A.bx[q];
+    for (int q = tid; q < N; q += nt) p[6 * N + q] = A.mbig[q];
+    for (int q = tid; q < 5 * N; q += nt) p[7 * N + q] = A.ngfbig[q];
+    const double* X0 = p;
+    const double* V0 = p + 3 * N;
+    const double* mb = p + 6 * N;
+    const double* ngf = p + 7 * N;
+    __syncthreads();
     __shared__ double head[FT_HEAD];
-    auto call = [&](const double* X, const double* V, double* out, double* T, DeviceStatus* st) {
-        massive_call(A, X, V, out, T, st, mb, ngf, head);
+    auto call = [&](const double* Xc, const double* Vc, double* out, double* T, DeviceStatus* st) {
+        massive_call(A, Xc, Vc, out, T, st, mb, ngf, head);
     };
-    __shared__ double wmax[8];
-    __shared__ int wbad[8];
-    for (int k = tid; k < N; k += nt) {
+    for (int k = tid; k < N; k += nt)
         for (int c = 0; c < 3; ++c) {
             const int z = c * N + k;
-            S.X[z] = X0[z]; S.V[z] = V0[z]; S.XE[z] = X0[z]; S.VE[z] = V0[z];
+            X[z] = X0[z]; V[z] = V0[z]; XE[z] = X0[z]; VE[z] = V0[z];
         }
-        const double tmp1 = X0[k] * X0[k] + X0[N + k] * X0[N + k] + X0[2 * N + k] * X0[2 * N + k];
-        const double tmp2 = V0[k] * V0[k] + V0[N + k] * V0[N + k] + V0[2 * N + k] * V0[2 * N + k];
-        S.XS[k] = 1.0 / fmax(tmp1, 1e-300);
-        S.VS[k] = 1.0 / fmax(tmp2, 1e-300);
+    call(X0, V0, A0, n == 1 ? A.table : A.tscr + (size_t)(n - 2) * stride, &A.lvst[0]);
+    int row = 1;
+    for (int m = 1; m < n; ++m) row += bs_level_forces(VARIANT, m);
+    DeviceStatus* st = &A.lvst[n];
+    const double h = level_h<VARIANT>(A.h0, n);
+    const double h2n = level_h2<VARIANT>(A.h0, n);
+    double* Dn = A.draw + (size_t)(n - 1) * 6 * N;
+    if (VARIANT == 1) {
+        const double hx2 = h * 2.0;
+        for (int k = 1 + tid; k < N; k += nt)
+            for (int c = 0; c < 3; ++c) {
+                const int z = c * N + k;
+                X[z] = X0[z] + h * V0[z];
+                V[z] = V0[z] + h * A0[z];
+            }
+        call(X, V, Acc, A.table + (size_t)(row++) * stride, st);
+        for (int k = 1 + tid; k < N; k += nt)
+            for (int c = 0; c < 3; ++c) {
+                const int z = c * N + k;
+                XE[z] = X0[z] + hx2 * V[z];
+                VE[z] = V0[z] + hx2 * Acc[z];
+            }
+        for (int j = 2; j <= n; ++j) {
+            call(XE, VE, Acc, A.table + (size_t)(row++) * stride, st);
+            for (int k = 1 + tid; k < N; k += nt)
+                for (int c = 0; c < 3; ++c) {
+                    const int z = c * N + k;
+                    X[z] = X[z] + hx2 * VE[z];
+                    V[z] = V[z] + hx2 * Acc[z];
+                }
+            call(X, V, Acc, A.table + (size_t)(row++) * stride, st);
+            for (int k = 1 + tid; k < N; k += nt)
+                for (int c = 0; c < 3; ++c) {
+                    const int z = c * N + k;
+                    XE[z] = XE[z] + hx2 * V[z];
+                    VE[z] = VE[z] + hx2 * Acc[z];
+                }
+        }
+        call(XE, VE, Acc, A.table + (size_t)(row++) * stride, st);
+        for (int k = 1 + tid; k < N; k += nt)
+            for (int c = 0; c < 3; ++c) {
+                const int z = c * N + k;
+                Dn[z] = 0.5 * (XE[z] + X[z] + h * VE[z]);
+                Dn[3 * N + z] = 0.5 * (VE[z] + V[z] + h * Acc[z]);
+            }
+    } else {
+        const double hby2 = 0.5 * h, h2by2 = 0.5 * h2n;
+        for (int k = 1 + tid; k < N; k += nt)
+            for (int c = 0; c < 3; ++c) {
+                const int z = c * N + k;
+                B[z] = 0.5 * A0[z];
+                C[z] = 0.0;
+                XE[z] = h2by2 * A0[z] + h * V0[z] + X0[z];
+            }
+        for (int j = 2; j <= n; ++j) {
+            call(XE, V0, Acc, A.table + (size_t)(row++) * stride, st);
+            const double tmp0 = h * double(j);
+            for (int k = 1 + tid; k < N; k += nt)
+                for (int c = 0; c < 3; ++c) {
+                    const int z = c * N + k;
+                    B[z] = B[z] + Acc[z];
+                    C[z] = C[z] + B[z];
+                    XE[z] = h2n * C[z] + h2by2 * A0[z] + tmp0 * V0[z] + X0[z];
+                }
+        }
+        call(XE, V0, Acc, A.table + (size_t)(row++) * stride, st);
+        for (int k = 1 + tid; k < N; k += nt)
+            for (int c = 0; c < 3; ++c) {
+                const int z = c * N + k;
+                Dn[z] = XE[z];
+                Dn[3 * N + z] = h * B[z] + hby2 * Acc[z] + V0[z];
+            }
     }
-    int row = 0;
-    call(X0, V0, S.A0, A.table, &A.lvst[0]);
-    ++row;
+}
+
+// The massive set's extrapolation in level order (one CTA): the Neville
+// updates (mercury6_2.for:3352-3366), each thread its own bodies, then from
+// level 4 on the level's error maximum and candidate state.
+template <int VARIANT> __global__ void __launch_bounds__(256) bs_massive_extrap_kernel(BsArgs A) {
+    const int N = A.f.nsplit, tid = threadIdx.x, nt = blockDim.x;
+    const int L = bs_levels(VARIANT);
+    double* D = A.draw;
+    __shared__ double wmax[8];
+    __shared__ int wbad[8];
     for (int n = 1; n <= L; ++n) {
-        DeviceStatus* st = &A.lvst[n];
-        const double h = level_h<VARIANT>(A.h0, n);
         const double h2n = level_h2<VARIANT>(A.h0, n);
-        if (VARIANT == 1) {
-            const double hx2 = h * 2.0;
-            for (int k = 1 + tid; k < N; k += nt)
-                for (int c = 0; c < 3; ++c) {
-                    const int z = c * N + k;
-                    S.X[z] = X0[z] + h * V0[z];
-                    S.V[z] = V0[z] + h * S.A0[z];
-                }
-            call(S.X, S.V, S.A, A.table + (size_t)(row++) * stride, st);
-            for (int k = 1 + tid; k < N; k += nt)
-                for (int c = 0; c < 3; ++c) {
-                    const int z = c * N + k;
-                    S.XE[z] = X0[z] + hx2 * S.V[z];
-                    S.VE[z] = V0[z] + hx2 * S.A[z];
-                }
-            for (int j = 2; j <= n; ++j) {
-                call(S.XE, S.VE, S.A, A.table + (size_t)(row++) * stride, st);
-                for (int k = 1 + tid; k < N; k += nt)
-                    for (int c = 0; c < 3; ++c) {
-                        const int z = c * N + k;
-                        S.X[z] = S.X[z] + hx2 * S.VE[z];
-                        S.V[z] = S.V[z] + hx2 * S.A[z];
-                    }
-                call(S.X, S.V, S.A, A.table + (size_t)(row++) * stride, st);
-                for (int k = 1 + tid; k < N; k += nt)
-                    for (int c = 0; c < 3; ++c) {
-                        const int z = c * N + k;
-                        S.XE[z] = S.XE[z] + hx2 * S.V[z];
-                        S.VE[z] = S.VE[z] + hx2 * S.A[z];
-                    }
-            }
-            call(S.XE, S.VE, S.A, A.table + (size_t)(row++) * stride, st);
-            double* Dn = S.D + (size_t)(n - 1) * 6 * N;
-            for (int k = 1 + tid; k < N; k += nt)
-                for (int c = 0; c < 3; ++c) {
-                    const int z = c * N + k;
-                    Dn[z] = 0.5 * (S.XE[z] + S.X[z] + h * S.VE[z]);
-                    Dn[3 * N + z] = 0.5 * (S.VE[z] + S.V[z] + h * S.A[z]);
-                }
-        } else {
-            const double hby2 = 0.5 * h, h2by2 = 0.5 * h2n;
-            for (int k = 1 + tid; k < N; k += nt)
-                for (int c = 0; c < 3; ++c) {
-                    const int z = c * N + k;
-                    S.B[z] = 0.5 * S.A0[z];
-                    S.C[z] = 0.0;
-                    S.XE[z] = h2by2 * S.A0[z] + h * V0[z] + X0[z];
-                }
-            for (int j = 2; j <= n; ++j) {
-                call(S.XE, V0, S.A, A.table + (size_t)(row++) * stride, st);
-                const double tmp0 = h * double(j);
-                for (int k = 1 + tid; k < N; k += nt)
-                    for (int c = 0; c < 3; ++c) {
-                        const int z = c * N + k;
-                        S.B[z] = S.B[z] + S.A[z];
-                        S.C[z] = S.C[z] + S.B[z];
-                        S.XE[z] = h2n * S.C[z] + h2by2 * S.A0[z] + tmp0 * V0[z] + X0[z];
-                    }
-            }
-            call(S.XE, V0, S.A, A.table + (size_t)(row++) * stride, st);
-            double* Dn = S.D + (size_t)(n - 1) * 6 * N;
-            for (int k = 1 + tid; k < N; k += nt)
-                for (int c = 0; c < 3; ++c) {
-                    const int z = c * N + k;
-                    Dn[z] = S.XE[z];
-                    Dn[3 * N + z] = h * S.B[z] + hby2 * S.A[z] + V0[z];
-                }
-        }
-        // Neville update (mercury6_2.for:3352-3366), each thread its own bodies
         for (int j = n - 1; j >= 1; --j) {
             const double tmp0 = 1.0 / (level_h2<VARIANT>(A.h0, j) - h2n);
             const double tmp1 = tmp0 * level_h2<VARIANT>(A.h0, j + 1);
             const double tmp2 = tmp0 * h2n;
-            double* Dj = S.D + (size_t)(j - 1) * 6 * N;
-            const double* Dj1 = S.D + (size_t)j * 6 * N;
+            double* Dj = D + (size_t)(j - 1) * 6 * N;
+            const double* Dj1 = D + (size_t)j * 6 * N;
             for (int k = 1 + tid; k < N; k += nt)
                 for (int c = 0; c < 6; ++c) Dj[c * N + k] = tmp1 * Dj1[c * N + k] - tmp2 * Dj[c * N + k];
         }
@@ -346,14 +342,20 @@ template <int VARIANT, bool STAGED> __global__ void __launch_bounds__(256) bs_ma
             int bad = 0;
             double* cand = A.bcand + (size_t)(n - 4) * 6 * N;
             for (int k = 1 + tid; k < N; k += nt) {
+                const double* X0 = A.bx;
+                const double* V0 = A.bx + 3 * N;
+                const double tmp1 = X0[k] * X0[k] + X0[N + k] * X0[N + k] + X0[2 * N + k] * X0[2 * N + k];
+                const double tmp2 = V0[k] * V0[k] + V0[N + k] * V0[N + k] + V0[2 * N + k] * V0[2 * N + k];
+                const double xscal = 1.0 / fmax(tmp1, 1e-300);
+                const double vscal = 1.0 / fmax(tmp2, 1e-300);
                 double q[6];
-                for (int c = 0; c < 6; ++c) q[c] = S.D[c * N + k];
+                for (int c = 0; c < 6; ++c) q[c] = D[c * N + k];
                 double e;
-                if (body_error(q, S.XS[k], S.VS[k], e)) emax = fmax(emax, e);
+                if (body_error(q, xscal, vscal, e)) emax = fmax(emax, e);
                 else bad = 1;
                 for (int c = 0; c < 6; ++c) {
                     double s = q[c];
-                    for (int j = 2; j <= n; ++j) s = s + S.D[(size_t)(j - 1) * 6 * N + c * N + k];
+                    for (int j = 2; j <= n; ++j) s = s + D[(size_t)(j - 1) * 6 * N + c * N + k];
                     cand[c * N + k] = s;
                 }
             }
@@ -375,17 +377,22 @@ template <int VARIANT, bool STAGED> __global__ void __launch_bounds__(256) bs_ma
 }
 
 // ------------------------------------------------------------ particles
-// Each thread advances one particle slot through every level; its
-// extrapolation table lives in shared-memory columns D(j, c).
-template <int VARIANT> __global__ void __launch_bounds__(128) bs_particle_kernel(BsArgs A) {
-    extern __shared__ double dcol[];
-    const int L = bs_levels(VARIANT), nb = A.f.nbig - 1, stride = force_row(nb), S = A.npcap;
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+// Thirty-two particle slots per CTA, one lane each; warp w computes the raw
+// states D(n) of levels w + 1 and L - w (n + (L + 1 - n) force calls per warp,
+// balanced) into shared memory, from the start-of-step force that warp 0
+// computes. Warp 0 then runs the Neville updates in level order, each level's
+// error maximum and candidate state: per particle the same statements, in the
+// same order, as a level loop would run them.
+template <int VARIANT> __global__ void __launch_bounds__(bs_levels(VARIANT) * 16) bs_particle_kernel(BsArgs A) {
+    constexpr int L = bs_levels(VARIANT);
+    __shared__ double dsm[L][6][32];
+    __shared__ double a0sm[3][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int p = blockIdx.x * 32 + lane;
     const bool ok = p < A.np;
-    const int T = blockDim.x;
-    auto D = [&](int j, int c) -> double& { return dcol[((j - 1) * 6 + c) * T + threadIdx.x]; };
-    double3 x0 = make_double3(0.0, 0.0, 0.0), v0 = x0, a0 = x0;
-    double xscal = 0.0, vscal = 0.0, mj = 0.0, g5[5] = {0, 0, 0, 0, 0};
+    const int nb = A.f.nbig - 1, stride = force_row(nb), S = A.npcap;
+    double3 x0 = make_double3(0.0, 0.0, 0.0), v0 = x0;
+    double mj = 0.0, g5[5] = {0, 0, 0, 0, 0};
     // the encounter subsystem (BS2 only): mfo_hkce from the member's pairs
     const bool hkce = VARIANT == 2 && A.hkce;
     int g = 0;
@@ -398,19 +405,24 @@ template <int VARIANT> __global__ void __launch_bounds__(128) bs_particle_kernel
         v0 = make_double3(A.px[3 * S + p], A.px[4 * S + p], A.px[5 * S + p]);
         mj = A.pconst[p];
         for (int c = 0; c < 5; ++c) g5[c] = A.pconst[(3 + c) * (size_t)S + p];
-        const double tmp1 = x0.x * x0.x + x0.y * x0.y + x0.z * x0.z;
-        const double tmp2 = v0.x * v0.x + v0.y * v0.y + v0.z * v0.z;
-        xscal = 1.0 / fmax(tmp1, 1e-300);
-        vscal = 1.0 / fmax(tmp2, 1e-300);
         if (hkce) {
             g = A.f.nsplit + A.perm[p];
             rcrit_p = A.pconst[(size_t)PC_RCRIT * S + p];
         }
-        a0 = force(x0, v0, A.table, &A.lvst[0]);
+        if (w == 0) {
+            const double3 a = force(x0, v0, A.table, &A.lvst[0]);
+            a0sm[0][lane] = a.x;
+            a0sm[1][lane] = a.y;
+            a0sm[2][lane] = a.z;
+        }
     }
-    int row = 1;
+    __syncthreads();
+    const double3 a0 = ok ? make_double3(a0sm[0][lane], a0sm[1][lane], a0sm[2][lane]) : make_double3(0.0, 0.0, 0.0);
 #pragma unroll 1
-    for (int n = 1; n <= L; ++n) {
+    for (int half = 0; half < 2 && ok; ++half) {
+        const int n = half == 0 ? w + 1 : L - w;
+        int row = 1;
+        for (int m = 1; m < n; ++m) row += bs_level_forces(VARIANT, m);
         DeviceStatus* st = &A.lvst[n];
         const double h = level_h<VARIANT>(A.h0, n);
         const double h2n = level_h2<VARIANT>(A.h0, n);
@@ -418,54 +430,69 @@ template <int VARIANT> __global__ void __launch_bounds__(128) bs_particle_kernel
             const double* Tr = A.table + (size_t)(row++) * stride;
             return force(x, v, Tr, st);
         };
-        if (ok) {
-            if (VARIANT == 1) {
-                const double hx2 = h * 2.0;
-                double3 x = make_double3(x0.x + h * v0.x, x0.y + h * v0.y, x0.z + h * v0.z);
-                double3 v = make_double3(v0.x + h * a0.x, v0.y + h * a0.y, v0.z + h * a0.z);
-                double3 a = call(x, v);
-                double3 xe = make_double3(x0.x + hx2 * v.x, x0.y + hx2 * v.y, x0.z + hx2 * v.z);
-                double3 ve = make_double3(v0.x + hx2 * a.x, v0.y + hx2 * a.y, v0.z + hx2 * a.z);
+        auto D = [&](int c) -> double& { return dsm[n - 1][c][lane]; };
+        if (VARIANT == 1) {
+            const double hx2 = h * 2.0;
+            double3 x = make_double3(x0.x + h * v0.x, x0.y + h * v0.y, x0.z + h * v0.z);
+            double3 v = make_double3(v0.x + h * a0.x, v0.y + h * a0.y, v0.z + h * a0.z);
+            double3 a = call(x, v);
+            double3 xe = make_double3(x0.x + hx2 * v.x, x0.y + hx2 * v.y, x0.z + hx2 * v.z);
+            double3 ve = make_double3(v0.x + hx2 * a.x, v0.y + hx2 * a.y, v0.z + hx2 * a.z);
 #pragma unroll 1
-                for (int j = 2; j <= n; ++j) {
-                    a = call(xe, ve);
-                    x = make_double3(x.x + hx2 * ve.x, x.y + hx2 * ve.y, x.z + hx2 * ve.z);
-                    v = make_double3(v.x + hx2 * a.x, v.y + hx2 * a.y, v.z + hx2 * a.z);
-                    a = call(x, v);
-                    xe = make_double3(xe.x + hx2 * v.x, xe.y + hx2 * v.y, xe.z + hx2 * v.z);
-                    ve = make_double3(ve.x + hx2 * a.x, ve.y + hx2 * a.y, ve.z + hx2 * a.z);
-                }
+            for (int j = 2; j <= n; ++j) {
                 a = call(xe, ve);
-                D(n, 0) = 0.5 * (xe.x + x.x + h * ve.x);
-                D(n, 1) = 0.5 * (xe.y + x.y + h * ve.y);
-                D(n, 2) = 0.5 * (xe.z + x.z + h * ve.z);
-                D(n, 3) = 0.5 * (ve.x + v.x + h * a.x);
-                D(n, 4) = 0.5 * (ve.y + v.y + h * a.y);
-                D(n, 5) = 0.5 * (ve.z + v.z + h * a.z);
-            } else {
-                const double hby2 = 0.5 * h, h2by2 = 0.5 * h2n;
-                double3 b = make_double3(0.5 * a0.x, 0.5 * a0.y, 0.5 * a0.z);
-                double3 c = make_double3(0.0, 0.0, 0.0);
-                double3 xe = make_double3(h2by2 * a0.x + h * v0.x + x0.x, h2by2 * a0.y + h * v0.y + x0.y,
-                                          h2by2 * a0.z + h * v0.z + x0.z);
-#pragma unroll 1
-                for (int j = 2; j <= n; ++j) {
-                    const double3 a = call(xe, v0);
-                    const double tmp0 = h * double(j);
-                    b = make_double3(b.x + a.x, b.y + a.y, b.z + a.z);
-                    c = make_double3(c.x + b.x, c.y + b.y, c.z + b.z);
-                    xe = make_double3(h2n * c.x + h2by2 * a0.x + tmp0 * v0.x + x0.x,
-                                      h2n * c.y + h2by2 * a0.y + tmp0 * v0.y + x0.y,
-                                      h2n * c.z + h2by2 * a0.z + tmp0 * v0.z + x0.z);
-                }
-                const double3 a = call(xe, v0);
-                D(n, 0) = xe.x;
-                D(n, 1) = xe.y;
-                D(n, 2) = xe.z;
-                D(n, 3) = h * b.x + hby2 * a.x + v0.x;
-                D(n, 4) = h * b.y + hby2 * a.y + v0.y;
-                D(n, 5) = h * b.z + hby2 * a.z + v0.z;
+                x = make_double3(x.x + hx2 * ve.x, x.y + hx2 * ve.y, x.z + hx2 * ve.z);
+                v = make_double3(v.x + hx2 * a.x, v.y + hx2 * a.y, v.z + hx2 * a.z);
+                a = call(x, v);
+                xe = make_double3(xe.x + hx2 * v.x, xe.y + hx2 * v.y, xe.z + hx2 * v.z);
+                ve = make_double3(ve.x + hx2 * a.x, ve.y + hx2 * a.y, ve.z + hx2 * a.z);
             }
+            a = call(xe, ve);
+            D(0) = 0.5 * (xe.x + x.x + h * ve.x);
+            D(1) = 0.5 * (xe.y + x.y + h * ve.y);
+            D(2) = 0.5 * (xe.z + x.z + h * ve.z);
+            D(3) = 0.5 * (ve.x + v.x + h * a.x);
+            D(4) = 0.5 * (ve.y + v.y + h * a.y);
+            D(5) = 0.5 * (ve.z + v.z + h * a.z);
+        } else {
+            const double hby2 = 0.5 * h, h2by2 = 0.5 * h2n;
+            double3 b = make_double3(0.5 * a0.x, 0.5 * a0.y, 0.5 * a0.z);
+            double3 c = make_double3(0.0, 0.0, 0.0);
+            double3 xe = make_double3(h2by2 * a0.x + h * v0.x + x0.x, h2by2 * a0.y + h * v0.y + x0.y,
+                                      h2by2 * a0.z + h * v0.z + x0.z);
+#pragma unroll 1
+            for (int j = 2; j <= n; ++j) {
+                const double3 a = call(xe, v0);
+                const double tmp0 = h * double(j);
+                b = make_double3(b.x + a.x, b.y + a.y, b.z + a.z);
+                c = make_double3(c.x + b.x, c.y + b.y, c.z + b.z);
+                xe = make_double3(h2n * c.x + h2by2 * a0.x + tmp0 * v0.x + x0.x,
+                                  h2n * c.y + h2by2 * a0.y + tmp0 * v0.y + x0.y,
+                                  h2n * c.z + h2by2 * a0.z + tmp0 * v0.z + x0.z);
+            }
+            const double3 a = call(xe, v0);
+            D(0) = xe.x;
+            D(1) = xe.y;
+            D(2) = xe.z;
+            D(3) = h * b.x + hby2 * a.x + v0.x;
+            D(4) = h * b.y + hby2 * a.y + v0.y;
+            D(5) = h * b.z + hby2 * a.z + v0.z;
+        }
+    }
+    __syncthreads();
+    if (w != 0) return;
+    double xscal = 0.0, vscal = 0.0;
+    if (ok) {
+        const double tmp1 = x0.x * x0.x + x0.y * x0.y + x0.z * x0.z;
+        const double tmp2 = v0.x * v0.x + v0.y * v0.y + v0.z * v0.z;
+        xscal = 1.0 / fmax(tmp1, 1e-300);
+        vscal = 1.0 / fmax(tmp2, 1e-300);
+    }
+    auto D = [&](int j, int c) -> double& { return dsm[j - 1][c][lane]; };
+#pragma unroll 1
+    for (int n = 1; n <= L; ++n) {
+        if (ok) {
+            const double h2n = level_h2<VARIANT>(A.h0, n);
 #pragma unroll 1
             for (int j = n - 1; j >= 1; --j) {
                 const double tmp0 = 1.0 / (level_h2<VARIANT>(A.h0, j) - h2n);
@@ -473,8 +500,6 @@ template <int VARIANT> __global__ void __launch_bounds__(128) bs_particle_kernel
                 const double tmp2 = tmp0 * h2n;
                 for (int c = 0; c < 6; ++c) D(j, c) = tmp1 * D(j + 1, c) - tmp2 * D(j, c);
             }
-        } else {
-            row += bs_level_forces(VARIANT, n);
         }
         if (n > 3) {
             double emax = 0.0;
@@ -496,7 +521,7 @@ template <int VARIANT> __global__ void __launch_bounds__(128) bs_particle_kernel
                 emax = fmax(emax, __shfl_xor_sync(FULLMASK, emax, o));
                 bad |= __shfl_xor_sync(FULLMASK, bad, o);
             }
-            if ((threadIdx.x & 31) == 0 && (emax > 0.0 || bad)) level_error(emax, !bad, &A.errs[n]);
+            if (lane == 0 && (emax > 0.0 || bad)) level_error(emax, !bad, &A.errs[n]);
         }
     }
 }
@@ -599,22 +624,14 @@ __global__ void __launch_bounds__(128) bs_commit_kernel(BsCommitArgs A) {
 
 template <int VARIANT> void launch_variant(const BsArgs& a, cudaStream_t s) {
     const int N = a.f.nsplit;
-    const size_t msmem = sizeof(double) * ((size_t)bs_massive_scratch(VARIANT) + 12) * N;
-    if (msmem <= 200 * 1024) {
-        if (msmem > 48 * 1024)
-            cudaFuncSetAttribute(bs_massive_kernel<VARIANT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)msmem);
-        const int threads = std::min(256, std::max(32, (N + 31) / 32 * 32));
-        bs_massive_kernel<VARIANT, true><<<1, threads, msmem, s>>>(a);
-    } else {
-        bs_massive_kernel<VARIANT, false><<<1, 256, 0, s>>>(a);
-    }
+    const size_t msmem = sizeof(double) * ((size_t)BS_LEVEL_ROWS + 12) * N;
+    if (msmem > 48 * 1024)
+        cudaFuncSetAttribute(bs_massive_level_kernel<VARIANT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msmem);
+    const int mthreads = std::min(256, std::max(32, (N + 31) / 32 * 32));
+    bs_massive_level_kernel<VARIANT><<<bs_levels(VARIANT), mthreads, msmem, s>>>(a);
+    bs_massive_extrap_kernel<VARIANT><<<1, mthreads, 0, s>>>(a);
     if (a.np <= 0) return;
-    const int threads = 128;
-    const size_t smem = sizeof(double) * 6 * bs_levels(VARIANT) * threads;
-    if (smem > 48 * 1024)
-        cudaFuncSetAttribute(bs_particle_kernel<VARIANT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    bs_particle_kernel<VARIANT><<<(a.np + threads - 1) / threads, threads, smem, s>>>(a);
+    bs_particle_kernel<VARIANT><<<(a.np + 31) / 32, bs_levels(VARIANT) * 16, 0, s>>>(a);
 }
 
 }  // namespace

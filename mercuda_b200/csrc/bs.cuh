@@ -22,9 +22,15 @@ __host__ __device__ constexpr int bs_level_forces(int variant, int n) { return v
 __host__ __device__ constexpr int bs_rows(int variant) { return variant == 1 ? 1 + 72 : 1 + 78; }
 // Candidate states kept per body: levels 4 .. bs_levels.
 __host__ __device__ constexpr int bs_candidates(int variant) { return bs_levels(variant) - 3; }
-// Massive-set scratch rows ([rows][nsplit] doubles): eight 3-vectors, the two
-// error scales and the extrapolation table.
-__host__ __device__ constexpr int bs_massive_scratch(int variant) { return 26 + 6 * bs_levels(variant); }
+// Shared-memory rows ([rows][nsplit] doubles) of one level CTA of the massive
+// set: eight 3-vectors (states, accelerations, B, C); then 12 more for the
+// starting state, masses and non-gravitational constants.
+constexpr int BS_LEVEL_ROWS = 24;
+// Global scratch of the massive set: the raw level states D(n) [levels][6][nsplit],
+// then the private start-of-step table rows of levels 2.. [levels - 1][force_row(nb)].
+__host__ __device__ constexpr size_t bs_massive_scratch(int variant, int nsplit, int nb) {
+    return (size_t)bs_levels(variant) * 6 * nsplit + (size_t)(bs_levels(variant) - 1) * force_row(nb);
+}
 
 struct BsArgs {
     ForceCfg f;
@@ -34,7 +40,8 @@ struct BsArgs {
     const double* bx;            // [9][nsplit] start-of-step state of the massive set
     const double* mbig;
     const double* ngfbig;        // [nsplit][5]
-    double* bscr;                // [bs_massive_scratch][nsplit]
+    double* draw;                // [levels][6][nsplit] raw level states of the massive set
+    double* tscr;                // [levels - 1][force_row(nb)] private start-of-step rows
     const double* px;            // [9][npcap] start-of-step particle state
     const double* pconst;        // [PCONST_ROWS][npcap]
     double* table;               // [bs_rows][force_row(nb)]
