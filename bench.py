@@ -638,8 +638,11 @@ def run_hybrid_adjoint(args, rank, world, dist):
                           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
               flush=True)
         return
+    import ctypes
+
     import torch
     from mercuda_b200.adjoint import hybrid_timing, hybrid_trajectory
+    from mercuda_b200.backend import load_library
 
     sysw = make(args.seed, args.particles, rank)
     nb = sysw.nbig
@@ -655,13 +658,26 @@ def run_hybrid_adjoint(args, rank, world, dist):
         return x0.grad.cpu().numpy()
 
     ranks = Ranks(dist, device="cuda")
+    lib = load_library()
+
+    def dropin(reset):
+        """Kernels the drop-in calls launched since the last reset."""
+        launched = ctypes.c_int64(0)
+        lib.mercury_b200_dropin_time(None, ctypes.byref(launched), int(reset))
+        return launched.value
+
     for _ in range(max(1, args.warmup)):
         once()
     ranks.barrier()
+    dropin(True)
     with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clocks:
         t0 = time.perf_counter()
         gx = once()
         e2e_s = time.perf_counter() - t0
+    # forward: the drop-in HYBRID calls' kernels; backward: per segment the
+    # recompute and VJP kernels and, where members were recorded, their index
+    nseg = (args.steps + args.checkpoint_every - 1) // args.checkpoint_every
+    launches = dropin(True) + 3 * nseg
     fwd, bwd, members = hybrid_timing()
     ms = fwd + bwd
     ms, e2e_s = ranks.max(ms), ranks.max(e2e_s)
@@ -681,7 +697,7 @@ def run_hybrid_adjoint(args, rank, world, dist):
                                      "forward_wall_ms": fwd, "backward_ms": bwd, "backward_over_forward": bwd / fwd,
                                      "member_steps": members, "checkpoint_every": args.checkpoint_every,
                                      "grad_finite": bool(np.all(np.isfinite(gx)))},
-                          "clocks": clocks.summary(),
+                          "clocks": clocks.summary(), "gpu_launches": launches,
                           "e2e": {"value": world * args.particles * args.steps / e2e_s, "unit": UNIT,
                                   "h2d_bytes_per_step": args.particles * 7 * 8 / args.steps,
                                   "d2h_bytes_per_step": args.particles * 3 * 8 / args.steps,

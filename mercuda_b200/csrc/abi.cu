@@ -443,7 +443,7 @@ void bs_step_once(double time, double* h, double* hdid, double tol, int64_t* rej
         a.adj = c.adj.p;
         a.perm = c.permp();
         launch_bs_sequence(a, c.stream);
-        c.dropin_launches += 1 + (c.np > 0 ? 1 : 0);
+        c.dropin_launches += 2 + (c.np > 0 ? 1 : 0);  // level CTAs, extrapolation, particles
         check(cudaGetLastError(), "launch");
         unsigned long long errs[13];
         DeviceStatus lv[13];
@@ -924,20 +924,50 @@ int reorder_slots(int src, double h, cudaStream_t st) {
     return 1 - src;
 }
 
-void sort_events(std::vector<MercuryEvent>& ev, std::vector<int>* steps) {
-    std::vector<size_t> idx(ev.size());
-    for (size_t k = 0; k < idx.size(); ++k) idx[k] = k;
-    auto key = [&](size_t k) {
-        const MercuryEvent& e = ev[k];
-        const int s = steps ? (*steps)[k] : 0;
-        return std::make_tuple(s, std::min(e.i, e.j), std::max(e.i, e.j));
+// The order of records ev by (step, min(i,j), max(i,j)), ties in record
+// order: a counting sort of (pair key, record) by step, then each step's
+// short run by (key, record). steps == null: all in one step.
+void order_events(const std::vector<MercuryEvent>& ev, const std::vector<int>* steps, std::vector<uint32_t>& order) {
+    const size_t n = ev.size();
+    order.resize(n);
+    if (n == 0) return;
+    struct Item {
+        uint64_t key;
+        uint32_t k;
     };
-    std::stable_sort(idx.begin(), idx.end(), [&](size_t a, size_t b) { return key(a) < key(b); });
+    std::vector<size_t> first(2, 0);
+    if (steps) {
+        int smax = 0;
+        for (size_t k = 0; k < n; ++k) smax = std::max(smax, (*steps)[k]);
+        first.assign((size_t)smax + 2, 0);
+        for (size_t k = 0; k < n; ++k) ++first[(size_t)(*steps)[k] + 1];
+        for (size_t s = 1; s < first.size(); ++s) first[s] += first[s - 1];
+    } else {
+        first[1] = n;
+    }
+    std::vector<Item> items(n);
+    {
+        std::vector<size_t> fill(first.begin(), first.end() - 1);
+        for (size_t k = 0; k < n; ++k) {
+            const MercuryEvent& e = ev[k];
+            const uint64_t key = ((uint64_t)(uint32_t)std::min(e.i, e.j) << 32) | (uint32_t)std::max(e.i, e.j);
+            items[fill[steps ? (size_t)(*steps)[k] : 0]++] = Item{key, (uint32_t)k};
+        }
+    }
+    for (size_t s = 0; s + 1 < first.size(); ++s)
+        std::sort(items.begin() + first[s], items.begin() + first[s + 1],
+                  [](const Item& a, const Item& b) { return a.key < b.key || (a.key == b.key && a.k < b.k); });
+    for (size_t q = 0; q < n; ++q) order[q] = items[q].k;
+}
+
+void sort_events(std::vector<MercuryEvent>& ev, std::vector<int>* steps) {
+    std::vector<uint32_t> order;
+    order_events(ev, steps, order);
     std::vector<MercuryEvent> out(ev.size());
-    std::vector<int> so(ev.size());
-    for (size_t k = 0; k < idx.size(); ++k) {
-        out[k] = ev[idx[k]];
-        if (steps) so[k] = (*steps)[idx[k]];
+    std::vector<int> so(steps ? ev.size() : 0);
+    for (size_t q = 0; q < order.size(); ++q) {
+        out[q] = ev[order[q]];
+        if (steps) so[q] = (*steps)[order[q]];
     }
     ev.swap(out);
     if (steps) steps->swap(so);
@@ -1210,6 +1240,7 @@ int mercury_cuda_events(double time, double h, double rcen, const MercuryEvent**
             else e.time = e.time + time;
         }
         sort_events(c.host_events, nullptr);
+        c.event_order.clear();
         *count = nev;
         *result = c.host_events.data();
         return 0;
@@ -1619,7 +1650,9 @@ int mercury_b200_mvs_advance(double time, double h, int nsteps, double rcen, int
             if (e.kind == EV_CENTRAL) e.time = te - h + e.time;
             else e.time = e.time + te;
         }
-        sort_events(c.host_events, &c.host_steps);
+        // records stay in arrival order; mercury_b200_events gathers them in
+        // (step, min(i,j), max(i,j)) order straight into the caller's arrays
+        order_events(c.host_events, &c.host_steps, c.event_order);
         *nevents = nev;
         return 0;
     } catch (const std::exception& e) {
@@ -1630,9 +1663,13 @@ int mercury_b200_mvs_advance(double time, double h, int nsteps, double rcen, int
 int mercury_b200_events(MercuryEvent* dst, int* steps, int cap) {
     Context& c = ctx();
     const int nev = (int)c.host_events.size();
-    const int k = std::min(cap, nev);
-    if (k > 0) std::memcpy(dst, c.host_events.data(), sizeof(MercuryEvent) * k);
-    if (steps && k > 0 && (int)c.host_steps.size() >= k) std::memcpy(steps, c.host_steps.data(), sizeof(int) * k);
+    const int k = std::max(0, std::min(cap, nev));
+    const bool ordered = c.event_order.size() == c.host_events.size();
+    for (int q = 0; q < k; ++q) {
+        const size_t r = ordered ? c.event_order[q] : (size_t)q;
+        dst[q] = c.host_events[r];
+        if (steps && r < c.host_steps.size()) steps[q] = c.host_steps[r];
+    }
     return nev;
 }
 

@@ -123,6 +123,7 @@ struct Context {
     DeviceStatus* status_host = nullptr;
     std::vector<MercuryEvent> host_events;
     std::vector<int> host_steps;
+    std::vector<uint32_t> event_order;   // last advance: host_events in (step, min, max) order
     int pair_events = 0;
     // staging
     DBuf<double> transfer;
@@ -194,6 +195,7 @@ struct Context {
         status.release();
         host_events.clear();
         host_steps.clear();
+        event_order.clear();
         n = nbig = np = npcap = 0;
         stepped = false;
         reset = true;
