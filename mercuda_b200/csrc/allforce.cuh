@@ -179,4 +179,117 @@ static __device__ void row_head(const double* X, const double* m, const ForceCfg
     T[6] = 0.0; T[7] = 0.0;
 }
 
+// ---- The massive set's mfo_all by a whole CTA. For sets of up to
+// MASSIVE_PAR_MAX bodies the CTA first computes, one term per thread, every
+// product the sequential loops above accumulate (massive_terms), so that the
+// head (row_head_terms) and each body's acceleration (massive_allforce_terms)
+// only add them up in mfo_grav's order: the same roundings in the same order,
+// with the sqrt/divide chains of all pairs in flight at once.
+constexpr int MASSIVE_PAR_MAX = 32;
+// Shared-memory doubles the terms need: body k's q-th direct term at
+// [(k * N + q) * 3], then body i's indirect and oblateness-reaction terms at
+// [N * N * 3 + i * 6].
+__host__ __device__ constexpr int massive_par_scratch(int N) { return N <= MASSIVE_PAR_MAX ? N * N * 3 + N * 6 : 0; }
+
+// Number of body k's direct terms that come from earlier Big bodies (they are
+// subtracted); later bodies' terms follow (they are added).
+__device__ __forceinline__ int massive_earlier(int k, const ForceCfg& f) { return (k < f.nbig ? k : f.nbig) - 1; }
+
+static __device__ void massive_terms(const double* X, const double* m, const ForceCfg& f, double* PT, DeviceStatus* st) {
+    const int N = f.nsplit;
+    for (int q = threadIdx.x; q < N * N; q += blockDim.x) {
+        const int k = q / N, o = q - k * N;
+        if (k < 1 || o < 1 || o == k) continue;
+        const int ne = massive_earlier(k, f);
+        int slot;
+        double dx, dy, dz;
+        if (o <= ne) {  // earlier Big body o: k is its "j"
+            slot = o - 1;
+            dx = X[k] - X[o]; dy = X[N + k] - X[N + o]; dz = X[2 * N + k] - X[2 * N + o];
+        } else if (k < f.nbig && o > k) {  // later body o: k is its Big "i"
+            slot = ne + (o - k - 1);
+            dx = X[o] - X[k]; dy = X[N + o] - X[N + k]; dz = X[2 * N + o] - X[2 * N + k];
+        } else {
+            continue;
+        }
+        const double s2 = dx * dx + dy * dy + dz * dz;
+        if (s2 <= 0.0) raise_fault(st, FAULT_COINCIDENT);
+        const double s_1 = 1.0 / sqrt(s2);
+        const double s_3 = s_1 * s_1 * s_1;
+        const double t = s_3 * m[o];
+        double* out = PT + ((size_t)k * N + slot) * 3;
+        out[0] = t * dx;
+        out[1] = t * dy;
+        out[2] = t * dz;
+    }
+    double* HT = PT + (size_t)N * N * 3;
+    for (int i = 1 + threadIdx.x; i < N; i += blockDim.x) {
+        const double3 p = make_double3(X[i], X[N + i], X[2 * N + i]);
+        const double s2 = p.x * p.x + p.y * p.y + p.z * p.z;
+        const double s_1 = 1.0 / sqrt(s2);
+        const double r3 = s_1 * s_1 * s_1;
+        const double tmp1 = m[i] * r3;
+        double* out = HT + (size_t)i * 6;
+        out[0] = tmp1 * p.x;
+        out[1] = tmp1 * p.y;
+        out[2] = tmp1 * p.z;
+        if (f.obl) {
+            const double3 ao = oblate_accel(p, f.jcen, f.m0);
+            const double tmp4 = m[i] / f.m0;
+            out[3] = tmp4 * ao.x;
+            out[4] = tmp4 * ao.y;
+            out[5] = tmp4 * ao.z;
+        }
+    }
+}
+
+// row_head from the terms (one thread).
+static __device__ void row_head_terms(const double* PT, const ForceCfg& f, double* T) {
+    const int N = f.nsplit;
+    const double* HT = PT + (size_t)N * N * 3;
+    double sx = 0.0, sy = 0.0, sz = 0.0, ax = 0.0, ay = 0.0, az = 0.0;
+    for (int i = 1; i < N; ++i) {
+        const double* t = HT + (size_t)i * 6;
+        sx = sx - t[0];
+        sy = sy - t[1];
+        sz = sz - t[2];
+        if (f.obl) {
+            ax = ax - t[3];
+            ay = ay - t[4];
+            az = az - t[5];
+        }
+    }
+    T[0] = sx; T[1] = sy; T[2] = sz;
+    T[3] = ax; T[4] = ay; T[5] = az;
+    T[6] = 0.0; T[7] = 0.0;
+}
+
+// massive_allforce from the terms.
+__device__ __forceinline__ double3 massive_allforce_terms(int k, const double* X, const double* V, const double* m,
+                                                          const double* ngfbig, const double* T, const ForceCfg& f,
+                                                          const double* PT, DeviceStatus* st) {
+    const int N = f.nsplit;
+    const double3 x = make_double3(X[k], X[N + k], X[2 * N + k]);
+    const double3 v = make_double3(V[k], V[N + k], V[2 * N + k]);
+    const double s2c = x.x * x.x + x.y * x.y + x.z * x.z;
+    if (s2c <= 0.0) raise_fault(st, FAULT_COINCIDENT);
+    const double ri = 1.0 / sqrt(s2c);
+    const double r3 = ri * ri * ri;
+    double3 a = make_double3(0.0, 0.0, 0.0);
+    const int ne = massive_earlier(k, f);
+    const int nl = k < f.nbig ? N - k - 1 : 0;
+    const double* t = PT + (size_t)k * N * 3;
+    for (int q = 0; q < ne; ++q, t += 3) {
+        a.x = a.x - t[0];
+        a.y = a.y - t[1];
+        a.z = a.z - t[2];
+    }
+    for (int q = 0; q < nl; ++q, t += 3) {
+        a.x = a.x + t[0];
+        a.y = a.y + t[1];
+        a.z = a.z + t[2];
+    }
+    return finish_force(a, x, v, ri, r3, T, f, m[k], ngfbig + 5 * k, st);
+}
+
 }  // namespace mb200

@@ -165,11 +165,12 @@ __device__ double3 hkce_particle_force_jvp(const BsArgs& A, int g, const double3
 }
 
 // ------------------------------------------------------------ massive set
-// One force call of the massive set into S.A (or A0) and table row T; mb
-// and ngf are the set's masses and non-gravitational constants, head a
-// shared copy of the row's head for the set's own forces.
+// One force call of the massive set into `out` and table row T; mb and ngf
+// are the set's masses and non-gravitational constants, head a shared copy of
+// the row's head for the set's own forces, PT shared scratch for the terms
+// computed in parallel (null: the sequential loops).
 __device__ void massive_call(const BsArgs& A, const double* X, const double* V, double* out, double* T,
-                             DeviceStatus* st, const double* mb, const double* ngf, double* head) {
+                             DeviceStatus* st, const double* mb, const double* ngf, double* head, double* PT) {
     const ForceCfg& f = A.f;
     const int N = f.nsplit;
     __syncthreads();
@@ -185,8 +186,13 @@ __device__ void massive_call(const BsArgs& A, const double* X, const double* V, 
         __syncthreads();
         return;
     }
+    if (PT) {
+        massive_terms(X, mb, f, PT, st);
+        __syncthreads();
+    }
     if (threadIdx.x == 0) {
-        row_head(X, mb, f, T);
+        if (PT) row_head_terms(PT, f, T);
+        else row_head(X, mb, f, T);
         for (int q = 0; q < FT_HEAD; ++q) head[q] = T[q];
     }
     __syncthreads();
@@ -196,7 +202,8 @@ __device__ void massive_call(const BsArgs& A, const double* X, const double* V, 
             row[0] = X[k]; row[1] = X[N + k]; row[2] = X[2 * N + k]; row[3] = mb[k];
         }
         if (k < 1) continue;
-        const double3 a = massive_allforce(k, X, V, mb, ngf, head, f, st);
+        const double3 a = PT ? massive_allforce_terms(k, X, V, mb, ngf, head, f, PT, st)
+                             : massive_allforce(k, X, V, mb, ngf, head, f, st);
         out[k] = a.x; out[N + k] = a.y; out[2 * N + k] = a.z;
     }
     __syncthreads();
@@ -232,10 +239,11 @@ template <int VARIANT> __global__ void __launch_bounds__(256) bs_massive_level_k
     const double* V0 = p + 3 * N;
     const double* mb = p + 6 * N;
     const double* ngf = p + 7 * N;
+    double* PT = massive_par_scratch(N) ? p + 12 * N : nullptr;
     __syncthreads();
     __shared__ double head[FT_HEAD];
     auto call = [&](const double* Xc, const double* Vc, double* out, double* T, DeviceStatus* st) {
-        massive_call(A, Xc, Vc, out, T, st, mb, ngf, head);
+        massive_call(A, Xc, Vc, out, T, st, mb, ngf, head, PT);
     };
     for (int k = tid; k < N; k += nt)
         for (int c = 0; c < 3; ++c) {
@@ -624,10 +632,12 @@ __global__ void __launch_bounds__(128) bs_commit_kernel(BsCommitArgs A) {
 
 template <int VARIANT> void launch_variant(const BsArgs& a, cudaStream_t s) {
     const int N = a.f.nsplit;
-    const size_t msmem = sizeof(double) * ((size_t)BS_LEVEL_ROWS + 12) * N;
+    const size_t msmem = sizeof(double) * (((size_t)BS_LEVEL_ROWS + 12) * N + massive_par_scratch(N));
     if (msmem > 48 * 1024)
         cudaFuncSetAttribute(bs_massive_level_kernel<VARIANT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msmem);
-    const int mthreads = std::min(256, std::max(32, (N + 31) / 32 * 32));
+    // one warp per 32 bodies, and with the parallel force terms enough for one term each
+    int mthreads = std::min(256, std::max(32, (N + 31) / 32 * 32));
+    if (massive_par_scratch(N)) mthreads = std::max(mthreads, std::min(256, (N * N + 31) / 32 * 32));
     bs_massive_level_kernel<VARIANT><<<bs_levels(VARIANT), mthreads, msmem, s>>>(a);
     bs_massive_extrap_kernel<VARIANT><<<1, mthreads, 0, s>>>(a);
     if (a.np <= 0) return;

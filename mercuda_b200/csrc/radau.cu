@@ -223,7 +223,7 @@ template <bool STAGED> __global__ void __launch_bounds__(256) ra15_massive_kerne
     const bool vpred = (f.ngflag != 0 || f.pn == 1);
     __shared__ double blockmax[8];
     __shared__ double head[FT_HEAD];
-    double *X, *V, *B, *G, *a1;
+    double *X, *V, *B, *G, *a1, *PT = nullptr;
     const double *x1, *v1, *mb, *ngf;
     if (STAGED) {
         X = sm;
@@ -235,6 +235,7 @@ template <bool STAGED> __global__ void __launch_bounds__(256) ra15_massive_kerne
         double* sv1 = sx1 + 3 * N;
         double* smb = sv1 + 3 * N;
         double* sngf = smb + N;
+        PT = massive_par_scratch(N) ? sngf + 5 * N : nullptr;
         for (int q = tid; q < 3 * N; q += nt) {
             sx1[q] = A.bx[q];
             sv1[q] = A.bx[3 * N + q];
@@ -260,11 +261,22 @@ template <bool STAGED> __global__ void __launch_bounds__(256) ra15_massive_kerne
     }
     // the head of a table row: written to the table for the particles and
     // kept in shared memory for the massive set's forces
+    // (with PT the force terms are computed by every thread first; the
+    // caller synchronizes before and after)
     auto write_head = [&](double* T) {
+        if (PT) {
+            massive_terms(X, mb, f, PT, A.status);
+            __syncthreads();
+        }
         if (tid == 0) {
-            row_head(X, mb, f, T);
+            if (PT) row_head_terms(PT, f, T);
+            else row_head(X, mb, f, T);
             for (int q = 0; q < FT_HEAD; ++q) head[q] = T[q];
         }
+    };
+    auto force = [&](int k, const double* Vc) {
+        return PT ? massive_allforce_terms(k, X, Vc, mb, ngf, head, f, PT, A.status)
+                  : massive_allforce(k, X, Vc, mb, ngf, head, f, A.status);
     };
     double localmax = 0.0;
     // sequence start: force at (x1, v1), G from B
@@ -282,7 +294,7 @@ template <bool STAGED> __global__ void __launch_bounds__(256) ra15_massive_kerne
             row[0] = X[k]; row[1] = X[N + k]; row[2] = X[2 * N + k]; row[3] = mb[k];
         }
         if (k < 1) continue;
-        const double3 a = massive_allforce(k, X, V, mb, ngf, head, f, A.status);
+        const double3 a = force(k, V);
         a1[k] = a.x; a1[N + k] = a.y; a1[2 * N + k] = a.z;
         for (int c = 0; c < 3; ++c) {
             double b[7], g[7];
@@ -317,7 +329,7 @@ template <bool STAGED> __global__ void __launch_bounds__(256) ra15_massive_kerne
                     row[0] = X[k]; row[1] = X[N + k]; row[2] = X[2 * N + k]; row[3] = mb[k];
                 }
                 if (k < 1) continue;
-                const double3 a = massive_allforce(k, X, vpred ? V : v1, mb, ngf, head, f, A.status);
+                const double3 a = force(k, vpred ? V : v1);
                 const double ac[3] = {a.x, a.y, a.z};
                 for (int c = 0; c < 3; ++c) {
                     double b[7], g[7];
@@ -637,12 +649,15 @@ int nblocks(int n, int t) { return (n + t - 1) / t; }
 void launch_ra15_sequence(const Ra15Args& a, cudaStream_t s) {
     ensure_constants();
     const int N = a.f.nsplit;
-    const size_t smem = sizeof(double) * (size_t)63 * N;  // x, v, B, G, a1, x1, v1 (57 N), m, ngf
+    // x, v, B, G, a1, x1, v1 (57 N), m, ngf, then the force terms
+    const size_t smem = sizeof(double) * ((size_t)63 * N + massive_par_scratch(N));
     if (smem <= 200 * 1024) {
         if (smem > 48 * 1024)
             cudaFuncSetAttribute(ra15_massive_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        // one warp per 32 bodies, at most 8
-        const int threads = std::min(256, std::max(32, (N + 31) / 32 * 32));
+        // one warp per 32 bodies, at most 8, and with the parallel force terms
+        // enough for one term each
+        int threads = std::min(256, std::max(32, (N + 31) / 32 * 32));
+        if (massive_par_scratch(N)) threads = std::max(threads, std::min(256, (N * N + 31) / 32 * 32));
         ra15_massive_kernel<true><<<1, threads, smem, s>>>(a);
     } else {
         ra15_massive_kernel<false><<<1, 256, 0, s>>>(a);
