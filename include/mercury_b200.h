@@ -63,6 +63,20 @@ int mercury_b200_ejections(double h, int physical, double rmax, int i0, int* ids
  * is one launch here. */
 int mercury_b200_encode_ce(const MercuryEvent* events, int n, double mcen, double rcen, double rmax, char* lines,
                            int* count);
+/* Adaptive steps (RADAU, BS, BS2) of one system whose massless particles are
+ * split across processes, each holding the whole massive set and its own
+ * particles: before every step-control decision the library passes its
+ * maxima to fn, which must replace each by the maximum over all processes
+ * (an all-reduce MAX). RADAU passes one value (max |b7|, +inf after a
+ * non-finite force or predictor); BS/BS2 pass 26 (the error maximum of levels
+ * 0..12, +inf where non-finite, then 1 or 0 for a failed force at each
+ * level). With every process taking the same decisions, each one's particles
+ * follow the steps the whole system would take in one process, bit for bit.
+ * Applies to the resident system only, never to HYBRID's encounter subsystem.
+ * fn = NULL (the default) reduces nothing. No counterpart in the reference,
+ * which runs one process. */
+typedef void (*mercury_b200_reduce_fn)(double* values, int count, void* user);
+int mercury_b200_set_step_reduce(mercury_b200_reduce_fn fn, void* user);
 /* Launch shape of the particle kernel: threads per CTA (multiple of 32) and
  * steps fused per launch (0 = automatic); a negative value keeps the setting. */
 int mercury_b200_set_launch(int particle_threads, int steps_per_launch);

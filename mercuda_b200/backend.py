@@ -53,7 +53,10 @@ EXTENSION_SYMBOLS = ["mercury_b200_mvs_advance", "mercury_b200_events", "mercury
                      "mercury_b200_energy", "mercury_b200_hybrid_adjoint_forward",
                      "mercury_b200_hybrid_adjoint_backward", "mercury_b200_hybrid_adjoint_timing",
                      "mercury_b200_hybrid_adjoint_free", "mercury_b200_ejections",
-                     "mercury_b200_encode_ce"]
+                     "mercury_b200_encode_ce", "mercury_b200_set_step_reduce"]
+
+# fn(values, count, user) of mercury_b200_set_step_reduce
+REDUCE_FN = C.CFUNCTYPE(None, C.POINTER(C.c_double), C.c_int, C.c_void_p)
 
 
 class BackendError(RuntimeError):
@@ -98,6 +101,7 @@ def load_library(path: Path | str | None = None) -> C.CDLL:
     L.mercury_b200_energy.argtypes = [D, I, PD, PD, PD]
     L.mercury_b200_ejections.argtypes = [D, I, D, I, PI, I, PI]
     L.mercury_b200_encode_ce.argtypes = [C.c_void_p, I, D, D, D, C.c_void_p, PI]
+    L.mercury_b200_set_step_reduce.argtypes = [C.c_void_p, C.c_void_p]
     L.mercury_b200_batch_upload.argtypes = [I, PI, PI, PD, PD, PD, PD, PD, PD]
     L.mercury_b200_batch_advance.argtypes = [D, I, D, PI]
     L.mercury_b200_batch_events.argtypes = [C.c_void_p, PI, PI, I]
@@ -383,6 +387,12 @@ class Backend:
                                            C.byref(count)) != 0:
             raise BackendError("ejection screen failed")
         return ids[:min(count.value, cap)].copy()
+
+    def set_step_reduce(self, fn) -> None:
+        """Install (a REDUCE_FN callback, kept alive by the caller) or clear
+        (None) the cross-process reduction of the adaptive step control."""
+        self._reduce = fn
+        self.lib.mercury_b200_set_step_reduce(C.cast(fn, C.c_void_p) if fn is not None else None, None)
 
     def fp64_peak(self):
         tf, ms = D(0.0), D(0.0)

@@ -24,6 +24,17 @@ int g_active = 0;
 Context& ctx() { return g_contexts[g_active]; }
 int active_context() { return g_active; }
 
+// Cross-process reduction of the adaptive step control's maxima (particles of
+// one system split across processes); null: one process.
+mercury_b200_reduce_fn g_step_reduce = nullptr;
+void* g_step_reduce_user = nullptr;
+
+// Replace each value by its maximum over the processes sharing the resident
+// system (the encounter subsystem of HYBRID is never shared).
+void reduce_step_maxima(double* values, int count) {
+    if (g_step_reduce && g_active == 0) g_step_reduce(values, count, g_step_reduce_user);
+}
+
 int report(const std::exception& e) {
     std::fprintf(stderr, "MERCURY CUDA: %s\n", e.what());
     return 1;
@@ -359,7 +370,9 @@ void ra15_step_once(double time, double* h, double* hdid, double tol, int64_t* r
         c.nforces += 1 + 7 * niter;
         double err;
         std::memcpy(&err, &bits, sizeof(err));
-        if (c.status_host->fault || !std::isfinite(err)) throw std::runtime_error("Nonfinite RADAU force or predictor");
+        if (c.status_host->fault || !std::isfinite(err)) err = INFINITY;
+        reduce_step_maxima(&err, 1);
+        if (!std::isfinite(err)) throw std::runtime_error("Nonfinite RADAU force or predictor");
         err = err / (72.0 * std::pow(std::fabs(t), 7.0));
         double next = err == 0.0 ? t * 1.4 : std::copysign(std::pow(tol / err, 1.0 / 9.0), t);
         if (reset && std::fabs(next / t) < 1.0) {
@@ -450,15 +463,21 @@ void bs_step_once(double time, double* h, double* hdid, double tol, int64_t* rej
         check(cudaMemcpyAsync(errs, c.bs_errs.p, sizeof(errs), cudaMemcpyDeviceToHost, c.stream), "status");
         check(cudaMemcpyAsync(lv, c.bs_lvst.p, sizeof(lv), cudaMemcpyDeviceToHost, c.stream), "status");
         check(cudaStreamSynchronize(c.stream), "step");
+        // per level: the error maximum, then whether a force failed
         const int fails = FAULT_NGF | FAULT_COINCIDENT;
-        if (lv[0].fault & fails) throw std::runtime_error("BS force failed");
+        double red[26];
+        for (int n = 0; n < 13; ++n) {
+            std::memcpy(&red[n], &errs[n], sizeof(double));
+            red[13 + n] = (lv[n].fault & fails) ? 1.0 : 0.0;
+        }
+        reduce_step_maxima(red, 26);
+        if (red[13] > 0.0) throw std::runtime_error("BS force failed");
         int accepted = 0;
         for (int n = 1; n <= L && !accepted; ++n) {
             forces += bs_level_forces(V, n);
-            if (lv[n].fault & fails) throw std::runtime_error("BS force failed");
+            if (red[13 + n] > 0.0) throw std::runtime_error("BS force failed");
             if (n <= 3) continue;
-            double e;
-            std::memcpy(&e, &errs[n], sizeof(e));
+            const double e = red[n];
             if (!std::isfinite(e)) throw std::runtime_error(nonfinite);
             if (e <= tol2) accepted = n;
         }
@@ -1775,6 +1794,12 @@ int mercury_b200_ejections(double h, int physical, double rmax, int i0, int* ids
     } catch (const std::exception& e) {
         return report(e);
     }
+}
+
+int mercury_b200_set_step_reduce(mercury_b200_reduce_fn fn, void* user) {
+    g_step_reduce = fn;
+    g_step_reduce_user = user;
+    return 0;
 }
 
 int mercury_b200_set_launch(int particle_threads, int steps_per_launch) {

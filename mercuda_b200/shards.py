@@ -10,6 +10,12 @@ host-side equivalent of the reference's per-step event list and download
 (mercury_cuda.cu:466-493, the records of mercury_gpu.f90:206-247), now with
 global body ids.
 
+The adaptive integrators (RADAU, BS, BS2) shard the same way with one real
+exchange: their step control takes the maximum of an error measure over every
+body, so each attempt's maxima are all-reduced (MAX) across ranks through the
+library's step-reduce hook (`step_reduce`); every rank then takes the same
+decisions and its particles follow the whole system's steps bit for bit.
+
 Every rank takes the same collective steps in the same order. The classes are
 backend-agnostic: `ShardedRun` drives any object with the `upload`,
 `mvs_advance`, `download` methods of `backend.Backend`, and `Ranks` works over
@@ -163,3 +169,23 @@ class ShardedRun:
             X[ids] = xs
             V[ids] = vs
         return X, V
+
+
+def step_reduce(ranks: Ranks):
+    """A callback for Backend.set_step_reduce: replaces the library's
+    step-control maxima by their maximum over all ranks (all-reduce MAX, on
+    the ranks' device). Keep the returned object alive while it is installed."""
+    import ctypes
+
+    from .backend import REDUCE_FN
+
+    def reduce(ptr, count, user):
+        if ranks.dist is None:
+            return
+        import torch
+        vals = np.ctypeslib.as_array(ptr, shape=(count,))
+        t = torch.tensor(vals, dtype=torch.float64, device=ranks.device)
+        ranks.dist.all_reduce(t, op=ranks.dist.ReduceOp.MAX)
+        vals[:] = t.cpu().numpy()
+
+    return REDUCE_FN(reduce)

@@ -82,6 +82,15 @@ def worker(rank, world, port, out_dir, case):
             else:
                 assert got is None and states is None
                 np.savez(Path(out_dir) / f"rank{rank}.npz", own_n=len(own[0]), t=t)
+        elif case == "reduce":
+            # the adaptive step control's maxima, all-reduced through the
+            # library's callback type (called here as the library calls it)
+            import ctypes
+            from mercuda_b200.shards import step_reduce
+            cb = step_reduce(ranks)
+            vals = (ctypes.c_double * 4)(float(rank), -float(rank), float("inf") if rank == 1 else 0.0, 5.0)
+            cb(vals, 4, None)
+            np.savez(Path(out_dir) / f"rank{rank}.npz", vals=np.array(list(vals)))
         elif case == "mismatch":
             s = system()
             shard, ids = particle_shard(s, rank, world)
@@ -123,6 +132,12 @@ def test_sharded_run_equals_unsharded(tmp_path, oracle):
     assert float(r0["value"]) == 100.0
     npart = s.n - s.nbig
     assert int(r0["own_n"]) == s.nbig + (npart + 1) // 2 and int(r1["own_n"]) == s.nbig + npart // 2
+
+
+def test_step_reduce_takes_the_maximum_over_ranks(tmp_path):
+    r0, r1 = launch(tmp_path, "reduce")
+    want = [1.0, 0.0, float("inf"), 5.0]
+    assert list(r0["vals"]) == want and list(r1["vals"]) == want
 
 
 def test_ranks_that_disagree_fail_together(tmp_path):
