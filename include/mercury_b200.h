@@ -63,6 +63,19 @@ int mercury_b200_ejections(double h, int physical, double rmax, int i0, int* ids
  * is one launch here. */
 int mercury_b200_encode_ce(const MercuryEvent* events, int n, double mcen, double rcen, double rmax, char* lines,
                            int* count);
+/* mdt_hkce's substep loop (mercury6_2.for:3898-3937) over the active
+ * encounter subsystem, inside the library: from local time 0 to h, BS2
+ * substeps (mercury_cuda_reset + mercury_cuda_step, dtflag 1 then 2) of
+ * length *hrec (clipped to the remainder), each followed by
+ * mercury_cuda_events at time + tlocal, exactly as a host drives these
+ * drop-in calls, without a download per substep. *hrec receives the last
+ * substep length tried (mdt_hkce's hrec), *forces the force calls, *nrecords
+ * the number of close-encounter and collision records (central-body records
+ * left out; subsystem ids, 1-based), fetched with mercury_b200_events(dst,
+ * NULL, cap). Call between mercury_cuda_encounter_enter and
+ * mercury_cuda_download / _exit. */
+int mercury_b200_encounter_run(double time, double h, double tol, double rcen, double* hrec, int64_t* forces,
+                               int* nrecords);
 /* Adaptive steps (RADAU, BS, BS2) of one system whose massless particles are
  * split across processes, each holding the whole massive set and its own
  * particles: before every step-control decision the library passes its

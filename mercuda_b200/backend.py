@@ -53,7 +53,8 @@ EXTENSION_SYMBOLS = ["mercury_b200_mvs_advance", "mercury_b200_events", "mercury
                      "mercury_b200_energy", "mercury_b200_hybrid_adjoint_forward",
                      "mercury_b200_hybrid_adjoint_backward", "mercury_b200_hybrid_adjoint_timing",
                      "mercury_b200_hybrid_adjoint_free", "mercury_b200_ejections",
-                     "mercury_b200_encode_ce", "mercury_b200_set_step_reduce"]
+                     "mercury_b200_encode_ce", "mercury_b200_set_step_reduce",
+                     "mercury_b200_encounter_run"]
 
 # fn(values, count, user) of mercury_b200_set_step_reduce
 REDUCE_FN = C.CFUNCTYPE(None, C.POINTER(C.c_double), C.c_int, C.c_void_p)
@@ -102,6 +103,7 @@ def load_library(path: Path | str | None = None) -> C.CDLL:
     L.mercury_b200_ejections.argtypes = [D, I, D, I, PI, I, PI]
     L.mercury_b200_encode_ce.argtypes = [C.c_void_p, I, D, D, D, C.c_void_p, PI]
     L.mercury_b200_set_step_reduce.argtypes = [C.c_void_p, C.c_void_p]
+    L.mercury_b200_encounter_run.argtypes = [D, D, D, D, PD, PI64, PI]
     L.mercury_b200_batch_upload.argtypes = [I, PI, PI, PD, PD, PD, PD, PD, PD]
     L.mercury_b200_batch_advance.argtypes = [D, I, D, PI]
     L.mercury_b200_batch_events.argtypes = [C.c_void_p, PI, PI, I]
@@ -251,11 +253,15 @@ class Backend:
         self.forces += nf.value
 
     # mdt_hy's CUDA branch with mdt_hkce's (mercury6_2.for:3646-3659, 3798-3940)
-    def hybrid_step(self, sys: System, time: float, h: float, tol: float, state: dict, rcen: float = 0.005):
+    def hybrid_step(self, sys: System, time: float, h: float, tol: float, state: dict, rcen: float = 0.005,
+                    fused: bool = True):
         """One HYBRID step of sys (democratic-heliocentric masses/radii/rcrit on
         the host; positions live on the device). `state` carries dtflag and hrec
         between calls. Returns the encounter records of the subsystem (global
-        1-based ids) and the number of encounter pairs."""
+        1-based ids) and the number of encounter pairs. The encounter
+        subsystem's substeps run inside the library (mercury_b200_encounter_run)
+        or, with fused=False, one drop-in call at a time from here as
+        mercury_gpu.f90's host loop makes them; the results are the same."""
         if state.get("dtflag", 0) == 0:
             state["hrec"] = h
         x = np.zeros((sys.n, 3))
@@ -288,25 +294,43 @@ class Backend:
             outer_n = self.n
             self.n = nbs
             try:
-                dtflag, tlocal, hlocal = 1, 0.0, math.copysign(state["hrec"], h)
-                while True:
-                    tmp0 = abs(h) - abs(tlocal)
-                    state["hrec"] = hlocal
-                    if abs(hlocal) > tmp0:
-                        hlocal = math.copysign(tmp0, h)
-                    hdid, hlocal = self.step(tlocal, hlocal, tol, dtflag)
-                    dtflag = 2
-                    xbs, vbs = self.download()
-                    tlocal = tlocal + hdid
-                    for e in self.events(time + tlocal, hdid, rcen):
-                        if e["kind"] & 8:
-                            continue
+                if fused:
+                    # the same drop-in calls, looped inside the library
+                    hrec, nf, nrec = D(state["hrec"]), C.c_int64(0), I(0)
+                    if self.lib.mercury_b200_encounter_run(time, h, tol, rcen, C.byref(hrec), C.byref(nf),
+                                                           C.byref(nrec)) != 0:
+                        raise BackendError("CUDA integration step failed")
+                    state["hrec"] = hrec.value
+                    self.forces += nf.value
+                    sub_ev = np.zeros(nrec.value, dtype=EVENT_DTYPE)
+                    if nrec.value:
+                        self.lib.mercury_b200_events(sub_ev.ctypes.data_as(C.c_void_p), None, nrec.value)
+                    for e in sub_ev:
                         e = e.copy()
                         e["i"] = index[e["i"] - 1] + 1
                         e["j"] = index[e["j"] - 1] + 1
                         records.append(e)
-                    if not (tlocal - h) * h < 0.0:
-                        break
+                    xbs, vbs = self.download()
+                else:
+                    dtflag, tlocal, hlocal = 1, 0.0, math.copysign(state["hrec"], h)
+                    while True:
+                        tmp0 = abs(h) - abs(tlocal)
+                        state["hrec"] = hlocal
+                        if abs(hlocal) > tmp0:
+                            hlocal = math.copysign(tmp0, h)
+                        hdid, hlocal = self.step(tlocal, hlocal, tol, dtflag)
+                        dtflag = 2
+                        xbs, vbs = self.download()
+                        tlocal = tlocal + hdid
+                        for e in self.events(time + tlocal, hdid, rcen):
+                            if e["kind"] & 8:
+                                continue
+                            e = e.copy()
+                            e["i"] = index[e["i"] - 1] + 1
+                            e["j"] = index[e["j"] - 1] + 1
+                            records.append(e)
+                        if not (tlocal - h) * h < 0.0:
+                            break
             finally:
                 self.lib.mercury_cuda_encounter_exit()
                 self.n = outer_n

@@ -1796,6 +1796,46 @@ int mercury_b200_ejections(double h, int physical, double rmax, int i0, int* ids
     }
 }
 
+int mercury_b200_encounter_run(double time, double h, double tol, double rcen, double* hrec, int64_t* forces,
+                                int* nrecords) {
+    try {
+        if (g_active != 1) throw std::runtime_error("no encounter subsystem active");
+        std::vector<MercuryEvent> keep;
+        int64_t nforces = 0;
+        int dtflag = 1;
+        double tlocal = 0.0, hlocal = std::copysign(*hrec, h);
+        for (;;) {
+            const double tmp0 = std::fabs(h) - std::fabs(tlocal);
+            *hrec = hlocal;
+            if (std::fabs(hlocal) > tmp0) hlocal = std::copysign(tmp0, h);
+            mercury_cuda_reset(dtflag);
+            double hdid = 0.0;
+            int64_t nf = 0, nr = 0;
+            if (mercury_cuda_step(tlocal, &hlocal, &hdid, tol, &nf, &nr))
+                throw std::runtime_error("encounter step failed");
+            nforces += nf;
+            dtflag = 2;
+            tlocal = tlocal + hdid;
+            const MercuryEvent* ev = nullptr;
+            int count = 0;
+            if (mercury_cuda_events(time + tlocal, hdid, rcen, &ev, &count))
+                throw std::runtime_error("encounter events failed");
+            for (int k = 0; k < count; ++k)
+                if (!(ev[k].kind & EV_CENTRAL)) keep.push_back(ev[k]);
+            if (!((tlocal - h) * h < 0.0)) break;
+        }
+        Context& c = ctx();
+        c.host_events.swap(keep);
+        c.host_steps.clear();
+        c.event_order.clear();
+        *forces = nforces;
+        *nrecords = (int)c.host_events.size();
+        return 0;
+    } catch (const std::exception& e) {
+        return report(e);
+    }
+}
+
 int mercury_b200_set_step_reduce(mercury_b200_reduce_fn fn, void* user) {
     g_step_reduce = fn;
     g_step_reduce_user = user;

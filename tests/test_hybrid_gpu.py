@@ -19,14 +19,14 @@ from mercuda_b200.system import K2, System, make_system, mce_init
 pytestmark = pytest.mark.gpu
 
 
-def run_device(cuda_lib, sys, h, nsteps, tol=1e-12, rcen=0.005):
+def run_device(cuda_lib, sys, h, nsteps, tol=1e-12, rcen=0.005, fused=True):
     be = Backend("HYBRID", cuda_lib)
     be.configure()
     be.upload(sys)
     state = {"dtflag": 0}
     events, pairs, t = [], 0, 0.0
     for _ in range(nsteps):
-        ev, npair = be.hybrid_step(sys, t, h, tol, state, rcen)
+        ev, npair = be.hybrid_step(sys, t, h, tol, state, rcen, fused=fused)
         pairs += npair
         t = t + h
         events.append(ev)
@@ -109,3 +109,16 @@ def test_hybrid_particles_and_encounters(cuda_lib, oracle):
     mv = (sys.m[1:, None] * v[1:]).sum(axis=0) / sys.m[0]
     vh[1:] = v[1:] + mv
     assert np.allclose(xp, x) and np.max(np.abs(vp - vh)) < 1e-15
+
+
+def test_encounter_loop_in_library_matches_drop_in_calls(cuda_lib):
+    """mercury_b200_encounter_run makes the drop-in calls of mdt_hkce's host
+    loop inside the library: the same states, records, pairs and force calls
+    as driving them one at a time."""
+    sys0 = make_system(seed=4, n_particles=1500, nplanets=8, near_fraction=0.05, h=8.0)
+    a = run_device(cuda_lib, sys0.copy(), 8.0, 10, fused=True)
+    b = run_device(cuda_lib, sys0.copy(), 8.0, 10, fused=False)
+    assert a[5] == b[5] and a[5] > 10 and a[6] == b[6]
+    for k in range(4):
+        assert np.array_equal(a[k], b[k])
+    assert a[4].tobytes() == b[4].tobytes()
