@@ -234,9 +234,13 @@ class Backend:
         """Kick, solar drift, Kepler drift and mce_snif. Returns (ce, pi, pj); the
         members' rows of x, v receive their pre-drift states."""
         n = self.n
-        ce = np.zeros(n, dtype=np.int32)
-        pi = np.zeros(cap, dtype=np.int32)
-        pj = np.zeros(cap, dtype=np.int32)
+        # work arrays kept between steps: the library writes ce and the pair
+        # lists only when there are pairs, and reads back only members' rows
+        buf = getattr(self, "_begin_buf", None)
+        if buf is None or len(buf[0]) != n or len(buf[1]) != cap:
+            buf = (np.zeros(n, dtype=np.int32), np.zeros(cap, dtype=np.int32), np.zeros(cap, dtype=np.int32))
+            self._begin_buf = buf
+        ce, pi, pj = buf
         count, nf = I(0), C.c_int64(0)
         rc = self.lib.mercury_cuda_hybrid_begin(h, _p(np.ascontiguousarray(rcrit, dtype=np.float64)), int(flag),
                                                 cap, ce.ctypes.data_as(PI), C.byref(count), pi.ctypes.data_as(PI),
@@ -264,16 +268,18 @@ class Backend:
         mercury_gpu.f90's host loop makes them; the results are the same."""
         if state.get("dtflag", 0) == 0:
             state["hrec"] = h
-        x = np.zeros((sys.n, 3))
-        v = np.zeros((sys.n, 3))
+        # host rows of the members only pass through x, v (kept between steps)
+        rows = getattr(self, "_step_rows", None)
+        if rows is None or rows[0].shape[0] != sys.n:
+            rows = (np.zeros((sys.n, 3)), np.zeros((sys.n, 3)))
+            self._step_rows = rows
+        x, v = rows
         ce, pi, pj = self.hybrid_begin(h, sys.rcrit, state.get("dtflag", 0), x, v)
         state["dtflag"] = 2
         records = []
         if len(pi):
             sub = np.concatenate([[0], np.nonzero(ce[1:])[0] + 1])
             index = sub.tolist()
-            back = np.full(sys.n, -1, dtype=np.int64)
-            back[sub] = np.arange(len(sub))
             nbsbig = 1 + int(np.count_nonzero(sub[1:] < sys.nbig))
             nbs = len(sub)
             mbs = sys.m[sub].copy()
@@ -285,8 +291,9 @@ class Backend:
             rcebs = sys.rce[sub].copy()
             rphybs = sys.rphys[sub].copy()
             rcritbs[0] = rcebs[0] = rphybs[0] = 0.0
-            ibs = np.ascontiguousarray(back[pi - 1] + 1, dtype=np.int32)
-            jbs = np.ascontiguousarray(back[pj - 1] + 1, dtype=np.int32)
+            # subsystem index of each pair member (sub is sorted)
+            ibs = np.ascontiguousarray(np.searchsorted(sub, pi - 1) + 1, dtype=np.int32)
+            jbs = np.ascontiguousarray(np.searchsorted(sub, pj - 1) + 1, dtype=np.int32)
             if self.lib.mercury_cuda_encounter_enter(nbs, nbsbig, _p(mbs), _p(xbs), _p(vbs), _p(rcritbs), _p(rcebs),
                                                      _p(rphybs), len(ibs), ibs.ctypes.data_as(PI),
                                                      jbs.ctypes.data_as(PI)) != 0:

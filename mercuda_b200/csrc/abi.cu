@@ -1434,12 +1434,17 @@ int mercury_cuda_hybrid_finish(double h, const double* m, const double* xx, cons
                                   cudaMemcpyHostToDevice, c.stream),
                   "members");
             scatter_members(c.hy_ids.p, nm, c.hy_packed.p, c.bigstate[out].p, c.pstate[out].p);
-            c.transfer.reserve((size_t)6 * c.n);
-            check(cudaMemcpyAsync(c.transfer.p, m, sizeof(double) * c.n, cudaMemcpyHostToDevice, c.stream), "upload");
-            scatter_rows(c.transfer.p, c.n, 1, c.nsplit, c.mbig.p, c.nsplit, c.pm(), c.npcap, c.inv.p, c.stream);
+            c.dropin_launches += 1;
+            // the masses (changed only where the host merged bodies)
+            if (c.m_host.size() != (size_t)c.n || std::memcmp(m, c.m_host.data(), sizeof(double) * c.n) != 0) {
+                c.transfer.reserve((size_t)6 * c.n);
+                check(cudaMemcpyAsync(c.transfer.p, m, sizeof(double) * c.n, cudaMemcpyHostToDevice, c.stream),
+                      "upload");
+                scatter_rows(c.transfer.p, c.n, 1, c.nsplit, c.mbig.p, c.nsplit, c.pm(), c.npcap, c.inv.p, c.stream);
+                c.m_host.assign(m, m + c.n);
+                c.dropin_launches += 1;
+            }
             check(cudaStreamSynchronize(c.stream), "upload");
-            c.m_host.assign(m, m + c.n);
-            c.dropin_launches += 2;
         }
         check(cudaMemsetAsync(c.status.p, 0, sizeof(DeviceStatus), c.stream), "memset");
         launch_hybrid_finish(hybrid_args(h, 0), c.stream);
