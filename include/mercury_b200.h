@@ -63,6 +63,13 @@ int mercury_b200_ejections(double h, int physical, double rmax, int i0, int* ids
  * is one launch here. */
 int mercury_b200_encode_ce(const MercuryEvent* events, int n, double mcen, double rcen, double rmax, char* lines,
                            int* count);
+/* Between mercury_cuda_hybrid_begin and _finish: replace the set of bodies
+ * (0-based indices 1 .. n-1 of the resident system) whose rows
+ * mercury_cuda_hybrid_finish takes from its x, v arrays, which otherwise are
+ * the members that hybrid_begin's pairs named. A process holding a share of
+ * the particles lists the Big bodies that any process found in an encounter
+ * (their subsystem end states) besides its own members. */
+int mercury_b200_hybrid_members(const int* ids, int count);
 /* mdt_hkce's substep loop (mercury6_2.for:3898-3937) over the active
  * encounter subsystem, inside the library: from local time 0 to h, BS2
  * substeps (mercury_cuda_reset + mercury_cuda_step, dtflag 1 then 2) of

@@ -54,7 +54,7 @@ EXTENSION_SYMBOLS = ["mercury_b200_mvs_advance", "mercury_b200_events", "mercury
                      "mercury_b200_hybrid_adjoint_backward", "mercury_b200_hybrid_adjoint_timing",
                      "mercury_b200_hybrid_adjoint_free", "mercury_b200_ejections",
                      "mercury_b200_encode_ce", "mercury_b200_set_step_reduce",
-                     "mercury_b200_encounter_run"]
+                     "mercury_b200_encounter_run", "mercury_b200_hybrid_members"]
 
 # fn(values, count, user) of mercury_b200_set_step_reduce
 REDUCE_FN = C.CFUNCTYPE(None, C.POINTER(C.c_double), C.c_int, C.c_void_p)
@@ -104,6 +104,7 @@ def load_library(path: Path | str | None = None) -> C.CDLL:
     L.mercury_b200_encode_ce.argtypes = [C.c_void_p, I, D, D, D, C.c_void_p, PI]
     L.mercury_b200_set_step_reduce.argtypes = [C.c_void_p, C.c_void_p]
     L.mercury_b200_encounter_run.argtypes = [D, D, D, D, PD, PI64, PI]
+    L.mercury_b200_hybrid_members.argtypes = [PI, I]
     L.mercury_b200_batch_upload.argtypes = [I, PI, PI, PD, PD, PD, PD, PD, PD]
     L.mercury_b200_batch_advance.argtypes = [D, I, D, PI]
     L.mercury_b200_batch_events.argtypes = [C.c_void_p, PI, PI, I]
@@ -279,73 +280,94 @@ class Backend:
         records = []
         if len(pi):
             sub = np.concatenate([[0], np.nonzero(ce[1:])[0] + 1])
-            index = sub.tolist()
-            nbsbig = 1 + int(np.count_nonzero(sub[1:] < sys.nbig))
-            nbs = len(sub)
-            mbs = sys.m[sub].copy()
-            xbs = x[sub].copy()
-            vbs = v[sub].copy()
-            xbs[0] = 0.0
-            vbs[0] = 0.0
-            rcritbs = sys.rcrit[sub].copy()
-            rcebs = sys.rce[sub].copy()
-            rphybs = sys.rphys[sub].copy()
-            rcritbs[0] = rcebs[0] = rphybs[0] = 0.0
-            # subsystem index of each pair member (sub is sorted)
-            ibs = np.ascontiguousarray(np.searchsorted(sub, pi - 1) + 1, dtype=np.int32)
-            jbs = np.ascontiguousarray(np.searchsorted(sub, pj - 1) + 1, dtype=np.int32)
-            if self.lib.mercury_cuda_encounter_enter(nbs, nbsbig, _p(mbs), _p(xbs), _p(vbs), _p(rcritbs), _p(rcebs),
-                                                     _p(rphybs), len(ibs), ibs.ctypes.data_as(PI),
-                                                     jbs.ctypes.data_as(PI)) != 0:
-                raise BackendError("CUDA encounter initialization failed")
-            outer_n = self.n
-            self.n = nbs
-            try:
-                if fused:
-                    # the same drop-in calls, looped inside the library
-                    hrec, nf, nrec = D(state["hrec"]), C.c_int64(0), I(0)
-                    if self.lib.mercury_b200_encounter_run(time, h, tol, rcen, C.byref(hrec), C.byref(nf),
-                                                           C.byref(nrec)) != 0:
-                        raise BackendError("CUDA integration step failed")
-                    state["hrec"] = hrec.value
-                    self.forces += nf.value
-                    sub_ev = np.zeros(nrec.value, dtype=EVENT_DTYPE)
-                    if nrec.value:
-                        self.lib.mercury_b200_events(sub_ev.ctypes.data_as(C.c_void_p), None, nrec.value)
-                    for e in sub_ev:
-                        e = e.copy()
-                        e["i"] = index[e["i"] - 1] + 1
-                        e["j"] = index[e["j"] - 1] + 1
-                        records.append(e)
-                    xbs, vbs = self.download()
-                else:
-                    dtflag, tlocal, hlocal = 1, 0.0, math.copysign(state["hrec"], h)
-                    while True:
-                        tmp0 = abs(h) - abs(tlocal)
-                        state["hrec"] = hlocal
-                        if abs(hlocal) > tmp0:
-                            hlocal = math.copysign(tmp0, h)
-                        hdid, hlocal = self.step(tlocal, hlocal, tol, dtflag)
-                        dtflag = 2
-                        xbs, vbs = self.download()
-                        tlocal = tlocal + hdid
-                        for e in self.events(time + tlocal, hdid, rcen):
-                            if e["kind"] & 8:
-                                continue
-                            e = e.copy()
-                            e["i"] = index[e["i"] - 1] + 1
-                            e["j"] = index[e["j"] - 1] + 1
-                            records.append(e)
-                        if not (tlocal - h) * h < 0.0:
-                            break
-            finally:
-                self.lib.mercury_cuda_encounter_exit()
-                self.n = outer_n
+            xbs, vbs, records = self.encounter_subsystem(sub, sys.nbig, sys.m[sub], x[sub], v[sub], sys.rcrit[sub],
+                                                         sys.rce[sub], sys.rphys[sub], pi, pj, time, h, tol, state,
+                                                         rcen, fused)
             x[sub[1:]] = xbs[1:]
             v[sub[1:]] = vbs[1:]
         self.hybrid_finish(h, sys.m, x, v)
         events = np.array(records, dtype=EVENT_DTYPE) if records else np.zeros(0, dtype=EVENT_DTYPE)
         return events, len(pi)
+
+    def encounter_subsystem(self, sub, nbig, m, x, v, rcrit, rce, rphys, pi, pj, time, h, tol, state, rcen,
+                            fused=True):
+        """mdt_hkce (mercury6_2.for:3798-3940) through the drop-in calls: the
+        central body and the members sub[1:] (sorted global 0-based indices;
+        sub[0] = 0) with masses, pre-drift states and radii in the same order
+        (row 0 is ignored), encounter pairs pi/pj (global 1-based). Returns the
+        members' end states (rows as sub) and the close-encounter records
+        with global 1-based ids."""
+        sub = np.asarray(sub)
+        index = sub.tolist()
+        nbs = len(sub)
+        nbsbig = 1 + int(np.count_nonzero(sub[1:] < nbig))
+        mbs = np.ascontiguousarray(m, dtype=np.float64).copy()
+        xbs = np.array(x, dtype=np.float64)
+        vbs = np.array(v, dtype=np.float64)
+        xbs[0] = 0.0
+        vbs[0] = 0.0
+        rcritbs = np.array(rcrit, dtype=np.float64)
+        rcebs = np.array(rce, dtype=np.float64)
+        rphybs = np.array(rphys, dtype=np.float64)
+        rcritbs[0] = rcebs[0] = rphybs[0] = 0.0
+        # subsystem index of each pair member (sub is sorted)
+        ibs = np.ascontiguousarray(np.searchsorted(sub, np.asarray(pi) - 1) + 1, dtype=np.int32)
+        jbs = np.ascontiguousarray(np.searchsorted(sub, np.asarray(pj) - 1) + 1, dtype=np.int32)
+        if self.lib.mercury_cuda_encounter_enter(nbs, nbsbig, _p(mbs), _p(xbs), _p(vbs), _p(rcritbs), _p(rcebs),
+                                                 _p(rphybs), len(ibs), ibs.ctypes.data_as(PI),
+                                                 jbs.ctypes.data_as(PI)) != 0:
+            raise BackendError("CUDA encounter initialization failed")
+        records = []
+        outer_n = self.n
+        self.n = nbs
+        try:
+            if fused:
+                # the same drop-in calls, looped inside the library
+                hrec, nf, nrec = D(state["hrec"]), C.c_int64(0), I(0)
+                if self.lib.mercury_b200_encounter_run(time, h, tol, rcen, C.byref(hrec), C.byref(nf),
+                                                       C.byref(nrec)) != 0:
+                    raise BackendError("CUDA integration step failed")
+                state["hrec"] = hrec.value
+                self.forces += nf.value
+                sub_ev = np.zeros(nrec.value, dtype=EVENT_DTYPE)
+                if nrec.value:
+                    self.lib.mercury_b200_events(sub_ev.ctypes.data_as(C.c_void_p), None, nrec.value)
+                for e in sub_ev:
+                    e = e.copy()
+                    e["i"] = index[e["i"] - 1] + 1
+                    e["j"] = index[e["j"] - 1] + 1
+                    records.append(e)
+                xbs, vbs = self.download()
+            else:
+                dtflag, tlocal, hlocal = 1, 0.0, math.copysign(state["hrec"], h)
+                while True:
+                    tmp0 = abs(h) - abs(tlocal)
+                    state["hrec"] = hlocal
+                    if abs(hlocal) > tmp0:
+                        hlocal = math.copysign(tmp0, h)
+                    hdid, hlocal = self.step(tlocal, hlocal, tol, dtflag)
+                    dtflag = 2
+                    xbs, vbs = self.download()
+                    tlocal = tlocal + hdid
+                    for e in self.events(time + tlocal, hdid, rcen):
+                        if e["kind"] & 8:
+                            continue
+                        e = e.copy()
+                        e["i"] = index[e["i"] - 1] + 1
+                        e["j"] = index[e["j"] - 1] + 1
+                        records.append(e)
+                    if not (tlocal - h) * h < 0.0:
+                        break
+        finally:
+            self.lib.mercury_cuda_encounter_exit()
+            self.n = outer_n
+        return xbs, vbs, records
+
+    def hybrid_members(self, ids) -> None:
+        """The bodies (0-based) whose rows hybrid_finish takes from x, v."""
+        ids = np.ascontiguousarray(ids, dtype=np.int32)
+        if self.lib.mercury_b200_hybrid_members(ids.ctypes.data_as(PI), len(ids)) != 0:
+            raise BackendError("CUDA hybrid member list rejected")
 
     # mal_hvar's step loop (mercury6_2.for:423-470) through the drop-in calls:
     # steps clipped to tstop, dtflag = 1 (a fresh RA15 sequence) when a clipped

@@ -1801,6 +1801,30 @@ int mercury_b200_ejections(double h, int physical, double rmax, int i0, int* ids
     }
 }
 
+int mercury_b200_hybrid_members(const int* ids, int count) {
+    Context& c = ctx();
+    try {
+        require_system();
+        if (!c.hy_begun) throw std::runtime_error("hybrid_members outside a HYBRID step");
+        if (count < 0 || (count > 0 && !ids)) throw std::runtime_error("invalid member list");
+        std::vector<int> m(ids, ids + count);
+        std::sort(m.begin(), m.end());
+        m.erase(std::unique(m.begin(), m.end()), m.end());
+        for (int j : m)
+            if (j < 1 || j >= c.n) throw std::runtime_error("member id out of range");
+        c.hy_members = m;
+        const int nm = (int)m.size();
+        if (nm) {
+            c.hy_ids.reserve(nm);
+            c.hy_packed.reserve((size_t)6 * nm);
+            h2d(c.hy_ids.p, m.data(), sizeof(int) * nm, c.stream, "members");
+        }
+        return 0;
+    } catch (const std::exception& e) {
+        return report(e);
+    }
+}
+
 int mercury_b200_encounter_run(double time, double h, double tol, double rcen, double* hrec, int64_t* forces,
                                 int* nrecords) {
     try {

@@ -189,3 +189,61 @@ def step_reduce(ranks: Ranks):
         vals[:] = t.cpu().numpy()
 
     return REDUCE_FN(reduce)
+
+
+def sharded_hybrid_step(backend, ranks: Ranks, shard: System, ids: np.ndarray, time: float, h: float, tol: float,
+                        state: dict, rcen: float = 0.005, fused: bool = True):
+    """One HYBRID step (mdt_hy, mercury6_2.for:3618-3782) of this rank's shard
+    of one system: every Big body and this rank's particles, `ids` the global
+    0-based index of each shard body (sorted, Big bodies first).
+
+    mce_snif's pairs of every rank are all-gathered with the members'
+    pre-drift states, and every rank integrates the one global encounter
+    subsystem that a single process would (the same members, pair list and
+    BS2 substeps, so the same results); each rank then takes the end states
+    of every Big member and of its own particle members. Returns the
+    subsystem's records (global 1-based ids, the same on every rank) and the
+    global number of encounter pairs."""
+    from .backend import EVENT_DTYPE
+
+    ids = np.asarray(ids, dtype=np.int64)
+    n, nbig = shard.n, shard.nbig
+    if state.get("dtflag", 0) == 0:
+        state["hrec"] = h
+    rows = getattr(backend, "_shard_rows", None)
+    if rows is None or rows[0].shape[0] != n:
+        rows = (np.zeros((n, 3)), np.zeros((n, 3)))
+        backend._shard_rows = rows
+    x, v = rows
+    ce, pi, pj = backend.hybrid_begin(h, shard.rcrit, state.get("dtflag", 0), x, v)
+    state["dtflag"] = 2
+    local = np.nonzero(ce[1:])[0] + 1 if len(pi) else np.zeros(0, dtype=np.int64)
+    mine = (ids[pi - 1] + 1, ids[pj - 1] + 1, ids[local],
+            np.column_stack([shard.m[local], x[local], v[local], shard.rcrit[local], shard.rce[local],
+                             shard.rphys[local]]) if len(local) else np.zeros((0, 10)))
+    parts = ranks.gather(mine, everywhere=True)
+    gpi = np.concatenate([p[0] for p in parts]).astype(np.int64)
+    gpj = np.concatenate([p[1] for p in parts]).astype(np.int64)
+    records = []
+    if len(gpi):
+        # the pair list a single process would find: unique, sorted by (i, j)
+        pairs = np.unique(np.stack([gpi, gpj], axis=1), axis=0)
+        gpi, gpj = pairs[:, 0], pairs[:, 1]
+        members, first = np.unique(np.concatenate([p[2] for p in parts]), return_index=True)
+        data = np.concatenate([p[3] for p in parts])[first]
+        sub = np.concatenate([[0], members])
+        central = np.zeros((1, 10))
+        central[0, 0] = shard.m[0]
+        d = np.concatenate([central, data])
+        xbs, vbs, records = backend.encounter_subsystem(sub, nbig, d[:, 0], d[:, 1:4], d[:, 4:7], d[:, 7], d[:, 8],
+                                                        d[:, 9], gpi, gpj, time, h, tol, state, rcen, fused)
+        # the members this shard holds: every Big member and its own particles
+        pos = np.searchsorted(ids, members)
+        held = (pos < n) & (ids[np.minimum(pos, n - 1)] == members)
+        apply = pos[held]
+        x[apply] = xbs[1:][held]
+        v[apply] = vbs[1:][held]
+        backend.hybrid_members(apply)
+    backend.hybrid_finish(h, shard.m, x, v)
+    events = np.array(records, dtype=EVENT_DTYPE) if records else np.zeros(0, dtype=EVENT_DTYPE)
+    return events, len(gpi)
