@@ -83,6 +83,21 @@ int mercury_b200_hybrid_members(const int* ids, int count);
  * mercury_cuda_download / _exit. */
 int mercury_b200_encounter_run(double time, double h, double tol, double rcen, double* hrec, int64_t* forces,
                                int* nrecords);
+/* mxx_sync's epoch synchronisation (mercury6_2.for:7442-7574) before a run,
+ * in two parts. mercury_b200_epoch_order (host only) gives its order of the
+ * nsml Small bodies: sorted by epoch with mxx_sort's Shell sort, reversed when
+ * the last is further from tstart than the first; order[k] is the 0-based
+ * Small body at position k. The host uploads the system in that order
+ * (configure(2), mdt_bs1), the Big bodies at their common epoch *time, Small
+ * body j at epoch[j] (epoch[n], Big entries ignored), and calls
+ * mercury_b200_sync_epochs: for each Small body j in order, the bodies before
+ * it are advanced by mdt_bs1 steps (clipped to dtout and to j's epoch,
+ * mercury_support.f90:202-212) until they reach j's epoch, then j joins. On
+ * return every body is at *time, the last epoch; *steps counts the BS steps.
+ * Massless Small bodies only. The reference runs this on the host before its
+ * GPU backend is selected (mercury6_2.for:158-185). */
+int mercury_b200_epoch_order(int nsml, const double* epochs, double tstart, int* order);
+int mercury_b200_sync_epochs(const double* epoch, double* time, double h0, double tol, double dtout, int* steps);
 /* Adaptive steps (RADAU, BS, BS2) of one system whose massless particles are
  * split across processes, each holding the whole massive set and its own
  * particles: before every step-control decision the library passes its

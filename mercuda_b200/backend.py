@@ -54,7 +54,8 @@ EXTENSION_SYMBOLS = ["mercury_b200_mvs_advance", "mercury_b200_events", "mercury
                      "mercury_b200_hybrid_adjoint_backward", "mercury_b200_hybrid_adjoint_timing",
                      "mercury_b200_hybrid_adjoint_free", "mercury_b200_ejections",
                      "mercury_b200_encode_ce", "mercury_b200_set_step_reduce",
-                     "mercury_b200_encounter_run", "mercury_b200_hybrid_members"]
+                     "mercury_b200_encounter_run", "mercury_b200_hybrid_members", "mercury_b200_epoch_order",
+                     "mercury_b200_sync_epochs"]
 
 # fn(values, count, user) of mercury_b200_set_step_reduce
 REDUCE_FN = C.CFUNCTYPE(None, C.POINTER(C.c_double), C.c_int, C.c_void_p)
@@ -105,6 +106,8 @@ def load_library(path: Path | str | None = None) -> C.CDLL:
     L.mercury_b200_set_step_reduce.argtypes = [C.c_void_p, C.c_void_p]
     L.mercury_b200_encounter_run.argtypes = [D, D, D, D, PD, PI64, PI]
     L.mercury_b200_hybrid_members.argtypes = [PI, I]
+    L.mercury_b200_epoch_order.argtypes = [I, PD, D, PI]
+    L.mercury_b200_sync_epochs.argtypes = [PD, PD, D, D, D, PI]
     L.mercury_b200_batch_upload.argtypes = [I, PI, PI, PD, PD, PD, PD, PD, PD]
     L.mercury_b200_batch_advance.argtypes = [D, I, D, PI]
     L.mercury_b200_batch_events.argtypes = [C.c_void_p, PI, PI, I]
@@ -132,6 +135,16 @@ def load_library(path: Path | str | None = None) -> C.CDLL:
 def _p(a: np.ndarray):
     assert a.dtype == np.float64 and a.flags.c_contiguous, "float64 C-contiguous array required"
     return a.ctypes.data_as(PD)
+
+
+def epoch_order(epochs: np.ndarray, tstart: float, lib: C.CDLL | None = None) -> np.ndarray:
+    """mxx_sync's order of the Small bodies: order[k] = the Small body at position k."""
+    L = lib or load_library()
+    e = np.ascontiguousarray(epochs, dtype=np.float64)
+    order = np.zeros(max(1, len(e)), dtype=np.int32)
+    if L.mercury_b200_epoch_order(len(e), _p(e), tstart, order.ctypes.data_as(PI)) != 0:
+        raise BackendError("epoch ordering failed")
+    return order[:len(e)].copy()
 
 
 def encode_ce(events: np.ndarray, mcen: float, rcen: float, rmax: float, lib: C.CDLL | None = None) -> np.ndarray:
@@ -362,6 +375,15 @@ class Backend:
             self.lib.mercury_cuda_encounter_exit()
             self.n = outer_n
         return xbs, vbs, records
+
+    def sync_epochs(self, epoch: np.ndarray, time: float, h0: float, tol: float, dtout: float):
+        """mxx_sync's integration of the uploaded system (in its order, see
+        epoch_order): returns (the common epoch reached, BS steps)."""
+        ep = np.ascontiguousarray(epoch, dtype=np.float64)
+        t, steps = D(time), I(0)
+        if self.lib.mercury_b200_sync_epochs(_p(ep), C.byref(t), h0, tol, dtout, C.byref(steps)) != 0:
+            raise BackendError("epoch synchronisation failed")
+        return t.value, steps.value
 
     def hybrid_members(self, ids) -> None:
         """The bodies (0-based) whose rows hybrid_finish takes from x, v."""

@@ -455,6 +455,7 @@ void bs_step_once(double time, double* h, double* hdid, double tol, int64_t* rej
         a.adj_off = c.adj_off.p;
         a.adj = c.adj.p;
         a.perm = c.permp();
+        a.active_np = c.bs_active_np >= 0 ? std::min(c.bs_active_np, c.np) : c.np;
         launch_bs_sequence(a, c.stream);
         c.dropin_launches += 2 + (c.np > 0 ? 1 : 0);  // level CTAs, extrapolation, particles
         check(cudaGetLastError(), "launch");
@@ -496,6 +497,9 @@ void bs_step_once(double time, double* h, double* hdid, double tol, int64_t* rej
         k.bx = c.bigstate[in].p;
         k.bx_out = c.bigstate[out].p;
         k.px_out = c.pstate[out].p;
+        k.px = c.pstate[in].p;
+        k.perm = c.permp();
+        k.active_np = a.active_np;
         launch_bs_commit(k, c.stream);
         c.dropin_launches += 1;
         if (c.tangent && c.encounter && V == 2 && c.np > 0) {
@@ -1859,6 +1863,98 @@ int mercury_b200_encounter_run(double time, double h, double tol, double rcen, d
         c.event_order.clear();
         *forces = nforces;
         *nrecords = (int)c.host_events.size();
+        return 0;
+    } catch (const std::exception& e) {
+        return report(e);
+    }
+}
+
+// Fortran SPACING(x) for double x: 2^(EXPONENT(x) - 53), TINY for 0.
+static double fortran_spacing(double x) {
+    x = std::fabs(x);
+    if (x == 0.0) return 2.2250738585072014e-308;
+    int e = 0;
+    std::frexp(x, &e);
+    return std::ldexp(1.0, e - 53);
+}
+
+// mercury_support.f90:202-212: the tolerance of an epoch and a step towards it.
+static double epoch_epsilon(double t, double target) {
+    return std::max(1e-13, 2.0 * fortran_spacing(std::max(std::fabs(t), std::fabs(target))));
+}
+static double clipped_step(double t, double target, double proposed, double cap) {
+    const double step =
+        std::copysign(std::min(std::min(std::fabs(target - t), std::fabs(proposed)), std::fabs(cap)), target - t);
+    if (!std::isfinite(step) || t + step == t)
+        throw std::runtime_error("Timestep cannot advance the epoch; loosen tolerance or inspect the orbit");
+    return step;
+}
+
+int mercury_b200_epoch_order(int nsml, const double* epochs, double tstart, int* order) {
+    try {
+        if (nsml < 0 || (nsml > 0 && (!epochs || !order))) throw std::runtime_error("invalid epoch arrays");
+        // mxx_sort (mercury6_2.for:7392-7421): Shell sort with gaps 1, 4, 13, ...
+        std::vector<double> x(epochs, epochs + nsml);
+        std::vector<int> index(nsml);
+        for (int i = 0; i < nsml; ++i) index[i] = i;
+        int inc = 1;
+        while (inc < nsml / 3) inc = 3 * inc + 1;
+        while (inc >= 1) {
+            for (int i = inc; i < nsml; ++i) {
+                const double y = x[i];
+                const int iy = index[i];
+                int j = i;
+                while (j >= inc) {
+                    if (x[j - inc] <= y) break;
+                    x[j] = x[j - inc];
+                    index[j] = index[j - inc];
+                    j = j - inc;
+                }
+                x[j] = y;
+                index[j] = iy;
+            }
+            inc = inc / 3;
+        }
+        // mxx_sync (mercury6_2.for:7473-7486): the epoch furthest from tstart first
+        if (nsml > 0 && std::fabs(x[0] - tstart) < std::fabs(x[nsml - 1] - tstart))
+            for (int j = 0; j < nsml / 2; ++j) {
+                std::swap(x[j], x[nsml - 1 - j]);
+                std::swap(index[j], index[nsml - 1 - j]);
+            }
+        for (int i = 0; i < nsml; ++i) order[i] = index[i];
+        return 0;
+    } catch (const std::exception& e) {
+        return report(e);
+    }
+}
+
+int mercury_b200_sync_epochs(const double* epoch, double* time, double h0, double tol, double dtout, int* steps) {
+    Context& c = ctx();
+    try {
+        require_system();
+        if (c.algorithm != 2) throw std::runtime_error("epoch synchronisation needs algorithm 2 (mdt_bs1)");
+        if (c.nsplit != c.nbig) throw std::runtime_error("epoch synchronisation needs massless Small bodies");
+        struct Restore {
+            Context& c;
+            ~Restore() { c.bs_active_np = -1; }
+        } restore{c};
+        double t = *time, h = h0;
+        int count = 0;
+        // mxx_sync (mercury6_2.for:7556-7570): the bodies before Small body j
+        // are integrated by mdt_bs1 to j's epoch, then j joins
+        for (int j = c.nbig; j < c.n; ++j) {
+            c.bs_active_np = j - c.nbig;
+            while (std::fabs(t - epoch[j]) > epoch_epsilon(t, epoch[j])) {
+                h = clipped_step(t, epoch[j], h, dtout);
+                double hdid = 0.0;
+                int64_t rejected = 0;
+                bs_step_once(t, &h, &hdid, tol, &rejected);
+                t = t + hdid;
+                ++count;
+            }
+        }
+        *time = t;
+        if (steps) *steps = count;
         return 0;
     } catch (const std::exception& e) {
         return report(e);

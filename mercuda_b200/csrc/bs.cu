@@ -397,7 +397,7 @@ template <int VARIANT> __global__ void __launch_bounds__(bs_levels(VARIANT) * 16
     __shared__ double a0sm[3][32];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int p = blockIdx.x * 32 + lane;
-    const bool ok = p < A.np;
+    const bool ok = p < A.np && A.perm[p] < A.active_np;
     const int nb = A.f.nbig - 1, stride = force_row(nb), S = A.npcap;
     double3 x0 = make_double3(0.0, 0.0, 0.0), v0 = x0;
     double mj = 0.0, g5[5] = {0, 0, 0, 0, 0};
@@ -625,6 +625,10 @@ __global__ void __launch_bounds__(128) bs_commit_kernel(BsCommitArgs A) {
     }
     const int p = q - N;
     if (p >= A.np) return;
+    if (A.perm[p] >= A.active_np) {
+        for (int c = 0; c < 9; ++c) A.px_out[(size_t)c * S + p] = A.px[(size_t)c * S + p];
+        return;
+    }
     const double* cand = A.pcand + (size_t)A.cand * 6 * S;
     for (int c = 0; c < 6; ++c) A.px_out[(size_t)c * S + p] = cand[(size_t)c * S + p];
     for (int c = 6; c < 9; ++c) A.px_out[(size_t)c * S + p] = 0.0;

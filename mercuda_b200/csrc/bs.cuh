@@ -61,6 +61,7 @@ struct BsArgs {
     const int* adj_off;
     const int2* adj;
     const int* perm;             // slot -> particle index
+    int active_np;               // particles with index >= active_np sit the step out (epoch synchronisation)
 };
 
 struct BsCommitArgs {
@@ -71,6 +72,9 @@ struct BsCommitArgs {
     const double* bx;            // start-of-step state (central body row copied)
     double* bx_out;              // [9][nsplit]
     double* px_out;              // [9][npcap]
+    const double* px;            // start-of-step particle state (kept by inactive particles)
+    const int* perm;             // slot -> particle index
+    int active_np;               // as in BsArgs
 };
 
 void launch_bs_sequence(const BsArgs& a, cudaStream_t s);

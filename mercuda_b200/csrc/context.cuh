@@ -111,6 +111,8 @@ struct Context {
     bool encounter = false;
     DBuf<int> adj_off;
     DBuf<int2> adj;
+    // BS steps integrate only the particles with index < bs_active_np (-1: all)
+    int bs_active_np = -1;
     // with tangent set (HYBRID adjoint), every accepted BS2 step also advances
     // the massless members' 6x6 Jacobians tg [36][npcap]
     bool tangent = false;

@@ -95,6 +95,10 @@ def lib() -> C.CDLL:
         L.oracle_mxx_ejec.restype = I
         L.oracle_mio_ce.argtypes = [C.c_void_p, I, D, D, D, C.c_void_p]
         L.oracle_mio_ce.restype = I
+        L.oracle_epoch_order.argtypes = [I, PD, D, C.POINTER(I)]
+        L.oracle_epoch_order.restype = I
+        L.oracle_mxx_sync.argtypes = [I, I, PD, PD, PD, PD, I, I, PD, PD, PD, D, D, D, C.POINTER(I)]
+        L.oracle_mxx_sync.restype = I
         L.oracle_mxx_en.argtypes = [I, PD, PD, PD, C.c_void_p, PD, PD]
         L.oracle_mxx_en.restype = None
         _lib = L
@@ -345,6 +349,28 @@ def mio_ce(events, mcen, rcen, rmax):
     k = lib().oracle_mio_ce(ev.ctypes.data_as(C.c_void_p), len(ev), float(mcen), float(rcen), float(rmax),
                             lines.ctypes.data_as(C.c_void_p))
     return lines[:k].copy()
+
+
+def epoch_order(epochs, tstart):
+    """mxx_sync's order of the Small bodies (mxx_sort, then furthest from tstart first)."""
+    e = _f64(epochs)
+    order = np.zeros(max(1, len(e)), dtype=np.int32)
+    lib().oracle_epoch_order(len(e), _p(e), float(tstart), order.ctypes.data_as(C.POINTER(I)))
+    return order[:len(e)].copy()
+
+
+def mxx_sync(sys, epoch, time, h0, tol, dtout):
+    """mxx_sync's integration on sys (bodies already in its order, in place):
+    returns (final time, BS steps)."""
+    s = sys
+    t = D(float(time))
+    steps = I(0)
+    ep = _f64(epoch)
+    rc = lib().oracle_mxx_sync(s.n, s.nbig, _p(s.m), _p(s.x), _p(s.v), _p(s.ngf), s.ngflag, int(s.pn), _p(s.jcen),
+                               _p(ep), C.byref(t), float(h0), float(tol), float(dtout), C.byref(steps))
+    if rc:
+        raise RuntimeError("oracle mxx_sync failed")
+    return t.value, steps.value
 
 
 def mxx_en(m, x, v, jcen, spin=None):

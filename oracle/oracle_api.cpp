@@ -541,6 +541,84 @@ int oracle_mio_ce(const Event* ev, int n, double mcen, double rcen, double rmax,
     return k;
 }
 
+// mxx_sync's ordering (mercury6_2.for:7468-7486 with mxx_sort, 7392-7421):
+// Small bodies by epoch (Shell sort, gaps 1, 4, 13, ...), reversed when the
+// last is further from tstart than the first. order[k] = the 0-based Small
+// body at position k.
+int oracle_epoch_order(int nsml, const double* epochs, double tstart, int* order) {
+    std::vector<double> epsml(epochs, epochs + nsml);
+    std::vector<int> indx(nsml);
+    for (int i = 1; i <= nsml; ++i) indx[i - 1] = i;
+    int inc = 1;
+    while (inc < nsml / 3) inc = 3 * inc + 1;
+    while (inc >= 1) {
+        for (int i = inc + 1; i <= nsml; ++i) {
+            const double y = epsml[i - 1];
+            const int iy = indx[i - 1];
+            int j = i;
+            while (j > inc) {
+                if (epsml[j - inc - 1] <= y) break;
+                epsml[j - 1] = epsml[j - inc - 1];
+                indx[j - 1] = indx[j - inc - 1];
+                j = j - inc;
+            }
+            epsml[j - 1] = y;
+            indx[j - 1] = iy;
+        }
+        inc = inc / 3;
+    }
+    if (nsml > 0 && std::fabs(epsml[0] - tstart) < std::fabs(epsml[nsml - 1] - tstart)) {
+        const int k = nsml + 1;
+        for (int j = 1; j <= nsml / 2; ++j) {
+            const int l = k - j;
+            std::swap(epsml[j - 1], epsml[l - 1]);
+            std::swap(indx[j - 1], indx[l - 1]);
+        }
+    }
+    for (int i = 0; i < nsml; ++i) order[i] = indx[i] - 1;
+    return 0;
+}
+
+// mxx_sync's integration (mercury6_2.for:7556-7570) on bodies already in its
+// order: for each Small body j, the bodies before it are advanced by mdt_bs1
+// to j's epoch (steps clipped by mercury_support.f90:207-212, epochs matched
+// within 202-205). *time: in the Big bodies' epoch, out the last epoch.
+// Returns nonzero on a failure; *steps counts the BS steps.
+int oracle_mxx_sync(int n, int nbig, const double* m, double* x, double* v, const double* ngf, int ngflag, int pn,
+                    const double* jcen, const double* epoch, double* time, double h0, double tol, double dtout,
+                    int* steps) {
+    auto spacing = [](double a) {
+        a = std::fabs(a);
+        if (a == 0.0) return 2.2250738585072014e-308;
+        int e = 0;
+        std::frexp(a, &e);
+        return std::ldexp(1.0, e - 53);
+    };
+    auto eps = [&](double t, double target) {
+        return std::max(1e-13, 2.0 * spacing(std::max(std::fabs(t), std::fabs(target))));
+    };
+    double t = *time, h = h0;
+    int count = 0;
+    for (int j = nbig + 1; j <= n; ++j) {
+        const int nsofar = j - 1;
+        while (std::fabs(t - epoch[j - 1]) > eps(t, epoch[j - 1])) {
+            const double target = epoch[j - 1];
+            const double step = std::copysign(
+                std::min(std::min(std::fabs(target - t), std::fabs(h)), std::fabs(dtout)), target - t);
+            if (!std::isfinite(step) || t + step == t) return 1;
+            h = step;
+            double hdid = 0.0;
+            if (oracle::mdt_bs1(t, h, hdid, tol, jcen, nsofar, nbig, m, x, v, ngf, ngflag, pn, nullptr, nullptr))
+                return 1;
+            t = t + hdid;
+            ++count;
+        }
+    }
+    *time = t;
+    *steps = count;
+    return 0;
+}
+
 // mxx_en of n bodies (Fortran layout); s may be null. out = {e, l2}.
 void oracle_mxx_en(int n, const double* m, const double* xh, const double* vh, const double* s, const double* jcen,
                    double* out) {
