@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <thread>
 
 #include "../../include/mercury_b200.h"
 #include "context.cuh"
@@ -769,13 +770,25 @@ void order_particles(int n, int nbig, double mu, const double* xx, const double*
     Context& c = ctx();
     const int np = n - nbig;
     std::vector<int> bucket(np), count(257, 0), perm(c.npcap), inv(c.npcap);
-    for (int p = 0; p < np; ++p) {
-        const double* x = xx + 3 * (size_t)(nbig + p);
-        const double* v = vv + 3 * (size_t)(nbig + p);
-        const int b = path_bucket(x[0], x[1], x[2], v[0], v[1], v[2], mu);
-        bucket[p] = b;
-        count[b + 1]++;
+    // the keys on the host's cores (a million particles take ~0.1 s on one)
+    auto keys = [&](int lo, int hi) {
+        for (int p = lo; p < hi; ++p) {
+            const double* x = xx + 3 * (size_t)(nbig + p);
+            const double* v = vv + 3 * (size_t)(nbig + p);
+            bucket[p] = path_bucket(x[0], x[1], x[2], v[0], v[1], v[2], mu);
+        }
+    };
+    const int nthreads = np < 65536 ? 1 : (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    if (nthreads == 1) {
+        keys(0, np);
+    } else {
+        std::vector<std::thread> pool;
+        const int chunk = (np + nthreads - 1) / nthreads;
+        for (int k = 0; k < nthreads; ++k)
+            pool.emplace_back(keys, std::min(np, k * chunk), std::min(np, (k + 1) * chunk));
+        for (auto& th : pool) th.join();
     }
+    for (int p = 0; p < np; ++p) count[bucket[p] + 1]++;
     for (int k = 0; k < 256; ++k) count[k + 1] += count[k];
     for (int p = 0; p < np; ++p) {
         const int slot = count[bucket[p]]++;
@@ -977,9 +990,24 @@ void order_events(const std::vector<MercuryEvent>& ev, const std::vector<int>* s
             items[fill[steps ? (size_t)(*steps)[k] : 0]++] = Item{key, (uint32_t)k};
         }
     }
-    for (size_t s = 0; s + 1 < first.size(); ++s)
-        std::sort(items.begin() + first[s], items.begin() + first[s + 1],
-                  [](const Item& a, const Item& b) { return a.key < b.key || (a.key == b.key && a.k < b.k); });
+    // the steps' runs are independent: sort them on the host's cores
+    const size_t nruns = first.size() - 1;
+    auto sort_runs = [&](size_t lo, size_t hi) {
+        for (size_t s = lo; s < hi; ++s)
+            std::sort(items.begin() + first[s], items.begin() + first[s + 1],
+                      [](const Item& a, const Item& b) { return a.key < b.key || (a.key == b.key && a.k < b.k); });
+    };
+    const size_t nthreads =
+        n < 262144 ? 1 : std::max<size_t>(1, std::min<size_t>({16, std::thread::hardware_concurrency(), nruns}));
+    if (nthreads == 1) {
+        sort_runs(0, nruns);
+    } else {
+        std::vector<std::thread> pool;
+        const size_t chunk = (nruns + nthreads - 1) / nthreads;
+        for (size_t k = 0; k < nthreads; ++k)
+            pool.emplace_back(sort_runs, std::min(nruns, k * chunk), std::min(nruns, (k + 1) * chunk));
+        for (auto& th : pool) th.join();
+    }
     for (size_t q = 0; q < n; ++q) order[q] = items[q].k;
 }
 
