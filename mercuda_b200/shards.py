@@ -182,11 +182,16 @@ def step_reduce(ranks: Ranks):
     def reduce(ptr, count, user):
         if ranks.dist is None:
             return
-        import torch
         vals = np.ctypeslib.as_array(ptr, shape=(count,))
-        t = torch.tensor(vals, dtype=torch.float64, device=ranks.device)
-        ranks.dist.all_reduce(t, op=ranks.dist.ReduceOp.MAX)
-        vals[:] = t.cpu().numpy()
+        try:
+            import torch
+            t = torch.tensor(vals, dtype=torch.float64, device=ranks.device)
+            ranks.dist.all_reduce(t, op=ranks.dist.ReduceOp.MAX)
+            vals[:] = t.cpu().numpy()
+        except Exception:  # noqa: BLE001 - an exception cannot cross the C callback
+            # a failed exchange must not let this rank decide alone: +inf makes
+            # the library fail the step loudly
+            vals[:] = np.inf
 
     return REDUCE_FN(reduce)
 
