@@ -424,8 +424,9 @@ class Backend:
         nev = I(0)
         if self.lib.mercury_b200_mvs_advance(time, h, int(nsteps), rcen, int(steps_per_launch), C.byref(nev)) != 0:
             raise BackendError("CUDA integration step failed")
-        events = np.zeros(nev.value, dtype=EVENT_DTYPE)
-        steps = np.zeros(nev.value, dtype=np.int32)
+        # every record is written by the library: no need to clear the arrays
+        events = np.empty(nev.value, dtype=EVENT_DTYPE)
+        steps = np.empty(nev.value, dtype=np.int32)
         if nev.value:
             self.lib.mercury_b200_events(events.ctypes.data_as(C.c_void_p), steps.ctypes.data_as(PI), nev.value)
         return events, steps
