@@ -3,12 +3,16 @@
 // velocities, 12 levels, mercury6_2.for:3428-3596), with force = mfo_all.
 //
 // The Fortran stops at the first level n > 3 whose global error passes; that
-// decision needs the maximum over every body. One launch pair computes every
-// level instead: the massive-set CTA writes a force table row per force call
-// and the particle kernel runs all levels per particle with its extrapolation
-// table in shared memory, each reducing a per-level error maximum and storing
-// the level's extrapolated state. The host then takes the first passing level
-// (or halves the step) and a commit pass copies that level's state.
+// decision needs the maximum over every body. One sequence of launches
+// computes every level instead, the levels side by side (they are independent
+// given the start-of-step state and force): one massive-set CTA per level
+// writes that level's force table rows and raw state, an extrapolation pass
+// runs the massive set's Neville updates in level order, and the particle
+// kernel gives each warp a balanced pair of levels for 32 particles, then
+// extrapolates in level order. Each reduces a per-level error maximum and
+// stores the level's extrapolated state. The host then takes the first
+// passing level (or halves the step) and a commit pass copies that level's
+// state.
 #pragma once
 #include "allforce.cuh"
 #include "common.cuh"
