@@ -266,7 +266,12 @@ void particles_and_events(const MvsParticleArgs& pa, cudaStream_t s) {
 // Grows the event or candidate buffer after an overflow flagged in the status.
 void grow_after_overflow() {
     Context& c = ctx();
-    if (c.status_host->overflow & 1) ensure_events(std::max(2 * (int)c.events.n, c.status_host->events + 1024));
+    // a quarter of headroom: the next run of a similar system rarely needs more
+    if (c.status_host->overflow & 1) {
+        const long long need = c.status_host->events;
+        ensure_events((int)std::min<long long>(INT32_MAX / 2, std::max<long long>(2LL * c.events.n,
+                                                                                   need + need / 4 + 1024)));
+    }
     if (c.status_host->overflow & 2) {
         c.cands.reserve(2 * c.cands.n + 4096);
     }
@@ -1109,6 +1114,7 @@ int mercury_cuda_upload(int n, int nbig, int pn, int ngflag, const double* m, co
         c.ngflag = ngflag;
         for (int k = 0; k < 3; ++k) c.jcen[k] = jcen[k];
         c.m_host.assign(m, m + n);
+        c.event_rate = 0.0;
         c.mbig.reserve(ns);
         c.rcebig.reserve(ns);
         c.rphysbig.reserve(ns);
@@ -1592,6 +1598,15 @@ int mercury_b200_mvs_advance(double time, double h, int nsteps, double rcen, int
         const int nchunks = (nsteps + K - 1) / K;
         const int stride = tab_stride(nb);
         ensure_tables(nsteps + nchunks, nsteps);
+        // room for this run's records at the rate the earlier runs showed, so
+        // that a long run is not redone after an event-buffer overflow
+        if (c.event_rate > 0.0) {
+            const double want = c.event_rate * nsteps * 1.25 + 1024.0;
+            size_t free_b = 0, total_b = 0;
+            if (want > (double)c.events.n && cudaMemGetInfo(&free_b, &total_b) == cudaSuccess &&
+                want * (sizeof(MercuryEvent) + sizeof(int)) < 0.25 * (double)free_b)
+                ensure_events((int)want);
+        }
         if ((int)c.chunk_done.size() < nchunks) {
             size_t old = c.chunk_done.size();
             c.chunk_done.resize(nchunks);
@@ -1686,6 +1701,7 @@ int mercury_b200_mvs_advance(double time, double h, int nsteps, double rcen, int
         c.stepped = false;  // per-step event/previous semantics do not apply after a multi-step run
         c.pair_events = 0;
         const int nev = c.status_host->events;
+        c.event_rate = std::max(c.event_rate, (double)nev / nsteps);
         c.host_events.resize(nev);
         c.host_steps.resize(nev);
         if (nev) {

@@ -126,6 +126,7 @@ struct Context {
     std::vector<MercuryEvent> host_events;
     std::vector<int> host_steps;
     std::vector<uint32_t> event_order;   // last advance: host_events in (step, min, max) order
+    double event_rate = 0.0;             // most event records per step seen by an advance of this system
     int pair_events = 0;
     // staging
     DBuf<double> transfer;
@@ -198,6 +199,7 @@ struct Context {
         host_events.clear();
         host_steps.clear();
         event_order.clear();
+        event_rate = 0.0;
         n = nbig = np = npcap = 0;
         stepped = false;
         reset = true;
