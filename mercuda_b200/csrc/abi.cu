@@ -1600,8 +1600,12 @@ int mercury_b200_mvs_advance(double time, double h, int nsteps, double rcen, int
         ensure_tables(nsteps + nchunks, nsteps);
         // room for this run's records at the rate the earlier runs showed, so
         // that a long run is not redone after an event-buffer overflow
-        if (c.event_rate > 0.0) {
-            const double want = c.event_rate * nsteps * 1.25 + 1024.0;
+        {
+            // without history, room for encounters of 0.1 % of the particles per step
+            // (at most 2^24 records on a guess)
+            const double rate = c.event_rate > 0.0 ? c.event_rate * 1.25 : c.np * 1e-3;
+            double want = rate * nsteps + 1024.0;
+            if (c.event_rate <= 0.0) want = std::min(want, 16777216.0);
             size_t free_b = 0, total_b = 0;
             if (want > (double)c.events.n && cudaMemGetInfo(&free_b, &total_b) == cudaSuccess &&
                 want * (sizeof(MercuryEvent) + sizeof(int)) < 0.25 * (double)free_b)
