@@ -1741,10 +1741,22 @@ int mercury_b200_events(MercuryEvent* dst, int* steps, int cap) {
     const int nev = (int)c.host_events.size();
     const int k = std::max(0, std::min(cap, nev));
     const bool ordered = c.event_order.size() == c.host_events.size();
-    for (int q = 0; q < k; ++q) {
-        const size_t r = ordered ? c.event_order[q] : (size_t)q;
-        dst[q] = c.host_events[r];
-        if (steps && r < c.host_steps.size()) steps[q] = c.host_steps[r];
+    auto copy = [&](int lo, int hi) {
+        for (int q = lo; q < hi; ++q) {
+            const size_t r = ordered ? c.event_order[q] : (size_t)q;
+            dst[q] = c.host_events[r];
+            if (steps && r < c.host_steps.size()) steps[q] = c.host_steps[r];
+        }
+    };
+    // a few hundred MB for a long run: gather on the host's cores
+    const int nthreads = k < (1 << 18) ? 1 : (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    if (nthreads == 1) {
+        copy(0, k);
+    } else {
+        std::vector<std::thread> pool;
+        const int chunk = (k + nthreads - 1) / nthreads;
+        for (int w = 0; w < nthreads; ++w) pool.emplace_back(copy, std::min(k, w * chunk), std::min(k, (w + 1) * chunk));
+        for (auto& th : pool) th.join();
     }
     return nev;
 }
