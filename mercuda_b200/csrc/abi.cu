@@ -988,11 +988,45 @@ void order_events(const std::vector<MercuryEvent>& ev, const std::vector<int>* s
     }
     std::vector<Item> items(n);
     {
-        std::vector<size_t> fill(first.begin(), first.end() - 1);
-        for (size_t k = 0; k < n; ++k) {
-            const MercuryEvent& e = ev[k];
-            const uint64_t key = ((uint64_t)(uint32_t)std::min(e.i, e.j) << 32) | (uint32_t)std::max(e.i, e.j);
-            items[fill[steps ? (size_t)(*steps)[k] : 0]++] = Item{key, (uint32_t)k};
+        // stable scatter by step; with several threads each takes a contiguous
+        // chunk of records and its own slice of every step's run (chunk order)
+        const size_t nb = first.size() - 1;
+        const size_t nthreads =
+            (!steps || n < 262144) ? 1 : std::max<size_t>(1, std::min<size_t>(16, std::thread::hardware_concurrency()));
+        const size_t chunk = (n + nthreads - 1) / nthreads;
+        std::vector<std::vector<size_t>> fill(nthreads, std::vector<size_t>(nb, 0));
+        if (nthreads == 1) {
+            for (size_t s = 0; s < nb; ++s) fill[0][s] = first[s];
+        } else {
+            auto count = [&](size_t t) {
+                for (size_t k = t * chunk; k < std::min(n, (t + 1) * chunk); ++k) ++fill[t][(size_t)(*steps)[k]];
+            };
+            std::vector<std::thread> pool;
+            for (size_t w = 0; w < nthreads; ++w) pool.emplace_back(count, w);
+            for (auto& th : pool) th.join();
+            for (size_t s = 0; s < nb; ++s) {
+                size_t at = first[s];
+                for (size_t w = 0; w < nthreads; ++w) {
+                    const size_t c = fill[w][s];
+                    fill[w][s] = at;
+                    at += c;
+                }
+            }
+        }
+        auto scatter = [&](size_t t) {
+            std::vector<size_t>& f = fill[t];
+            for (size_t k = t * chunk; k < std::min(n, (t + 1) * chunk); ++k) {
+                const MercuryEvent& e = ev[k];
+                const uint64_t key = ((uint64_t)(uint32_t)std::min(e.i, e.j) << 32) | (uint32_t)std::max(e.i, e.j);
+                items[f[steps ? (size_t)(*steps)[k] : 0]++] = Item{key, (uint32_t)k};
+            }
+        };
+        if (nthreads == 1) {
+            scatter(0);
+        } else {
+            std::vector<std::thread> pool;
+            for (size_t w = 0; w < nthreads; ++w) pool.emplace_back(scatter, w);
+            for (auto& th : pool) th.join();
         }
     }
     // the steps' runs are independent: sort them on the host's cores
