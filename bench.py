@@ -198,7 +198,72 @@ def run_reference(args, rank):
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    gpu = reference_cuda_rate(args)
+    if gpu is not None:
+        line["reference_cuda"] = gpu
     print(json.dumps(line), flush=True)
+
+
+REF_CUDA = Path(__file__).resolve().parent / "oracle" / "_ref" / "libmercury_cuda_ref.so"
+DROPIN_STEPS = 46
+
+
+def dropin_steps(lib, sysw, nsteps, warm=2):
+    """Upload sysw and time nsteps drop-in MVS steps (mercury_cuda_step +
+    mercury_cuda_events per step, as mal_hcon makes them) by wall clock: the
+    calls are synchronous. Returns particle-steps/s of the massless bodies."""
+    import ctypes
+    D_, I_ = ctypes.c_double, ctypes.c_int
+    PD_ = ctypes.POINTER(D_)
+    lib.mercury_cuda_upload.argtypes = [I_, I_, I_, I_, PD_, PD_, PD_, PD_, PD_, PD_, PD_]
+    lib.mercury_cuda_step.argtypes = [D_, PD_, PD_, D_, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]
+    lib.mercury_cuda_events.argtypes = [D_, D_, D_, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(I_)]
+    lib.mercury_cuda_reset.argtypes = [I_]
+    lib.mercury_cuda_reset.restype = None
+    lib.mercury_cuda_free.restype = None
+    arrays = [np.ascontiguousarray(a, dtype=np.float64) for a in (sysw.m, sysw.x, sysw.v, sysw.ngf, sysw.jcen,
+                                                                  sysw.rce, sysw.rphys)]
+    ptr = [a.ctypes.data_as(PD_) for a in arrays]
+    if lib.mercury_cuda_configure(1) != 0 or lib.mercury_cuda_upload(sysw.n, sysw.nbig, 0, sysw.ngflag, *ptr) != 0:
+        raise RuntimeError("drop-in upload failed")
+    t, t0 = 0.0, None
+    for k in range(warm + nsteps):
+        if k == warm:
+            t0 = time.perf_counter()
+        lib.mercury_cuda_reset(0 if k == 0 else 2)
+        hh, hd = D_(H), D_(0.0)
+        nf, nr = ctypes.c_int64(0), ctypes.c_int64(0)
+        if lib.mercury_cuda_step(t, ctypes.byref(hh), ctypes.byref(hd), 0.0, ctypes.byref(nf), ctypes.byref(nr)):
+            raise RuntimeError("drop-in step failed")
+        evp, cnt = ctypes.c_void_p(), I_(0)
+        if lib.mercury_cuda_events(t + H, H, RCEN, ctypes.byref(evp), ctypes.byref(cnt)):
+            raise RuntimeError("drop-in events failed")
+        t = t + H
+    dt = time.perf_counter() - t0
+    lib.mercury_cuda_free()
+    return (sysw.n - sysw.nbig) * nsteps / dt
+
+
+def reference_cuda_rate(args):
+    """The reference's own CUDA backend (its mercury_cuda.cu built unchanged
+    for sm_100a into oracle/_ref by oracle/Makefile's ref target) stepping the
+    same workload on this GPU through its C ABI, one drop-in step and events
+    call per step: the existing GPU code this path replaces. None without a
+    GPU or without the built library."""
+    if not REF_CUDA.exists():
+        return None
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return None
+    except ImportError:
+        return None
+    import ctypes
+    lib = ctypes.CDLL(str(REF_CUDA))
+    value = dropin_steps(lib, workload(args.particles, args.seed), DROPIN_STEPS)
+    return {"value": value, "unit": UNIT, "steps": DROPIN_STEPS, "particles": args.particles,
+            "note": "the reference's CUDA backend on this GPU: mercury_cuda_step + mercury_cuda_events per step, "
+                    "wall clock (synchronous calls)"}
 
 
 ADAPTIVE = {"radau": ("RADAU", 4), "bs": ("BS", 2), "bs2": ("BS2", 3)}
@@ -803,6 +868,12 @@ def main():
         e2e = {"value": world * args.particles * args.steps / e2e_s, "unit": UNIT,
                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                "note": "wall clock around the synchronous C-ABI calls: upload, fused run, download, events"}
+    dropin = None
+    if world == 1:
+        # like for like with the reference's CUDA backend (its arm's
+        # reference_cuda): one drop-in step and events call per step
+        dropin = {"value": dropin_steps(b.lib, workload(args.particles, args.seed), DROPIN_STEPS), "unit": UNIT,
+                  "steps": DROPIN_STEPS, "note": "mercury_cuda_step + mercury_cuda_events per step, wall clock"}
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -838,6 +909,8 @@ def main():
             "e2e": e2e,
             "cpu_baseline": cpu,
         }
+        if dropin is not None:
+            line["dropin_per_step"] = dropin
         print(json.dumps(line), flush=True)
     b.free()
     if dist:
