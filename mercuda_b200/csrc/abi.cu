@@ -259,6 +259,7 @@ void particles_and_events(const MvsParticleArgs& pa, cudaStream_t s) {
     ca.event_step = c.event_step.p;
     ca.event_cap = (int)c.events.n;
     ca.status = c.status.p;
+    ca.step_base = 0;
     if (ca.nb > 0) launch_classify(ca, s);
     check(cudaMemsetAsync(&c.status.p->cands, 0, sizeof(int), s), "memset");
 }
@@ -577,6 +578,7 @@ void screen_pairs(double h) {
             ca.event_step = c.event_step.p;
             ca.event_cap = (int)c.events.n;
             ca.status = c.status.p;
+            ca.step_base = 0;
             launch_classify(ca, c.stream);
         }
         check(cudaGetLastError(), "screen");
@@ -810,25 +812,32 @@ void order_particles(int n, int nbig, double mu, const double* xx, const double*
 }
 
 // Device re-ordering of the slots as the state evolves (scattered or eccentric
-// particles move to the Newton path): a stable partition, for the step size h
-// of the coming launch, into the slots whose drift takes the Newton solver
-// (unbound, e > 0.6, or max(e n/0.04, n/0.4)·|h| >= 1) followed by the rest.
-// Warp ballots give in-block ranks and one scan gives block offsets, so the
-// pass is deterministic, atomic-free and writes contiguous runs.
-__device__ __forceinline__ bool newton_path(const double* x, int S, int s, double mu, double absh) {
+// particles move to the universal-variable solver): a stable partition, for
+// the step size h of the coming launch, by the drift path of drift_dan
+// (mercury6_2.for:7637-7685) so that a warp's 32 particles take one path:
+//   0  unbound (drift_kepu_p3solve guess, hyperbolic Stumpff series)
+//   1  bound, e > 0.6 (drift_kepu with the sine guess, most iterations)
+//   2  bound, e <= 0.6, max(e n/0.04, n/0.4)·|h| >= 1 (drift_kepu)
+//   3  the rest (drift_kepmd, no iteration)
+// Buckets 0-2 lead so that the particle kernel's dynamic tiles take the slow
+// slots first. Warp ballots give in-block ranks and one scan per bucket gives
+// block offsets, so the pass is deterministic, atomic-free and writes
+// contiguous runs.
+constexpr int PATH_BUCKETS = 4;
+__device__ __forceinline__ int drift_bucket(const double* x, int S, int s, double mu, double absh) {
     const double x0 = x[s], x1 = x[S + s], x2 = x[2 * S + s];
     const double v0 = x[3 * S + s], v1 = x[4 * S + s], v2 = x[5 * S + s];
     const double r = sqrt(x0 * x0 + x1 * x1 + x2 * x2);
     const double vv = v0 * v0 + v1 * v1 + v2 * v2;
     const double u = x0 * v0 + x1 * v1 + x2 * v2;
     const double alpha = 2.0 * mu / r - vv;
-    if (!(alpha > 0.0)) return true;
+    if (!(alpha > 0.0)) return 0;
     const double a = mu / alpha;
     const double en = sqrt(mu / (a * a * a));
     const double ec = 1.0 - r / a, es = u / (en * a * a);
     const double e = sqrt(ec * ec + es * es);
-    if (!(e <= 0.6)) return true;
-    return fmax(e * en / 0.04, en / 0.4) * absh >= 1.0;
+    if (!(e <= 0.6)) return 1;
+    return fmax(e * en / 0.04, en / 0.4) * absh >= 1.0 ? 2 : 3;
 }
 
 struct PartitionArgs {
@@ -841,9 +850,8 @@ struct PartitionArgs {
     const int* pin;
     int* pout;
     int* inv;
-    int* bslow;  // [nblk] Newton-path count per block, then exclusive offsets
-    int* bfast;  // [nblk] the other count, then exclusive offsets
-    int* total;  // [1] Newton-path total
+    int* hist;   // [PATH_BUCKETS][nblk] per-block counts, then exclusive offsets within the bucket
+    int* base;   // [PATH_BUCKETS] first slot of each bucket
 };
 
 constexpr int PART_THREADS = 256;
@@ -872,57 +880,74 @@ __device__ __forceinline__ int block_rank(bool flag, int* nset) {
 __global__ void __launch_bounds__(PART_THREADS) partition_count_kernel(PartitionArgs A) {
     const int s = blockIdx.x * PART_THREADS + threadIdx.x;
     const bool valid = s < A.np;
-    const bool slow = valid && newton_path(A.xin, A.npcap, s, A.mu, A.absh);
-    int nslow;
-    block_rank(slow, &nslow);
-    if (threadIdx.x == 0) {
-        const int nvalid = min(PART_THREADS, A.np - blockIdx.x * PART_THREADS);
-        A.bslow[blockIdx.x] = nslow;
-        A.bfast[blockIdx.x] = nvalid - nslow;
+    const int key = valid ? drift_bucket(A.xin, A.npcap, s, A.mu, A.absh) : -1;
+    for (int b = 0; b < PATH_BUCKETS; ++b) {
+        int n;
+        block_rank(key == b, &n);
+        if (threadIdx.x == 0) A.hist[b * A.nblk + blockIdx.x] = n;
     }
 }
 
-// Exclusive scans of the per-block counts (one CTA of 1024 threads).
+// Exclusive scans of the per-block counts of every bucket and the buckets'
+// first slots (one CTA of 1024 threads: per-thread runs, warp shuffles, one
+// warp over the warp totals).
 __global__ void __launch_bounds__(1024) partition_scan_kernel(PartitionArgs A) {
-    __shared__ int sum_slow[1024], sum_fast[1024];
-    const int t = threadIdx.x, per = (A.nblk + 1023) / 1024;
-    const int lo = t * per, hi = min(A.nblk, lo + per);
-    int a = 0, b = 0;
-    for (int k = lo; k < hi; ++k) { a += A.bslow[k]; b += A.bfast[k]; }
-    sum_slow[t] = a;
-    sum_fast[t] = b;
-    __syncthreads();
-    if (t == 0) {
-        int ra = 0, rb = 0;
-        for (int k = 0; k < 1024; ++k) {
-            const int xa = sum_slow[k], xb = sum_fast[k];
-            sum_slow[k] = ra;
-            sum_fast[k] = rb;
-            ra += xa;
-            rb += xb;
+    __shared__ int warp_sum[32];
+    __shared__ int bucket_total[PATH_BUCKETS];
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    const int per = (A.nblk + 1023) / 1024;
+    const int lo = min(A.nblk, t * per), hi = min(A.nblk, lo + per);
+    for (int b = 0; b < PATH_BUCKETS; ++b) {
+        int* h = A.hist + (size_t)b * A.nblk;
+        int run = 0;
+        for (int k = lo; k < hi; ++k) run += h[k];
+        int incl = run;
+        for (int d = 1; d < 32; d <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= d) incl += y;
         }
-        *A.total = ra;
+        if (lane == 31) warp_sum[w] = incl;
+        __syncthreads();
+        if (w == 0) {
+            const int mine = warp_sum[lane];
+            int wincl = mine;
+            for (int d = 1; d < 32; d <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, wincl, d);
+                if (lane >= d) wincl += y;
+            }
+            warp_sum[lane] = wincl - mine;
+            if (lane == 31) bucket_total[b] = wincl;
+        }
+        __syncthreads();
+        int off = warp_sum[w] + incl - run;
+        for (int k = lo; k < hi; ++k) {
+            const int x = h[k];
+            h[k] = off;
+            off += x;
+        }
+        __syncthreads();
     }
-    __syncthreads();
-    a = sum_slow[t];
-    b = sum_fast[t];
-    for (int k = lo; k < hi; ++k) {
-        const int xa = A.bslow[k], xb = A.bfast[k];
-        A.bslow[k] = a;
-        A.bfast[k] = b;
-        a += xa;
-        b += xb;
+    if (t == 0) {
+        int acc = 0;
+        for (int b = 0; b < PATH_BUCKETS; ++b) {
+            A.base[b] = acc;
+            acc += bucket_total[b];
+        }
     }
 }
 
 __global__ void __launch_bounds__(PART_THREADS) partition_scatter_kernel(PartitionArgs A) {
     const int s = blockIdx.x * PART_THREADS + threadIdx.x;
     const bool valid = s < A.np;
-    const bool slow = valid && newton_path(A.xin, A.npcap, s, A.mu, A.absh);
-    int nslow;
-    const int rank = block_rank(slow, &nslow);
+    const int key = valid ? drift_bucket(A.xin, A.npcap, s, A.mu, A.absh) : -1;
+    int rank = 0;
+    for (int b = 0; b < PATH_BUCKETS; ++b) {
+        int n;
+        const int r = block_rank(key == b, &n);
+        if (key == b) rank = r;
+    }
     if (!valid) return;
-    const int ns = slow ? A.bslow[blockIdx.x] + rank : *A.total + A.bfast[blockIdx.x] + rank;
+    const int ns = A.base[key] + A.hist[key * A.nblk + blockIdx.x] + rank;
     const size_t S = A.npcap;
     for (int c = 0; c < 9; ++c) A.xout[c * S + ns] = A.xin[c * S + s];
     for (int c = 0; c < PCONST_ROWS; ++c) A.cout[c * S + ns] = A.cin[c * S + s];
@@ -939,7 +964,7 @@ int reorder_slots(int src, double h, cudaStream_t st) {
     c.steps_since_order = 0;
     if (c.np < 64) return src;
     const int nblk = (c.np + PART_THREADS - 1) / PART_THREADS;
-    c.order_hist.reserve((size_t)2 * nblk + 1);
+    c.order_hist.reserve((size_t)PATH_BUCKETS * nblk + PATH_BUCKETS);
     PartitionArgs a;
     a.np = c.np;
     a.npcap = c.npcap;
@@ -953,9 +978,8 @@ int reorder_slots(int src, double h, cudaStream_t st) {
     a.pin = c.perm[c.kc].p;
     a.pout = c.perm[1 - c.kc].p;
     a.inv = c.inv.p;
-    a.bslow = c.order_hist.p;
-    a.bfast = c.order_hist.p + nblk;
-    a.total = c.order_hist.p + 2 * nblk;
+    a.hist = c.order_hist.p;
+    a.base = c.order_hist.p + (size_t)PATH_BUCKETS * nblk;
     c.dropin_launches += 3;
     partition_count_kernel<<<nblk, PART_THREADS, 0, st>>>(a);
     partition_scan_kernel<<<1, 1024, 0, st>>>(a);

@@ -694,7 +694,7 @@ __global__ void __launch_bounds__(256) classify_kernel(ClassifyArgs A) {
         const int slot = atomicAdd(&A.status->events, 1);
         if (slot < A.event_cap) {
             pair_record(A.events + slot, I, J, pc, hm1, c.body + 2, c.id, false);
-            A.event_step[slot] = c.step;
+            A.event_step[slot] = c.step + A.step_base;
         } else {
             atomicOr(&A.status->overflow, 1);
         }

@@ -177,6 +177,7 @@ struct ClassifyArgs {
     int* event_step;
     int event_cap;
     DeviceStatus* status;
+    int step_base;         // added to a candidate's step in event_step
 };
 void launch_classify(const ClassifyArgs& a, cudaStream_t s);
 

@@ -592,7 +592,7 @@ __global__ void __launch_bounds__(256) screen_massive_kernel(ScreenArgs A) {
             const int slot = atomicAdd(&A.status->events, 1);
             if (slot < A.event_cap) {
                 pair_record(A.events + slot, I, J, pc, hm1, i + 1, j + 1, A.mbig[j] > A.mbig[i] && j < A.nbig);
-                A.event_step[slot] = 0;
+                A.event_step[slot] = A.step;
             } else {
                 atomicOr(&A.status->overflow, 1);
             }

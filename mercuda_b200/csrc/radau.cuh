@@ -86,6 +86,7 @@ struct ScreenArgs {
     EncounterCandidate* cands;
     int cand_cap;
     DeviceStatus* status;
+    int step;              // event_step of this screen's records
 };
 void launch_screen(const ScreenArgs& a, cudaStream_t s);
 
