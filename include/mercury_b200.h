@@ -70,12 +70,17 @@ int mercury_b200_encode_ce(const MercuryEvent* events, int n, double mcen, doubl
  * the particles lists the Big bodies that any process found in an encounter
  * (their subsystem end states) besides its own members. */
 int mercury_b200_hybrid_members(const int* ids, int count);
-/* mdt_hkce's substep loop (mercury6_2.for:3898-3937) over the active
+/* mdt_hkce's substep loop (mercury6_2.for:3884-3937) over the active
  * encounter subsystem, inside the library: from local time 0 to h, BS2
  * substeps (mercury_cuda_reset + mercury_cuda_step, dtflag 1 then 2) of
- * length *hrec (clipped to the remainder), each followed by
- * mercury_cuda_events at time + tlocal, exactly as a host drives these
- * drop-in calls, without a download per substep. *hrec receives the last
+ * length *hrec (clipped to the remainder), each followed by the pair screen
+ * of mercury_cuda_events at time + tlocal, with the arithmetic of a host
+ * driving these drop-in calls (the same states, records and force calls) but
+ * one host round trip per BS2 attempt (its level decision) and no download
+ * per substep; the records stay on the device until the run ends, and after
+ * a record-buffer overflow the run is redone from its start with larger
+ * buffers. With member tangents kept (the HYBRID adjoint) the drop-in calls
+ * are made one by one. *hrec receives the last
  * substep length tried (mdt_hkce's hrec), *forces the force calls, *nrecords
  * the number of close-encounter and collision records (central-body records
  * left out; subsystem ids, 1-based), fetched with mercury_b200_events(dst,
@@ -112,6 +117,12 @@ int mercury_b200_sync_epochs(const double* epoch, double* time, double h0, doubl
  * which runs one process. */
 typedef void (*mercury_b200_reduce_fn)(double* values, int count, void* user);
 int mercury_b200_set_step_reduce(mercury_b200_reduce_fn fn, void* user);
+/* Starting capacity of the close-encounter record and candidate buffers of
+ * every later upload (cap > 0; 0 restores the default of max(4096, particles
+ * / 64) records and max(16384, particles / 2) candidates). The buffers grow
+ * after an overflow and the affected step or run is redone, so the results
+ * do not depend on it; a small capacity exercises those paths in tests. */
+int mercury_b200_set_event_capacity(int cap);
 /* Launch shape of the particle kernel: threads per CTA (multiple of 32) and
  * steps fused per launch (0 = automatic); a negative value keeps the setting. */
 int mercury_b200_set_launch(int particle_threads, int steps_per_launch);

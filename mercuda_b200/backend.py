@@ -55,7 +55,7 @@ EXTENSION_SYMBOLS = ["mercury_b200_mvs_advance", "mercury_b200_events", "mercury
                      "mercury_b200_hybrid_adjoint_free", "mercury_b200_ejections",
                      "mercury_b200_encode_ce", "mercury_b200_set_step_reduce",
                      "mercury_b200_encounter_run", "mercury_b200_hybrid_members", "mercury_b200_epoch_order",
-                     "mercury_b200_sync_epochs"]
+                     "mercury_b200_sync_epochs", "mercury_b200_set_event_capacity"]
 
 # fn(values, count, user) of mercury_b200_set_step_reduce
 REDUCE_FN = C.CFUNCTYPE(None, C.POINTER(C.c_double), C.c_int, C.c_void_p)
@@ -104,6 +104,7 @@ def load_library(path: Path | str | None = None) -> C.CDLL:
     L.mercury_b200_ejections.argtypes = [D, I, D, I, PI, I, PI]
     L.mercury_b200_encode_ce.argtypes = [C.c_void_p, I, D, D, D, C.c_void_p, PI]
     L.mercury_b200_set_step_reduce.argtypes = [C.c_void_p, C.c_void_p]
+    L.mercury_b200_set_event_capacity.argtypes = [C.c_int]
     L.mercury_b200_encounter_run.argtypes = [D, D, D, D, PD, PI64, PI]
     L.mercury_b200_hybrid_members.argtypes = [PI, I]
     L.mercury_b200_epoch_order.argtypes = [I, PD, D, PI]
@@ -290,16 +291,15 @@ class Backend:
         x, v = rows
         ce, pi, pj = self.hybrid_begin(h, sys.rcrit, state.get("dtflag", 0), x, v)
         state["dtflag"] = 2
-        records = []
+        events = np.zeros(0, dtype=EVENT_DTYPE)
         if len(pi):
             sub = np.concatenate([[0], np.nonzero(ce[1:])[0] + 1])
-            xbs, vbs, records = self.encounter_subsystem(sub, sys.nbig, sys.m[sub], x[sub], v[sub], sys.rcrit[sub],
+            xbs, vbs, events = self.encounter_subsystem(sub, sys.nbig, sys.m[sub], x[sub], v[sub], sys.rcrit[sub],
                                                          sys.rce[sub], sys.rphys[sub], pi, pj, time, h, tol, state,
                                                          rcen, fused)
             x[sub[1:]] = xbs[1:]
             v[sub[1:]] = vbs[1:]
         self.hybrid_finish(h, sys.m, x, v)
-        events = np.array(records, dtype=EVENT_DTYPE) if records else np.zeros(0, dtype=EVENT_DTYPE)
         return events, len(pi)
 
     def encounter_subsystem(self, sub, nbig, m, x, v, rcrit, rce, rphys, pi, pj, time, h, tol, state, rcen,
@@ -309,7 +309,7 @@ class Backend:
         sub[0] = 0) with masses, pre-drift states and radii in the same order
         (row 0 is ignored), encounter pairs pi/pj (global 1-based). Returns the
         members' end states (rows as sub) and the close-encounter records
-        with global 1-based ids."""
+        with global 1-based ids (an EVENT_DTYPE array)."""
         sub = np.asarray(sub)
         index = sub.tolist()
         nbs = len(sub)
@@ -345,11 +345,10 @@ class Backend:
                 sub_ev = np.zeros(nrec.value, dtype=EVENT_DTYPE)
                 if nrec.value:
                     self.lib.mercury_b200_events(sub_ev.ctypes.data_as(C.c_void_p), None, nrec.value)
-                for e in sub_ev:
-                    e = e.copy()
-                    e["i"] = index[e["i"] - 1] + 1
-                    e["j"] = index[e["j"] - 1] + 1
-                    records.append(e)
+                    # subsystem ids -> global ids
+                    sub_ev["i"] = sub[sub_ev["i"] - 1] + 1
+                    sub_ev["j"] = sub[sub_ev["j"] - 1] + 1
+                records = sub_ev
                 xbs, vbs = self.download()
             else:
                 dtflag, tlocal, hlocal = 1, 0.0, math.copysign(state["hrec"], h)
@@ -374,6 +373,8 @@ class Backend:
         finally:
             self.lib.mercury_cuda_encounter_exit()
             self.n = outer_n
+        if not isinstance(records, np.ndarray):
+            records = np.array(records, dtype=EVENT_DTYPE) if records else np.zeros(0, dtype=EVENT_DTYPE)
         return xbs, vbs, records
 
     def sync_epochs(self, epoch: np.ndarray, time: float, h0: float, tol: float, dtout: float):

@@ -139,6 +139,10 @@ bool is_mvs(int alg) { return alg == 1 || alg == 9; }
 // launched, since the last reset.
 double g_dropin_ms = 0.0;
 
+// > 0: the starting capacity of the record and candidate buffers of each
+// upload (mercury_b200_set_event_capacity).
+int g_event_cap = 0;
+
 // Adds the device time of one drop-in call (CUDA events on the library
 // stream around it) to the total.
 struct DropinTimer {
@@ -417,10 +421,10 @@ void ra15_step_once(double time, double* h, double* hdid, double tol, int64_t* r
     }
 }
 
-// One mdt_bs1 (algorithm 2) or mdt_bs2 (algorithm 3) step with the Fortran's
-// control (mercury6_2.for:3380-3404, 3568-3596): the first level n > 3 whose
-// global error is <= tol^2 is taken, else the step is halved and redone.
-void bs_step_once(double time, double* h, double* hdid, double tol, int64_t* rejected) {
+// Every level of one mdt_bs1 (algorithm 2) or mdt_bs2 (algorithm 3) attempt
+// at trial step h from the current state buffer: per-level error maxima in
+// bs_errs, per-level force faults in bs_lvst, candidates for the commit.
+BsArgs launch_bs_attempt(double h) {
     Context& c = ctx();
     const int V = c.algorithm == 2 ? 1 : 2;
     const int L = bs_levels(V), nb = c.nbig - 1, N = c.nsplit;
@@ -430,100 +434,130 @@ void bs_step_once(double time, double* h, double* hdid, double tol, int64_t* rej
     c.bs_pcand.reserve((size_t)bs_candidates(V) * 6 * c.npcap);
     c.bs_errs.reserve(13);
     c.bs_lvst.reserve(13);
+    const int in = c.cur;
+    check(cudaMemsetAsync(c.bs_errs.p, 0, sizeof(unsigned long long) * 13, c.stream), "memset");
+    check(cudaMemsetAsync(c.bs_lvst.p, 0, sizeof(DeviceStatus) * 13, c.stream), "memset");
+    BsArgs a{};
+    a.f = force_cfg();
+    a.variant = V;
+    a.np = c.np;
+    a.npcap = c.npcap;
+    a.h0 = h;
+    a.bx = c.bigstate[in].p;
+    a.mbig = c.mbig.p;
+    a.ngfbig = c.ngfbig.p;
+    a.draw = c.bs_scr.p;
+    a.tscr = c.bs_scr.p + (size_t)L * 6 * N;
+    a.px = c.pstate[in].p;
+    a.pconst = c.pconst[c.kc].p;
+    a.table = c.ftab.p;
+    a.bcand = c.bs_bcand.p;
+    a.pcand = c.bs_pcand.p;
+    a.errs = c.bs_errs.p;
+    a.lvst = c.bs_lvst.p;
+    a.hkce = c.encounter ? 1 : 0;
+    a.rcrit = c.rcritbig.p;
+    a.adj_off = c.adj_off.p;
+    a.adj = c.adj.p;
+    a.perm = c.permp();
+    a.active_np = c.bs_active_np >= 0 ? std::min(c.bs_active_np, c.np) : c.np;
+    launch_bs_sequence(a, c.stream);
+    c.dropin_launches += 2 + (c.np > 0 ? 1 : 0);  // level CTAs, extrapolation, particles
+    check(cudaGetLastError(), "launch");
+    return a;
+}
+
+// The Fortran's choice (mercury6_2.for:3380-3404, 3568-3596) from the level
+// maxima errs and faults lv of an attempt: the first level n > 3 whose global
+// error is <= tol^2, or 0 when the step is to be halved and redone. Adds the
+// force calls of the levels it looked at to *forces.
+int bs_accept_level(const unsigned long long* errs, const DeviceStatus* lv, int V, double tol, int64_t* forces) {
+    const int L = bs_levels(V);
     const double tol2 = tol * tol;
-    const int in = c.cur, out = 1 - c.cur;
-    int64_t forces = 1;  // the start-of-step force
     const char* nonfinite = V == 1 ? "Nonfinite BS extrapolation; inspect input or close encounters"
                                    : "Nonfinite BS2 force or extrapolation";
+    // per level: the error maximum, then whether a force failed
+    const int fails = FAULT_NGF | FAULT_COINCIDENT;
+    double red[26];
+    for (int n = 0; n < 13; ++n) {
+        std::memcpy(&red[n], &errs[n], sizeof(double));
+        red[13 + n] = (lv[n].fault & fails) ? 1.0 : 0.0;
+    }
+    reduce_step_maxima(red, 26);
+    if (red[13] > 0.0) throw std::runtime_error("BS force failed");
+    for (int n = 1; n <= L; ++n) {
+        *forces += bs_level_forces(V, n);
+        if (red[13 + n] > 0.0) throw std::runtime_error("BS force failed");
+        if (n <= 3) continue;
+        const double e = red[n];
+        if (!std::isfinite(e)) throw std::runtime_error(nonfinite);
+        if (e <= tol2) return n;
+    }
+    return 0;
+}
+
+// Copies level `accepted` of attempt a into the other state buffer (and
+// pushes the encounter members' tangents through it when they are kept).
+void launch_bs_commit_of(const BsArgs& a, int accepted) {
+    Context& c = ctx();
+    const int in = c.cur, out = 1 - c.cur;
+    BsCommitArgs k{};
+    k.nsplit = c.nsplit;
+    k.np = c.np;
+    k.npcap = c.npcap;
+    k.cand = accepted - 4;
+    k.bcand = c.bs_bcand.p;
+    k.pcand = c.bs_pcand.p;
+    k.bx = c.bigstate[in].p;
+    k.bx_out = c.bigstate[out].p;
+    k.px_out = c.pstate[out].p;
+    k.px = c.pstate[in].p;
+    k.perm = c.permp();
+    k.active_np = a.active_np;
+    launch_bs_commit(k, c.stream);
+    c.dropin_launches += 1;
+    if (c.tangent && c.encounter && a.variant == 2 && c.np > 0) {
+        launch_bs2_tangent(a, accepted, c.tg.p, c.stream);
+        c.dropin_launches += 1;
+    }
+    check(cudaGetLastError(), "launch");
+}
+
+// The next trial step after an accepted level (mercury6_2.for:3389-3390, 3581-3582).
+void bs_next_trial(int V, int accepted, double* h) {
+    if (V == 1) {
+        if (accepted == 8) *h = *h * 0.55;
+    } else {
+        if (accepted >= 8) *h = *h * 0.55;
+    }
+    if (accepted < 7) *h = *h * 1.3;
+}
+
+// One mdt_bs1 (algorithm 2) or mdt_bs2 (algorithm 3) step with the Fortran's
+// control: attempts at halved steps until a level passes, then the commit.
+void bs_step_once(double time, double* h, double* hdid, double tol, int64_t* rejected) {
+    Context& c = ctx();
+    int64_t forces = 1;  // the start-of-step force
     for (;;) {
         if (time + *h == time) throw std::runtime_error("BS cannot advance time at the requested tolerance");
-        check(cudaMemsetAsync(c.bs_errs.p, 0, sizeof(unsigned long long) * 13, c.stream), "memset");
-        check(cudaMemsetAsync(c.bs_lvst.p, 0, sizeof(DeviceStatus) * 13, c.stream), "memset");
-        BsArgs a{};
-        a.f = force_cfg();
-        a.variant = V;
-        a.np = c.np;
-        a.npcap = c.npcap;
-        a.h0 = *h;
-        a.bx = c.bigstate[in].p;
-        a.mbig = c.mbig.p;
-        a.ngfbig = c.ngfbig.p;
-        a.draw = c.bs_scr.p;
-        a.tscr = c.bs_scr.p + (size_t)L * 6 * N;
-        a.px = c.pstate[in].p;
-        a.pconst = c.pconst[c.kc].p;
-        a.table = c.ftab.p;
-        a.bcand = c.bs_bcand.p;
-        a.pcand = c.bs_pcand.p;
-        a.errs = c.bs_errs.p;
-        a.lvst = c.bs_lvst.p;
-        a.hkce = c.encounter ? 1 : 0;
-        a.rcrit = c.rcritbig.p;
-        a.adj_off = c.adj_off.p;
-        a.adj = c.adj.p;
-        a.perm = c.permp();
-        a.active_np = c.bs_active_np >= 0 ? std::min(c.bs_active_np, c.np) : c.np;
-        launch_bs_sequence(a, c.stream);
-        c.dropin_launches += 2 + (c.np > 0 ? 1 : 0);  // level CTAs, extrapolation, particles
-        check(cudaGetLastError(), "launch");
+        const BsArgs a = launch_bs_attempt(*h);
         unsigned long long errs[13];
         DeviceStatus lv[13];
         check(cudaMemcpyAsync(errs, c.bs_errs.p, sizeof(errs), cudaMemcpyDeviceToHost, c.stream), "status");
         check(cudaMemcpyAsync(lv, c.bs_lvst.p, sizeof(lv), cudaMemcpyDeviceToHost, c.stream), "status");
         check(cudaStreamSynchronize(c.stream), "step");
-        // per level: the error maximum, then whether a force failed
-        const int fails = FAULT_NGF | FAULT_COINCIDENT;
-        double red[26];
-        for (int n = 0; n < 13; ++n) {
-            std::memcpy(&red[n], &errs[n], sizeof(double));
-            red[13 + n] = (lv[n].fault & fails) ? 1.0 : 0.0;
-        }
-        reduce_step_maxima(red, 26);
-        if (red[13] > 0.0) throw std::runtime_error("BS force failed");
-        int accepted = 0;
-        for (int n = 1; n <= L && !accepted; ++n) {
-            forces += bs_level_forces(V, n);
-            if (red[13 + n] > 0.0) throw std::runtime_error("BS force failed");
-            if (n <= 3) continue;
-            const double e = red[n];
-            if (!std::isfinite(e)) throw std::runtime_error(nonfinite);
-            if (e <= tol2) accepted = n;
-        }
+        const int accepted = bs_accept_level(errs, lv, a.variant, tol, &forces);
         if (!accepted) {
             ++*rejected;
             *h = *h * 0.5;
             continue;
         }
-        BsCommitArgs k{};
-        k.nsplit = N;
-        k.np = c.np;
-        k.npcap = c.npcap;
-        k.cand = accepted - 4;
-        k.bcand = c.bs_bcand.p;
-        k.pcand = c.bs_pcand.p;
-        k.bx = c.bigstate[in].p;
-        k.bx_out = c.bigstate[out].p;
-        k.px_out = c.pstate[out].p;
-        k.px = c.pstate[in].p;
-        k.perm = c.permp();
-        k.active_np = a.active_np;
-        launch_bs_commit(k, c.stream);
-        c.dropin_launches += 1;
-        if (c.tangent && c.encounter && V == 2 && c.np > 0) {
-            launch_bs2_tangent(a, accepted, c.tg.p, c.stream);
-            c.dropin_launches += 1;
-        }
-        check(cudaGetLastError(), "launch");
+        launch_bs_commit_of(a, accepted);
         check(cudaStreamSynchronize(c.stream), "step");
         *hdid = *h;
-        if (V == 1) {
-            if (accepted == 8) *h = *h * 0.55;
-        } else {
-            if (accepted >= 8) *h = *h * 0.55;
-        }
-        if (accepted < 7) *h = *h * 1.3;
+        bs_next_trial(a.variant, accepted, h);
         c.nforces += forces;
-        c.cur = out;
+        c.cur = 1 - c.cur;
         c.stepped = true;
         c.pair_events = 0;
         return;
@@ -533,55 +567,65 @@ void bs_step_once(double time, double* h, double* hdid, double tol, int64_t* rej
 // mce_stat between the buffers before and after the last step of an adaptive
 // integrator (mercury6_2.for:1765-1918): Big/massive pairs by one CTA, the
 // particles' box overlaps as candidates, classified like the MVS path's.
-void screen_pairs(double h) {
+// Records are appended at the status counter and tagged `step`; the caller
+// clears the candidate counter first.
+void launch_pair_screen(double h, int step) {
     Context& c = ctx();
     const int nb = c.nbig - 1;
     c.boxes.reserve((size_t)4 * std::max(1, nb));
     c.detail.reserve((size_t)std::max(1, nb) * TAB_DETAIL);
     const int prev = 1 - c.cur;
+    ScreenArgs a{};
+    a.nbig = c.nbig;
+    a.nsplit = c.nsplit;
+    a.np = c.np;
+    a.npcap = c.npcap;
+    a.h = h;
+    a.b0 = c.bigstate[prev].p;
+    a.b1 = c.bigstate[c.cur].p;
+    a.mbig = c.mbig.p;
+    a.rcebig = c.rcebig.p;
+    a.rphysbig = c.rphysbig.p;
+    a.p0 = c.pstate[prev].p;
+    a.p1 = c.pstate[c.cur].p;
+    a.pconst = c.pconst[c.kc].p;
+    a.perm = c.permp();
+    a.boxes = c.boxes.p;
+    a.detail = c.detail.p;
+    a.events = c.events.p;
+    a.event_step = c.event_step.p;
+    a.event_cap = (int)c.events.n;
+    a.cands = c.cands.p;
+    a.cand_cap = (int)c.cands.n;
+    a.status = c.status.p;
+    a.step = step;
+    launch_screen(a, c.stream);
+    c.dropin_launches += 1 + (c.np > 0 && nb > 0 ? 2 : 0);
+    if (nb > 0 && c.np > 0) {
+        ClassifyArgs ca{};
+        ca.nb = nb;
+        ca.nbig = c.nbig;
+        ca.h = h;
+        ca.detail = c.detail.p;
+        ca.cands = c.cands.p;
+        ca.cand_cap = (int)c.cands.n;
+        ca.events = c.events.p;
+        ca.event_step = c.event_step.p;
+        ca.event_cap = (int)c.events.n;
+        ca.status = c.status.p;
+        ca.step_base = step;
+        launch_classify(ca, c.stream);
+    }
+    check(cudaGetLastError(), "screen");
+}
+
+// The pair screen of the last step, its records from slot 0 (grown and redone
+// after an overflow).
+void screen_pairs(double h) {
+    Context& c = ctx();
     for (int attempt = 0;; ++attempt) {
         check(cudaMemsetAsync(c.status.p, 0, sizeof(DeviceStatus), c.stream), "memset");
-        ScreenArgs a{};
-        a.nbig = c.nbig;
-        a.nsplit = c.nsplit;
-        a.np = c.np;
-        a.npcap = c.npcap;
-        a.h = h;
-        a.b0 = c.bigstate[prev].p;
-        a.b1 = c.bigstate[c.cur].p;
-        a.mbig = c.mbig.p;
-        a.rcebig = c.rcebig.p;
-        a.rphysbig = c.rphysbig.p;
-        a.p0 = c.pstate[prev].p;
-        a.p1 = c.pstate[c.cur].p;
-        a.pconst = c.pconst[c.kc].p;
-        a.perm = c.permp();
-        a.boxes = c.boxes.p;
-        a.detail = c.detail.p;
-        a.events = c.events.p;
-        a.event_step = c.event_step.p;
-        a.event_cap = (int)c.events.n;
-        a.cands = c.cands.p;
-        a.cand_cap = (int)c.cands.n;
-        a.status = c.status.p;
-        launch_screen(a, c.stream);
-        c.dropin_launches += 1 + (c.np > 0 && nb > 0 ? 2 : 0);
-        if (nb > 0 && c.np > 0) {
-            ClassifyArgs ca;
-            ca.nb = nb;
-            ca.nbig = c.nbig;
-            ca.h = h;
-            ca.detail = c.detail.p;
-            ca.cands = c.cands.p;
-            ca.cand_cap = (int)c.cands.n;
-            ca.events = c.events.p;
-            ca.event_step = c.event_step.p;
-            ca.event_cap = (int)c.events.n;
-            ca.status = c.status.p;
-            ca.step_base = 0;
-            launch_classify(ca, c.stream);
-        }
-        check(cudaGetLastError(), "screen");
+        launch_pair_screen(h, 0);
         read_status();
         if (c.status_host->overflow) {
             if (attempt > 8) throw std::runtime_error("event buffer growth failed");
@@ -1188,8 +1232,16 @@ int mercury_cuda_upload(int n, int nbig, int pn, int ngflag, const double* m, co
         c.inv.reserve(c.npcap);
         c.kc = 0;
         c.status.reserve(1);
-        ensure_events(std::max(4096, c.np / 64));
-        c.cands.reserve(std::max(16384, c.np / 2));
+        if (g_event_cap > 0) {
+            c.events.release();
+            c.event_step.release();
+            c.cands.release();
+            ensure_events(g_event_cap);
+            c.cands.reserve(g_event_cap);
+        } else {
+            ensure_events(std::max(4096, c.np / 64));
+            c.cands.reserve(std::max(16384, c.np / 2));
+        }
         c.transfer.reserve((size_t)6 * n);
         if (c.algorithm == 4) {
             c.ra_bb.reserve((size_t)21 * ns);
@@ -1947,33 +1999,164 @@ int mercury_b200_hybrid_members(const int* ids, int count) {
     }
 }
 
-int mercury_b200_encounter_run(double time, double h, double tol, double rcen, double* hrec, int64_t* forces,
-                                int* nrecords) {
-    try {
-        if (g_active != 1) throw std::runtime_error("no encounter subsystem active");
-        std::vector<MercuryEvent> keep;
+namespace {
+
+// Adds the device time between two completed events on the library stream
+// to the drop-in total.
+void add_dropin_span(cudaEvent_t a, cudaEvent_t b) {
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, a, b) == cudaSuccess) g_dropin_ms += ms;
+}
+
+// mdt_hkce's substep loop (mercury6_2.for:3884-3937) with the arithmetic of
+// the drop-in calls (mercury_cuda_step, then the pair screen of
+// mercury_cuda_events, per substep) and one host round trip per BS2 attempt:
+// the level maxima, level faults and status come back in one pinned
+// readback, and the commit, the pair screen and the next attempt are queued
+// behind the host's decision. The screens' records stay on the device,
+// tagged with their substep, until the subsystem reaches h. The states do not
+// depend on the records, so after an event or candidate overflow the buffers
+// grow and the run is redone from its starting state.
+void encounter_run_queued(double time, double h, double tol, double* hrec, int64_t* nforces_out,
+                          std::vector<MercuryEvent>& keep) {
+    Context& c = ctx();
+    if (c.algorithm != 3) throw std::runtime_error("the encounter subsystem steps by algorithm 3 (mdt_bs2)");
+    const int V = 2;
+    mercury_cuda_reset(1);
+    const int cur0 = c.cur;
+    const double hrec0 = *hrec;
+    const int64_t nforces0 = c.nforces;
+    const size_t np_el = c.pstate[cur0].n, nb_el = c.bigstate[cur0].n;
+    c.snapshot.reserve(np_el + nb_el);
+    check(cudaMemcpyAsync(c.snapshot.p, c.pstate[cur0].p, sizeof(double) * np_el, cudaMemcpyDeviceToDevice, c.stream),
+          "snapshot");
+    check(cudaMemcpyAsync(c.snapshot.p + np_el, c.bigstate[cur0].p, sizeof(double) * nb_el,
+                          cudaMemcpyDeviceToDevice, c.stream),
+          "snapshot");
+    std::vector<double> tstep;   // time + tlocal at the end of each substep
+    int max_cands = 0;
+    for (int redo = 0;; ++redo) {
+        check(cudaMemsetAsync(c.status.p, 0, sizeof(DeviceStatus), c.stream), "memset");
+        tstep.clear();
         int64_t nforces = 0;
-        int dtflag = 1;
         double tlocal = 0.0, hlocal = std::copysign(*hrec, h);
+        bool queued = false;   // a commit + screen whose device time is not yet added
         for (;;) {
             const double tmp0 = std::fabs(h) - std::fabs(tlocal);
             *hrec = hlocal;
             if (std::fabs(hlocal) > tmp0) hlocal = std::copysign(tmp0, h);
-            mercury_cuda_reset(dtflag);
-            double hdid = 0.0;
-            int64_t nf = 0, nr = 0;
-            if (mercury_cuda_step(tlocal, &hlocal, &hdid, tol, &nf, &nr))
-                throw std::runtime_error("encounter step failed");
-            nforces += nf;
-            dtflag = 2;
+            int64_t forces = 1;  // the start-of-step force
+            int accepted = 0;
+            BsArgs a{};
+            for (;;) {
+                if (tlocal + hlocal == tlocal)
+                    throw std::runtime_error("BS cannot advance time at the requested tolerance");
+                check(cudaEventRecord(c.d0, c.stream), "event");
+                a = launch_bs_attempt(hlocal);
+                check(cudaMemcpyAsync(c.bs_rb->errs, c.bs_errs.p, sizeof(c.bs_rb->errs), cudaMemcpyDeviceToHost,
+                                      c.stream),
+                      "status");
+                check(cudaMemcpyAsync(c.bs_rb->lv, c.bs_lvst.p, sizeof(c.bs_rb->lv), cudaMemcpyDeviceToHost, c.stream),
+                      "status");
+                check(cudaMemcpyAsync(&c.bs_rb->st, c.status.p, sizeof(DeviceStatus), cudaMemcpyDeviceToHost, c.stream),
+                      "status");
+                check(cudaEventRecord(c.d1, c.stream), "event");
+                check(cudaEventSynchronize(c.d1), "step");
+                add_dropin_span(c.d0, c.d1);
+                if (queued) add_dropin_span(c.q0, c.q1);
+                queued = false;
+                // the candidates of the last queued screen (cleared before the next)
+                max_cands = std::max(max_cands, c.bs_rb->st.cands);
+                accepted = bs_accept_level(c.bs_rb->errs, c.bs_rb->lv, V, tol, &forces);
+                if (accepted) break;
+                hlocal = hlocal * 0.5;
+            }
+            check(cudaEventRecord(c.q0, c.stream), "event");
+            launch_bs_commit_of(a, accepted);
+            const double hdid = hlocal;
+            bs_next_trial(V, accepted, &hlocal);
+            nforces += forces;
+            c.nforces += forces;
+            c.cur = 1 - c.cur;
+            c.stepped = true;
             tlocal = tlocal + hdid;
-            const MercuryEvent* ev = nullptr;
-            int count = 0;
-            if (mercury_cuda_events(time + tlocal, hdid, rcen, &ev, &count))
-                throw std::runtime_error("encounter events failed");
-            for (int k = 0; k < count; ++k)
-                if (!(ev[k].kind & EV_CENTRAL)) keep.push_back(ev[k]);
+            tstep.push_back(time + tlocal);
+            check(cudaMemsetAsync(&c.status.p->cands, 0, sizeof(int), c.stream), "memset");
+            launch_pair_screen(hdid, (int)tstep.size() - 1);
+            check(cudaEventRecord(c.q1, c.stream), "event");
+            queued = true;
             if (!((tlocal - h) * h < 0.0)) break;
+        }
+        read_status();
+        if (queued) add_dropin_span(c.q0, c.q1);
+        max_cands = std::max(max_cands, c.status_host->cands);
+        if (!c.status_host->overflow) {
+            const int nev = c.status_host->events;
+            std::vector<MercuryEvent> ev(nev);
+            std::vector<int> steps(nev);
+            if (nev) {
+                check(cudaMemcpy(ev.data(), c.events.p, sizeof(MercuryEvent) * nev, cudaMemcpyDeviceToHost), "events");
+                check(cudaMemcpy(steps.data(), c.event_step.p, sizeof(int) * nev, cudaMemcpyDeviceToHost), "events");
+            }
+            // the drop-in events call adds the substep's end time to each record
+            for (int k = 0; k < nev; ++k) ev[k].time = ev[k].time + tstep[steps[k]];
+            std::vector<uint32_t> order;
+            order_events(ev, &steps, order);
+            keep.resize(nev);
+            for (int k = 0; k < nev; ++k) keep[k] = ev[order[k]];
+            c.pair_events = 0;
+            *nforces_out = nforces;
+            return;
+        }
+        if (redo > 8) throw std::runtime_error("event buffer growth failed");
+        grow_after_overflow();
+        if (c.status_host->overflow & 2) c.cands.reserve((size_t)max_cands + max_cands / 4 + 4096);
+        check(cudaMemcpyAsync(c.pstate[cur0].p, c.snapshot.p, sizeof(double) * np_el, cudaMemcpyDeviceToDevice,
+                              c.stream),
+              "restore");
+        check(cudaMemcpyAsync(c.bigstate[cur0].p, c.snapshot.p + np_el, sizeof(double) * nb_el,
+                              cudaMemcpyDeviceToDevice, c.stream),
+              "restore");
+        c.cur = cur0;
+        *hrec = hrec0;
+        c.nforces = nforces0;
+    }
+}
+
+}  // namespace
+
+int mercury_b200_encounter_run(double time, double h, double tol, double rcen, double* hrec, int64_t* forces,
+                               int* nrecords) {
+    try {
+        if (g_active != 1) throw std::runtime_error("no encounter subsystem active");
+        std::vector<MercuryEvent> keep;
+        int64_t nforces = 0;
+        if (!ctx().tangent) {
+            encounter_run_queued(time, h, tol, hrec, &nforces, keep);
+        } else {
+            // the members' tangents are kept: the drop-in calls one by one
+            int dtflag = 1;
+            double tlocal = 0.0, hlocal = std::copysign(*hrec, h);
+            for (;;) {
+                const double tmp0 = std::fabs(h) - std::fabs(tlocal);
+                *hrec = hlocal;
+                if (std::fabs(hlocal) > tmp0) hlocal = std::copysign(tmp0, h);
+                mercury_cuda_reset(dtflag);
+                double hdid = 0.0;
+                int64_t nf = 0, nr = 0;
+                if (mercury_cuda_step(tlocal, &hlocal, &hdid, tol, &nf, &nr))
+                    throw std::runtime_error("encounter step failed");
+                nforces += nf;
+                dtflag = 2;
+                tlocal = tlocal + hdid;
+                const MercuryEvent* ev = nullptr;
+                int count = 0;
+                if (mercury_cuda_events(time + tlocal, hdid, rcen, &ev, &count))
+                    throw std::runtime_error("encounter events failed");
+                for (int k = 0; k < count; ++k)
+                    if (!(ev[k].kind & EV_CENTRAL)) keep.push_back(ev[k]);
+                if (!((tlocal - h) * h < 0.0)) break;
+            }
         }
         Context& c = ctx();
         c.host_events.swap(keep);
@@ -2077,6 +2260,12 @@ int mercury_b200_sync_epochs(const double* epoch, double* time, double h0, doubl
     } catch (const std::exception& e) {
         return report(e);
     }
+}
+
+int mercury_b200_set_event_capacity(int cap) {
+    if (cap < 0) return 1;
+    g_event_cap = cap;
+    return 0;
 }
 
 int mercury_b200_set_step_reduce(mercury_b200_reduce_fn fn, void* user) {

@@ -144,6 +144,16 @@ struct Context {
     // timing events of the drop-in calls, and the kernels they launched
     cudaEvent_t d0 = nullptr, d1 = nullptr;
     int64_t dropin_launches = 0;
+    // the encounter subsystem's queued substeps: one pinned readback per BS2
+    // attempt (level maxima, level faults, status) and timing events around
+    // each queued commit + pair screen
+    struct BsReadback {
+        unsigned long long errs[13];
+        DeviceStatus lv[13];
+        DeviceStatus st;
+    };
+    BsReadback* bs_rb = nullptr;
+    cudaEvent_t q0 = nullptr, q1 = nullptr;
     int particle_threads = 128;
     int steps_per_launch = 0;   // 0 = automatic
 
@@ -170,6 +180,9 @@ struct Context {
             check(cudaEventCreate(&d0), "event");
             check(cudaEventCreate(&d1), "event");
             check(cudaMallocHost(reinterpret_cast<void**>(&status_host), sizeof(DeviceStatus)), "pinned");
+            check(cudaEventCreate(&q0), "event");
+            check(cudaEventCreate(&q1), "event");
+            check(cudaMallocHost(reinterpret_cast<void**>(&bs_rb), sizeof(BsReadback)), "pinned");
         }
     }
     void release_all() {

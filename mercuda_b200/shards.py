@@ -229,7 +229,7 @@ def sharded_hybrid_step(backend, ranks: Ranks, shard: System, ids: np.ndarray, t
     parts = ranks.gather(mine, everywhere=True)
     gpi = np.concatenate([p[0] for p in parts]).astype(np.int64)
     gpj = np.concatenate([p[1] for p in parts]).astype(np.int64)
-    records = []
+    events = np.zeros(0, dtype=EVENT_DTYPE)
     if len(gpi):
         # the pair list a single process would find: unique, sorted by (i, j)
         pairs = np.unique(np.stack([gpi, gpj], axis=1), axis=0)
@@ -240,7 +240,7 @@ def sharded_hybrid_step(backend, ranks: Ranks, shard: System, ids: np.ndarray, t
         central = np.zeros((1, 10))
         central[0, 0] = shard.m[0]
         d = np.concatenate([central, data])
-        xbs, vbs, records = backend.encounter_subsystem(sub, nbig, d[:, 0], d[:, 1:4], d[:, 4:7], d[:, 7], d[:, 8],
+        xbs, vbs, events = backend.encounter_subsystem(sub, nbig, d[:, 0], d[:, 1:4], d[:, 4:7], d[:, 7], d[:, 8],
                                                         d[:, 9], gpi, gpj, time, h, tol, state, rcen, fused)
         # the members this shard holds: every Big member and its own particles
         pos = np.searchsorted(ids, members)
@@ -250,5 +250,4 @@ def sharded_hybrid_step(backend, ranks: Ranks, shard: System, ids: np.ndarray, t
         v[apply] = vbs[1:][held]
         backend.hybrid_members(apply)
     backend.hybrid_finish(h, shard.m, x, v)
-    events = np.array(records, dtype=EVENT_DTYPE) if records else np.zeros(0, dtype=EVENT_DTYPE)
     return events, len(gpi)

@@ -122,3 +122,24 @@ def test_encounter_loop_in_library_matches_drop_in_calls(cuda_lib):
     for k in range(4):
         assert np.array_equal(a[k], b[k])
     assert a[4].tobytes() == b[4].tobytes()
+
+
+def test_encounter_loop_redone_after_buffer_overflow(cuda_lib):
+    """With record and candidate buffers of one entry, the library's substep
+    loop overflows, grows its buffers and redoes the subsystem's run from its
+    starting state (the drop-in calls grow and redo each screen instead): the
+    same states, records, pairs and force calls as with the default buffers."""
+    sys0 = make_system(seed=4, n_particles=1500, nplanets=8, near_fraction=0.05, h=8.0)
+    want = run_device(cuda_lib, sys0.copy(), 8.0, 10, fused=True)
+    assert cuda_lib.mercury_b200_set_event_capacity(1) == 0
+    try:
+        a = run_device(cuda_lib, sys0.copy(), 8.0, 10, fused=True)
+        b = run_device(cuda_lib, sys0.copy(), 8.0, 10, fused=False)
+    finally:
+        cuda_lib.mercury_b200_set_event_capacity(0)
+    assert len(want[4]) > 1
+    for got in (a, b):
+        assert got[5] == want[5] and got[6] == want[6]
+        for k in range(4):
+            assert np.array_equal(got[k], want[k])
+        assert got[4].tobytes() == want[4].tobytes()
