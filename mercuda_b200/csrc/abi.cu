@@ -1033,12 +1033,25 @@ int reorder_slots(int src, double h, cudaStream_t st) {
     return 1 - src;
 }
 
+// Resizes a host record array to n entries. Beyond its capacity it is
+// re-allocated with a quarter of headroom and without copying the old entries
+// (the caller overwrites them), so that the next run of a similar system,
+// which may bring a few more records, does not grow it again: growing a few
+// hundred MB by copy costs more than the run's other host work.
+template <class T> void size_records(std::vector<T>& v, size_t n) {
+    if (n > v.capacity()) {
+        std::vector<T>().swap(v);
+        v.reserve(n + n / 4);
+    }
+    v.resize(n);
+}
+
 // The order of records ev by (step, min(i,j), max(i,j)), ties in record
 // order: a counting sort of (pair key, record) by step, then each step's
 // short run by (key, record). steps == null: all in one step.
 void order_events(const std::vector<MercuryEvent>& ev, const std::vector<int>* steps, std::vector<uint32_t>& order) {
     const size_t n = ev.size();
-    order.resize(n);
+    size_records(order, n);
     if (n == 0) return;
     struct Item {
         uint64_t key;
@@ -1054,7 +1067,9 @@ void order_events(const std::vector<MercuryEvent>& ev, const std::vector<int>* s
     } else {
         first[1] = n;
     }
-    std::vector<Item> items(n);
+    // kept between calls (the library's calls come from one host thread)
+    static std::vector<Item> items;
+    size_records(items, n);
     {
         // stable scatter by step; with several threads each takes a contiguous
         // chunk of records and its own slice of every step's run (chunk order)
@@ -1816,8 +1831,8 @@ int mercury_b200_mvs_advance(double time, double h, int nsteps, double rcen, int
         c.pair_events = 0;
         const int nev = c.status_host->events;
         c.event_rate = std::max(c.event_rate, (double)nev / nsteps);
-        c.host_events.resize(nev);
-        c.host_steps.resize(nev);
+        size_records(c.host_events, nev);
+        size_records(c.host_steps, nev);
         if (nev) {
             check(cudaMemcpy(c.host_events.data(), c.events.p, sizeof(MercuryEvent) * nev, cudaMemcpyDeviceToHost),
                   "events");
