@@ -1365,10 +1365,13 @@ int mercury_cuda_events(double time, double h, double rcen, const MercuryEvent**
             launch_dh_shift(c.bigstate[c.cur].p, c.mbig.p, c.nsplit, c.m_host[0], c.hy_off.p + 3, c.stream);
             c.dropin_launches += 2;
         }
+        int head = 0;   // records read back with the status
         for (int attempt = 0;; ++attempt) {
-            // restart the counter after the step's pair events, then screen for central impacts
-            DeviceStatus st = {0, c.pair_events, 0, 0};
-            check(cudaMemcpyAsync(c.status.p, &st, sizeof(st), cudaMemcpyHostToDevice, c.stream), "status");
+            // restart the counter after the step's pair events (from pinned
+            // memory: the copy does not block), then screen for central impacts
+            *c.status_host = DeviceStatus{0, c.pair_events, 0, 0};
+            check(cudaMemcpyAsync(c.status.p, c.status_host, sizeof(DeviceStatus), cudaMemcpyHostToDevice, c.stream),
+                  "status");
             const int total = c.nsplit - 1 + c.np;
             if (c.stepped && total > 0) {
                 CentralArgs a;
@@ -1395,7 +1398,15 @@ int mercury_cuda_events(double time, double h, double rcen, const MercuryEvent**
                 c.dropin_launches += 1;
                 check(cudaGetLastError(), "central");
             }
-            read_status();
+            // the status and the first records in one round trip
+            head = c.stepped ? std::min(Context::EVENT_HEAD, (int)c.events.n) : 0;
+            check(cudaMemcpyAsync(c.status_host, c.status.p, sizeof(DeviceStatus), cudaMemcpyDeviceToHost, c.stream),
+                  "status");
+            if (head > 0)
+                check(cudaMemcpyAsync(c.ev_head, c.events.p, sizeof(MercuryEvent) * head, cudaMemcpyDeviceToHost,
+                                      c.stream),
+                      "events");
+            check(cudaStreamSynchronize(c.stream), "step");
             if (!c.status_host->overflow) break;
             if (attempt > 8) throw std::runtime_error("event buffer growth failed");
             // keep the pair events: copy them out, grow, copy back
@@ -1413,10 +1424,15 @@ int mercury_cuda_events(double time, double h, double rcen, const MercuryEvent**
                 h2d(c.events.p, keep.data(), sizeof(MercuryEvent) * c.pair_events, c.stream, "events");
         }
         const int nev = c.stepped ? c.status_host->events : 0;
-        c.host_events.resize(nev);
-        if (nev)
-            check(cudaMemcpy(c.host_events.data(), c.events.p, sizeof(MercuryEvent) * nev, cudaMemcpyDeviceToHost),
-                  "events");
+        size_records(c.host_events, nev);
+        if (nev) {
+            const int got = std::min(nev, head);
+            std::memcpy(c.host_events.data(), c.ev_head, sizeof(MercuryEvent) * got);
+            if (nev > got)
+                check(cudaMemcpy(c.host_events.data() + got, c.events.p + got, sizeof(MercuryEvent) * (nev - got),
+                                 cudaMemcpyDeviceToHost),
+                      "events");
+        }
         for (auto& e : c.host_events) {
             if (e.kind == EV_CENTRAL) e.time = time - h + e.time;
             else e.time = e.time + time;

@@ -154,6 +154,9 @@ struct Context {
     };
     BsReadback* bs_rb = nullptr;
     cudaEvent_t q0 = nullptr, q1 = nullptr;
+    // the first records of a drop-in events call, read back with its status
+    static constexpr int EVENT_HEAD = 1024;
+    MercuryEvent* ev_head = nullptr;
     int particle_threads = 128;
     int steps_per_launch = 0;   // 0 = automatic
 
@@ -183,6 +186,7 @@ struct Context {
             check(cudaEventCreate(&q0), "event");
             check(cudaEventCreate(&q1), "event");
             check(cudaMallocHost(reinterpret_cast<void**>(&bs_rb), sizeof(BsReadback)), "pinned");
+            check(cudaMallocHost(reinterpret_cast<void**>(&ev_head), sizeof(MercuryEvent) * EVENT_HEAD), "pinned");
         }
     }
     void release_all() {
