@@ -67,10 +67,11 @@ RCEN = 0.005
 FLOPS_PER_PARTICLE_STEP = 376.06
 # Bytes per particle-step if every step read and wrote x, v (and nothing else).
 BYTES_PER_PARTICLE_STEP = 96.0
-# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of one 31-step
-# launch of the particle kernel on this 1M-particle workload, from the ncu
-# capture summarised in profiles/mvs_particle_kernel_1M.md.
-TRAFFIC_PER_31_STEP_LAUNCH = (99.764224 + 157.014528) * 1e6
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum, MB) of one
+# launch of the particle kernel on this 1M-particle workload, by steps per
+# launch, from ncu captures of this bench's own command (the launch list and
+# traffic summary of the particle kernel are kept beside the sources).
+TRAFFIC_MB_PER_LAUNCH = {31: (99.764224, 157.014528)}
 CLOCK_QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
                "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -169,6 +170,64 @@ def cpu_baseline(particles: int, steps: int, seed: int):
     O.mvs_run(sysc, 0.0, H, steps, RCEN, central=True, threads=cores)
     dt = time.perf_counter() - t0
     return particles * steps / dt, cores, dt
+
+
+_PINNED_KEEP = []
+
+
+def pinned_like(a: np.ndarray) -> np.ndarray:
+    """A copy of a in page-locked host memory (torch's pinned allocator), the
+    host buffers of the end-to-end measurement: their copies run by DMA."""
+    import torch
+    t = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
+    _PINNED_KEEP.append(t)
+    out = t.numpy()
+    out[...] = a
+    return out
+
+
+def pinned_system(s):
+    """The system with its host arrays in page-locked memory."""
+    p = s.copy()
+    for name in ("m", "x", "v", "ngf", "rce", "rphys", "rcrit"):
+        setattr(p, name, pinned_like(getattr(s, name)))
+    return p
+
+
+def h2d_bytes(s) -> int:
+    """Bytes mercury_cuda_upload copies host -> device: x, v, m, rce, rphys,
+    and ngf when a force law reads it (ngflag != 0)."""
+    return s.n * (3 + 3 + 1 + 1 + 1 + (5 if s.ngflag else 0)) * 8
+
+
+def one_step_parity(lib, particles: int, seed: int):
+    """Parity of this run's workload, checked beside the CPU leg: the whole
+    system stepped once through the drop-in calls (step + events) against the
+    oracle's step of the same arrays. Returns the worst relative error of the
+    states, the share of bodies bit-identical to the oracle, and whether the
+    event lists (ids, kinds, order) are identical."""
+    from mercuda_b200.backend import Backend
+    from oracle import oracle as O
+    sysw = workload(particles, seed)
+    b = Backend("MVS", lib=lib)
+    b.configure()
+    b.upload(sysw)
+    b.step(0.0, H, dtflag=0)
+    x, v = b.download()
+    ev = b.events(H, H, RCEN)
+    b.free()
+    ref = sysw.copy()
+    rev, _ = O.mvs_run(ref, 0.0, H, 1, RCEN, central=True, threads=os.cpu_count() or 1)
+
+    def rel(a, r):
+        scale = np.maximum(np.linalg.norm(r, axis=1, keepdims=True), 1e-300)
+        return float(np.max(np.abs(a - r) / scale))
+
+    key = lambda e: (int(e["i"]), int(e["j"]), int(e["kind"]), int(e["now"]))
+    same = np.all(x == ref.x, axis=1) & np.all(v == ref.v, axis=1)
+    return {"max_rel_err_one_step": max(rel(x, ref.x), rel(v, ref.v)), "bitwise_fraction": float(same.mean()),
+            "pairs_equal": [key(e) for e in ev] == [key(e) for e in rev], "events": int(len(rev)),
+            "n_checked": int(sysw.n), "bar": 1e-12}
 
 
 def run_reference(args, rank):
@@ -342,16 +401,17 @@ def run_adaptive(args, rank, world, dist):
     value = world * args.particles * args.steps / (ms * 1e-3)
     e2e = None
     if not args.no_e2e:
-        fresh = adaptive_workload(args.particles, args.seed, rank)
+        fresh = pinned_system(adaptive_workload(args.particles, args.seed, rank))
+        out = (pinned_like(np.zeros((fresh.n, 3))), pinned_like(np.zeros((fresh.n, 3))))
         barrier()
         t0 = time.perf_counter()
         b.upload(fresh)
         run(0.0, ADAPTIVE_H0, args.steps)
-        x, v = b.download()
+        x, v = b.download(out=out)
         barrier()
         e2e_s = time.perf_counter() - t0
         e2e_s = ranks.max(e2e_s)
-        h2d = fresh.n * (3 + 3 + 1 + 1 + 1 + 5) * 8
+        h2d = h2d_bytes(fresh)
         e2e = {"value": world * args.particles * args.steps / e2e_s, "unit": UNIT,
                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": fresh.n * 48 / args.steps,
                "note": "wall clock around upload, the drop-in step + events calls of every step, download"}
@@ -435,18 +495,19 @@ def run_hybrid(args, rank, world, dist):
     value = world * args.particles * args.steps / (ms * 1e-3)
     e2e = None
     if not args.no_e2e:
-        fresh = mce_init(workload(args.particles, args.seed, HYBRID_NEAR, rank), H, 3.0)
+        fresh = pinned_system(mce_init(workload(args.particles, args.seed, HYBRID_NEAR, rank), H, 3.0))
+        out = (pinned_like(np.zeros((fresh.n, 3))), pinned_like(np.zeros((fresh.n, 3))))
         barrier()
         t0 = time.perf_counter()
         b.upload(fresh)
         state = {"dtflag": 0}
         sysw = fresh
         run(0.0, args.steps)
-        x, v = b.download()
+        x, v = b.download(out=out)
         barrier()
         e2e_s = time.perf_counter() - t0
         e2e_s = ranks.max(e2e_s)
-        h2d = fresh.n * (3 + 3 + 1 + 1 + 1 + 5 + 1) * 8
+        h2d = h2d_bytes(fresh) + fresh.n * 8
         e2e = {"value": world * args.particles * args.steps / e2e_s, "unit": UNIT,
                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": fresh.n * 48 / args.steps,
                "note": "wall clock around upload, hybrid_begin, the encounter subsystem, hybrid_finish and the "
@@ -851,7 +912,8 @@ def main():
         # multi-step run + event records and final state back (D2H).
         # Through the sharded driver: rank 0 receives the whole job's event
         # records (global ids); each rank reads its own states back.
-        fresh = workload(args.particles, args.seed, rank=rank)
+        fresh = pinned_system(workload(args.particles, args.seed, rank=rank))
+        xo, vo = pinned_like(np.zeros((fresh.n, 3))), pinned_like(np.zeros((fresh.n, 3)))
         nbig = fresh.nbig
         ids = np.concatenate([np.arange(nbig), nbig + rank * args.particles + np.arange(args.particles)])
         run = ShardedRun(ranks, b)
@@ -859,15 +921,15 @@ def main():
         t0 = time.perf_counter()
         run.upload(fresh, ids, nbig + world * args.particles)
         got = run.advance(0.0, H, args.steps, RCEN, args.steps_per_launch)
-        x, v = run.download(gather=False)
+        x, v = run.download(gather=False, out=(xo, vo))
         barrier()
         e2e_s = time.perf_counter() - t0
         e2e_s = ranks.max(e2e_s)
-        h2d = fresh.n * (3 + 3 + 1 + 1 + 1 + 5) * 8
-        d2h = fresh.n * 6 * 8 + run.local_events * 128
+        d2h = fresh.n * 6 * 8 + run.local_events * (128 + 4)
         e2e = {"value": world * args.particles * args.steps / e2e_s, "unit": UNIT,
-               "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
-               "note": "wall clock around the synchronous C-ABI calls: upload, fused run, download, events"}
+               "h2d_bytes_per_step": h2d_bytes(fresh) / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+               "note": "wall clock around the synchronous C-ABI calls from page-locked host arrays: upload, "
+                       "fused run, event records, download"}
     dropin = None
     if world == 1:
         # like for like with the reference's CUDA backend (its arm's
@@ -876,11 +938,14 @@ def main():
                   "steps": DROPIN_STEPS, "note": "mercury_cuda_step + mercury_cuda_events per step, wall clock"}
 
     cpu = None
+    parity = None
     if rank == 0 and not args.no_cpu_baseline:
         sample_particles, sample_steps = 300_000, 457
         v_cpu, cores, dt = cpu_baseline(sample_particles, sample_steps, args.seed)
         cpu = {"value": v_cpu, "unit": UNIT, "cores": cores, "kind": "port",
                "sample": f"{sample_particles} particles of the same generator x {sample_steps} steps ({dt:.1f} s)"}
+        # the oracle as the checker of this workload (after every timed region)
+        parity = one_step_parity(b.lib, args.particles, args.seed)
 
     if rank == 0:
         line = {
@@ -895,9 +960,9 @@ def main():
                              "each launch reads and writes it once"},
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak_tflops, "unit": "TFLOP/s",
                          "frac": achieved / peak_tflops,
-                         "traffic": (TRAFFIC_PER_31_STEP_LAUNCH * args.particles / 1e6
-                                     if steps_per_launch == 31 else None),
-                         "traffic_unit": "bytes per launch (ncu, 1M particles, 31 steps)",
+                         "traffic": (sum(TRAFFIC_MB_PER_LAUNCH[steps_per_launch]) * args.particles
+                                     if steps_per_launch in TRAFFIC_MB_PER_LAUNCH else None),
+                         "traffic_unit": f"bytes per launch (ncu, {steps_per_launch} steps, scaled from 1M particles)",
                          "peak_source": "measured in this run: fma() chains on every SM (2 FLOP/FMA)",
                          "flops_per_particle_step": FLOPS_PER_PARTICLE_STEP,
                          "kernel_ms_per_launch": kernel_ms},
@@ -911,6 +976,8 @@ def main():
         }
         if dropin is not None:
             line["dropin_per_step"] = dropin
+        if parity is not None:
+            line["parity"] = parity
         print(json.dumps(line), flush=True)
     b.free()
     if dist:

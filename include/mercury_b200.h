@@ -246,9 +246,14 @@ void mercury_b200_hybrid_adjoint_free(void);
  * Scratch lives in one static device array (about 2.2 MB per device, held
  * until exit) that every call shares: calls that overlap on the GPU (other
  * streams, other host threads) race on it. The first call on a device looks
- * up the array's address and initializes it (one synchronizing kernel), so
- * make that first call before any stream capture. The call is synchronous on
- * `stream` (a cudaStream_t; 0 = legacy default stream). */
+ * up the array's address and fills its slot map with one kernel on `stream`,
+ * waiting for that stream; with CUDA's lazy module loading that first call is
+ * also when the driver loads this library's device code, and with it the
+ * array, so it may allocate: make the first call during set-up, before any
+ * stream capture. Each call reads the central mass back from mbig[0] and then
+ * waits for `stream` at its end (a cudaStream_t; 0 = legacy default stream);
+ * an error already pending from the caller's earlier work makes it fail
+ * without clearing that error. */
 int mercury_b200_mvs_step_noalloc(int nbig, int np, const double* mbig, const double* rcebig,
                                   const double* rphysbig, const double* ngfbig, const double* big_in,
                                   double* big_out, const double* part_in, double* part_out,

@@ -215,9 +215,16 @@ class Backend:
         return np.frombuffer(bytes(buf), dtype=EVENT_DTYPE).copy()
 
     # gpu_pull / gpu_old (mercury_gpu.f90:180-185, 202-205)
-    def download(self, previous: bool = False):
-        x = np.zeros((self.n, 3))
-        v = np.zeros((self.n, 3))
+    def download(self, previous: bool = False, out=None):
+        """(x, v) of every body; `out` = (x, v) float64 (n, 3) arrays to fill
+        (page-locked host arrays are written directly by DMA)."""
+        if out is not None:
+            x, v = out
+            assert x.shape == v.shape == (self.n, 3) and x.dtype == v.dtype == np.float64
+            assert x.flags.c_contiguous and v.flags.c_contiguous
+        else:
+            x = np.empty((self.n, 3))
+            v = np.empty((self.n, 3))
         if self.lib.mercury_cuda_download(_p(x), _p(v), int(previous)) != 0:
             raise BackendError("CUDA previous state download failed" if previous else "CUDA download failed")
         return x, v

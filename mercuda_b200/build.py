@@ -39,17 +39,35 @@ def _stale() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> Path:
-    """Compile the library if any source is newer than it (or if forced)."""
+    """Compile the library if any source is newer than it (or if forced): each
+    translation unit to an object file in parallel, then one link."""
     if not force and not _stale():
         return LIB
-    cmd = [nvcc(), *ARCH, *FLAGS, *[str(CSRC / s) for s in SOURCES], "-o", str(LIB) + ".tmp"]
-    if verbose:
-        print(" ".join(cmd), flush=True)
-    res = subprocess.run(cmd, capture_output=True, text=True)
-    if res.returncode != 0:
-        raise RuntimeError("nvcc failed:\n" + res.stdout + res.stderr)
-    if verbose and res.stderr:
-        print(res.stderr, file=sys.stderr)
+    import concurrent.futures as cf
+    import tempfile
+
+    compile_flags = [f for f in FLAGS if f not in ("-shared", "-cudart", "static", "-Xlinker", "--no-undefined")]
+    with tempfile.TemporaryDirectory(prefix="mb200_build_") as tmp:
+        objs = [str(Path(tmp) / (Path(s).stem + ".o")) for s in SOURCES]
+        cmds = [[nvcc(), *ARCH, *compile_flags, "-c", str(CSRC / s), "-o", o] for s, o in zip(SOURCES, objs)]
+        if verbose:
+            for cmd in cmds:
+                print(" ".join(cmd), flush=True)
+        workers = max(1, min(len(cmds), os.cpu_count() or 1))
+        with cf.ThreadPoolExecutor(workers) as pool:
+            results = list(pool.map(lambda c: subprocess.run(c, capture_output=True, text=True), cmds))
+        for res in results:
+            if res.returncode != 0:
+                raise RuntimeError("nvcc failed:\n" + res.stdout + res.stderr)
+            if verbose and res.stderr:
+                print(res.stderr, file=sys.stderr)
+        link = [nvcc(), *ARCH, "-shared", "-cudart", "static", "-Xlinker", "--no-undefined", *objs, "-o",
+                str(LIB) + ".tmp"]
+        if verbose:
+            print(" ".join(link), flush=True)
+        res = subprocess.run(link, capture_output=True, text=True)
+        if res.returncode != 0:
+            raise RuntimeError("nvcc link failed:\n" + res.stdout + res.stderr)
     os.replace(str(LIB) + ".tmp", LIB)
     return LIB
 

@@ -2,8 +2,11 @@
 // points (include/mercury_b200.h): host orchestration of the device context.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <thread>
+
+#include <cub/device/device_radix_sort.cuh>
 
 #include "../../include/mercury_b200.h"
 #include "context.cuh"
@@ -39,6 +42,32 @@ void reduce_step_maxima(double* values, int count) {
 int report(const std::exception& e) {
     std::fprintf(stderr, "MERCURY CUDA: %s\n", e.what());
     return 1;
+}
+
+// Failure injection for testing a host's error handling without a GPU fault
+// (the reference tests rewrite and relink its CPU stub for this,
+// tests/test_edges.py:18-32): MERCURY_B200_FAIL lists, comma-separated, the
+// points that fail on purpose: an entry point's name without its prefix
+// (configure, upload, step, events, download, export, force, limits,
+// hybrid_begin, hybrid_finish, encounter_enter, encounter_update, advance),
+// "memory" (the upload's workspace guard sees no free device memory) or
+// "growth" (an event-buffer growth fails). Read on every call.
+bool injected(const char* point) {
+    const char* env = std::getenv("MERCURY_B200_FAIL");
+    if (!env || !*env) return false;
+    const size_t len = std::strlen(point);
+    for (const char* p = env; *p;) {
+        const char* end = std::strchr(p, ',');
+        const size_t n = end ? (size_t)(end - p) : std::strlen(p);
+        if (n == len && std::strncmp(p, point, n) == 0) return true;
+        if (!end) break;
+        p = end + 1;
+    }
+    return false;
+}
+
+void inject(const char* point) {
+    if (injected(point)) throw std::runtime_error(std::string("injected failure: ") + point);
 }
 
 namespace {
@@ -156,6 +185,15 @@ struct DropinTimer {
     }
 };
 
+// Device bytes an upload of n bodies holds: the double-buffered particle
+// state and constants, the slot maps, the upload stage, the transfer rows,
+// the fused run's snapshot and the record buffers (~0.8 KB a body), plus the
+// per-body B and E series of RA15 (algorithm 4).
+size_t workspace_bytes(int n, int algorithm) {
+    const size_t per_body = 800 + (algorithm == 4 ? 336 : 0);
+    return (size_t)n * per_body;
+}
+
 void require_system() {
     if (ctx().n <= 0) throw std::runtime_error("no system uploaded");
 }
@@ -163,6 +201,7 @@ void require_system() {
 void ensure_events(int cap) {
     Context& c = ctx();
     if ((int)c.events.n < cap) {
+        if (injected("growth") && c.events.n > 0) throw std::runtime_error("event buffer growth failed");
         c.events.reserve(cap);
         c.event_step.reserve(cap);
     }
@@ -187,6 +226,7 @@ MvsBigArgs big_args(int in, int out, int nsteps, int reset, int central, int ste
     Context& c = ctx();
     MvsBigArgs a{};
     a.nbig = c.nbig;
+    a.nmass = c.nsplit;
     a.ngflag = c.ngflag;
     a.obl = (c.jcen[0] != 0.0 || c.jcen[1] != 0.0 || c.jcen[2] != 0.0);
     a.reset = reset;
@@ -218,7 +258,7 @@ MvsParticleArgs particle_args(int in, int out, int nsteps, int reset, int centra
     a.np = c.np;
     a.npcap = c.npcap;
     a.nb = c.nbig - 1;
-    a.nbig = c.nbig;
+    a.nbig = c.nsplit;   // particle ids follow the bodies held by the Big-body CTA
     a.nsteps = nsteps;
     a.reset = reset;
     a.central = central;
@@ -644,15 +684,15 @@ void screen_pairs(double h) {
 // (unless big_only) corr_part receive the corrected heliocentric states.
 void run_corrector(double h, bool big_only = false) {
     Context& c = ctx();
-    const int nbig = c.nbig;
+    const int nbig = c.nbig, ns = c.nsplit;
     ensure_tables(4, 1);
-    c.corr_big.reserve((size_t)9 * nbig);
+    c.corr_big.reserve((size_t)9 * ns);
     c.corr_part.reserve((size_t)6 * c.npcap);
     check(cudaMemsetAsync(c.status.p, 0, sizeof(DeviceStatus), c.stream), "memset");
     MvsBigArgs b = big_args(c.cur, c.cur, 0, 0, 0, 0, h, 0.0, c.tab.p, c.detail.p);
     b.out.x = c.corr_big.p;
-    b.out.v = c.corr_big.p + 3 * nbig;
-    b.out.a = c.corr_big.p + 6 * nbig;
+    b.out.v = c.corr_big.p + 3 * ns;
+    b.out.a = c.corr_big.p + 6 * ns;
     CorrectorArgs k{};
     k.np = big_only ? 0 : c.np;
     k.npcap = c.npcap;
@@ -680,18 +720,17 @@ void run_corrector(double h, bool big_only = false) {
 
 void export_corrected(double h, double* xx, double* vv) {
     Context& c = ctx();
-    const int nbig = c.nbig;
+    const int ns = c.nsplit;
     run_corrector(h);
     c.transfer.reserve((size_t)6 * c.n);
-    for (int part = 0; part < 2; ++part) {
-        gather_kernel<<<blocks(c.n), 256, 0, c.stream>>>(c.transfer.p, c.n, 3, nbig, c.corr_big.p + 3 * part * nbig,
-                                                          nbig, c.corr_part.p + (size_t)3 * part * c.npcap, c.npcap,
+    for (int part = 0; part < 2; ++part)
+        gather_kernel<<<blocks(c.n), 256, 0, c.stream>>>(c.transfer.p + (size_t)3 * part * c.n, c.n, 3, ns,
+                                                          c.corr_big.p + 3 * part * ns, ns,
+                                                          c.corr_part.p + (size_t)3 * part * c.npcap, c.npcap,
                                                           c.inv.p);
-        check(cudaMemcpyAsync(part ? vv : xx, c.transfer.p, sizeof(double) * 3 * c.n, cudaMemcpyDeviceToHost,
-                              c.stream),
-              "export");
-        check(cudaStreamSynchronize(c.stream), "export");
-    }
+    check(cudaGetLastError(), "export");
+    const size_t bytes = sizeof(double) * 3 * (size_t)c.n;
+    copy_out({{c.transfer.p, xx, bytes}, {c.transfer.p + (size_t)3 * c.n, vv, bytes}}, c.stream);
 }
 
 // mxx_ejec's test (mercury6_2.for:7078-7080): bodies from index `first` on
@@ -817,42 +856,57 @@ __host__ __device__ inline int path_bucket(double x0, double x1, double x2, doub
     return b < 1 ? 1 : b;
 }
 
-void order_particles(int n, int nbig, double mu, const double* xx, const double* vv) {
+__global__ void path_key_kernel(const double* x, const double* v, int nbig, int np, double mu, unsigned char* key,
+                                int* idx) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= np) return;
+    const double* xp = x + 3 * (size_t)(nbig + p);
+    const double* vp = v + 3 * (size_t)(nbig + p);
+    key[p] = (unsigned char)path_bucket(xp[0], xp[1], xp[2], vp[0], vp[1], vp[2], mu);
+    idx[p] = p;
+}
+
+// perm (slot -> particle) from the sorted particle indices; padding slots map
+// to themselves; inv (particle -> slot).
+__global__ void slot_maps_kernel(const int* sorted, int np, int npcap, int* perm, int* inv) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= npcap) return;
+    const int p = s < np ? sorted[s] : s;
+    perm[s] = p;
+    inv[p] = s;
+}
+
+// The upload's slot order on the device: particles in ascending path_bucket
+// key (a stable radix sort of the 8-bit keys, so ties keep particle order),
+// from the staged host rows x, v of the n bodies (the first nbig are not
+// particles).
+void order_particles(int n, int nbig, double mu, const double* x, const double* v) {
     Context& c = ctx();
     const int np = n - nbig;
-    std::vector<int> bucket(np), count(257, 0), perm(c.npcap), inv(c.npcap);
-    // the keys on the host's cores (a million particles take ~0.1 s on one)
-    auto keys = [&](int lo, int hi) {
-        for (int p = lo; p < hi; ++p) {
-            const double* x = xx + 3 * (size_t)(nbig + p);
-            const double* v = vv + 3 * (size_t)(nbig + p);
-            bucket[p] = path_bucket(x[0], x[1], x[2], v[0], v[1], v[2], mu);
-        }
-    };
-    const int nthreads = np < 65536 ? 1 : (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
-    if (nthreads == 1) {
-        keys(0, np);
-    } else {
-        std::vector<std::thread> pool;
-        const int chunk = (np + nthreads - 1) / nthreads;
-        for (int k = 0; k < nthreads; ++k)
-            pool.emplace_back(keys, std::min(np, k * chunk), std::min(np, (k + 1) * chunk));
-        for (auto& th : pool) th.join();
-    }
-    for (int p = 0; p < np; ++p) count[bucket[p] + 1]++;
-    for (int k = 0; k < 256; ++k) count[k + 1] += count[k];
-    for (int p = 0; p < np; ++p) {
-        const int slot = count[bucket[p]]++;
-        perm[slot] = p;
-        inv[p] = slot;
-    }
-    for (int p = np; p < c.npcap; ++p) {  // padding slot maps to itself
-        perm[p] = p;
-        inv[p] = p;
-    }
-    h2d(c.perm[c.kc].p, perm.data(), sizeof(int) * c.npcap, c.stream);
-    h2d(c.inv.p, inv.data(), sizeof(int) * c.npcap, c.stream);
     c.steps_since_order = 0;
+    if (np <= 0) {
+        slot_maps_kernel<<<blocks(c.npcap), 256, 0, c.stream>>>(nullptr, 0, c.npcap, c.perm[c.kc].p, c.inv.p);
+        check(cudaGetLastError(), "order");
+        return;
+    }
+    // scratch: keys in/out (bytes), indices in/out (ints), then the sort's own
+    auto align = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    size_t temp = 0;
+    check(cub::DeviceRadixSort::SortPairs(nullptr, temp, (const unsigned char*)nullptr, (unsigned char*)nullptr,
+                                          (const int*)nullptr, (int*)nullptr, np, 0, 8, c.stream),
+          "order");
+    const size_t kb = align(np), ib = align(sizeof(int) * (size_t)np);
+    c.order_scratch.reserve(2 * kb + 2 * ib + align(temp));
+    char* base = c.order_scratch.p;
+    unsigned char* kin = reinterpret_cast<unsigned char*>(base);
+    unsigned char* kout = kin + kb;
+    int* iin = reinterpret_cast<int*>(base + 2 * kb);
+    int* iout = reinterpret_cast<int*>(base + 2 * kb + ib);
+    void* tmp = base + 2 * kb + 2 * ib;
+    path_key_kernel<<<blocks(np), 256, 0, c.stream>>>(x, v, nbig, np, mu, kin, iin);
+    check(cub::DeviceRadixSort::SortPairs(tmp, temp, kin, kout, iin, iout, np, 0, 8, c.stream), "order");
+    slot_maps_kernel<<<blocks(c.npcap), 256, 0, c.stream>>>(iout, np, c.npcap, c.perm[c.kc].p, c.inv.p);
+    check(cudaGetLastError(), "order");
 }
 
 // Device re-ordering of the slots as the state evolves (scattered or eccentric
@@ -1149,20 +1203,110 @@ void sort_events(std::vector<MercuryEvent>& ev, std::vector<int>* steps) {
 void download_buffer(int which, double* xx, double* vv) {
     Context& c = ctx();
     c.transfer.reserve((size_t)6 * c.n);
-    // x and v rows as two 3-component passes
+    // x rows then v rows, read back together
     for (int part = 0; part < 2; ++part) {
         const double* big = c.bigstate[which].p + 3 * part * c.nsplit;
         const double* prt = c.pstate[which].p + (size_t)3 * part * c.npcap;
-        gather_kernel<<<blocks(c.n), 256, 0, c.stream>>>(c.transfer.p, c.n, 3, c.nsplit, big, c.nsplit, prt, c.npcap,
-                                                          c.inv.p);
-        check(cudaMemcpyAsync(part ? vv : xx, c.transfer.p, sizeof(double) * 3 * c.n, cudaMemcpyDeviceToHost,
-                              c.stream),
-              "download");
-        check(cudaStreamSynchronize(c.stream), "download");
+        gather_kernel<<<blocks(c.n), 256, 0, c.stream>>>(c.transfer.p + (size_t)3 * part * c.n, c.n, 3, c.nsplit,
+                                                          big, c.nsplit, prt, c.npcap, c.inv.p);
+    }
+    check(cudaGetLastError(), "download");
+    const size_t bytes = sizeof(double) * 3 * (size_t)c.n;
+    copy_out({{c.transfer.p, xx, bytes}, {c.transfer.p + (size_t)3 * c.n, vv, bytes}}, c.stream);
+}
+
+// Runs fn(lo, hi) over [0, total) on up to 16 of the host's cores (one
+// thread below 4 MB).
+template <class F> void host_parallel(size_t total, F fn) {
+    const size_t nthreads = total < ((size_t)4 << 20)
+                                ? 1
+                                : std::max<size_t>(1, std::min<size_t>(16, std::thread::hardware_concurrency()));
+    if (nthreads == 1) {
+        fn((size_t)0, total);
+        return;
+    }
+    const size_t chunk = (total + nthreads - 1) / nthreads;
+    std::vector<std::thread> pool;
+    for (size_t t = 0; t < nthreads; ++t) {
+        const size_t lo = std::min(total, t * chunk), hi = std::min(total, lo + chunk);
+        if (lo < hi) pool.emplace_back(fn, lo, hi);
+    }
+    for (auto& th : pool) th.join();
+}
+
+// Copies the byte range [lo, hi) of the concatenated spans between their
+// host arrays and the page-locked area (to_stage: host -> area).
+void stage_bytes(const std::vector<HostSpan>& spans, const std::vector<size_t>& at, char* area, size_t lo, size_t hi,
+                 bool to_stage) {
+    size_t base = 0;
+    for (size_t k = 0; k < spans.size(); ++k) {
+        if (at[k] == SIZE_MAX) continue;
+        const size_t b0 = base, b1 = base + spans[k].bytes;
+        base = b1;
+        const size_t s = std::max(lo, b0), e = std::min(hi, b1);
+        if (s >= e) continue;
+        char* host = static_cast<char*>(spans[k].host) + (s - b0);
+        char* st = area + at[k] + (s - b0);
+        if (to_stage) std::memcpy(st, host, e - s);
+        else std::memcpy(host, st, e - s);
     }
 }
 
 }  // namespace
+
+bool host_pinned(const void* p) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();   // plain pageable memory on older drivers
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+// The pageable spans' offsets in the page-locked area (SIZE_MAX: the span is
+// page-locked and copied directly); returns their total size.
+static size_t stage_plan(const std::vector<HostSpan>& spans, std::vector<size_t>& at) {
+    size_t total = 0;
+    at.assign(spans.size(), SIZE_MAX);
+    for (size_t k = 0; k < spans.size(); ++k) {
+        if (spans[k].bytes == 0 || host_pinned(spans[k].host)) continue;
+        at[k] = total;
+        total += spans[k].bytes;
+    }
+    return total;
+}
+
+void copy_in(const std::vector<HostSpan>& spans, cudaStream_t stream) {
+    Context& c = ctx();
+    std::vector<size_t> at;
+    const size_t staged = stage_plan(spans, at);
+    if (staged) {
+        c.reserve_pinned(staged);
+        host_parallel(staged, [&](size_t lo, size_t hi) { stage_bytes(spans, at, c.pinned, lo, hi, true); });
+    }
+    for (size_t k = 0; k < spans.size(); ++k) {
+        if (spans[k].bytes == 0) continue;
+        const void* src = at[k] == SIZE_MAX ? spans[k].host : c.pinned + at[k];
+        check(cudaMemcpyAsync(spans[k].dev, src, spans[k].bytes, cudaMemcpyHostToDevice, stream), "upload");
+    }
+    check(cudaStreamSynchronize(stream), "upload");
+}
+
+void copy_out(const std::vector<HostSpan>& spans, cudaStream_t stream) {
+    Context& c = ctx();
+    std::vector<size_t> at;
+    const size_t staged = stage_plan(spans, at);
+    if (staged) c.reserve_pinned(staged);
+    for (size_t k = 0; k < spans.size(); ++k) {
+        if (spans[k].bytes == 0) continue;
+        void* dst = at[k] == SIZE_MAX ? spans[k].host : c.pinned + at[k];
+        check(cudaMemcpyAsync(dst, spans[k].dev, spans[k].bytes, cudaMemcpyDeviceToHost, stream), "download");
+    }
+    check(cudaStreamSynchronize(stream), "download");
+    if (staged)
+        host_parallel(staged, [&](size_t lo, size_t hi) { stage_bytes(spans, at, c.pinned, lo, hi, false); });
+}
+
 
 void scatter_rows(const double* rows, int n, int comps, int nbig, double* big, int big_stride, double* part,
                   int part_stride, const int* inv, cudaStream_t s) {
@@ -1193,6 +1337,7 @@ int mercury_cuda_configure(int method) {
     if (method != 1 && method != 2 && method != 3 && method != 4 && method != 9 && method != 10) return 1;
     Context& c = ctx();
     try {
+        inject("configure");
         if (method != c.algorithm) mercury_cuda_free();
         c.algorithm = method;
         c.reset = true;
@@ -1210,17 +1355,34 @@ int mercury_cuda_upload(int n, int nbig, int pn, int ngflag, const double* m, co
                         const double* ng, const double* jcen, const double* limits, const double* radii) {
     Context& c = ctx();
     try {
+        inject("upload");
         if (n < 1 || nbig < 1 || nbig > n) throw std::runtime_error("invalid body counts");
         if (is_mvs(c.algorithm) && nbig > 512) throw std::runtime_error("more than 512 Big bodies");
-        c.ensure_streams();
-        if (is_mvs(c.algorithm))
-            for (int j = nbig; j < n; ++j)
-                if (m[j] != 0.0) throw std::runtime_error("MVS with massive Small bodies not available in this build");
         int nmass = nbig;
         for (int j = nbig; j < n; ++j)
             if (m[j] != 0.0) nmass = j + 1;
-        const int ns = is_mvs(c.algorithm) ? nbig : nmass;
+        // MVS: massive Small bodies move as test particles and act on nothing
+        // but the central body's oblateness reaction (mfo_mvs,
+        // mercury6_2.for:5061-5068); the Big-body CTA holds them (up to 512
+        // bodies in all). Without oblateness more of them are exactly massless
+        // for the map and stay in the particle slots.
+        const bool obl = jcen[0] != 0.0 || jcen[1] != 0.0 || jcen[2] != 0.0;
+        int ns = nmass;
+        if (is_mvs(c.algorithm) && nmass > 512) {
+            if (obl) throw std::runtime_error("MVS with oblateness and more than 512 Big and massive Small bodies");
+            ns = nbig;
+        }
         if (ns > 512) throw std::runtime_error("more than 512 Big and massive Small bodies");
+        // Workspace guard, as the reference's (mercury_cuda.cu:384-388): a
+        // system that needs more device memory than 80% of what is free
+        // fails here with a message instead of part-way through allocating.
+        const size_t need = workspace_bytes(n, c.algorithm);
+        if ((size_t)9 * (size_t)std::max(2, (n - ns + 1) & ~1) > c.pstate[0].n || injected("memory")) {
+            size_t free_b = 0, total_b = 0;
+            if (!injected("memory")) check(cudaMemGetInfo(&free_b, &total_b), "memory");
+            if ((double)need > 0.8 * (double)free_b) throw std::runtime_error("Insufficient device workspace memory");
+        }
+        c.ensure_streams();
         c.n = n;
         c.nbig = nbig;
         c.nmass = nmass;
@@ -1276,31 +1438,40 @@ int mercury_cuda_upload(int n, int nbig, int pn, int ngflag, const double* m, co
         check(cudaMemsetAsync(c.pconst[0].p, 0, sizeof(double) * PCONST_ROWS * c.npcap, s), "memset");
         check(cudaMemsetAsync(c.pconst[1].p, 0, sizeof(double) * PCONST_ROWS * c.npcap, s), "memset");
         c.cur = 0;
-        order_particles(n, ns, m[0], xx, vv);
-        // positions and velocities
-        for (int part = 0; part < 2; ++part) {
-            check(cudaMemcpyAsync(c.transfer.p, part ? vv : xx, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s),
-                  "upload");
-            scatter_rows(c.transfer.p, n, 3, ns, c.bigstate[0].p + 3 * part * ns, ns,
+        // Every host array in one round of copies into the upload stage (ngf
+        // only when a force law reads it: with ngflag 0 no kernel does, and
+        // its rows stay zero), then the slot order and the layout on the device.
+        const size_t N = (size_t)n;
+        const bool ngf_read = ngflag != 0;
+        c.stage.reserve(9 * N + (ngf_read ? 5 * N : 0));
+        double* sx = c.stage.p;
+        double* sv = sx + 3 * N;
+        double* sm = sv + 3 * N;
+        double* sr = sm + N;
+        double* sp = sr + N;
+        double* sg = sp + N;
+        std::vector<HostSpan> spans = {{sx, const_cast<double*>(xx), 24 * N}, {sv, const_cast<double*>(vv), 24 * N},
+                                       {sm, const_cast<double*>(m), 8 * N}, {sr, const_cast<double*>(limits), 8 * N},
+                                       {sp, const_cast<double*>(radii), 8 * N}};
+        if (ngf_read) spans.push_back({sg, const_cast<double*>(ng), 40 * N});
+        copy_in(spans, s);
+        order_particles(n, ns, m[0], sx, sv);
+        for (int part = 0; part < 2; ++part)
+            scatter_rows(part ? sv : sx, n, 3, ns, c.bigstate[0].p + 3 * part * ns, ns,
                          c.pstate[0].p + (size_t)3 * part * c.npcap, c.npcap, c.inv.p, s);
-            check(cudaStreamSynchronize(s), "upload");
-        }
-        // per-body scalars: masses, radii
-        const double* scalars[3] = {m, limits, radii};
+        const double* scalars[3] = {sm, sr, sp};
         double* bigdst[3] = {c.mbig.p, c.rcebig.p, c.rphysbig.p};
         double* pdst[3] = {c.pm(), c.prce(), c.prphys()};
-        for (int q = 0; q < 3; ++q) {
-            check(cudaMemcpyAsync(c.transfer.p, scalars[q], sizeof(double) * n, cudaMemcpyHostToDevice, s), "upload");
-            scatter_rows(c.transfer.p, n, 1, ns, bigdst[q], ns, pdst[q], c.npcap, c.inv.p, s);
-            check(cudaStreamSynchronize(s), "upload");
-        }
+        for (int q = 0; q < 3; ++q) scatter_rows(scalars[q], n, 1, ns, bigdst[q], ns, pdst[q], c.npcap, c.inv.p, s);
         // ngf: Big rows stay interleaved (5 per body); particles become SoA
-        check(cudaMemcpyAsync(c.ngfbig.p, ng, sizeof(double) * 5 * ns, cudaMemcpyHostToDevice, s), "upload");
-        c.transfer.reserve((size_t)6 * n);
-        check(cudaMemcpyAsync(c.transfer.p, ng, sizeof(double) * 5 * n, cudaMemcpyHostToDevice, s), "upload");
-        scatter_rows(c.transfer.p, n, 5, ns, nullptr, 0, c.pngf(), c.npcap, c.inv.p, s);
-        check(cudaStreamSynchronize(s), "upload");
+        if (ngf_read) {
+            check(cudaMemcpyAsync(c.ngfbig.p, sg, sizeof(double) * 5 * ns, cudaMemcpyDeviceToDevice, s), "upload");
+            scatter_rows(sg, n, 5, ns, nullptr, 0, c.pngf(), c.npcap, c.inv.p, s);
+        } else {
+            check(cudaMemsetAsync(c.ngfbig.p, 0, sizeof(double) * 5 * ns, s), "upload");
+        }
         check(cudaGetLastError(), "upload");
+        check(cudaStreamSynchronize(s), "upload");
         c.reset = true;
         c.stepped = false;
         return 0;
@@ -1312,6 +1483,7 @@ int mercury_cuda_upload(int n, int nbig, int pn, int ngflag, const double* m, co
 int mercury_cuda_step(double time, double* h, double* hdid, double tol, int64_t* forces, int64_t* rejected) {
     Context& c = ctx();
     try {
+        inject("step");
         require_system();
         DropinTimer timer;
         *rejected = 0;
@@ -1338,6 +1510,7 @@ int mercury_cuda_step(double time, double* h, double* hdid, double tol, int64_t*
 int mercury_cuda_download(double* xx, double* vv, int previous) {
     Context& c = ctx();
     try {
+        inject("download");
         require_system();
         const int which = previous ? 1 - c.cur : c.cur;
         download_buffer(which, xx, vv);
@@ -1353,6 +1526,7 @@ int mercury_cuda_download(double* xx, double* vv, int previous) {
 int mercury_cuda_events(double time, double h, double rcen, const MercuryEvent** result, int* count) {
     Context& c = ctx();
     try {
+        inject("events");
         require_system();
         DropinTimer timer;
         const int prev = 1 - c.cur;
@@ -1450,6 +1624,7 @@ int mercury_cuda_events(double time, double h, double rcen, const MercuryEvent**
 int mercury_cuda_force(double* a) {
     Context& c = ctx();
     try {
+        inject("force");
         require_system();
         const int nb = c.nbig - 1, ns = c.nsplit;
         c.ftab.reserve((size_t)force_row(nb));
@@ -1486,6 +1661,7 @@ int mercury_cuda_force(double* a) {
 int mercury_cuda_export(double h, int physical, double* xx, double* vv) {
     Context& c = ctx();
     try {
+        inject("export");
         require_system();
         if (physical && c.algorithm == 1) {
             export_corrected(h, xx, vv);
@@ -1502,6 +1678,7 @@ int mercury_cuda_export(double h, int physical, double* xx, double* vv) {
 int mercury_cuda_limits(const double* limits) {
     Context& c = ctx();
     try {
+        inject("limits");
         require_system();
         check(cudaMemcpyAsync(c.transfer.p, limits, sizeof(double) * c.n, cudaMemcpyHostToDevice, c.stream), "limits");
         scatter_rows(c.transfer.p, c.n, 1, c.nsplit, c.rcebig.p, c.nsplit, c.prce(), c.npcap, c.inv.p, c.stream);
@@ -1516,6 +1693,7 @@ int mercury_cuda_hybrid_begin(double h, const double* crit, int flag, int cap, i
                               double* xx, double* vv, int64_t* forces) {
     Context& c = ctx();
     try {
+        inject("hybrid_begin");
         require_system();
         if (c.algorithm != 10) throw std::runtime_error("hybrid_begin needs algorithm 10");
         DropinTimer timer;
@@ -1596,6 +1774,7 @@ int mercury_cuda_hybrid_begin(double h, const double* crit, int flag, int cap, i
 int mercury_cuda_hybrid_finish(double h, const double* m, const double* xx, const double* vv, int64_t* forces) {
     Context& c = ctx();
     try {
+        inject("hybrid_finish");
         require_system();
         if (!c.hy_begun) throw std::runtime_error("hybrid_finish without hybrid_begin");
         DropinTimer timer;
@@ -1648,6 +1827,7 @@ int mercury_cuda_encounter_enter(int n, int nb, const double* m, const double* x
                                  const double* crit, const double* limits, const double* radii, int np,
                                  const int* pi, const int* pj) {
     try {
+        inject("encounter_enter");
         if (g_active != 0) throw std::runtime_error("encounter subsystem already active");
         g_active = 1;
         Context& c = ctx();
@@ -1698,6 +1878,7 @@ int mercury_cuda_encounter_enter(int n, int nb, const double* m, const double* x
 int mercury_cuda_encounter_update(const double* m, const double* xx, const double* vv) {
     Context& c = ctx();
     try {
+        inject("encounter_update");
         require_system();
         if (g_active != 1) throw std::runtime_error("no encounter subsystem active");
         c.transfer.reserve((size_t)6 * c.n);
@@ -1728,6 +1909,7 @@ int mercury_b200_mvs_advance(double time, double h, int nsteps, double rcen, int
     (void)time;
     Context& c = ctx();
     try {
+        inject("advance");
         require_system();
         if (!is_mvs(c.algorithm)) throw std::runtime_error("MVS advance needs algorithm 1 or 9");
         if (nsteps < 1) throw std::runtime_error("nsteps must be positive");
@@ -1765,7 +1947,7 @@ int mercury_b200_mvs_advance(double time, double h, int nsteps, double rcen, int
         }
         // keep the starting state (and slot order) so that an event-buffer
         // overflow can be redone from it
-        c.snapshot.reserve((size_t)9 * c.npcap + 9 * c.nbig);
+        c.snapshot.reserve((size_t)9 * c.npcap + 9 * c.nsplit);
         c.snap_const.reserve((size_t)PCONST_ROWS * c.npcap);
         c.snap_perm.reserve((size_t)2 * c.npcap);
         const int kc0 = c.kc;
@@ -1773,7 +1955,7 @@ int mercury_b200_mvs_advance(double time, double h, int nsteps, double rcen, int
             check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, c.stream), "snapshot");
         };
         copy(c.snapshot.p, c.pstate[c.cur].p, sizeof(double) * 9 * c.npcap);
-        copy(c.snapshot.p + 9 * c.npcap, c.bigstate[c.cur].p, sizeof(double) * 9 * c.nbig);
+        copy(c.snapshot.p + 9 * c.npcap, c.bigstate[c.cur].p, sizeof(double) * 9 * c.nsplit);
         copy(c.snap_const.p, c.pconst[kc0].p, sizeof(double) * PCONST_ROWS * c.npcap);
         copy(c.snap_perm.p, c.perm[kc0].p, sizeof(int) * c.npcap);
         copy(c.snap_perm.p + c.npcap, c.inv.p, sizeof(int) * c.npcap);
@@ -1828,7 +2010,7 @@ int mercury_b200_mvs_advance(double time, double h, int nsteps, double rcen, int
                 c.last_kernel_launches = launches;
                 // the Big and particle states must end in the same buffer index
                 if (bcur != pcur)
-                    copy(c.bigstate[pcur].p, c.bigstate[bcur].p, sizeof(double) * 9 * c.nbig);
+                    copy(c.bigstate[pcur].p, c.bigstate[bcur].p, sizeof(double) * 9 * c.nsplit);
                 c.cur = pcur;
                 break;
             }
@@ -1836,7 +2018,7 @@ int mercury_b200_mvs_advance(double time, double h, int nsteps, double rcen, int
             grow_after_overflow();
             c.kc = kc0;
             copy(c.pstate[c.cur].p, c.snapshot.p, sizeof(double) * 9 * c.npcap);
-            copy(c.bigstate[c.cur].p, c.snapshot.p + 9 * c.npcap, sizeof(double) * 9 * c.nbig);
+            copy(c.bigstate[c.cur].p, c.snapshot.p + 9 * c.npcap, sizeof(double) * 9 * c.nsplit);
             copy(c.pconst[kc0].p, c.snap_const.p, sizeof(double) * PCONST_ROWS * c.npcap);
             copy(c.perm[kc0].p, c.snap_perm.p, sizeof(int) * c.npcap);
             copy(c.inv.p, c.snap_perm.p + c.npcap, sizeof(int) * c.npcap);
@@ -1849,11 +2031,10 @@ int mercury_b200_mvs_advance(double time, double h, int nsteps, double rcen, int
         c.event_rate = std::max(c.event_rate, (double)nev / nsteps);
         size_records(c.host_events, nev);
         size_records(c.host_steps, nev);
-        if (nev) {
-            check(cudaMemcpy(c.host_events.data(), c.events.p, sizeof(MercuryEvent) * nev, cudaMemcpyDeviceToHost),
-                  "events");
-            check(cudaMemcpy(c.host_steps.data(), c.event_step.p, sizeof(int) * nev, cudaMemcpyDeviceToHost), "events");
-        }
+        if (nev)
+            copy_out({{c.events.p, c.host_events.data(), sizeof(MercuryEvent) * (size_t)nev},
+                      {c.event_step.p, c.host_steps.data(), sizeof(int) * (size_t)nev}},
+                     c.stream);
         // absolute times: the driver's clock advances by time = time + h per step
         std::vector<double> tend(nsteps);
         double t = time;
@@ -1936,7 +2117,7 @@ int mercury_b200_energy(double h, int physical, const double* spin, double* e, d
         if (physical && c.algorithm == 1) {
             run_corrector(h, true);
             a.big = c.corr_big.p;
-            a.bs = c.nbig;
+            a.bs = c.nsplit;
         } else {
             a.big = c.bigstate[c.cur].p;
             a.bs = c.nsplit;

@@ -131,6 +131,21 @@ struct Context {
     // staging
     DBuf<double> transfer;
     DBuf<double> snapshot;
+    // upload: the host arrays as they arrive ([3n] x, [3n] v, [n] m, rce,
+    // rphys, [5n] ngf), the slot-order sort's keys, indices and scratch, and
+    // a page-locked host area for copies from and to pageable host arrays
+    DBuf<double> stage;
+    DBuf<char> order_scratch;
+    char* pinned = nullptr;
+    size_t pinned_n = 0;
+    void reserve_pinned(size_t bytes) {
+        if (bytes <= pinned_n) return;
+        if (pinned) cudaFreeHost(pinned);
+        pinned = nullptr;
+        pinned_n = 0;
+        check(cudaMallocHost(reinterpret_cast<void**>(&pinned), bytes), "pinned staging");
+        pinned_n = bytes;
+    }
     // streams and timers
     cudaStream_t stream = nullptr, stream_big = nullptr;
     std::vector<cudaEvent_t> chunk_done;
@@ -194,8 +209,12 @@ struct Context {
                                 &pstate[1], &pconst[0], &pconst[1], &tab, &detail, &transfer, &snapshot, &snap_const,
                                 &ra_bb, &ra_be, &ra_bg, &ra_bpx, &ra_pb, &ra_pe, &ftab, &force_out, &boxes, &corr_big, &corr_part, &energy_scr,
                                 &bs_scr, &bs_bcand, &bs_pcand, &rcritbig, &hy_scr, &hy_tab, &hy_off,
-                                &hy_packed, &tg};
+                                &hy_packed, &tg, &stage};
         for (auto* b : bufs) b->release();
+        order_scratch.release();
+        if (pinned) cudaFreeHost(pinned);
+        pinned = nullptr;
+        pinned_n = 0;
         DBuf<int>* ibufs[] = {&perm[0], &perm[1], &inv, &order_bucket, &order_hist, &snap_perm, &ej_ids};
         for (auto* b : ibufs) b->release();
         ra_max.release();
@@ -233,5 +252,21 @@ void gather_rows(double* rows, int n, int comps, int nbig, const double* big, in
                  int part_stride, const int* inv, cudaStream_t s);
 
 int report(const std::exception& e);
+
+// One array of a host <-> device transfer: a host array (pageable or
+// page-locked) and its device range.
+struct HostSpan {
+    void* dev;
+    void* host;
+    size_t bytes;
+};
+// True for page-locked host memory (cudaMallocHost, cudaHostAlloc, cudaHostRegister).
+bool host_pinned(const void* p);
+// Copy every span host -> device (copy_in) or device -> host (copy_out) on
+// `stream`, returning when the data has landed. Page-locked host arrays are
+// copied directly by DMA; pageable ones go through the context's page-locked
+// area, which the host's cores fill or empty in parallel.
+void copy_in(const std::vector<HostSpan>& spans, cudaStream_t stream);
+void copy_out(const std::vector<HostSpan>& spans, cudaStream_t stream);
 
 }  // namespace mb200

@@ -42,10 +42,13 @@ struct BigSmem {
     }
 };
 
-// mco_h2j for the Big bodies (mercury6_2.for:2613-2682), one thread.
-__device__ void big_h2j(int nbig, const double* m, const double* X, const double* V, double* XJ, double* VJ) {
+// Bodies held by the Big-body CTA (Big, then massive Small bodies).
+__device__ __forceinline__ int big_count(const MvsBigArgs& A) { return A.nmass > A.nbig ? A.nmass : A.nbig; }
+
+// mco_h2j for the Big bodies (mercury6_2.for:2613-2682), one thread; arrays
+// [3][S].
+__device__ void big_h2j(int nbig, const double* m, const double* X, const double* V, double* XJ, double* VJ, int S) {
     if (nbig < 2) return;
-    const int S = nbig;
     double mtot = m[1];
     double mx[3], mv[3];
     for (int c = 0; c < 3; ++c) {
@@ -76,10 +79,10 @@ __device__ void big_h2j(int nbig, const double* m, const double* X, const double
     }
 }
 
-// mco_j2h for the Big bodies (mercury6_2.for:2700-2770), one thread.
-__device__ void big_j2h(int nbig, const double* m, const double* XJ, const double* VJ, double* X, double* V) {
+// mco_j2h for the Big bodies (mercury6_2.for:2700-2770), one thread; arrays
+// [3][S].
+__device__ void big_j2h(int nbig, const double* m, const double* XJ, const double* VJ, double* X, double* V, int S) {
     if (nbig < 2) return;
-    const int S = nbig;
     double mtot = m[1];
     double temp = m[1] / (mtot + m[0]);
     double mx[3], mv[3];
@@ -113,8 +116,12 @@ __device__ void big_j2h(int nbig, const double* m, const double* XJ, const doubl
 // mfo_mvs for the Big bodies plus the indirect term a0tp that every Small
 // body receives (mercury6_2.for:4946-5070), with mfo_ngf for Big bodies.
 // Writes S.ACC = (angf + 0) + a and S.misc = {a0, a0tp, acen}. All threads.
+// With massive Small bodies held (A.nmass > nbig) their oblateness terms
+// enter acen in body order, as mfo_obl sums over every body
+// (mercury6_2.for:5176-5230); their own accelerations follow from the force
+// row (small_type_force).
 __device__ void big_force(const MvsBigArgs& A, BigSmem& S, const double* V_ngf) {
-    const int nbig = A.nbig, N = nbig, tid = threadIdx.x, nt = blockDim.x;
+    const int nbig = A.nbig, N = big_count(A), tid = threadIdx.x, nt = blockDim.x;
     const double* m = A.m;
     double* a0 = S.misc;
     double* a0tp = S.misc + 3;
@@ -161,12 +168,12 @@ __device__ void big_force(const MvsBigArgs& A, BigSmem& S, const double* V_ngf) 
         }
     }
     if (A.obl)
-        for (int k = 1 + tid; k < nbig; k += nt) st3(S.AOBL, N, k, oblate_accel(ld3(S.X, N, k), A.jcen, m[0]));
+        for (int k = 1 + tid; k < N; k += nt) st3(S.AOBL, N, k, oblate_accel(ld3(S.X, N, k), A.jcen, m[0]));
     __syncthreads();
     if (tid == 0) {
         acen[0] = acen[1] = acen[2] = 0.0;
         if (A.obl)
-            for (int k = 1; k < nbig; ++k) {
+            for (int k = 1; k < N; ++k) {
                 const double tmp4 = m[k] / m[0];
                 const double3 ao = ld3(S.AOBL, N, k);
                 acen[0] = acen[0] - tmp4 * ao.x;
@@ -216,9 +223,9 @@ __device__ void big_force(const MvsBigArgs& A, BigSmem& S, const double* V_ngf) 
     __syncthreads();
 }
 
-// Force row of a table: head {a0tp, acen} and per-body {x, m}.
+// Force row of a table: head {a0tp, acen} and per-Big-body {x, m}.
 __device__ void write_force_table(const MvsBigArgs& A, const BigSmem& S, double* row) {
-    const int nbig = A.nbig, N = nbig;
+    const int nbig = A.nbig, N = big_count(A);
     if (threadIdx.x == 0)
         for (int c = 0; c < 6; ++c) row[c] = S.misc[3 + c];
     for (int k = 1 + threadIdx.x; k < nbig; k += blockDim.x) {
@@ -230,27 +237,54 @@ __device__ void write_force_table(const MvsBigArgs& A, const BigSmem& S, double*
     }
 }
 
-// The Big bodies' drift of mdt_mvs: h2j, Kepler drift of each Jacobi body
-// with gm_j, j2h (mercury6_2.for:4031-4046). All threads.
-__device__ void big_drift(const MvsBigArgs& A, BigSmem& S, double h) {
-    const int nbig = A.nbig, N = nbig, tid = threadIdx.x, nt = blockDim.x;
-    if (tid == 0) big_h2j(nbig, A.m, S.X, S.V, S.XJ, S.VJ);
-    __syncthreads();
-    for (int k = 1 + tid; k < nbig; k += nt) {
-        double3 p = ld3(S.XJ, N, k), w = ld3(S.VJ, N, k);
-        drift_one(S.GM[k], p, w, h);
-        st3(S.XJ, N, k, p);
-        st3(S.VJ, N, k, w);
+// Accelerations of the massive Small bodies held by the CTA: the particles'
+// mfo_mvs + mfo_ngf statements (small_body_force) against the force row just
+// written. All threads; the row must be visible (after __syncthreads).
+__device__ void small_type_force(const MvsBigArgs& A, BigSmem& S, const double* row, const double* V_ngf) {
+    const int nbig = A.nbig, N = big_count(A), nb = nbig - 1;
+    const bool ngf = A.ngflag == 1 || A.ngflag == 3;
+    for (int k = nbig + threadIdx.x; k < N; k += blockDim.x) {
+        const double3 x = ld3(S.X, N, k), v = ld3(V_ngf, N, k);
+        auto g = [&](int c) -> double { return A.ngf[5 * k + c]; };
+        double3 a;
+        if (ngf) a = A.obl ? small_body_force<true, true>(x, v, g, row, nb, A.jcen, A.m[0], A.status)
+                           : small_body_force<true, false>(x, v, g, row, nb, A.jcen, A.m[0], A.status);
+        else a = A.obl ? small_body_force<false, true>(x, v, g, row, nb, A.jcen, A.m[0], A.status)
+                       : small_body_force<false, false>(x, v, g, row, nb, A.jcen, A.m[0], A.status);
+        st3(S.ACC, N, k, a);
     }
     __syncthreads();
-    if (tid == 0) big_j2h(nbig, A.m, S.XJ, S.VJ, S.X, S.V);
+}
+
+// The drift of mdt_mvs: h2j, Kepler drift of each Jacobi Big body with gm_j,
+// j2h; each massive Small body drifts heliocentrically about the central
+// mass (mercury6_2.for:4031-4052). All threads.
+__device__ void big_drift(const MvsBigArgs& A, BigSmem& S, double h) {
+    const int nbig = A.nbig, N = big_count(A), tid = threadIdx.x, nt = blockDim.x;
+    if (tid == 0) big_h2j(nbig, A.m, S.X, S.V, S.XJ, S.VJ, N);
+    __syncthreads();
+    for (int k = 1 + tid; k < N; k += nt) {
+        if (k < nbig) {
+            double3 p = ld3(S.XJ, N, k), w = ld3(S.VJ, N, k);
+            drift_one(S.GM[k], p, w, h);
+            st3(S.XJ, N, k, p);
+            st3(S.VJ, N, k, w);
+        } else {
+            double3 p = ld3(S.X, N, k), w = ld3(S.V, N, k);
+            drift_one(A.m[0], p, w, h);
+            st3(S.X, N, k, p);
+            st3(S.V, N, k, w);
+        }
+    }
+    __syncthreads();
+    if (tid == 0) big_j2h(nbig, A.m, S.XJ, S.VJ, S.X, S.V, N);
     __syncthreads();
 }
 
 __device__ void big_load(const MvsBigArgs& A, BigSmem& S, double* smem) {
-    const int nbig = A.nbig, N = nbig, tid = threadIdx.x, nt = blockDim.x;
-    S.carve(smem, nbig);
-    for (int k = tid; k < nbig; k += nt)
+    const int nbig = A.nbig, N = big_count(A), tid = threadIdx.x, nt = blockDim.x;
+    S.carve(smem, N);
+    for (int k = tid; k < N; k += nt)
         for (int c = 0; c < 3; ++c) {
             S.X[c * N + k] = A.in.x[c * N + k];
             S.V[c * N + k] = A.in.v[c * N + k];
@@ -267,22 +301,24 @@ __device__ void big_load(const MvsBigArgs& A, BigSmem& S, double* smem) {
     __syncthreads();
 }
 
-// The Big-body integrator of one system (all threads of the CTA).
+// The Big-body integrator of one system (all threads of the CTA), with the
+// massive Small bodies it holds (A.nmass > nbig).
 __device__ void big_run(const MvsBigArgs& A, double* smem) {
-    const int nbig = A.nbig, N = nbig, nb = nbig - 1, tid = threadIdx.x, nt = blockDim.x;
+    const int nbig = A.nbig, N = big_count(A), nb = nbig - 1, tid = threadIdx.x, nt = blockDim.x;
     const int stride = tab_stride(nb);
     BigSmem S;
     big_load(A, S, smem);
     if (A.reset) {
-        if (tid == 0) big_h2j(nbig, A.m, S.X, S.V, S.XJ, S.VJ);
+        if (tid == 0) big_h2j(nbig, A.m, S.X, S.V, S.XJ, S.VJ, N);
         __syncthreads();
         big_force(A, S, S.V);
         write_force_table(A, S, A.tab);
         __syncthreads();
+        if (N > nbig) small_type_force(A, S, A.tab, S.V);
     }
     const double h = A.h, hby2 = 0.5 * h, hm1 = 1.0 / h;
     for (int s = 0; s < A.nsteps; ++s) {
-        for (int k = 1 + tid; k < nbig; k += nt)
+        for (int k = 1 + tid; k < N; k += nt)
             for (int c = 0; c < 3; ++c) {
                 const int z = c * N + k;
                 S.XS[z] = S.X[z];
@@ -315,12 +351,21 @@ __device__ void big_run(const MvsBigArgs& A, double* smem) {
             d[12] = A.rce[k];
             d[13] = A.rphys[k];
         }
-        // mce_stat between Big bodies (pairs 1 <= i < j < nbig).
-        const int npair = nb * (nb - 1) / 2;
+        // mce_stat between Big bodies (pairs 1 <= i < j < nbig), then between
+        // Big bodies and the massive Small bodies held (i < nbig <= j < N).
+        const int npair_big = nb * (nb - 1) / 2;
+        const int npair = npair_big + nb * (N - nbig);
         for (int q = tid; q < npair; q += nt) {
-            int i = 1, rem = q;
-            while (rem >= nbig - 1 - i) { rem -= nbig - 1 - i; ++i; }
-            const int j = i + 1 + rem;
+            int i = 1, j;
+            if (q < npair_big) {
+                int rem = q;
+                while (rem >= nbig - 1 - i) { rem -= nbig - 1 - i; ++i; }
+                j = i + 1 + rem;
+            } else {
+                const int r = q - npair_big;
+                i = 1 + r / (N - nbig);
+                j = nbig + r % (N - nbig);
+            }
             double lo_i, hi_i, lo_j, hi_j, ylo_i, yhi_i, ylo_j, yhi_j;
             const double pi_ = A.rce[i] * 1.2, pj_ = A.rce[j] * 1.2;
             box_extent(S.X0[i], S.X[i], S.V0[i], S.V[i], h, lo_i, hi_i);
@@ -336,7 +381,7 @@ __device__ void big_run(const MvsBigArgs& A, double* smem) {
             if (pair_classify(I, J, A.rce[i], A.rce[j], A.rphys[i], A.rphys[j], h, pc)) {
                 const int slot = atomicAdd(&A.status->events, 1);
                 if (slot < A.event_cap) {
-                    pair_record(A.events + slot, I, J, pc, hm1, i + 1, j + 1, A.m[j] > A.m[i]);
+                    pair_record(A.events + slot, I, J, pc, hm1, i + 1, j + 1, A.m[j] > A.m[i] && j < nbig);
                     A.event_step[slot] = A.step0 + s;
                     if (A.event_sys) A.event_sys[slot] = A.sys;
                 } else {
@@ -347,14 +392,18 @@ __device__ void big_run(const MvsBigArgs& A, double* smem) {
         __syncthreads();
         big_force(A, S, S.V);
         write_force_table(A, S, row);
-        for (int k = 1 + tid; k < nbig; k += nt)
+        if (N > nbig) {
+            __syncthreads();
+            small_type_force(A, S, row, S.V);
+        }
+        for (int k = 1 + tid; k < N; k += nt)
             for (int c = 0; c < 3; ++c) {
                 const int z = c * N + k;
                 S.V[z] = S.V[z] + hby2 * S.ACC[z];
             }
         __syncthreads();
         if (A.central)
-            for (int k = 1 + tid; k < nbig; k += nt) {
+            for (int k = 1 + tid; k < N; k += nt) {
                 double temp;
                 if (central_impact(ld3(S.XS, N, k), ld3(S.VS, N, k), ld3(S.X, N, k), ld3(S.V, N, k), A.m[0],
                                    A.m[k], h, A.rcen, temp)) {
@@ -376,7 +425,7 @@ __device__ void big_run(const MvsBigArgs& A, double* smem) {
             }
     }
     __syncthreads();
-    for (int k = tid; k < nbig; k += nt)
+    for (int k = tid; k < N; k += nt)
         for (int c = 0; c < 3; ++c) {
             A.out.x[c * N + k] = S.X[c * N + k];
             A.out.v[c * N + k] = S.V[c * N + k];
@@ -614,12 +663,20 @@ __global__ void __launch_bounds__(128, MB200_PARTICLE_MIN_BLOCKS) mvs_particle_k
 // force table of each of the four kicks.
 __global__ void __launch_bounds__(128) mvs_corrector_big_kernel(MvsBigArgs A, CorrectorArgs K) {
     extern __shared__ double smem[];
-    const int nbig = A.nbig, N = nbig, nb = nbig - 1, tid = threadIdx.x, nt = blockDim.x;
+    const int nbig = A.nbig, N = big_count(A), nb = nbig - 1, tid = threadIdx.x, nt = blockDim.x;
     const int stride = tab_stride(nb);
     BigSmem S;
     big_load(A, S, smem);
+    auto force = [&](double* row) {
+        big_force(A, S, S.V);
+        write_force_table(A, S, row);
+        if (N > nbig) {
+            __syncthreads();
+            small_type_force(A, S, row, S.V);
+        }
+    };
     auto kick = [&](double hk, bool subtract) {
-        for (int k = 1 + tid; k < nbig; k += nt)
+        for (int k = 1 + tid; k < N; k += nt)
             for (int c = 0; c < 3; ++c) {
                 const int z = c * N + k;
                 const double term = hk * S.ACC[z];
@@ -629,16 +686,14 @@ __global__ void __launch_bounds__(128) mvs_corrector_big_kernel(MvsBigArgs A, Co
     };
     for (int k = 0; k < 2; ++k) {
         big_drift(A, S, K.ha[k]);
-        big_force(A, S, S.V);
-        write_force_table(A, S, A.tab + (size_t)(2 * k) * stride);
+        force(A.tab + (size_t)(2 * k) * stride);
         kick(K.hb[k], K.forward != 0);
         big_drift(A, S, -2.0 * K.ha[k]);
-        big_force(A, S, S.V);
-        write_force_table(A, S, A.tab + (size_t)(2 * k + 1) * stride);
+        force(A.tab + (size_t)(2 * k + 1) * stride);
         kick(K.hb[k], K.forward == 0);
         big_drift(A, S, K.ha[k]);
     }
-    for (int k = tid; k < nbig; k += nt)
+    for (int k = tid; k < N; k += nt)
         for (int c = 0; c < 3; ++c) {
             A.out.x[c * N + k] = S.X[c * N + k];
             A.out.v[c * N + k] = S.V[c * N + k];
@@ -896,7 +951,8 @@ int mvs_max_steps_per_launch(int nb) {
 }
 
 void launch_mvs_corrector(const MvsBigArgs& big, const CorrectorArgs& a, cudaStream_t s) {
-    const size_t smem = sizeof(double) * ((size_t)12 * 3 * big.nbig + big.nbig + 16);
+    const int N = big.nmass > big.nbig ? big.nmass : big.nbig;
+    const size_t smem = sizeof(double) * ((size_t)12 * 3 * N + N + 16);
     if (smem > 48 * 1024)
         cudaFuncSetAttribute(mvs_corrector_big_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     mvs_corrector_big_kernel<<<1, 128, smem, s>>>(big, a);
@@ -946,7 +1002,8 @@ void launch_classify(const ClassifyArgs& a, cudaStream_t s) {
 }
 
 void launch_mvs_big(const MvsBigArgs& a, cudaStream_t s) {
-    const size_t smem = sizeof(double) * ((size_t)12 * 3 * a.nbig + a.nbig + 16);
+    const int N = a.nmass > a.nbig ? a.nmass : a.nbig;
+    const size_t smem = sizeof(double) * ((size_t)12 * 3 * N + N + 16);
     if (smem > 48 * 1024)
         cudaFuncSetAttribute(mvs_big_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     mvs_big_kernel<<<1, 128, smem, s>>>(a);

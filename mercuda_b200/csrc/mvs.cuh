@@ -31,6 +31,11 @@ struct BigState {
 
 struct MvsBigArgs {
     int nbig;
+    // Bodies held by the CTA: 0..nbig-1 Big, nbig..nmass-1 massive Small
+    // bodies (MVS with central-body oblateness: they enter the oblateness
+    // reaction acen that every body feels, mfo_mvs mercury6_2.for:5061-5068,
+    // but move as test particles). nmass <= nbig: Big bodies only.
+    int nmass;
     int ngflag;
     int obl;
     int reset;          // recompute the cached acceleration before the first kick
@@ -59,7 +64,7 @@ struct MvsParticleArgs {
     int np;             // number of test particles
     int npcap;          // allocated length of every particle array (even)
     int nb;             // Big bodies (nbig - 1)
-    int nbig;
+    int nbig;           // bodies before the particle slots (event ids: nbig + particle + 1)
     int nsteps;
     int reset;
     int central;

@@ -12,7 +12,9 @@
 // exits.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdio>
+#include <mutex>
 
 #include "../../include/mercury_b200.h"
 #include "mvs.cuh"
@@ -52,22 +54,29 @@ __global__ void finish_pair_times(MercuryEvent* ev, const DeviceStatus* st, int 
 }
 
 // The device address of the scratch array, looked up once per device (with
-// that device current): host code may not use the symbol itself as an address.
+// that device current): host code may not use the symbol itself as an
+// address. The first call on a device also fills the identity slot map, on
+// the caller's stream, and waits for that stream; host threads making their
+// first calls at the same time take turns (the mutex), and later calls read
+// the published address without locking.
 constexpr int MAX_DEVICES = 64;
-double* scratch_address[MAX_DEVICES] = {};
+std::atomic<double*> scratch_address[MAX_DEVICES] = {};
+std::mutex scratch_setup;
 
-double* scratch_for_current_device() {
+double* scratch_for_current_device(cudaStream_t s) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES) return nullptr;
-    if (!scratch_address[dev]) {
-        double* ptr = nullptr;
-        if (cudaGetSymbolAddress(reinterpret_cast<void**>(&ptr), noalloc_scratch) != cudaSuccess) return nullptr;
-        int* perm = reinterpret_cast<int*>(ptr + SCR_PERM);
-        identity_slots<<<(NOALLOC_MAX_PARTICLES + 255) / 256, 256>>>(perm, NOALLOC_MAX_PARTICLES);
-        if (cudaDeviceSynchronize() != cudaSuccess) return nullptr;
-        scratch_address[dev] = ptr;
-    }
-    return scratch_address[dev];
+    double* ptr = scratch_address[dev].load(std::memory_order_acquire);
+    if (ptr) return ptr;
+    std::lock_guard<std::mutex> lock(scratch_setup);
+    ptr = scratch_address[dev].load(std::memory_order_acquire);
+    if (ptr) return ptr;
+    if (cudaGetSymbolAddress(reinterpret_cast<void**>(&ptr), noalloc_scratch) != cudaSuccess) return nullptr;
+    int* perm = reinterpret_cast<int*>(ptr + SCR_PERM);
+    identity_slots<<<(NOALLOC_MAX_PARTICLES + 255) / 256, 256, 0, s>>>(perm, NOALLOC_MAX_PARTICLES);
+    if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) return nullptr;
+    scratch_address[dev].store(ptr, std::memory_order_release);
+    return ptr;
 }
 
 int fail(const char* what) {
@@ -90,9 +99,12 @@ extern "C" int mercury_b200_mvs_step_noalloc(int nbig, int np, const double* mbi
     if (np < 0 || np > NOALLOC_MAX_PARTICLES) return fail("noalloc step: at most 262144 particles");
     if (event_cap < 0 || event_cap > NOALLOC_MAX_EVENTS) return fail("noalloc step: event_cap must be 0..8192");
     if (!(h != 0.0)) return fail("noalloc step: zero step");
-    double* scr = scratch_for_current_device();
-    if (!scr) return fail("noalloc step: scratch address lookup failed");
+    // An error left by earlier work of the caller is reported as such (and
+    // left in place), not blamed on this step.
+    if (cudaPeekAtLastError() != cudaSuccess) return fail("noalloc step: a CUDA error was pending before the call");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    double* scr = scratch_for_current_device(s);
+    if (!scr) return fail("noalloc step: scratch address lookup failed");
     DeviceStatus* status = reinterpret_cast<DeviceStatus*>(scr + SCR_STATUS);
     double* tab = scr + SCR_TAB;
     double* detail = scr + SCR_DETAIL;
@@ -127,6 +139,7 @@ extern "C" int mercury_b200_mvs_step_noalloc(int nbig, int np, const double* mbi
     b.event_cap = event_cap;
     b.status = status;
     launch_mvs_big(b, s);
+    if (cudaGetLastError() != cudaSuccess) return fail("noalloc step: Big-body launch failed");
 
     if (np > 0) {
         MvsParticleArgs p{};
@@ -162,6 +175,7 @@ extern "C" int mercury_b200_mvs_step_noalloc(int nbig, int np, const double* mbi
             return fail("noalloc step: reading the central mass failed");
         p.mu = mu;
         launch_mvs_particles(p, s, 128);
+        if (cudaGetLastError() != cudaSuccess) return fail("noalloc step: particle launch failed");
         if (nbig > 1) {
             ClassifyArgs c{};
             c.nb = nbig - 1;
@@ -175,15 +189,17 @@ extern "C" int mercury_b200_mvs_step_noalloc(int nbig, int np, const double* mbi
             c.event_cap = event_cap;
             c.status = status;
             launch_classify(c, s);
+            if (cudaGetLastError() != cudaSuccess) return fail("noalloc step: classify launch failed");
         }
     }
-    if (event_cap > 0)
+    if (event_cap > 0) {
         finish_pair_times<<<(event_cap + 255) / 256, 256, 0, s>>>(events, status, event_cap, time + h);
+        if (cudaGetLastError() != cudaSuccess) return fail("noalloc step: record-time launch failed");
+    }
     DeviceStatus host_status{};
     if (cudaMemcpyAsync(&host_status, status, sizeof(DeviceStatus), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
         cudaStreamSynchronize(s) != cudaSuccess)
-        return fail("noalloc step: launch failed");
-    if (cudaGetLastError() != cudaSuccess) return fail("noalloc step: launch failed");
+        return fail("noalloc step: the step's kernels failed");
     if (event_count) *event_count = host_status.events;
     if (host_status.fault) return fail("MVS force failed");
     if (host_status.overflow) return fail("noalloc step: event or candidate capacity exceeded");

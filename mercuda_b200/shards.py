@@ -156,8 +156,8 @@ class ShardedRun:
         st = np.concatenate([p[1] for p in parts])
         return order_events(ev, st)
 
-    def download(self, gather: bool = True):
-        x, v = self.backend.download()
+    def download(self, gather: bool = True, out=None):
+        x, v = self.backend.download(out=out) if out is not None else self.backend.download()
         if not gather:
             return x, v
         parts = self.ranks.gather((self.ids, x, v))

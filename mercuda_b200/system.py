@@ -13,6 +13,7 @@ implementation is handed the same float64 arrays.
 """
 from __future__ import annotations
 
+import math
 from dataclasses import dataclass, field, replace
 
 import numpy as np
@@ -129,12 +130,22 @@ def mce_init(sys: System, h: float, cefac: float = 3.0) -> System:
         aa = np.where(2.0 * gm == r * v2, 0.0, gm * r / (2.0 * gm - r * v2))
     aa = np.where(aa <= 0.0, r, aa)
     a[1:] = aa
-    hill[1:] = aa * np.power(third * m[1:] / m[0], third)
+    # x**(1/3) as the Fortran's real power computes it: the C library's pow,
+    # one body at a time, wherever the bits matter (numpy's vectorised power
+    # may differ in the last bit). For massless bodies hill = a * 0**(1/3) = 0
+    # and rphys = 0 * (...), which no rounding of the power changes.
+    cbrt_c = lambda q: np.array([math.pow(float(t), third) for t in q]) if len(q) else np.zeros(0)
+    massive = np.nonzero(m[1:] != 0.0)[0] + 1
+    with np.errstate(over="ignore", invalid="ignore"):
+        hill[1:] = aa * np.power(third * m[1:] / m[0], third)
+    hill[massive] = aa[massive - 1] * cbrt_c(third * m[massive] / m[0])
     temp = 2.25 * m[0] / np.pi
     sys.rce = np.zeros(n)
     sys.rphys = np.zeros(n)
     sys.rce[1:] = hill[1:] * sys.rceh[1:]
-    sys.rphys[1:] = hill[1:] / a[1:] * np.power(temp / sys.rho[1:], third)
+    with np.errstate(divide="ignore", over="ignore", invalid="ignore"):
+        sys.rphys[1:] = hill[1:] / a[1:] * np.power(temp / sys.rho[1:], third)
+    sys.rphys[massive] = hill[massive] / a[massive] * cbrt_c(temp / sys.rho[massive])
     amin = min(9.9e29, float(np.min(a[1:]))) if n > 1 else 9.9e29
     vmax = np.sqrt(m[0] / amin)
     tmp = 0.4 * abs(h) * vmax

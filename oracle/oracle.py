@@ -65,6 +65,8 @@ def lib() -> C.CDLL:
         L.oracle_mvs_corrector.argtypes = [I, I, I, PD, PD, PD, PD, I, PD, D, PD, PD]
         L.oracle_mvs_corrector.restype = I
         L.oracle_mce_hill.argtypes = [I, PD, PD, PD, PD, PD]
+        L.oracle_mce_init.argtypes = [D, D, I, PD, PD, PD, PD, PD, PD, PD, PD, I]
+        L.oracle_mce_init.restype = None
         L.oracle_mvs_run.argtypes = [I, I, PD, PD, PD, PD, I, PD, PD, PD, D, D, I, D, I, I]
         L.oracle_mvs_run.restype = C.c_void_p
         L.oracle_run_status.argtypes = [C.c_void_p]
@@ -184,6 +186,17 @@ def mce_hill(m, x, v):
     a = np.zeros(n)
     lib().oracle_mce_hill(n, _p(m), _p(_f64(x)), _p(_f64(v)), _p(hill), _p(a))
     return hill, a
+
+
+def mce_init(m, x, v, rho, rceh, h, cefac, rcritflag=1):
+    """mce_init's limits (mercury6_2.for:1339-1380): (rce, rphys, rcrit); the
+    central body's entries stay zero."""
+    m, x, v, rho, rceh = map(_f64, (m, x, v, rho, rceh))
+    n = len(m)
+    rce, rphys, rcrit = np.zeros(n), np.zeros(n), np.zeros(n)
+    lib().oracle_mce_init(float(h), float(cefac), n, _p(m), _p(x), _p(v), _p(rho), _p(rceh), _p(rphys), _p(rce),
+                          _p(rcrit), int(rcritflag))
+    return rce, rphys, rcrit
 
 
 def mvs_run(sys, time0: float, h: float, nsteps: int, rcen: float, central: bool = True,

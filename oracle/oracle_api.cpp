@@ -112,6 +112,12 @@ void oracle_mce_hill(int n, const double* m, const double* x, const double* v, d
     oracle::mce_hill<double>(n, m, x, v, hill, a);
 }
 
+void oracle_mce_init(double h, double cefac, int n, const double* m, const double* x, const double* v,
+                     const double* rho, const double* rceh, double* rphys, double* rce, double* rcrit,
+                     int rcritflag) {
+    oracle::mce_init<double>(h, cefac, n, m, x, v, rho, rceh, rphys, rce, rcrit, rcritflag);
+}
+
 // The step loop of mal_hcon (mercury6_2.for:700-781) for MVS: nsteps calls of
 // mdt_mvs, each followed (if central != 0) by mce_cent on the heliocentric
 // states before and after the step; time advances by time = time + h.

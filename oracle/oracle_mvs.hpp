@@ -825,4 +825,29 @@ template <class R> void mce_hill(int nbod, const R* m, const R* x, const R* v, R
     }
 }
 
+// mce_init's limits, mercury6_2.for:1339-1380 (the close-encounter file
+// header it also writes is I/O and not restated): rce = hill * rceh,
+// rphys = hill / a * (2.25 m1 / (pi rho))^(1/3), and with rcritflag
+// rcrit = max(hill * cefac, 0.4 |h| sqrt(m1 / amin)).
+template <class R>
+void mce_init(R h, R cefac, int nbod, const R* m, const R* x, const R* v, const R* rho, const R* rceh, R* rphys,
+              R* rce, R* rcrit, int rcritflag) {
+    const R N2 = 0.4, THIRD = 0.3333333333333333, PI = 3.141592653589793;
+    const R HUGE_ = 9.9e29;
+    std::vector<R> a(nbod), hill(nbod);
+    R amin = HUGE_;
+    mce_hill(nbod, m, x, v, hill.data(), a.data());
+    R temp = R(2.25) * m[0] / PI;
+    for (int j = 1; j < nbod; ++j) {
+        rce[j] = hill[j] * rceh[j];
+        rphys[j] = hill[j] / a[j] * Pow(temp / rho[j], THIRD);
+        amin = std::min(a[j], amin);
+    }
+    if (rcritflag == 1) {
+        const R vmax = Sqrt(m[0] / amin);
+        temp = N2 * std::fabs(h) * vmax;
+        for (int j = 1; j < nbod; ++j) rcrit[j] = std::max(hill[j] * cefac, temp);
+    }
+}
+
 }  // namespace oracle

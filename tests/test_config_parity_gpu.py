@@ -1,0 +1,284 @@
+"""GPU parity at the sizes of the path's benchmark configurations.
+
+C0: the plain MVS system exactly as stated (10,000 massless particles about
+8 planets, h = 8 d, 46 steps covering 365 d, 3-Hill-radius encounter screen,
+central screen at 0.005 AU), through the drop-in per-step calls and the fused
+run. C1: the same generator with 1% of the particles inside 5 Hill radii of a
+planet, at 100,000 particles over 457 steps (10 yr) and at 1,000,000 particles
+for one drop-in step plus a fused run; HYBRID at 100,000 particles. C2: RADAU
+(tol 1e-12) and BS at 100,000 particles with 1PN, radiation pressure and
+Yarkovsky. C3: 4,096 batched systems. C4: the adjoint gradient of 100,000
+particles over 1,000 steps, checked on 64 random particles.
+
+Gates: 1e-12 relative after one step; encounter pair lists (step, ids, kind)
+identical; records bit-identical wherever both bodies of the record end the
+run bit-identical to the oracle (their arithmetic took the same statements),
+the others within 1e-9 relative in time and distance. States after a run are
+held to the stated drift (1e-9 relative after 365 d; 1e-7 after 10 yr of
+close encounters that amplify the Kepler seed's last-ulp differences).
+"""
+import numpy as np
+import pytest
+
+from adaptive_cases import compare_events
+from mercuda_b200.backend import Backend, Batch
+from mercuda_b200.system import make_batch, make_system, mce_init
+
+pytestmark = pytest.mark.gpu
+
+H = 8.0
+RCEN = 0.005
+
+
+def rel_err(a, b):
+    scale = np.maximum(np.linalg.norm(b, axis=1, keepdims=True), 1e-300)
+    return float(np.max(np.abs(a - b) / scale)) if len(a) else 0.0
+
+
+def same_rows(x, v, rx, rv):
+    return np.all(x == rx, axis=1) & np.all(v == rv, axis=1)
+
+
+def compare_records(got, got_steps, want, want_steps, same, rce):
+    """Pair lists equal; records bit-identical where both bodies are; returns
+    (records compared bytewise, records compared to tolerance)."""
+    def key(e, s):
+        return (int(s), min(int(e["i"]), int(e["j"])), max(int(e["i"]), int(e["j"])), int(e["kind"]))
+
+    gk = sorted(range(len(got)), key=lambda q: (key(got[q], got_steps[q]), float(got[q]["time"])))
+    wk = sorted(range(len(want)), key=lambda q: (key(want[q], want_steps[q]), float(want[q]["time"])))
+    gkeys = [key(got[q], got_steps[q]) for q in gk]
+    wkeys = [key(want[q], want_steps[q]) for q in wk]
+    if gkeys != wkeys:
+        extra = sorted(set(gkeys) ^ set(wkeys))
+        margins = []
+        for k in extra[:20]:
+            src = [(got[q], got_steps[q]) for q in gk if key(got[q], got_steps[q]) == k] or \
+                  [(want[q], want_steps[q]) for q in wk if key(want[q], want_steps[q]) == k]
+            e = src[0][0]
+            r = max(rce[int(e["i"]) - 1], rce[int(e["j"]) - 1])
+            margins.append((k, float(e["distance"]), float(r), abs(float(e["distance"]) - r) / max(r, 1e-300)))
+        raise AssertionError(f"pair lists differ in {len(extra)} records; (key, distance, rce, margin): {margins}")
+    bitwise = tolerance = 0
+    for qg, qw in zip(gk, wk):
+        e, w = got[qg], want[qw]
+        i, j = int(w["i"]) - 1, int(w["j"]) - 1
+        if w["kind"] != 8 and same[i] and same[j]:
+            assert e.tobytes() == w.tobytes(), (gkeys, e, w)
+            bitwise += 1
+        else:
+            assert abs(e["time"] - w["time"]) <= 1e-9 * max(1.0, abs(w["time"]))
+            assert abs(e["distance"] - w["distance"]) <= 1e-9 * max(1e-12, abs(w["distance"]))
+            tolerance += 1
+    return bitwise, tolerance
+
+
+def mvs_backend(cuda_lib, sys0):
+    b = Backend("MVS", lib=cuda_lib)
+    b.configure()
+    b.upload(sys0)
+    return b
+
+
+@pytest.mark.parametrize("mode", ["dropin", "fused"])
+def test_c0_exact(cuda_lib, oracle, mode):
+    """Config 0 exactly: 10,000 particles, 46 steps of 8 d."""
+    sys0 = make_system(seed=100, n_particles=10_000, near_fraction=0.0, h=H)
+    ref = sys0.copy()
+    want, want_steps = oracle.mvs_run(ref, 0.0, H, 46, RCEN, central=True, threads=16)
+    b = mvs_backend(cuda_lib, sys0)
+    if mode == "dropin":
+        got, got_steps, t = [], [], 0.0
+        for k in range(46):
+            b.step(t, H, dtflag=0 if k == 0 else 2)
+            if k == 0:
+                x1, v1 = b.download()
+                one = sys0.copy()
+                oracle.mvs_run(one, 0.0, H, 1, RCEN, central=False, threads=16)
+                assert rel_err(x1, one.x) <= 1e-12 and rel_err(v1, one.v) <= 1e-12
+            ev = b.events(t + H, H, RCEN)
+            got.append(ev)
+            got_steps.append(np.full(len(ev), k, dtype=np.int32))
+            t += H
+        got, got_steps = np.concatenate(got), np.concatenate(got_steps)
+    else:
+        got, got_steps = b.mvs_advance(0.0, H, 46, RCEN)
+    x, v = b.download()
+    b.free()
+    assert rel_err(x, ref.x) < 1e-9 and rel_err(v, ref.v) < 1e-9
+    same = same_rows(x, v, ref.x, ref.v)
+    assert same.mean() > 0.9
+    assert len(want) > 0
+    nb, nt = compare_records(got, got_steps, want, want_steps, same, sys0.rce)
+    assert nb + nt == len(want)
+
+
+def test_c1_100k_457_steps(cuda_lib, oracle):
+    """Config 1 at 100,000 particles over 10 yr (457 steps), fused."""
+    sys0 = make_system(seed=101, n_particles=100_000, near_fraction=0.01, h=H)
+    ref = sys0.copy()
+    want, want_steps = oracle.mvs_run(ref, 0.0, H, 457, RCEN, central=True, threads=16)
+    b = mvs_backend(cuda_lib, sys0)
+    got, got_steps = b.mvs_advance(0.0, H, 457, RCEN)
+    x, v = b.download()
+    b.free()
+    same = same_rows(x, v, ref.x, ref.v)
+    assert same.mean() > 0.9, same.mean()
+    assert rel_err(x, ref.x) < 1e-7
+    assert len(want) > 1000
+    compare_records(got, got_steps, want, want_steps, same, sys0.rce)
+
+
+def test_c1_1m_step_and_fused(cuda_lib, oracle):
+    """Config 1 at 1,000,000 particles: one drop-in step at 1e-12, then a
+    fused run of 8 more steps; pair lists identical."""
+    sys0 = make_system(seed=102, n_particles=1_000_000, near_fraction=0.01, h=H)
+    ref = sys0.copy()
+    want1, _ = oracle.mvs_run(ref, 0.0, H, 1, RCEN, central=True, threads=16)
+    b = mvs_backend(cuda_lib, sys0)
+    b.step(0.0, H, dtflag=0)
+    x, v = b.download()
+    got1 = b.events(H, H, RCEN)
+    assert rel_err(x, ref.x) <= 1e-12 and rel_err(v, ref.v) <= 1e-12
+    same = same_rows(x, v, ref.x, ref.v)
+    assert same.mean() > 0.95
+    compare_records(got1, np.zeros(len(got1), np.int32), want1, np.zeros(len(want1), np.int32), same, sys0.rce)
+    want, want_steps = oracle.mvs_run(ref, H, H, 8, RCEN, central=True, threads=16)
+    got, got_steps = b.mvs_advance(H, H, 8, RCEN)
+    x, v = b.download()
+    b.free()
+    same = same_rows(x, v, ref.x, ref.v)
+    assert rel_err(x, ref.x) < 1e-11
+    compare_records(got, got_steps, want, want_steps, same, sys0.rce)
+
+
+def test_c1_hybrid_100k(cuda_lib, oracle):
+    """HYBRID on the config-1 generator (natural encounters) at 100,000 particles."""
+    sys0 = mce_init(make_system(seed=103, n_particles=100_000, near_fraction=0.0, h=H), H, 3.0)
+    ref = sys0.copy()
+    nsteps = 4
+    want = oracle.hy_run(ref, 0.0, H, nsteps, 1e-12, RCEN)
+    b = Backend("HYBRID", cuda_lib)
+    b.configure()
+    b.upload(sys0)
+    state = {"dtflag": 0}
+    events, pairs, t = [], 0, 0.0
+    for _ in range(nsteps):
+        ev, npair = b.hybrid_step(sys0, t, H, 1e-12, state, RCEN)
+        pairs += npair
+        t += H
+        events.append(ev)
+        events.append(b.events(t, H, RCEN))
+    x, v = b.download()
+    b.free()
+    assert pairs == want[3] and pairs > 100
+    assert np.max(np.abs(x - ref.x)) < 1e-10 and np.max(np.abs(v - ref.v)) < 1e-10
+    key = lambda e: (min(e["i"], e["j"]), max(e["i"], e["j"]), int(e["kind"]))
+    assert sorted(map(key, np.concatenate(events))) == sorted(map(key, want[0]))
+
+
+def c2_system(n, seed=104):
+    sys0 = make_system(seed=seed, n_particles=n, near_fraction=0.0, h=H)
+    rng = np.random.default_rng(seed + 1)
+    npart = sys0.n - sys0.nbig
+    sys0.ngf[sys0.nbig:, 3] = rng.uniform(0.01, 0.3, npart)
+    sys0.ngf[sys0.nbig:, 4] = np.exp(rng.uniform(np.log(1e-15), np.log(1e-13), npart)) * rng.choice([-1, 1], npart)
+    sys0.pn = 1
+    return sys0
+
+
+@pytest.mark.parametrize("name,alg", [("RADAU", 4), ("BS", 2)])
+def test_c2_adaptive_100k(cuda_lib, oracle, name, alg):
+    """Config 2 at 100,000 particles: the first accepted steps of RADAU (tol
+    1e-12) and BS with 1PN, PR and Yarkovsky, from h = 2 d."""
+    sys0 = c2_system(100_000)
+    ref = sys0.copy()
+    steps = 3
+    rev, rst, rh, rdone, rforces, _ = oracle.hvar_run(ref, alg, 0.0, 1e9, 2.0, 1e-12, RCEN, max_steps=steps)
+    b = Backend(name, cuda_lib)
+    b.configure()
+    b.upload(sys0)
+    ev, st, h, done = b.hvar_run(0.0, 1e9, 2.0, 1e-12, RCEN, max_steps=steps)
+    x, v = b.download()
+    forces = b.forces
+    b.free()
+    assert done == rdone == steps and h == rh and forces == rforces
+    assert rel_err(x, ref.x) <= 1e-12 and rel_err(v, ref.v) <= 1e-12
+    assert same_rows(x, v, ref.x, ref.v).mean() > 0.999
+    compare_events(ev, rev)
+
+
+def test_c3_batched_4096(cuda_lib, oracle):
+    """Config 3: 4,096 systems of uneven size in one batched advance of 10
+    steps against the oracle run of each system."""
+    systems, h = make_batch(seed=105, nsys=4096)
+    nsteps = 10
+    b = Batch(systems, h, cuda_lib)
+    ev, sy, st = b.advance(0.0, nsteps, RCEN)
+    out = b.download()
+    b.free()
+    worst = 0.0
+    for k, (s, hs) in enumerate(zip(systems, h)):
+        ref = s.copy()
+        rev, rst = oracle.mvs_run(ref, 0.0, float(hs), nsteps, RCEN, central=True, threads=4)
+        x, v = out[k]
+        worst = max(worst, rel_err(x, ref.x), rel_err(v, ref.v))
+        same = same_rows(x, v, ref.x, ref.v)
+        compare_records(ev[sy == k], st[sy == k], rev, rst, same, s.rce)
+    assert worst < 1e-10, worst
+
+
+def test_c4_adjoint_64_of_100k(cuda_lib, oracle):
+    """Config 4: dL/d(x0, v0, yar) of L = sum |x_final|^2 for 100,000 particles,
+    1,000 steps of 8 d, checkpoint every 50; 64 random particles against the
+    oracle's FP64 tangent map (variational equations of the same statements)
+    at 1e-6 and against central differences of the oracle (relative step
+    1e-7) at 1e-4 (the difference quotient's own error)."""
+    import torch
+    from mercuda_b200.adjoint import mvs_trajectory
+
+    s = make_system(seed=106, n_particles=100_000, nplanets=8, near_fraction=0.0, h=H)
+    rng = np.random.default_rng(107)
+    npart = s.n - s.nbig
+    s.ngf[s.nbig:, 4] = np.exp(rng.uniform(np.log(1e-15), np.log(1e-13), npart)) * rng.choice([-1, 1], npart)
+    nb = s.nbig
+    dev = torch.device("cuda")
+    x0 = torch.tensor(s.x[nb:], device=dev, requires_grad=True)
+    v0 = torch.tensor(s.v[nb:], device=dev, requires_grad=True)
+    yar = torch.tensor(s.ngf[nb:, 4], device=dev, requires_grad=True)
+    xf, _ = mvs_trajectory(x0, v0, yar, (s.m[:nb], s.x[:nb], s.v[:nb]), H, 1000, 50)
+    (xf ** 2).sum().backward()
+    got = np.concatenate([x0.grad.cpu().numpy(), v0.grad.cpu().numpy(), yar.grad.cpu().numpy()[:, None]], axis=1)
+    pick = np.sort(rng.choice(npart, 64, replace=False))
+    sub = s.copy()
+    keep = np.concatenate([np.arange(nb), nb + pick])
+    for name in ("m", "x", "v", "ngf", "rce", "rphys", "rcrit", "rceh", "rho"):
+        setattr(sub, name, getattr(s, name)[keep].copy())
+    ref = sub.copy()
+    J = oracle.mvs_jacobian(ref, H, 1000)
+    xfin = ref.x[nb:]
+    want = np.einsum("prk,pr->pk", J, np.concatenate([2 * xfin, np.zeros_like(xfin)], axis=1))
+    g = got[pick]
+    for cols in (slice(0, 3), slice(3, 6), slice(6, 7)):
+        scale = np.abs(want[:, cols]).max(axis=1, keepdims=True)
+        err = np.max(np.abs(g[:, cols] - want[:, cols]) / scale)
+        assert err < 1e-6, (cols, err)
+    # central differences: every particle's parameter k perturbed at once
+    # (massless particles are independent), relative step 1e-7
+    params = np.concatenate([sub.x[nb:], sub.v[nb:], sub.ngf[nb:, 4:5]], axis=1)
+    fd = np.zeros_like(want)
+    for k in range(7):
+        eps = 1e-7 * np.maximum(np.abs(params[:, k]), 1e-300)
+        loss = []
+        for sign in (1.0, -1.0):
+            t = sub.copy()
+            p = params.copy()
+            p[:, k] += sign * eps
+            t.x[nb:], t.v[nb:], t.ngf[nb:, 4] = p[:, :3], p[:, 3:6], p[:, 6]
+            oracle.mvs_run(t, 0.0, H, 1000, RCEN, central=False, threads=8)
+            loss.append((t.x[nb:] ** 2).sum(axis=1))
+        fd[:, k] = (loss[0] - loss[1]) / (2 * eps)
+    for cols in (slice(0, 3), slice(3, 6), slice(6, 7)):
+        scale = np.abs(fd[:, cols]).max(axis=1, keepdims=True)
+        err = np.max(np.abs(g[:, cols] - fd[:, cols]) / scale)
+        assert err < 1e-4, (cols, err)

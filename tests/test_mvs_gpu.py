@@ -215,3 +215,57 @@ def test_per_step_loop_long_run_with_reordering(backend, oracle):
     prev = sys0.copy()
     oracle.mvs_run(prev, 0.0, 8.0, 99, 0.005, central=False, threads=4)
     assert rel_err(x0, prev.x) < 1e-9
+
+
+@pytest.mark.parametrize("oblate", [False, True])
+def test_massive_small_bodies(backend, oracle, oblate):
+    """Semi-active Small bodies under MVS, which the reference accepts
+    (mercury_cuda.cu:400-401): they move as test particles and, with the
+    central body's oblateness, enter the reaction term acen that every body
+    feels (mfo_mvs, mercury6_2.for:5061-5068). One step at 1e-12, then a
+    fused run and per-step drop-in calls against the oracle."""
+    from adaptive_cases import hvar_system
+    sys0 = hvar_system(massive=True, pn=0)
+    if oblate:
+        sys0.jcen[:] = [0.1, -1e-3, 0.0]
+    assert np.count_nonzero(sys0.m[sys0.nbig:]) > 5
+    backend.upload(sys0)
+    backend.step(0.0, 0.5, dtflag=0)
+    x, v = backend.download()
+    ev = backend.events(0.5, 0.5, 0.005)
+    ref, rev = oracle_events_one_step(oracle, sys0, 0.5, 0.005)
+    assert rel_err(x, ref.x) <= REL_ONE_STEP and rel_err(v, ref.v) <= REL_ONE_STEP
+    assert event_key(ev) == event_key(rev)
+    # fused run from the start
+    backend.upload(sys0)
+    ev, steps = backend.mvs_advance(0.0, 0.5, 128, 0.005)
+    x, v = backend.download()
+    xe, ve = backend.export(0.5, physical=True)
+    ref = sys0.copy()
+    rev, rsteps = oracle.mvs_run(ref, 0.0, 0.5, 128, 0.005, central=True, threads=1)
+    assert rel_err(x, ref.x) < 1e-11 and rel_err(v, ref.v) < 1e-11
+    assert np.array_equal(steps, rsteps) and event_key(ev) == event_key(rev)
+    want_x, want_v = oracle.mvs_corrector(ref, 0.5, forward=True)
+    assert np.max(np.abs(xe - want_x)) < 1e-12 and np.max(np.abs(ve - want_v)) < 1e-12
+
+
+def test_massive_small_bodies_particles_and_oblateness(backend, oracle):
+    """A workload-sized system with a few massive Small bodies among massless
+    ones and central-body oblateness: the massive ones ride in the Big-body
+    CTA, the rest in particle slots, with event ids mapped through both."""
+    sys0 = make_system(seed=31, n_particles=3000, near_fraction=0.03)
+    sys0.m[sys0.nbig:sys0.nbig + 40:4] = 1e-9 * K2
+    sys0.jcen[:] = [1e-6, -1e-9, 0.0]
+    backend.upload(sys0)
+    got, t = [], 0.0
+    for k in range(12):
+        backend.step(t, 8.0, dtflag=0 if k == 0 else 2)
+        got.extend((k, int(e["i"]), int(e["j"]), int(e["kind"])) for e in backend.events(t + 8.0, 8.0, 0.005))
+        t += 8.0
+    x, v = backend.download()
+    ref = sys0.copy()
+    rev, rsteps = oracle.mvs_run(ref, 0.0, 8.0, 12, 0.005, central=True, threads=1)
+    assert rel_err(x, ref.x) < 1e-11 and rel_err(v, ref.v) < 1e-11
+    assert got == [(int(s), int(e["i"]), int(e["j"]), int(e["kind"])) for s, e in zip(rsteps, rev)]
+    e0, l0 = backend.energy(8.0, physical=True)
+    assert np.isfinite(e0) and np.isfinite(l0)

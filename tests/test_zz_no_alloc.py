@@ -117,3 +117,77 @@ def test_noalloc_step_matches_drop_in_step(cuda_lib):
             assert abs(g["time"] - w["time"]) <= 1e-9 * max(1.0, abs(w["time"]))
             assert abs(g["distance"] - w["distance"]) <= 1e-9 * max(1e-12, w["distance"])
         time += H
+
+
+def _noalloc_args(sys0, dev, event_cap):
+    """Device arrays of sys0 as the allocation-free step takes them."""
+    import torch
+    nbig, n = sys0.nbig, sys0.n
+    npart = n - nbig
+    npcap = max(2, npart + (npart & 1))
+
+    def dev_array(a):
+        return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).to(dev)
+
+    big = np.zeros((9, nbig))
+    big[0:3] = sys0.x[:nbig].T
+    big[3:6] = sys0.v[:nbig].T
+    part = np.zeros((9, npcap))
+    part[0:3, :npart] = sys0.x[nbig:].T
+    part[3:6, :npart] = sys0.v[nbig:].T
+    const = np.zeros((8, npcap))
+    const[0, :npart] = sys0.m[nbig:]
+    const[1, :npart] = sys0.rce[nbig:]
+    const[2, :npart] = sys0.rphys[nbig:]
+    const[3:8, :npart] = sys0.ngf[nbig:].T
+    keep = dict(mbig=dev_array(sys0.m[:nbig]), rce=dev_array(sys0.rce[:nbig]), rphys=dev_array(sys0.rphys[:nbig]),
+                ngf=dev_array(sys0.ngf[:nbig]), big_in=dev_array(big),
+                big_out=torch.zeros((9, nbig), dtype=torch.float64, device=dev), part_in=dev_array(part),
+                part_out=torch.zeros((9, npcap), dtype=torch.float64, device=dev), const=dev_array(const),
+                events=torch.zeros(max(1, event_cap) * EVENT_DTYPE.itemsize, dtype=torch.uint8, device=dev))
+    return keep, npart
+
+
+def _call(cuda_lib, sys0, keep, npart, event_cap, count, stream, time=0.0, reset=1):
+    p = lambda t: C.c_void_p(t.data_ptr())
+    return cuda_lib.mercury_b200_mvs_step_noalloc(
+        sys0.nbig, npart, p(keep["mbig"]), p(keep["rce"]), p(keep["rphys"]), p(keep["ngf"]), p(keep["big_in"]),
+        p(keep["big_out"]), p(keep["part_in"]), p(keep["part_out"]), p(keep["const"]), sys0.ngflag, time, H, reset,
+        p(keep["events"]), event_cap, C.byref(count), stream)
+
+
+def test_noalloc_limits_overflow_and_memory(cuda_lib, capfd):
+    """Sizes beyond the stated limits are refused with a message before any
+    device work; a record buffer smaller than the step's records fails the
+    call and reports the records' total; a system of Big bodies only steps;
+    and calls after the first leave the device's free memory unchanged."""
+    import torch
+    dev = torch.device("cuda:0")
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    null = C.c_void_p(0)
+    count = C.c_int(-1)
+    for nbig, np_, cap, msg in [(65, 10, 16, "nbig must be 1..64"), (9, 262145, 16, "at most 262144 particles"),
+                                (9, 10, 8193, "event_cap must be 0..8192")]:
+        rc = cuda_lib.mercury_b200_mvs_step_noalloc(nbig, np_, null, null, null, null, null, null, null, null,
+                                                    null, 0, 0.0, H, 1, null, cap, C.byref(count), stream)
+        assert rc == 1 and msg in capfd.readouterr().err
+    # encounter records beyond a small event buffer
+    sys0 = make_system(seed=42, n_particles=4001, near_fraction=0.2)
+    keep, npart = _noalloc_args(sys0, dev, 2)
+    rc = _call(cuda_lib, sys0, keep, npart, 2, count, stream)
+    assert rc == 1 and count.value > 2
+    assert "capacity exceeded" in capfd.readouterr().err
+    # no test particles at all
+    big_only = make_system(seed=43, n_particles=0)
+    keep0, np0 = _noalloc_args(big_only, dev, 16)
+    assert _call(cuda_lib, big_only, keep0, np0, 16, count, stream) == 0
+    # the same steps again and again: the device's free memory does not move
+    keep, npart = _noalloc_args(sys0, dev, EVENT_CAP)
+    assert _call(cuda_lib, sys0, keep, npart, EVENT_CAP, count, stream) == 0
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for k in range(5):
+        assert _call(cuda_lib, sys0, keep, npart, EVENT_CAP, count, stream, reset=0) == 0
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
