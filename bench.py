@@ -77,6 +77,19 @@ CLOCK_QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.ac
                "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
 
+def config_of(args, text, **extra):
+    """The workload's config, the same dict in both arms (the reference arm
+    states the sample it could time in its cpu_baseline instead)."""
+    cfg = {"workload": text, "particles_per_gpu": args.particles, "seed": args.seed}
+    cfg.update(extra)
+    return cfg
+
+
+MVS_TEXT = ("MVS, {n} massless particles + 8 planets per GPU, h=8 d, 1% near planets, encounter + central screens "
+            "every step")
+MVS_L2 = "state 9 doubles/particle double-buffered (144 MB) > 126 MB L2; each launch reads and writes it once"
+
+
 def parse_args():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
@@ -89,6 +102,8 @@ def parse_args():
     p.add_argument("--threads", type=int, default=0)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-extras", action="store_true",
+                   help="skip the batched and adjoint summaries of the default MVS line")
     p.add_argument("--workload", default="mvs", choices=["mvs", "radau", "bs", "bs2", "hybrid", "batch", "adjoint",
                                                          "hybrid_adjoint"])
     p.add_argument("--checkpoint-every", type=int, default=50)
@@ -252,8 +267,7 @@ def run_reference(args, rank):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": f"MVS, {args.particles} massless particles + 8 planets, h=8 d, 1% near planets",
-                   "particles": particles, "h_days": H},
+        "config": config_of(args, MVS_TEXT.format(n=args.particles), h_days=H, l2=MVS_L2),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -301,6 +315,83 @@ def dropin_steps(lib, sysw, nsteps, warm=2):
     dt = time.perf_counter() - t0
     lib.mercury_cuda_free()
     return (sysw.n - sysw.nbig) * nsteps / dt
+
+
+def load_reference_cuda():
+    """The reference's CUDA backend (mercury_cuda.cu built unchanged for
+    sm_100a into oracle/_ref by oracle/Makefile's ref target) with the
+    argument types of its 16 drop-in entry points; None without a GPU or the
+    built library."""
+    if not REF_CUDA.exists():
+        return None
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return None
+    except ImportError:
+        return None
+    import ctypes
+    D_, I_ = ctypes.c_double, ctypes.c_int
+    PD_, PI_, P64 = ctypes.POINTER(D_), ctypes.POINTER(I_), ctypes.POINTER(ctypes.c_int64)
+    L = ctypes.CDLL(str(REF_CUDA))
+    L.mercury_cuda_available.restype = I_
+    L.mercury_cuda_configure.argtypes = [I_]
+    L.mercury_cuda_reset.argtypes = [I_]
+    L.mercury_cuda_reset.restype = None
+    L.mercury_cuda_limits.argtypes = [PD_]
+    L.mercury_cuda_export.argtypes = [D_, I_, PD_, PD_]
+    L.mercury_cuda_upload.argtypes = [I_, I_, I_, I_, PD_, PD_, PD_, PD_, PD_, PD_, PD_]
+    L.mercury_cuda_step.argtypes = [D_, PD_, PD_, D_, P64, P64]
+    L.mercury_cuda_download.argtypes = [PD_, PD_, I_]
+    L.mercury_cuda_events.argtypes = [D_, D_, D_, ctypes.POINTER(ctypes.c_void_p), PI_]
+    L.mercury_cuda_force.argtypes = [PD_]
+    L.mercury_cuda_hybrid_begin.argtypes = [D_, PD_, I_, I_, PI_, PI_, PI_, PI_, PD_, PD_, P64]
+    L.mercury_cuda_hybrid_finish.argtypes = [D_, PD_, PD_, PD_, P64]
+    L.mercury_cuda_encounter_enter.argtypes = [I_, I_, PD_, PD_, PD_, PD_, PD_, PD_, I_, PI_, PI_]
+    L.mercury_cuda_encounter_update.argtypes = [PD_, PD_, PD_]
+    L.mercury_cuda_encounter_exit.restype = None
+    L.mercury_cuda_free.restype = None
+    return L if L.mercury_cuda_available() else None
+
+
+def adaptive_wall_rate(lib, name, sysw, warmup, steps):
+    """Wall-clock particle-steps/s of the drop-in step + events calls as
+    mal_hvar makes them (synchronous calls), after `warmup` steps."""
+    from mercuda_b200.backend import Backend
+    b = Backend(name, lib=lib)
+    b.configure()
+    b.upload(sysw)
+    t, h, dtflag = 0.0, ADAPTIVE_H0, 0
+    for k in range(warmup + steps):
+        if k == warmup:
+            t0 = time.perf_counter()
+        hdid, h = b.step(t, h, ADAPTIVE_TOL, dtflag)
+        dtflag = 2
+        t = t + hdid
+        b.events(t, hdid, RCEN)
+    dt = time.perf_counter() - t0
+    b.free()
+    return (sysw.n - sysw.nbig) * steps / dt
+
+
+def hybrid_wall_rate(lib, sysw, warmup, steps, fused):
+    """Wall-clock particle-steps/s of HYBRID steps through the drop-in calls
+    (hybrid_begin, the encounter subsystem as mdt_hkce drives it, hybrid_finish,
+    the central screen), after `warmup` steps."""
+    from mercuda_b200.backend import Backend
+    b = Backend("HYBRID", lib=lib)
+    b.configure()
+    b.upload(sysw)
+    state, t = {"dtflag": 0}, 0.0
+    for k in range(warmup + steps):
+        if k == warmup:
+            t0 = time.perf_counter()
+        b.hybrid_step(sysw, t, H, 1e-12, state, RCEN, fused=fused)
+        t = t + H
+        b.events(t, H, RCEN)
+    dt = time.perf_counter() - t0
+    b.free()
+    return (sysw.n - sysw.nbig) * steps / dt
 
 
 def reference_cuda_rate(args):
@@ -365,7 +456,7 @@ def run_adaptive(args, rank, world, dist):
         line = {"impl": "reference", "metric": metric, "value": value, "unit": UNIT, "n_gpus": args.gpus,
                 "steps": done, "warmup": 0, "ms_per_step": dt * 1e3 / max(1, done), "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": workload_text, "particles": particles},
+                "config": config_of(args, workload_text),
                 "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample},
                 "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
@@ -415,6 +506,19 @@ def run_adaptive(args, rank, world, dist):
         e2e = {"value": world * args.particles * args.steps / e2e_s, "unit": UNIT,
                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": fresh.n * 48 / args.steps,
                "note": "wall clock around upload, the drop-in step + events calls of every step, download"}
+    ref_gpu = None
+    if world == 1:
+        # like for like with the reference's own CUDA backend on this GPU: the
+        # same drop-in calls on the same workload, wall clock for both
+        ref_lib = load_reference_cuda()
+        if ref_lib is not None:
+            steps_cmp = min(args.steps, 10)
+            ours = adaptive_wall_rate(b.lib, name, adaptive_workload(args.particles, args.seed), 2, steps_cmp)
+            theirs = adaptive_wall_rate(ref_lib, name, adaptive_workload(args.particles, args.seed), 2, steps_cmp)
+            ref_gpu = {"value": theirs, "unit": UNIT, "steps": steps_cmp, "dropin_wall": ours,
+                       "ratio_vs_reference_cuda": ours / theirs,
+                       "note": "the reference's CUDA backend and this library through the same drop-in step + "
+                               "events calls on this GPU, wall clock"}
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         particles = min(args.particles, 20_000)
@@ -425,12 +529,14 @@ def run_adaptive(args, rank, world, dist):
         line = {"metric": metric, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": workload_text, "particles_per_gpu": args.particles, "seed": args.seed,
-                           "h_last": h, "t_end_days": t,
-                           "l2": "per step the state, B/E (RA15) or candidates (BS) exceed 126 MB only above "
-                                 "~300K particles; measured as is"},
+                "config": config_of(args, workload_text),
+                "run": {"h_last": h, "t_end_days": t,
+                        "l2": "per step the state, B/E (RA15) or candidates (BS) exceed 126 MB only above "
+                              "~300K particles; measured as is"},
                 "clocks": clocks.summary(), "gpu_launches": launches, "events": nev, "e2e": e2e,
                 "cpu_baseline": cpu}
+        if ref_gpu is not None:
+            line["reference_cuda"] = ref_gpu
         print(json.dumps(line), flush=True)
     b.free()
 
@@ -455,7 +561,7 @@ def run_hybrid(args, rank, world, dist):
         print(json.dumps({"impl": "reference", "metric": metric, "value": value, "unit": UNIT, "n_gpus": args.gpus,
                           "steps": args.steps, "warmup": 0, "ms_per_step": dt * 1e3 / args.steps,
                           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                          "data": "synthetic", "config": {"workload": workload_text, "particles": particles},
+                          "data": "synthetic", "config": config_of(args, workload_text),
                           "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
                                            "sample": sample},
                           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
@@ -512,6 +618,20 @@ def run_hybrid(args, rank, world, dist):
                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": fresh.n * 48 / args.steps,
                "note": "wall clock around upload, hybrid_begin, the encounter subsystem, hybrid_finish and the "
                        "central screen of every step, download"}
+    ref_gpu = None
+    if world == 1:
+        # like for like with the reference's own CUDA backend on this GPU: the
+        # drop-in HYBRID calls driven as mdt_hy / mdt_hkce drive them, wall clock
+        ref_lib = load_reference_cuda()
+        if ref_lib is not None:
+            steps_cmp = min(args.steps, 3)
+            fresh = lambda: mce_init(workload(args.particles, args.seed, HYBRID_NEAR), H, 3.0)
+            ours = hybrid_wall_rate(b.lib, fresh(), 1, steps_cmp, fused=True)
+            theirs = hybrid_wall_rate(ref_lib, fresh(), 1, steps_cmp, fused=False)
+            ref_gpu = {"value": theirs, "unit": UNIT, "steps": steps_cmp, "dropin_wall": ours,
+                       "ratio_vs_reference_cuda": ours / theirs,
+                       "note": "the reference's CUDA backend (its drop-in calls one by one, as its Fortran host "
+                               "makes them) and this library on this GPU, wall clock"}
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         from oracle import oracle as O
@@ -526,12 +646,106 @@ def run_hybrid(args, rank, world, dist):
         print(json.dumps({"metric": metric, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                           "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
                           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                          "config": {"workload": workload_text, "particles_per_gpu": args.particles,
-                                     "seed": args.seed, "encounter_pairs": pairs,
-                                     "wall_ms_per_step": wall * 1e3 / args.steps},
+                          "config": config_of(args, workload_text),
+                          "run": {"encounter_pairs": pairs, "wall_ms_per_step": wall * 1e3 / args.steps},
                           "clocks": clocks.summary(), "gpu_launches": launches, "events": nev, "e2e": e2e,
-                          "cpu_baseline": cpu}), flush=True)
+                          "cpu_baseline": cpu, "reference_cuda": ref_gpu}), flush=True)
     b.free()
+
+
+def plain_loop_ms(systems, hs, steps, sample_every=8):
+    """The plain per-system kernel loop the batched launch replaces: every
+    sample_every-th system (a uniform sample of the seeded batch) uploaded to
+    the single-system path, one warm-up step, then `steps` fused MVS steps,
+    whose device time (CUDA events around the launches,
+    mercury_b200_timing) is summed; scaled to the whole batch. Uploads,
+    downloads and the warm-up are outside the timed sum."""
+    from mercuda_b200.backend import Backend
+    be = Backend("MVS")
+    be.configure()
+    total_ms, count = 0.0, 0
+    for k in range(0, len(systems), sample_every):
+        be.upload(systems[k])
+        be.mvs_advance(0.0, float(hs[k]), 1, RCEN)
+        be.mvs_advance(float(hs[k]), float(hs[k]), steps, RCEN)
+        total_ms += be.timing()["advance_ms"]
+        count += 1
+    be.free()
+    return total_ms * len(systems) / count, count
+
+
+def batched_summary(seed: int, steps: int, nsys: int = 4096):
+    """The batched extension on the 4,096-system workload beside the MVS line:
+    device particle-steps/s of one batched advance (after a tuning + warm-up
+    advance), the launch shape the tuner chose, and the speed-up over the
+    plain per-system kernel loop."""
+    from mercuda_b200.backend import Batch
+    from mercuda_b200.system import make_batch
+    systems, hs = make_batch(seed=seed + 100, nsys=nsys)
+    total = sum(s.n - s.nbig for s in systems)
+    b = Batch(systems, hs)
+    b.advance(0.0, steps, RCEN)
+    b.advance(0.0, steps, RCEN)
+    tm = b.timing()
+    b.free()
+    plain_ms, sampled = plain_loop_ms(systems, hs, steps)
+    return {"value": total * steps / (tm["ms"] * 1e-3), "unit": UNIT, "systems": nsys, "particles": total,
+            "steps": steps, "batched_ms": tm["ms"], "plain_loop_ms": plain_ms,
+            "speedup_vs_plain_loop": plain_ms / tm["ms"], "threads_per_cta": tm["threads"],
+            "steps_per_launch": tm["steps_per_launch"], "gpu_launches": tm["launches"],
+            "plain_loop_sample": f"{sampled} of {nsys} systems (every 8th), device time of each system's "
+                                 f"{steps}-step advance, scaled"}
+
+
+def adjoint_summary(seed: int, particles: int = 100_000, steps: int = 1000, every: int = 50):
+    """The adjoint extension (config 4) beside the MVS line: forward and
+    backward device time of dL/d(x0, v0, yar), L = sum |x_final|^2, and the
+    gradients of 64 random particles for the oracle check (done by the
+    caller beside the CPU leg). Returns (summary, gradients, system, picks)."""
+    import torch
+    from mercuda_b200.adjoint import mvs_trajectory, timing
+    s = workload(particles, seed, 0.0)
+    rng = np.random.default_rng(seed + 7)
+    npart = s.n - s.nbig
+    s.ngf[s.nbig:, 4] = np.exp(rng.uniform(np.log(1e-15), np.log(1e-13), npart)) * rng.choice([-1, 1], npart)
+    nb = s.nbig
+    dev = torch.device("cuda")
+
+    def once():
+        x0 = torch.tensor(s.x[nb:], device=dev, requires_grad=True)
+        v0 = torch.tensor(s.v[nb:], device=dev, requires_grad=True)
+        yar = torch.tensor(s.ngf[nb:, 4], device=dev, requires_grad=True)
+        xf, _ = mvs_trajectory(x0, v0, yar, (s.m[:nb], s.x[:nb], s.v[:nb]), H, steps, every)
+        (xf ** 2).sum().backward()
+        return np.concatenate([x0.grad.cpu().numpy(), v0.grad.cpu().numpy(), yar.grad.cpu().numpy()[:, None]],
+                              axis=1)
+
+    once()
+    g = once()
+    fwd, bwd = timing()
+    pick = np.sort(rng.choice(npart, 64, replace=False))
+    return ({"particles": particles, "steps": steps, "checkpoint_every": every, "forward_ms": fwd,
+             "backward_ms": bwd, "backward_over_forward": bwd / fwd,
+             "value": particles * steps / ((fwd + bwd) * 1e-3), "unit": UNIT}, g[pick], s, pick)
+
+
+def adjoint_oracle_error(s, pick, got, steps: int = 1000):
+    """Worst relative error of the picked particles' gradients (per block:
+    position, velocity, yar) against the oracle's FP64 tangent map."""
+    from oracle import oracle as O
+    nb = s.nbig
+    sub = s.copy()
+    keep = np.concatenate([np.arange(nb), nb + pick])
+    for name in ("m", "x", "v", "ngf", "rce", "rphys", "rcrit", "rceh", "rho"):
+        setattr(sub, name, getattr(s, name)[keep].copy())
+    J = O.mvs_jacobian(sub, H, steps)
+    xf = sub.x[nb:]
+    want = np.einsum("prk,pr->pk", J, np.concatenate([2 * xf, np.zeros_like(xf)], axis=1))
+    worst = 0.0
+    for cols in (slice(0, 3), slice(3, 6), slice(6, 7)):
+        scale = np.abs(want[:, cols]).max(axis=1, keepdims=True)
+        worst = max(worst, float(np.max(np.abs(got[:, cols] - want[:, cols]) / scale)))
+    return worst
 
 
 def run_batch(args, rank, world, dist):
@@ -557,7 +771,9 @@ def run_batch(args, rank, world, dist):
         print(json.dumps({"impl": "reference", "metric": metric, "value": value, "unit": UNIT, "n_gpus": args.gpus,
                           "steps": args.steps, "warmup": 0, "ms_per_step": dt * 1e3 / args.steps,
                           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                          "data": "synthetic", "config": {"workload": workload_text, "systems_sampled": len(sample)},
+                          "data": "synthetic",
+                          "config": config_of(args, workload_text, systems_per_gpu=args.systems,
+                                              particles_per_gpu=total),
                           "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
                                            "sample": f"{len(sample)} of the systems x {args.steps} steps"},
                           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
@@ -595,19 +811,11 @@ def run_batch(args, rank, world, dist):
                "d2h_bytes_per_step": nb * 48 / args.steps,
                "note": "wall clock around the batched upload, advance (events included) and download"}
     b.free()
-    # the plain loop: every system through the single-system path in turn
-    stride = max(1, len(systems) // 128)
-    sample = list(zip(systems[::stride], hs[::stride]))
+    # the plain loop: each system through the single-system path in turn
     barrier()
-    t0 = time.perf_counter()
-    for sys_, h_ in sample:
-        be = Backend("MVS")
-        be.configure()
-        be.upload(sys_)
-        be.mvs_advance(0.0, float(h_), args.steps, RCEN)
-        be.download()
+    plain_ms, sampled = plain_loop_ms(systems, hs, args.steps)
     barrier()
-    loop_s = (time.perf_counter() - t0) * len(systems) / len(sample)
+    sample = list(zip(systems[::8], hs[::8]))
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         from oracle import oracle as O
@@ -621,17 +829,17 @@ def run_batch(args, rank, world, dist):
         cpu = {"value": done / dt, "unit": UNIT, "cores": cores, "kind": "port",
                "sample": f"32 of the systems x {args.steps} steps ({dt:.1f} s)"}
     if rank == 0:
-        batch_s = (total * args.steps / e2e["value"]) if e2e else ms * 1e-3
         print(json.dumps({"metric": metric, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                           "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
                           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                          "config": {"workload": workload_text, "systems_per_gpu": args.systems,
-                                     "particles_per_gpu": total, "threads_per_cta": tm["threads"],
+                          "config": config_of(args, workload_text, systems_per_gpu=args.systems,
+                                              particles_per_gpu=total),
+                          "run": {"particles": total, "threads_per_cta": tm["threads"],
                                      "steps_per_launch": tm["steps_per_launch"],
-                                     "plain_loop_s_estimated": loop_s,
-                                     "batched_e2e_s": batch_s,
-                                     "speedup_vs_plain_loop": loop_s / batch_s,
-                                     "loop_sample_systems": len(sample)},
+                                     "plain_loop_ms": plain_ms, "batched_ms": ms,
+                                     "speedup_vs_plain_loop": plain_ms / ms,
+                                     "plain_loop_sample": f"{sampled} of {len(systems)} systems (every 8th), "
+                                                          "device time of each system's advance, scaled"},
                           "clocks": clocks.summary(), "gpu_launches": tm["launches"], "events": int(len(ev)),
                           "e2e": e2e, "cpu_baseline": cpu}), flush=True)
 
@@ -665,7 +873,7 @@ def run_adjoint(args, rank, world, dist):
         print(json.dumps({"impl": "reference", "metric": metric, "value": value, "unit": UNIT, "n_gpus": args.gpus,
                           "steps": args.steps, "warmup": 0, "ms_per_step": dt * 1e3 / args.steps,
                           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                          "data": "synthetic", "config": {"workload": workload_text, "particles": n},
+                          "data": "synthetic", "config": config_of(args, workload_text),
                           "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
                                            "sample": f"{n} particles x {args.steps} steps, forward-mode tangents "
                                                      f"of the oracle ({dt:.1f} s)"},
@@ -710,8 +918,8 @@ def run_adjoint(args, rank, world, dist):
         print(json.dumps({"metric": metric, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                           "warmup": max(1, args.warmup), "ms_per_step": ms / args.steps, "higher_is_better": True,
                           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                          "config": {"workload": workload_text, "particles_per_gpu": args.particles,
-                                     "forward_ms": fwd, "backward_ms": bwd, "backward_over_forward": bwd / fwd,
+                          "config": config_of(args, workload_text),
+                          "run": {"forward_ms": fwd, "backward_ms": bwd, "backward_over_forward": bwd / fwd,
                                      "checkpoint_every": args.checkpoint_every,
                                      "grad_finite": bool(np.all(np.isfinite(gx)))},
                           "clocks": clocks.summary(), "gpu_launches": 3,
@@ -757,7 +965,7 @@ def run_hybrid_adjoint(args, rank, world, dist):
         print(json.dumps({"impl": "reference", "metric": metric, "value": value, "unit": UNIT, "n_gpus": args.gpus,
                           "steps": args.steps, "warmup": 0, "ms_per_step": dt * 1e3 / args.steps,
                           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                          "data": "synthetic", "config": {"workload": workload_text, "particles": n},
+                          "data": "synthetic", "config": config_of(args, workload_text),
                           "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
                                            "sample": f"{n} particles x {args.steps} steps, forward-mode tangents "
                                                      f"of the oracle's mdt_hy ({dt:.1f} s)"},
@@ -819,8 +1027,8 @@ def run_hybrid_adjoint(args, rank, world, dist):
         print(json.dumps({"metric": metric, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                           "warmup": max(1, args.warmup), "ms_per_step": ms / args.steps, "higher_is_better": True,
                           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                          "config": {"workload": workload_text, "particles_per_gpu": args.particles,
-                                     "forward_wall_ms": fwd, "backward_ms": bwd, "backward_over_forward": bwd / fwd,
+                          "config": config_of(args, workload_text),
+                          "run": {"forward_wall_ms": fwd, "backward_ms": bwd, "backward_over_forward": bwd / fwd,
                                      "member_steps": members, "checkpoint_every": args.checkpoint_every,
                                      "grad_finite": bool(np.all(np.isfinite(gx)))},
                           "clocks": clocks.summary(), "gpu_launches": launches,
@@ -937,9 +1145,19 @@ def main():
         dropin = {"value": dropin_steps(b.lib, workload(args.particles, args.seed), DROPIN_STEPS), "unit": UNIT,
                   "steps": DROPIN_STEPS, "note": "mercury_cuda_step + mercury_cuda_events per step, wall clock"}
 
+    # the metric's second half on the same GPU: the batched launch against the
+    # plain per-system loop, and the adjoint against the forward sweep
+    batched = adjoint = None
+    if world == 1 and not args.no_extras:
+        batched = batched_summary(args.seed, args.steps)
+        adjoint, adj_grads, adj_sys, adj_pick = adjoint_summary(args.seed)
+
     cpu = None
     parity = None
     if rank == 0 and not args.no_cpu_baseline:
+        if adjoint is not None:
+            # the oracle as the checker of the adjoint's gradients (64 particles)
+            adjoint["grad_rel_err_vs_oracle_64"] = adjoint_oracle_error(adj_sys, adj_pick, adj_grads)
         sample_particles, sample_steps = 300_000, 457
         v_cpu, cores, dt = cpu_baseline(sample_particles, sample_steps, args.seed)
         cpu = {"value": v_cpu, "unit": UNIT, "cores": cores, "kind": "port",
@@ -952,12 +1170,8 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"MVS, {args.particles} massless particles + 8 planets per GPU, h=8 d, "
-                                   "1% near planets, encounter + central screens every step",
-                       "particles_per_gpu": args.particles, "h_days": H, "seed": args.seed,
-                       "steps_per_launch": steps_per_launch, "threads_per_cta": args.threads or 128,
-                       "l2": "state 9 doubles/particle double-buffered (144 MB) > 126 MB L2; "
-                             "each launch reads and writes it once"},
+            "config": config_of(args, MVS_TEXT.format(n=args.particles), h_days=H, l2=MVS_L2),
+            "run": {"steps_per_launch": steps_per_launch, "threads_per_cta": args.threads or 128},
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak_tflops, "unit": "TFLOP/s",
                          "frac": achieved / peak_tflops,
                          "traffic": (sum(TRAFFIC_MB_PER_LAUNCH[steps_per_launch]) * args.particles
@@ -978,6 +1192,10 @@ def main():
             line["dropin_per_step"] = dropin
         if parity is not None:
             line["parity"] = parity
+        if batched is not None:
+            line["batched"] = batched
+        if adjoint is not None:
+            line["adjoint"] = adjoint
         print(json.dumps(line), flush=True)
     b.free()
     if dist:

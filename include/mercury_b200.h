@@ -153,9 +153,12 @@ int mercury_b200_batch_advance(double time, int nsteps, double rcen, int* nevent
 int mercury_b200_batch_events(MercuryEvent* events, int* sys, int* steps, int cap);
 /* Current state of every body into the concatenated host arrays x, v. */
 int mercury_b200_batch_download(double* x, double* v);
-/* Launch shape: particle CTA size (64, 128 or 256; 0 = tune on the next
- * advance), steps per launch (0 = automatic), CUDA-graph replay of the
- * chunk loop (1/0); a negative value keeps the setting. */
+/* Launch shape: particle CTA size (64, 128 or 256; 0 = tuned), steps per
+ * launch (1..64; 0 = tuned), CUDA-graph replay of the chunk loop (1/0); a
+ * negative value keeps the setting. Before the first advance after an upload
+ * or a change here, the library times short trial runs of every free choice
+ * (steps per launch 8, 16, 31, 64 x CTA size 64, 128, 256), rolls the state
+ * back, and keeps the fastest per step. */
 int mercury_b200_batch_set(int threads, int steps_per_launch, int use_graph);
 /* Device time and kernel count of the last advance, and the launch shape it used. */
 int mercury_b200_batch_timing(double* ms, int* launches, int* threads, int* steps_per_launch);

@@ -8,8 +8,9 @@
 //               classification of its encounter candidates
 //
 // The chunk loop of a run is captured once into a CUDA graph and replayed for
-// later runs of the same shape. The particle kernel's CTA size is chosen by
-// timing the first chunk of the first run.
+// later runs of the same shape. The launch shape (steps per launch and the
+// particle kernel's CTA size) is chosen by timing short trial runs before the
+// first run (tune).
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -50,6 +51,7 @@ struct Batch {
     int cur = 0;
     bool reset = true;
     int threads = 0;                 // 0: tune on the first run
+    int tuned_K = 31, tuned_threads = 128;
     int forced_threads = 0, forced_K = 0, use_graph = 1;
     cudaStream_t stream = nullptr, stream_big = nullptr;
     cudaEvent_t t0 = nullptr, t1 = nullptr;
@@ -227,34 +229,55 @@ int enqueue_run(Batch& B, int nsteps, double rcen, int reset0, int central) {
     return launches;
 }
 
-// Times one chunk of the particle kernel for each CTA size and keeps the
-// fastest; the state is not advanced (outputs go to the other buffer).
-void tune(Batch& B, double rcen) {
-    if (B.forced_threads > 0) {
-        B.threads = B.forced_threads;
-        return;
-    }
-    B.threads = 128;
-    if (B.ntiles == 0) return;
-    const int ks = B.K;
-    check(cudaMemsetAsync(B.status.p, 0, sizeof(DeviceStatus), B.stream), "memset");
-    launch_mvs_big_batch(big_chunk(B, 0, ks, B.reset ? 1 : 0, 1, 0, rcen), B.nsys, B.max_nbig, B.stream);
-    float best = 1e30f;
-    for (int threads : {64, 128, 256}) {
-        check(cudaMemsetAsync(&B.status.p->next_tile, 0, sizeof(int), B.stream), "memset");
-        check(cudaMemsetAsync(&B.status.p->events, 0, sizeof(int), B.stream), "memset");
-        check(cudaMemsetAsync(&B.status.p->cands, 0, sizeof(int), B.stream), "memset");
-        check(cudaEventRecord(B.t0, B.stream), "event");
-        launch_mvs_particles_batch(particle_chunk(B, 0, ks, B.reset ? 1 : 0, 1, 0, rcen), B.stream, threads);
-        check(cudaEventRecord(B.t1, B.stream), "event");
-        check(cudaEventSynchronize(B.t1), "tune");
-        float ms = 0.0f;
-        check(cudaEventElapsedTime(&ms, B.t0, B.t1), "tune");
-        if (ms < best) {
-            best = ms;
+// The launch shape of a batch: for every steps-per-launch K (8, 16, 31, 64)
+// and particle CTA size (64, 128, 256) a short pipelined trial run of two
+// chunks (Big-body CTAs on their stream ahead of the particle launches, as
+// the real runs make them), timed with CUDA events; the fastest time per step
+// wins. The trials start from the batch's state and it is restored after
+// them (the snapshot), so tuning advances nothing. A forced CTA size or K
+// (mercury_b200_batch_set) limits the search to it; the choice is kept and
+// reported by mercury_b200_batch_timing.
+void tune(Batch& B, double rcen, int nsteps) {
+    std::vector<int> Ks = {8, 16, 31, 64};
+    std::vector<int> Ts = {64, 128, 256};
+    if (B.forced_K > 0) Ks = {B.forced_K};
+    if (B.forced_threads > 0) Ts = {B.forced_threads};
+    for (int& k : Ks) k = std::max(1, std::min(k, nsteps));
+    std::sort(Ks.begin(), Ks.end());
+    Ks.erase(std::unique(Ks.begin(), Ks.end()), Ks.end());
+    B.threads = Ts[0];
+    B.tuned_K = Ks[0];
+    if (B.ntiles == 0 || (Ks.size() == 1 && Ts.size() == 1)) return;
+    const size_t bigs = B.bm.n;
+    auto copy = [&](void* d, const void* src, size_t bytes) {
+        check(cudaMemcpyAsync(d, src, bytes, cudaMemcpyDeviceToDevice, B.stream), "tune");
+    };
+    copy(B.snap.p, B.pstate[B.cur].p, sizeof(double) * 9 * B.npcap);
+    copy(B.snap.p + 9 * (size_t)B.npcap, B.bigbuf[B.cur].p, sizeof(double) * 9 * bigs);
+    B.ensure_chunk_events(2);
+    double best = 1e300;
+    for (int K : Ks) {
+        layout_tables(B, K);
+        const int steps = std::min(nsteps, 2 * K);
+        for (int threads : Ts) {
             B.threads = threads;
+            check(cudaEventRecord(B.t0, B.stream), "event");
+            enqueue_run(B, steps, rcen, B.reset ? 1 : 0, 1);
+            check(cudaEventRecord(B.t1, B.stream), "event");
+            check(cudaEventSynchronize(B.t1), "tune");
+            float ms = 0.0f;
+            check(cudaEventElapsedTime(&ms, B.t0, B.t1), "tune");
+            const double per_step = ms / steps;
+            if (per_step < best) {
+                best = per_step;
+                B.tuned_K = K;
+                B.tuned_threads = threads;
+            }
+            copy(B.pstate[B.cur].p, B.snap.p, sizeof(double) * 9 * B.npcap);
+            copy(B.bigbuf[B.cur].p, B.snap.p + 9 * (size_t)B.npcap, sizeof(double) * 9 * bigs);
         }
     }
+    B.threads = B.tuned_threads;
     check(cudaGetLastError(), "tune");
 }
 
@@ -429,6 +452,8 @@ int mercury_b200_batch_upload(int nsys, const int* body_offset, const int* nbig,
         B.cur = 0;
         B.reset = true;
         B.threads = 0;
+        B.tuned_K = 31;
+        B.tuned_threads = 128;
         return 0;
     } catch (const std::exception& e) {
         return report(e);
@@ -440,13 +465,13 @@ int mercury_b200_batch_advance(double time, int nsteps, double rcen, int* nevent
     try {
         if (B.nsys < 1) throw std::runtime_error("no batch uploaded");
         if (nsteps < 1) throw std::runtime_error("nsteps must be positive");
-        int K = B.forced_K > 0 ? B.forced_K : 31;
+        if (B.threads == 0) tune(B, rcen, nsteps);
+        int K = B.forced_K > 0 ? B.forced_K : B.tuned_K;
         K = std::max(1, std::min(K, nsteps));
         if (K != B.K) layout_tables(B, K);
         const int nchunks = (nsteps + K - 1) / K;
         B.ensure_chunk_events(std::max(2, nchunks));
         const int reset0 = B.reset ? 1 : 0;
-        if (B.threads == 0) tune(B, rcen);
         // starting state, for a redo after an event-buffer overflow
         const size_t bigs = B.bm.n;
         auto copy = [&](void* d, const void* s, size_t bytes) {
@@ -583,9 +608,12 @@ int mercury_b200_batch_set(int threads, int steps_per_launch, int use_graph) {
     if (threads > 0 && threads != 64 && threads != 128 && threads != 256) return 1;
     if (threads >= 0) {
         B.forced_threads = threads;
-        B.threads = threads;
+        B.threads = 0;   // tuned again (over K only when threads is forced)
     }
-    if (steps_per_launch >= 0) B.forced_K = std::min(steps_per_launch, 64);
+    if (steps_per_launch >= 0) {
+        B.forced_K = std::min(steps_per_launch, 64);
+        B.threads = 0;
+    }
     if (use_graph >= 0) B.use_graph = use_graph ? 1 : 0;
     return 0;
 }

@@ -22,6 +22,25 @@ template <int VARIANT> __device__ __forceinline__ double level_h2(double h0, int
     return h * h;
 }
 
+// The Neville update of mdt_bs1/mdt_bs2 (mercury6_2.for:3352-3366,
+// 3545-3560) for level n and j < n: D(j) = tmp1 * D(j + 1) - tmp2 * D(j) with
+// tmp0 = 1 / (h2(j) - h2(n)), tmp1 = tmp0 * h2(j + 1), tmp2 = tmp0 * h2(n).
+// The coefficients depend on the trial step only, so each CTA evaluates the
+// L(L-1)/2 pairs once (the same statements) into co[coef_index(n, j)].
+__host__ __device__ constexpr int coef_index(int n, int j) { return (n - 1) * (n - 2) / 2 + j - 1; }
+template <int VARIANT> __device__ __forceinline__ void neville_coefficients(double h0, double (*co)[2]) {
+    constexpr int L = bs_levels(VARIANT);
+    for (int q = threadIdx.x; q < L * (L - 1) / 2; q += blockDim.x) {
+        int n = 2;
+        while (q >= n * (n - 1) / 2) ++n;
+        const int j = q - (n - 1) * (n - 2) / 2 + 1;
+        const double h2n = level_h2<VARIANT>(h0, n);
+        const double tmp0 = 1.0 / (level_h2<VARIANT>(h0, j) - h2n);
+        co[q][0] = tmp0 * level_h2<VARIANT>(h0, j + 1);
+        co[q][1] = tmp0 * h2n;
+    }
+}
+
 __device__ __forceinline__ void level_error(double err, bool finite, unsigned long long* dst) {
     atomicMax(dst, finite ? (unsigned long long)__double_as_longlong(err) : ERR_NONFINITE);
 }
@@ -325,30 +344,42 @@ template <int VARIANT> __global__ void __launch_bounds__(256) bs_massive_level_k
     }
 }
 
-// The massive set's extrapolation in level order (one CTA): the Neville
-// updates (mercury6_2.for:3352-3366), each thread its own bodies, then from
-// level 4 on the level's error maximum and candidate state.
+// The massive set's extrapolation in level order (one CTA): per level the
+// Neville updates (mercury6_2.for:3352-3366) with one thread per (body,
+// component) and the coefficients computed once, then from level 4 on each
+// (body, component)'s candidate sum and each body's error term for the
+// level's maximum.
 template <int VARIANT> __global__ void __launch_bounds__(256) bs_massive_extrap_kernel(BsArgs A) {
     const int N = A.f.nsplit, tid = threadIdx.x, nt = blockDim.x;
-    const int L = bs_levels(VARIANT);
+    constexpr int L = bs_levels(VARIANT);
     double* D = A.draw;
+    __shared__ double co[L * (L - 1) / 2][2];
     __shared__ double wmax[8];
     __shared__ int wbad[8];
+    neville_coefficients<VARIANT>(A.h0, co);
+    __syncthreads();
+    const int nb1 = N - 1, M = 6 * nb1;
     for (int n = 1; n <= L; ++n) {
-        const double h2n = level_h2<VARIANT>(A.h0, n);
-        for (int j = n - 1; j >= 1; --j) {
-            const double tmp0 = 1.0 / (level_h2<VARIANT>(A.h0, j) - h2n);
-            const double tmp1 = tmp0 * level_h2<VARIANT>(A.h0, j + 1);
-            const double tmp2 = tmp0 * h2n;
-            double* Dj = D + (size_t)(j - 1) * 6 * N;
-            const double* Dj1 = D + (size_t)j * 6 * N;
-            for (int k = 1 + tid; k < N; k += nt)
-                for (int c = 0; c < 6; ++c) Dj[c * N + k] = tmp1 * Dj1[c * N + k] - tmp2 * Dj[c * N + k];
+        for (int q = tid; q < M; q += nt) {
+            const int c = q / nb1, k = 1 + q % nb1;
+            for (int j = n - 1; j >= 1; --j) {
+                const double* cj = co[coef_index(n, j)];
+                double* Dj = D + (size_t)(j - 1) * 6 * N;
+                const double* Dj1 = D + (size_t)j * 6 * N;
+                Dj[c * N + k] = cj[0] * Dj1[c * N + k] - cj[1] * Dj[c * N + k];
+            }
         }
         if (n > 3) {
+            __syncthreads();
+            double* cand = A.bcand + (size_t)(n - 4) * 6 * N;
+            for (int q = tid; q < M; q += nt) {
+                const int c = q / nb1, k = 1 + q % nb1;
+                double s = D[c * N + k];
+                for (int j = 2; j <= n; ++j) s = s + D[(size_t)(j - 1) * 6 * N + c * N + k];
+                cand[c * N + k] = s;
+            }
             double emax = 0.0;
             int bad = 0;
-            double* cand = A.bcand + (size_t)(n - 4) * 6 * N;
             for (int k = 1 + tid; k < N; k += nt) {
                 const double* X0 = A.bx;
                 const double* V0 = A.bx + 3 * N;
@@ -356,16 +387,11 @@ template <int VARIANT> __global__ void __launch_bounds__(256) bs_massive_extrap_
                 const double tmp2 = V0[k] * V0[k] + V0[N + k] * V0[N + k] + V0[2 * N + k] * V0[2 * N + k];
                 const double xscal = 1.0 / fmax(tmp1, 1e-300);
                 const double vscal = 1.0 / fmax(tmp2, 1e-300);
-                double q[6];
-                for (int c = 0; c < 6; ++c) q[c] = D[c * N + k];
+                double q6[6];
+                for (int c = 0; c < 6; ++c) q6[c] = D[c * N + k];
                 double e;
-                if (body_error(q, xscal, vscal, e)) emax = fmax(emax, e);
+                if (body_error(q6, xscal, vscal, e)) emax = fmax(emax, e);
                 else bad = 1;
-                for (int c = 0; c < 6; ++c) {
-                    double s = q[c];
-                    for (int j = 2; j <= n; ++j) s = s + D[(size_t)(j - 1) * 6 * N + c * N + k];
-                    cand[c * N + k] = s;
-                }
             }
             for (int o = 16; o; o >>= 1) {
                 emax = fmax(emax, __shfl_xor_sync(FULLMASK, emax, o));
@@ -388,14 +414,20 @@ template <int VARIANT> __global__ void __launch_bounds__(256) bs_massive_extrap_
 // Thirty-two particle slots per CTA, one lane each; warp w computes the raw
 // states D(n) of levels w + 1 and L - w (n + (L + 1 - n) force calls per warp,
 // balanced) into shared memory, from the start-of-step force that warp 0
-// computes. Warp 0 then runs the Neville updates in level order, each level's
-// error maximum and candidate state: per particle the same statements, in the
-// same order, as a level loop would run them.
+// computes. Then warp w takes components w, w + (warps), ... of every
+// particle through the Neville updates in level order, in registers, with the
+// coefficients computed once per CTA, writing each level's candidate
+// component and the error inputs; last, the warps share the levels' error
+// maxima. Per particle and component the same statements, in the same order,
+// as a level loop would run them.
 template <int VARIANT> __global__ void __launch_bounds__(bs_levels(VARIANT) * 16) bs_particle_kernel(BsArgs A) {
     constexpr int L = bs_levels(VARIANT);
+    constexpr int NW = L * 16 / 32;   // warps of the CTA
     __shared__ double dsm[L][6][32];
     __shared__ double a0sm[3][32];
+    __shared__ double co[L * (L - 1) / 2][2];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    neville_coefficients<VARIANT>(A.h0, co);
     const int p = blockIdx.x * 32 + lane;
     const bool ok = p < A.np && A.perm[p] < A.active_np;
     const int nb = A.f.nbig - 1, stride = force_row(nb), S = A.npcap;
@@ -488,7 +520,32 @@ template <int VARIANT> __global__ void __launch_bounds__(bs_levels(VARIANT) * 16
         }
     }
     __syncthreads();
-    if (w != 0) return;
+    // Neville updates in level order, one component per warp pass: D(j) of the
+    // lane's particle in registers; after level n (n > 3) the candidate
+    // component D(1) + ... + D(n) goes out and D(1) stays in dsm for the error
+    if (ok) {
+        for (int c = w; c < 6; c += NW) {
+            double D[L];
+#pragma unroll
+            for (int n = 0; n < L; ++n) D[n] = dsm[n][c][lane];
+#pragma unroll
+            for (int n = 1; n <= L; ++n) {
+#pragma unroll
+                for (int j = n - 1; j >= 1; --j) {
+                    const double* cj = co[coef_index(n, j)];
+                    D[j - 1] = cj[0] * D[j] - cj[1] * D[j - 1];
+                }
+                if (n > 3) {
+                    double sum = D[0];
+#pragma unroll
+                    for (int j = 2; j <= n; ++j) sum = sum + D[j - 1];
+                    A.pcand[(size_t)(n - 4) * 6 * S + (size_t)c * S + p] = sum;
+                    dsm[n - 1][c][lane] = D[0];
+                }
+            }
+        }
+    }
+    __syncthreads();
     double xscal = 0.0, vscal = 0.0;
     if (ok) {
         const double tmp1 = x0.x * x0.x + x0.y * x0.y + x0.z * x0.z;
@@ -496,41 +553,22 @@ template <int VARIANT> __global__ void __launch_bounds__(bs_levels(VARIANT) * 16
         xscal = 1.0 / fmax(tmp1, 1e-300);
         vscal = 1.0 / fmax(tmp2, 1e-300);
     }
-    auto D = [&](int j, int c) -> double& { return dsm[j - 1][c][lane]; };
-#pragma unroll 1
-    for (int n = 1; n <= L; ++n) {
+    // each level's error maximum (mercury6_2.for:3372-3378), levels shared by the warps
+    for (int n = 4 + w; n <= L; n += NW) {
+        double emax = 0.0;
+        int bad = 0;
         if (ok) {
-            const double h2n = level_h2<VARIANT>(A.h0, n);
-#pragma unroll 1
-            for (int j = n - 1; j >= 1; --j) {
-                const double tmp0 = 1.0 / (level_h2<VARIANT>(A.h0, j) - h2n);
-                const double tmp1 = tmp0 * level_h2<VARIANT>(A.h0, j + 1);
-                const double tmp2 = tmp0 * h2n;
-                for (int c = 0; c < 6; ++c) D(j, c) = tmp1 * D(j + 1, c) - tmp2 * D(j, c);
-            }
+            double q[6];
+            for (int c = 0; c < 6; ++c) q[c] = dsm[n - 1][c][lane];
+            double e;
+            if (body_error(q, xscal, vscal, e)) emax = e;
+            else bad = 1;
         }
-        if (n > 3) {
-            double emax = 0.0;
-            int bad = 0;
-            if (ok) {
-                double q[6];
-                for (int c = 0; c < 6; ++c) q[c] = D(1, c);
-                double e;
-                if (body_error(q, xscal, vscal, e)) emax = e;
-                else bad = 1;
-                double* cand = A.pcand + (size_t)(n - 4) * 6 * S;
-                for (int c = 0; c < 6; ++c) {
-                    double s = q[c];
-                    for (int j = 2; j <= n; ++j) s = s + D(j, c);
-                    cand[(size_t)c * S + p] = s;
-                }
-            }
-            for (int o = 16; o; o >>= 1) {
-                emax = fmax(emax, __shfl_xor_sync(FULLMASK, emax, o));
-                bad |= __shfl_xor_sync(FULLMASK, bad, o);
-            }
-            if (lane == 0 && (emax > 0.0 || bad)) level_error(emax, !bad, &A.errs[n]);
+        for (int o = 16; o; o >>= 1) {
+            emax = fmax(emax, __shfl_xor_sync(FULLMASK, emax, o));
+            bad |= __shfl_xor_sync(FULLMASK, bad, o);
         }
+        if (lane == 0 && (emax > 0.0 || bad)) level_error(emax, !bad, &A.errs[n]);
     }
 }
 

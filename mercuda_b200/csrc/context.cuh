@@ -182,11 +182,13 @@ struct Context {
     int* permp() { return perm[kc].p; }
     int steps_since_order = 0;
 
+    // The massive set's state buffer k as the MVS Big-body CTA reads it
+    // (stride nsplit: Big bodies, then the massive Small bodies it holds).
     BigState big(int k) {
         BigState b;
         b.x = bigstate[k].p;
-        b.v = bigstate[k].p + 3 * nbig;
-        b.a = bigstate[k].p + 6 * nbig;
+        b.v = bigstate[k].p + 3 * nsplit;
+        b.a = bigstate[k].p + 6 * nsplit;
         return b;
     }
     void ensure_streams() {
