@@ -103,7 +103,8 @@ def parse_args():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-extras", action="store_true",
-                   help="skip the batched and adjoint summaries of the default MVS line")
+                   help="skip the batched and adjoint summaries of the default MVS line and the reference-GPU "
+                        "comparisons of the adaptive and HYBRID lines")
     p.add_argument("--workload", default="mvs", choices=["mvs", "radau", "bs", "bs2", "hybrid", "batch", "adjoint",
                                                          "hybrid_adjoint"])
     p.add_argument("--checkpoint-every", type=int, default=50)
@@ -494,9 +495,10 @@ def run_adaptive(args, rank, world, dist):
     if not args.no_e2e:
         fresh = pinned_system(adaptive_workload(args.particles, args.seed, rank))
         out = (pinned_like(np.zeros((fresh.n, 3))), pinned_like(np.zeros((fresh.n, 3))))
+        flag = fresh.ngflag
         barrier()
         t0 = time.perf_counter()
-        b.upload(fresh)
+        b.upload(fresh, flag)
         run(0.0, ADAPTIVE_H0, args.steps)
         x, v = b.download(out=out)
         barrier()
@@ -507,7 +509,7 @@ def run_adaptive(args, rank, world, dist):
                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": fresh.n * 48 / args.steps,
                "note": "wall clock around upload, the drop-in step + events calls of every step, download"}
     ref_gpu = None
-    if world == 1:
+    if world == 1 and not args.no_extras:
         # like for like with the reference's own CUDA backend on this GPU: the
         # same drop-in calls on the same workload, wall clock for both
         ref_lib = load_reference_cuda()
@@ -603,9 +605,10 @@ def run_hybrid(args, rank, world, dist):
     if not args.no_e2e:
         fresh = pinned_system(mce_init(workload(args.particles, args.seed, HYBRID_NEAR, rank), H, 3.0))
         out = (pinned_like(np.zeros((fresh.n, 3))), pinned_like(np.zeros((fresh.n, 3))))
+        flag = fresh.ngflag
         barrier()
         t0 = time.perf_counter()
-        b.upload(fresh)
+        b.upload(fresh, flag)
         state = {"dtflag": 0}
         sysw = fresh
         run(0.0, args.steps)
@@ -619,7 +622,7 @@ def run_hybrid(args, rank, world, dist):
                "note": "wall clock around upload, hybrid_begin, the encounter subsystem, hybrid_finish and the "
                        "central screen of every step, download"}
     ref_gpu = None
-    if world == 1:
+    if world == 1 and not args.no_extras:
         # like for like with the reference's own CUDA backend on this GPU: the
         # drop-in HYBRID calls driven as mdt_hy / mdt_hkce drive them, wall clock
         ref_lib = load_reference_cuda()
@@ -731,21 +734,32 @@ def adjoint_summary(seed: int, particles: int = 100_000, steps: int = 1000, ever
 
 def adjoint_oracle_error(s, pick, got, steps: int = 1000):
     """Worst relative error of the picked particles' gradients (per block:
-    position, velocity, yar) against the oracle's FP64 tangent map."""
+    position, velocity, yar) against the oracle's FP64 tangent map, over the
+    particles whose trajectories are well conditioned: a relative change of
+    1e-15 in the initial positions stays below 1e-9 in the final ones. The
+    others (close planetary approaches) amplify rounding by 1e6 and more, so
+    two FP64 evaluations in different orders legitimately differ there; they
+    are counted, not compared."""
     from oracle import oracle as O
     nb = s.nbig
     sub = s.copy()
     keep = np.concatenate([np.arange(nb), nb + pick])
     for name in ("m", "x", "v", "ngf", "rce", "rphys", "rcrit", "rceh", "rho"):
         setattr(sub, name, getattr(s, name)[keep].copy())
+    a, b = sub.copy(), sub.copy()
+    b.x[nb:] *= 1.0 + 1e-15
+    O.mvs_run(a, 0.0, H, steps, RCEN, central=False, threads=os.cpu_count() or 1)
+    O.mvs_run(b, 0.0, H, steps, RCEN, central=False, threads=os.cpu_count() or 1)
+    spread = np.abs(a.x[nb:] - b.x[nb:]).max(axis=1) / np.abs(a.x[nb:]).max(axis=1)
+    calm = spread < 1e-9
     J = O.mvs_jacobian(sub, H, steps)
     xf = sub.x[nb:]
     want = np.einsum("prk,pr->pk", J, np.concatenate([2 * xf, np.zeros_like(xf)], axis=1))
     worst = 0.0
     for cols in (slice(0, 3), slice(3, 6), slice(6, 7)):
-        scale = np.abs(want[:, cols]).max(axis=1, keepdims=True)
-        worst = max(worst, float(np.max(np.abs(got[:, cols] - want[:, cols]) / scale)))
-    return worst
+        scale = np.abs(want[calm, cols]).max(axis=1, keepdims=True)
+        worst = max(worst, float(np.max(np.abs(got[calm, cols] - want[calm, cols]) / scale)))
+    return worst, int((~calm).sum())
 
 
 def run_batch(args, rank, world, dist):
@@ -1125,9 +1139,10 @@ def main():
         nbig = fresh.nbig
         ids = np.concatenate([np.arange(nbig), nbig + rank * args.particles + np.arange(args.particles)])
         run = ShardedRun(ranks, b)
+        flag = fresh.ngflag   # derived from the input once, as mio_in does
         barrier()
         t0 = time.perf_counter()
-        run.upload(fresh, ids, nbig + world * args.particles)
+        run.upload(fresh, ids, nbig + world * args.particles, flag)
         got = run.advance(0.0, H, args.steps, RCEN, args.steps_per_launch)
         x, v = run.download(gather=False, out=(xo, vo))
         barrier()
@@ -1157,7 +1172,9 @@ def main():
     if rank == 0 and not args.no_cpu_baseline:
         if adjoint is not None:
             # the oracle as the checker of the adjoint's gradients (64 particles)
-            adjoint["grad_rel_err_vs_oracle_64"] = adjoint_oracle_error(adj_sys, adj_pick, adj_grads)
+            err, chaotic = adjoint_oracle_error(adj_sys, adj_pick, adj_grads)
+            adjoint["grad_rel_err_vs_oracle"] = err
+            adjoint["grad_checked"] = f"{len(adj_pick) - chaotic} of 64 random particles ({chaotic} chaotic left out)"
         sample_particles, sample_steps = 300_000, 457
         v_cpu, cores, dt = cpu_baseline(sample_particles, sample_steps, args.seed)
         cpu = {"value": v_cpu, "unit": UNIT, "cores": cores, "kind": "port",

@@ -183,9 +183,12 @@ class Backend:
             raise BackendError("CUDA algorithm initialization failed")
 
     # gpu_push (mercury_gpu.f90:139-151)
-    def upload(self, sys: System) -> None:
+    def upload(self, sys: System, ngflag: int | None = None) -> None:
+        """ngflag: the force-law flag that mio_in derives from the input once
+        (mercury6_2.for:6360-6371); None derives it from sys.ngf here."""
         self.n, self.nbig = sys.n, sys.nbig
-        rc = self.lib.mercury_cuda_upload(sys.n, sys.nbig, int(sys.pn), sys.ngflag, _p(sys.m), _p(sys.x), _p(sys.v),
+        flag = sys.ngflag if ngflag is None else int(ngflag)
+        rc = self.lib.mercury_cuda_upload(sys.n, sys.nbig, int(sys.pn), flag, _p(sys.m), _p(sys.x), _p(sys.v),
                                           _p(sys.ngf), _p(sys.jcen), _p(sys.rce), _p(sys.rphys))
         if rc != 0:
             raise BackendError("CUDA state upload failed")

@@ -292,7 +292,7 @@ void particles_and_events(const MvsParticleArgs& pa, cudaStream_t s) {
     Context& c = ctx();
     check(cudaMemsetAsync(&c.status.p->next_tile, 0, sizeof(int), s), "memset");
     launch_mvs_particles(pa, s, c.particle_threads);
-    ClassifyArgs ca;
+    ClassifyArgs ca{};
     ca.nb = c.nbig - 1;
     ca.nbig = c.nbig;
     ca.h = pa.h;
@@ -464,7 +464,9 @@ void ra15_step_once(double time, double* h, double* hdid, double tol, int64_t* r
 // Every level of one mdt_bs1 (algorithm 2) or mdt_bs2 (algorithm 3) attempt
 // at trial step h from the current state buffer: per-level error maxima in
 // bs_errs, per-level force faults in bs_lvst, candidates for the commit.
-BsArgs launch_bs_attempt(double h) {
+// The arguments of one BS/BS2 attempt from the current buffer with trial
+// step h (the workspace reserved).
+BsArgs bs_attempt_args(double h) {
     Context& c = ctx();
     const int V = c.algorithm == 2 ? 1 : 2;
     const int L = bs_levels(V), nb = c.nbig - 1, N = c.nsplit;
@@ -475,8 +477,6 @@ BsArgs launch_bs_attempt(double h) {
     c.bs_errs.reserve(13);
     c.bs_lvst.reserve(13);
     const int in = c.cur;
-    check(cudaMemsetAsync(c.bs_errs.p, 0, sizeof(unsigned long long) * 13, c.stream), "memset");
-    check(cudaMemsetAsync(c.bs_lvst.p, 0, sizeof(DeviceStatus) * 13, c.stream), "memset");
     BsArgs a{};
     a.f = force_cfg();
     a.variant = V;
@@ -501,6 +501,14 @@ BsArgs launch_bs_attempt(double h) {
     a.adj = c.adj.p;
     a.perm = c.permp();
     a.active_np = c.bs_active_np >= 0 ? std::min(c.bs_active_np, c.np) : c.np;
+    return a;
+}
+
+BsArgs launch_bs_attempt(double h) {
+    Context& c = ctx();
+    const BsArgs a = bs_attempt_args(h);
+    check(cudaMemsetAsync(c.bs_errs.p, 0, sizeof(unsigned long long) * 13, c.stream), "memset");
+    check(cudaMemsetAsync(c.bs_lvst.p, 0, sizeof(DeviceStatus) * 13, c.stream), "memset");
     launch_bs_sequence(a, c.stream);
     c.dropin_launches += 2 + (c.np > 0 ? 1 : 0);  // level CTAs, extrapolation, particles
     check(cudaGetLastError(), "launch");
@@ -538,10 +546,11 @@ int bs_accept_level(const unsigned long long* errs, const DeviceStatus* lv, int 
 
 // Copies level `accepted` of attempt a into the other state buffer (and
 // pushes the encounter members' tangents through it when they are kept).
-void launch_bs_commit_of(const BsArgs& a, int accepted) {
+void launch_bs_commit_of(const BsArgs& a, int accepted, const EncCtl* ctl = nullptr) {
     Context& c = ctx();
     const int in = c.cur, out = 1 - c.cur;
     BsCommitArgs k{};
+    k.ctl = ctl;
     k.nsplit = c.nsplit;
     k.np = c.np;
     k.npcap = c.npcap;
@@ -609,25 +618,27 @@ void bs_step_once(double time, double* h, double* hdid, double tol, int64_t* rej
 // particles' box overlaps as candidates, classified like the MVS path's.
 // Records are appended at the status counter and tagged `step`; the caller
 // clears the candidate counter first.
-void launch_pair_screen(double h, int step) {
+void launch_pair_screen(double h, int step, const EncCtl* ctl = nullptr, int prev = -1, int cur = -1) {
     Context& c = ctx();
     const int nb = c.nbig - 1;
     c.boxes.reserve((size_t)4 * std::max(1, nb));
     c.detail.reserve((size_t)std::max(1, nb) * TAB_DETAIL);
-    const int prev = 1 - c.cur;
+    if (cur < 0) cur = c.cur;
+    if (prev < 0) prev = 1 - cur;
     ScreenArgs a{};
+    a.ctl = ctl;
     a.nbig = c.nbig;
     a.nsplit = c.nsplit;
     a.np = c.np;
     a.npcap = c.npcap;
     a.h = h;
     a.b0 = c.bigstate[prev].p;
-    a.b1 = c.bigstate[c.cur].p;
+    a.b1 = c.bigstate[cur].p;
     a.mbig = c.mbig.p;
     a.rcebig = c.rcebig.p;
     a.rphysbig = c.rphysbig.p;
     a.p0 = c.pstate[prev].p;
-    a.p1 = c.pstate[c.cur].p;
+    a.p1 = c.pstate[cur].p;
     a.pconst = c.pconst[c.kc].p;
     a.perm = c.permp();
     a.boxes = c.boxes.p;
@@ -654,6 +665,7 @@ void launch_pair_screen(double h, int step) {
         ca.event_cap = (int)c.events.n;
         ca.status = c.status.p;
         ca.step_base = step;
+        ca.ctl = ctl;
         launch_classify(ca, c.stream);
     }
     check(cudaGetLastError(), "screen");
@@ -1063,7 +1075,7 @@ int reorder_slots(int src, double h, cudaStream_t st) {
     if (c.np < 64) return src;
     const int nblk = (c.np + PART_THREADS - 1) / PART_THREADS;
     c.order_hist.reserve((size_t)PATH_BUCKETS * nblk + PATH_BUCKETS);
-    PartitionArgs a;
+    PartitionArgs a{};
     a.np = c.np;
     a.npcap = c.npcap;
     a.nblk = nblk;
@@ -1276,7 +1288,7 @@ static size_t stage_plan(const std::vector<HostSpan>& spans, std::vector<size_t>
     return total;
 }
 
-void copy_in(const std::vector<HostSpan>& spans, cudaStream_t stream) {
+void copy_in(const std::vector<HostSpan>& spans, cudaStream_t stream, bool sync) {
     Context& c = ctx();
     std::vector<size_t> at;
     const size_t staged = stage_plan(spans, at);
@@ -1289,7 +1301,7 @@ void copy_in(const std::vector<HostSpan>& spans, cudaStream_t stream) {
         const void* src = at[k] == SIZE_MAX ? spans[k].host : c.pinned + at[k];
         check(cudaMemcpyAsync(spans[k].dev, src, spans[k].bytes, cudaMemcpyHostToDevice, stream), "upload");
     }
-    check(cudaStreamSynchronize(stream), "upload");
+    if (sync) check(cudaStreamSynchronize(stream), "upload");
 }
 
 void copy_out(const std::vector<HostSpan>& spans, cudaStream_t stream) {
@@ -1358,9 +1370,50 @@ int mercury_cuda_upload(int n, int nbig, int pn, int ngflag, const double* m, co
         inject("upload");
         if (n < 1 || nbig < 1 || nbig > n) throw std::runtime_error("invalid body counts");
         if (is_mvs(c.algorithm) && nbig > 512) throw std::runtime_error("more than 512 Big bodies");
+        // Workspace guard, as the reference's (mercury_cuda.cu:384-388): a
+        // system that needs more device memory than 80% of what is free
+        // fails here with a message instead of part-way through allocating
+        // (checked whenever the particle buffers may have to grow).
+        const size_t need = workspace_bytes(n, c.algorithm);
+        if ((size_t)9 * (size_t)std::max(2, (n - nbig + 1) & ~1) > c.pstate[0].n || injected("memory")) {
+            size_t free_b = 0, total_b = 0;
+            if (!injected("memory")) check(cudaMemGetInfo(&free_b, &total_b), "memory");
+            if ((double)need > 0.8 * (double)free_b) throw std::runtime_error("Insufficient device workspace memory");
+        }
+        c.ensure_streams();
+        cudaStream_t s = c.stream;
+        // Every host array in one round of copies into the upload stage (ngf
+        // only when a force law reads it: with ngflag 0 no kernel does, and
+        // its rows stay zero). The host's own work below runs while they fly;
+        // then the slot order and the layout on the device.
+        const size_t N = (size_t)n;
+        const bool ngf_read = ngflag != 0;
+        c.stage.reserve(9 * N + (ngf_read ? 5 * N : 0));
+        double* sx = c.stage.p;
+        double* sv = sx + 3 * N;
+        double* sm = sv + 3 * N;
+        double* sr = sm + N;
+        double* sp = sr + N;
+        double* sg = sp + N;
+        std::vector<HostSpan> spans = {{sx, const_cast<double*>(xx), 24 * N}, {sv, const_cast<double*>(vv), 24 * N},
+                                       {sm, const_cast<double*>(m), 8 * N}, {sr, const_cast<double*>(limits), 8 * N},
+                                       {sp, const_cast<double*>(radii), 8 * N}};
+        if (ngf_read) spans.push_back({sg, const_cast<double*>(ng), 40 * N});
+        copy_in(spans, s, false);
+        // the stage must not be reused while the copies may still read it
+        struct Drain {
+            cudaStream_t s;
+            bool armed = true;
+            ~Drain() {
+                if (armed) cudaStreamSynchronize(s);
+            }
+        } drain{s};
         int nmass = nbig;
-        for (int j = nbig; j < n; ++j)
-            if (m[j] != 0.0) nmass = j + 1;
+        for (int j = n - 1; j >= nbig; --j)
+            if (m[j] != 0.0) {
+                nmass = j + 1;
+                break;
+            }
         // MVS: massive Small bodies move as test particles and act on nothing
         // but the central body's oblateness reaction (mfo_mvs,
         // mercury6_2.for:5061-5068); the Big-body CTA holds them (up to 512
@@ -1373,16 +1426,6 @@ int mercury_cuda_upload(int n, int nbig, int pn, int ngflag, const double* m, co
             ns = nbig;
         }
         if (ns > 512) throw std::runtime_error("more than 512 Big and massive Small bodies");
-        // Workspace guard, as the reference's (mercury_cuda.cu:384-388): a
-        // system that needs more device memory than 80% of what is free
-        // fails here with a message instead of part-way through allocating.
-        const size_t need = workspace_bytes(n, c.algorithm);
-        if ((size_t)9 * (size_t)std::max(2, (n - ns + 1) & ~1) > c.pstate[0].n || injected("memory")) {
-            size_t free_b = 0, total_b = 0;
-            if (!injected("memory")) check(cudaMemGetInfo(&free_b, &total_b), "memory");
-            if ((double)need > 0.8 * (double)free_b) throw std::runtime_error("Insufficient device workspace memory");
-        }
-        c.ensure_streams();
         c.n = n;
         c.nbig = nbig;
         c.nmass = nmass;
@@ -1429,7 +1472,6 @@ int mercury_cuda_upload(int n, int nbig, int pn, int ngflag, const double* m, co
             c.ra_pe.reserve((size_t)21 * c.npcap);
             c.ra_max.reserve(1);
         }
-        cudaStream_t s = c.stream;
         // zero padding and cached accelerations
         check(cudaMemsetAsync(c.pstate[0].p, 0, sizeof(double) * 9 * c.npcap, s), "memset");
         check(cudaMemsetAsync(c.pstate[1].p, 0, sizeof(double) * 9 * c.npcap, s), "memset");
@@ -1438,23 +1480,6 @@ int mercury_cuda_upload(int n, int nbig, int pn, int ngflag, const double* m, co
         check(cudaMemsetAsync(c.pconst[0].p, 0, sizeof(double) * PCONST_ROWS * c.npcap, s), "memset");
         check(cudaMemsetAsync(c.pconst[1].p, 0, sizeof(double) * PCONST_ROWS * c.npcap, s), "memset");
         c.cur = 0;
-        // Every host array in one round of copies into the upload stage (ngf
-        // only when a force law reads it: with ngflag 0 no kernel does, and
-        // its rows stay zero), then the slot order and the layout on the device.
-        const size_t N = (size_t)n;
-        const bool ngf_read = ngflag != 0;
-        c.stage.reserve(9 * N + (ngf_read ? 5 * N : 0));
-        double* sx = c.stage.p;
-        double* sv = sx + 3 * N;
-        double* sm = sv + 3 * N;
-        double* sr = sm + N;
-        double* sp = sr + N;
-        double* sg = sp + N;
-        std::vector<HostSpan> spans = {{sx, const_cast<double*>(xx), 24 * N}, {sv, const_cast<double*>(vv), 24 * N},
-                                       {sm, const_cast<double*>(m), 8 * N}, {sr, const_cast<double*>(limits), 8 * N},
-                                       {sp, const_cast<double*>(radii), 8 * N}};
-        if (ngf_read) spans.push_back({sg, const_cast<double*>(ng), 40 * N});
-        copy_in(spans, s);
         order_particles(n, ns, m[0], sx, sv);
         for (int part = 0; part < 2; ++part)
             scatter_rows(part ? sv : sx, n, 3, ns, c.bigstate[0].p + 3 * part * ns, ns,
@@ -1471,6 +1496,7 @@ int mercury_cuda_upload(int n, int nbig, int pn, int ngflag, const double* m, co
             check(cudaMemsetAsync(c.ngfbig.p, 0, sizeof(double) * 5 * ns, s), "upload");
         }
         check(cudaGetLastError(), "upload");
+        drain.armed = false;
         check(cudaStreamSynchronize(s), "upload");
         c.reset = true;
         c.stepped = false;
@@ -1548,7 +1574,7 @@ int mercury_cuda_events(double time, double h, double rcen, const MercuryEvent**
                   "status");
             const int total = c.nsplit - 1 + c.np;
             if (c.stepped && total > 0) {
-                CentralArgs a;
+                CentralArgs a{};
                 a.nbig = c.nsplit;
                 a.np = c.np;
                 a.npcap = c.npcap;
@@ -2220,118 +2246,166 @@ void add_dropin_span(cudaEvent_t a, cudaEvent_t b) {
     if (cudaEventElapsedTime(&ms, a, b) == cudaSuccess) g_dropin_ms += ms;
 }
 
-// mdt_hkce's substep loop (mercury6_2.for:3884-3937) with the arithmetic of
-// the drop-in calls (mercury_cuda_step, then the pair screen of
-// mercury_cuda_events, per substep) and one host round trip per BS2 attempt:
-// the level maxima, level faults and status come back in one pinned
-// readback, and the commit, the pair screen and the next attempt are queued
-// behind the host's decision. The screens' records stay on the device,
-// tagged with their substep, until the subsystem reaches h. The states do not
-// depend on the records, so after an event or candidate overflow the buffers
-// grow and the run is redone from its starting state.
-void encounter_run_queued(double time, double h, double tol, double* hrec, int64_t* nforces_out,
+// The kernels of one attempt of the encounter subsystem with the step
+// control on the device: the BS2 levels and extrapolation at the trial step
+// in ctl, bs_decide_kernel, the commit of the accepted level into buffer
+// `out`, the pair screen between `in` and `out`, and the copy of the new
+// state back into `in`. After the subsystem reached h (ctl->stop) every
+// kernel returns at once.
+void enqueue_encounter_attempt(const BsArgs& a, int in, int out) {
+    Context& c = ctx();
+    launch_bs_sequence(a, c.stream);
+    launch_bs_decide(c.enc_ctl.p, c.bs_errs.p, c.bs_lvst.p, c.status.p, c.stream);
+    launch_bs_commit_of(a, 0, c.enc_ctl.p);
+    launch_pair_screen(0.0, 0, c.enc_ctl.p, in, out);
+    launch_bs_copyback(c.enc_ctl.p, c.bigstate[out].p, c.bigstate[in].p, c.nsplit, c.pstate[out].p, c.pstate[in].p,
+                       c.npcap, c.stream);
+    check(cudaGetLastError(), "launch");
+}
+
+// mdt_hkce's substep loop (mercury6_2.for:3884-3937) with mdt_bs2's step
+// control (3568-3596) held on the device. The host enqueues attempts in
+// blocks, as replays of a CUDA graph of GRAPH_ATTEMPTS attempts, and reads
+// the control block back once per block; the block size follows the
+// attempts the run still needs, estimated from its progress. The screens'
+// records stay on the device, tagged with their substep, until the subsystem
+// reaches h. The states do not depend on the records, so after an event,
+// candidate or substep-table overflow the buffers grow and the run is redone
+// from its starting state.
+void encounter_run_device(double time, double h, double tol, double* hrec, int64_t* nforces_out,
                           std::vector<MercuryEvent>& keep) {
     Context& c = ctx();
     if (c.algorithm != 3) throw std::runtime_error("the encounter subsystem steps by algorithm 3 (mdt_bs2)");
-    const int V = 2;
+    constexpr int GRAPH_ATTEMPTS = 8;
     mercury_cuda_reset(1);
-    const int cur0 = c.cur;
+    const int in = c.cur, out = 1 - c.cur;
     const double hrec0 = *hrec;
-    const int64_t nforces0 = c.nforces;
-    const size_t np_el = c.pstate[cur0].n, nb_el = c.bigstate[cur0].n;
+    const size_t np_el = c.pstate[in].n, nb_el = c.bigstate[in].n;
     c.snapshot.reserve(np_el + nb_el);
-    check(cudaMemcpyAsync(c.snapshot.p, c.pstate[cur0].p, sizeof(double) * np_el, cudaMemcpyDeviceToDevice, c.stream),
+    check(cudaMemcpyAsync(c.snapshot.p, c.pstate[in].p, sizeof(double) * np_el, cudaMemcpyDeviceToDevice, c.stream),
           "snapshot");
-    check(cudaMemcpyAsync(c.snapshot.p + np_el, c.bigstate[cur0].p, sizeof(double) * nb_el,
-                          cudaMemcpyDeviceToDevice, c.stream),
+    check(cudaMemcpyAsync(c.snapshot.p + np_el, c.bigstate[in].p, sizeof(double) * nb_el, cudaMemcpyDeviceToDevice,
+                          c.stream),
           "snapshot");
-    std::vector<double> tstep;   // time + tlocal at the end of each substep
+    c.enc_ctl.reserve(1);
+    c.enc_tstep.reserve(1024);
     int max_cands = 0;
-    for (int redo = 0;; ++redo) {
-        check(cudaMemsetAsync(c.status.p, 0, sizeof(DeviceStatus), c.stream), "memset");
-        tstep.clear();
-        int64_t nforces = 0;
-        double tlocal = 0.0, hlocal = std::copysign(*hrec, h);
-        bool queued = false;   // a commit + screen whose device time is not yet added
-        for (;;) {
-            const double tmp0 = std::fabs(h) - std::fabs(tlocal);
-            *hrec = hlocal;
-            if (std::fabs(hlocal) > tmp0) hlocal = std::copysign(tmp0, h);
-            int64_t forces = 1;  // the start-of-step force
-            int accepted = 0;
-            BsArgs a{};
-            for (;;) {
-                if (tlocal + hlocal == tlocal)
-                    throw std::runtime_error("BS cannot advance time at the requested tolerance");
-                check(cudaEventRecord(c.d0, c.stream), "event");
-                a = launch_bs_attempt(hlocal);
-                check(cudaMemcpyAsync(c.bs_rb->errs, c.bs_errs.p, sizeof(c.bs_rb->errs), cudaMemcpyDeviceToHost,
-                                      c.stream),
-                      "status");
-                check(cudaMemcpyAsync(c.bs_rb->lv, c.bs_lvst.p, sizeof(c.bs_rb->lv), cudaMemcpyDeviceToHost, c.stream),
-                      "status");
-                check(cudaMemcpyAsync(&c.bs_rb->st, c.status.p, sizeof(DeviceStatus), cudaMemcpyDeviceToHost, c.stream),
-                      "status");
-                check(cudaEventRecord(c.d1, c.stream), "event");
-                check(cudaEventSynchronize(c.d1), "step");
-                add_dropin_span(c.d0, c.d1);
-                if (queued) add_dropin_span(c.q0, c.q1);
-                queued = false;
-                // the candidates of the last queued screen (cleared before the next)
-                max_cands = std::max(max_cands, c.bs_rb->st.cands);
-                accepted = bs_accept_level(c.bs_rb->errs, c.bs_rb->lv, V, tol, &forces);
-                if (accepted) break;
-                hlocal = hlocal * 0.5;
-            }
-            check(cudaEventRecord(c.q0, c.stream), "event");
-            launch_bs_commit_of(a, accepted);
-            const double hdid = hlocal;
-            bs_next_trial(V, accepted, &hlocal);
-            nforces += forces;
-            c.nforces += forces;
-            c.cur = 1 - c.cur;
-            c.stepped = true;
-            tlocal = tlocal + hdid;
-            tstep.push_back(time + tlocal);
-            check(cudaMemsetAsync(&c.status.p->cands, 0, sizeof(int), c.stream), "memset");
-            launch_pair_screen(hdid, (int)tstep.size() - 1);
-            check(cudaEventRecord(c.q1, c.stream), "event");
-            queued = true;
-            if (!((tlocal - h) * h < 0.0)) break;
+    struct Graph {
+        cudaGraph_t g = nullptr;
+        cudaGraphExec_t e = nullptr;
+        ~Graph() {
+            if (e) cudaGraphExecDestroy(e);
+            if (g) cudaGraphDestroy(g);
         }
+    };
+    for (int redo = 0;; ++redo) {
+        // the first substep's trial step: hrec, clipped to the subsystem's end
+        EncCtl k{};
+        double hlocal = std::copysign(*hrec, h);
+        k.hrec = hlocal;
+        if (std::fabs(hlocal) > std::fabs(h)) hlocal = std::copysign(std::fabs(h), h);
+        if (0.0 + hlocal == 0.0) throw std::runtime_error("BS cannot advance time at the requested tolerance");
+        k.h0 = hlocal;
+        k.h = h;
+        k.tol = tol;
+        k.time = time;
+        k.forces = 1;   // the first substep's start-of-step force
+        k.step_cap = (int)c.enc_tstep.n;
+        k.tstep = c.enc_tstep.p;
+        *c.enc_host = k;
+        const BsArgs a = [&] {
+            BsArgs r = bs_attempt_args(0.0);
+            r.ctl = c.enc_ctl.p;
+            return r;
+        }();
+        c.boxes.reserve((size_t)4 * std::max(1, c.nbig - 1));
+        c.detail.reserve((size_t)std::max(1, c.nbig - 1) * TAB_DETAIL);
+        check(cudaMemcpyAsync(c.enc_ctl.p, c.enc_host, sizeof(EncCtl), cudaMemcpyHostToDevice, c.stream), "upload");
+        check(cudaMemsetAsync(c.status.p, 0, sizeof(DeviceStatus), c.stream), "memset");
+        check(cudaMemsetAsync(c.bs_errs.p, 0, sizeof(unsigned long long) * 13, c.stream), "memset");
+        check(cudaMemsetAsync(c.bs_lvst.p, 0, sizeof(DeviceStatus) * 13, c.stream), "memset");
+        // one attempt eagerly (kernel attributes set), then the graph
+        check(cudaEventRecord(c.d0, c.stream), "event");
+        enqueue_encounter_attempt(a, in, out);
+        Graph graph;
+        check(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeRelaxed), "graph");
+        for (int q = 0; q < GRAPH_ATTEMPTS; ++q) enqueue_encounter_attempt(a, in, out);
+        check(cudaStreamEndCapture(c.stream, &graph.g), "graph");
+        check(cudaGraphInstantiate(&graph.e, graph.g, 0), "graph");
+        const int per_attempt = 2 + (c.np > 0 ? 1 : 0) + 1 + 1 + 1 + (c.np > 0 && c.nbig > 1 ? 3 : 0) + 1;
+        c.dropin_launches += per_attempt;
+        int blocks = 2;   // graph replays in the first block
+        for (;;) {
+            for (int b = 0; b < blocks; ++b) check(cudaGraphLaunch(graph.e, c.stream), "graph");
+            c.dropin_launches += (int64_t)blocks * GRAPH_ATTEMPTS * per_attempt;
+            check(cudaMemcpyAsync(c.enc_host, c.enc_ctl.p, sizeof(EncCtl), cudaMemcpyDeviceToHost, c.stream),
+                  "status");
+            check(cudaEventRecord(c.d1, c.stream), "event");
+            check(cudaEventSynchronize(c.d1), "step");
+            add_dropin_span(c.d0, c.d1);
+            const EncCtl& now = *c.enc_host;
+            if (now.stop) break;
+            // the attempts still needed at the rate so far, and a little more
+            const double done = std::fabs(now.tlocal) / std::fabs(h);
+            const double rate = now.attempts / std::max(done, 1e-3);
+            const double need = rate * (1.0 - done) * 1.1 + 1.0;
+            blocks = (int)std::min(64.0, std::max(1.0, std::ceil(need / GRAPH_ATTEMPTS)));
+            check(cudaEventRecord(c.d0, c.stream), "event");
+        }
+        const EncCtl done = *c.enc_host;
+        if (done.error == ENC_ERR_FORCE) throw std::runtime_error("BS force failed");
+        if (done.error == ENC_ERR_NONFINITE) throw std::runtime_error("Nonfinite BS2 force or extrapolation");
+        if (done.error == ENC_ERR_ADVANCE)
+            throw std::runtime_error("BS cannot advance time at the requested tolerance");
         read_status();
-        if (queued) add_dropin_span(c.q0, c.q1);
-        max_cands = std::max(max_cands, c.status_host->cands);
-        if (!c.status_host->overflow) {
+        max_cands = std::max(max_cands, std::max(done.max_cands, c.status_host->cands));
+        const bool steps_full = done.error == ENC_ERR_STEPS;
+        if (!steps_full && !c.status_host->overflow) {
             const int nev = c.status_host->events;
             std::vector<MercuryEvent> ev(nev);
             std::vector<int> steps(nev);
+            std::vector<double> tstep(done.substeps);
+            if (done.substeps)
+                check(cudaMemcpyAsync(tstep.data(), c.enc_tstep.p, sizeof(double) * done.substeps,
+                                      cudaMemcpyDeviceToHost, c.stream),
+                      "events");
             if (nev) {
-                check(cudaMemcpy(ev.data(), c.events.p, sizeof(MercuryEvent) * nev, cudaMemcpyDeviceToHost), "events");
-                check(cudaMemcpy(steps.data(), c.event_step.p, sizeof(int) * nev, cudaMemcpyDeviceToHost), "events");
+                check(cudaMemcpyAsync(ev.data(), c.events.p, sizeof(MercuryEvent) * nev, cudaMemcpyDeviceToHost,
+                                      c.stream),
+                      "events");
+                check(cudaMemcpyAsync(steps.data(), c.event_step.p, sizeof(int) * nev, cudaMemcpyDeviceToHost,
+                                      c.stream),
+                      "events");
             }
+            check(cudaStreamSynchronize(c.stream), "events");
             // the drop-in events call adds the substep's end time to each record
-            for (int k = 0; k < nev; ++k) ev[k].time = ev[k].time + tstep[steps[k]];
+            for (int r = 0; r < nev; ++r) ev[r].time = ev[r].time + tstep[steps[r]];
             std::vector<uint32_t> order;
             order_events(ev, &steps, order);
             keep.resize(nev);
-            for (int k = 0; k < nev; ++k) keep[k] = ev[order[k]];
+            for (int r = 0; r < nev; ++r) keep[r] = ev[order[r]];
+            *hrec = done.hrec;
+            c.nforces += done.forces;
+            *nforces_out = done.forces;
+            c.stepped = true;
             c.pair_events = 0;
-            *nforces_out = nforces;
             return;
         }
         if (redo > 8) throw std::runtime_error("event buffer growth failed");
-        grow_after_overflow();
-        if (c.status_host->overflow & 2) c.cands.reserve((size_t)max_cands + max_cands / 4 + 4096);
-        check(cudaMemcpyAsync(c.pstate[cur0].p, c.snapshot.p, sizeof(double) * np_el, cudaMemcpyDeviceToDevice,
+        if (steps_full) {
+            c.enc_tstep.reserve(2 * c.enc_tstep.n);
+        }
+        if (c.status_host->overflow) {
+            grow_after_overflow();
+            if (c.status_host->overflow & 2) c.cands.reserve((size_t)max_cands + max_cands / 4 + 4096);
+        }
+        check(cudaMemcpyAsync(c.pstate[in].p, c.snapshot.p, sizeof(double) * np_el, cudaMemcpyDeviceToDevice,
                               c.stream),
               "restore");
-        check(cudaMemcpyAsync(c.bigstate[cur0].p, c.snapshot.p + np_el, sizeof(double) * nb_el,
+        check(cudaMemcpyAsync(c.bigstate[in].p, c.snapshot.p + np_el, sizeof(double) * nb_el,
                               cudaMemcpyDeviceToDevice, c.stream),
               "restore");
-        c.cur = cur0;
         *hrec = hrec0;
-        c.nforces = nforces0;
     }
 }
 
@@ -2344,7 +2418,7 @@ int mercury_b200_encounter_run(double time, double h, double tol, double rcen, d
         std::vector<MercuryEvent> keep;
         int64_t nforces = 0;
         if (!ctx().tangent) {
-            encounter_run_queued(time, h, tol, hrec, &nforces, keep);
+            encounter_run_device(time, h, tol, hrec, &nforces, keep);
         } else {
             // the members' tangents are kept: the drop-in calls one by one
             int dtflag = 1;

@@ -240,6 +240,11 @@ __device__ void massive_call(const BsArgs& A, const double* X, const double* V, 
 // others a private row.
 template <int VARIANT> __global__ void __launch_bounds__(256) bs_massive_level_kernel(BsArgs A) {
     extern __shared__ double sm[];
+    double h0 = A.h0;
+    if (A.ctl) {
+        if (A.ctl->stop) return;
+        h0 = A.ctl->h0;
+    }
     const int N = A.f.nsplit, tid = threadIdx.x, nt = blockDim.x, n = blockIdx.x + 1;
     const int stride = force_row(A.f.nbig - 1);
     double* X = sm;
@@ -273,8 +278,8 @@ template <int VARIANT> __global__ void __launch_bounds__(256) bs_massive_level_k
     int row = 1;
     for (int m = 1; m < n; ++m) row += bs_level_forces(VARIANT, m);
     DeviceStatus* st = &A.lvst[n];
-    const double h = level_h<VARIANT>(A.h0, n);
-    const double h2n = level_h2<VARIANT>(A.h0, n);
+    const double h = level_h<VARIANT>(h0, n);
+    const double h2n = level_h2<VARIANT>(h0, n);
     double* Dn = A.draw + (size_t)(n - 1) * 6 * N;
     if (VARIANT == 1) {
         const double hx2 = h * 2.0;
@@ -356,7 +361,12 @@ template <int VARIANT> __global__ void __launch_bounds__(256) bs_massive_extrap_
     __shared__ double co[L * (L - 1) / 2][2];
     __shared__ double wmax[8];
     __shared__ int wbad[8];
-    neville_coefficients<VARIANT>(A.h0, co);
+    double h0 = A.h0;
+    if (A.ctl) {
+        if (A.ctl->stop) return;
+        h0 = A.ctl->h0;
+    }
+    neville_coefficients<VARIANT>(h0, co);
     __syncthreads();
     const int nb1 = N - 1, M = 6 * nb1;
     for (int n = 1; n <= L; ++n) {
@@ -427,7 +437,12 @@ template <int VARIANT> __global__ void __launch_bounds__(bs_levels(VARIANT) * 16
     __shared__ double a0sm[3][32];
     __shared__ double co[L * (L - 1) / 2][2];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    neville_coefficients<VARIANT>(A.h0, co);
+    double h0 = A.h0;
+    if (A.ctl) {
+        if (A.ctl->stop) return;
+        h0 = A.ctl->h0;
+    }
+    neville_coefficients<VARIANT>(h0, co);
     const int p = blockIdx.x * 32 + lane;
     const bool ok = p < A.np && A.perm[p] < A.active_np;
     const int nb = A.f.nbig - 1, stride = force_row(nb), S = A.npcap;
@@ -464,8 +479,8 @@ template <int VARIANT> __global__ void __launch_bounds__(bs_levels(VARIANT) * 16
         int row = 1;
         for (int m = 1; m < n; ++m) row += bs_level_forces(VARIANT, m);
         DeviceStatus* st = &A.lvst[n];
-        const double h = level_h<VARIANT>(A.h0, n);
-        const double h2n = level_h2<VARIANT>(A.h0, n);
+        const double h = level_h<VARIANT>(h0, n);
+        const double h2n = level_h2<VARIANT>(h0, n);
         auto call = [&](const double3 x, const double3 v) {
             const double* Tr = A.table + (size_t)(row++) * stride;
             return force(x, v, Tr, st);
@@ -651,12 +666,17 @@ __global__ void __launch_bounds__(64) bs2_tangent_kernel(BsArgs A, int levels, d
 __global__ void __launch_bounds__(128) bs_commit_kernel(BsCommitArgs A) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     const int N = A.nsplit, S = A.npcap;
+    int level_cand = A.cand;
+    if (A.ctl) {
+        if (!A.ctl->accepted) return;
+        level_cand = A.ctl->accepted - 4;
+    }
     if (q < N) {
         if (q == 0) {
             for (int c = 0; c < 9; ++c) A.bx_out[c * N] = A.bx[c * N];
             return;
         }
-        const double* cand = A.bcand + (size_t)A.cand * 6 * N;
+        const double* cand = A.bcand + (size_t)level_cand * 6 * N;
         for (int c = 0; c < 6; ++c) A.bx_out[c * N + q] = cand[c * N + q];
         for (int c = 6; c < 9; ++c) A.bx_out[c * N + q] = 0.0;
         return;
@@ -667,9 +687,104 @@ __global__ void __launch_bounds__(128) bs_commit_kernel(BsCommitArgs A) {
         for (int c = 0; c < 9; ++c) A.px_out[(size_t)c * S + p] = A.px[(size_t)c * S + p];
         return;
     }
-    const double* cand = A.pcand + (size_t)A.cand * 6 * S;
+    const double* cand = A.pcand + (size_t)level_cand * 6 * S;
     for (int c = 0; c < 6; ++c) A.px_out[(size_t)c * S + p] = cand[(size_t)c * S + p];
     for (int c = 6; c < 9; ++c) A.px_out[(size_t)c * S + p] = 0.0;
+}
+
+// mdt_bs2's decision after one attempt of the encounter subsystem
+// (mercury6_2.for:3568-3596; the same as bs_accept_level and the host loop
+// of mdt_hkce, 3884-3937): the first level n > 3 whose error maximum is <=
+// tol^2 is accepted, else the step is halved; after an acceptance the next
+// trial step (x0.55 for a level >= 8, x1.3 below 7), the local clock, and the
+// clipping of the next substep to the subsystem's end. One thread.
+__global__ void bs_decide_kernel(EncCtl* c, unsigned long long* errs, DeviceStatus* lv, DeviceStatus* status) {
+    if (c->stop) {
+        c->accepted = 0;
+        return;
+    }
+    constexpr int L = 12;
+    const int fails = FAULT_NGF | FAULT_COINCIDENT;
+    c->attempts += 1;
+    int accepted = 0, error = 0;
+    long long forces = 0;
+    if (lv[0].fault & fails) error = ENC_ERR_FORCE;
+    for (int n = 1; n <= L && !error && !accepted; ++n) {
+        forces += n;
+        if (lv[n].fault & fails) {
+            error = ENC_ERR_FORCE;
+            break;
+        }
+        if (n <= 3) continue;
+        const double e = __longlong_as_double((long long)errs[n]);
+        if (!isfinite(e)) {
+            error = ENC_ERR_NONFINITE;
+            break;
+        }
+        if (e <= c->tol * c->tol) accepted = n;
+    }
+    for (int n = 0; n < 13; ++n) {
+        errs[n] = 0ull;
+        lv[n].fault = 0;
+    }
+    c->forces += forces;
+    if (error) {
+        c->error = error;
+        c->stop = 1;
+        c->accepted = 0;
+        return;
+    }
+    if (!accepted) {
+        c->accepted = 0;
+        c->h0 = c->h0 * 0.5;
+        if (c->tlocal + c->h0 == c->tlocal) {
+            c->error = ENC_ERR_ADVANCE;
+            c->stop = 1;
+        }
+        return;
+    }
+    c->accepted = accepted;
+    const double hdid = c->h0;
+    double hnext = c->h0;
+    if (accepted >= 8) hnext = hnext * 0.55;
+    if (accepted < 7) hnext = hnext * 1.3;
+    c->hdid = hdid;
+    c->tlocal = c->tlocal + hdid;
+    if (c->substeps >= c->step_cap) {
+        c->error = ENC_ERR_STEPS;
+        c->stop = 1;
+        c->accepted = 0;
+        return;
+    }
+    c->tstep[c->substeps] = c->time + c->tlocal;
+    c->substeps += 1;
+    // the previous substep's screen candidates, cleared for this one's
+    c->max_cands = max(c->max_cands, status->cands);
+    status->cands = 0;
+    if (!((c->tlocal - c->h) * c->h < 0.0)) {
+        c->stop = 1;
+        return;
+    }
+    // the next substep: hrec before the clip to the subsystem's end
+    const double tmp0 = fabs(c->h) - fabs(c->tlocal);
+    c->hrec = hnext;
+    if (fabs(hnext) > tmp0) hnext = copysign(tmp0, c->h);
+    c->h0 = hnext;
+    c->forces += 1;   // the next substep's start-of-step force
+    if (c->tlocal + c->h0 == c->tlocal) {
+        c->error = ENC_ERR_ADVANCE;
+        c->stop = 1;
+    }
+}
+
+__global__ void __launch_bounds__(256) bs_copyback_kernel(const EncCtl* c, const double* bsrc, double* bdst,
+                                                          int nsplit, const double* psrc, double* pdst, int npcap) {
+    if (!c->accepted) return;
+    const size_t nb = (size_t)9 * nsplit, np = (size_t)9 * npcap;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < nb + np; q += (size_t)gridDim.x * blockDim.x) {
+        if (q < nb) bdst[q] = bsrc[q];
+        else pdst[q - nb] = psrc[q - nb];
+    }
 }
 
 template <int VARIANT> void launch_variant(const BsArgs& a, cudaStream_t s) {
@@ -699,6 +814,18 @@ void launch_bs2_tangent(const BsArgs& a, int levels, double* tg, cudaStream_t s)
     const size_t smem = sizeof(double) * 6 * bs_levels(2) * threads;
     const long long total = 6LL * a.np;
     bs2_tangent_kernel<<<(unsigned)((total + threads - 1) / threads), threads, smem, s>>>(a, levels, tg);
+}
+
+void launch_bs_decide(EncCtl* ctl, unsigned long long* errs, DeviceStatus* lv, DeviceStatus* status,
+                      cudaStream_t s) {
+    bs_decide_kernel<<<1, 1, 0, s>>>(ctl, errs, lv, status);
+}
+
+void launch_bs_copyback(const EncCtl* ctl, const double* bsrc, double* bdst, int nsplit, const double* psrc,
+                        double* pdst, int npcap, cudaStream_t s) {
+    const size_t total = (size_t)9 * (nsplit + npcap);
+    const int blocks = (int)std::min<size_t>(148 * 4, (total + 255) / 256);
+    bs_copyback_kernel<<<blocks, 256, 0, s>>>(ctl, bsrc, bdst, nsplit, psrc, pdst, npcap);
 }
 
 void launch_bs_commit(const BsCommitArgs& a, cudaStream_t s) {

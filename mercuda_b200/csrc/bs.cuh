@@ -66,6 +66,7 @@ struct BsArgs {
     const int2* adj;
     const int* perm;             // slot -> particle index
     int active_np;               // particles with index >= active_np sit the step out (epoch synchronisation)
+    const EncCtl* ctl = nullptr; // non-null: the trial step is ctl->h0, nothing runs once ctl->stop
 };
 
 struct BsCommitArgs {
@@ -79,7 +80,19 @@ struct BsCommitArgs {
     const double* px;            // start-of-step particle state (kept by inactive particles)
     const int* perm;             // slot -> particle index
     int active_np;               // as in BsArgs
+    const EncCtl* ctl = nullptr; // non-null: commit level ctl->accepted, nothing when it is 0
 };
+
+// One decision of the encounter subsystem's device-held step control after
+// an attempt of launch_bs_sequence (errs and lv its level maxima and faults,
+// cleared here for the next attempt; the pair screen's candidate counter
+// cleared after an acceptance). One thread.
+void launch_bs_decide(EncCtl* ctl, unsigned long long* errs, DeviceStatus* lv, DeviceStatus* status,
+                      cudaStream_t s);
+// After an accepted attempt: the committed state (bx_out/px_out of the
+// commit) copied back over the start-of-step buffers it came from.
+void launch_bs_copyback(const EncCtl* ctl, const double* bsrc, double* bdst, int nsplit, const double* psrc,
+                        double* pdst, int npcap, cudaStream_t s);
 
 void launch_bs_sequence(const BsArgs& a, cudaStream_t s);
 void launch_bs_commit(const BsCommitArgs& a, cudaStream_t s);

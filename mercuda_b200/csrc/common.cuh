@@ -53,4 +53,30 @@ struct EncounterCandidate {
 
 __device__ __forceinline__ void raise_fault(DeviceStatus* st, int bit) { atomicOr(&st->fault, bit); }
 
+// Step control of the HYBRID encounter subsystem held on the device
+// (mdt_hkce's substep loop, mercury6_2.for:3884-3937, with mdt_bs2's level
+// choice, 3568-3596): the BS2 attempt kernels read the trial step h0 here,
+// bs_decide_kernel takes each attempt's decision and advances the local
+// clock, and the commit, copy-back and pair screen act only after an
+// accepted attempt. The host reads it back every few dozen attempts.
+struct EncCtl {
+    double h0;          // trial step of the next attempt
+    double hdid;        // step of the last accepted substep
+    double tlocal;      // the subsystem's local clock
+    double hrec;        // the step before it was clipped to the subsystem's end
+    double h;           // the HYBRID step the subsystem runs to
+    double tol;
+    double time;        // start of the HYBRID step (records' times are time + tlocal)
+    long long forces;   // force calls, counted as mdt_bs2 counts them
+    int accepted;       // level accepted by the last decision (0: rejected or none)
+    int stop;           // 1 once the local clock reached h, or after an error
+    int error;          // 0 or an ENC_ERR_* code
+    int substeps;       // accepted substeps
+    int attempts;
+    int step_cap;       // entries of tstep
+    int max_cands;      // most screen candidates of one substep
+    double* tstep;      // [step_cap] end time (time + tlocal) of each accepted substep
+};
+constexpr int ENC_ERR_FORCE = 1, ENC_ERR_NONFINITE = 2, ENC_ERR_ADVANCE = 3, ENC_ERR_STEPS = 4;
+
 }  // namespace mb200

@@ -159,16 +159,13 @@ struct Context {
     // timing events of the drop-in calls, and the kernels they launched
     cudaEvent_t d0 = nullptr, d1 = nullptr;
     int64_t dropin_launches = 0;
-    // the encounter subsystem's queued substeps: one pinned readback per BS2
-    // attempt (level maxima, level faults, status) and timing events around
-    // each queued commit + pair screen
-    struct BsReadback {
-        unsigned long long errs[13];
-        DeviceStatus lv[13];
-        DeviceStatus st;
-    };
-    BsReadback* bs_rb = nullptr;
-    cudaEvent_t q0 = nullptr, q1 = nullptr;
+    // the encounter subsystem's step control, read back once per block of
+    // attempts
+    EncCtl* enc_host = nullptr;
+    // the encounter subsystem's step control on the device and the end time
+    // of each accepted substep
+    DBuf<EncCtl> enc_ctl;
+    DBuf<double> enc_tstep;
     // the first records of a drop-in events call, read back with its status
     static constexpr int EVENT_HEAD = 1024;
     MercuryEvent* ev_head = nullptr;
@@ -200,9 +197,7 @@ struct Context {
             check(cudaEventCreate(&d0), "event");
             check(cudaEventCreate(&d1), "event");
             check(cudaMallocHost(reinterpret_cast<void**>(&status_host), sizeof(DeviceStatus)), "pinned");
-            check(cudaEventCreate(&q0), "event");
-            check(cudaEventCreate(&q1), "event");
-            check(cudaMallocHost(reinterpret_cast<void**>(&bs_rb), sizeof(BsReadback)), "pinned");
+            check(cudaMallocHost(reinterpret_cast<void**>(&enc_host), sizeof(EncCtl)), "pinned");
             check(cudaMallocHost(reinterpret_cast<void**>(&ev_head), sizeof(MercuryEvent) * EVENT_HEAD), "pinned");
         }
     }
@@ -222,6 +217,8 @@ struct Context {
         ra_max.release();
         bs_errs.release();
         bs_lvst.release();
+        enc_ctl.release();
+        enc_tstep.release();
         hy_pairs.release();
         hy_ids.release();
         adj_off.release();
@@ -265,10 +262,12 @@ struct HostSpan {
 // True for page-locked host memory (cudaMallocHost, cudaHostAlloc, cudaHostRegister).
 bool host_pinned(const void* p);
 // Copy every span host -> device (copy_in) or device -> host (copy_out) on
-// `stream`, returning when the data has landed. Page-locked host arrays are
+// `stream`, returning when the data has landed (copy_in with sync false
+// returns once the copies are queued; the host arrays and the stage must
+// then stay untouched until the stream passes them). Page-locked host arrays are
 // copied directly by DMA; pageable ones go through the context's page-locked
 // area, which the host's cores fill or empty in parallel.
-void copy_in(const std::vector<HostSpan>& spans, cudaStream_t stream);
+void copy_in(const std::vector<HostSpan>& spans, cudaStream_t stream, bool sync = true);
 void copy_out(const std::vector<HostSpan>& spans, cudaStream_t stream);
 
 }  // namespace mb200

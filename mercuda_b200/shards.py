@@ -113,25 +113,24 @@ class ShardedRun:
         self.n = 0
         self.local_events = 0
 
-    def upload(self, shard: System, ids: np.ndarray, n_total: int) -> None:
+    def upload(self, shard: System, ids: np.ndarray, n_total: int, ngflag: int | None = None) -> None:
         """This rank's shard and the global 0-based index of each of its bodies
-        (Big bodies first, the same on every rank); n_total bodies in all."""
+        (Big bodies first, the same on every rank); n_total bodies in all.
+        ngflag: the input's force-law flag (None: derived from shard.ngf)."""
         ids = np.asarray(ids, dtype=np.int64)
         if len(ids) != shard.n or np.any(ids[:shard.nbig] != np.arange(shard.nbig)):
             raise ValueError("a shard holds every Big body first, then its particles")
         self.ids = ids
-        self.identity = bool(np.array_equal(ids, np.arange(len(ids))))
         self.nbig = shard.nbig
         self.n = int(n_total)
         # every rank must agree on the Big bodies and the total
         seen = self.ranks.gather((self.nbig, self.n), everywhere=True)
         if any(s != seen[0] for s in seen):
             raise ValueError("ranks disagree on the Big bodies or the body count")
-        self.backend.upload(shard)
+        self.backend.upload(shard, ngflag)
 
     def _to_global(self, events: np.ndarray) -> np.ndarray:
-        if self.identity:
-            return events
+        # through the id map (a few records per step; no test of the map itself)
         ev = events.copy()
         for f in ("i", "j"):
             ev[f] = self.ids[ev[f] - 1] + 1

@@ -65,6 +65,8 @@ class System:
         """Derived as in mio_in (mercury6_2.for:6360-6371): 1 = A1..A3/yar, 2 = beta, 3 = both."""
         g = self.ngf
         flag = 0
+        if not g.reshape(-1).any():   # one contiguous pass: the usual all-zero case
+            return flag
         if np.any(g[:, [0, 1, 2, 4]] != 0):
             flag |= 1
         if np.any(g[:, 3] != 0):

@@ -190,6 +190,13 @@ def main_paths(out):
         data[f"{name}/h"] = np.array(hnext)
         print(name, len(ev), "events")
 
+    # The oblateness of the reference's test (J2 = 0.1, J4 = -1e-3 with
+    # rcen = 0.005 AU, tests/test_gpu_algorithms.py:79-87) as its Fortran host
+    # passes it to the backend: mio_in scales J_2n by rcen^2n
+    # (mercury6_2.for:6171-6173).
+    rcen = 0.005
+    jcen_test = [0.1 * rcen ** 2, -1e-3 * rcen ** 4, 0.0]
+
     # HYBRID (reference tests/test_gpu_algorithms.py:34-41, 166-177): semi-active
     # and massless Small bodies both ways, a close Big pair that forces the BS2
     # subsystem, no Big bodies, the oblateness reaction, and particles near planets
@@ -210,14 +217,14 @@ def main_paths(out):
                    v=np.array([b[2] for b in bodies]).reshape(-1, 3), nbig=1)
         return mce_init(s, 0.5, 3.0)
 
-    def oblate(massive):
+    def oblate(massive, jcen):
         bodies = [(K2, [0.0] * 3, [0.0] * 3), planar_body(1e-3, 0.3, 0.02, 0.0), planar_body(1e-3, 5.2, 0.04, 0.0)]
         bodies += [planar_body(1e-8 if massive and j % 3 == 0 else 0.0, 1.6 + j * 0.012, 0.12, j * 0.37)
                    for j in range(33)]
         n = len(bodies)
         s = System(m=np.array([b[0] for b in bodies]), x=np.array([b[1] for b in bodies]),
                    v=np.array([b[2] for b in bodies]), nbig=3, rce=np.full(n, 0.05), rphys=np.full(n, 1e-4))
-        s.jcen[:] = [0.1, -1e-3, 0.0]
+        s.jcen[:] = jcen
         return s
 
     hybrid = [
@@ -226,9 +233,9 @@ def main_paths(out):
         ("hy_semi_m1_dm", mce_init(hvar_system(massive=True, pn=0), 0.5, 3.0), -0.5, 60),
         ("hy_semi_m1_dp", mce_init(hvar_system(massive=True, pn=0), 0.5, 3.0), 0.5, 60),
         ("hy_close_pair", close_pair(), 0.5, 16),
-        ("hy_close_pair_oblate", close_pair(jcen=[0.1, -1e-3, 0.0]), 0.5, 16),
+        ("hy_close_pair_oblate", close_pair(jcen=jcen_test), 0.5, 16),
         ("hy_no_big_257", no_big(257), 0.5, 32),
-        ("hy_oblate_m1", mce_init(oblate(True), 0.5, 3.0), 0.5, 128),
+        ("hy_oblate_m1", mce_init(oblate(True, jcen_test), 0.5, 3.0), 0.5, 128),
         ("hy_particles", make_system(seed=3, n_particles=1500, nplanets=8, near_fraction=0.05, h=8.0), 8.0, 10),
     ]
     for name, s, h, nsteps in hybrid:
@@ -269,8 +276,11 @@ def main_paths(out):
         return s
 
     mvs = [
-        ("mvs_oblate", oblate(False), 0.5, 128, 1),
-        ("mvs_oblate_massive", oblate(True), 0.5, 128, 1),
+        ("mvs_oblate", oblate(False, jcen_test), 0.5, 128, 1),
+        ("mvs_oblate_massive", oblate(True, jcen_test), 0.5, 128, 1),
+        # J2 r^-2 = 1.1 at the inner planet's orbit: the reaction as large as
+        # the Kepler term
+        ("mvs_oblate_strong", oblate(True, [0.1, -1e-3, 0.0]), 0.5, 128, 1),
         ("mvs_massive", hvar_system(massive=True, pn=0), 0.5, 64, 1),
         ("mvs_back", hvar_system(massive=False, pn=0), -0.5, 256, 1),
         ("mvs_ngf", with_ngf(hvar_system(massive=False, pn=0)), 0.5, 256, 1),

@@ -236,8 +236,8 @@ def test_c4_adjoint_64_of_100k(cuda_lib, oracle):
     """Config 4: dL/d(x0, v0, yar) of L = sum |x_final|^2 for 100,000 particles,
     1,000 steps of 8 d, checkpoint every 50; 64 random particles against the
     oracle's FP64 tangent map (variational equations of the same statements)
-    at 1e-6 and against central differences of the oracle (relative step
-    1e-7) at 1e-3 (the difference quotient's own error)."""
+    at 1e-6 and against central differences of the oracle at 1e-3 (the
+    difference quotient's own error)."""
     import torch
     from mercuda_b200.adjoint import mvs_trajectory
 
@@ -268,11 +268,14 @@ def test_c4_adjoint_64_of_100k(cuda_lib, oracle):
         err = np.max(np.abs(g[:, cols] - want[:, cols]) / scale)
         assert err < 1e-6, (cols, err)
     # central differences: every particle's parameter k perturbed at once
-    # (massless particles are independent), relative step 1e-7
+    # (massless particles are independent), relative step 1e-7 for x and v.
+    # yar (1e-15..1e-13) moves a particle by ~1e-7 AU over 1,000 steps, so a
+    # relative step of 1e-7 is lost in the trajectory's rounding; the state is
+    # linear in yar far beyond its own size, so its step is 10 |yar|.
     params = np.concatenate([sub.x[nb:], sub.v[nb:], sub.ngf[nb:, 4:5]], axis=1)
     fd = np.zeros_like(want)
     for k in range(7):
-        eps = 1e-7 * np.maximum(np.abs(params[:, k]), 1e-300)
+        eps = (10.0 if k == 6 else 1e-7) * np.maximum(np.abs(params[:, k]), 1e-300)
         loss = []
         for sign in (1.0, -1.0):
             t = sub.copy()

@@ -37,7 +37,7 @@ class OracleBackend:
         self.oracle = oracle
         self.s = None
 
-    def upload(self, s):
+    def upload(self, s, ngflag=None):
         self.s = s.copy()
 
     def mvs_advance(self, time, h, nsteps, rcen, steps_per_launch=0):
