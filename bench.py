@@ -71,7 +71,11 @@ BYTES_PER_PARTICLE_STEP = 96.0
 # launch of the particle kernel on this 1M-particle workload, by steps per
 # launch, from ncu captures of this bench's own command (the launch list and
 # traffic summary of the particle kernel are kept beside the sources).
-TRAFFIC_MB_PER_LAUNCH = {31: (99.764224, 157.014528)}
+TRAFFIC_MB_PER_LAUNCH = {31: (99.764224, 157.014528), 20: (99.714304, 127.000576)}
+# The FP64 pipe of the same captures: sm__pipe_fp64_cycles_active (fraction
+# of peak sustained), sm__inst_executed_pipe_fp64 per particle-step (warp
+# instructions x 32), smsp__issue_active (fraction), by steps per launch.
+FP64_PIPE_BY_K = {20: (0.4949, 730.4, 0.5463)}
 CLOCK_QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
                "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -1196,7 +1200,12 @@ def main():
                          "traffic_unit": f"bytes per launch (ncu, {steps_per_launch} steps, scaled from 1M particles)",
                          "peak_source": "measured in this run: fma() chains on every SM (2 FLOP/FMA)",
                          "flops_per_particle_step": FLOPS_PER_PARTICLE_STEP,
-                         "kernel_ms_per_launch": kernel_ms},
+                         "kernel_ms_per_launch": kernel_ms,
+                         "fp64_pipe": ({"frac": FP64_PIPE_BY_K[steps_per_launch][0],
+                                        "inst_per_particle_step": FP64_PIPE_BY_K[steps_per_launch][1],
+                                        "issue_active": FP64_PIPE_BY_K[steps_per_launch][2],
+                                        "source": f"ncu, one {steps_per_launch}-step launch of this workload"}
+                                       if steps_per_launch in FP64_PIPE_BY_K else None)},
             "clocks": clk,
             "gpu_launches": tm["kernel_launches"],
             "events": int(len(events)),

@@ -546,11 +546,10 @@ int bs_accept_level(const unsigned long long* errs, const DeviceStatus* lv, int 
 
 // Copies level `accepted` of attempt a into the other state buffer (and
 // pushes the encounter members' tangents through it when they are kept).
-void launch_bs_commit_of(const BsArgs& a, int accepted, const EncCtl* ctl = nullptr) {
+void launch_bs_commit_of(const BsArgs& a, int accepted) {
     Context& c = ctx();
     const int in = c.cur, out = 1 - c.cur;
     BsCommitArgs k{};
-    k.ctl = ctl;
     k.nsplit = c.nsplit;
     k.np = c.np;
     k.npcap = c.npcap;
@@ -618,15 +617,13 @@ void bs_step_once(double time, double* h, double* hdid, double tol, int64_t* rej
 // particles' box overlaps as candidates, classified like the MVS path's.
 // Records are appended at the status counter and tagged `step`; the caller
 // clears the candidate counter first.
-void launch_pair_screen(double h, int step, const EncCtl* ctl = nullptr, int prev = -1, int cur = -1) {
+void launch_pair_screen(double h, int step) {
     Context& c = ctx();
     const int nb = c.nbig - 1;
     c.boxes.reserve((size_t)4 * std::max(1, nb));
     c.detail.reserve((size_t)std::max(1, nb) * TAB_DETAIL);
-    if (cur < 0) cur = c.cur;
-    if (prev < 0) prev = 1 - cur;
+    const int cur = c.cur, prev = 1 - cur;
     ScreenArgs a{};
-    a.ctl = ctl;
     a.nbig = c.nbig;
     a.nsplit = c.nsplit;
     a.np = c.np;
@@ -665,7 +662,6 @@ void launch_pair_screen(double h, int step, const EncCtl* ctl = nullptr, int pre
         ca.event_cap = (int)c.events.n;
         ca.status = c.status.p;
         ca.step_base = step;
-        ca.ctl = ctl;
         launch_classify(ca, c.stream);
     }
     check(cudaGetLastError(), "screen");
@@ -919,6 +915,86 @@ void order_particles(int n, int nbig, double mu, const double* x, const double* 
     check(cub::DeviceRadixSort::SortPairs(tmp, temp, kin, kout, iin, iout, np, 0, 8, c.stream), "order");
     slot_maps_kernel<<<blocks(c.npcap), 256, 0, c.stream>>>(iout, np, c.npcap, c.perm[c.kc].p, c.inv.p);
     check(cudaGetLastError(), "order");
+}
+
+// The records of a fused run in (step, min(i,j), max(i,j)) order on the
+// device: a 64-bit key per record (the step above the two 1-based ids, each
+// in `idbits` bits; one record per pair per step makes the keys distinct),
+// a radix sort of (key, record index), then a gather that also turns each
+// record's time into an absolute one as the host would: tend[s] is the
+// driver's clock after step s (time + h added step by step), central-body
+// records hold their entry time from the step's start, pair records their
+// minimum time from its end.
+__global__ void event_key_kernel(const MercuryEvent* ev, const int* step, int n, int idbits,
+                                 unsigned long long* key, int* idx) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const unsigned long long i = (unsigned)ev[k].i, j = (unsigned)ev[k].j;
+    const unsigned long long lo = i < j ? i : j, hi = i < j ? j : i;
+    key[k] = ((unsigned long long)(unsigned)step[k] << (2 * idbits)) | (lo << idbits) | hi;
+    idx[k] = k;
+}
+
+__global__ void event_gather_kernel(const MercuryEvent* ev, const int* step, const int* order, int n,
+                                   const double* tend, double h, MercuryEvent* out, int* out_step) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    const int k = order[r];
+    MercuryEvent e = ev[k];
+    const int s = step[k];
+    const double te = tend[s];
+    if (e.kind == EV_CENTRAL) e.time = te - h + e.time;
+    else e.time = e.time + te;
+    store_event(out + r, e);
+    out_step[r] = s;
+}
+
+// Bits for one 1-based id of n bodies, or 0 when (step, id, id) keys of a
+// run of nsteps steps do not fit in 64 bits.
+int event_id_bits(int n, int nsteps) {
+    int idbits = 1, stepbits = 1;
+    while ((1ll << idbits) <= (long long)n) ++idbits;
+    while ((1ll << stepbits) < (long long)nsteps) ++stepbits;
+    return 2 * idbits + stepbits <= 64 ? idbits : 0;
+}
+
+// Orders the nev records of the last fused run into c.ev_sorted /
+// c.ev_sorted_step (see event_key_kernel). False when the keys do not fit.
+bool order_events_device(int nev, int nsteps, const std::vector<double>& tend, double h) {
+    Context& c = ctx();
+    const int idbits = event_id_bits(c.n, nsteps);
+    if (!idbits) return false;
+    int stepbits = 1;
+    while ((1ll << stepbits) < (long long)nsteps) ++stepbits;
+    const int end_bit = 2 * idbits + stepbits;
+    auto align = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    size_t temp = 0;
+    check(cub::DeviceRadixSort::SortPairs(nullptr, temp, (const unsigned long long*)nullptr,
+                                          (unsigned long long*)nullptr, (const int*)nullptr, (int*)nullptr, nev, 0,
+                                          end_bit, c.stream),
+          "events");
+    const size_t kb = align(sizeof(unsigned long long) * (size_t)nev), ib = align(sizeof(int) * (size_t)nev);
+    const size_t tb = align(sizeof(double) * (size_t)nsteps);
+    c.order_scratch.reserve(2 * kb + 2 * ib + tb + align(temp));
+    char* base = c.order_scratch.p;
+    auto* kin = reinterpret_cast<unsigned long long*>(base);
+    auto* kout = reinterpret_cast<unsigned long long*>(base + kb);
+    int* iin = reinterpret_cast<int*>(base + 2 * kb);
+    int* iout = reinterpret_cast<int*>(base + 2 * kb + ib);
+    double* dtend = reinterpret_cast<double*>(base + 2 * kb + 2 * ib);
+    void* tmp = base + 2 * kb + 2 * ib + tb;
+    c.ev_sorted.reserve(nev);
+    c.ev_sorted_step.reserve(nev);
+    check(cudaMemcpyAsync(dtend, tend.data(), sizeof(double) * (size_t)nsteps, cudaMemcpyHostToDevice, c.stream),
+          "events");
+    event_key_kernel<<<blocks(nev), 256, 0, c.stream>>>(c.events.p, c.event_step.p, nev, idbits, kin, iin);
+    check(cub::DeviceRadixSort::SortPairs(tmp, temp, kin, kout, iin, iout, nev, 0, end_bit, c.stream), "events");
+    event_gather_kernel<<<blocks(nev), 256, 0, c.stream>>>(c.events.p, c.event_step.p, iout, nev, dtend, h,
+                                                           c.ev_sorted.p, c.ev_sorted_step.p);
+    check(cudaGetLastError(), "events");
+    // the host array of tend is read by the copy above: wait for it
+    check(cudaStreamSynchronize(c.stream), "events");
+    return true;
 }
 
 // Device re-ordering of the slots as the state evolves (scattered or eccentric
@@ -1437,6 +1513,7 @@ int mercury_cuda_upload(int n, int nbig, int pn, int ngflag, const double* m, co
         for (int k = 0; k < 3; ++k) c.jcen[k] = jcen[k];
         c.m_host.assign(m, m + n);
         c.event_rate = 0.0;
+        c.ev_device = 0;
         c.mbig.reserve(ns);
         c.rcebig.reserve(ns);
         c.rphysbig.reserve(ns);
@@ -1624,6 +1701,7 @@ int mercury_cuda_events(double time, double h, double rcen, const MercuryEvent**
                 h2d(c.events.p, keep.data(), sizeof(MercuryEvent) * c.pair_events, c.stream, "events");
         }
         const int nev = c.stepped ? c.status_host->events : 0;
+        c.ev_device = 0;
         size_records(c.host_events, nev);
         if (nev) {
             const int got = std::min(nev, head);
@@ -2055,12 +2133,6 @@ int mercury_b200_mvs_advance(double time, double h, int nsteps, double rcen, int
         c.pair_events = 0;
         const int nev = c.status_host->events;
         c.event_rate = std::max(c.event_rate, (double)nev / nsteps);
-        size_records(c.host_events, nev);
-        size_records(c.host_steps, nev);
-        if (nev)
-            copy_out({{c.events.p, c.host_events.data(), sizeof(MercuryEvent) * (size_t)nev},
-                      {c.event_step.p, c.host_steps.data(), sizeof(int) * (size_t)nev}},
-                     c.stream);
         // absolute times: the driver's clock advances by time = time + h per step
         std::vector<double> tend(nsteps);
         double t = time;
@@ -2068,6 +2140,23 @@ int mercury_b200_mvs_advance(double time, double h, int nsteps, double rcen, int
             t = t + h;
             tend[s] = t;
         }
+        // ordered on the device; mercury_b200_events copies them straight
+        // into the caller's arrays
+        c.host_events.clear();
+        c.host_steps.clear();
+        c.event_order.clear();
+        c.ev_device = 0;
+        if (nev && order_events_device(nev, nsteps, tend, h)) {
+            c.ev_device = nev;
+            *nevents = nev;
+            return 0;
+        }
+        size_records(c.host_events, nev);
+        size_records(c.host_steps, nev);
+        if (nev)
+            copy_out({{c.events.p, c.host_events.data(), sizeof(MercuryEvent) * (size_t)nev},
+                      {c.event_step.p, c.host_steps.data(), sizeof(int) * (size_t)nev}},
+                     c.stream);
         for (int k = 0; k < nev; ++k) {
             MercuryEvent& e = c.host_events[k];
             const double te = tend[c.host_steps[k]];
@@ -2086,6 +2175,21 @@ int mercury_b200_mvs_advance(double time, double h, int nsteps, double rcen, int
 
 int mercury_b200_events(MercuryEvent* dst, int* steps, int cap) {
     Context& c = ctx();
+    if (c.ev_device > 0) {
+        // the last fused run's records, ordered on the device
+        const int nev = c.ev_device;
+        const size_t k = (size_t)std::max(0, std::min(cap, nev));
+        if (k == 0) return nev;
+        try {
+            std::vector<HostSpan> spans = {{c.ev_sorted.p, dst, sizeof(MercuryEvent) * k}};
+            if (steps) spans.push_back({c.ev_sorted_step.p, steps, sizeof(int) * k});
+            copy_out(spans, c.stream);
+        } catch (const std::exception& e) {
+            report(e);
+            return -1;
+        }
+        return nev;
+    }
     const int nev = (int)c.host_events.size();
     const int k = std::max(0, std::min(cap, nev));
     const bool ordered = c.event_order.size() == c.host_events.size();
@@ -2246,39 +2350,29 @@ void add_dropin_span(cudaEvent_t a, cudaEvent_t b) {
     if (cudaEventElapsedTime(&ms, a, b) == cudaSuccess) g_dropin_ms += ms;
 }
 
-// The kernels of one attempt of the encounter subsystem with the step
-// control on the device: the BS2 levels and extrapolation at the trial step
-// in ctl, bs_decide_kernel, the commit of the accepted level into buffer
-// `out`, the pair screen between `in` and `out`, and the copy of the new
-// state back into `in`. After the subsystem reached h (ctl->stop) every
-// kernel returns at once.
-void enqueue_encounter_attempt(const BsArgs& a, int in, int out) {
-    Context& c = ctx();
-    launch_bs_sequence(a, c.stream);
-    launch_bs_decide(c.enc_ctl.p, c.bs_errs.p, c.bs_lvst.p, c.status.p, c.stream);
-    launch_bs_commit_of(a, 0, c.enc_ctl.p);
-    launch_pair_screen(0.0, 0, c.enc_ctl.p, in, out);
-    launch_bs_copyback(c.enc_ctl.p, c.bigstate[out].p, c.bigstate[in].p, c.nsplit, c.pstate[out].p, c.pstate[in].p,
-                       c.npcap, c.stream);
-    check(cudaGetLastError(), "launch");
-}
-
 // mdt_hkce's substep loop (mercury6_2.for:3884-3937) with mdt_bs2's step
-// control (3568-3596) held on the device. The host enqueues attempts in
-// blocks, as replays of a CUDA graph of GRAPH_ATTEMPTS attempts, and reads
-// the control block back once per block; the block size follows the
-// attempts the run still needs, estimated from its progress. The screens'
-// records stay on the device, tagged with their substep, until the subsystem
-// reaches h. The states do not depend on the records, so after an event,
-// candidate or substep-table overflow the buffers grow and the run is redone
-// from its starting state.
+// control (3568-3596) held on the device. One attempt is three launches: the
+// massive set's levels (keeping its start state), the particles' levels with
+// the massive set's extrapolation as the last CTA, and enc_post_kernel (the
+// decision in every thread, the next attempt's control block, and after an
+// acceptance the in-place commit and the substep's pair screen). Attempts
+// alternate between two control blocks and two sets of level maxima
+// (attempt parity p reads set p and prepares set 1 - p), so that no launch
+// reads what it writes. After the subsystem reached h every launch returns at
+// once. The host enqueues attempts in blocks, as replays of a CUDA graph of
+// GRAPH_ATTEMPTS attempts, and reads the control block back once per block;
+// the block size follows the attempts still needed, estimated from the
+// progress. Records stay on the device, tagged with their substep, until the
+// subsystem reaches h. The states do not depend on the records, so after an
+// event-buffer or substep-table overflow the buffers grow and the run is
+// redone from its starting state.
 void encounter_run_device(double time, double h, double tol, double* hrec, int64_t* nforces_out,
                           std::vector<MercuryEvent>& keep) {
     Context& c = ctx();
     if (c.algorithm != 3) throw std::runtime_error("the encounter subsystem steps by algorithm 3 (mdt_bs2)");
-    constexpr int GRAPH_ATTEMPTS = 8;
+    constexpr int GRAPH_ATTEMPTS = 8;   // even: a replay leaves the parity where it found it
     mercury_cuda_reset(1);
-    const int in = c.cur, out = 1 - c.cur;
+    const int in = c.cur;
     const double hrec0 = *hrec;
     const size_t np_el = c.pstate[in].n, nb_el = c.bigstate[in].n;
     c.snapshot.reserve(np_el + nb_el);
@@ -2287,9 +2381,11 @@ void encounter_run_device(double time, double h, double tol, double* hrec, int64
     check(cudaMemcpyAsync(c.snapshot.p + np_el, c.bigstate[in].p, sizeof(double) * nb_el, cudaMemcpyDeviceToDevice,
                           c.stream),
           "snapshot");
-    c.enc_ctl.reserve(1);
+    c.enc_ctl.reserve(2);
     c.enc_tstep.reserve(1024);
-    int max_cands = 0;
+    c.enc_bpre.reserve((size_t)6 * c.nsplit);
+    c.bs_errs.reserve(26);
+    c.bs_lvst.reserve(26);
     struct Graph {
         cudaGraph_t g = nullptr;
         cudaGraphExec_t e = nullptr;
@@ -2313,32 +2409,64 @@ void encounter_run_device(double time, double h, double tol, double* hrec, int64
         k.step_cap = (int)c.enc_tstep.n;
         k.tstep = c.enc_tstep.p;
         *c.enc_host = k;
-        const BsArgs a = [&] {
-            BsArgs r = bs_attempt_args(0.0);
-            r.ctl = c.enc_ctl.p;
-            return r;
-        }();
-        c.boxes.reserve((size_t)4 * std::max(1, c.nbig - 1));
-        c.detail.reserve((size_t)std::max(1, c.nbig - 1) * TAB_DETAIL);
+        BsArgs base = bs_attempt_args(0.0);
+        base.bx_pre = c.enc_bpre.p;
+        base.fuse_extrap = 1;
+        auto attempt = [&](int p) {
+            BsArgs a = base;
+            a.ctl = c.enc_ctl.p + p;
+            a.errs = c.bs_errs.p + 13 * p;
+            a.lvst = c.bs_lvst.p + 13 * p;
+            launch_bs_sequence(a, c.stream);
+            EncPostArgs e{};
+            e.ctl_in = c.enc_ctl.p + p;
+            e.ctl_out = c.enc_ctl.p + (1 - p);
+            e.errs = a.errs;
+            e.lvst = a.lvst;
+            e.errs_next = c.bs_errs.p + 13 * (1 - p);
+            e.lvst_next = c.bs_lvst.p + 13 * (1 - p);
+            e.nbig = c.nbig;
+            e.nsplit = c.nsplit;
+            e.np = c.np;
+            e.npcap = c.npcap;
+            e.active_np = a.active_np;
+            e.bx_pre = c.enc_bpre.p;
+            e.bx = c.bigstate[in].p;
+            e.bcand = a.bcand;
+            e.pcand = a.pcand;
+            e.px = c.pstate[in].p;
+            e.mbig = c.mbig.p;
+            e.rcebig = c.rcebig.p;
+            e.rphysbig = c.rphysbig.p;
+            e.pconst = c.pconst[c.kc].p;
+            e.perm = c.permp();
+            e.events = c.events.p;
+            e.event_step = c.event_step.p;
+            e.event_cap = (int)c.events.n;
+            e.status = c.status.p;
+            launch_enc_post(e, c.stream);
+            check(cudaGetLastError(), "launch");
+        };
         check(cudaMemcpyAsync(c.enc_ctl.p, c.enc_host, sizeof(EncCtl), cudaMemcpyHostToDevice, c.stream), "upload");
         check(cudaMemsetAsync(c.status.p, 0, sizeof(DeviceStatus), c.stream), "memset");
-        check(cudaMemsetAsync(c.bs_errs.p, 0, sizeof(unsigned long long) * 13, c.stream), "memset");
-        check(cudaMemsetAsync(c.bs_lvst.p, 0, sizeof(DeviceStatus) * 13, c.stream), "memset");
-        // one attempt eagerly (kernel attributes set), then the graph
+        check(cudaMemsetAsync(c.bs_errs.p, 0, sizeof(unsigned long long) * 26, c.stream), "memset");
+        check(cudaMemsetAsync(c.bs_lvst.p, 0, sizeof(DeviceStatus) * 26, c.stream), "memset");
+        // attempt 0 eagerly (kernel attributes set), then the graph of attempts
+        // 1.. GRAPH_ATTEMPTS (parities 1, 0, 1, ...); after every block the
+        // newest control block is copy 1
         check(cudaEventRecord(c.d0, c.stream), "event");
-        enqueue_encounter_attempt(a, in, out);
+        attempt(0);
         Graph graph;
         check(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeRelaxed), "graph");
-        for (int q = 0; q < GRAPH_ATTEMPTS; ++q) enqueue_encounter_attempt(a, in, out);
+        for (int q = 0; q < GRAPH_ATTEMPTS; ++q) attempt((1 + q) % 2);
         check(cudaStreamEndCapture(c.stream, &graph.g), "graph");
         check(cudaGraphInstantiate(&graph.e, graph.g, 0), "graph");
-        const int per_attempt = 2 + (c.np > 0 ? 1 : 0) + 1 + 1 + 1 + (c.np > 0 && c.nbig > 1 ? 3 : 0) + 1;
-        c.dropin_launches += per_attempt;
+        c.dropin_launches += 3;
         int blocks = 2;   // graph replays in the first block
         for (;;) {
             for (int b = 0; b < blocks; ++b) check(cudaGraphLaunch(graph.e, c.stream), "graph");
-            c.dropin_launches += (int64_t)blocks * GRAPH_ATTEMPTS * per_attempt;
-            check(cudaMemcpyAsync(c.enc_host, c.enc_ctl.p, sizeof(EncCtl), cudaMemcpyDeviceToHost, c.stream),
+            c.dropin_launches += (int64_t)blocks * GRAPH_ATTEMPTS * 3;
+            check(cudaMemcpyAsync(c.enc_host, c.enc_ctl.p + 1, sizeof(EncCtl), cudaMemcpyDeviceToHost, c.stream),
                   "status");
             check(cudaEventRecord(c.d1, c.stream), "event");
             check(cudaEventSynchronize(c.d1), "step");
@@ -2358,7 +2486,6 @@ void encounter_run_device(double time, double h, double tol, double* hrec, int64
         if (done.error == ENC_ERR_ADVANCE)
             throw std::runtime_error("BS cannot advance time at the requested tolerance");
         read_status();
-        max_cands = std::max(max_cands, std::max(done.max_cands, c.status_host->cands));
         const bool steps_full = done.error == ENC_ERR_STEPS;
         if (!steps_full && !c.status_host->overflow) {
             const int nev = c.status_host->events;
@@ -2392,13 +2519,8 @@ void encounter_run_device(double time, double h, double tol, double* hrec, int64
             return;
         }
         if (redo > 8) throw std::runtime_error("event buffer growth failed");
-        if (steps_full) {
-            c.enc_tstep.reserve(2 * c.enc_tstep.n);
-        }
-        if (c.status_host->overflow) {
-            grow_after_overflow();
-            if (c.status_host->overflow & 2) c.cands.reserve((size_t)max_cands + max_cands / 4 + 4096);
-        }
+        if (steps_full) c.enc_tstep.reserve(2 * c.enc_tstep.n);
+        if (c.status_host->overflow) grow_after_overflow();
         check(cudaMemcpyAsync(c.pstate[in].p, c.snapshot.p, sizeof(double) * np_el, cudaMemcpyDeviceToDevice,
                               c.stream),
               "restore");
@@ -2446,6 +2568,7 @@ int mercury_b200_encounter_run(double time, double h, double tol, double rcen, d
         }
         Context& c = ctx();
         c.host_events.swap(keep);
+        c.ev_device = 0;
         c.host_steps.clear();
         c.event_order.clear();
         *forces = nforces;

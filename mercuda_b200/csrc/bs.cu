@@ -4,6 +4,7 @@
 #include <algorithm>
 #include "allforce.cuh"
 #include "bs.cuh"
+#include "mvs.cuh"
 
 namespace mb200 {
 namespace {
@@ -114,21 +115,36 @@ __device__ double3 hkce_force(const BsArgs& A, int k, const double* X) {
     return hkce_central(a, make_double3(X[k], X[N + k], X[2 * N + k]), A.f.m0);
 }
 
-// mfo_hkce for a massless member (subsystem index g) against table row T:
-// every pair has a Big first body i, whose position is in the row.
-__device__ double3 hkce_particle_force(const BsArgs& A, int g, const double3 x, double rcrit_p, const double* T) {
+// Pairs of a massless member kept in its CTA's shared memory for the
+// sequence (partner, rc = max(rcrit_i, rcrit_member)); further pairs are read
+// from the pair list where they are used.
+constexpr int PAIR_CACHE = 4;
+
+// hkce_particle_force with the member's first PAIR_CACHE pairs from the
+// lane-strided shared copies ci / crc (npair pairs in all) and the Big bodies
+// (x, y, z, m) from the body block B of a table row. The same terms in the
+// same order.
+__device__ __forceinline__ double3 hkce_member_force(const BsArgs& A, int g, int npair, const int* ci,
+                                                     const double* crc, const double3 x, double rcrit_p,
+                                                     const double* B) {
     double3 a = make_double3(0.0, 0.0, 0.0);
-    for (int e = A.adj_off[g]; e < A.adj_off[g + 1]; ++e) {
-        const int i = A.adj[e].x;
-        const double* row = T + FT_HEAD + 4 * (i - 1);
+    auto term = [&](int i, double rc) {
+        const double* row = B + 4 * (i - 1);
         const double dx = x.x - row[0], dy = x.y - row[1], dz = x.z - row[2];
         double tmp2;
-        if (!hkce_pair(dx * dx + dy * dy + dz * dz, fmax(A.rcrit[i], rcrit_p), tmp2)) continue;
+        if (!hkce_pair(dx * dx + dy * dy + dz * dz, rc, tmp2)) return;
         const double faci = tmp2 * row[3];
         a.x = a.x - faci * dx;
         a.y = a.y - faci * dy;
         a.z = a.z - faci * dz;
-    }
+    };
+    const int nc = npair < PAIR_CACHE ? npair : PAIR_CACHE;
+    for (int q = 0; q < nc; ++q) term(ci[32 * q], crc[32 * q]);
+    if (npair > PAIR_CACHE)
+        for (int e = A.adj_off[g] + PAIR_CACHE; e < A.adj_off[g + 1]; ++e) {
+            const int i = A.adj[e].x;
+            term(i, fmax(A.rcrit[i], rcrit_p));
+        }
     return hkce_central(a, x, A.f.m0);
 }
 
@@ -247,6 +263,8 @@ template <int VARIANT> __global__ void __launch_bounds__(256) bs_massive_level_k
     }
     const int N = A.f.nsplit, tid = threadIdx.x, nt = blockDim.x, n = blockIdx.x + 1;
     const int stride = force_row(A.f.nbig - 1);
+    if (A.bx_pre && n == 1)
+        for (int q = tid; q < 6 * N; q += nt) A.bx_pre[q] = A.bx[q];
     double* X = sm;
     double* V = sm + 3 * N;
     double* XE = sm + 6 * N;
@@ -349,18 +367,61 @@ template <int VARIANT> __global__ void __launch_bounds__(256) bs_massive_level_k
     }
 }
 
-// The massive set's extrapolation in level order (one CTA): per level the
-// Neville updates (mercury6_2.for:3352-3366) with one thread per (body,
-// component) and the coefficients computed once, then from level 4 on each
-// (body, component)'s candidate sum and each body's error term for the
-// level's maximum.
-template <int VARIANT> __global__ void __launch_bounds__(256) bs_massive_extrap_kernel(BsArgs A) {
-    const int N = A.f.nsplit, tid = threadIdx.x, nt = blockDim.x;
+// The massive set's extrapolation in level order (mercury6_2.for:3352-3378)
+// by the calling block: one thread per (body, component) takes its raw level
+// states D(1..L) through the Neville updates in registers, writes each
+// level's candidate sum from level 4 on, and parks D(1) after level n in
+// level n's raw slot; then one thread per (body, level) adds the body's error
+// term to the level's maximum. Per (body, component) the same statements in
+// the same order as a level loop; a maximum does not depend on the order.
+template <int VARIANT> __device__ void massive_extrap_block(const BsArgs& A, const double (*co)[2]) {
     constexpr int L = bs_levels(VARIANT);
-    double* D = A.draw;
+    const int N = A.f.nsplit, nb1 = N - 1, M = 6 * nb1, tid = threadIdx.x, nt = blockDim.x;
+    double* raw = A.draw;
+    for (int q = tid; q < M; q += nt) {
+        const int c = q / nb1, k = 1 + q % nb1;
+        double D[L];
+#pragma unroll
+        for (int n = 0; n < L; ++n) D[n] = raw[(size_t)n * 6 * N + c * N + k];
+#pragma unroll
+        for (int n = 1; n <= L; ++n) {
+#pragma unroll
+            for (int j = n - 1; j >= 1; --j) {
+                // read where used: hoisted out of the (body, component) loop
+                // the 66 coefficient pairs would not fit in registers
+                const volatile double* cj = co[coef_index(n, j)];
+                D[j - 1] = cj[0] * D[j] - cj[1] * D[j - 1];
+            }
+            if (n > 3) {
+                double sum = D[0];
+#pragma unroll
+                for (int j = 2; j <= n; ++j) sum = sum + D[j - 1];
+                A.bcand[(size_t)(n - 4) * 6 * N + c * N + k] = sum;
+            }
+            raw[(size_t)(n - 1) * 6 * N + c * N + k] = D[0];
+        }
+    }
+    __syncthreads();
+    const double* X0 = A.bx;
+    const double* V0 = A.bx + 3 * N;
+    for (int q = tid; q < nb1 * (L - 3); q += nt) {
+        const int k = 1 + q % nb1, n = 4 + q / nb1;
+        const double tmp1 = X0[k] * X0[k] + X0[N + k] * X0[N + k] + X0[2 * N + k] * X0[2 * N + k];
+        const double tmp2 = V0[k] * V0[k] + V0[N + k] * V0[N + k] + V0[2 * N + k] * V0[2 * N + k];
+        const double xscal = 1.0 / fmax(tmp1, 1e-300);
+        const double vscal = 1.0 / fmax(tmp2, 1e-300);
+        double q6[6];
+        for (int c = 0; c < 6; ++c) q6[c] = raw[(size_t)(n - 1) * 6 * N + c * N + k];
+        double e = 0.0;
+        const bool finite = body_error(q6, xscal, vscal, e);
+        level_error(e, finite, &A.errs[n]);
+    }
+}
+
+// The massive set's extrapolation as a launch of its own (one CTA).
+template <int VARIANT> __global__ void __launch_bounds__(256) bs_massive_extrap_kernel(BsArgs A) {
+    constexpr int L = bs_levels(VARIANT);
     __shared__ double co[L * (L - 1) / 2][2];
-    __shared__ double wmax[8];
-    __shared__ int wbad[8];
     double h0 = A.h0;
     if (A.ctl) {
         if (A.ctl->stop) return;
@@ -368,56 +429,7 @@ template <int VARIANT> __global__ void __launch_bounds__(256) bs_massive_extrap_
     }
     neville_coefficients<VARIANT>(h0, co);
     __syncthreads();
-    const int nb1 = N - 1, M = 6 * nb1;
-    for (int n = 1; n <= L; ++n) {
-        for (int q = tid; q < M; q += nt) {
-            const int c = q / nb1, k = 1 + q % nb1;
-            for (int j = n - 1; j >= 1; --j) {
-                const double* cj = co[coef_index(n, j)];
-                double* Dj = D + (size_t)(j - 1) * 6 * N;
-                const double* Dj1 = D + (size_t)j * 6 * N;
-                Dj[c * N + k] = cj[0] * Dj1[c * N + k] - cj[1] * Dj[c * N + k];
-            }
-        }
-        if (n > 3) {
-            __syncthreads();
-            double* cand = A.bcand + (size_t)(n - 4) * 6 * N;
-            for (int q = tid; q < M; q += nt) {
-                const int c = q / nb1, k = 1 + q % nb1;
-                double s = D[c * N + k];
-                for (int j = 2; j <= n; ++j) s = s + D[(size_t)(j - 1) * 6 * N + c * N + k];
-                cand[c * N + k] = s;
-            }
-            double emax = 0.0;
-            int bad = 0;
-            for (int k = 1 + tid; k < N; k += nt) {
-                const double* X0 = A.bx;
-                const double* V0 = A.bx + 3 * N;
-                const double tmp1 = X0[k] * X0[k] + X0[N + k] * X0[N + k] + X0[2 * N + k] * X0[2 * N + k];
-                const double tmp2 = V0[k] * V0[k] + V0[N + k] * V0[N + k] + V0[2 * N + k] * V0[2 * N + k];
-                const double xscal = 1.0 / fmax(tmp1, 1e-300);
-                const double vscal = 1.0 / fmax(tmp2, 1e-300);
-                double q6[6];
-                for (int c = 0; c < 6; ++c) q6[c] = D[c * N + k];
-                double e;
-                if (body_error(q6, xscal, vscal, e)) emax = fmax(emax, e);
-                else bad = 1;
-            }
-            for (int o = 16; o; o >>= 1) {
-                emax = fmax(emax, __shfl_xor_sync(FULLMASK, emax, o));
-                bad |= __shfl_xor_sync(FULLMASK, bad, o);
-            }
-            if ((tid & 31) == 0) { wmax[tid >> 5] = emax; wbad[tid >> 5] = bad; }
-            __syncthreads();
-            if (tid == 0) {
-                double m = 0.0;
-                int b = 0;
-                for (int w = 0; w < (nt + 31) / 32; ++w) { m = fmax(m, wmax[w]); b |= wbad[w]; }
-                level_error(m, !b, &A.errs[n]);
-            }
-        }
-        __syncthreads();
-    }
+    massive_extrap_block<VARIANT>(A, co);
 }
 
 // ------------------------------------------------------------ particles
@@ -436,6 +448,12 @@ template <int VARIANT> __global__ void __launch_bounds__(bs_levels(VARIANT) * 16
     __shared__ double dsm[L][6][32];
     __shared__ double a0sm[3][32];
     __shared__ double co[L * (L - 1) / 2][2];
+    // encounter members: their first pairs, and (A.stage_bodies) the Big
+    // bodies' (x, y, z, m) of every table row, [rows][4 nb]
+    __shared__ int pair_n[32];
+    __shared__ int pair_i[PAIR_CACHE * 32];
+    __shared__ double pair_rc[PAIR_CACHE * 32];
+    extern __shared__ double staged[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     double h0 = A.h0;
     if (A.ctl) {
@@ -443,6 +461,12 @@ template <int VARIANT> __global__ void __launch_bounds__(bs_levels(VARIANT) * 16
         h0 = A.ctl->h0;
     }
     neville_coefficients<VARIANT>(h0, co);
+    if (A.fuse_extrap && blockIdx.x == gridDim.x - 1) {
+        // the launch's last CTA: the massive set's extrapolation
+        __syncthreads();
+        massive_extrap_block<VARIANT>(A, co);
+        return;
+    }
     const int p = blockIdx.x * 32 + lane;
     const bool ok = p < A.np && A.perm[p] < A.active_np;
     const int nb = A.f.nbig - 1, stride = force_row(nb), S = A.npcap;
@@ -450,22 +474,45 @@ template <int VARIANT> __global__ void __launch_bounds__(bs_levels(VARIANT) * 16
     double mj = 0.0, g5[5] = {0, 0, 0, 0, 0};
     // the encounter subsystem (BS2 only): mfo_hkce from the member's pairs
     const bool hkce = VARIANT == 2 && A.hkce;
+    const bool stage = hkce && A.stage_bodies;
+    const int bw = 4 * nb;   // body block of a table row
     int g = 0;
     double rcrit_p = 0.0;
-    auto force = [&](const double3 x, const double3 v, const double* Tr, DeviceStatus* st) {
-        return hkce ? hkce_particle_force(A, g, x, rcrit_p, Tr) : particle_allforce(x, v, Tr, nb, A.f, mj, g5, st);
+    if (hkce) {
+        if (ok) {
+            g = A.f.nsplit + A.perm[p];
+            rcrit_p = A.pconst[(size_t)PC_RCRIT * S + p];
+        }
+        if (w == 0) {
+            const int e0 = ok ? A.adj_off[g] : 0, e1 = ok ? A.adj_off[g + 1] : 0;
+            pair_n[lane] = e1 - e0;
+            for (int q = 0; q < PAIR_CACHE && e0 + q < e1; ++q) {
+                const int i = A.adj[e0 + q].x;
+                pair_i[32 * q + lane] = i;
+                pair_rc[32 * q + lane] = fmax(A.rcrit[i], rcrit_p);
+            }
+        }
+        if (stage)
+            for (int q = threadIdx.x; q < bs_rows(VARIANT) * bw; q += blockDim.x) {
+                const int r = q / bw;
+                staged[q] = A.table[(size_t)r * stride + FT_HEAD + (q - r * bw)];
+            }
+        __syncthreads();
+    }
+    const int npair = hkce ? pair_n[lane] : 0;
+    auto force = [&](const double3 x, const double3 v, int r, DeviceStatus* st) {
+        if (hkce)
+            return hkce_member_force(A, g, npair, pair_i + lane, pair_rc + lane, x, rcrit_p,
+                                     stage ? staged + (size_t)r * bw : A.table + (size_t)r * stride + FT_HEAD);
+        return particle_allforce(x, v, A.table + (size_t)r * stride, nb, A.f, mj, g5, st);
     };
     if (ok) {
         x0 = make_double3(A.px[p], A.px[S + p], A.px[2 * S + p]);
         v0 = make_double3(A.px[3 * S + p], A.px[4 * S + p], A.px[5 * S + p]);
         mj = A.pconst[p];
         for (int c = 0; c < 5; ++c) g5[c] = A.pconst[(3 + c) * (size_t)S + p];
-        if (hkce) {
-            g = A.f.nsplit + A.perm[p];
-            rcrit_p = A.pconst[(size_t)PC_RCRIT * S + p];
-        }
         if (w == 0) {
-            const double3 a = force(x0, v0, A.table, &A.lvst[0]);
+            const double3 a = force(x0, v0, 0, &A.lvst[0]);
             a0sm[0][lane] = a.x;
             a0sm[1][lane] = a.y;
             a0sm[2][lane] = a.z;
@@ -481,10 +528,7 @@ template <int VARIANT> __global__ void __launch_bounds__(bs_levels(VARIANT) * 16
         DeviceStatus* st = &A.lvst[n];
         const double h = level_h<VARIANT>(h0, n);
         const double h2n = level_h2<VARIANT>(h0, n);
-        auto call = [&](const double3 x, const double3 v) {
-            const double* Tr = A.table + (size_t)(row++) * stride;
-            return force(x, v, Tr, st);
-        };
+        auto call = [&](const double3 x, const double3 v) { return force(x, v, row++, st); };
         auto D = [&](int c) -> double& { return dsm[n - 1][c][lane]; };
         if (VARIANT == 1) {
             const double hx2 = h * 2.0;
@@ -666,11 +710,7 @@ __global__ void __launch_bounds__(64) bs2_tangent_kernel(BsArgs A, int levels, d
 __global__ void __launch_bounds__(128) bs_commit_kernel(BsCommitArgs A) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     const int N = A.nsplit, S = A.npcap;
-    int level_cand = A.cand;
-    if (A.ctl) {
-        if (!A.ctl->accepted) return;
-        level_cand = A.ctl->accepted - 4;
-    }
+    const int level_cand = A.cand;
     if (q < N) {
         if (q == 0) {
             for (int c = 0; c < 9; ++c) A.bx_out[c * N] = A.bx[c * N];
@@ -693,19 +733,22 @@ __global__ void __launch_bounds__(128) bs_commit_kernel(BsCommitArgs A) {
 }
 
 // mdt_bs2's decision after one attempt of the encounter subsystem
-// (mercury6_2.for:3568-3596; the same as bs_accept_level and the host loop
-// of mdt_hkce, 3884-3937): the first level n > 3 whose error maximum is <=
+// (mercury6_2.for:3568-3596; the host loop of mdt_hkce, 3884-3937) applied
+// to the control block c: the first level n > 3 whose error maximum is <=
 // tol^2 is accepted, else the step is halved; after an acceptance the next
-// trial step (x0.55 for a level >= 8, x1.3 below 7), the local clock, and the
-// clipping of the next substep to the subsystem's end. One thread.
-__global__ void bs_decide_kernel(EncCtl* c, unsigned long long* errs, DeviceStatus* lv, DeviceStatus* status) {
-    if (c->stop) {
-        c->accepted = 0;
-        return;
+// trial step (x0.55 for a level >= 8, x1.3 below 7), the local clock, the
+// substep count and the clipping of the next substep to the subsystem's end.
+// Returns the accepted level (0: rejected, stopped or failed). A pure
+// function of its inputs, so every thread of a launch reaches the same
+// decision.
+__device__ __forceinline__ int enc_decide(EncCtl& c, const unsigned long long* errs, const DeviceStatus* lv) {
+    if (c.stop) {
+        c.accepted = 0;
+        return 0;
     }
     constexpr int L = 12;
     const int fails = FAULT_NGF | FAULT_COINCIDENT;
-    c->attempts += 1;
+    c.attempts += 1;
     int accepted = 0, error = 0;
     long long forces = 0;
     if (lv[0].fault & fails) error = ENC_ERR_FORCE;
@@ -721,69 +764,180 @@ __global__ void bs_decide_kernel(EncCtl* c, unsigned long long* errs, DeviceStat
             error = ENC_ERR_NONFINITE;
             break;
         }
-        if (e <= c->tol * c->tol) accepted = n;
+        if (e <= c.tol * c.tol) accepted = n;
     }
-    for (int n = 0; n < 13; ++n) {
-        errs[n] = 0ull;
-        lv[n].fault = 0;
-    }
-    c->forces += forces;
+    c.forces += forces;
     if (error) {
-        c->error = error;
-        c->stop = 1;
-        c->accepted = 0;
-        return;
+        c.error = error;
+        c.stop = 1;
+        c.accepted = 0;
+        return 0;
     }
     if (!accepted) {
-        c->accepted = 0;
-        c->h0 = c->h0 * 0.5;
-        if (c->tlocal + c->h0 == c->tlocal) {
-            c->error = ENC_ERR_ADVANCE;
-            c->stop = 1;
+        c.accepted = 0;
+        c.h0 = c.h0 * 0.5;
+        if (c.tlocal + c.h0 == c.tlocal) {
+            c.error = ENC_ERR_ADVANCE;
+            c.stop = 1;
         }
-        return;
+        return 0;
     }
-    c->accepted = accepted;
-    const double hdid = c->h0;
-    double hnext = c->h0;
+    c.accepted = accepted;
+    const double hdid = c.h0;
+    double hnext = c.h0;
     if (accepted >= 8) hnext = hnext * 0.55;
     if (accepted < 7) hnext = hnext * 1.3;
-    c->hdid = hdid;
-    c->tlocal = c->tlocal + hdid;
-    if (c->substeps >= c->step_cap) {
-        c->error = ENC_ERR_STEPS;
-        c->stop = 1;
-        c->accepted = 0;
-        return;
+    c.hdid = hdid;
+    c.tlocal = c.tlocal + hdid;
+    if (c.substeps >= c.step_cap) {
+        c.error = ENC_ERR_STEPS;
+        c.stop = 1;
+        c.accepted = 0;
+        return 0;
     }
-    c->tstep[c->substeps] = c->time + c->tlocal;
-    c->substeps += 1;
-    // the previous substep's screen candidates, cleared for this one's
-    c->max_cands = max(c->max_cands, status->cands);
-    status->cands = 0;
-    if (!((c->tlocal - c->h) * c->h < 0.0)) {
-        c->stop = 1;
-        return;
+    c.substeps += 1;
+    if (!((c.tlocal - c.h) * c.h < 0.0)) {
+        c.stop = 1;
+        return accepted;
     }
     // the next substep: hrec before the clip to the subsystem's end
-    const double tmp0 = fabs(c->h) - fabs(c->tlocal);
-    c->hrec = hnext;
-    if (fabs(hnext) > tmp0) hnext = copysign(tmp0, c->h);
-    c->h0 = hnext;
-    c->forces += 1;   // the next substep's start-of-step force
-    if (c->tlocal + c->h0 == c->tlocal) {
-        c->error = ENC_ERR_ADVANCE;
-        c->stop = 1;
+    const double tmp0 = fabs(c.h) - fabs(c.tlocal);
+    c.hrec = hnext;
+    if (fabs(hnext) > tmp0) hnext = copysign(tmp0, c.h);
+    c.h0 = hnext;
+    c.forces += 1;   // the next substep's start-of-step force
+    if (c.tlocal + c.h0 == c.tlocal) {
+        c.error = ENC_ERR_ADVANCE;
+        c.stop = 1;
     }
+    return accepted;
 }
 
-__global__ void __launch_bounds__(256) bs_copyback_kernel(const EncCtl* c, const double* bsrc, double* bdst,
-                                                          int nsplit, const double* psrc, double* pdst, int npcap) {
-    if (!c->accepted) return;
-    const size_t nb = (size_t)9 * nsplit, np = (size_t)9 * npcap;
-    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < nb + np; q += (size_t)gridDim.x * blockDim.x) {
-        if (q < nb) bdst[q] = bsrc[q];
-        else pdst[q - nb] = psrc[q - nb];
+// Everything after one attempt of the encounter subsystem, in one launch:
+// the decision (every thread), the new control block and the cleared level
+// maxima of the next attempt (thread 0 of block 0), and after an acceptance
+// the commit of the accepted level in place with mce_stat between the
+// attempt's start and the committed state (mercury6_2.for:1765-1918): the
+// Big bodies' boxes and end states in each block's shared memory, the
+// massive pairs and the massive set's commit in block 0 (from the start
+// state the level kernel kept), one particle slot per thread with its box
+// test and classification inline. Records carry the substep index.
+__global__ void __launch_bounds__(128) enc_post_kernel(EncPostArgs A) {
+    extern __shared__ double sh[];
+    EncCtl c = *A.ctl_in;
+    const int acc = enc_decide(c, A.errs, A.lvst);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (acc) c.tstep[c.substeps - 1] = c.time + c.tlocal;
+        *A.ctl_out = c;
+        for (int n = 0; n < 13; ++n) {
+            A.errs_next[n] = 0ull;
+            A.lvst_next[n] = DeviceStatus{};
+        }
+    }
+    if (!acc) return;
+    const int N = A.nsplit, nb = A.nbig - 1, S = A.npcap;
+    const double h = c.hdid, hm1 = 1.0 / h;
+    const int step = c.substeps - 1;
+    const double* bpost = A.bcand + (size_t)(acc - 4) * 6 * N;
+    const double* ppost = A.pcand + (size_t)(acc - 4) * 6 * S;
+    auto ends = [&](int k) {
+        return PairEnds{make_double3(A.bx_pre[k], A.bx_pre[N + k], A.bx_pre[2 * N + k]),
+                        make_double3(A.bx_pre[3 * N + k], A.bx_pre[4 * N + k], A.bx_pre[5 * N + k]),
+                        make_double3(bpost[k], bpost[N + k], bpost[2 * N + k]),
+                        make_double3(bpost[3 * N + k], bpost[4 * N + k], bpost[5 * N + k])};
+    };
+    auto box = [&](int k, double* bx) {
+        const PairEnds E = ends(k);
+        const double pad = A.rcebig[k] * 1.2;
+        double lo, hi;
+        box_extent(E.x0.x, E.x1.x, E.v0.x, E.v1.x, h, lo, hi);
+        bx[0] = lo - pad;
+        bx[1] = hi + pad;
+        box_extent(E.x0.y, E.x1.y, E.v0.y, E.v1.y, h, lo, hi);
+        bx[2] = lo - pad;
+        bx[3] = hi + pad;
+    };
+    double* sbox = sh;                                  // [nb][4]
+    double* sdet = sh + 4 * (size_t)(nb > 0 ? nb : 1);  // [nb][TAB_DETAIL]
+    for (int k = 1 + threadIdx.x; k < A.nbig; k += blockDim.x) {
+        box(k, sbox + 4 * (k - 1));
+        const PairEnds E = ends(k);
+        double* d = sdet + (size_t)(k - 1) * TAB_DETAIL;
+        const double3 q[4] = {E.x0, E.v0, E.x1, E.v1};
+        for (int w = 0; w < 4; ++w) {
+            d[3 * w] = q[w].x;
+            d[3 * w + 1] = q[w].y;
+            d[3 * w + 2] = q[w].z;
+        }
+        d[12] = A.rcebig[k];
+        d[13] = A.rphysbig[k];
+    }
+    __syncthreads();
+    auto record = [&](const PairEnds& I, const PairEnds& J, const PairClass& pc, int id_i, int id_j, bool swap) {
+        const int slot = atomicAdd(&A.status->events, 1);
+        if (slot < A.event_cap) {
+            pair_record(A.events + slot, I, J, pc, hm1, id_i, id_j, swap);
+            A.event_step[slot] = step;
+        } else {
+            atomicOr(&A.status->overflow, 1);
+        }
+    };
+    if (blockIdx.x == 0) {
+        // pairs within the massive set: i Big, i < j < nsplit
+        const int npair_max = nb * (N - 1);
+        for (int q = threadIdx.x; q < npair_max; q += blockDim.x) {
+            const int i = 1 + q / (N - 1), j = 1 + q % (N - 1);
+            if (j <= i) continue;
+            double bi[4], bj[4];
+            box(i, bi);
+            box(j, bj);
+            if (!(bi[1] >= bj[0] && bj[1] >= bi[0] && bi[3] >= bj[2] && bj[3] >= bi[2])) continue;
+            PairClass pc;
+            const PairEnds I = ends(i), J = ends(j);
+            if (pair_classify(I, J, A.rcebig[i], A.rcebig[j], A.rphysbig[i], A.rphysbig[j], h, pc))
+                record(I, J, pc, i + 1, j + 1, A.mbig[j] > A.mbig[i] && j < A.nbig);
+        }
+        // the massive set's commit (the central body's row stays)
+        for (int k = 1 + threadIdx.x; k < N; k += blockDim.x) {
+            for (int q = 0; q < 6; ++q) A.bx[q * N + k] = bpost[q * N + k];
+            for (int q = 6; q < 9; ++q) A.bx[q * N + k] = 0.0;
+        }
+    }
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= A.np) return;
+    const bool moves = A.perm[p] < A.active_np;
+    const PairEnds J{make_double3(A.px[p], A.px[S + p], A.px[2 * S + p]),
+                     make_double3(A.px[3 * S + p], A.px[4 * S + p], A.px[5 * S + p]),
+                     moves ? make_double3(ppost[p], ppost[S + p], ppost[2 * S + p])
+                           : make_double3(A.px[p], A.px[S + p], A.px[2 * S + p]),
+                     moves ? make_double3(ppost[3 * S + p], ppost[4 * S + p], ppost[5 * S + p])
+                           : make_double3(A.px[3 * S + p], A.px[4 * S + p], A.px[5 * S + p])};
+    const double rce = A.pconst[S + p], rphys = A.pconst[2 * (size_t)S + p];
+    double lo_x, hi_x, lo_y, hi_y;
+    box_extent(J.x0.x, J.x1.x, J.v0.x, J.v1.x, h, lo_x, hi_x);
+    box_extent(J.x0.y, J.x1.y, J.v0.y, J.v1.y, h, lo_y, hi_y);
+    const double pad = rce * 1.2;
+    lo_x -= pad;
+    hi_x += pad;
+    lo_y -= pad;
+    hi_y += pad;
+    for (int b = 0; b < nb; ++b) {
+        const double* bb = sbox + 4 * b;
+        if (!(bb[1] >= lo_x && hi_x >= bb[0] && bb[3] >= lo_y && hi_y >= bb[2])) continue;
+        const double* d = sdet + (size_t)b * TAB_DETAIL;
+        const PairEnds I{make_double3(d[0], d[1], d[2]), make_double3(d[3], d[4], d[5]),
+                         make_double3(d[6], d[7], d[8]), make_double3(d[9], d[10], d[11])};
+        PairClass pc;
+        if (pair_classify(I, J, d[12], rce, d[13], rphys, h, pc)) record(I, J, pc, b + 2, N + A.perm[p] + 1, false);
+    }
+    if (moves) {
+        A.px[p] = J.x1.x;
+        A.px[S + p] = J.x1.y;
+        A.px[2 * S + p] = J.x1.z;
+        A.px[3 * S + p] = J.v1.x;
+        A.px[4 * S + p] = J.v1.y;
+        A.px[5 * S + p] = J.v1.z;
+        for (int q = 6; q < 9; ++q) A.px[(size_t)q * S + p] = 0.0;
     }
 }
 
@@ -792,13 +946,29 @@ template <int VARIANT> void launch_variant(const BsArgs& a, cudaStream_t s) {
     const size_t msmem = sizeof(double) * (((size_t)BS_LEVEL_ROWS + 12) * N + massive_par_scratch(N));
     if (msmem > 48 * 1024)
         cudaFuncSetAttribute(bs_massive_level_kernel<VARIANT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msmem);
-    // one warp per 32 bodies, and with the parallel force terms enough for one term each
+    // one warp per 32 bodies, and with the parallel force terms (mfo_all)
+    // enough for one term each
     int mthreads = std::min(256, std::max(32, (N + 31) / 32 * 32));
-    if (massive_par_scratch(N)) mthreads = std::max(mthreads, std::min(256, (N * N + 31) / 32 * 32));
+    if (massive_par_scratch(N) && !a.hkce) mthreads = std::max(mthreads, std::min(256, (N * N + 31) / 32 * 32));
     bs_massive_level_kernel<VARIANT><<<bs_levels(VARIANT), mthreads, msmem, s>>>(a);
-    bs_massive_extrap_kernel<VARIANT><<<1, mthreads, 0, s>>>(a);
-    if (a.np <= 0) return;
-    bs_particle_kernel<VARIANT><<<(a.np + 31) / 32, bs_levels(VARIANT) * 16, 0, s>>>(a);
+    if (!a.fuse_extrap) bs_massive_extrap_kernel<VARIANT><<<1, mthreads, 0, s>>>(a);
+    const int pblocks = (a.np > 0 ? (a.np + 31) / 32 : 0) + (a.fuse_extrap ? 1 : 0);
+    if (pblocks <= 0) return;
+    size_t psmem = 0;
+    BsArgs b = a;
+    b.stage_bodies = 0;
+    if (VARIANT == 2 && a.hkce) {
+        // the Big bodies of every table row, while that stays modest
+        const size_t bytes = sizeof(double) * (size_t)bs_rows(VARIANT) * 4 * (size_t)(a.f.nbig - 1);
+        if (bytes <= 96 * 1024) {
+            psmem = bytes;
+            b.stage_bodies = 1;
+            if (bytes > 16 * 1024)
+                cudaFuncSetAttribute(bs_particle_kernel<VARIANT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)bytes);
+        }
+    }
+    bs_particle_kernel<VARIANT><<<pblocks, bs_levels(VARIANT) * 16, psmem, s>>>(b);
 }
 
 }  // namespace
@@ -816,16 +986,12 @@ void launch_bs2_tangent(const BsArgs& a, int levels, double* tg, cudaStream_t s)
     bs2_tangent_kernel<<<(unsigned)((total + threads - 1) / threads), threads, smem, s>>>(a, levels, tg);
 }
 
-void launch_bs_decide(EncCtl* ctl, unsigned long long* errs, DeviceStatus* lv, DeviceStatus* status,
-                      cudaStream_t s) {
-    bs_decide_kernel<<<1, 1, 0, s>>>(ctl, errs, lv, status);
-}
-
-void launch_bs_copyback(const EncCtl* ctl, const double* bsrc, double* bdst, int nsplit, const double* psrc,
-                        double* pdst, int npcap, cudaStream_t s) {
-    const size_t total = (size_t)9 * (nsplit + npcap);
-    const int blocks = (int)std::min<size_t>(148 * 4, (total + 255) / 256);
-    bs_copyback_kernel<<<blocks, 256, 0, s>>>(ctl, bsrc, bdst, nsplit, psrc, pdst, npcap);
+void launch_enc_post(const EncPostArgs& a, cudaStream_t s) {
+    const int nb = a.nbig - 1;
+    const size_t smem = sizeof(double) * (size_t)(nb > 0 ? nb : 1) * (4 + TAB_DETAIL);
+    if (smem > 48 * 1024) cudaFuncSetAttribute(enc_post_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const int blocks = std::max(1, (a.np + 127) / 128);
+    enc_post_kernel<<<blocks, 128, smem, s>>>(a);
 }
 
 void launch_bs_commit(const BsCommitArgs& a, cudaStream_t s) {

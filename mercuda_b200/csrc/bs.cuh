@@ -67,6 +67,9 @@ struct BsArgs {
     const int* perm;             // slot -> particle index
     int active_np;               // particles with index >= active_np sit the step out (epoch synchronisation)
     const EncCtl* ctl = nullptr; // non-null: the trial step is ctl->h0, nothing runs once ctl->stop
+    double* bx_pre = nullptr;    // non-null: [6][nsplit] copy of the massive set's start state (level kernel)
+    int fuse_extrap = 0;         // 1: the massive set's extrapolation runs as the particle launch's last CTA
+    int stage_bodies = 0;        // set at launch: the particle kernel keeps the table's Big bodies in shared memory
 };
 
 struct BsCommitArgs {
@@ -80,19 +83,36 @@ struct BsCommitArgs {
     const double* px;            // start-of-step particle state (kept by inactive particles)
     const int* perm;             // slot -> particle index
     int active_np;               // as in BsArgs
-    const EncCtl* ctl = nullptr; // non-null: commit level ctl->accepted, nothing when it is 0
 };
 
-// One decision of the encounter subsystem's device-held step control after
-// an attempt of launch_bs_sequence (errs and lv its level maxima and faults,
-// cleared here for the next attempt; the pair screen's candidate counter
-// cleared after an acceptance). One thread.
-void launch_bs_decide(EncCtl* ctl, unsigned long long* errs, DeviceStatus* lv, DeviceStatus* status,
-                      cudaStream_t s);
-// After an accepted attempt: the committed state (bx_out/px_out of the
-// commit) copied back over the start-of-step buffers it came from.
-void launch_bs_copyback(const EncCtl* ctl, const double* bsrc, double* bdst, int nsplit, const double* psrc,
-                        double* pdst, int npcap, cudaStream_t s);
+// Everything after one attempt of the encounter subsystem (enc_post_kernel):
+// the step decision from this attempt's level maxima and faults, the control
+// block of the next attempt with its level maxima cleared, and after an
+// acceptance the commit in place and the pair screen of the substep.
+struct EncPostArgs {
+    const EncCtl* ctl_in;              // the control block this attempt ran with
+    EncCtl* ctl_out;                   // the next attempt's
+    const unsigned long long* errs;    // [13] this attempt's level maxima
+    const DeviceStatus* lvst;          // [13] and force faults
+    unsigned long long* errs_next;     // [13] cleared for the next attempt
+    DeviceStatus* lvst_next;           // [13]
+    int nbig, nsplit, np, npcap, active_np;
+    const double* bx_pre;              // [6][nsplit] massive set at the attempt's start
+    double* bx;                        // [9][nsplit] massive set, committed in place
+    const double* bcand;               // BsArgs::bcand
+    const double* pcand;               // BsArgs::pcand
+    double* px;                        // [9][npcap] particles, committed in place
+    const double* mbig;
+    const double* rcebig;
+    const double* rphysbig;
+    const double* pconst;              // rows 1, 2: rce, rphys of the particle slots
+    const int* perm;
+    MercuryEvent* events;
+    int* event_step;
+    int event_cap;
+    DeviceStatus* status;
+};
+void launch_enc_post(const EncPostArgs& a, cudaStream_t s);
 
 void launch_bs_sequence(const BsArgs& a, cudaStream_t s);
 void launch_bs_commit(const BsCommitArgs& a, cudaStream_t s);

@@ -55,10 +55,11 @@ __device__ __forceinline__ void raise_fault(DeviceStatus* st, int bit) { atomicO
 
 // Step control of the HYBRID encounter subsystem held on the device
 // (mdt_hkce's substep loop, mercury6_2.for:3884-3937, with mdt_bs2's level
-// choice, 3568-3596): the BS2 attempt kernels read the trial step h0 here,
-// bs_decide_kernel takes each attempt's decision and advances the local
-// clock, and the commit, copy-back and pair screen act only after an
-// accepted attempt. The host reads it back every few dozen attempts.
+// choice, 3568-3596): the BS2 attempt kernels read the trial step h0 here;
+// the post-attempt kernel takes each attempt's decision, advances the local
+// clock into the next attempt's copy (two copies alternate), and commits and
+// screens only after an acceptance. The host reads it back every few dozen
+// attempts.
 struct EncCtl {
     double h0;          // trial step of the next attempt
     double hdid;        // step of the last accepted substep
@@ -74,7 +75,6 @@ struct EncCtl {
     int substeps;       // accepted substeps
     int attempts;
     int step_cap;       // entries of tstep
-    int max_cands;      // most screen candidates of one substep
     double* tstep;      // [step_cap] end time (time + tlocal) of each accepted substep
 };
 constexpr int ENC_ERR_FORCE = 1, ENC_ERR_NONFINITE = 2, ENC_ERR_ADVANCE = 3, ENC_ERR_STEPS = 4;

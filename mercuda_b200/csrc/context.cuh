@@ -126,6 +126,11 @@ struct Context {
     std::vector<MercuryEvent> host_events;
     std::vector<int> host_steps;
     std::vector<uint32_t> event_order;   // last advance: host_events in (step, min, max) order
+    // the last fused run's records in (step, min, max) order on the device
+    // (ev_device of them; 0: the records are in host_events)
+    DBuf<MercuryEvent> ev_sorted;
+    DBuf<int> ev_sorted_step;
+    int ev_device = 0;
     double event_rate = 0.0;             // most event records per step seen by an advance of this system
     int pair_events = 0;
     // staging
@@ -162,10 +167,12 @@ struct Context {
     // the encounter subsystem's step control, read back once per block of
     // attempts
     EncCtl* enc_host = nullptr;
-    // the encounter subsystem's step control on the device and the end time
-    // of each accepted substep
+    // the encounter subsystem's step control on the device (two copies that
+    // alternate between attempts), the end time of each accepted substep, and
+    // the massive set's state at the start of the current attempt
     DBuf<EncCtl> enc_ctl;
     DBuf<double> enc_tstep;
+    DBuf<double> enc_bpre;
     // the first records of a drop-in events call, read back with its status
     static constexpr int EVENT_HEAD = 1024;
     MercuryEvent* ev_head = nullptr;
@@ -219,6 +226,7 @@ struct Context {
         bs_lvst.release();
         enc_ctl.release();
         enc_tstep.release();
+        enc_bpre.release();
         hy_pairs.release();
         hy_ids.release();
         adj_off.release();
@@ -231,6 +239,9 @@ struct Context {
         event_step.release();
         cands.release();
         status.release();
+        ev_sorted.release();
+        ev_sorted_step.release();
+        ev_device = 0;
         host_events.clear();
         host_steps.clear();
         event_order.clear();

@@ -735,15 +735,8 @@ __global__ void __launch_bounds__(128) mvs_corrector_particle_kernel(CorrectorAr
 // mce_stat's test for each encounter candidate of the last launch
 // (mercury6_2.for:1815-1908) and the record it produces.
 __global__ void __launch_bounds__(256) classify_kernel(ClassifyArgs A) {
-    double h = A.h;
-    int step_base = A.step_base;
-    if (A.ctl) {
-        if (!A.ctl->accepted) return;
-        h = A.ctl->hdid;
-        step_base = A.ctl->substeps - 1;
-    }
     const int count = min(A.status->cands, A.cand_cap);
-    const double hm1 = 1.0 / h;
+    const double hm1 = 1.0 / A.h;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
         const EncounterCandidate& c = A.cands[k];
         const double* d = A.detail + ((size_t)c.step * A.nb + c.body) * TAB_DETAIL;
@@ -752,11 +745,11 @@ __global__ void __launch_bounds__(256) classify_kernel(ClassifyArgs A) {
         const PairEnds J{make_double3(c.x0[0], c.x0[1], c.x0[2]), make_double3(c.v0[0], c.v0[1], c.v0[2]),
                          make_double3(c.x1[0], c.x1[1], c.x1[2]), make_double3(c.v1[0], c.v1[1], c.v1[2])};
         PairClass pc;
-        if (!pair_classify(I, J, d[12], c.rce, d[13], c.rphys, h, pc)) continue;
+        if (!pair_classify(I, J, d[12], c.rce, d[13], c.rphys, A.h, pc)) continue;
         const int slot = atomicAdd(&A.status->events, 1);
         if (slot < A.event_cap) {
             pair_record(A.events + slot, I, J, pc, hm1, c.body + 2, c.id, false);
-            A.event_step[slot] = c.step + step_base;
+            A.event_step[slot] = c.step + A.step_base;
         } else {
             atomicOr(&A.status->overflow, 1);
         }

@@ -183,7 +183,6 @@ struct ClassifyArgs {
     int event_cap;
     DeviceStatus* status;
     int step_base;         // added to a candidate's step in event_step
-    const EncCtl* ctl = nullptr;  // non-null: h and step_base from the last accepted substep, nothing after a rejection
 };
 void launch_classify(const ClassifyArgs& a, cudaStream_t s);
 

@@ -546,14 +546,7 @@ __global__ void __launch_bounds__(128) force_particle_kernel(ForceAllArgs A) {
 // ---------------------------------------------------------------- screen
 __global__ void __launch_bounds__(256) screen_massive_kernel(ScreenArgs A) {
     const int N = A.nsplit, nb = A.nbig - 1;
-    double h = A.h;
-    int step = A.step;
-    if (A.ctl) {
-        if (!A.ctl->accepted) return;
-        h = A.ctl->hdid;
-        step = A.ctl->substeps - 1;
-    }
-    const double hm1 = 1.0 / h;
+    const double h = A.h, hm1 = 1.0 / h;
     auto ends = [&](int k) {
         return PairEnds{make_double3(A.b0[k], A.b0[N + k], A.b0[2 * N + k]),
                         make_double3(A.b0[3 * N + k], A.b0[4 * N + k], A.b0[5 * N + k]),
@@ -599,7 +592,7 @@ __global__ void __launch_bounds__(256) screen_massive_kernel(ScreenArgs A) {
             const int slot = atomicAdd(&A.status->events, 1);
             if (slot < A.event_cap) {
                 pair_record(A.events + slot, I, J, pc, hm1, i + 1, j + 1, A.mbig[j] > A.mbig[i] && j < A.nbig);
-                A.event_step[slot] = step;
+                A.event_step[slot] = A.step;
             } else {
                 atomicOr(&A.status->overflow, 1);
             }
@@ -609,11 +602,6 @@ __global__ void __launch_bounds__(256) screen_massive_kernel(ScreenArgs A) {
 
 __global__ void __launch_bounds__(128) screen_particle_kernel(ScreenArgs A) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x, S = A.npcap, nb = A.nbig - 1;
-    double h = A.h;
-    if (A.ctl) {
-        if (!A.ctl->accepted) return;
-        h = A.ctl->hdid;
-    }
     const bool ok = p < A.np;
     double3 x0, v0, x1, v1;
     double lo_x = 0, hi_x = 0, lo_y = 0, hi_y = 0, rce = 0, rphys = 0;
@@ -625,8 +613,8 @@ __global__ void __launch_bounds__(128) screen_particle_kernel(ScreenArgs A) {
         rce = A.pconst[S + p];
         rphys = A.pconst[2 * (size_t)S + p];
         const double pad = rce * 1.2;
-        box_extent(x0.x, x1.x, v0.x, v1.x, h, lo_x, hi_x);
-        box_extent(x0.y, x1.y, v0.y, v1.y, h, lo_y, hi_y);
+        box_extent(x0.x, x1.x, v0.x, v1.x, A.h, lo_x, hi_x);
+        box_extent(x0.y, x1.y, v0.y, v1.y, A.h, lo_y, hi_y);
         lo_x -= pad; hi_x += pad; lo_y -= pad; hi_y += pad;
     }
     for (int b = 0; b < nb; ++b) {

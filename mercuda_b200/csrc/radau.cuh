@@ -87,7 +87,6 @@ struct ScreenArgs {
     int cand_cap;
     DeviceStatus* status;
     int step;              // event_step of this screen's records
-    const EncCtl* ctl = nullptr;  // non-null: h and step from the last accepted substep, nothing after a rejection
 };
 void launch_screen(const ScreenArgs& a, cudaStream_t s);
 
