@@ -204,12 +204,13 @@ __device__ double3 hkce_particle_force_jvp(const BsArgs& A, int g, const double3
 // are the set's masses and non-gravitational constants, head a shared copy of
 // the row's head for the set's own forces, PT shared scratch for the terms
 // computed in parallel (null: the sequential loops).
+template <bool HKCE>
 __device__ void massive_call(const BsArgs& A, const double* X, const double* V, double* out, double* T,
                              DeviceStatus* st, const double* mb, const double* ngf, double* head, double* PT) {
     const ForceCfg& f = A.f;
     const int N = f.nsplit;
     __syncthreads();
-    if (A.hkce) {
+    if (HKCE) {
         for (int k = 1 + threadIdx.x; k < N; k += blockDim.x) {
             if (k < f.nbig) {
                 double* row = T + FT_HEAD + 4 * (k - 1);
@@ -254,7 +255,7 @@ __device__ void massive_call(const BsArgs& A, const double* X, const double* V, 
 // Neville updates in level order. The start-of-step force is computed by
 // every CTA (the same statements), level 1's writing table row 0 and the
 // others a private row.
-template <int VARIANT> __global__ void __launch_bounds__(256) bs_massive_level_kernel(BsArgs A) {
+template <int VARIANT, bool HKCE> __global__ void __launch_bounds__(256) bs_massive_level_kernel(BsArgs A) {
     extern __shared__ double sm[];
     double h0 = A.h0;
     if (A.ctl) {
@@ -285,7 +286,7 @@ template <int VARIANT> __global__ void __launch_bounds__(256) bs_massive_level_k
     __syncthreads();
     __shared__ double head[FT_HEAD];
     auto call = [&](const double* Xc, const double* Vc, double* out, double* T, DeviceStatus* st) {
-        massive_call(A, Xc, Vc, out, T, st, mb, ngf, head, PT);
+        massive_call<HKCE>(A, Xc, Vc, out, T, st, mb, ngf, head, PT);
     };
     for (int k = tid; k < N; k += nt)
         for (int c = 0; c < 3; ++c) {
@@ -442,7 +443,10 @@ template <int VARIANT> __global__ void __launch_bounds__(256) bs_massive_extrap_
 // component and the error inputs; last, the warps share the levels' error
 // maxima. Per particle and component the same statements, in the same order,
 // as a level loop would run them.
-template <int VARIANT> __global__ void __launch_bounds__(bs_levels(VARIANT) * 16) bs_particle_kernel(BsArgs A) {
+// With mfo_hkce (encounter members: a few pairs each) three CTAs share an SM,
+// so that a subsystem of up to 444 x 32 members runs in one wave.
+template <int VARIANT, bool HKCE>
+__global__ void __launch_bounds__(bs_levels(VARIANT) * 16, HKCE ? 3 : 1) bs_particle_kernel(BsArgs A) {
     constexpr int L = bs_levels(VARIANT);
     constexpr int NW = L * 16 / 32;   // warps of the CTA
     __shared__ double dsm[L][6][32];
@@ -473,7 +477,7 @@ template <int VARIANT> __global__ void __launch_bounds__(bs_levels(VARIANT) * 16
     double3 x0 = make_double3(0.0, 0.0, 0.0), v0 = x0;
     double mj = 0.0, g5[5] = {0, 0, 0, 0, 0};
     // the encounter subsystem (BS2 only): mfo_hkce from the member's pairs
-    const bool hkce = VARIANT == 2 && A.hkce;
+    constexpr bool hkce = VARIANT == 2 && HKCE;
     const bool stage = hkce && A.stage_bodies;
     const int bw = 4 * nb;   // body block of a table row
     int g = 0;
@@ -509,8 +513,10 @@ template <int VARIANT> __global__ void __launch_bounds__(bs_levels(VARIANT) * 16
     if (ok) {
         x0 = make_double3(A.px[p], A.px[S + p], A.px[2 * S + p]);
         v0 = make_double3(A.px[3 * S + p], A.px[4 * S + p], A.px[5 * S + p]);
-        mj = A.pconst[p];
-        for (int c = 0; c < 5; ++c) g5[c] = A.pconst[(3 + c) * (size_t)S + p];
+        if (!hkce) {
+            mj = A.pconst[p];
+            for (int c = 0; c < 5; ++c) g5[c] = A.pconst[(3 + c) * (size_t)S + p];
+        }
         if (w == 0) {
             const double3 a = force(x0, v0, 0, &A.lvst[0]);
             a0sm[0][lane] = a.x;
@@ -748,18 +754,28 @@ __device__ __forceinline__ int enc_decide(EncCtl& c, const unsigned long long* e
     }
     constexpr int L = 12;
     const int fails = FAULT_NGF | FAULT_COINCIDENT;
+    // every level's maximum and fault word first: independent loads in flight together
+    unsigned long long em[L + 1];
+    int fw[L + 1];
+#pragma unroll
+    for (int n = 0; n <= L; ++n) {
+        em[n] = errs[n];
+        fw[n] = lv[n].fault;
+    }
     c.attempts += 1;
     int accepted = 0, error = 0;
     long long forces = 0;
-    if (lv[0].fault & fails) error = ENC_ERR_FORCE;
-    for (int n = 1; n <= L && !error && !accepted; ++n) {
+    if (fw[0] & fails) error = ENC_ERR_FORCE;
+#pragma unroll
+    for (int n = 1; n <= L; ++n) {
+        if (error || accepted) break;
         forces += n;
-        if (lv[n].fault & fails) {
+        if (fw[n] & fails) {
             error = ENC_ERR_FORCE;
             break;
         }
         if (n <= 3) continue;
-        const double e = __longlong_as_double((long long)errs[n]);
+        const double e = __longlong_as_double((long long)em[n]);
         if (!isfinite(e)) {
             error = ENC_ERR_NONFINITE;
             break;
@@ -941,41 +957,46 @@ __global__ void __launch_bounds__(128) enc_post_kernel(EncPostArgs A) {
     }
 }
 
-template <int VARIANT> void launch_variant(const BsArgs& a, cudaStream_t s) {
+// mfo_all (HKCE false) or, for mdt_bs2 in the encounter subsystem, mfo_hkce:
+// separate instantiations, so that the encounter kernels carry neither the
+// registers nor the code of the general force law.
+template <int VARIANT, bool HKCE> void launch_variant(const BsArgs& a, cudaStream_t s) {
     const int N = a.f.nsplit;
     const size_t msmem = sizeof(double) * (((size_t)BS_LEVEL_ROWS + 12) * N + massive_par_scratch(N));
     if (msmem > 48 * 1024)
-        cudaFuncSetAttribute(bs_massive_level_kernel<VARIANT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msmem);
+        cudaFuncSetAttribute(bs_massive_level_kernel<VARIANT, HKCE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)msmem);
     // one warp per 32 bodies, and with the parallel force terms (mfo_all)
     // enough for one term each
     int mthreads = std::min(256, std::max(32, (N + 31) / 32 * 32));
     if (massive_par_scratch(N) && !a.hkce) mthreads = std::max(mthreads, std::min(256, (N * N + 31) / 32 * 32));
-    bs_massive_level_kernel<VARIANT><<<bs_levels(VARIANT), mthreads, msmem, s>>>(a);
+    bs_massive_level_kernel<VARIANT, HKCE><<<bs_levels(VARIANT), mthreads, msmem, s>>>(a);
     if (!a.fuse_extrap) bs_massive_extrap_kernel<VARIANT><<<1, mthreads, 0, s>>>(a);
     const int pblocks = (a.np > 0 ? (a.np + 31) / 32 : 0) + (a.fuse_extrap ? 1 : 0);
     if (pblocks <= 0) return;
     size_t psmem = 0;
     BsArgs b = a;
     b.stage_bodies = 0;
-    if (VARIANT == 2 && a.hkce) {
+    if (VARIANT == 2 && HKCE) {
         // the Big bodies of every table row, while that stays modest
         const size_t bytes = sizeof(double) * (size_t)bs_rows(VARIANT) * 4 * (size_t)(a.f.nbig - 1);
         if (bytes <= 96 * 1024) {
             psmem = bytes;
             b.stage_bodies = 1;
             if (bytes > 16 * 1024)
-                cudaFuncSetAttribute(bs_particle_kernel<VARIANT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                cudaFuncSetAttribute(bs_particle_kernel<VARIANT, HKCE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)bytes);
         }
     }
-    bs_particle_kernel<VARIANT><<<pblocks, bs_levels(VARIANT) * 16, psmem, s>>>(b);
+    bs_particle_kernel<VARIANT, HKCE><<<pblocks, bs_levels(VARIANT) * 16, psmem, s>>>(b);
 }
 
 }  // namespace
 
 void launch_bs_sequence(const BsArgs& a, cudaStream_t s) {
-    if (a.variant == 1) launch_variant<1>(a, s);
-    else launch_variant<2>(a, s);
+    if (a.variant == 1) launch_variant<1, false>(a, s);
+    else if (a.hkce) launch_variant<2, true>(a, s);
+    else launch_variant<2, false>(a, s);
 }
 
 void launch_bs2_tangent(const BsArgs& a, int levels, double* tg, cudaStream_t s) {
