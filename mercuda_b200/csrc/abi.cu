@@ -287,8 +287,9 @@ MvsParticleArgs particle_args(int in, int out, int nsteps, int reset, int centra
 }
 
 // Particle kernel of one launch followed by the classification of its
-// encounter candidates into event records (same stream).
-void particles_and_events(const MvsParticleArgs& pa, cudaStream_t s) {
+// encounter candidates into event records (same stream). detail is the base
+// of the run's pair details: a candidate carries its step within the run.
+void particles_and_events(const MvsParticleArgs& pa, const double* detail, cudaStream_t s) {
     Context& c = ctx();
     check(cudaMemsetAsync(&c.status.p->next_tile, 0, sizeof(int), s), "memset");
     launch_mvs_particles(pa, s, c.particle_threads);
@@ -296,7 +297,7 @@ void particles_and_events(const MvsParticleArgs& pa, cudaStream_t s) {
     ca.nb = c.nbig - 1;
     ca.nbig = c.nbig;
     ca.h = pa.h;
-    ca.detail = c.detail.p;
+    ca.detail = detail;
     ca.cands = c.cands.p;
     ca.cand_cap = (int)c.cands.n;
     ca.events = c.events.p;
@@ -322,6 +323,91 @@ void grow_after_overflow() {
     }
 }
 
+// The per-step MVS path (one mercury_cuda_step per step, as mal_hcon calls
+// it) runs the next step's Big bodies ahead: the Big bodies never feel the
+// particles, so as soon as a step is committed their next step with the same
+// h runs on the second stream into spare buffers (state, force table, pair
+// records, status) while the host works. The next mercury_cuda_step with the
+// same h and no reset takes it (the spare state becomes the step's output,
+// its records and faults are merged into the step's status on the device);
+// any other call that may change the system first orders the library stream
+// after it and drops it.
+constexpr int SPEC_RECORDS = 1024;   // Big-pair records a speculative step may hold
+
+__global__ void spec_merge_kernel(const DeviceStatus* ss, const MercuryEvent* sev, int scap, DeviceStatus* st,
+                                  MercuryEvent* ev, int* ev_step, int cap) {
+    const int n = ss->events;
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        st->events = n;
+        st->fault |= ss->fault;
+        if (n > scap || n > cap || ss->overflow) st->overflow |= 1;
+    }
+    const int m = min(n, min(scap, cap));
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) {
+        store_event(ev + k, sev[k]);
+        ev_step[k] = 0;
+    }
+}
+
+void spec_drop() {
+    Context& c = ctx();
+    if (!c.spec_live) return;
+    // also host-side: later calls may copy into its inputs synchronously
+    c.spec_live = false;
+    check(cudaEventSynchronize(c.spec_done), "step");
+}
+
+void spec_launch(double h) {
+    Context& c = ctx();
+    const int nb = c.nbig - 1;
+    c.spec_big.reserve((size_t)9 * c.nsplit);
+    c.spec_tab.reserve((size_t)2 * tab_stride(nb));
+    c.spec_detail.reserve((size_t)std::max(1, nb) * TAB_DETAIL);
+    c.spec_events.reserve(SPEC_RECORDS);
+    c.spec_event_step.reserve(SPEC_RECORDS);
+    c.spec_status.reserve(1);
+    if (!c.spec_done) {
+        check(cudaEventCreateWithFlags(&c.spec_done, cudaEventDisableTiming), "event");
+        check(cudaEventCreateWithFlags(&c.spec_ready, cudaEventDisableTiming), "event");
+    }
+    check(cudaEventRecord(c.spec_ready, c.stream), "event");
+    check(cudaStreamWaitEvent(c.stream_big, c.spec_ready, 0), "wait");
+    check(cudaMemsetAsync(c.spec_status.p, 0, sizeof(DeviceStatus), c.stream_big), "memset");
+    MvsBigArgs a = big_args(c.cur, 1 - c.cur, 1, 0, 0, 0, h, 0.0, c.spec_tab.p, c.spec_detail.p);
+    a.out.x = c.spec_big.p;
+    a.out.v = c.spec_big.p + 3 * c.nsplit;
+    a.out.a = c.spec_big.p + 6 * c.nsplit;
+    a.events = c.spec_events.p;
+    a.event_step = c.spec_event_step.p;
+    a.event_cap = SPEC_RECORDS;
+    a.status = c.spec_status.p;
+    launch_mvs_big(a, c.stream_big);
+    check(cudaGetLastError(), "launch");
+    check(cudaEventRecord(c.spec_done, c.stream_big), "event");
+    c.dropin_launches += 1;
+    c.spec_live = true;
+    c.spec_h = h;
+    c.spec_from = c.cur;
+}
+
+// The speculative Big-body step as this step's, when it was made for it.
+bool spec_take(double h) {
+    Context& c = ctx();
+    if (!c.spec_live) return false;
+    if (c.spec_h != h || c.spec_from != c.cur || c.reset) {
+        spec_drop();
+        return false;
+    }
+    check(cudaStreamWaitEvent(c.stream, c.spec_done, 0), "wait");
+    c.spec_live = false;
+    std::swap(c.bigstate[1 - c.cur], c.spec_big);
+    spec_merge_kernel<<<4, 256, 0, c.stream>>>(c.spec_status.p, c.spec_events.p, SPEC_RECORDS, c.status.p,
+                                               c.events.p, c.event_step.p, (int)c.events.n);
+    check(cudaGetLastError(), "launch");
+    c.dropin_launches += 1;
+    return true;
+}
+
 // One MVS step (mdt_mvs) of the whole system: Big-body CTA then the particle
 // kernel, double-buffered so the pre-step state stays available. Pair events
 // are left in the event buffer with tmin in their time field.
@@ -329,6 +415,7 @@ void mvs_step_once(double h) {
     Context& c = ctx();
     if (c.steps_since_order >= 32) {
         const int src = c.cur;
+        spec_drop();
         c.cur = reorder_slots(src, h, c.stream);
         // the Big bodies share the buffer index: carry their state across
         if (c.cur != src)
@@ -342,10 +429,16 @@ void mvs_step_once(double h) {
         check(cudaMemsetAsync(c.status.p, 0, sizeof(DeviceStatus), c.stream), "memset");
         const int in = c.cur, out = 1 - c.cur;
         const int reset = c.reset ? 1 : 0;
-        launch_mvs_big(big_args(in, out, 1, reset, 0, 0, h, 0.0, c.tab.p, c.detail.p), c.stream);
-        c.dropin_launches += 1 + (c.np > 0 ? 1 + (c.nbig > 1 ? 1 : 0) : 0);
-        if (c.np > 0)
-            particles_and_events(particle_args(in, out, 1, reset, 0, 0, h, 0.0, c.tab.p, c.detail.p), c.stream);
+        const bool ahead = attempt == 0 && spec_take(h);
+        const double* tab = ahead ? c.spec_tab.p : c.tab.p;
+        const double* det = ahead ? c.spec_detail.p : c.detail.p;
+        if (!ahead) {
+            spec_drop();
+            launch_mvs_big(big_args(in, out, 1, reset, 0, 0, h, 0.0, c.tab.p, c.detail.p), c.stream);
+            c.dropin_launches += 1;
+        }
+        c.dropin_launches += c.np > 0 ? 1 + (c.nbig > 1 ? 1 : 0) : 0;
+        if (c.np > 0) particles_and_events(particle_args(in, out, 1, reset, 0, 0, h, 0.0, tab, det), det, c.stream);
         check(cudaGetLastError(), "launch");
         read_status();
         if (c.status_host->fault) throw std::runtime_error("MVS force failed");
@@ -359,6 +452,7 @@ void mvs_step_once(double h) {
         c.cur = out;
         c.reset = false;
         c.stepped = true;
+        if (c.steps_since_order < 32) spec_launch(h);
         return;
     }
 }
@@ -1418,6 +1512,11 @@ int mercury_cuda_available(void) {
 
 void mercury_cuda_free(void) {
     Context& c = ctx();
+    try {
+        spec_drop();
+    } catch (const std::exception& e) {
+        report(e);
+    }
     c.release_all();
 }
 
@@ -1425,6 +1524,7 @@ int mercury_cuda_configure(int method) {
     if (method != 1 && method != 2 && method != 3 && method != 4 && method != 9 && method != 10) return 1;
     Context& c = ctx();
     try {
+        spec_drop();
         inject("configure");
         if (method != c.algorithm) mercury_cuda_free();
         c.algorithm = method;
@@ -1436,13 +1536,14 @@ int mercury_cuda_configure(int method) {
 }
 
 void mercury_cuda_reset(int flag) {
-    if (flag != 2) ctx().reset = true;
+    if (flag != 2) ctx().reset = true;   // a speculative Big-body step is not taken after this
 }
 
 int mercury_cuda_upload(int n, int nbig, int pn, int ngflag, const double* m, const double* xx, const double* vv,
                         const double* ng, const double* jcen, const double* limits, const double* radii) {
     Context& c = ctx();
     try {
+        spec_drop();
         inject("upload");
         if (n < 1 || nbig < 1 || nbig > n) throw std::runtime_error("invalid body counts");
         if (is_mvs(c.algorithm) && nbig > 512) throw std::runtime_error("more than 512 Big bodies");
@@ -1728,6 +1829,7 @@ int mercury_cuda_events(double time, double h, double rcen, const MercuryEvent**
 int mercury_cuda_force(double* a) {
     Context& c = ctx();
     try {
+        spec_drop();
         inject("force");
         require_system();
         const int nb = c.nbig - 1, ns = c.nsplit;
@@ -1782,6 +1884,7 @@ int mercury_cuda_export(double h, int physical, double* xx, double* vv) {
 int mercury_cuda_limits(const double* limits) {
     Context& c = ctx();
     try {
+        spec_drop();
         inject("limits");
         require_system();
         check(cudaMemcpyAsync(c.transfer.p, limits, sizeof(double) * c.n, cudaMemcpyHostToDevice, c.stream), "limits");
@@ -1797,6 +1900,7 @@ int mercury_cuda_hybrid_begin(double h, const double* crit, int flag, int cap, i
                               double* xx, double* vv, int64_t* forces) {
     Context& c = ctx();
     try {
+        spec_drop();
         inject("hybrid_begin");
         require_system();
         if (c.algorithm != 10) throw std::runtime_error("hybrid_begin needs algorithm 10");
@@ -1878,6 +1982,7 @@ int mercury_cuda_hybrid_begin(double h, const double* crit, int flag, int cap, i
 int mercury_cuda_hybrid_finish(double h, const double* m, const double* xx, const double* vv, int64_t* forces) {
     Context& c = ctx();
     try {
+        spec_drop();
         inject("hybrid_finish");
         require_system();
         if (!c.hy_begun) throw std::runtime_error("hybrid_finish without hybrid_begin");
@@ -1931,6 +2036,7 @@ int mercury_cuda_encounter_enter(int n, int nb, const double* m, const double* x
                                  const double* crit, const double* limits, const double* radii, int np,
                                  const int* pi, const int* pj) {
     try {
+        spec_drop();
         inject("encounter_enter");
         if (g_active != 0) throw std::runtime_error("encounter subsystem already active");
         g_active = 1;
@@ -2013,6 +2119,7 @@ int mercury_b200_mvs_advance(double time, double h, int nsteps, double rcen, int
     (void)time;
     Context& c = ctx();
     try {
+        spec_drop();
         inject("advance");
         require_system();
         if (!is_mvs(c.algorithm)) throw std::runtime_error("MVS advance needs algorithm 1 or 9");
@@ -2087,7 +2194,7 @@ int mercury_b200_mvs_advance(double time, double h, int nsteps, double rcen, int
                     pcur = reorder_slots(pcur, h, c.stream);
                     check(cudaStreamWaitEvent(c.stream, c.chunk_done[ch], 0), "wait");
                     check(cudaEventRecord(c.kt0[ch], c.stream), "event");
-                    particles_and_events(particle_args(pcur, 1 - pcur, ks, reset, 1, s0, h, rcen, tab, det),
+                    particles_and_events(particle_args(pcur, 1 - pcur, ks, reset, 1, s0, h, rcen, tab, det), c.detail.p,
                                          c.stream);
                     launches += (nb > 0) ? 2 : 1;
                     check(cudaEventRecord(c.kt1[ch], c.stream), "event");
@@ -2320,6 +2427,7 @@ int mercury_b200_ejections(double h, int physical, double rmax, int i0, int* ids
 int mercury_b200_hybrid_members(const int* ids, int count) {
     Context& c = ctx();
     try {
+        spec_drop();
         require_system();
         if (!c.hy_begun) throw std::runtime_error("hybrid_members outside a HYBRID step");
         if (count < 0 || (count > 0 && !ids)) throw std::runtime_error("invalid member list");
@@ -2641,6 +2749,7 @@ int mercury_b200_epoch_order(int nsml, const double* epochs, double tstart, int*
 int mercury_b200_sync_epochs(const double* epoch, double* time, double h0, double tol, double dtout, int* steps) {
     Context& c = ctx();
     try {
+        spec_drop();
         require_system();
         if (c.algorithm != 2) throw std::runtime_error("epoch synchronisation needs algorithm 2 (mdt_bs1)");
         if (c.nsplit != c.nbig) throw std::runtime_error("epoch synchronisation needs massless Small bodies");

@@ -164,6 +164,17 @@ struct Context {
     // timing events of the drop-in calls, and the kernels they launched
     cudaEvent_t d0 = nullptr, d1 = nullptr;
     int64_t dropin_launches = 0;
+    // the per-step MVS path's speculative next Big-body step: its output
+    // state, force table, pair details, records and status, and whether one is
+    // in flight for (spec_h, from buffer spec_from)
+    DBuf<double> spec_big, spec_tab, spec_detail;
+    DBuf<MercuryEvent> spec_events;
+    DBuf<int> spec_event_step;
+    DBuf<DeviceStatus> spec_status;
+    cudaEvent_t spec_done = nullptr, spec_ready = nullptr;
+    bool spec_live = false;
+    double spec_h = 0.0;
+    int spec_from = -1;
     // the encounter subsystem's step control, read back once per block of
     // attempts
     EncCtl* enc_host = nullptr;
@@ -227,6 +238,13 @@ struct Context {
         enc_ctl.release();
         enc_tstep.release();
         enc_bpre.release();
+        spec_big.release();
+        spec_tab.release();
+        spec_detail.release();
+        spec_events.release();
+        spec_event_step.release();
+        spec_status.release();
+        spec_live = false;
         hy_pairs.release();
         hy_ids.release();
         adj_off.release();

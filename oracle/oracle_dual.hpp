@@ -2,12 +2,14 @@
 // templated routines. Running mdt_mvs over Dual<N> propagates N tangent
 // directions through exactly the statements the oracle restates (the
 // variational equations of the kick and the Kepler drift as the code computes
-// them, iterations included); with massless test particles every particle can
-// share the same N seeds, since none of them acts on another body.
+// them; the universal-variable solve takes its root's tangent, kepu_tangent
+// below); with massless test particles every particle can share the same N
+// seeds, since none of them acts on another body.
 #pragma once
 #include <cmath>
 
 #include "oracle_scalar.hpp"
+#include "oracle_mvs.hpp"
 
 namespace oracle {
 
@@ -93,5 +95,28 @@ template <int N> inline Dual<N> Sign(const Dual<N>& a, const Dual<N>& b) {
 }
 template <int N> inline Dual<N> Max(const Dual<N>& a, const Dual<N>& b) { return a.v > b.v ? a : b; }
 template <int N> inline Dual<N> Min(const Dual<N>& a, const Dual<N>& b) { return a.v < b.v ? a : b; }
+
+// kepu_tangent for dual numbers (see oracle_mvs.hpp): at the anomaly sk the
+// solver stopped at, the tangent of sk becomes that of the root,
+// d sk - dF / F_s with F the universal Kepler residual and F_s = fp, and the
+// Stumpff terms and fp are evaluated again with it (same values).
+template <int N>
+inline void kepu_tangent(Dual<N>& sk, const Dual<N>& dt, const Dual<N>& r0, const Dual<N>& mu, const Dual<N>& alpha,
+                         const Dual<N>& u, Dual<N>& fp, Dual<N>& c1, Dual<N>& c2, Dual<N>& c3) {
+    auto terms = [&](Dual<N>& c0) {
+        const Dual<N> s2 = sk * sk;
+        Dual<N> x = s2 * alpha;
+        drift_kepu_stumpff(x, c0, c1, c2, c3);
+        c1 = c1 * sk;
+        c2 = c2 * s2;
+        c3 = c3 * sk * s2;
+        fp = r0 * c0 + u * c1 + mu * c2;
+    };
+    Dual<N> c0;
+    terms(c0);
+    const Dual<N> f = r0 * c1 + u * c2 + mu * c3 - dt;
+    for (int k = 0; k < N; ++k) sk.d[k] = sk.d[k] - f.d[k] / fp.v;
+    terms(c0);
+}
 
 }  // namespace oracle

@@ -129,10 +129,25 @@ template <class R> void drift_kepu_guess(R dt, R r0, R mu, R alpha, R u, R& s) {
     }
 }
 
+// The tangent of the universal-variable solve. Both solvers below stop once
+// the residual at the current anomaly s_k is below DANBYB and return the
+// Stumpff terms at s_k. Their values are converged, but the derivative that
+// flows through the iterations is that of the iterate before the last one
+// and can be far from the root's own derivative when the iteration started
+// from a poor guess: a perturbation of 1e-10 already changes the number of
+// iterations, and finite differences of the map see the root's derivative
+// ds/dtheta = -F_theta / F_s. kepu_tangent replaces the tangent of s_k by
+// that one (one Newton update of the tangent alone) and recomputes the
+// returned terms from it; the values stay what they were. A no-op for plain
+// and counting scalars; the dual-number overload is beside Dual.
+template <class R>
+inline void kepu_tangent(R&, const R&, const R&, const R&, const R&, const R&, R&, R&, R&, R&) {}
+
 // drift_kepu_new, mercury6_2.for:8073-8122: up to 7 quartic Newton iterations.
 template <class R>
 void drift_kepu_new(R& s, R dt, R r0, R mu, R alpha, R u, R& fp, R& c1, R& c2, R& c3, int& iflgn) {
     for (int nc = 0; nc <= 6; ++nc) {
+        R sk = s;
         R s2 = s * s;
         R x = s2 * alpha, c0;
         drift_kepu_stumpff(x, c0, c1, c2, c3);
@@ -150,6 +165,7 @@ void drift_kepu_new(R& s, R dt, R r0, R mu, R alpha, R u, R& fp, R& c1, R& c2, R
         R fdt = f / dt;
         if (fdt * fdt < R(DANBYB) * R(DANBYB)) {
             iflgn = 0;
+            kepu_tangent(sk, dt, r0, mu, alpha, u, fp, c1, c2, c3);
             return;
         }
     }
@@ -162,6 +178,7 @@ void drift_kepu_lag(R& s, R dt, R r0, R mu, R alpha, R u, R& fp, R& c1, R& c2, R
     const int ncmax = 400;
     const R ln = 5.0;
     for (int nc = 0; nc <= ncmax; ++nc) {
+        R sk = s;
         R x = s * s * alpha, c0;
         drift_kepu_stumpff(x, c0, c1, c2, c3);
         c1 = c1 * s;
@@ -177,6 +194,7 @@ void drift_kepu_lag(R& s, R dt, R r0, R mu, R alpha, R u, R& fp, R& c1, R& c2, R
         R fdt = f / dt;
         if (fdt * fdt < R(DANBYB) * R(DANBYB)) {
             iflg = 0;
+            kepu_tangent(sk, dt, r0, mu, alpha, u, fp, c1, c2, c3);
             return;
         }
     }
