@@ -595,6 +595,11 @@ BsArgs bs_attempt_args(double h) {
     a.adj = c.adj.p;
     a.perm = c.permp();
     a.active_np = c.bs_active_np >= 0 ? std::min(c.bs_active_np, c.np) : c.np;
+    if (V == 2 && !a.hkce && c.np > 0) {
+        // mdt_bs2 with mfo_all: the particles' levels 9..12 only when needed
+        c.bs_ptab.reserve((size_t)8 * 6 * c.npcap);
+        a.ptab = c.bs_ptab.p;
+    }
     return a;
 }
 
@@ -613,8 +618,9 @@ BsArgs launch_bs_attempt(double h) {
 // maxima errs and faults lv of an attempt: the first level n > 3 whose global
 // error is <= tol^2, or 0 when the step is to be halved and redone. Adds the
 // force calls of the levels it looked at to *forces.
-int bs_accept_level(const unsigned long long* errs, const DeviceStatus* lv, int V, double tol, int64_t* forces) {
-    const int L = bs_levels(V);
+int bs_accept_level(const unsigned long long* errs, const DeviceStatus* lv, int V, double tol, int64_t* forces,
+                    int first = 1, int last = 0) {
+    const int L = last > 0 ? last : bs_levels(V);
     const double tol2 = tol * tol;
     const char* nonfinite = V == 1 ? "Nonfinite BS extrapolation; inspect input or close encounters"
                                    : "Nonfinite BS2 force or extrapolation";
@@ -627,7 +633,7 @@ int bs_accept_level(const unsigned long long* errs, const DeviceStatus* lv, int 
     }
     reduce_step_maxima(red, 26);
     if (red[13] > 0.0) throw std::runtime_error("BS force failed");
-    for (int n = 1; n <= L; ++n) {
+    for (int n = first; n <= L; ++n) {
         *forces += bs_level_forces(V, n);
         if (red[13 + n] > 0.0) throw std::runtime_error("BS force failed");
         if (n <= 3) continue;
@@ -685,10 +691,26 @@ void bs_step_once(double time, double* h, double* hdid, double tol, int64_t* rej
         const BsArgs a = launch_bs_attempt(*h);
         unsigned long long errs[13];
         DeviceStatus lv[13];
-        check(cudaMemcpyAsync(errs, c.bs_errs.p, sizeof(errs), cudaMemcpyDeviceToHost, c.stream), "status");
-        check(cudaMemcpyAsync(lv, c.bs_lvst.p, sizeof(lv), cudaMemcpyDeviceToHost, c.stream), "status");
-        check(cudaStreamSynchronize(c.stream), "step");
-        const int accepted = bs_accept_level(errs, lv, a.variant, tol, &forces);
+        auto read_levels = [&] {
+            check(cudaMemcpyAsync(errs, c.bs_errs.p, sizeof(errs), cudaMemcpyDeviceToHost, c.stream), "status");
+            check(cudaMemcpyAsync(lv, c.bs_lvst.p, sizeof(lv), cudaMemcpyDeviceToHost, c.stream), "status");
+            check(cudaStreamSynchronize(c.stream), "step");
+        };
+        read_levels();
+        int accepted = 0;
+        if (a.ptab) {
+            // levels 1..8 first; 9..12 of the particles only when none passed
+            accepted = bs_accept_level(errs, lv, a.variant, tol, &forces, 1, 8);
+            if (!accepted) {
+                launch_bs_particles_late(a, c.stream);
+                c.dropin_launches += 1;
+                check(cudaGetLastError(), "launch");
+                read_levels();
+                accepted = bs_accept_level(errs, lv, a.variant, tol, &forces, 9, bs_levels(a.variant));
+            }
+        } else {
+            accepted = bs_accept_level(errs, lv, a.variant, tol, &forces);
+        }
         if (!accepted) {
             ++*rejected;
             *h = *h * 0.5;

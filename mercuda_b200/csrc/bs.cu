@@ -445,11 +445,21 @@ template <int VARIANT> __global__ void __launch_bounds__(256) bs_massive_extrap_
 // as a level loop would run them.
 // With mfo_hkce (encounter members: a few pairs each) three CTAs share an SM,
 // so that a subsystem of up to 444 x 32 members runs in one wave.
-template <int VARIANT, bool HKCE>
-__global__ void __launch_bounds__(bs_levels(VARIANT) * 16, HKCE ? 3 : 1) bs_particle_kernel(BsArgs A) {
+//
+// Levels LO..HI only (LO > 1 or HI < L): the plain mdt_bs2 step runs levels
+// 1..8 first and 9..12 only when none of 4..8 passed (its step control aims
+// at level 7), so that most steps make 36 of the 78 force calls. The first
+// stage keeps each particle's Neville tableau after level HI in A.ptab and
+// the second resumes from it; the statements and their order per particle
+// and component are those of one pass over all levels.
+// Registers are held to ~170 (the full sequence's 192 threads twice per SM).
+template <int VARIANT, bool HKCE, int LO = 1, int HI = bs_levels(VARIANT)>
+__global__ void __launch_bounds__((HI - LO + 1) * 16, HKCE ? 3 : 384 / ((HI - LO + 1) * 16))
+    bs_particle_kernel(BsArgs A) {
     constexpr int L = bs_levels(VARIANT);
-    constexpr int NW = L * 16 / 32;   // warps of the CTA
-    __shared__ double dsm[L][6][32];
+    constexpr int NW = (HI - LO + 1) / 2;   // warps of the CTA: levels LO + w and HI - w
+    static_assert((HI - LO + 1) % 2 == 0, "levels come in pairs");
+    __shared__ double dsm[HI][6][32];
     __shared__ double a0sm[3][32];
     __shared__ double co[L * (L - 1) / 2][2];
     // encounter members: their first pairs, and (A.stage_bodies) the Big
@@ -528,7 +538,7 @@ __global__ void __launch_bounds__(bs_levels(VARIANT) * 16, HKCE ? 3 : 1) bs_part
     const double3 a0 = ok ? make_double3(a0sm[0][lane], a0sm[1][lane], a0sm[2][lane]) : make_double3(0.0, 0.0, 0.0);
 #pragma unroll 1
     for (int half = 0; half < 2 && ok; ++half) {
-        const int n = half == 0 ? w + 1 : L - w;
+        const int n = half == 0 ? LO + w : HI - w;
         int row = 1;
         for (int m = 1; m < n; ++m) row += bs_level_forces(VARIANT, m);
         DeviceStatus* st = &A.lvst[n];
@@ -590,11 +600,14 @@ __global__ void __launch_bounds__(bs_levels(VARIANT) * 16, HKCE ? 3 : 1) bs_part
     // component D(1) + ... + D(n) goes out and D(1) stays in dsm for the error
     if (ok) {
         for (int c = w; c < 6; c += NW) {
-            double D[L];
+            double D[HI];
+            // levels before LO: their tableau as the first stage left it
 #pragma unroll
-            for (int n = 0; n < L; ++n) D[n] = dsm[n][c][lane];
+            for (int n = 0; n < LO - 1; ++n) D[n] = A.ptab[((size_t)n * 6 + c) * S + p];
 #pragma unroll
-            for (int n = 1; n <= L; ++n) {
+            for (int n = LO - 1; n < HI; ++n) D[n] = dsm[n][c][lane];
+#pragma unroll
+            for (int n = LO; n <= HI; ++n) {
 #pragma unroll
                 for (int j = n - 1; j >= 1; --j) {
                     const double* cj = co[coef_index(n, j)];
@@ -608,6 +621,10 @@ __global__ void __launch_bounds__(bs_levels(VARIANT) * 16, HKCE ? 3 : 1) bs_part
                     dsm[n - 1][c][lane] = D[0];
                 }
             }
+            if (HI < L) {
+#pragma unroll
+                for (int n = 0; n < HI; ++n) A.ptab[((size_t)n * 6 + c) * S + p] = D[n];
+            }
         }
     }
     __syncthreads();
@@ -619,7 +636,7 @@ __global__ void __launch_bounds__(bs_levels(VARIANT) * 16, HKCE ? 3 : 1) bs_part
         vscal = 1.0 / fmax(tmp2, 1e-300);
     }
     // each level's error maximum (mercury6_2.for:3372-3378), levels shared by the warps
-    for (int n = 4 + w; n <= L; n += NW) {
+    for (int n = (LO > 4 ? LO : 4) + w; n <= HI; n += NW) {
         double emax = 0.0;
         int bad = 0;
         if (ok) {
@@ -988,10 +1005,20 @@ template <int VARIANT, bool HKCE> void launch_variant(const BsArgs& a, cudaStrea
                                      (int)bytes);
         }
     }
+    if (VARIANT == 2 && !HKCE && a.ptab) {
+        // the plain mdt_bs2 step: levels 1..8 now, 9..12 on demand (launch_bs_particles_late)
+        bs_particle_kernel<2, false, 1, 8><<<pblocks, 8 * 16, 0, s>>>(b);
+        return;
+    }
     bs_particle_kernel<VARIANT, HKCE><<<pblocks, bs_levels(VARIANT) * 16, psmem, s>>>(b);
 }
 
 }  // namespace
+
+void launch_bs_particles_late(const BsArgs& a, cudaStream_t s) {
+    if (a.variant != 2 || a.hkce || !a.ptab || a.np <= 0) return;
+    bs_particle_kernel<2, false, 9, 12><<<(a.np + 31) / 32, 4 * 16, 0, s>>>(a);
+}
 
 void launch_bs_sequence(const BsArgs& a, cudaStream_t s) {
     if (a.variant == 1) launch_variant<1, false>(a, s);

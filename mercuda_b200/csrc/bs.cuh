@@ -70,6 +70,9 @@ struct BsArgs {
     double* bx_pre = nullptr;    // non-null: [6][nsplit] copy of the massive set's start state (level kernel)
     int fuse_extrap = 0;         // 1: the massive set's extrapolation runs as the particle launch's last CTA
     int stage_bodies = 0;        // set at launch: the particle kernel keeps the table's Big bodies in shared memory
+    double* ptab = nullptr;      // mdt_bs2 with mfo_all: [8][6][npcap] the particles' Neville tableau after
+                                 // level 8; non-null makes launch_bs_sequence run the particles' levels 1..8
+                                 // only (launch_bs_particles_late runs 9..12)
 };
 
 struct BsCommitArgs {
@@ -115,6 +118,9 @@ struct EncPostArgs {
 void launch_enc_post(const EncPostArgs& a, cudaStream_t s);
 
 void launch_bs_sequence(const BsArgs& a, cudaStream_t s);
+// Levels 9..12 of the particles after a launch_bs_sequence with a.ptab set,
+// adding to the same level maxima and candidates.
+void launch_bs_particles_late(const BsArgs& a, cudaStream_t s);
 void launch_bs_commit(const BsCommitArgs& a, cudaStream_t s);
 // Tangent of the accepted mdt_bs2 step (levels = accepted level) of the
 // encounter subsystem's massless members: tg [36][npcap], entry

@@ -94,7 +94,7 @@ struct Context {
     DBuf<int> ej_ids;                // mxx_ejec screen: count, then the ids found
     // Bulirsch-Stoer: massive-set scratch, per-level candidate states, per-level
     // error maxima and force-fault words
-    DBuf<double> bs_scr, bs_bcand, bs_pcand;
+    DBuf<double> bs_scr, bs_bcand, bs_pcand, bs_ptab;
     DBuf<unsigned long long> bs_errs;
     DBuf<DeviceStatus> bs_lvst;
     // HYBRID: rcrit of the massive set, the massive set after the first solar
@@ -223,7 +223,7 @@ struct Context {
         DBuf<double>* bufs[] = {&mbig, &rcebig, &rphysbig, &ngfbig, &bigstate[0], &bigstate[1], &pstate[0],
                                 &pstate[1], &pconst[0], &pconst[1], &tab, &detail, &transfer, &snapshot, &snap_const,
                                 &ra_bb, &ra_be, &ra_bg, &ra_bpx, &ra_pb, &ra_pe, &ftab, &force_out, &boxes, &corr_big, &corr_part, &energy_scr,
-                                &bs_scr, &bs_bcand, &bs_pcand, &rcritbig, &hy_scr, &hy_tab, &hy_off,
+                                &bs_scr, &bs_bcand, &bs_pcand, &bs_ptab, &rcritbig, &hy_scr, &hy_tab, &hy_off,
                                 &hy_packed, &tg, &stage};
         for (auto* b : bufs) b->release();
         order_scratch.release();
