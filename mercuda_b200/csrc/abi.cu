@@ -1084,12 +1084,15 @@ bool order_events_device(int nev, int nsteps, const std::vector<double>& tend, d
     while ((1ll << stepbits) < (long long)nsteps) ++stepbits;
     const int end_bit = 2 * idbits + stepbits;
     auto align = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    // scratch for a quarter more records than this run's, so that the next
+    // run of a similar system does not reallocate
+    const int room = nev + nev / 4 + 1024;
     size_t temp = 0;
     check(cub::DeviceRadixSort::SortPairs(nullptr, temp, (const unsigned long long*)nullptr,
-                                          (unsigned long long*)nullptr, (const int*)nullptr, (int*)nullptr, nev, 0,
-                                          end_bit, c.stream),
+                                          (unsigned long long*)nullptr, (const int*)nullptr, (int*)nullptr, room, 0,
+                                          64, c.stream),
           "events");
-    const size_t kb = align(sizeof(unsigned long long) * (size_t)nev), ib = align(sizeof(int) * (size_t)nev);
+    const size_t kb = align(sizeof(unsigned long long) * (size_t)room), ib = align(sizeof(int) * (size_t)room);
     const size_t tb = align(sizeof(double) * (size_t)nsteps);
     c.order_scratch.reserve(2 * kb + 2 * ib + tb + align(temp));
     char* base = c.order_scratch.p;
@@ -1099,8 +1102,10 @@ bool order_events_device(int nev, int nsteps, const std::vector<double>& tend, d
     int* iout = reinterpret_cast<int*>(base + 2 * kb + ib);
     double* dtend = reinterpret_cast<double*>(base + 2 * kb + 2 * ib);
     void* tmp = base + 2 * kb + 2 * ib + tb;
-    c.ev_sorted.reserve(nev);
-    c.ev_sorted_step.reserve(nev);
+    if ((int)c.ev_sorted.n < nev) {
+        c.ev_sorted.reserve(room);
+        c.ev_sorted_step.reserve(room);
+    }
     check(cudaMemcpyAsync(dtend, tend.data(), sizeof(double) * (size_t)nsteps, cudaMemcpyHostToDevice, c.stream),
           "events");
     event_key_kernel<<<blocks(nev), 256, 0, c.stream>>>(c.events.p, c.event_step.p, nev, idbits, kin, iin);

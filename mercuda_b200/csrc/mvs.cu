@@ -474,8 +474,11 @@ struct Cols {
     static constexpr int CEN = 21;     // 4: mce_cent start quantities
     static constexpr int NGF = 25;     // 10: five coefficients per particle
     static constexpr int count(bool ngf) { return ngf ? 35 : 25; }
+    // column stride: the kernel's largest CTA, so that a column offset is a
+    // constant (base already points at the thread's own entry)
+    static constexpr int STRIDE = 128;
     volatile double* base;
-    __device__ volatile double& at(int c) const { return base[c * blockDim.x + threadIdx.x]; }
+    __device__ volatile double& at(int c) const { return base[c * STRIDE]; }
     __device__ double3 ld3(int c) const { return make_double3(at(c), at(c + 1), at(c + 2)); }
     __device__ void st3(int c, double3 v) const { at(c) = v.x; at(c + 1) = v.y; at(c + 2) = v.z; }
 };
@@ -577,7 +580,7 @@ __global__ void __launch_bounds__(128, MB200_PARTICLE_MIN_BLOCKS) mvs_particle_k
     const int nb = A.nb, stride = tab_stride(nb);
     const int rows = A.nsteps + (A.reset ? 1 : 0);
     double* stab = smem;
-    const Cols cols{smem + (size_t)rows * stride};
+    const Cols cols{smem + (size_t)rows * stride + threadIdx.x};
     const double* gtab = A.tab + (A.reset ? 0 : stride);
     for (int k = threadIdx.x; k < rows * stride; k += blockDim.x) stab[k] = gtab[k];
     __syncthreads();
@@ -936,7 +939,7 @@ void launch_variant(const MvsParticleArgs& a, cudaStream_t s, int threads) {
 
 size_t mvs_particle_smem(int nb, int nsteps, int reset, int threads, bool ngf) {
     return sizeof(double) * ((size_t)tab_stride(nb) * (size_t)(nsteps + (reset ? 1 : 0)) +
-                             (size_t)threads * Cols::count(ngf));
+                             (size_t)Cols::STRIDE * Cols::count(ngf));
 }
 
 // Steps fused per launch: the staged tables are kept to ~18 KB so that, with

@@ -130,11 +130,11 @@ class ShardedRun:
         self.backend.upload(shard, ngflag)
 
     def _to_global(self, events: np.ndarray) -> np.ndarray:
-        # through the id map (a few records per step; no test of the map itself)
-        ev = events.copy()
+        """The records with global ids, in place (the array is the backend's
+        fresh copy)."""
         for f in ("i", "j"):
-            ev[f] = self.ids[ev[f] - 1] + 1
-        return ev
+            events[f] = self.ids[events[f] - 1] + 1
+        return events
 
     def advance(self, time: float, h: float, nsteps: int, rcen: float, steps_per_launch: int = 0):
         events, steps = self.backend.mvs_advance(time, h, nsteps, rcen, steps_per_launch)
