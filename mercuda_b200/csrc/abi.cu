@@ -110,6 +110,24 @@ struct CentralArgs {
     DeviceStatus* status;
 };
 
+// Drops the central-body records from the first status->events records (one
+// thread: a step's few hundred records, on the rare call whose radius or step
+// differs from the one the step screened with).
+__global__ void drop_central_kernel(MercuryEvent* ev, int* ev_step, int cap, DeviceStatus* st) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    const int n = min(st->events, cap);
+    int m = 0;
+    for (int k = 0; k < n; ++k) {
+        if (ev[k].kind == EV_CENTRAL) continue;
+        if (m != k) {
+            ev[m] = ev[k];
+            ev_step[m] = ev_step[k];
+        }
+        ++m;
+    }
+    st->events = m;
+}
+
 __global__ void central_kernel(CentralArgs A) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     const int nb = A.nbig - 1, total = nb + A.np;
@@ -357,7 +375,7 @@ void spec_drop() {
     check(cudaEventSynchronize(c.spec_done), "step");
 }
 
-void spec_launch(double h) {
+void spec_launch(double h, double rcen) {
     Context& c = ctx();
     const int nb = c.nbig - 1;
     c.spec_big.reserve((size_t)9 * c.nsplit);
@@ -373,7 +391,7 @@ void spec_launch(double h) {
     check(cudaEventRecord(c.spec_ready, c.stream), "event");
     check(cudaStreamWaitEvent(c.stream_big, c.spec_ready, 0), "wait");
     check(cudaMemsetAsync(c.spec_status.p, 0, sizeof(DeviceStatus), c.stream_big), "memset");
-    MvsBigArgs a = big_args(c.cur, 1 - c.cur, 1, 0, 0, 0, h, 0.0, c.spec_tab.p, c.spec_detail.p);
+    MvsBigArgs a = big_args(c.cur, 1 - c.cur, 1, 0, rcen > 0.0 ? 1 : 0, 0, h, rcen, c.spec_tab.p, c.spec_detail.p);
     a.out.x = c.spec_big.p;
     a.out.v = c.spec_big.p + 3 * c.nsplit;
     a.out.a = c.spec_big.p + 6 * c.nsplit;
@@ -387,14 +405,15 @@ void spec_launch(double h) {
     c.dropin_launches += 1;
     c.spec_live = true;
     c.spec_h = h;
+    c.spec_rcen = rcen;
     c.spec_from = c.cur;
 }
 
 // The speculative Big-body step as this step's, when it was made for it.
-bool spec_take(double h) {
+bool spec_take(double h, double rcen) {
     Context& c = ctx();
     if (!c.spec_live) return false;
-    if (c.spec_h != h || c.spec_from != c.cur || c.reset) {
+    if (c.spec_h != h || c.spec_rcen != rcen || c.spec_from != c.cur || c.reset) {
         spec_drop();
         return false;
     }
@@ -410,7 +429,11 @@ bool spec_take(double h) {
 
 // One MVS step (mdt_mvs) of the whole system: Big-body CTA then the particle
 // kernel, double-buffered so the pre-step state stays available. Pair events
-// are left in the event buffer with tmin in their time field.
+// are left in the event buffer with tmin in their time field. Once an events
+// call has named the central body's radius, the step screens for central
+// impacts in the same kernels (mce_cent with that radius, as the fused run
+// does) and the next events call with the same radius and h only reads the
+// records back.
 void mvs_step_once(double h) {
     Context& c = ctx();
     if (c.steps_since_order >= 32) {
@@ -429,16 +452,18 @@ void mvs_step_once(double h) {
         check(cudaMemsetAsync(c.status.p, 0, sizeof(DeviceStatus), c.stream), "memset");
         const int in = c.cur, out = 1 - c.cur;
         const int reset = c.reset ? 1 : 0;
-        const bool ahead = attempt == 0 && spec_take(h);
+        const double rc = c.dropin_rcen;
+        const int cen = rc > 0.0 ? 1 : 0;
+        const bool ahead = attempt == 0 && spec_take(h, rc);
         const double* tab = ahead ? c.spec_tab.p : c.tab.p;
         const double* det = ahead ? c.spec_detail.p : c.detail.p;
         if (!ahead) {
             spec_drop();
-            launch_mvs_big(big_args(in, out, 1, reset, 0, 0, h, 0.0, c.tab.p, c.detail.p), c.stream);
+            launch_mvs_big(big_args(in, out, 1, reset, cen, 0, h, rc, c.tab.p, c.detail.p), c.stream);
             c.dropin_launches += 1;
         }
         c.dropin_launches += c.np > 0 ? 1 + (c.nbig > 1 ? 1 : 0) : 0;
-        if (c.np > 0) particles_and_events(particle_args(in, out, 1, reset, 0, 0, h, 0.0, tab, det), det, c.stream);
+        if (c.np > 0) particles_and_events(particle_args(in, out, 1, reset, cen, 0, h, rc, tab, det), det, c.stream);
         check(cudaGetLastError(), "launch");
         read_status();
         if (c.status_host->fault) throw std::runtime_error("MVS force failed");
@@ -449,10 +474,13 @@ void mvs_step_once(double h) {
         }
         c.nforces += 1 + reset;
         c.pair_events = c.status_host->events;
+        c.step_central = cen != 0;
+        c.step_rcen = rc;
+        c.step_h = h;
         c.cur = out;
         c.reset = false;
         c.stepped = true;
-        if (c.steps_since_order < 32) spec_launch(h);
+        if (c.steps_since_order < 32) spec_launch(h, rc);
         return;
     }
 }
@@ -1642,6 +1670,7 @@ int mercury_cuda_upload(int n, int nbig, int pn, int ngflag, const double* m, co
         c.m_host.assign(m, m + n);
         c.event_rate = 0.0;
         c.ev_device = 0;
+        c.step_central = false;
         c.mbig.reserve(ns);
         c.rcebig.reserve(ns);
         c.rphysbig.reserve(ns);
@@ -1763,6 +1792,24 @@ int mercury_cuda_events(double time, double h, double rcen, const MercuryEvent**
         const int prev = 1 - c.cur;
         if (!is_mvs(c.algorithm) && c.algorithm != 10 && c.stepped) screen_pairs(h);
         const bool dh = c.algorithm == 10 && c.stepped;
+        // an MVS step that screened for central impacts itself (mvs_step_once)
+        bool central_done = false;
+        if (c.stepped && c.step_central) {
+            if (rcen == c.step_rcen && h == c.step_h) {
+                central_done = true;
+            } else {
+                *c.status_host = DeviceStatus{0, c.pair_events, 0, 0};
+                check(cudaMemcpyAsync(c.status.p, c.status_host, sizeof(DeviceStatus), cudaMemcpyHostToDevice,
+                                      c.stream),
+                      "status");
+                drop_central_kernel<<<1, 1, 0, c.stream>>>(c.events.p, c.event_step.p, (int)c.events.n, c.status.p);
+                c.dropin_launches += 1;
+                read_status();
+                c.pair_events = c.status_host->events;
+                c.step_central = false;
+            }
+        }
+        c.dropin_rcen = rcen;
         if (dh) {
             // heliocentric velocities of both states (mco_dh2h)
             c.hy_off.reserve(6);
@@ -1778,7 +1825,7 @@ int mercury_cuda_events(double time, double h, double rcen, const MercuryEvent**
             check(cudaMemcpyAsync(c.status.p, c.status_host, sizeof(DeviceStatus), cudaMemcpyHostToDevice, c.stream),
                   "status");
             const int total = c.nsplit - 1 + c.np;
-            if (c.stepped && total > 0) {
+            if (c.stepped && total > 0 && !central_done) {
                 CentralArgs a{};
                 a.nbig = c.nsplit;
                 a.np = c.np;
@@ -1976,8 +2023,15 @@ int mercury_cuda_hybrid_begin(double h, const double* crit, int flag, int cap, i
                 ce[pairs[k].x] = 2;
                 ce[pairs[k].y] = 2;
             }
-            for (int j = 1; j < c.n; ++j)
-                if (ce[j]) c.hy_members.push_back(j);
+            // the members in ascending order: the pairs' bodies (not a scan of ce)
+            c.hy_members.reserve((size_t)2 * npairs);
+            for (int k = 0; k < npairs; ++k) {
+                c.hy_members.push_back(pairs[k].x);
+                c.hy_members.push_back(pairs[k].y);
+            }
+            std::sort(c.hy_members.begin(), c.hy_members.end());
+            c.hy_members.erase(std::unique(c.hy_members.begin(), c.hy_members.end()), c.hy_members.end());
+            if (!c.hy_members.empty() && c.hy_members.front() == 0) c.hy_members.erase(c.hy_members.begin());
             const int nm = (int)c.hy_members.size();
             c.hy_ids.reserve(nm);
             c.hy_packed.reserve((size_t)6 * nm);

@@ -167,6 +167,10 @@ struct Context {
     // the per-step MVS path's speculative next Big-body step: its output
     // state, force table, pair details, records and status, and whether one is
     // in flight for (spec_h, from buffer spec_from)
+    // the central body's radius of the last drop-in events call (0: none yet),
+    // and whether the last step screened for central impacts with it (for h)
+    double dropin_rcen = 0.0, step_rcen = 0.0, step_h = 0.0, spec_rcen = 0.0;
+    bool step_central = false;
     DBuf<double> spec_big, spec_tab, spec_detail;
     DBuf<MercuryEvent> spec_events;
     DBuf<int> spec_event_step;
@@ -245,6 +249,8 @@ struct Context {
         spec_event_step.release();
         spec_status.release();
         spec_live = false;
+        dropin_rcen = 0.0;
+        step_central = false;
         hy_pairs.release();
         hy_ids.release();
         adj_off.release();
