@@ -305,26 +305,27 @@ MvsParticleArgs particle_args(int in, int out, int nsteps, int reset, int centra
 }
 
 // Particle kernel of one launch followed by the classification of its
-// encounter candidates into event records (same stream). detail is the base
-// of the run's pair details: a candidate carries its step within the run.
+// encounter candidates into event records (same stream, the records, status
+// and candidates pa names). detail is the base of the run's pair details: a
+// candidate carries its step within the run.
 void particles_and_events(const MvsParticleArgs& pa, const double* detail, cudaStream_t s) {
     Context& c = ctx();
-    check(cudaMemsetAsync(&c.status.p->next_tile, 0, sizeof(int), s), "memset");
+    check(cudaMemsetAsync(&pa.status->next_tile, 0, sizeof(int), s), "memset");
     launch_mvs_particles(pa, s, c.particle_threads);
     ClassifyArgs ca{};
     ca.nb = c.nbig - 1;
     ca.nbig = c.nbig;
     ca.h = pa.h;
     ca.detail = detail;
-    ca.cands = c.cands.p;
-    ca.cand_cap = (int)c.cands.n;
-    ca.events = c.events.p;
-    ca.event_step = c.event_step.p;
-    ca.event_cap = (int)c.events.n;
-    ca.status = c.status.p;
+    ca.cands = pa.cands;
+    ca.cand_cap = pa.cand_cap;
+    ca.events = pa.events;
+    ca.event_step = pa.event_step;
+    ca.event_cap = pa.event_cap;
+    ca.status = pa.status;
     ca.step_base = 0;
     if (ca.nb > 0) launch_classify(ca, s);
-    check(cudaMemsetAsync(&c.status.p->cands, 0, sizeof(int), s), "memset");
+    check(cudaMemsetAsync(&pa.status->cands, 0, sizeof(int), s), "memset");
 }
 
 // Grows the event or candidate buffer after an overflow flagged in the status.
@@ -342,18 +343,34 @@ void grow_after_overflow() {
 }
 
 // The per-step MVS path (one mercury_cuda_step per step, as mal_hcon calls
-// it) runs the next step's Big bodies ahead: the Big bodies never feel the
-// particles, so as soon as a step is committed their next step with the same
-// h runs on the second stream into spare buffers (state, force table, pair
-// records, status) while the host works. The next mercury_cuda_step with the
-// same h and no reset takes it (the spare state becomes the step's output,
-// its records and faults are merged into the step's status on the device);
-// any other call that may change the system first orders the library stream
-// after it and drops it.
-constexpr int SPEC_RECORDS = 1024;   // Big-pair records a speculative step may hold
+// it) runs the next step ahead: as soon as a step is committed, the next step
+// with the same h (Big bodies, particles, their pair records and status) runs
+// on the second stream into spare buffers while the host handles this step's
+// events, and its status and first records are read back into pinned memory
+// on that stream. The next mercury_cuda_step with the same h, the same
+// central radius and no reset takes it: the spare states become the step's
+// output (the pre-step state stays in place for download(previous)) and the
+// records and status are already on the host. A speculative step that
+// faulted or overflowed a buffer is dropped and the step is made again on the
+// library stream, which reports or grows as usual.
+//
+// The Big bodies never feel the particles, so the Big-body step after the
+// speculative one runs on a third stream beside the speculative particles
+// (in the CTA slot the particle grid leaves free), and the next speculative
+// step starts from its output: the particles' step is then the only kernel
+// on the critical path of a step.
+//
+// Every call that may change the system or the buffers the speculative steps
+// read first drops them (and waits for them); the calls that run beside them
+// (events, download, export, energy) touch none of their outputs. The
+// candidate buffer is shared: only steps and runs use it, and they drop the
+// speculation first.
+constexpr int AHEAD_RECORDS = 1024;   // records a Big-body step run ahead may hold
 
-__global__ void spec_merge_kernel(const DeviceStatus* ss, const MercuryEvent* sev, int scap, DeviceStatus* st,
-                                  MercuryEvent* ev, int* ev_step, int cap) {
+// Copies the records of a Big-body step run ahead to the head of a step's
+// record buffer and starts that step's status from its count and faults.
+__global__ void spec_merge_kernel(const DeviceStatus* ss, const MercuryEvent* sev, const int* sstep, int scap,
+                                  DeviceStatus* st, MercuryEvent* ev, int* ev_step, int cap) {
     const int n = ss->events;
     if (threadIdx.x == 0 && blockIdx.x == 0) {
         st->events = n;
@@ -363,67 +380,163 @@ __global__ void spec_merge_kernel(const DeviceStatus* ss, const MercuryEvent* se
     const int m = min(n, min(scap, cap));
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) {
         store_event(ev + k, sev[k]);
-        ev_step[k] = 0;
+        ev_step[k] = sstep[k];
     }
+}
+
+// Waits for the speculative step (host-side: later calls may copy into its
+// inputs synchronously); the Big-body step ahead keeps running.
+void spec_wait() {
+    Context& c = ctx();
+    if (!c.spec_live) return;
+    c.spec_live = false;
+    check(cudaEventSynchronize(c.spec_done), "step");
 }
 
 void spec_drop() {
     Context& c = ctx();
-    if (!c.spec_live) return;
-    // also host-side: later calls may copy into its inputs synchronously
-    c.spec_live = false;
-    check(cudaEventSynchronize(c.spec_done), "step");
+    spec_wait();
+    if (!c.ah_live) return;
+    c.ah_live = false;
+    check(cudaEventSynchronize(c.ah_done), "step");
+}
+
+// An entry point that may change the system or read it in a way a step
+// ahead does not expect: no step ahead, no records waiting on the host.
+void drop_speculation() {
+    spec_drop();
+    ctx().head_ready = false;
+}
+
+// Resizes b to exactly n elements (a swapped-in record buffer keeps the
+// library's event capacity).
+template <class T> void reserve_exact(DBuf<T>& b, size_t n) {
+    if (b.n != n) b.release();
+    b.reserve(n);
+}
+
+BigState big_state_at(double* p, int nsplit) {
+    BigState b;
+    b.x = p;
+    b.v = p + 3 * (size_t)nsplit;
+    b.a = p + 6 * (size_t)nsplit;
+    return b;
 }
 
 void spec_launch(double h, double rcen) {
     Context& c = ctx();
     const int nb = c.nbig - 1;
-    c.spec_big.reserve((size_t)9 * c.nsplit);
-    c.spec_tab.reserve((size_t)2 * tab_stride(nb));
-    c.spec_detail.reserve((size_t)std::max(1, nb) * TAB_DETAIL);
-    c.spec_events.reserve(SPEC_RECORDS);
-    c.spec_event_step.reserve(SPEC_RECORDS);
+    const int cen = rcen > 0.0 ? 1 : 0;
+    const size_t big_el = (size_t)9 * c.nsplit, tab_el = (size_t)2 * tab_stride(nb);
+    const size_t det_el = (size_t)std::max(1, nb) * TAB_DETAIL;
+    c.spec_big.reserve(big_el);
+    c.spec_part.reserve((size_t)9 * c.npcap);
+    c.spec_tab.reserve(tab_el);
+    c.spec_detail.reserve(det_el);
+    reserve_exact(c.spec_events, c.events.n);
+    reserve_exact(c.spec_event_step, c.events.n);
     c.spec_status.reserve(1);
+    c.ah_state.reserve(big_el);
+    c.ah_tab.reserve(tab_el);
+    c.ah_detail.reserve(det_el);
+    c.ah_events.reserve(AHEAD_RECORDS);
+    c.ah_event_step.reserve(AHEAD_RECORDS);
+    c.ah_status.reserve(1);
     if (!c.spec_done) {
-        check(cudaEventCreateWithFlags(&c.spec_done, cudaEventDisableTiming), "event");
-        check(cudaEventCreateWithFlags(&c.spec_ready, cudaEventDisableTiming), "event");
+        for (cudaEvent_t* e : {&c.spec_done, &c.spec_ready, &c.ah_done, &c.spec_merged})
+            check(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "event");
     }
+    cudaStream_t s = c.stream_big, sa = c.stream_ahead;
     check(cudaEventRecord(c.spec_ready, c.stream), "event");
-    check(cudaStreamWaitEvent(c.stream_big, c.spec_ready, 0), "wait");
-    check(cudaMemsetAsync(c.spec_status.p, 0, sizeof(DeviceStatus), c.stream_big), "memset");
-    MvsBigArgs a = big_args(c.cur, 1 - c.cur, 1, 0, rcen > 0.0 ? 1 : 0, 0, h, rcen, c.spec_tab.p, c.spec_detail.p);
-    a.out.x = c.spec_big.p;
-    a.out.v = c.spec_big.p + 3 * c.nsplit;
-    a.out.a = c.spec_big.p + 6 * c.nsplit;
-    a.events = c.spec_events.p;
-    a.event_step = c.spec_event_step.p;
-    a.event_cap = SPEC_RECORDS;
-    a.status = c.spec_status.p;
-    launch_mvs_big(a, c.stream_big);
-    check(cudaGetLastError(), "launch");
-    check(cudaEventRecord(c.spec_done, c.stream_big), "event");
+    check(cudaStreamWaitEvent(s, c.spec_ready, 0), "wait");
+    const int cap = (int)c.spec_events.n;
+    check(cudaMemsetAsync(c.spec_status.p, 0, sizeof(DeviceStatus), s), "memset");
+    if (c.ah_live && c.ah_h == h && c.ah_rcen == rcen) {
+        // this step's Big bodies ran ahead: their state, table rows and
+        // details become the step's, their records its first records
+        check(cudaStreamWaitEvent(s, c.ah_done, 0), "wait");
+        std::swap(c.spec_big, c.ah_state);
+        std::swap(c.spec_tab, c.ah_tab);
+        std::swap(c.spec_detail, c.ah_detail);
+        spec_merge_kernel<<<4, 256, 0, s>>>(c.ah_status.p, c.ah_events.p, c.ah_event_step.p, AHEAD_RECORDS,
+                                            c.spec_status.p, c.spec_events.p, c.spec_event_step.p, cap);
+    } else {
+        spec_drop();
+        MvsBigArgs a = big_args(c.cur, 1 - c.cur, 1, 0, cen, 0, h, rcen, c.spec_tab.p, c.spec_detail.p);
+        a.out = big_state_at(c.spec_big.p, c.nsplit);
+        a.events = c.spec_events.p;
+        a.event_step = c.spec_event_step.p;
+        a.event_cap = cap;
+        a.status = c.spec_status.p;
+        launch_mvs_big(a, s);
+    }
+    c.ah_live = false;
     c.dropin_launches += 1;
+    // the next Big-body step, from this one's state, once the buffers it
+    // writes are read
+    check(cudaEventRecord(c.spec_merged, s), "event");
+    check(cudaStreamWaitEvent(sa, c.spec_merged, 0), "wait");
+    check(cudaMemsetAsync(c.ah_status.p, 0, sizeof(DeviceStatus), sa), "memset");
+    MvsBigArgs b = big_args(c.cur, 1 - c.cur, 1, 0, cen, 0, h, rcen, c.ah_tab.p, c.ah_detail.p);
+    b.in = big_state_at(c.spec_big.p, c.nsplit);
+    b.out = big_state_at(c.ah_state.p, c.nsplit);
+    b.events = c.ah_events.p;
+    b.event_step = c.ah_event_step.p;
+    b.event_cap = AHEAD_RECORDS;
+    b.status = c.ah_status.p;
+    launch_mvs_big(b, sa);
+    check(cudaEventRecord(c.ah_done, sa), "event");
+    c.dropin_launches += 1;
+    c.ah_live = true;
+    c.ah_h = h;
+    c.ah_rcen = rcen;
+    if (c.np > 0) {
+        MvsParticleArgs pa = particle_args(c.cur, 1 - c.cur, 1, 0, cen, 0, h, rcen, c.spec_tab.p, c.spec_detail.p);
+        pa.xout = c.spec_part.p;
+        pa.events = c.spec_events.p;
+        pa.event_step = c.spec_event_step.p;
+        pa.event_cap = cap;
+        pa.status = c.spec_status.p;
+        particles_and_events(pa, c.spec_detail.p, s);
+        c.dropin_launches += 1 + (nb > 0 ? 1 : 0);
+    }
+    check(cudaMemcpyAsync(c.spec_status_host, c.spec_status.p, sizeof(DeviceStatus), cudaMemcpyDeviceToHost, s),
+          "status");
+    const int head = std::min(Context::EVENT_HEAD, cap);
+    if (head > 0)
+        check(cudaMemcpyAsync(c.spec_head, c.spec_events.p, sizeof(MercuryEvent) * head, cudaMemcpyDeviceToHost, s),
+              "events");
+    check(cudaGetLastError(), "launch");
+    check(cudaEventRecord(c.spec_done, s), "event");
     c.spec_live = true;
     c.spec_h = h;
     c.spec_rcen = rcen;
     c.spec_from = c.cur;
 }
 
-// The speculative Big-body step as this step's, when it was made for it.
+// The speculative step as this step, when it was made for it and ended
+// without a fault or an overflow. The Big-body step run ahead of it stays.
 bool spec_take(double h, double rcen) {
     Context& c = ctx();
     if (!c.spec_live) return false;
-    if (c.spec_h != h || c.spec_rcen != rcen || c.spec_from != c.cur || c.reset) {
+    const bool match = c.spec_h == h && c.spec_rcen == rcen && c.spec_from == c.cur && !c.reset;
+    spec_wait();
+    const DeviceStatus st = *c.spec_status_host;
+    if (!match || st.fault || st.overflow) {
         spec_drop();
         return false;
     }
-    check(cudaStreamWaitEvent(c.stream, c.spec_done, 0), "wait");
-    c.spec_live = false;
-    std::swap(c.bigstate[1 - c.cur], c.spec_big);
-    spec_merge_kernel<<<4, 256, 0, c.stream>>>(c.spec_status.p, c.spec_events.p, SPEC_RECORDS, c.status.p,
-                                               c.events.p, c.event_step.p, (int)c.events.n);
-    check(cudaGetLastError(), "launch");
-    c.dropin_launches += 1;
+    const int out = 1 - c.cur;
+    std::swap(c.bigstate[out], c.spec_big);
+    std::swap(c.pstate[out], c.spec_part);
+    std::swap(c.events, c.spec_events);
+    std::swap(c.event_step, c.spec_event_step);
+    std::swap(c.ev_head, c.spec_head);
+    *c.status_host = st;
+    check(cudaMemcpyAsync(c.status.p, c.spec_status.p, sizeof(DeviceStatus), cudaMemcpyDeviceToDevice, c.stream),
+          "status");
+    c.head_ready = true;
+    c.head_count = std::min(Context::EVENT_HEAD, (int)c.events.n);
     return true;
 }
 
@@ -447,42 +560,36 @@ void mvs_step_once(double h) {
                   "copy");
     }
     c.steps_since_order += 1;
-    for (int attempt = 0;; ++attempt) {
+    const double rc = c.dropin_rcen;
+    const int cen = rc > 0.0 ? 1 : 0;
+    const bool ahead = spec_take(h, rc);
+    for (int attempt = 0; !ahead; ++attempt) {
+        c.head_ready = false;
         ensure_tables(2, 1);
         check(cudaMemsetAsync(c.status.p, 0, sizeof(DeviceStatus), c.stream), "memset");
         const int in = c.cur, out = 1 - c.cur;
         const int reset = c.reset ? 1 : 0;
-        const double rc = c.dropin_rcen;
-        const int cen = rc > 0.0 ? 1 : 0;
-        const bool ahead = attempt == 0 && spec_take(h, rc);
-        const double* tab = ahead ? c.spec_tab.p : c.tab.p;
-        const double* det = ahead ? c.spec_detail.p : c.detail.p;
-        if (!ahead) {
-            spec_drop();
-            launch_mvs_big(big_args(in, out, 1, reset, cen, 0, h, rc, c.tab.p, c.detail.p), c.stream);
-            c.dropin_launches += 1;
-        }
-        c.dropin_launches += c.np > 0 ? 1 + (c.nbig > 1 ? 1 : 0) : 0;
-        if (c.np > 0) particles_and_events(particle_args(in, out, 1, reset, cen, 0, h, rc, tab, det), det, c.stream);
+        launch_mvs_big(big_args(in, out, 1, reset, cen, 0, h, rc, c.tab.p, c.detail.p), c.stream);
+        c.dropin_launches += 1 + (c.np > 0 ? 1 + (c.nbig > 1 ? 1 : 0) : 0);
+        if (c.np > 0)
+            particles_and_events(particle_args(in, out, 1, reset, cen, 0, h, rc, c.tab.p, c.detail.p), c.detail.p,
+                                 c.stream);
         check(cudaGetLastError(), "launch");
         read_status();
         if (c.status_host->fault) throw std::runtime_error("MVS force failed");
-        if (c.status_host->overflow) {
-            if (attempt > 8) throw std::runtime_error("event buffer growth failed");
-            grow_after_overflow();
-            continue;  // the input buffers are untouched: redo the step
-        }
-        c.nforces += 1 + reset;
-        c.pair_events = c.status_host->events;
-        c.step_central = cen != 0;
-        c.step_rcen = rc;
-        c.step_h = h;
-        c.cur = out;
-        c.reset = false;
-        c.stepped = true;
-        if (c.steps_since_order < 32) spec_launch(h, rc);
-        return;
+        if (!c.status_host->overflow) break;
+        if (attempt > 8) throw std::runtime_error("event buffer growth failed");
+        grow_after_overflow();   // the input buffers are untouched: redo the step
     }
+    c.nforces += 1 + (c.reset ? 1 : 0);
+    c.pair_events = c.status_host->events;
+    c.step_central = cen != 0;
+    c.step_rcen = rc;
+    c.step_h = h;
+    c.cur = 1 - c.cur;
+    c.reset = false;
+    c.stepped = true;
+    if (c.steps_since_order < 32) spec_launch(h, rc);
 }
 
 ForceCfg force_cfg() {
@@ -1568,7 +1675,7 @@ int mercury_cuda_available(void) {
 void mercury_cuda_free(void) {
     Context& c = ctx();
     try {
-        spec_drop();
+        drop_speculation();
     } catch (const std::exception& e) {
         report(e);
     }
@@ -1579,7 +1686,7 @@ int mercury_cuda_configure(int method) {
     if (method != 1 && method != 2 && method != 3 && method != 4 && method != 9 && method != 10) return 1;
     Context& c = ctx();
     try {
-        spec_drop();
+        drop_speculation();
         inject("configure");
         if (method != c.algorithm) mercury_cuda_free();
         c.algorithm = method;
@@ -1598,7 +1705,7 @@ int mercury_cuda_upload(int n, int nbig, int pn, int ngflag, const double* m, co
                         const double* ng, const double* jcen, const double* limits, const double* radii) {
     Context& c = ctx();
     try {
-        spec_drop();
+        drop_speculation();
         inject("upload");
         if (n < 1 || nbig < 1 || nbig > n) throw std::runtime_error("invalid body counts");
         if (is_mvs(c.algorithm) && nbig > 512) throw std::runtime_error("more than 512 Big bodies");
@@ -1818,7 +1925,15 @@ int mercury_cuda_events(double time, double h, double rcen, const MercuryEvent**
             c.dropin_launches += 2;
         }
         int head = 0;   // records read back with the status
-        for (int attempt = 0;; ++attempt) {
+        // a step taken from the step ahead brought its status and first
+        // records to the host already
+        const bool fast = central_done && c.head_ready && !dh;
+        c.head_ready = false;
+        if (fast) {
+            c.status_host->events = c.pair_events;
+            head = c.head_count;
+        }
+        for (int attempt = 0; !fast; ++attempt) {
             // restart the counter after the step's pair events (from pinned
             // memory: the copy does not block), then screen for central impacts
             *c.status_host = DeviceStatus{0, c.pair_events, 0, 0};
@@ -1903,7 +2018,7 @@ int mercury_cuda_events(double time, double h, double rcen, const MercuryEvent**
 int mercury_cuda_force(double* a) {
     Context& c = ctx();
     try {
-        spec_drop();
+        drop_speculation();
         inject("force");
         require_system();
         const int nb = c.nbig - 1, ns = c.nsplit;
@@ -1958,7 +2073,7 @@ int mercury_cuda_export(double h, int physical, double* xx, double* vv) {
 int mercury_cuda_limits(const double* limits) {
     Context& c = ctx();
     try {
-        spec_drop();
+        drop_speculation();
         inject("limits");
         require_system();
         check(cudaMemcpyAsync(c.transfer.p, limits, sizeof(double) * c.n, cudaMemcpyHostToDevice, c.stream), "limits");
@@ -1974,7 +2089,7 @@ int mercury_cuda_hybrid_begin(double h, const double* crit, int flag, int cap, i
                               double* xx, double* vv, int64_t* forces) {
     Context& c = ctx();
     try {
-        spec_drop();
+        drop_speculation();
         inject("hybrid_begin");
         require_system();
         if (c.algorithm != 10) throw std::runtime_error("hybrid_begin needs algorithm 10");
@@ -2063,7 +2178,7 @@ int mercury_cuda_hybrid_begin(double h, const double* crit, int flag, int cap, i
 int mercury_cuda_hybrid_finish(double h, const double* m, const double* xx, const double* vv, int64_t* forces) {
     Context& c = ctx();
     try {
-        spec_drop();
+        drop_speculation();
         inject("hybrid_finish");
         require_system();
         if (!c.hy_begun) throw std::runtime_error("hybrid_finish without hybrid_begin");
@@ -2117,7 +2232,7 @@ int mercury_cuda_encounter_enter(int n, int nb, const double* m, const double* x
                                  const double* crit, const double* limits, const double* radii, int np,
                                  const int* pi, const int* pj) {
     try {
-        spec_drop();
+        drop_speculation();
         inject("encounter_enter");
         if (g_active != 0) throw std::runtime_error("encounter subsystem already active");
         g_active = 1;
@@ -2200,7 +2315,7 @@ int mercury_b200_mvs_advance(double time, double h, int nsteps, double rcen, int
     (void)time;
     Context& c = ctx();
     try {
-        spec_drop();
+        drop_speculation();
         inject("advance");
         require_system();
         if (!is_mvs(c.algorithm)) throw std::runtime_error("MVS advance needs algorithm 1 or 9");
@@ -2508,7 +2623,7 @@ int mercury_b200_ejections(double h, int physical, double rmax, int i0, int* ids
 int mercury_b200_hybrid_members(const int* ids, int count) {
     Context& c = ctx();
     try {
-        spec_drop();
+        drop_speculation();
         require_system();
         if (!c.hy_begun) throw std::runtime_error("hybrid_members outside a HYBRID step");
         if (count < 0 || (count > 0 && !ids)) throw std::runtime_error("invalid member list");
@@ -2830,7 +2945,7 @@ int mercury_b200_epoch_order(int nsml, const double* epochs, double tstart, int*
 int mercury_b200_sync_epochs(const double* epoch, double* time, double h0, double tol, double dtout, int* steps) {
     Context& c = ctx();
     try {
-        spec_drop();
+        drop_speculation();
         require_system();
         if (c.algorithm != 2) throw std::runtime_error("epoch synchronisation needs algorithm 2 (mdt_bs1)");
         if (c.nsplit != c.nbig) throw std::runtime_error("epoch synchronisation needs massless Small bodies");

@@ -152,7 +152,7 @@ struct Context {
         pinned_n = bytes;
     }
     // streams and timers
-    cudaStream_t stream = nullptr, stream_big = nullptr;
+    cudaStream_t stream = nullptr, stream_big = nullptr, stream_ahead = nullptr;
     std::vector<cudaEvent_t> chunk_done;
     cudaEvent_t t0 = nullptr, t1 = nullptr;
     std::vector<cudaEvent_t> kt0, kt1;
@@ -164,21 +164,38 @@ struct Context {
     // timing events of the drop-in calls, and the kernels they launched
     cudaEvent_t d0 = nullptr, d1 = nullptr;
     int64_t dropin_launches = 0;
-    // the per-step MVS path's speculative next Big-body step: its output
-    // state, force table, pair details, records and status, and whether one is
-    // in flight for (spec_h, from buffer spec_from)
     // the central body's radius of the last drop-in events call (0: none yet),
     // and whether the last step screened for central impacts with it (for h)
     double dropin_rcen = 0.0, step_rcen = 0.0, step_h = 0.0, spec_rcen = 0.0;
     bool step_central = false;
-    DBuf<double> spec_big, spec_tab, spec_detail;
+    // the per-step MVS path's speculative next step: its Big-body and particle
+    // states, force table, pair details, records and status (on the device and
+    // read back into pinned memory with the first records), and whether one is
+    // in flight for (spec_h, from buffer spec_from)
+    DBuf<double> spec_big, spec_part, spec_tab, spec_detail;
     DBuf<MercuryEvent> spec_events;
     DBuf<int> spec_event_step;
     DBuf<DeviceStatus> spec_status;
+    DeviceStatus* spec_status_host = nullptr;
+    MercuryEvent* spec_head = nullptr;
     cudaEvent_t spec_done = nullptr, spec_ready = nullptr;
     bool spec_live = false;
     double spec_h = 0.0;
     int spec_from = -1;
+    // the Big-body step after the speculative one (same h and radius), run
+    // on a third stream beside the speculative step's particles: its state,
+    // table rows, details, records and status
+    DBuf<double> ah_state, ah_tab, ah_detail;
+    DBuf<MercuryEvent> ah_events;
+    DBuf<int> ah_event_step;
+    DBuf<DeviceStatus> ah_status;
+    cudaEvent_t ah_done = nullptr, spec_merged = nullptr;
+    bool ah_live = false;
+    double ah_h = 0.0, ah_rcen = 0.0;
+    // the last step's status and first records are in status_host / ev_head
+    // already (head_count records)
+    bool head_ready = false;
+    int head_count = 0;
     // the encounter subsystem's step control, read back once per block of
     // attempts
     EncCtl* enc_host = nullptr;
@@ -214,6 +231,7 @@ struct Context {
         if (!stream) {
             check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "stream");
             check(cudaStreamCreateWithFlags(&stream_big, cudaStreamNonBlocking), "stream");
+            check(cudaStreamCreateWithFlags(&stream_ahead, cudaStreamNonBlocking), "stream");
             check(cudaEventCreate(&t0), "event");
             check(cudaEventCreate(&t1), "event");
             check(cudaEventCreate(&d0), "event");
@@ -221,6 +239,8 @@ struct Context {
             check(cudaMallocHost(reinterpret_cast<void**>(&status_host), sizeof(DeviceStatus)), "pinned");
             check(cudaMallocHost(reinterpret_cast<void**>(&enc_host), sizeof(EncCtl)), "pinned");
             check(cudaMallocHost(reinterpret_cast<void**>(&ev_head), sizeof(MercuryEvent) * EVENT_HEAD), "pinned");
+            check(cudaMallocHost(reinterpret_cast<void**>(&spec_head), sizeof(MercuryEvent) * EVENT_HEAD), "pinned");
+            check(cudaMallocHost(reinterpret_cast<void**>(&spec_status_host), sizeof(DeviceStatus)), "pinned");
         }
     }
     void release_all() {
@@ -243,12 +263,21 @@ struct Context {
         enc_tstep.release();
         enc_bpre.release();
         spec_big.release();
+        spec_part.release();
         spec_tab.release();
         spec_detail.release();
         spec_events.release();
         spec_event_step.release();
         spec_status.release();
+        ah_state.release();
+        ah_tab.release();
+        ah_detail.release();
+        ah_events.release();
+        ah_event_step.release();
+        ah_status.release();
+        ah_live = false;
         spec_live = false;
+        head_ready = false;
         dropin_rcen = 0.0;
         step_central = false;
         hy_pairs.release();

@@ -217,6 +217,51 @@ def test_per_step_loop_long_run_with_reordering(backend, oracle):
     assert rel_err(x0, prev.x) < 1e-9
 
 
+def test_per_step_loop_with_changes_between_steps(backend, oracle):
+    """Per-step calls whose step size and central radius change between steps,
+    with other calls in between (previous-state download, export, force): the
+    next step, made ahead of the call while the host handles the records,
+    must be taken only when it was made for that call. Every step's records
+    and the final states match the oracle stepping the same sequence."""
+    sys0 = make_system(seed=21, n_particles=2500, near_fraction=0.05)
+    backend.upload(sys0)
+    ref = sys0.copy()
+    plan = [(8.0, 0.005)] * 5 + [(4.0, 0.005)] * 3 + [(8.0, 0.01)] * 4 + [(-8.0, 0.01)] * 2 + [(8.0, 0.005)] * 6
+    time = 0.0
+    for k, (h, rc) in enumerate(plan):
+        backend.step(time, h, dtflag=0 if k == 0 else 2)
+        if k % 4 == 1:
+            backend.download(previous=True)
+        if k == 9:
+            backend.force()
+        if k == 15:
+            backend.export(h)
+        ev = backend.events(time + h, h, rc)
+        rev, _ = oracle.mvs_run(ref, time, h, 1, rc, central=True, threads=4)
+        assert event_key(ev) == event_key(rev), k
+        time += h
+    x, v = backend.download()
+    assert rel_err(x, ref.x) < 1e-9 and rel_err(v, ref.v) < 1e-9
+
+
+def test_per_step_loop_many_records(backend, oracle):
+    """Consecutive steps with more records than are read back with the status
+    (1,024): the rest come from the device, every step."""
+    sys0 = make_system(seed=4, n_particles=12000, near_fraction=1.0, planet_kw=dict(mmin=1e-3, mmax=1e-3))
+    sys0.rce[1:sys0.nbig] *= 20.0
+    backend.upload(sys0)
+    ref = sys0.copy()
+    time, counts = 0.0, []
+    for k in range(4):
+        backend.step(time, 8.0, dtflag=0 if k == 0 else 2)
+        ev = backend.events(time + 8.0, 8.0, 0.005)
+        rev, _ = oracle.mvs_run(ref, time, 8.0, 1, 0.005, central=True, threads=4)
+        assert event_key(ev) == event_key(rev), k
+        counts.append(len(ev))
+        time += 8.0
+    assert min(counts) > 1024
+
+
 @pytest.mark.parametrize("oblate", [False, True])
 def test_massive_small_bodies(backend, oracle, oblate):
     """Semi-active Small bodies under MVS, which the reference accepts
