@@ -17,6 +17,17 @@ extern "C" {
  * steps_per_launch at a time (0 = automatic). *nevents receives the number of
  * event records, fetched with mercury_b200_events. */
 int mercury_b200_mvs_advance(double time, double h, int nsteps, double rcen, int steps_per_launch, int* nevents);
+/* Upload, advance and download in one call: the same results as
+ * mercury_cuda_upload(n, nbig, pn, ngflag, m, xx, vv, ng, jcen, limits, radii),
+ * mercury_b200_mvs_advance(time, h, nsteps, rcen, steps_per_launch, nevents)
+ * and mercury_cuda_download(xout, vout, 0). When the run is one launch and
+ * every host array is page-locked, the particles are copied in and out in
+ * chunks while other chunks are stepped; the system stays uploaded in its end
+ * state and the records are fetched with mercury_b200_events. */
+int mercury_b200_mvs_run(int n, int nbig, int pn, int ngflag, const double* m, const double* xx, const double* vv,
+                         const double* ng, const double* jcen, const double* limits, const double* radii,
+                         double time, double h, int nsteps, double rcen, int steps_per_launch, double* xout,
+                         double* vout, int* nevents);
 /* Copy up to cap records of the last advance, sorted by (step, min(i,j),
  * max(i,j)), with the 0-based step of each; returns the total count. */
 int mercury_b200_events(MercuryEvent* events, int* steps, int cap);

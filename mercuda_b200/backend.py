@@ -44,7 +44,7 @@ DROP_IN_SYMBOLS = [
     "mercury_cuda_encounter_enter", "mercury_cuda_encounter_update", "mercury_cuda_encounter_exit",
     "mercury_cuda_free",
 ]
-EXTENSION_SYMBOLS = ["mercury_b200_mvs_advance", "mercury_b200_events", "mercury_b200_timing",
+EXTENSION_SYMBOLS = ["mercury_b200_mvs_advance", "mercury_b200_mvs_run", "mercury_b200_events", "mercury_b200_timing",
                      "mercury_b200_set_launch", "mercury_b200_fp64_peak", "mercury_b200_mvs_step_noalloc",
                      "mercury_b200_dropin_time", "mercury_b200_batch_upload", "mercury_b200_batch_advance",
                      "mercury_b200_batch_events", "mercury_b200_batch_download", "mercury_b200_batch_set",
@@ -95,6 +95,7 @@ def load_library(path: Path | str | None = None) -> C.CDLL:
     L.mercury_cuda_encounter_exit.restype = None
     L.mercury_cuda_free.restype = None
     L.mercury_b200_mvs_advance.argtypes = [D, D, I, D, I, PI]
+    L.mercury_b200_mvs_run.argtypes = [I, I, I, I, PD, PD, PD, PD, PD, PD, PD, D, D, I, D, I, PD, PD, PI]
     L.mercury_b200_events.argtypes = [C.c_void_p, PI, I]
     L.mercury_b200_timing.argtypes = [PD, PD, PI, PI]
     L.mercury_b200_set_launch.argtypes = [I, I]
@@ -441,6 +442,29 @@ class Backend:
         if nev.value:
             self.lib.mercury_b200_events(events.ctypes.data_as(C.c_void_p), steps.ctypes.data_as(PI), nev.value)
         return events, steps
+
+    def mvs_run(self, sys: System, time: float, h: float, nsteps: int, rcen: float, steps_per_launch: int = 0,
+                ngflag: int | None = None, out=None):
+        """upload(sys) + mvs_advance + download() in one library call
+        (mercury_b200_mvs_run): with page-locked host arrays (sys's and `out`'s)
+        the particles' copies overlap their steps. Returns (events, steps, x, v)."""
+        self.n, self.nbig = sys.n, sys.nbig
+        flag = sys.ngflag if ngflag is None else int(ngflag)
+        if out is None:
+            out = (np.empty((sys.n, 3)), np.empty((sys.n, 3)))
+        x, v = out
+        assert x.shape == v.shape == (sys.n, 3) and x.dtype == v.dtype == np.float64
+        nev = I(0)
+        if self.lib.mercury_b200_mvs_run(sys.n, sys.nbig, int(sys.pn), flag, _p(sys.m), _p(sys.x), _p(sys.v),
+                                         _p(sys.ngf), _p(sys.jcen), _p(sys.rce), _p(sys.rphys), time, h,
+                                         int(nsteps), rcen, int(steps_per_launch), _p(x), _p(v),
+                                         C.byref(nev)) != 0:
+            raise BackendError("CUDA integration step failed")
+        events = np.empty(nev.value, dtype=EVENT_DTYPE)
+        steps = np.empty(nev.value, dtype=np.int32)
+        if nev.value:
+            self.lib.mercury_b200_events(events.ctypes.data_as(C.c_void_p), steps.ctypes.data_as(PI), nev.value)
+        return events, steps, x, v
 
     def timing(self):
         a, k, n, L = D(0.0), D(0.0), I(0), I(0)

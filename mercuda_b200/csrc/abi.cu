@@ -1,6 +1,7 @@
 // The drop-in C ABI (include/mercury_cuda.h) and the MVS extension entry
 // points (include/mercury_b200.h): host orchestration of the device context.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -310,7 +311,7 @@ MvsParticleArgs particle_args(int in, int out, int nsteps, int reset, int centra
 // candidate carries its step within the run.
 void particles_and_events(const MvsParticleArgs& pa, const double* detail, cudaStream_t s) {
     Context& c = ctx();
-    check(cudaMemsetAsync(&pa.status->next_tile, 0, sizeof(int), s), "memset");
+    check(cudaMemsetAsync(pa.tiles ? pa.tiles : &pa.status->next_tile, 0, sizeof(int), s), "memset");
     launch_mvs_particles(pa, s, c.particle_threads);
     ClassifyArgs ca{};
     ca.nb = c.nbig - 1;
@@ -1168,6 +1169,46 @@ void order_particles(int n, int nbig, double mu, const double* x, const double* 
     check(cudaGetLastError(), "order");
 }
 
+// Slot maps of one chunk of particles [base, base + cnt) ordered within its
+// own slots: perm[base + r] = base + sorted[r] and its inverse; with pad, the
+// padding slot after the chunk maps to itself.
+__global__ void chunk_slot_maps_kernel(const int* sorted, int cnt, int base, int pad, int* perm, int* inv) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= cnt + pad) return;
+    const int p = base + (r < cnt ? sorted[r] : r);
+    perm[base + r] = p;
+    inv[p] = base + r;
+}
+
+// The upload's slot order for the particles [plo, phi) alone (the same keys
+// and stable sort as order_particles, within the chunk's slots), from the
+// staged rows x, v of the bodies; pad: the chunk ends at the padding slot;
+// cap: the largest chunk of the run.
+void order_chunk(int plo, int phi, int pad, int cap, double mu, const double* x, const double* v, cudaStream_t s) {
+    Context& c = ctx();
+    const int cnt = phi - plo;
+    auto align = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    // scratch laid out for the largest chunk (cap), so that it is not
+    // reallocated between chunks (an empty chunk only sizes it)
+    size_t temp = 0;
+    check(cub::DeviceRadixSort::SortPairs(nullptr, temp, (const unsigned char*)nullptr, (unsigned char*)nullptr,
+                                          (const int*)nullptr, (int*)nullptr, cap, 0, 8, s),
+          "order");
+    const size_t kb = align(cap), ib = align(sizeof(int) * (size_t)cap);
+    c.order_scratch.reserve(2 * kb + 2 * ib + align(temp));
+    if (cnt <= 0) return;
+    char* base = c.order_scratch.p;
+    unsigned char* kin = reinterpret_cast<unsigned char*>(base);
+    unsigned char* kout = kin + kb;
+    int* iin = reinterpret_cast<int*>(base + 2 * kb);
+    int* iout = reinterpret_cast<int*>(base + 2 * kb + ib);
+    void* tmp = base + 2 * kb + 2 * ib;
+    path_key_kernel<<<blocks(cnt), 256, 0, s>>>(x, v, c.nsplit + plo, cnt, mu, kin, iin);
+    check(cub::DeviceRadixSort::SortPairs(tmp, temp, kin, kout, iin, iout, cnt, 0, 8, s), "order");
+    chunk_slot_maps_kernel<<<blocks(cnt + pad), 256, 0, s>>>(iout, cnt, plo, pad, c.perm[c.kc].p, c.inv.p);
+    check(cudaGetLastError(), "order");
+}
+
 // The records of a fused run in (step, min(i,j), max(i,j)) order on the
 // device: a 64-bit key per record (the step above the two 1-based ids, each
 // in `idbits` bits; one record per pair per step makes the keys distinct),
@@ -1661,6 +1702,177 @@ void gather_rows(double* rows, int n, int comps, int nbig, const double* big, in
     gather_kernel<<<blocks(n), 256, 0, s>>>(rows, n, comps, nbig, big, big_stride, part, part_stride, inv);
 }
 
+// The upload's checks: body counts and the workspace guard, as the
+// reference's (mercury_cuda.cu:384-388): a system that needs more device
+// memory than 80% of what is free fails here with a message instead of
+// part-way through allocating (checked whenever the particle buffers may have
+// to grow).
+void upload_checks(int n, int nbig) {
+    Context& c = ctx();
+    if (n < 1 || nbig < 1 || nbig > n) throw std::runtime_error("invalid body counts");
+    if (is_mvs(c.algorithm) && nbig > 512) throw std::runtime_error("more than 512 Big bodies");
+    const size_t need = workspace_bytes(n, c.algorithm);
+    if ((size_t)9 * (size_t)std::max(2, (n - nbig + 1) & ~1) > c.pstate[0].n || injected("memory")) {
+        size_t free_b = 0, total_b = 0;
+        if (!injected("memory")) check(cudaMemGetInfo(&free_b, &total_b), "memory");
+        if ((double)need > 0.8 * (double)free_b) throw std::runtime_error("Insufficient device workspace memory");
+    }
+}
+
+// The upload's layout of a system on the device: the massive set, every
+// buffer's size, zeroed states and constants (on the library stream). The
+// host rows are not read here except for the masses.
+// One past the last body at or after nbig whose mass is not zero (nbig if
+// none). m[j] != 0.0 is the bits without the sign bit being non-zero (a NaN
+// counts as massive, -0.0 as massless); blocks of 512 are tested by OR-ing
+// those bits (a loop the compiler vectorizes), on up to 16 host threads for
+// large n, each taking a range and reporting its last massive body.
+int last_massive(const double* m, int n, int nbig) {
+    auto last_in = [m](int lo, int hi) -> int {
+        constexpr int B = 512;
+        for (int top = hi; top > lo;) {
+            const int bot = std::max(lo, top - B);
+            uint64_t acc = 0;
+            for (int j = bot; j < top; ++j) {
+                uint64_t b;
+                std::memcpy(&b, m + j, sizeof(b));
+                acc |= b << 1;
+            }
+            if (acc != 0)
+                for (int j = top - 1; j >= bot; --j)
+                    if (m[j] != 0.0) return j;
+            top = bot;
+        }
+        return -1;
+    };
+    const int count = n - nbig;
+    const int nthreads = count < (1 << 18) ? 1 : (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    int last = -1;
+    if (nthreads == 1) {
+        last = last_in(nbig, n);
+    } else {
+        std::vector<int> found(nthreads, -1);
+        std::vector<std::thread> pool;
+        const int chunk = (count + nthreads - 1) / nthreads;
+        for (int t = 0; t < nthreads; ++t) {
+            const int lo = nbig + std::min(count, t * chunk), hi = nbig + std::min(count, (t + 1) * chunk);
+            pool.emplace_back([&, t, lo, hi] { found[t] = last_in(lo, hi); });
+        }
+        for (auto& th : pool) th.join();
+        for (int f : found) last = std::max(last, f);
+    }
+    return last >= 0 ? last + 1 : nbig;
+}
+
+void upload_layout(int n, int nbig, int pn, int ngflag, const double* m, const double* jcen) {
+    Context& c = ctx();
+    cudaStream_t s = c.stream;
+    const int nmass = last_massive(m, n, nbig);
+    // MVS: massive Small bodies move as test particles and act on nothing
+    // but the central body's oblateness reaction (mfo_mvs,
+    // mercury6_2.for:5061-5068); the Big-body CTA holds them (up to 512
+    // bodies in all). Without oblateness more of them are exactly massless
+    // for the map and stay in the particle slots.
+    const bool obl = jcen[0] != 0.0 || jcen[1] != 0.0 || jcen[2] != 0.0;
+    int ns = nmass;
+    if (is_mvs(c.algorithm) && nmass > 512) {
+        if (obl) throw std::runtime_error("MVS with oblateness and more than 512 Big and massive Small bodies");
+        ns = nbig;
+    }
+    if (ns > 512) throw std::runtime_error("more than 512 Big and massive Small bodies");
+    c.n = n;
+    c.nbig = nbig;
+    c.nmass = nmass;
+    c.nsplit = ns;
+    c.np = n - ns;
+    c.npcap = std::max(2, (c.np + 1) & ~1);
+    c.pn = pn != 0 ? 1 : 0;
+    c.ngflag = ngflag;
+    for (int k = 0; k < 3; ++k) c.jcen[k] = jcen[k];
+    // HYBRID compares the masses of every body between calls; the others
+    // read the central mass only
+    c.m_host.assign(m, m + (c.algorithm == 10 ? n : 1));
+    c.event_rate = 0.0;
+    c.ev_device = 0;
+    c.step_central = false;
+    c.mbig.reserve(ns);
+    c.rcebig.reserve(ns);
+    c.rphysbig.reserve(ns);
+    c.ngfbig.reserve((size_t)5 * ns);
+    for (int k = 0; k < 2; ++k) {
+        c.bigstate[k].reserve((size_t)9 * ns);
+        c.pstate[k].reserve((size_t)9 * c.npcap);
+    }
+    for (int k = 0; k < 2; ++k) {
+        c.pconst[k].reserve((size_t)PCONST_ROWS * c.npcap);
+        c.perm[k].reserve(c.npcap);
+    }
+    c.inv.reserve(c.npcap);
+    c.kc = 0;
+    c.status.reserve(1);
+    if (g_event_cap > 0) {
+        c.events.release();
+        c.event_step.release();
+        c.cands.release();
+        ensure_events(g_event_cap);
+        c.cands.reserve(g_event_cap);
+    } else {
+        ensure_events(std::max(4096, c.np / 64));
+        c.cands.reserve(std::max(16384, c.np / 2));
+    }
+    c.transfer.reserve((size_t)6 * n);
+    if (c.algorithm == 4) {
+        c.ra_bb.reserve((size_t)21 * ns);
+        c.ra_be.reserve((size_t)21 * ns);
+        c.ra_bg.reserve((size_t)21 * ns);
+        c.ra_bpx.reserve((size_t)6 * ns);
+        c.ra_pb.reserve((size_t)21 * c.npcap);
+        c.ra_pe.reserve((size_t)21 * c.npcap);
+        c.ra_max.reserve(1);
+    }
+    // zero padding and cached accelerations
+    check(cudaMemsetAsync(c.pstate[0].p, 0, sizeof(double) * 9 * c.npcap, s), "memset");
+    check(cudaMemsetAsync(c.pstate[1].p, 0, sizeof(double) * 9 * c.npcap, s), "memset");
+    check(cudaMemsetAsync(c.bigstate[0].p, 0, sizeof(double) * 9 * ns, s), "memset");
+    check(cudaMemsetAsync(c.bigstate[1].p, 0, sizeof(double) * 9 * ns, s), "memset");
+    check(cudaMemsetAsync(c.pconst[0].p, 0, sizeof(double) * PCONST_ROWS * c.npcap, s), "memset");
+    check(cudaMemsetAsync(c.pconst[1].p, 0, sizeof(double) * PCONST_ROWS * c.npcap, s), "memset");
+    c.cur = 0;
+}
+
+// The staged host rows of the Big bodies and of the particles [plo, phi)
+// (particle indices, slots in the same range) into the device layout
+// through the slot map: x and v rows (3 per body) into the state, the
+// masses and radii, the ngf rows (5 per body) when a force law reads them.
+void scatter_staged(const double* sx, const double* sv, const double* sm, const double* sr, const double* sp,
+                    const double* sg, bool big, int plo, int phi, cudaStream_t s) {
+    Context& c = ctx();
+    const int ns = c.nsplit;
+    if (big) {
+        for (int part = 0; part < 2; ++part)
+            scatter_rows(part ? sv : sx, ns, 3, ns, c.bigstate[0].p + 3 * part * ns, ns, nullptr, 0, nullptr, s);
+        const double* scalars[3] = {sm, sr, sp};
+        double* bigdst[3] = {c.mbig.p, c.rcebig.p, c.rphysbig.p};
+        for (int q = 0; q < 3; ++q) scatter_rows(scalars[q], ns, 1, ns, bigdst[q], ns, nullptr, 0, nullptr, s);
+        if (sg) {
+            check(cudaMemcpyAsync(c.ngfbig.p, sg, sizeof(double) * 5 * ns, cudaMemcpyDeviceToDevice, s), "upload");
+        } else {
+            check(cudaMemsetAsync(c.ngfbig.p, 0, sizeof(double) * 5 * ns, s), "upload");
+        }
+    }
+    const int cnt = phi - plo;
+    if (cnt <= 0) return;
+    const size_t r0 = (size_t)ns + plo;
+    const int* inv = c.inv.p + plo;
+    for (int part = 0; part < 2; ++part)
+        scatter_rows((part ? sv : sx) + 3 * r0, cnt, 3, 0, nullptr, 0, c.pstate[0].p + (size_t)3 * part * c.npcap,
+                     c.npcap, inv, s);
+    const double* scalars[3] = {sm, sr, sp};
+    double* pdst[3] = {c.pm(), c.prce(), c.prphys()};
+    for (int q = 0; q < 3; ++q) scatter_rows(scalars[q] + r0, cnt, 1, 0, nullptr, 0, pdst[q], c.npcap, inv, s);
+    if (sg) scatter_rows(sg + 5 * r0, cnt, 5, 0, nullptr, 0, c.pngf(), c.npcap, inv, s);
+}
+
 }  // namespace mb200
 
 using namespace mb200;
@@ -1707,18 +1919,7 @@ int mercury_cuda_upload(int n, int nbig, int pn, int ngflag, const double* m, co
     try {
         drop_speculation();
         inject("upload");
-        if (n < 1 || nbig < 1 || nbig > n) throw std::runtime_error("invalid body counts");
-        if (is_mvs(c.algorithm) && nbig > 512) throw std::runtime_error("more than 512 Big bodies");
-        // Workspace guard, as the reference's (mercury_cuda.cu:384-388): a
-        // system that needs more device memory than 80% of what is free
-        // fails here with a message instead of part-way through allocating
-        // (checked whenever the particle buffers may have to grow).
-        const size_t need = workspace_bytes(n, c.algorithm);
-        if ((size_t)9 * (size_t)std::max(2, (n - nbig + 1) & ~1) > c.pstate[0].n || injected("memory")) {
-            size_t free_b = 0, total_b = 0;
-            if (!injected("memory")) check(cudaMemGetInfo(&free_b, &total_b), "memory");
-            if ((double)need > 0.8 * (double)free_b) throw std::runtime_error("Insufficient device workspace memory");
-        }
+        upload_checks(n, nbig);
         c.ensure_streams();
         cudaStream_t s = c.stream;
         // Every host array in one round of copies into the upload stage (ngf
@@ -1747,95 +1948,9 @@ int mercury_cuda_upload(int n, int nbig, int pn, int ngflag, const double* m, co
                 if (armed) cudaStreamSynchronize(s);
             }
         } drain{s};
-        int nmass = nbig;
-        for (int j = n - 1; j >= nbig; --j)
-            if (m[j] != 0.0) {
-                nmass = j + 1;
-                break;
-            }
-        // MVS: massive Small bodies move as test particles and act on nothing
-        // but the central body's oblateness reaction (mfo_mvs,
-        // mercury6_2.for:5061-5068); the Big-body CTA holds them (up to 512
-        // bodies in all). Without oblateness more of them are exactly massless
-        // for the map and stay in the particle slots.
-        const bool obl = jcen[0] != 0.0 || jcen[1] != 0.0 || jcen[2] != 0.0;
-        int ns = nmass;
-        if (is_mvs(c.algorithm) && nmass > 512) {
-            if (obl) throw std::runtime_error("MVS with oblateness and more than 512 Big and massive Small bodies");
-            ns = nbig;
-        }
-        if (ns > 512) throw std::runtime_error("more than 512 Big and massive Small bodies");
-        c.n = n;
-        c.nbig = nbig;
-        c.nmass = nmass;
-        c.nsplit = ns;
-        c.np = n - ns;
-        c.npcap = std::max(2, (c.np + 1) & ~1);
-        c.pn = pn != 0 ? 1 : 0;
-        c.ngflag = ngflag;
-        for (int k = 0; k < 3; ++k) c.jcen[k] = jcen[k];
-        c.m_host.assign(m, m + n);
-        c.event_rate = 0.0;
-        c.ev_device = 0;
-        c.step_central = false;
-        c.mbig.reserve(ns);
-        c.rcebig.reserve(ns);
-        c.rphysbig.reserve(ns);
-        c.ngfbig.reserve((size_t)5 * ns);
-        for (int k = 0; k < 2; ++k) {
-            c.bigstate[k].reserve((size_t)9 * ns);
-            c.pstate[k].reserve((size_t)9 * c.npcap);
-        }
-        for (int k = 0; k < 2; ++k) {
-            c.pconst[k].reserve((size_t)PCONST_ROWS * c.npcap);
-            c.perm[k].reserve(c.npcap);
-        }
-        c.inv.reserve(c.npcap);
-        c.kc = 0;
-        c.status.reserve(1);
-        if (g_event_cap > 0) {
-            c.events.release();
-            c.event_step.release();
-            c.cands.release();
-            ensure_events(g_event_cap);
-            c.cands.reserve(g_event_cap);
-        } else {
-            ensure_events(std::max(4096, c.np / 64));
-            c.cands.reserve(std::max(16384, c.np / 2));
-        }
-        c.transfer.reserve((size_t)6 * n);
-        if (c.algorithm == 4) {
-            c.ra_bb.reserve((size_t)21 * ns);
-            c.ra_be.reserve((size_t)21 * ns);
-            c.ra_bg.reserve((size_t)21 * ns);
-            c.ra_bpx.reserve((size_t)6 * ns);
-            c.ra_pb.reserve((size_t)21 * c.npcap);
-            c.ra_pe.reserve((size_t)21 * c.npcap);
-            c.ra_max.reserve(1);
-        }
-        // zero padding and cached accelerations
-        check(cudaMemsetAsync(c.pstate[0].p, 0, sizeof(double) * 9 * c.npcap, s), "memset");
-        check(cudaMemsetAsync(c.pstate[1].p, 0, sizeof(double) * 9 * c.npcap, s), "memset");
-        check(cudaMemsetAsync(c.bigstate[0].p, 0, sizeof(double) * 9 * ns, s), "memset");
-        check(cudaMemsetAsync(c.bigstate[1].p, 0, sizeof(double) * 9 * ns, s), "memset");
-        check(cudaMemsetAsync(c.pconst[0].p, 0, sizeof(double) * PCONST_ROWS * c.npcap, s), "memset");
-        check(cudaMemsetAsync(c.pconst[1].p, 0, sizeof(double) * PCONST_ROWS * c.npcap, s), "memset");
-        c.cur = 0;
-        order_particles(n, ns, m[0], sx, sv);
-        for (int part = 0; part < 2; ++part)
-            scatter_rows(part ? sv : sx, n, 3, ns, c.bigstate[0].p + 3 * part * ns, ns,
-                         c.pstate[0].p + (size_t)3 * part * c.npcap, c.npcap, c.inv.p, s);
-        const double* scalars[3] = {sm, sr, sp};
-        double* bigdst[3] = {c.mbig.p, c.rcebig.p, c.rphysbig.p};
-        double* pdst[3] = {c.pm(), c.prce(), c.prphys()};
-        for (int q = 0; q < 3; ++q) scatter_rows(scalars[q], n, 1, ns, bigdst[q], ns, pdst[q], c.npcap, c.inv.p, s);
-        // ngf: Big rows stay interleaved (5 per body); particles become SoA
-        if (ngf_read) {
-            check(cudaMemcpyAsync(c.ngfbig.p, sg, sizeof(double) * 5 * ns, cudaMemcpyDeviceToDevice, s), "upload");
-            scatter_rows(sg, n, 5, ns, nullptr, 0, c.pngf(), c.npcap, c.inv.p, s);
-        } else {
-            check(cudaMemsetAsync(c.ngfbig.p, 0, sizeof(double) * 5 * ns, s), "upload");
-        }
+        upload_layout(n, nbig, pn, ngflag, m, jcen);
+        order_particles(n, c.nsplit, m[0], sx, sv);
+        scatter_staged(sx, sv, sm, sr, sp, ngf_read ? sg : nullptr, true, 0, c.np, s);
         check(cudaGetLastError(), "upload");
         drain.armed = false;
         check(cudaStreamSynchronize(s), "upload");
@@ -2469,6 +2584,269 @@ int mercury_b200_mvs_advance(double time, double h, int nsteps, double rcen, int
         // records stay in arrival order; mercury_b200_events gathers them in
         // (step, min(i,j), max(i,j)) order straight into the caller's arrays
         order_events(c.host_events, &c.host_steps, c.event_order);
+        *nevents = nev;
+        return 0;
+    } catch (const std::exception& e) {
+        return report(e);
+    }
+}
+
+// Particles per chunk of mercury_b200_mvs_run (at least; at most 8 chunks).
+#ifndef MB200_RUN_CHUNK_PARTICLES
+#define MB200_RUN_CHUNK_PARTICLES (1 << 17)
+#endif
+constexpr int RUN_CHUNK_PARTICLES = MB200_RUN_CHUNK_PARTICLES;
+// Particle launches of mercury_b200_mvs_run (each over whole chunks).
+#ifndef MB200_RUN_LAUNCHES
+#define MB200_RUN_LAUNCHES 2
+#endif
+constexpr int RUN_LAUNCHES = MB200_RUN_LAUNCHES;
+
+// Upload, nsteps fused MVS steps and download in one call: the same as
+// mercury_cuda_upload, mercury_b200_mvs_advance and mercury_cuda_download
+// (previous = 0), with the particles' copies overlapped with their steps
+// when the run is one launch and the host arrays are page-locked. The Big
+// bodies go first and take their steps while the particles are copied in
+// chunks; each chunk is put in slot order within its own slots and stepped
+// as soon as it is in, and its end states (written as host rows by the
+// particle kernel) go back while the next chunk is stepped. Otherwise the
+// three calls are made one after the other.
+int mercury_b200_mvs_run(int n, int nbig, int pn, int ngflag, const double* m, const double* xx, const double* vv,
+                         const double* ng, const double* jcen, const double* limits, const double* radii,
+                         double time, double h, int nsteps, double rcen, int steps_per_launch, double* xout,
+                         double* vout, int* nevents) {
+    Context& c = ctx();
+    auto in_turn = [&]() -> int {
+        int rc = mercury_cuda_upload(n, nbig, pn, ngflag, m, xx, vv, ng, jcen, limits, radii);
+        if (rc == 0) rc = mercury_b200_mvs_advance(time, h, nsteps, rcen, steps_per_launch, nevents);
+        if (rc == 0) rc = mercury_cuda_download(xout, vout, 0);
+        return rc;
+    };
+    try {
+        if (!is_mvs(c.algorithm)) throw std::runtime_error("MVS run needs algorithm 1 or 9");
+        if (nsteps < 1) throw std::runtime_error("nsteps must be positive");
+        if (n < 1 || nbig < 1 || nbig > n) throw std::runtime_error("invalid body counts");
+        const int nb = nbig - 1;
+        int K = steps_per_launch > 0 ? steps_per_launch : (c.steps_per_launch > 0 ? c.steps_per_launch : 0);
+        if (K <= 0) K = mvs_max_steps_per_launch(nb);
+        K = std::min(K, mvs_max_steps_per_launch(nb));
+        const int nchunk = std::min(8, (n - nbig) / RUN_CHUNK_PARTICLES);
+        bool pinned = nchunk > 1 && K >= nsteps;
+        for (const void* p : {(const void*)xx, (const void*)vv, (const void*)m, (const void*)limits,
+                              (const void*)radii, (const void*)xout, (const void*)vout})
+            pinned = pinned && host_pinned(p);
+        if (pinned && ngflag != 0) pinned = host_pinned(ng);
+        if (!pinned) return in_turn();
+
+        drop_speculation();
+        inject("upload");
+        upload_checks(n, nbig);
+        c.ensure_streams();
+        cudaStream_t s = c.stream, sin = c.stream_ahead, sout = c.stream_out, sbig = c.stream_big;
+        const size_t N = (size_t)n;
+        const bool ngf_read = ngflag != 0;
+        c.stage.reserve(9 * N + (ngf_read ? 5 * N : 0));
+        double* sx = c.stage.p;
+        double* sv = sx + 3 * N;
+        double* sm = sv + 3 * N;
+        double* sr = sm + N;
+        double* sp = sr + N;
+        double* sg = ngf_read ? sp + N : nullptr;
+        // nothing below may return before the streams are drained: the stage
+        // and the caller's arrays are in use
+        struct Drain {
+            std::array<cudaStream_t, 4> ss;
+            bool armed = true;
+            ~Drain() {
+                if (armed)
+                    for (cudaStream_t q : ss) cudaStreamSynchronize(q);
+            }
+        } drain{{s, sin, sout, sbig}};
+        // chunk boundaries in particle indices (slots in the same ranges),
+        // multiples of 64 slots, for the particles after the Big bodies (a
+        // massive Small body moves the split: then the calls in turn)
+        const int np0 = n - nbig;
+        std::vector<int> lo(nchunk + 1);
+        for (int k = 0; k <= nchunk; ++k) lo[k] = k == nchunk ? np0 : (int)(((long long)k * np0 / nchunk) & ~63LL);
+        int cap = 0;
+        for (int k = 0; k < nchunk; ++k) cap = std::max(cap, lo[k + 1] - lo[k]);
+        // events: run_in[k + 1] chunk k copied in, run_in[0] the Big bodies'
+        // rows; run_done[q] launch q stepped, run_done[E] the Big bodies
+        // stepped, run_done[E + 1] every chunk laid out
+        const int E = std::max(nchunk, RUN_LAUNCHES);
+        if ((int)c.run_in.size() < E + 2) {
+            const size_t old = c.run_in.size();
+            c.run_in.resize(E + 2);
+            c.run_done.resize(E + 2);
+            for (size_t k = old; k < (size_t)E + 2; ++k) {
+                check(cudaEventCreateWithFlags(&c.run_in[k], cudaEventDisableTiming), "event");
+                check(cudaEventCreateWithFlags(&c.run_done[k], cudaEventDisableTiming), "event");
+            }
+        }
+        // copies in first (the earlier calls have drained every stream, so
+        // the stage is free): the Big bodies' rows, then every chunk's; the
+        // host's scan and the layout below run while they fly
+        auto rows_in = [&](size_t r0, size_t r1) {
+            auto h2d_rows = [&](double* dst, const double* src, size_t width) {
+                check(cudaMemcpyAsync(dst + r0 * width, src + r0 * width, sizeof(double) * width * (r1 - r0),
+                                      cudaMemcpyHostToDevice, sin),
+                      "upload");
+            };
+            h2d_rows(sx, xx, 3);
+            h2d_rows(sv, vv, 3);
+            h2d_rows(sm, m, 1);
+            h2d_rows(sr, limits, 1);
+            h2d_rows(sp, radii, 1);
+            if (ngf_read) h2d_rows(sg, ng, 5);
+        };
+        rows_in(0, nbig);
+        check(cudaEventRecord(c.run_in[0], sin), "event");
+        for (int k = 0; k < nchunk; ++k) {
+            rows_in(nbig + (size_t)lo[k], nbig + (size_t)lo[k + 1]);
+            check(cudaEventRecord(c.run_in[k + 1], sin), "event");
+        }
+        upload_layout(n, nbig, pn, ngflag, m, jcen);
+        if (c.nsplit != nbig) {
+            check(cudaStreamSynchronize(sin), "upload");
+            drain.armed = false;
+            return in_turn();
+        }
+        const int ns = c.nsplit, np = c.np;
+        // every buffer that may be reallocated (cudaFree waits for the device)
+        {
+            const double want = std::min(np * 1e-3 * nsteps + 1024.0, 16777216.0);
+            size_t free_b = 0, total_b = 0;
+            if (want > (double)c.events.n && cudaMemGetInfo(&free_b, &total_b) == cudaSuccess &&
+                want * (sizeof(MercuryEvent) + sizeof(int)) < 0.25 * (double)free_b)
+                ensure_events((int)want);
+        }
+        ensure_tables(nsteps + 1, nsteps);
+        order_chunk(0, 0, 0, cap, m[0], sx, sv, s);   // sizes the ordering scratch
+        c.run_tiles.reserve(RUN_LAUNCHES);
+        check(cudaMemsetAsync(c.run_tiles.p, 0, sizeof(int) * RUN_LAUNCHES, s), "memset");
+        // the Big bodies' steps, while the particles come in
+        check(cudaStreamWaitEvent(s, c.run_in[0], 0), "wait");
+        scatter_staged(sx, sv, sm, sr, sp, sg, true, 0, 0, s);
+        check(cudaMemsetAsync(c.status.p, 0, sizeof(DeviceStatus), s), "memset");
+        check(cudaEventRecord(c.t0, s), "event");
+        check(cudaStreamWaitEvent(sbig, c.t0, 0), "wait");
+        launch_mvs_big(big_args(0, 1, nsteps, 1, 1, 0, h, rcen, c.tab.p, c.detail.p), sbig);
+        check(cudaEventRecord(c.run_done[E], sbig), "event");
+        // each chunk in slot order and laid out as soon as it is in (while
+        // the next is copied)
+        for (int k = 0; k < nchunk; ++k) {
+            const int pad = (k == nchunk - 1 && c.npcap > np) ? 1 : 0;
+            check(cudaStreamWaitEvent(s, c.run_in[k + 1], 0), "wait");
+            order_chunk(lo[k], lo[k + 1], pad, cap, m[0], sx, sv, s);
+            scatter_staged(sx, sv, sm, sr, sp, sg, false, lo[k], lo[k + 1], s);
+        }
+        check(cudaStreamWaitEvent(s, c.run_done[E], 0), "wait");
+        check(cudaEventRecord(c.run_done[E + 1], s), "event");
+        // the particles' steps in a few launches on two streams, back to back
+        // (a launch's grid fills in as the one before drains), each launch's
+        // end states (written as host rows by the kernel) going back while the
+        // next is stepped
+        double* rx = c.transfer.p;
+        double* rv = c.transfer.p + 3 * N;
+        for (int q = 0; q < RUN_LAUNCHES; ++q) {
+            const int plo = lo[(size_t)q * nchunk / RUN_LAUNCHES], phi = lo[(size_t)(q + 1) * nchunk / RUN_LAUNCHES];
+            const int cnt = phi - plo;
+            if (cnt <= 0) continue;
+            cudaStream_t sq = q % 2 == 0 ? s : sbig;
+            if (q % 2 == 1) check(cudaStreamWaitEvent(sq, c.run_done[E + 1], 0), "wait");
+            MvsParticleArgs pa = particle_args(0, 1, nsteps, 1, 1, 0, h, rcen, c.tab.p, c.detail.p);
+            pa.np = cnt;
+            pa.xin += plo;
+            pa.xout += plo;
+            pa.m += plo;
+            pa.rce += plo;
+            pa.rphys += plo;
+            pa.ngf += plo;
+            pa.perm += plo;
+            pa.tiles = c.run_tiles.p + q;
+            pa.rows_x = rx + 3 * (size_t)ns;
+            pa.rows_v = rv + 3 * (size_t)ns;
+            launch_mvs_particles(pa, sq, c.particle_threads);
+            check(cudaEventRecord(c.run_done[q], sq), "event");
+            check(cudaStreamWaitEvent(sout, c.run_done[q], 0), "wait");
+            const size_t r0 = ns + (size_t)plo;
+            check(cudaMemcpyAsync(xout + 3 * r0, rx + 3 * r0, sizeof(double) * 3 * cnt, cudaMemcpyDeviceToHost, sout),
+                  "download");
+            check(cudaMemcpyAsync(vout + 3 * r0, rv + 3 * r0, sizeof(double) * 3 * cnt, cudaMemcpyDeviceToHost, sout),
+                  "download");
+        }
+        for (int q = 1; q < RUN_LAUNCHES; q += 2) check(cudaStreamWaitEvent(s, c.run_done[q], 0), "wait");
+        // the pair records of every chunk, the Big bodies' rows out
+        ClassifyArgs ca{};
+        ca.nb = nb;
+        ca.nbig = nbig;
+        ca.h = h;
+        ca.detail = c.detail.p;
+        ca.cands = c.cands.p;
+        ca.cand_cap = (int)c.cands.n;
+        ca.events = c.events.p;
+        ca.event_step = c.event_step.p;
+        ca.event_cap = (int)c.events.n;
+        ca.status = c.status.p;
+        ca.step_base = 0;
+        if (nb > 0 && np > 0) launch_classify(ca, s);
+        check(cudaMemsetAsync(&c.status.p->cands, 0, sizeof(int), s), "memset");
+        gather_rows(rx, ns, 3, ns, c.bigstate[1].p, ns, nullptr, 0, nullptr, s);
+        gather_rows(rv, ns, 3, ns, c.bigstate[1].p + 3 * ns, ns, nullptr, 0, nullptr, s);
+        check(cudaMemcpyAsync(xout, rx, sizeof(double) * 3 * ns, cudaMemcpyDeviceToHost, s), "download");
+        check(cudaMemcpyAsync(vout, rv, sizeof(double) * 3 * ns, cudaMemcpyDeviceToHost, s), "download");
+        check(cudaGetLastError(), "launch");
+        check(cudaEventRecord(c.t1, s), "event");
+        drain.armed = false;
+        for (cudaStream_t q : {sin, sout, sbig}) check(cudaStreamSynchronize(q), "step");
+        read_status();
+        c.steps_since_order = 0;
+        c.cur = 1;
+        c.stepped = false;
+        c.pair_events = 0;
+        if (c.status_host->fault) throw std::runtime_error("MVS force failed");
+        if (c.status_host->overflow) {
+            // more records than the buffers held: the whole run again from the
+            // uploaded states (still in buffer 0), with room
+            grow_after_overflow();
+            c.cur = 0;
+            c.reset = true;
+            const int rc = mercury_b200_mvs_advance(time, h, nsteps, rcen, steps_per_launch, nevents);
+            return rc ? rc : mercury_cuda_download(xout, vout, 0);
+        }
+        check(cudaEventElapsedTime(&c.last_advance_ms, c.t0, c.t1), "timer");
+        c.last_particle_launches = RUN_LAUNCHES;
+        c.last_kernel_launches = 1 + 10 * nchunk + RUN_LAUNCHES + 3;
+        c.nforces += nsteps + 1;
+        c.reset = false;
+        const int nev = c.status_host->events;
+        c.event_rate = std::max(c.event_rate, (double)nev / nsteps);
+        std::vector<double> tend(nsteps);
+        double t = time;
+        for (int q = 0; q < nsteps; ++q) {
+            t = t + h;
+            tend[q] = t;
+        }
+        c.host_events.clear();
+        c.host_steps.clear();
+        c.event_order.clear();
+        c.ev_device = 0;
+        if (nev && order_events_device(nev, nsteps, tend, h)) {
+            c.ev_device = nev;
+        } else if (nev) {
+            size_records(c.host_events, nev);
+            size_records(c.host_steps, nev);
+            copy_out({{c.events.p, c.host_events.data(), sizeof(MercuryEvent) * (size_t)nev},
+                      {c.event_step.p, c.host_steps.data(), sizeof(int) * (size_t)nev}},
+                     c.stream);
+            for (int k = 0; k < nev; ++k) {
+                MercuryEvent& e = c.host_events[k];
+                const double te = tend[c.host_steps[k]];
+                if (e.kind == EV_CENTRAL) e.time = te - h + e.time;
+                else e.time = e.time + te;
+            }
+            order_events(c.host_events, &c.host_steps, c.event_order);
+        }
         *nevents = nev;
         return 0;
     } catch (const std::exception& e) {

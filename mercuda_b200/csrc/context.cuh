@@ -152,10 +152,13 @@ struct Context {
         pinned_n = bytes;
     }
     // streams and timers
-    cudaStream_t stream = nullptr, stream_big = nullptr, stream_ahead = nullptr;
+    cudaStream_t stream = nullptr, stream_big = nullptr, stream_ahead = nullptr, stream_out = nullptr;
     std::vector<cudaEvent_t> chunk_done;
     cudaEvent_t t0 = nullptr, t1 = nullptr;
     std::vector<cudaEvent_t> kt0, kt1;
+    // mercury_b200_mvs_run's chunks: copied in, stepped; their work counters
+    std::vector<cudaEvent_t> run_in, run_done;
+    DBuf<int> run_tiles;
     float last_advance_ms = 0.0f;
     double last_particle_kernel_ms = 0.0;
     int last_particle_launches = 0;
@@ -232,6 +235,7 @@ struct Context {
             check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "stream");
             check(cudaStreamCreateWithFlags(&stream_big, cudaStreamNonBlocking), "stream");
             check(cudaStreamCreateWithFlags(&stream_ahead, cudaStreamNonBlocking), "stream");
+            check(cudaStreamCreateWithFlags(&stream_out, cudaStreamNonBlocking), "stream");
             check(cudaEventCreate(&t0), "event");
             check(cudaEventCreate(&t1), "event");
             check(cudaEventCreate(&d0), "event");
@@ -254,7 +258,7 @@ struct Context {
         if (pinned) cudaFreeHost(pinned);
         pinned = nullptr;
         pinned_n = 0;
-        DBuf<int>* ibufs[] = {&perm[0], &perm[1], &inv, &order_bucket, &order_hist, &snap_perm, &ej_ids};
+        DBuf<int>* ibufs[] = {&perm[0], &perm[1], &inv, &order_bucket, &order_hist, &snap_perm, &ej_ids, &run_tiles};
         for (auto* b : ibufs) b->release();
         ra_max.release();
         bs_errs.release();

@@ -595,9 +595,10 @@ __global__ void __launch_bounds__(128, MB200_PARTICLE_MIN_BLOCKS) mvs_particle_k
     const int S = A.npcap, H = S / 2;
     const double2* in = reinterpret_cast<const double2*>(A.xin);
     double2* out = reinterpret_cast<double2*>(A.xout);
+    int* const tiles = A.tiles ? A.tiles : &A.status->next_tile;
     for (;;) {
         int tile = 0;
-        if (lane == 0) tile = atomicAdd(&A.status->next_tile, 1);
+        if (lane == 0) tile = atomicAdd(tiles, 1);
         tile = __shfl_sync(FULL, tile, 0);
         if (tile >= ntiles) break;
         const int pair = tile * 32 + lane;
@@ -656,6 +657,25 @@ __global__ void __launch_bounds__(128, MB200_PARTICLE_MIN_BLOCKS) mvs_particle_k
             out[6 * H + pair] = make_double2(fa.x, acc.x);
             out[7 * H + pair] = make_double2(fa.y, acc.y);
             out[8 * H + pair] = make_double2(fa.z, acc.z);
+            if (A.rows_x) {
+                // rows in particle order for the copy back to the host
+                const int i0 = A.perm[j0];
+                A.rows_x[3 * (size_t)i0] = fx.x;
+                A.rows_x[3 * (size_t)i0 + 1] = fx.y;
+                A.rows_x[3 * (size_t)i0 + 2] = fx.z;
+                A.rows_v[3 * (size_t)i0] = fv.x;
+                A.rows_v[3 * (size_t)i0 + 1] = fv.y;
+                A.rows_v[3 * (size_t)i0 + 2] = fv.z;
+                if (j0 + 1 < A.np) {
+                    const int i1 = A.perm[j0 + 1];
+                    A.rows_x[3 * (size_t)i1] = x.x;
+                    A.rows_x[3 * (size_t)i1 + 1] = x.y;
+                    A.rows_x[3 * (size_t)i1 + 2] = x.z;
+                    A.rows_v[3 * (size_t)i1] = v.x;
+                    A.rows_v[3 * (size_t)i1 + 1] = v.y;
+                    A.rows_v[3 * (size_t)i1 + 2] = v.z;
+                }
+            }
         }
     }
 }

@@ -89,6 +89,9 @@ struct MvsParticleArgs {
     EncounterCandidate* cands;
     int cand_cap;
     DeviceStatus* status;
+    int* tiles;         // the launch's work counter, zeroed before it (null: status->next_tile)
+    double* rows_x;     // also the end states as host rows (3 per particle, by particle index), or null
+    double* rows_v;
 };
 
 // Output corrector mco_mvs2h / mco_h2mvs (mercury6_2.for:2107-2227,

@@ -113,10 +113,7 @@ class ShardedRun:
         self.n = 0
         self.local_events = 0
 
-    def upload(self, shard: System, ids: np.ndarray, n_total: int, ngflag: int | None = None) -> None:
-        """This rank's shard and the global 0-based index of each of its bodies
-        (Big bodies first, the same on every rank); n_total bodies in all.
-        ngflag: the input's force-law flag (None: derived from shard.ngf)."""
+    def _adopt(self, shard: System, ids: np.ndarray, n_total: int) -> None:
         ids = np.asarray(ids, dtype=np.int64)
         if len(ids) != shard.n or np.any(ids[:shard.nbig] != np.arange(shard.nbig)):
             raise ValueError("a shard holds every Big body first, then its particles")
@@ -127,7 +124,22 @@ class ShardedRun:
         seen = self.ranks.gather((self.nbig, self.n), everywhere=True)
         if any(s != seen[0] for s in seen):
             raise ValueError("ranks disagree on the Big bodies or the body count")
+
+    def upload(self, shard: System, ids: np.ndarray, n_total: int, ngflag: int | None = None) -> None:
+        """This rank's shard and the global 0-based index of each of its bodies
+        (Big bodies first, the same on every rank); n_total bodies in all.
+        ngflag: the input's force-law flag (None: derived from shard.ngf)."""
+        self._adopt(shard, ids, n_total)
         self.backend.upload(shard, ngflag)
+
+    def run(self, shard: System, ids: np.ndarray, n_total: int, time: float, h: float, nsteps: int, rcen: float,
+            steps_per_launch: int = 0, ngflag: int | None = None, out=None):
+        """upload + advance + this rank's own states back in one library call
+        per rank (Backend.mvs_run: the copies overlap the steps). Returns
+        (records as advance returns them, (x, v) of this rank's shard)."""
+        self._adopt(shard, ids, n_total)
+        events, steps, x, v = self.backend.mvs_run(shard, time, h, nsteps, rcen, steps_per_launch, ngflag, out)
+        return self._collect(events, steps), (x, v)
 
     def _to_global(self, events: np.ndarray) -> np.ndarray:
         """The records with global ids, in place (the array is the backend's
@@ -138,6 +150,10 @@ class ShardedRun:
 
     def advance(self, time: float, h: float, nsteps: int, rcen: float, steps_per_launch: int = 0):
         events, steps = self.backend.mvs_advance(time, h, nsteps, rcen, steps_per_launch)
+        return self._collect(events, steps)
+
+    def _collect(self, events: np.ndarray, steps: np.ndarray):
+        """This rank's records of a run as the whole system's, on rank 0."""
         self.local_events = len(events)   # records read back from this rank's device
         events = self._to_global(events)
         if self.ranks.rank != 0:
