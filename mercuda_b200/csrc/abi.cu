@@ -1764,10 +1764,16 @@ int last_massive(const double* m, int n, int nbig) {
     return last >= 0 ? last + 1 : nbig;
 }
 
+void upload_layout_for(int n, int nbig, int nmass, int pn, int ngflag, const double* m, const double* jcen);
+
 void upload_layout(int n, int nbig, int pn, int ngflag, const double* m, const double* jcen) {
+    upload_layout_for(n, nbig, last_massive(m, n, nbig), pn, ngflag, m, jcen);
+}
+
+// The layout for a massive set that ends at nmass (last_massive).
+void upload_layout_for(int n, int nbig, int nmass, int pn, int ngflag, const double* m, const double* jcen) {
     Context& c = ctx();
     cudaStream_t s = c.stream;
-    const int nmass = last_massive(m, n, nbig);
     // MVS: massive Small bodies move as test particles and act on nothing
     // but the central body's oblateness reaction (mfo_mvs,
     // mercury6_2.for:5061-5068); the Big-body CTA holds them (up to 512
@@ -1844,6 +1850,7 @@ void upload_layout(int n, int nbig, int pn, int ngflag, const double* m, const d
 // (particle indices, slots in the same range) into the device layout
 // through the slot map: x and v rows (3 per body) into the state, the
 // masses and radii, the ngf rows (5 per body) when a force law reads them.
+// sm null: the particles' masses are zero (their rows stay as zeroed).
 void scatter_staged(const double* sx, const double* sv, const double* sm, const double* sr, const double* sp,
                     const double* sg, bool big, int plo, int phi, cudaStream_t s) {
     Context& c = ctx();
@@ -1869,7 +1876,8 @@ void scatter_staged(const double* sx, const double* sv, const double* sm, const 
                      c.npcap, inv, s);
     const double* scalars[3] = {sm, sr, sp};
     double* pdst[3] = {c.pm(), c.prce(), c.prphys()};
-    for (int q = 0; q < 3; ++q) scatter_rows(scalars[q] + r0, cnt, 1, 0, nullptr, 0, pdst[q], c.npcap, inv, s);
+    for (int q = 0; q < 3; ++q)
+        if (scalars[q]) scatter_rows(scalars[q] + r0, cnt, 1, 0, nullptr, 0, pdst[q], c.npcap, inv, s);
     if (sg) scatter_rows(sg + 5 * r0, cnt, 5, 0, nullptr, 0, c.pngf(), c.npcap, inv, s);
 }
 
@@ -2591,26 +2599,24 @@ int mercury_b200_mvs_advance(double time, double h, int nsteps, double rcen, int
     }
 }
 
-// Particles per chunk of mercury_b200_mvs_run (at least; at most 8 chunks).
-#ifndef MB200_RUN_CHUNK_PARTICLES
-#define MB200_RUN_CHUNK_PARTICLES (1 << 17)
+// mercury_b200_mvs_run splits the particles into RUN_PARTS parts of at least
+// RUN_PART_MIN particles each (else the calls are made in turn).
+#ifndef MB200_RUN_PARTS
+#define MB200_RUN_PARTS 2
 #endif
-constexpr int RUN_CHUNK_PARTICLES = MB200_RUN_CHUNK_PARTICLES;
-// Particle launches of mercury_b200_mvs_run (each over whole chunks).
-#ifndef MB200_RUN_LAUNCHES
-#define MB200_RUN_LAUNCHES 2
-#endif
-constexpr int RUN_LAUNCHES = MB200_RUN_LAUNCHES;
+constexpr int RUN_PARTS = MB200_RUN_PARTS;
+constexpr int RUN_PART_MIN = 1 << 17;
 
 // Upload, nsteps fused MVS steps and download in one call: the same as
 // mercury_cuda_upload, mercury_b200_mvs_advance and mercury_cuda_download
 // (previous = 0), with the particles' copies overlapped with their steps
-// when the run is one launch and the host arrays are page-locked. The Big
-// bodies go first and take their steps while the particles are copied in
-// chunks; each chunk is put in slot order within its own slots and stepped
-// as soon as it is in, and its end states (written as host rows by the
-// particle kernel) go back while the next chunk is stepped. Otherwise the
-// three calls are made one after the other.
+// when the run is one launch, the host arrays are page-locked and the Small
+// bodies massless. The Big bodies go first and take their steps while the
+// particles are copied in a few parts; each part is put in slot order within
+// its own slots and stepped as soon as it is in (the next part is copied
+// meanwhile), and its end states (written as host rows by the particle
+// kernel) go back while the next part is stepped. Otherwise the three calls
+// are made one after the other.
 int mercury_b200_mvs_run(int n, int nbig, int pn, int ngflag, const double* m, const double* xx, const double* vv,
                          const double* ng, const double* jcen, const double* limits, const double* radii,
                          double time, double h, int nsteps, double rcen, int steps_per_launch, double* xout,
@@ -2630,8 +2636,9 @@ int mercury_b200_mvs_run(int n, int nbig, int pn, int ngflag, const double* m, c
         int K = steps_per_launch > 0 ? steps_per_launch : (c.steps_per_launch > 0 ? c.steps_per_launch : 0);
         if (K <= 0) K = mvs_max_steps_per_launch(nb);
         K = std::min(K, mvs_max_steps_per_launch(nb));
-        const int nchunk = std::min(8, (n - nbig) / RUN_CHUNK_PARTICLES);
-        bool pinned = nchunk > 1 && K >= nsteps;
+        const int np0 = n - nbig;
+        const int nparts = np0 >= RUN_PARTS * RUN_PART_MIN ? RUN_PARTS : 1;
+        bool pinned = nparts > 1 && K >= nsteps;
         for (const void* p : {(const void*)xx, (const void*)vv, (const void*)m, (const void*)limits,
                               (const void*)radii, (const void*)xout, (const void*)vout})
             pinned = pinned && host_pinned(p);
@@ -2662,31 +2669,28 @@ int mercury_b200_mvs_run(int n, int nbig, int pn, int ngflag, const double* m, c
                     for (cudaStream_t q : ss) cudaStreamSynchronize(q);
             }
         } drain{{s, sin, sout, sbig}};
-        // chunk boundaries in particle indices (slots in the same ranges),
-        // multiples of 64 slots, for the particles after the Big bodies (a
-        // massive Small body moves the split: then the calls in turn)
-        const int np0 = n - nbig;
-        std::vector<int> lo(nchunk + 1);
-        for (int k = 0; k <= nchunk; ++k) lo[k] = k == nchunk ? np0 : (int)(((long long)k * np0 / nchunk) & ~63LL);
+        // part boundaries in particle indices (slots in the same ranges),
+        // multiples of 64 slots, for the particles after the Big bodies
+        std::vector<int> lo(nparts + 1);
+        for (int q = 0; q <= nparts; ++q) lo[q] = q == nparts ? np0 : (int)(((long long)q * np0 / nparts) & ~63LL);
         int cap = 0;
-        for (int k = 0; k < nchunk; ++k) cap = std::max(cap, lo[k + 1] - lo[k]);
-        // events: run_in[k + 1] chunk k copied in, run_in[0] the Big bodies'
-        // rows; run_done[q] launch q stepped, run_done[E] the Big bodies
-        // stepped, run_done[E + 1] every chunk laid out
-        const int E = std::max(nchunk, RUN_LAUNCHES);
-        if ((int)c.run_in.size() < E + 2) {
+        for (int q = 0; q < nparts; ++q) cap = std::max(cap, lo[q + 1] - lo[q]);
+        // events: run_in[q + 1] part q copied in, run_in[0] the Big bodies'
+        // rows; run_done[q] part q stepped, run_done[nparts] the Big bodies
+        if ((int)c.run_in.size() < nparts + 1) {
             const size_t old = c.run_in.size();
-            c.run_in.resize(E + 2);
-            c.run_done.resize(E + 2);
-            for (size_t k = old; k < (size_t)E + 2; ++k) {
+            c.run_in.resize(nparts + 1);
+            c.run_done.resize(nparts + 1);
+            for (size_t k = old; k < (size_t)nparts + 1; ++k) {
                 check(cudaEventCreateWithFlags(&c.run_in[k], cudaEventDisableTiming), "event");
                 check(cudaEventCreateWithFlags(&c.run_done[k], cudaEventDisableTiming), "event");
             }
         }
         // copies in first (the earlier calls have drained every stream, so
-        // the stage is free): the Big bodies' rows, then every chunk's; the
-        // host's scan and the layout below run while they fly
-        auto rows_in = [&](size_t r0, size_t r1) {
+        // the stage is free): the Big bodies' rows, then every part's; the
+        // host's scan and the layout below run while they fly (the masses of
+        // the Big bodies only: a massless particle needs none)
+        auto rows_in = [&](size_t r0, size_t r1, bool mass) {
             auto h2d_rows = [&](double* dst, const double* src, size_t width) {
                 check(cudaMemcpyAsync(dst + r0 * width, src + r0 * width, sizeof(double) * width * (r1 - r0),
                                       cudaMemcpyHostToDevice, sin),
@@ -2694,23 +2698,28 @@ int mercury_b200_mvs_run(int n, int nbig, int pn, int ngflag, const double* m, c
             };
             h2d_rows(sx, xx, 3);
             h2d_rows(sv, vv, 3);
-            h2d_rows(sm, m, 1);
+            if (mass) h2d_rows(sm, m, 1);
             h2d_rows(sr, limits, 1);
             h2d_rows(sp, radii, 1);
             if (ngf_read) h2d_rows(sg, ng, 5);
         };
-        rows_in(0, nbig);
+        rows_in(0, nbig, true);
         check(cudaEventRecord(c.run_in[0], sin), "event");
-        for (int k = 0; k < nchunk; ++k) {
-            rows_in(nbig + (size_t)lo[k], nbig + (size_t)lo[k + 1]);
-            check(cudaEventRecord(c.run_in[k + 1], sin), "event");
+        for (int q = 0; q < nparts; ++q) {
+            rows_in(nbig + (size_t)lo[q], nbig + (size_t)lo[q + 1], false);
+            check(cudaEventRecord(c.run_in[q + 1], sin), "event");
         }
-        upload_layout(n, nbig, pn, ngflag, m, jcen);
-        if (c.nsplit != nbig) {
-            check(cudaStreamSynchronize(sin), "upload");
-            drain.armed = false;
-            return in_turn();
-        }
+        // the layout for massless particles; the host's scan of the masses
+        // runs beside the queueing below and is checked at the end
+        struct Scan {
+            int nmass = -1;
+            std::thread th;
+            ~Scan() {
+                if (th.joinable()) th.join();
+            }
+        } scan;
+        scan.th = std::thread([&scan, m, n, nbig] { scan.nmass = last_massive(m, n, nbig); });
+        upload_layout_for(n, nbig, nbig, pn, ngflag, m, jcen);
         const int ns = c.nsplit, np = c.np;
         // every buffer that may be reallocated (cudaFree waits for the device)
         {
@@ -2722,8 +2731,8 @@ int mercury_b200_mvs_run(int n, int nbig, int pn, int ngflag, const double* m, c
         }
         ensure_tables(nsteps + 1, nsteps);
         order_chunk(0, 0, 0, cap, m[0], sx, sv, s);   // sizes the ordering scratch
-        c.run_tiles.reserve(RUN_LAUNCHES);
-        check(cudaMemsetAsync(c.run_tiles.p, 0, sizeof(int) * RUN_LAUNCHES, s), "memset");
+        c.run_tiles.reserve(nparts);
+        check(cudaMemsetAsync(c.run_tiles.p, 0, sizeof(int) * nparts, s), "memset");
         // the Big bodies' steps, while the particles come in
         check(cudaStreamWaitEvent(s, c.run_in[0], 0), "wait");
         scatter_staged(sx, sv, sm, sr, sp, sg, true, 0, 0, s);
@@ -2731,29 +2740,19 @@ int mercury_b200_mvs_run(int n, int nbig, int pn, int ngflag, const double* m, c
         check(cudaEventRecord(c.t0, s), "event");
         check(cudaStreamWaitEvent(sbig, c.t0, 0), "wait");
         launch_mvs_big(big_args(0, 1, nsteps, 1, 1, 0, h, rcen, c.tab.p, c.detail.p), sbig);
-        check(cudaEventRecord(c.run_done[E], sbig), "event");
-        // each chunk in slot order and laid out as soon as it is in (while
-        // the next is copied)
-        for (int k = 0; k < nchunk; ++k) {
-            const int pad = (k == nchunk - 1 && c.npcap > np) ? 1 : 0;
-            check(cudaStreamWaitEvent(s, c.run_in[k + 1], 0), "wait");
-            order_chunk(lo[k], lo[k + 1], pad, cap, m[0], sx, sv, s);
-            scatter_staged(sx, sv, sm, sr, sp, sg, false, lo[k], lo[k + 1], s);
-        }
-        check(cudaStreamWaitEvent(s, c.run_done[E], 0), "wait");
-        check(cudaEventRecord(c.run_done[E + 1], s), "event");
-        // the particles' steps in a few launches on two streams, back to back
-        // (a launch's grid fills in as the one before drains), each launch's
-        // end states (written as host rows by the kernel) going back while the
-        // next is stepped
+        check(cudaEventRecord(c.run_done[nparts], sbig), "event");
+        // each part, once in: put in slot order, laid out, stepped; its end
+        // states (written as host rows by the kernel) go back while the next
+        // part is laid out and stepped
         double* rx = c.transfer.p;
         double* rv = c.transfer.p + 3 * N;
-        for (int q = 0; q < RUN_LAUNCHES; ++q) {
-            const int plo = lo[(size_t)q * nchunk / RUN_LAUNCHES], phi = lo[(size_t)(q + 1) * nchunk / RUN_LAUNCHES];
-            const int cnt = phi - plo;
-            if (cnt <= 0) continue;
-            cudaStream_t sq = q % 2 == 0 ? s : sbig;
-            if (q % 2 == 1) check(cudaStreamWaitEvent(sq, c.run_done[E + 1], 0), "wait");
+        for (int q = 0; q < nparts; ++q) {
+            const int plo = lo[q], phi = lo[q + 1], cnt = phi - plo;
+            const int pad = (q == nparts - 1 && c.npcap > np) ? 1 : 0;
+            check(cudaStreamWaitEvent(s, c.run_in[q + 1], 0), "wait");
+            order_chunk(plo, phi, pad, cap, m[0], sx, sv, s);
+            scatter_staged(sx, sv, nullptr, sr, sp, sg, false, plo, phi, s);
+            if (q == 0) check(cudaStreamWaitEvent(s, c.run_done[nparts], 0), "wait");
             MvsParticleArgs pa = particle_args(0, 1, nsteps, 1, 1, 0, h, rcen, c.tab.p, c.detail.p);
             pa.np = cnt;
             pa.xin += plo;
@@ -2766,8 +2765,8 @@ int mercury_b200_mvs_run(int n, int nbig, int pn, int ngflag, const double* m, c
             pa.tiles = c.run_tiles.p + q;
             pa.rows_x = rx + 3 * (size_t)ns;
             pa.rows_v = rv + 3 * (size_t)ns;
-            launch_mvs_particles(pa, sq, c.particle_threads);
-            check(cudaEventRecord(c.run_done[q], sq), "event");
+            launch_mvs_particles(pa, s, c.particle_threads);
+            check(cudaEventRecord(c.run_done[q], s), "event");
             check(cudaStreamWaitEvent(sout, c.run_done[q], 0), "wait");
             const size_t r0 = ns + (size_t)plo;
             check(cudaMemcpyAsync(xout + 3 * r0, rx + 3 * r0, sizeof(double) * 3 * cnt, cudaMemcpyDeviceToHost, sout),
@@ -2775,8 +2774,7 @@ int mercury_b200_mvs_run(int n, int nbig, int pn, int ngflag, const double* m, c
             check(cudaMemcpyAsync(vout + 3 * r0, rv + 3 * r0, sizeof(double) * 3 * cnt, cudaMemcpyDeviceToHost, sout),
                   "download");
         }
-        for (int q = 1; q < RUN_LAUNCHES; q += 2) check(cudaStreamWaitEvent(s, c.run_done[q], 0), "wait");
-        // the pair records of every chunk, the Big bodies' rows out
+        // the pair records of every part, the Big bodies' rows out
         ClassifyArgs ca{};
         ca.nb = nb;
         ca.nbig = nbig;
@@ -2797,9 +2795,11 @@ int mercury_b200_mvs_run(int n, int nbig, int pn, int ngflag, const double* m, c
         check(cudaMemcpyAsync(vout, rv, sizeof(double) * 3 * ns, cudaMemcpyDeviceToHost, s), "download");
         check(cudaGetLastError(), "launch");
         check(cudaEventRecord(c.t1, s), "event");
+        scan.th.join();
         drain.armed = false;
         for (cudaStream_t q : {sin, sout, sbig}) check(cudaStreamSynchronize(q), "step");
         read_status();
+        if (scan.nmass != nbig) return in_turn();   // a massive Small body
         c.steps_since_order = 0;
         c.cur = 1;
         c.stepped = false;
@@ -2815,8 +2815,8 @@ int mercury_b200_mvs_run(int n, int nbig, int pn, int ngflag, const double* m, c
             return rc ? rc : mercury_cuda_download(xout, vout, 0);
         }
         check(cudaEventElapsedTime(&c.last_advance_ms, c.t0, c.t1), "timer");
-        c.last_particle_launches = RUN_LAUNCHES;
-        c.last_kernel_launches = 1 + 10 * nchunk + RUN_LAUNCHES + 3;
+        c.last_particle_launches = nparts;
+        c.last_kernel_launches = 1 + 11 * nparts + 3;
         c.nforces += nsteps + 1;
         c.reset = false;
         const int nev = c.status_host->events;

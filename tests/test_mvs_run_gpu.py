@@ -81,7 +81,7 @@ def test_run_with_nongravitational_forces_and_oblateness(backend):
 def test_run_event_buffer_overflow_is_redone(backend, cuda_lib):
     """More records than the first guess of the buffer: the run is made again
     from the uploaded states with room, and nothing is dropped."""
-    sys0 = make_system(seed=4, n_particles=140_000, near_fraction=0.1, planet_kw=dict(mmin=1e-3, mmax=1e-3))
+    sys0 = make_system(seed=4, n_particles=300_000, near_fraction=0.05, planet_kw=dict(mmin=1e-3, mmax=1e-3))
     ev0, st0, x0, v0 = three_calls(backend, sys0, 2, 8.0, 0.005)
     s = pinned_system(sys0)
     out = (pinned(np.zeros((s.n, 3))), pinned(np.zeros((s.n, 3))))
