@@ -81,6 +81,12 @@ int mercury_b200_encode_ce(const MercuryEvent* events, int n, double mcen, doubl
  * the particles lists the Big bodies that any process found in an encounter
  * (their subsystem end states) besides its own members. */
 int mercury_b200_hybrid_members(const int* ids, int count);
+/* Between mercury_cuda_hybrid_begin and _finish: the bodies whose rows
+ * hybrid_finish takes (ascending 0-based indices, the central body left out:
+ * the members that hybrid_begin's pairs named, or the set given to
+ * mercury_b200_hybrid_members). Copies up to cap of them into ids and returns
+ * their number, or -1 outside a HYBRID step. */
+int mercury_b200_hybrid_member_list(int* ids, int cap);
 /* mdt_hkce's substep loop (mercury6_2.for:3884-3937) over the active
  * encounter subsystem, inside the library: from local time 0 to h, BS2
  * substeps (mercury_cuda_reset + mercury_cuda_step, dtflag 1 then 2) of

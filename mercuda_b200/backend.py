@@ -54,7 +54,8 @@ EXTENSION_SYMBOLS = ["mercury_b200_mvs_advance", "mercury_b200_mvs_run", "mercur
                      "mercury_b200_hybrid_adjoint_backward", "mercury_b200_hybrid_adjoint_timing",
                      "mercury_b200_hybrid_adjoint_free", "mercury_b200_ejections",
                      "mercury_b200_encode_ce", "mercury_b200_set_step_reduce",
-                     "mercury_b200_encounter_run", "mercury_b200_hybrid_members", "mercury_b200_epoch_order",
+                     "mercury_b200_encounter_run", "mercury_b200_hybrid_members", "mercury_b200_hybrid_member_list",
+                     "mercury_b200_epoch_order",
                      "mercury_b200_sync_epochs", "mercury_b200_set_event_capacity"]
 
 # fn(values, count, user) of mercury_b200_set_step_reduce
@@ -108,6 +109,7 @@ def load_library(path: Path | str | None = None) -> C.CDLL:
     L.mercury_b200_set_event_capacity.argtypes = [C.c_int]
     L.mercury_b200_encounter_run.argtypes = [D, D, D, D, PD, PI64, PI]
     L.mercury_b200_hybrid_members.argtypes = [PI, I]
+    L.mercury_b200_hybrid_member_list.argtypes = [PI, I]
     L.mercury_b200_epoch_order.argtypes = [I, PD, D, PI]
     L.mercury_b200_sync_epochs.argtypes = [PD, PD, D, D, D, PI]
     L.mercury_b200_batch_upload.argtypes = [I, PI, PI, PD, PD, PD, PD, PD, PD]
@@ -276,6 +278,17 @@ class Backend:
         self.forces += nf.value
         return ce, pi[:count.value].copy(), pj[:count.value].copy()
 
+    def hybrid_member_list(self) -> np.ndarray:
+        """The bodies (0-based, ascending, no central body) whose rows
+        hybrid_finish takes in the current HYBRID step."""
+        count = self.lib.mercury_b200_hybrid_member_list(None, 0)
+        if count < 0:
+            raise BackendError("no HYBRID step begun")
+        ids = np.empty(count, dtype=np.int32)
+        if count:
+            self.lib.mercury_b200_hybrid_member_list(ids.ctypes.data_as(PI), count)
+        return ids.astype(np.int64)
+
     def hybrid_finish(self, h: float, m: np.ndarray, x: np.ndarray, v: np.ndarray) -> None:
         nf = C.c_int64(0)
         if self.lib.mercury_cuda_hybrid_finish(h, _p(m), _p(x), _p(v), C.byref(nf)) != 0:
@@ -304,7 +317,9 @@ class Backend:
         state["dtflag"] = 2
         events = np.zeros(0, dtype=EVENT_DTYPE)
         if len(pi):
-            sub = np.concatenate([[0], np.nonzero(ce[1:])[0] + 1])
+            # the members as the library collected them from the pairs (the
+            # bodies that ce flags, without a scan of ce)
+            sub = np.concatenate([[0], self.hybrid_member_list()])
             xbs, vbs, events = self.encounter_subsystem(sub, sys.nbig, sys.m[sub], x[sub], v[sub], sys.rcrit[sub],
                                                          sys.rce[sub], sys.rphys[sub], pi, pj, time, h, tol, state,
                                                          rcen, fused)

@@ -1722,6 +1722,25 @@ void upload_checks(int n, int nbig) {
 // The upload's layout of a system on the device: the massive set, every
 // buffer's size, zeroed states and constants (on the library stream). The
 // host rows are not read here except for the masses.
+// Whether a[0..n) and b[0..n) hold the same bytes (compared on up to 16 host
+// threads for large n).
+bool same_doubles(const double* a, const double* b, size_t n) {
+    const size_t nthreads =
+        n < ((size_t)1 << 18) ? 1 : std::max<size_t>(1, std::min<size_t>(16, std::thread::hardware_concurrency()));
+    if (nthreads == 1) return std::memcmp(a, b, sizeof(double) * n) == 0;
+    std::vector<char> diff(nthreads, 0);
+    std::vector<std::thread> pool;
+    const size_t chunk = (n + nthreads - 1) / nthreads;
+    for (size_t t = 0; t < nthreads; ++t) {
+        const size_t lo = std::min(n, t * chunk), hi = std::min(n, lo + chunk);
+        pool.emplace_back([&, t, lo, hi] { diff[t] = std::memcmp(a + lo, b + lo, sizeof(double) * (hi - lo)) != 0; });
+    }
+    for (auto& th : pool) th.join();
+    for (char d : diff)
+        if (d) return false;
+    return true;
+}
+
 // One past the last body at or after nbig whose mass is not zero (nbig if
 // none). m[j] != 0.0 is the bits without the sign bit being non-zero (a NaN
 // counts as massive, -0.0 as massless); blocks of 512 are tested by OR-ing
@@ -2322,7 +2341,7 @@ int mercury_cuda_hybrid_finish(double h, const double* m, const double* xx, cons
             scatter_members(c.hy_ids.p, nm, c.hy_packed.p, c.bigstate[out].p, c.pstate[out].p);
             c.dropin_launches += 1;
             // the masses (changed only where the host merged bodies)
-            if (c.m_host.size() != (size_t)c.n || std::memcmp(m, c.m_host.data(), sizeof(double) * c.n) != 0) {
+            if (c.m_host.size() != (size_t)c.n || !same_doubles(m, c.m_host.data(), (size_t)c.n)) {
                 c.transfer.reserve((size_t)6 * c.n);
                 check(cudaMemcpyAsync(c.transfer.p, m, sizeof(double) * c.n, cudaMemcpyHostToDevice, c.stream),
                       "upload");
@@ -2996,6 +3015,14 @@ int mercury_b200_ejections(double h, int physical, double rmax, int i0, int* ids
     } catch (const std::exception& e) {
         return report(e);
     }
+}
+
+int mercury_b200_hybrid_member_list(int* ids, int cap) {
+    Context& c = ctx();
+    if (!c.hy_begun) return -1;
+    const int nm = (int)c.hy_members.size();
+    if (ids && cap > 0) std::memcpy(ids, c.hy_members.data(), sizeof(int) * (size_t)std::min(cap, nm));
+    return nm;
 }
 
 int mercury_b200_hybrid_members(const int* ids, int count) {
