@@ -76,11 +76,11 @@ BYTES_PER_PARTICLE_STEP = 96.0
 # launch of the particle kernel on this 1M-particle workload, by steps per
 # launch, from ncu captures of this bench's own command (the launch list and
 # traffic summary of the particle kernel are kept beside the sources).
-TRAFFIC_MB_PER_LAUNCH = {31: (99.764224, 157.014528), 20: (99.714304, 127.000576)}
+TRAFFIC_MB_PER_LAUNCH = {31: (99.764224, 157.014528), 20: (99.714304, 127.000576), 16: (98.81728, 89.934336)}
 # The FP64 pipe of the same captures: sm__pipe_fp64_cycles_active (fraction
 # of peak sustained), sm__inst_executed_pipe_fp64 per particle-step (warp
 # instructions x 32), smsp__issue_active (fraction), by steps per launch.
-FP64_PIPE_BY_K = {20: (0.4949, 730.4, 0.5463)}
+FP64_PIPE_BY_K = {20: (0.4949, 730.4, 0.5463), 16: (0.5006, 729.3, 0.5403)}
 CLOCK_QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
                "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -1178,9 +1178,10 @@ def main():
     ms = tm["advance_ms"]
     ms = ranks.max(ms)
     value = world * args.particles * args.steps / (ms * 1e-3)
-    launches = tm["particle_launches"]
-    kernel_ms = tm["particle_kernel_ms"] / max(1, launches)
-    steps_per_launch = -(-args.steps // max(1, launches))
+    # the roofline of the run's longest launch (the first is short so that the
+    # next launch's Big-body steps run beside its particles)
+    launch_list = b.advance_launches()
+    steps_per_launch, kernel_ms = max(launch_list) if launch_list else (args.steps, tm["particle_kernel_ms"])
     flops_per_launch = FLOPS_PER_PARTICLE_STEP * args.particles * steps_per_launch
     achieved = flops_per_launch / (kernel_ms * 1e-3) / 1e12
     clk = clocks.summary()
@@ -1251,7 +1252,8 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": config_of(args, MVS_TEXT.format(n=args.particles), h_days=H, l2=MVS_L2),
-            "run": {"steps_per_launch": steps_per_launch, "threads_per_cta": args.threads or 128},
+            "run": {"steps_per_launch": steps_per_launch, "launch_steps": [k for k, _ in launch_list],
+                    "threads_per_cta": args.threads or 128},
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak_tflops, "unit": "TFLOP/s",
                          "frac": achieved / peak_tflops,
                          "traffic": (sum(TRAFFIC_MB_PER_LAUNCH[steps_per_launch]) * args.particles

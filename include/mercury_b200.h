@@ -36,6 +36,9 @@ int mercury_b200_events(MercuryEvent* events, int* steps, int cap);
  * of kernels it launched on all streams. */
 int mercury_b200_timing(double* advance_ms, double* particle_kernel_ms, int* particle_launches,
                         int* kernel_launches);
+/* The launches of the last mercury_b200_mvs_advance: up to cap of their step
+ * counts and particle-kernel times (ms, CUDA events); returns their number. */
+int mercury_b200_advance_launches(int* steps, double* kernel_ms, int cap);
 /* Device time (CUDA events on the library's streams) spent in the drop-in
  * mercury_cuda_step, mercury_cuda_events and mercury_cuda_hybrid_begin/_finish
  * calls of the resident system and the encounter subsystem, and the number of

@@ -44,7 +44,8 @@ DROP_IN_SYMBOLS = [
     "mercury_cuda_encounter_enter", "mercury_cuda_encounter_update", "mercury_cuda_encounter_exit",
     "mercury_cuda_free",
 ]
-EXTENSION_SYMBOLS = ["mercury_b200_mvs_advance", "mercury_b200_mvs_run", "mercury_b200_events", "mercury_b200_timing",
+EXTENSION_SYMBOLS = ["mercury_b200_mvs_advance", "mercury_b200_mvs_run", "mercury_b200_advance_launches",
+                     "mercury_b200_events", "mercury_b200_timing",
                      "mercury_b200_set_launch", "mercury_b200_fp64_peak", "mercury_b200_mvs_step_noalloc",
                      "mercury_b200_dropin_time", "mercury_b200_batch_upload", "mercury_b200_batch_advance",
                      "mercury_b200_batch_events", "mercury_b200_batch_download", "mercury_b200_batch_set",
@@ -99,6 +100,7 @@ def load_library(path: Path | str | None = None) -> C.CDLL:
     L.mercury_b200_mvs_run.argtypes = [I, I, I, I, PD, PD, PD, PD, PD, PD, PD, D, D, I, D, I, PD, PD, PI]
     L.mercury_b200_events.argtypes = [C.c_void_p, PI, I]
     L.mercury_b200_timing.argtypes = [PD, PD, PI, PI]
+    L.mercury_b200_advance_launches.argtypes = [PI, PD, I]
     L.mercury_b200_set_launch.argtypes = [I, I]
     L.mercury_b200_fp64_peak.argtypes = [PD, PD]
     L.mercury_b200_dropin_time.argtypes = [PD, PI64, I]
@@ -486,6 +488,14 @@ class Backend:
         self.lib.mercury_b200_timing(C.byref(a), C.byref(k), C.byref(n), C.byref(L))
         return {"advance_ms": a.value, "particle_kernel_ms": k.value, "particle_launches": n.value,
                 "kernel_launches": L.value}
+
+    def advance_launches(self):
+        """[(steps, particle-kernel ms)] of each launch of the last fused run."""
+        n = self.lib.mercury_b200_advance_launches(None, None, 0)
+        steps = np.zeros(max(1, n), dtype=np.int32)
+        ms = np.zeros(max(1, n))
+        self.lib.mercury_b200_advance_launches(steps.ctypes.data_as(PI), _p(ms), n)
+        return [(int(steps[k]), float(ms[k])) for k in range(n)]
 
     def dropin_time(self, reset: bool = False):
         """(device ms, kernels launched) of the drop-in step/events calls since the last reset."""

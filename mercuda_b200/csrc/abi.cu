@@ -181,6 +181,9 @@ __global__ void central_kernel(CentralArgs A) {
 int blocks(int n, int t = 256) { return (n + t - 1) / t; }
 int reorder_slots(int src, double h, cudaStream_t st);
 
+// Steps after which a fused run re-sorts the particle slots by drift path.
+constexpr int ORDER_EVERY = 16;
+
 bool is_mvs(int alg) { return alg == 1 || alg == 9; }
 
 // Device time of the drop-in calls (both contexts) and the kernels they
@@ -2464,10 +2467,28 @@ int mercury_b200_mvs_advance(double time, double h, int nsteps, double rcen, int
         if (nsteps < 1) throw std::runtime_error("nsteps must be positive");
         const int nb = c.nbig - 1;
         int K = steps_per_launch > 0 ? steps_per_launch : (c.steps_per_launch > 0 ? c.steps_per_launch : 0);
+        const bool auto_K = K <= 0;
         if (K <= 0) K = mvs_max_steps_per_launch(nb);
         K = std::min(K, mvs_max_steps_per_launch(nb));
         K = std::max(1, std::min(K, nsteps));
-        const int nchunks = (nsteps + K - 1) / K;
+        // launch sizes: K steps each; with the automatic choice the first launch
+        // is short, so that its Big-body steps (one CTA, serial, ~20 us a step)
+        // hold up the particles briefly and the next launch's Big-body steps run
+        // beside its particles
+        std::vector<int>& ksz = c.launch_steps;
+        ksz.clear();
+        {
+            int left = nsteps;
+            if (auto_K && nsteps >= 10) {
+                ksz.push_back(std::max(1, (K + 4) / 5));
+                left -= ksz.back();
+            }
+            while (left > 0) {
+                ksz.push_back(std::min(K, left));
+                left -= ksz.back();
+            }
+        }
+        const int nchunks = (int)ksz.size();
         const int stride = tab_stride(nb);
         ensure_tables(nsteps + nchunks, nsteps);
         // room for this run's records at the rate the earlier runs showed, so
@@ -2509,6 +2530,7 @@ int mercury_b200_mvs_advance(double time, double h, int nsteps, double rcen, int
         copy(c.snap_perm.p, c.perm[kc0].p, sizeof(int) * c.npcap);
         copy(c.snap_perm.p + c.npcap, c.inv.p, sizeof(int) * c.npcap);
         const bool reset0 = c.reset;
+        const int order0 = c.steps_since_order;
         for (int attempt = 0;; ++attempt) {
             int launches = 0;
             check(cudaMemsetAsync(c.status.p, 0, sizeof(DeviceStatus), c.stream), "memset");
@@ -2516,8 +2538,9 @@ int mercury_b200_mvs_advance(double time, double h, int nsteps, double rcen, int
             check(cudaStreamWaitEvent(c.stream_big, c.t0, 0), "wait");
             int bcur = c.cur, pcur = c.cur;
             size_t row = 0;
-            for (int ch = 0; ch < nchunks; ++ch) {
-                const int s0 = ch * K, ks = std::min(K, nsteps - s0);
+            c.steps_since_order = order0;
+            for (int ch = 0, s0 = 0; ch < nchunks; s0 += ksz[ch], ++ch) {
+                const int ks = ksz[ch];
                 const int reset = (ch == 0 && reset0) ? 1 : 0;
                 double* tab = c.tab.p + row * stride;
                 double* det = c.detail.p + (size_t)s0 * std::max(1, nb) * TAB_DETAIL;
@@ -2526,10 +2549,13 @@ int mercury_b200_mvs_advance(double time, double h, int nsteps, double rcen, int
                 check(cudaEventRecord(c.chunk_done[ch], c.stream_big), "event");
                 bcur = 1 - bcur;
                 if (c.np > 0) {
-                    // re-sort the slots by drift path before every launch (cheap
-                    // next to the launch; particles change path as they evolve)
-                    if (c.np >= 64) launches += 3;
-                    pcur = reorder_slots(pcur, h, c.stream);
+                    // re-sort the slots by drift path before a launch once 16
+                    // steps have gone by since the last order (particles change
+                    // path as they evolve, slowly)
+                    if (c.steps_since_order >= ORDER_EVERY) {
+                        if (c.np >= 64) launches += 3;
+                        pcur = reorder_slots(pcur, h, c.stream);
+                    }
                     check(cudaStreamWaitEvent(c.stream, c.chunk_done[ch], 0), "wait");
                     check(cudaEventRecord(c.kt0[ch], c.stream), "event");
                     particles_and_events(particle_args(pcur, 1 - pcur, ks, reset, 1, s0, h, rcen, tab, det), c.detail.p,
@@ -2539,6 +2565,7 @@ int mercury_b200_mvs_advance(double time, double h, int nsteps, double rcen, int
                 }
                 pcur = 1 - pcur;
                 row += ks + 1;
+                c.steps_since_order += ks;
             }
             check(cudaStreamWaitEvent(c.stream, c.chunk_done[nchunks - 1], 0), "wait");
             check(cudaEventRecord(c.t1, c.stream), "event");
@@ -2548,10 +2575,12 @@ int mercury_b200_mvs_advance(double time, double h, int nsteps, double rcen, int
             if (!c.status_host->overflow) {
                 check(cudaEventElapsedTime(&c.last_advance_ms, c.t0, c.t1), "timer");
                 double ksum = 0.0;
+                c.launch_ms.assign(nchunks, 0.0);
                 if (c.np > 0)
                     for (int ch = 0; ch < nchunks; ++ch) {
                         float ms = 0.0f;
                         check(cudaEventElapsedTime(&ms, c.kt0[ch], c.kt1[ch]), "timer");
+                        c.launch_ms[ch] = ms;
                         ksum += ms;
                     }
                 c.last_particle_kernel_ms = ksum;
@@ -2921,6 +2950,16 @@ int mercury_b200_timing(double* advance_ms, double* particle_kernel_ms, int* par
     if (particle_launches) *particle_launches = c.last_particle_launches;
     if (kernel_launches) *kernel_launches = c.last_kernel_launches;
     return 0;
+}
+
+int mercury_b200_advance_launches(int* steps, double* kernel_ms, int cap) {
+    Context& c = ctx();
+    const int n = (int)c.launch_steps.size();
+    for (int k = 0; k < std::min(n, cap); ++k) {
+        if (steps) steps[k] = c.launch_steps[k];
+        if (kernel_ms) kernel_ms[k] = k < (int)c.launch_ms.size() ? c.launch_ms[k] : 0.0;
+    }
+    return n;
 }
 
 int mercury_b200_dropin_time(double* ms, int64_t* launches, int reset) {

@@ -156,6 +156,8 @@ struct Context {
     std::vector<cudaEvent_t> chunk_done;
     cudaEvent_t t0 = nullptr, t1 = nullptr;
     std::vector<cudaEvent_t> kt0, kt1;
+    std::vector<int> launch_steps;   // steps of each launch of the last fused run
+    std::vector<double> launch_ms;   // and each launch's particle-kernel time
     // mercury_b200_mvs_run's chunks: copied in, stepped; their work counters
     std::vector<cudaEvent_t> run_in, run_done;
     DBuf<int> run_tiles;
