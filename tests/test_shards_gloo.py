@@ -46,6 +46,16 @@ class OracleBackend:
     def download(self):
         return self.s.x.copy(), self.s.v.copy()
 
+    def mvs_run(self, s, time, h, nsteps, rcen, steps_per_launch=0, ngflag=None, out=None):
+        self.upload(s, ngflag)
+        ev, st = self.mvs_advance(time, h, nsteps, rcen, steps_per_launch)
+        x, v = self.download()
+        if out is not None:
+            out[0][...] = x
+            out[1][...] = v
+            x, v = out
+        return ev, st, x, v
+
 
 def system():
     from mercuda_b200.system import make_system
@@ -82,6 +92,20 @@ def worker(rank, world, port, out_dir, case):
             else:
                 assert got is None and states is None
                 np.savez(Path(out_dir) / f"rank{rank}.npz", own_n=len(own[0]), t=t)
+        elif case == "onecall":
+            # upload + advance + own states back in one call per rank
+            s = system()
+            shard, ids = particle_shard(s, rank, world)
+            run = ShardedRun(ranks, OracleBackend(O))
+            out = (np.zeros((shard.n, 3)), np.zeros((shard.n, 3)))
+            got, (x, v) = run.run(shard, ids, s.n, 0.0, H, NSTEPS, RCEN, out=out)
+            assert x is out[0] and v is out[1]
+            if rank == 0:
+                ev, st = got
+                np.savez(Path(out_dir) / "rank0.npz", ev=ev, st=st, x=x, v=v, ids=ids)
+            else:
+                assert got is None
+                np.savez(Path(out_dir) / f"rank{rank}.npz", x=x, v=v, ids=ids)
         elif case == "reduce":
             # the adaptive step control's maxima, all-reduced through the
             # library's callback type (called here as the library calls it)
@@ -132,6 +156,23 @@ def test_sharded_run_equals_unsharded(tmp_path, oracle):
     assert float(r0["value"]) == 100.0
     npart = s.n - s.nbig
     assert int(r0["own_n"]) == s.nbig + (npart + 1) // 2 and int(r1["own_n"]) == s.nbig + npart // 2
+
+
+def test_sharded_one_call_run_equals_unsharded(tmp_path, oracle):
+    """ShardedRun.run (one upload + run + download call per rank, as the
+    bench's end-to-end leg makes it): rank 0's records are the whole
+    system's, every rank's own states are its shard's rows of an unsharded
+    run."""
+    r0, r1 = launch(tmp_path, "onecall")
+    s = system()
+    ref = s.copy()
+    rev, rst = oracle.mvs_run(ref, 0.0, H, NSTEPS, RCEN, central=True, threads=1)
+    a, ast = canonical(r0["ev"], r0["st"])
+    b, bst = canonical(rev, rst)
+    assert np.array_equal(ast, bst) and a.tobytes() == b.tobytes()
+    for r in (r0, r1):
+        ids = r["ids"]
+        assert np.array_equal(r["x"], ref.x[ids]) and np.array_equal(r["v"], ref.v[ids])
 
 
 def test_step_reduce_takes_the_maximum_over_ranks(tmp_path):
