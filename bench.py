@@ -86,6 +86,18 @@ CLOCK_QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.ac
                "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
 
+def compact_steps(steps):
+    """Launch sizes as runs: [7, 31, 31, 6] -> "7 + 2x31 + 6"."""
+    parts, k = [], 0
+    while k < len(steps):
+        j = k
+        while j < len(steps) and steps[j] == steps[k]:
+            j += 1
+        parts.append(f"{j - k}x{steps[k]}" if j - k > 1 else str(steps[k]))
+        k = j
+    return " + ".join(parts)
+
+
 def config_of(args, text, **extra):
     """The workload's config, the same dict in both arms (the reference arm
     states the sample it could time in its cpu_baseline instead)."""
@@ -1252,7 +1264,8 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": config_of(args, MVS_TEXT.format(n=args.particles), h_days=H, l2=MVS_L2),
-            "run": {"steps_per_launch": steps_per_launch, "launch_steps": [k for k, _ in launch_list],
+            "run": {"steps_per_launch": steps_per_launch, "launches": len(launch_list),
+                    "launch_steps": compact_steps([k for k, _ in launch_list]),
                     "threads_per_cta": args.threads or 128},
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak_tflops, "unit": "TFLOP/s",
                          "frac": achieved / peak_tflops,
