@@ -332,6 +332,17 @@ void particles_and_events(const MvsParticleArgs& pa, const double* detail, cudaS
     check(cudaMemsetAsync(&pa.status->cands, 0, sizeof(int), s), "memset");
 }
 
+// Candidate room for a launch of `steps` steps: box overlaps run at 2-4 % of
+// the particles per step on a system with 1 % of its particles near planets,
+// so steps x np / 25, kept from one run to the next (not with a fixed
+// starting capacity set for tests, which exercise the overflow path).
+void ensure_candidates(int steps) {
+    Context& c = ctx();
+    if (g_event_cap > 0) return;
+    const size_t want = (size_t)std::max(1, steps) * (size_t)c.np / 25 + 16384;
+    if (c.cands.n < want) c.cands.reserve(want);
+}
+
 // Grows the event or candidate buffer after an overflow flagged in the status.
 void grow_after_overflow() {
     Context& c = ctx();
@@ -1846,7 +1857,7 @@ void upload_layout_for(int n, int nbig, int nmass, int pn, int ngflag, const dou
         c.cands.reserve(g_event_cap);
     } else {
         ensure_events(std::max(4096, c.np / 64));
-        c.cands.reserve(std::max(16384, c.np / 2));
+        c.cands.reserve(std::max(16384, c.np));
     }
     c.transfer.reserve((size_t)6 * n);
     if (c.algorithm == 4) {
@@ -2490,6 +2501,7 @@ int mercury_b200_mvs_advance(double time, double h, int nsteps, double rcen, int
         }
         const int nchunks = (int)ksz.size();
         const int stride = tab_stride(nb);
+        ensure_candidates(*std::max_element(ksz.begin(), ksz.end()));
         ensure_tables(nsteps + nchunks, nsteps);
         // room for this run's records at the rate the earlier runs showed, so
         // that a long run is not redone after an event-buffer overflow
@@ -2778,6 +2790,7 @@ int mercury_b200_mvs_run(int n, int nbig, int pn, int ngflag, const double* m, c
                 ensure_events((int)want);
         }
         ensure_tables(nsteps + 1, nsteps);
+        ensure_candidates(nsteps);   // every part's candidates before the one classification
         order_chunk(0, 0, 0, cap, m[0], sx, sv, s);   // sizes the ordering scratch
         c.run_tiles.reserve(nparts);
         check(cudaMemsetAsync(c.run_tiles.p, 0, sizeof(int) * nparts, s), "memset");
