@@ -76,11 +76,11 @@ BYTES_PER_PARTICLE_STEP = 96.0
 # launch of the particle kernel on this 1M-particle workload, by steps per
 # launch, from ncu captures of this bench's own command (the launch list and
 # traffic summary of the particle kernel are kept beside the sources).
-TRAFFIC_MB_PER_LAUNCH = {31: (99.764224, 157.014528), 20: (99.714304, 127.000576), 16: (98.81728, 89.934336)}
+TRAFFIC_MB_PER_LAUNCH = {31: (99.764224, 157.014528), 20: (99.714304, 127.000576), 16: (99.467776, 104.21376)}
 # The FP64 pipe of the same captures: sm__pipe_fp64_cycles_active (fraction
 # of peak sustained), sm__inst_executed_pipe_fp64 per particle-step (warp
 # instructions x 32), smsp__issue_active (fraction), by steps per launch.
-FP64_PIPE_BY_K = {20: (0.4949, 730.4, 0.5463), 16: (0.5006, 729.3, 0.5403)}
+FP64_PIPE_BY_K = {20: (0.4949, 730.4, 0.5463), 16: (0.4981, 729.3, 0.5397)}
 CLOCK_QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
                "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
