@@ -314,3 +314,22 @@ def test_massive_small_bodies_particles_and_oblateness(backend, oracle):
     assert got == [(int(s), int(e["i"]), int(e["j"]), int(e["kind"])) for s, e in zip(rsteps, rev)]
     e0, l0 = backend.energy(8.0, physical=True)
     assert np.isfinite(e0) and np.isfinite(l0)
+
+
+def test_fused_run_launch_schedule(backend):
+    """The automatic launch choice makes a short first launch (so that the
+    next launch's Big-body steps run beside its particles) and re-sorts the
+    slots only after 16 steps: the records and states equal those of one
+    launch of all the steps, and the launches are reported."""
+    sys0 = make_system(seed=22, n_particles=20000, near_fraction=0.05)
+    backend.upload(sys0)
+    ev_a, st_a = backend.mvs_advance(0.0, 8.0, 20, 0.005)
+    launches = backend.advance_launches()
+    assert [k for k, _ in launches] == [4, 16] and all(ms > 0.0 for _, ms in launches)
+    xa, va = backend.download()
+    backend.upload(sys0)
+    ev_b, st_b = backend.mvs_advance(0.0, 8.0, 20, 0.005, steps_per_launch=20)
+    assert [k for k, _ in backend.advance_launches()] == [20]
+    xb, vb = backend.download()
+    assert ev_a.tobytes() == ev_b.tobytes() and np.array_equal(st_a, st_b)
+    assert np.array_equal(xa, xb) and np.array_equal(va, vb)
