@@ -320,8 +320,13 @@ class Backend:
         events = np.zeros(0, dtype=EVENT_DTYPE)
         if len(pi):
             # the members as the library collected them from the pairs (the
-            # bodies that ce flags, without a scan of ce)
-            sub = np.concatenate([[0], self.hybrid_member_list()])
+            # bodies that ce flags, without a scan of ce); a library with the
+            # drop-in calls alone (the reference's) is scanned
+            if hasattr(self.lib, "mercury_b200_hybrid_member_list"):
+                members = self.hybrid_member_list()
+            else:
+                members = np.nonzero(ce[1:])[0] + 1
+            sub = np.concatenate([[0], members])
             xbs, vbs, events = self.encounter_subsystem(sub, sys.nbig, sys.m[sub], x[sub], v[sub], sys.rcrit[sub],
                                                          sys.rce[sub], sys.rphys[sub], pi, pj, time, h, tol, state,
                                                          rcen, fused)
